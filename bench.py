@@ -1,0 +1,363 @@
+"""Benchmark: 2D vector Hodge Laplacian (delta d + d delta) on a 1-form,
+4096 x 4096 nodes, FP64, single fused pass (the DEC operator throughput
+workload), on N GPUs of one node.
+
+A step is one Laplacian of the whole 4096^2 field.  The field (268 MB in,
+268 MB out) is larger than the 126 MB L2, so consecutive steps stream from
+HBM without an explicit flush.  Multi-GPU: every rank runs its own field
+(independent problems, no collective on the data path; weak scaling); the
+timed region is bracketed by a barrier and a device synchronisation and the
+reported time is the maximum over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference algorithm's CPU path (the oracle's
+C++/OpenMP restatement, reference-structured staged chain) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_NODES = 4096
+WORKLOAD = "2D vector Hodge Laplacian (delta d + d delta) of a 1-form, 4096x4096 nodes, spacing 1/4096, FP64, fused single pass"
+METRIC = "DEC op GB/s: 2D vector Hodge Laplacian, 1-form, 4096^2, FP64"
+
+
+def algorithmic_bytes(n, es=8):
+    """Read the 1-form once (n^2 nodes x 2 comps), write the (n-1)^2 x 2 result once."""
+    return (n * n * 2 + (n - 1) * (n - 1) * 2) * es
+
+
+def cell_updates(n):
+    return (n - 1) * (n - 1)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(name):
+    """DRAM bytes per launch from a committed ncu summary (profiles/<name>), if present."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device_index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self.thread is not None:
+                self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[2:6]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_baseline(steps=1, sample_n=1024, seed=2):
+    """Oracle staged chain (stored Hodge tensors, separate passes, FP64) on a
+    sample_n^2 sample of the workload; setup (Hodge fill) excluded."""
+    import oracle as O
+    from tests.helpers import gaussian_random_field
+    w = gaussian_random_field(sample_n, seed=seed)
+    coords = [np.arange(sample_n) / N_NODES, np.arange(sample_n) / N_NODES]
+    pos = O.position_from_coords(coords)
+    st = O.StagedLaplacian(2, 1, pos)
+    out = np.zeros((sample_n - 1, sample_n - 1, 2))
+    st.run(w, out)  # warm-up
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        st.run(w, out)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    gbs = algorithmic_bytes(sample_n) / t / 1e9
+    return {"value": gbs, "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{sample_n}x{sample_n} sample of the 4096^2 1-form, reference-structured staged chain "
+                      f"(d+star, transposed d+star, star, transposed d+star, d, add), Hodge fill excluded",
+            "cell_updates_per_s": cell_updates(sample_n) / t, "seconds_per_sample": t}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle as O
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    sample_n = 1024
+    cb = None
+    for _ in range(max(args.warmup, 0)):
+        pass
+    cb = cpu_baseline(steps=max(args.steps, 1), sample_n=sample_n)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["seconds_per_sample"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded k^-2 Gaussian random field)",
+        "config": {"workload": WORKLOAD, "sample": cb["sample"], "l2": "inputs larger than L2"},
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--extras", action="store_true", help="also time the unfused chain, FP32 and the 512^2 0-form")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    import similie_b200 as sil
+    from tests.helpers import gaussian_random_field
+
+    n = N_NODES
+    w_host = gaussian_random_field(n, seed=2 + rank)
+    coords = [np.arange(n) / n, np.arange(n) / n]
+    geo = sil.Geometry(coords)
+    inp = torch.from_numpy(w_host).cuda()
+    out = torch.empty((n - 1, n - 1, 2), device="cuda", dtype=torch.float64)
+    plan = sil.make_staged_laplacian(geo, out, inp, 1)
+    assert plan.kernel == 2, "the 4096^2 FP64 1-form must take the TMA kernel"
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    for _ in range(args.warmup):
+        plan.run(out, inp)
+    torch.cuda.synchronize()
+    plan.status()
+
+    # Device-timed region: CUDA events on the launching stream around every launch.
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        t_start.record(stream)
+        for s in range(args.steps):
+            evs[s][0].record(stream)
+            plan.run(out, inp)
+            evs[s][1].record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    total_ms = t_start.elapsed_time(t_end)
+    per_launch_ms = [a.elapsed_time(b) for a, b in evs]
+    plan.status()
+    if pg is not None:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    bytes_per_step = algorithmic_bytes(n)
+    value = world * bytes_per_step * args.steps / (total_ms * 1e-3) / 1e9
+    avg_launch_ms = statistics.mean(per_launch_ms)
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_per_step / (avg_launch_ms * 1e-3) / 1e9
+    traffic = ncu_traffic("lap2d_1form_tma_4096_fp64.md")
+
+    # End to end through the public API with host buffers: pinned H2D of the
+    # input, the Laplacian, D2H of the result, every step.
+    h_in = torch.from_numpy(w_host).pin_memory()
+    h_out = torch.empty((n - 1, n - 1, 2), dtype=torch.float64).pin_memory()
+    d_in = torch.empty_like(inp)
+    d_out = torch.empty_like(out)
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        d_in.copy_(h_in, non_blocking=True)
+        plan.run(d_out, d_in)
+        h_out.copy_(d_out, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        d_in.copy_(h_in, non_blocking=True)
+        plan.run(d_out, d_in)
+        h_out.copy_(d_out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    if pg is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * bytes_per_step * e2e_steps / (e2e_ms * 1e-3) / 1e9
+
+    extras = {}
+    if args.extras and rank == 0:
+        extras = run_extras(torch, sil, geo, inp, out, args)
+
+    if rank == 0:
+        cb = None
+        if not args.no_cpu_baseline and world == 1:
+            cb = cpu_baseline(steps=1)
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded k^-2 Gaussian random field per component)",
+            "config": {"workload": WORKLOAD, "global_batch": world, "nodes_per_rank": [n, n],
+                       "parallelism": f"independent fields x{world}", "l2": "inputs larger than L2 (268 MB in + 268 MB out per step)",
+                       "kernel": "lap2d_1form_tma_kernel<double>",
+                       "cell_updates_per_s": world * cell_updates(n) * args.steps / (total_ms * 1e-3)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
+                         "traffic": traffic, "algorithmic_bytes_per_launch": bytes_per_step,
+                         "avg_launch_ms": avg_launch_ms},
+            "cpu_baseline": cb,
+            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": int(n * n * 2 * 8),
+                    "d2h_bytes_per_step": int((n - 1) * (n - 1) * 2 * 8), "steps": e2e_steps,
+                    "ms_per_step": e2e_ms / e2e_steps},
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+        }
+        if extras:
+            line["extras"] = extras
+        print(json.dumps(line))
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def run_extras(torch, sil, geo, inp, out, args):
+    """Secondary measurements (not the headline): unfused chain, FP32, 512^2 0-form."""
+    from tests.helpers import sinusoid_field
+    res = {}
+    n = N_NODES
+
+    def timed(fn, steps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps
+
+    unf = sil.make_staged_laplacian(geo, out, inp, 1, mode="unfused")
+    ms = timed(lambda: unf.run(out, inp), 10)
+    res["unfused_fp64"] = {"ms": ms, "GB/s_algorithmic": algorithmic_bytes(n) / ms / 1e6,
+                           "scratch_bytes": unf.scratch_bytes}
+    gen_ms = timed(lambda: sil.laplacian(geo, out, inp, 1), 10)
+    res["table_driven_fused_fp64"] = {"ms": gen_ms, "GB/s_algorithmic": algorithmic_bytes(n) / gen_ms / 1e6}
+    i32 = inp.float()
+    o32 = torch.empty((n - 1, n - 1, 2), device="cuda", dtype=torch.float32)
+    p32 = sil.make_staged_laplacian(geo, o32, i32, 1)
+    ms32 = timed(lambda: p32.run(o32, i32), 20)
+    res["fused_fp32"] = {"ms": ms32, "GB/s_algorithmic": algorithmic_bytes(n, 4) / ms32 / 1e6, "kernel": p32.kernel}
+    m = 512
+    phi = torch.from_numpy(sinusoid_field(m, seed=1)[..., None].copy()).cuda()
+    g2 = sil.Geometry([np.arange(m) / m, np.arange(m) / m])
+    o2 = torch.empty((m - 1, m - 1, 1), device="cuda", dtype=torch.float64)
+    p2 = sil.make_staged_laplacian(g2, o2, phi, 0)
+    ms2 = timed(lambda: p2.run(o2, phi), 50)
+    res["scalar_512_fp64"] = {"ms": ms2, "cell_updates_per_s": (m - 1) ** 2 / (ms2 * 1e-3),
+                              "GB/s_algorithmic": (m * m + (m - 1) ** 2) * 8 / ms2 / 1e6, "note": "L2 resident"}
+    return res
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+/*
+ * sil_b200.h -- C ABI of the B200 (sm_100a) discrete-exterior-calculus library.
+ *
+ * Drop-in replacement for the device path of SimiLie's exterior-calculus
+ * operators and of its 2D magnetostatics residual-minimisation solve.  Every
+ * entry point is plain C: raw device pointers, sizes and strides, no C++ or
+ * framework types.  All functions are non-throwing and return sil_status.
+ * Asynchronous functions enqueue on the given CUDA stream (NULL = legacy
+ * default stream) and return once enqueued; the caller synchronises, as a
+ * SimiLie caller fences its Kokkos execution space.
+ *
+ * Fields follow SimiLie's DDC tensor-field layout: up to SIL_MAX_DIMS lattice
+ * dimensions with explicit element strides plus one form-component index.
+ * `front` is the absolute discrete coordinate of element 0 along each lattice
+ * dimension (the DDC domain front); operators sample between fields in
+ * absolute coordinates.  Form components are stored in the order of SimiLie's
+ * antisymmetric index (lexicographic combinations of the form dimensions).
+ * Dimensions not selected by `form_mask` are spectators (batch) dimensions.
+ */
+#ifndef SIL_B200_H
+#define SIL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SIL_MAX_DIMS 6
+
+typedef enum sil_status {
+    SIL_OK = 0,
+    SIL_ERR_INVALID = 1,      /* bad argument: shape, stride, rank, null pointer */
+    SIL_ERR_UNSUPPORTED = 2,  /* valid request this library does not implement */
+    SIL_ERR_CUDA = 3,         /* a CUDA runtime/driver call failed */
+    SIL_ERR_ALLOC = 4,        /* device allocation failed */
+    SIL_ERR_NONFINITE = 5,    /* a solve met NaN/Inf */
+    SIL_ERR_STALLED = 6,      /* a solve stopped making progress */
+    SIL_ERR_BUDGET = 7        /* a bounded device wait ran out */
+} sil_status;
+
+typedef enum sil_dtype { SIL_F64 = 0, SIL_F32 = 1 } sil_dtype;
+
+typedef void* sil_stream; /* a cudaStream_t */
+
+typedef struct sil_field {
+    void* data;                    /* device pointer to element 0 */
+    int32_t dtype;                 /* sil_dtype */
+    int32_t ndims;                 /* lattice (+ spectator) dimensions, 1..SIL_MAX_DIMS */
+    int32_t ncomp;                 /* stored form components, C(n, k) */
+    int32_t reserved;
+    int64_t front[SIL_MAX_DIMS];   /* absolute discrete coordinate of element 0 */
+    int64_t extent[SIL_MAX_DIMS];
+    int64_t stride[SIL_MAX_DIMS];  /* element strides */
+    int64_t comp_stride;           /* element stride of the form-component index */
+} sil_field;
+
+/* Human-readable name of a status and the last error message of this thread. */
+const char* sil_status_string(sil_status status);
+const char* sil_last_error(void);
+
+/* ---------------------------------------------------------------------- */
+/* Coboundary and its transpose (bit-exact in FP64 with the reference).    */
+
+/* d on a k-form: (d w)(s) = sum over the oriented boundary faces of each
+ * basis (k+1)-simplex, in chain order, of w sampled with clamping to the
+ * input domain.  out holds C(n, k+1) components.
+ * Replaces: sil::exterior::deriv / coboundary,
+ *   src/similie/exterior/coboundary.hpp:614-654, 698-709 (kernel 359-427). */
+sil_status sil_deriv(sil_stream stream, uint32_t form_mask, int k, const sil_field* in,
+                     sil_field* out);
+
+/* Transposed coboundary on a k-form (zero outside the input domain,
+ * backward shift of the second half-chain, negated chain sum).
+ * Replaces: sil::exterior::transposed_coboundary,
+ *   src/similie/exterior/coboundary.hpp:656-696 (kernel 523-605). */
+sil_status sil_transposed_coboundary(sil_stream stream, uint32_t form_mask, int k,
+                                     const sil_field* in, sil_field* out);
+
+/* ---------------------------------------------------------------------- */
+/* Geometry: a tensor-product (rectilinear) grid with the identity metric.  */
+/* The discrete Hodge star on such a grid is diagonal in the component      */
+/* basis; its factors are signed ratios of local edge lengths, computed on  */
+/* the fly from the per-axis coordinates (no stored per-node tensor).       */
+
+typedef struct sil_geometry_s* sil_geometry;
+
+/* coords[a] points to npoints[a] HOST doubles: node coordinates along form
+ * axis a (a = 0..n-1, in the order of the form dimensions).  front[a] is the
+ * absolute discrete coordinate of coords[a][0] (may be NULL for all zeros).
+ * Replaces the position + metric tensor fields passed to the staged
+ * operators (identity metric, position(i,j,...) = (x_i, y_j, ...)). */
+sil_status sil_geometry_create(sil_geometry* geometry, int n, const double* const* coords,
+                               const int64_t* npoints, const int64_t* front);
+sil_status sil_geometry_destroy(sil_geometry geometry);
+
+/* Hodge star of a k-form into an (n-k)-form at every node of `out`.
+ * Equivalent to tensor_prod(out, in, hodge) with the tensor that
+ * fill_discrete_hodge_star stores: src/similie/exterior/hodge_star.hpp:227-273. */
+sil_status sil_hodge_star(sil_geometry geometry, sil_stream stream, uint32_t form_mask, int k,
+                          const sil_field* in, sil_field* out);
+
+/* Write the per-node Hodge tensor SimiLie stores (Full<k> x Antisym<n-k>:
+ * n^k index tuples x C(n,n-k) components per node, tuple index slowest).
+ * Replaces: fill_discrete_hodge_star, src/similie/exterior/hodge_star.hpp:453-494. */
+sil_status sil_fill_discrete_hodge_star(sil_geometry geometry, sil_stream stream, int k_in,
+                                        sil_field* hodge);
+
+/* Codifferential of a k-form (k >= 1), one fused kernel (star, transposed d,
+ * star, sign (-1)^{n(k+1)+1}).
+ * Replaces: codifferential / StagedCodifferential::run,
+ *   src/similie/exterior/codifferential.hpp:321-508, 542-656. */
+sil_status sil_codifferential(sil_geometry geometry, sil_stream stream, uint32_t form_mask, int k,
+                              const sil_field* in, sil_field* out);
+
+/* ---------------------------------------------------------------------- */
+/* Hodge Laplacian (delta d for k = 0, delta d + d delta for 0 < k < n,     */
+/* d delta for k = n).                                                      */
+
+typedef enum sil_laplacian_mode {
+    SIL_LAPLACIAN_FUSED = 0,   /* single pass: each field read once, written once */
+    SIL_LAPLACIAN_UNFUSED = 1  /* reference kernel chain with intermediate fields */
+} sil_laplacian_mode;
+
+typedef struct sil_laplacian_plan_s* sil_laplacian_plan;
+
+/* Staged Laplacian: precomputes what run() needs for fields shaped like
+ * in_like / out_like (data pointers ignored) and owns any scratch.
+ * Replaces: make_staged_laplacian / StagedLaplacian ctor,
+ *   src/similie/exterior/laplacian.hpp:177-358, 360-648, 650-812. */
+sil_status sil_laplacian_plan_create(sil_laplacian_plan* plan, sil_geometry geometry,
+                                     uint32_t form_mask, int k, const sil_field* in_like,
+                                     const sil_field* out_like, int mode);
+/* Replaces: StagedLaplacian::run, laplacian.hpp:312-324, 599-647, 791-811. */
+sil_status sil_laplacian_run(sil_laplacian_plan plan, sil_stream stream, const sil_field* in,
+                             sil_field* out);
+sil_status sil_laplacian_plan_destroy(sil_laplacian_plan plan);
+/* Device bytes of scratch the plan owns (0 for the fused mode). */
+size_t sil_laplacian_plan_scratch_bytes(sil_laplacian_plan plan);
+/* Kernel the plan runs: 0 table-driven fused (any rank / layout), 1 fused 2D
+ * 0-form, 2 fused 2D 1-form with TMA-staged tiles, 3 unfused reference chain. */
+int sil_laplacian_plan_kernel(sil_laplacian_plan plan);
+/* Synchronising check of the plan's device error flag: SIL_ERR_BUDGET when a
+ * bounded wait inside a kernel ran out (the kernel returned early). */
+sil_status sil_laplacian_plan_status(sil_laplacian_plan plan);
+
+/* Plan-less Laplacian (free function form).
+ * Replaces: sil::exterior::laplacian, src/similie/exterior/laplacian.hpp:814-951. */
+sil_status sil_laplacian(sil_geometry geometry, sil_stream stream, uint32_t form_mask, int k,
+                         const sil_field* in, sil_field* out);
+
+/* ---------------------------------------------------------------------- */
+/* 2D linear magnetostatics: residual operator d^T(nu dA) with identity    */
+/* rows on the Dirichlet boundary, flat x-fastest layout row = i + nx*j.     */
+
+/* y = K a for one problem (device pointers, nx*ny doubles each).
+ * Replaces: MagnetostaticsOperator2D::apply,
+ *   onelab_interface/magnetostatics_onelab.hpp:1271-1426 (stencils 1095-1258). */
+sil_status sil_mag2d_apply(sil_stream stream, int64_t nx, int64_t ny, const double* node_mu,
+                           const double* a, double* y);
+
+typedef struct sil_mag2d_problem {
+    int64_t nx, ny;          /* nodes per axis (>= 3) */
+    const double* node_mu;   /* device, nx*ny: node permeability (mean of adjacent cells) */
+    const double* rhs;       /* device, nx*ny: right-hand side, 0 on the boundary */
+    double* solution;        /* device, nx*ny: written (initial guess is 0) */
+} sil_mag2d_problem;
+
+typedef enum sil_solver_kind {
+    SIL_SOLVER_CG_F64 = 0,      /* Jacobi-preconditioned CG, all FP64 */
+    SIL_SOLVER_MIXED_IR = 1     /* FP32 inner Jacobi-CG sweeps, FP64 residual/refinement */
+} sil_solver_kind;
+
+typedef struct sil_solve_settings {
+    int32_t solver;              /* sil_solver_kind */
+    int32_t max_iterations;      /* total inner iterations per problem */
+    double relative_tolerance;   /* stop when ||b - A x|| <= tol * ||b|| */
+    int32_t inner_iterations;    /* mixed: inner iterations per refinement step */
+    double inner_tolerance;      /* mixed: inner relative reduction per step */
+} sil_solve_settings;
+
+typedef struct sil_solve_diagnostics {
+    int32_t iterations;
+    int32_t converged;
+    int32_t refinements;
+    int32_t status;              /* sil_status of this problem */
+    double initial_residual_l2;
+    double final_residual_l2;
+    double final_relative_residual;
+} sil_solve_diagnostics;
+
+/* Solve a batch of independent problems on one device stream.  Writes one
+ * diagnostics record per problem into diag (HOST memory).  Synchronous.
+ * Replaces: solvers::minimize_strong_formulation_residual (linear branch),
+ *   src/similie/solvers/minimize_strong_formulation_residual.hpp:1308-1382
+ *   with the Jacobi-preconditioned Ginkgo CG it runs (1028-1304). */
+sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblems,
+                                 const sil_solve_settings* settings, sil_solve_diagnostics* diag,
+                                 sil_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIL_B200_H */

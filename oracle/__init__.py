@@ -1,0 +1,250 @@
+"""CPU oracle for SimiLie's DEC operators -- TEST INFRASTRUCTURE ONLY.
+
+A C++/OpenMP restatement of the reference algorithms (see sil_oracle.cpp for
+the file:line each routine follows).  Only the test-suite, the smoke check
+and the CPU-baseline leg of bench.py may use it, and only as the checker.
+
+Arrays are numpy float64.  A field array has its lattice axes first and the
+form-component axis last unless `comp_axis` says otherwise; any strides are
+accepted (component-first and component-last layouts both work).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+SILO_MAX_DIMS = 6
+
+
+class _Field(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.POINTER(ctypes.c_double)),
+        ("ndims", ctypes.c_int32),
+        ("ncomp", ctypes.c_int32),
+        ("front", ctypes.c_int64 * SILO_MAX_DIMS),
+        ("extent", ctypes.c_int64 * SILO_MAX_DIMS),
+        ("stride", ctypes.c_int64 * SILO_MAX_DIMS),
+        ("comp_stride", ctypes.c_int64),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = _build.build()
+        _lib = ctypes.CDLL(path)
+        P = ctypes.POINTER(_Field)
+        dp = ctypes.POINTER(ctypes.c_double)
+        i64 = ctypes.c_int64
+        _lib.silo_coboundary.argtypes = [ctypes.c_uint32, ctypes.c_int, P, P]
+        _lib.silo_transposed_coboundary.argtypes = [ctypes.c_uint32, ctypes.c_int, P, P]
+        _lib.silo_fill_hodge_star.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P]
+        _lib.silo_apply_hodge_star.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P]
+        _lib.silo_hodge_matrix.argtypes = [ctypes.c_int, ctypes.c_int, P, P, ctypes.POINTER(i64), dp]
+        _lib.silo_codifferential.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P, P]
+        _lib.silo_laplacian.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P, P]
+        _lib.silo_laplacian_prefilled.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(P), P, P]
+        _lib.silo_laplacian_hodge_ncomp.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        _lib.silo_laplacian_hodge_kin.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        _lib.silo_mag2d_node_mu.argtypes = [i64, i64, dp, ctypes.c_double, dp]
+        _lib.silo_mag2d_rhs.argtypes = [i64, i64, dp, dp, dp, dp]
+        _lib.silo_mag2d_apply.argtypes = [i64, i64, dp, dp, dp]
+        _lib.silo_mag2d_diagonal.argtypes = [i64, i64, dp, dp]
+        _lib.silo_mag2d_cg.argtypes = [i64, i64, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp]
+        _lib.silo_num_threads.argtypes = []
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def field(arr, comp_axis=-1, front=None):
+    """Describe a float64 numpy array as a strided oracle field."""
+    if arr.dtype != np.float64:
+        raise TypeError("oracle fields are float64")
+    nd = arr.ndim
+    comp_axis = comp_axis % nd
+    axes = [a for a in range(nd) if a != comp_axis]
+    f = _Field()
+    f.data = _ptr(arr)
+    f.ndims = len(axes)
+    f.ncomp = arr.shape[comp_axis]
+    for i, a in enumerate(axes):
+        f.front[i] = 0 if front is None else int(front[i])
+        f.extent[i] = arr.shape[a]
+        f.stride[i] = arr.strides[a] // 8
+    f.comp_stride = arr.strides[comp_axis] // 8
+    f._keep = arr
+    return f
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise ValueError(f"oracle {what} rejected its arguments (rc={rc})")
+
+
+def binom(n, k):
+    from math import comb
+    return comb(n, k) if 0 <= k <= n else 0
+
+
+def coboundary(inp, out, k, form_mask=None, comp_axis=-1, in_front=None, out_front=None):
+    """d on a k-form (clamped sampling); fills `out` in place."""
+    fi = field(inp, comp_axis, in_front)
+    fo = field(out, comp_axis, out_front)
+    mask = form_mask if form_mask is not None else (1 << fi.ndims) - 1
+    _check(lib().silo_coboundary(mask, k, ctypes.byref(fi), ctypes.byref(fo)), "coboundary")
+    return out
+
+
+def transposed_coboundary(inp, out, k, form_mask=None, comp_axis=-1, in_front=None, out_front=None):
+    fi = field(inp, comp_axis, in_front)
+    fo = field(out, comp_axis, out_front)
+    mask = form_mask if form_mask is not None else (1 << fi.ndims) - 1
+    _check(lib().silo_transposed_coboundary(mask, k, ctypes.byref(fi), ctypes.byref(fo)),
+           "transposed coboundary")
+    return out
+
+
+def position_from_coords(coords):
+    """Tensor-product position field (n comps per node) from 1D coordinates."""
+    grids = np.meshgrid(*[np.asarray(c, dtype=np.float64) for c in coords], indexing="ij")
+    return np.ascontiguousarray(np.stack(grids, axis=-1))
+
+
+def identity_metric(shape, n):
+    m = np.zeros(tuple(shape) + (n * n,), dtype=np.float64)
+    for i in range(n):
+        m[..., i * n + i] = 1.0
+    return m
+
+
+def hodge_ncomp(n, k_in):
+    return n ** k_in * binom(n, n - k_in)
+
+
+def fill_hodge_star(n, k_in, position, metric=None):
+    shape = position.shape[:-1]
+    hs = np.zeros(tuple(shape) + (hodge_ncomp(n, k_in),), dtype=np.float64)
+    fp = field(position)
+    fm = field(metric) if metric is not None else None
+    fh = field(hs)
+    _check(lib().silo_fill_hodge_star(n, k_in, ctypes.byref(fp),
+                                      ctypes.byref(fm) if fm is not None else None,
+                                      ctypes.byref(fh)), "fill_hodge_star")
+    return hs
+
+
+def apply_hodge_star(n, k_in, hodge, inp):
+    out = np.zeros(inp.shape[:-1] + (binom(n, n - k_in),), dtype=np.float64)
+    _check(lib().silo_apply_hodge_star(n, k_in, ctypes.byref(field(hodge)), ctypes.byref(field(inp)),
+                                       ctypes.byref(field(out))), "apply_hodge_star")
+    return out
+
+
+def hodge_matrix(n, k_in, position, node, metric=None):
+    m = np.zeros((binom(n, n - k_in), binom(n, k_in)), dtype=np.float64)
+    nd = (ctypes.c_int64 * n)(*node)
+    fm = field(metric) if metric is not None else None
+    _check(lib().silo_hodge_matrix(n, k_in, ctypes.byref(field(position)),
+                                   ctypes.byref(fm) if fm is not None else None, nd, _ptr(m)),
+           "hodge_matrix")
+    return m
+
+
+def codifferential(n, k, position, inp, metric=None, out_shape=None):
+    shape = out_shape if out_shape is not None else inp.shape[:-1]
+    out = np.zeros(tuple(shape) + (binom(n, k - 1),), dtype=np.float64)
+    fm = field(metric) if metric is not None else None
+    _check(lib().silo_codifferential(n, k, ctypes.byref(field(position)),
+                                     ctypes.byref(fm) if fm is not None else None,
+                                     ctypes.byref(field(inp)), ctypes.byref(field(out))),
+           "codifferential")
+    return out
+
+
+def laplacian(n, k, position, inp, metric=None, out_shape=None):
+    """Staged Hodge Laplacian; default output lattice is the input minus its last node per axis."""
+    shape = out_shape if out_shape is not None else tuple(s - 1 for s in inp.shape[:-1])
+    out = np.zeros(tuple(shape) + (binom(n, k),), dtype=np.float64)
+    fm = field(metric) if metric is not None else None
+    _check(lib().silo_laplacian(n, k, ctypes.byref(field(position)),
+                                ctypes.byref(fm) if fm is not None else None,
+                                ctypes.byref(field(inp)), ctypes.byref(field(out))), "laplacian")
+    return out
+
+
+class StagedLaplacian:
+    """Reference-structured staged Laplacian: stored Hodge tensors filled once,
+    then run() chains the separate d/Hodge/transposed-d passes."""
+
+    def __init__(self, n, k, position, metric=None):
+        self.n, self.k = n, k
+        self.hodges = []
+        for which in range(4):
+            nc = lib().silo_laplacian_hodge_ncomp(n, k, which)
+            if nc == 0:
+                self.hodges.append(None)
+                continue
+            kin = lib().silo_laplacian_hodge_kin(n, k, which)
+            self.hodges.append(fill_hodge_star(n, kin, position, metric))
+
+    def run(self, inp, out):
+        fields = [field(h) if h is not None else None for h in self.hodges]
+        P = ctypes.POINTER(_Field)
+        arr = (P * 4)(*[ctypes.pointer(f) if f is not None else P() for f in fields])
+        _check(lib().silo_laplacian_prefilled(self.n, self.k, arr, ctypes.byref(field(inp)),
+                                              ctypes.byref(field(out))), "laplacian")
+        return out
+
+
+# ----------------------------------------------------------------- magnetostatics 2D
+
+def mag2d_node_mu(nx, ny, cell_mu, mu0=1.0):
+    out = np.zeros(nx * ny)
+    c = np.ascontiguousarray(cell_mu, dtype=np.float64)
+    lib().silo_mag2d_node_mu(nx, ny, _ptr(c), mu0, _ptr(out))
+    return out
+
+
+def mag2d_rhs(x, y, cell_j):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    c = np.ascontiguousarray(cell_j, dtype=np.float64)
+    out = np.zeros(len(x) * len(y))
+    lib().silo_mag2d_rhs(len(x), len(y), _ptr(x), _ptr(y), _ptr(c), _ptr(out))
+    return out
+
+
+def mag2d_apply(nx, ny, node_mu, a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    mu = np.ascontiguousarray(node_mu, dtype=np.float64)
+    out = np.zeros(nx * ny)
+    lib().silo_mag2d_apply(nx, ny, _ptr(mu), _ptr(a), _ptr(out))
+    return out
+
+
+def mag2d_diagonal(nx, ny, node_mu):
+    mu = np.ascontiguousarray(node_mu, dtype=np.float64)
+    out = np.zeros(nx * ny)
+    lib().silo_mag2d_diagonal(nx, ny, _ptr(mu), _ptr(out))
+    return out
+
+
+def mag2d_cg(nx, ny, node_mu, rhs, tol=1e-10, max_iter=100000):
+    mu = np.ascontiguousarray(node_mu, dtype=np.float64)
+    b = np.ascontiguousarray(rhs, dtype=np.float64)
+    x = np.zeros(nx * ny)
+    rel = ctypes.c_double(0.0)
+    it = lib().silo_mag2d_cg(nx, ny, _ptr(mu), _ptr(b), _ptr(x), tol, max_iter, ctypes.byref(rel))
+    return x, it, rel.value
+
+
+def num_threads():
+    return lib().silo_num_threads()

@@ -1,0 +1,1271 @@
+// sil_oracle.cpp -- CPU restatement of SimiLie's DEC operators (TEST INFRASTRUCTURE).
+//
+// This file is the checker the CUDA library is compared against and the timed
+// CPU baseline; it is never part of the product path.  Each routine names the
+// reference source (paths relative to the SimiLie project root) it restates.
+// The restatement keeps the reference's order of floating-point operations
+// wherever the reference fixes one (chain order of the coboundary sums, the
+// pivoting order of the small-matrix routines, the staged kernel chain).
+
+#include "sil_oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr int MAXD = SILO_MAX_DIMS;
+constexpr int MAXN = 4;  // form dimension limit (tests cover 1D..4D)
+
+// ---------------------------------------------------------------- helpers
+
+int64_t binom(int n, int k)
+{
+    if (k < 0 || k > n) return 0;
+    int64_t r = 1;
+    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+    return r;
+}
+
+double factorial(int k)
+{
+    double r = 1.;
+    for (int i = 2; i <= k; ++i) r *= i;
+    return r;
+}
+
+int64_t ipow(int64_t b, int e)
+{
+    int64_t r = 1;
+    for (int i = 0; i < e; ++i) r *= b;
+    return r;
+}
+
+// Tangent basis of K-simplices over n dims: 0/1 vectors enumerated by
+// std::prev_permutation starting from [1..1,0..0].
+// Ref: src/similie/exterior/local_chain.hpp:413-437
+std::vector<std::array<int, MAXN>> tangent_basis(int n, int k)
+{
+    std::array<int, MAXN> p {};
+    for (int i = 0; i < n; ++i) p[i] = i < k ? 1 : 0;
+    std::vector<std::array<int, MAXN>> out;
+    do {
+        out.push_back(p);
+    } while (std::prev_permutation(p.begin(), p.begin() + n));
+    return out;
+}
+
+// Lexicographic k-combination of {0..n-1} <-> rank.
+// Ref: src/similie/exterior/reduction_and_reconstruction.hpp:190-236
+std::vector<int> combination_from_rank(int n, int k, int64_t rank)
+{
+    std::vector<int> ids(k);
+    int next_candidate = 0;
+    for (int i = 0; i < k; ++i) {
+        for (int candidate = next_candidate; candidate < n; ++candidate) {
+            int const remaining = k - i - 1;
+            int const remaining_space = n - candidate - 1;
+            int64_t const count = remaining == 0 ? 1 : binom(remaining_space, remaining);
+            if (rank < count) {
+                ids[i] = candidate;
+                next_candidate = candidate + 1;
+                break;
+            }
+            rank -= count;
+        }
+    }
+    return ids;
+}
+
+int64_t combination_rank(int n, std::vector<int> const& ids)
+{
+    int const k = static_cast<int>(ids.size());
+    int64_t rank = 0;
+    int next_candidate = 0;
+    for (int i = 0; i < k; ++i) {
+        for (int candidate = next_candidate; candidate < ids[i]; ++candidate) {
+            int const remaining = k - i - 1;
+            int const remaining_space = n - candidate - 1;
+            rank += remaining == 0 ? 1 : binom(remaining_space, remaining);
+        }
+        next_candidate = ids[i] + 1;
+    }
+    return rank;
+}
+
+// ---------------------------------------------------------------- simplices
+
+struct Simplex
+{
+    int n;
+    int64_t elem[MAXN];
+    int vect[MAXN];
+    bool negative;
+};
+
+// Constructor with reorientation of -1 entries.
+// Ref: src/similie/exterior/simplex.hpp:16-68, 118-129
+Simplex make_simplex(int n, int64_t const* elem, int const* vect, bool negative)
+{
+    Simplex s;
+    s.n = n;
+    bool neg = negative;
+    for (int d = 0; d < n; ++d) {
+        s.elem[d] = elem[d];
+        s.vect[d] = vect[d];
+        if (vect[d] == -1) {
+            s.elem[d] -= 1;
+            s.vect[d] = 1;
+            neg = !neg;
+        }
+    }
+    s.negative = neg;
+    return s;
+}
+
+// Ref: src/similie/exterior/boundary.hpp:295-317 (generate_local_half_subchain)
+void half_subchain(
+        int n,
+        int K,
+        int64_t const* elem,
+        int const* vect,
+        bool negative,
+        std::vector<Simplex>& chain)
+{
+    int id_dist = -1;
+    for (int i = 0; i < K; ++i) {
+        int array_[MAXN];
+        for (int d = 0; d < n; ++d) array_[d] = vect[d];
+        int id = id_dist + 1;
+        while (id < n && array_[id] == 0) ++id;
+        id_dist = id;
+        array_[id] = 0;
+        chain.push_back(make_simplex(n, elem, array_, ((negative ? 1 : 0) + i) % 2 != 0));
+    }
+}
+
+// Boundary of a K-simplex, LocalChain flavour.  Ref: src/similie/exterior/boundary.hpp:426-441
+std::vector<Simplex> boundary(int K, Simplex const& s)
+{
+    std::vector<Simplex> chain;
+    half_subchain(s.n, K, s.elem, s.vect, K % 2 != 0, chain);
+    int64_t shifted[MAXN];
+    int minus[MAXN];
+    for (int d = 0; d < s.n; ++d) {
+        shifted[d] = s.elem[d] + s.vect[d];
+        minus[d] = -s.vect[d];
+    }
+    half_subchain(s.n, K, shifted, minus, false, chain);
+    int const mult = (K % 2 ? 1 : -1) * (s.negative ? -1 : 1);
+    if (mult == -1) {
+        for (auto& f : chain) f.negative = !f.negative;
+    }
+    return chain;
+}
+
+// One face of the boundary of a basis simplex, as a sampling rule relative
+// to the node the simplex starts from.
+struct FaceRule
+{
+    int64_t offset[MAXN];
+    int comp;     // index of the face vector in the lower tangent basis
+    bool negative;
+};
+
+// Face rules for every component of d (Coboundary::run) or of the
+// transposed coboundary (TransposedCoboundary::run), with the -2 backward
+// shift on the second half-chain for the transposed flavour.
+// Ref: src/similie/exterior/coboundary.hpp:359-427 and 523-605
+std::vector<std::vector<FaceRule>> face_rules(int n, int k, bool transposed)
+{
+    auto const chain = tangent_basis(n, k + 1);
+    auto const lower = tangent_basis(n, k);
+    std::vector<std::vector<FaceRule>> rules;
+    int64_t origin[MAXN] = {0, 0, 0, 0};
+    for (auto const& v : chain) {
+        Simplex const s = make_simplex(n, origin, v.data(), false);
+        auto const faces = boundary(k + 1, s);
+        std::vector<FaceRule> comp_rules;
+        for (std::size_t j = 0; j < faces.size(); ++j) {
+            FaceRule r {};
+            for (int d = 0; d < n; ++d) r.offset[d] = faces[j].elem[d];
+            if (transposed && static_cast<int>(j) >= k + 1) {
+                for (int d = 0; d < n; ++d) {
+                    if (v[d] != 0 && faces[j].vect[d] == 0) {
+                        r.offset[d] -= 2;
+                        break;
+                    }
+                }
+            }
+            int comp = static_cast<int>(lower.size());
+            for (std::size_t c = 0; c < lower.size(); ++c) {
+                bool same = true;
+                for (int d = 0; d < n; ++d) same = same && (lower[c][d] == faces[j].vect[d]);
+                if (same) {
+                    comp = static_cast<int>(c);
+                    break;
+                }
+            }
+            r.comp = comp;
+            r.negative = faces[j].negative;
+            comp_rules.push_back(r);
+        }
+        rules.push_back(comp_rules);
+    }
+    return rules;
+}
+
+// ---------------------------------------------------------------- fields
+
+int64_t num_nodes(silo_field const& f)
+{
+    int64_t t = 1;
+    for (int d = 0; d < f.ndims; ++d) t *= f.extent[d];
+    return t;
+}
+
+void unravel(silo_field const& f, int64_t flat, int64_t* local)
+{
+    for (int d = f.ndims - 1; d >= 0; --d) {
+        local[d] = flat % f.extent[d];
+        flat /= f.extent[d];
+    }
+}
+
+int64_t offset_local(silo_field const& f, int64_t const* local)
+{
+    int64_t o = 0;
+    for (int d = 0; d < f.ndims; ++d) o += local[d] * f.stride[d];
+    return o;
+}
+
+bool contains_abs(silo_field const& f, int64_t const* abs)
+{
+    for (int d = 0; d < f.ndims; ++d) {
+        if (abs[d] < f.front[d] || abs[d] > f.front[d] + f.extent[d] - 1) return false;
+    }
+    return true;
+}
+
+int form_dims(uint32_t mask, int ndims, int* dims)
+{
+    int n = 0;
+    for (int d = 0; d < ndims; ++d) {
+        if (mask & (1u << d)) dims[n++] = d;
+    }
+    return n;
+}
+
+// d on a k-form with clamped sampling (ClampedTensorEvaluator,
+// src/similie/exterior/evaluators.hpp:30-46; misc/clamp_to_domain.hpp:17-47),
+// or the transposed coboundary with zero-outside sampling
+// (ZeroOutsideTensorEvaluator, evaluators.hpp:48-68; misc/domain_contains.hpp).
+// Summation in chain order from 0 (Cochain::integrate, cochain.hpp:187-198).
+int coboundary_impl(uint32_t mask, int k, silo_field const* in, silo_field* out, bool transposed)
+{
+    int dims[MAXD];
+    int const n = form_dims(mask, in->ndims, dims);
+    if (n < 1 || n > MAXN || k < 0 || k >= n) return -1;
+    if (in->ndims != out->ndims) return -1;
+    if (in->ncomp != binom(n, k) || out->ncomp != binom(n, k + 1)) return -1;
+    auto const rules = face_rules(n, k, transposed);
+    int64_t const total = num_nodes(*out);
+#pragma omp parallel for schedule(static)
+    for (int64_t flat = 0; flat < total; ++flat) {
+        int64_t local[MAXD];
+        unravel(*out, flat, local);
+        int64_t abs[MAXD];
+        for (int d = 0; d < out->ndims; ++d) abs[d] = out->front[d] + local[d];
+        double* o = out->data + offset_local(*out, local);
+        for (std::size_t c = 0; c < rules.size(); ++c) {
+            double acc = 0.;
+            for (auto const& r : rules[c]) {
+                int64_t s[MAXD];
+                for (int d = 0; d < in->ndims; ++d) s[d] = abs[d];
+                for (int a = 0; a < n; ++a) s[dims[a]] += r.offset[a];
+                double v;
+                if (!transposed) {
+                    for (int d = 0; d < in->ndims; ++d) {
+                        s[d] = std::min(std::max(s[d], in->front[d]), in->front[d] + in->extent[d] - 1);
+                    }
+                    int64_t sl[MAXD];
+                    for (int d = 0; d < in->ndims; ++d) sl[d] = s[d] - in->front[d];
+                    v = in->data[offset_local(*in, sl) + r.comp * in->comp_stride];
+                } else if (!contains_abs(*in, s)) {
+                    v = 0.0;
+                } else {
+                    int64_t sl[MAXD];
+                    for (int d = 0; d < in->ndims; ++d) sl[d] = s[d] - in->front[d];
+                    v = in->data[offset_local(*in, sl) + r.comp * in->comp_stride];
+                }
+                acc += (r.negative ? -1 : 1) * v;
+            }
+            o[c * out->comp_stride] = transposed ? -acc : acc;
+        }
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------- small matrices
+
+// Partial-pivot determinant, in place.  Ref: src/similie/misc/small_matrix.hpp:75-117
+double determinant(double* m, int n)
+{
+    if (n == 0) return 1.;
+    double det = 1.;
+    int sign = 1;
+    for (int i = 0; i < n; ++i) {
+        int pivot = i;
+        double pivot_abs = std::abs(m[i * n + i]);
+        for (int row = i + 1; row < n; ++row) {
+            double const cand = std::abs(m[row * n + i]);
+            if (cand > pivot_abs) {
+                pivot = row;
+                pivot_abs = cand;
+            }
+        }
+        if (pivot_abs == 0.) return 0.;
+        if (pivot != i) {
+            sign *= -1;
+            for (int col = 0; col < n; ++col) std::swap(m[i * n + col], m[pivot * n + col]);
+        }
+        double const diagonal = m[i * n + i];
+        det *= diagonal;
+        for (int row = i + 1; row < n; ++row) {
+            double const factor = m[row * n + i] / diagonal;
+            for (int col = i + 1; col < n; ++col) m[row * n + col] -= factor * m[i * n + col];
+            m[row * n + i] = 0.;
+        }
+    }
+    return sign * det;
+}
+
+// Gauss-Jordan inverse with partial pivoting.  Ref: src/similie/misc/small_matrix.hpp:120-180
+bool invert(double* inv, double const* m, int n)
+{
+    std::vector<double> w(m, m + n * n);
+    for (int i = 0; i < n * n; ++i) inv[i] = 0.;
+    for (int i = 0; i < n; ++i) inv[i * n + i] = 1.;
+    for (int i = 0; i < n; ++i) {
+        int pivot = i;
+        double pivot_abs = std::abs(w[i * n + i]);
+        for (int row = i + 1; row < n; ++row) {
+            double const cand = std::abs(w[row * n + i]);
+            if (cand > pivot_abs) {
+                pivot = row;
+                pivot_abs = cand;
+            }
+        }
+        if (pivot_abs == 0.) {
+            for (int j = 0; j < n * n; ++j) inv[j] = 0.;
+            return false;
+        }
+        if (pivot != i) {
+            for (int col = 0; col < n; ++col) {
+                std::swap(w[i * n + col], w[pivot * n + col]);
+                std::swap(inv[i * n + col], inv[pivot * n + col]);
+            }
+        }
+        double const diagonal = w[i * n + i];
+        for (int col = 0; col < n; ++col) {
+            w[i * n + col] /= diagonal;
+            inv[i * n + col] /= diagonal;
+        }
+        for (int row = 0; row < n; ++row) {
+            if (row == i) continue;
+            double const factor = w[row * n + i];
+            for (int col = 0; col < n; ++col) {
+                w[row * n + col] -= factor * w[i * n + col];
+                inv[row * n + col] -= factor * inv[i * n + col];
+            }
+        }
+    }
+    return true;
+}
+
+// Ref: src/similie/misc/small_matrix.hpp:183-198
+double submatrix_determinant(double const* m, int n, std::vector<int> const& rows, std::vector<int> const& cols)
+{
+    int const k = static_cast<int>(rows.size());
+    if (k == 0) return 1.;
+    std::vector<double> sub(k * k);
+    for (int i = 0; i < k; ++i)
+        for (int j = 0; j < k; ++j) sub[i * k + j] = m[rows[i] * n + cols[j]];
+    return determinant(sub.data(), k);
+}
+
+// Cofactor expansion along the first row.
+// Ref: src/similie/exterior/reduction_and_reconstruction.hpp:162-188
+double reduction_determinant(std::vector<double> const& m, int k)
+{
+    if (k == 0) return 1.;
+    if (k == 1) return m[0];
+    double det = 0.;
+    for (int col = 0; col < k; ++col) {
+        std::vector<double> minor((k - 1) * (k - 1));
+        for (int row = 1; row < k; ++row) {
+            int mc = 0;
+            for (int sc = 0; sc < k; ++sc) {
+                if (sc == col) continue;
+                minor[(row - 1) * (k - 1) + mc] = m[row * k + sc];
+                ++mc;
+            }
+        }
+        double const sign = (col % 2 == 0) ? 1. : -1.;
+        det += sign * m[col] * reduction_determinant(minor, k - 1);
+    }
+    return det;
+}
+
+std::vector<int> complement(int n, std::vector<int> const& ids)
+{
+    std::vector<int> c;
+    for (int i = 0; i < n; ++i) {
+        bool found = false;
+        for (int id : ids) found = found || id == i;
+        if (!found) c.push_back(i);
+    }
+    return c;
+}
+
+bool unique_ids(int n, std::vector<int> const& ids)
+{
+    for (std::size_t i = 0; i < ids.size(); ++i) {
+        if (ids[i] >= n) return false;
+        for (std::size_t j = i + 1; j < ids.size(); ++j)
+            if (ids[i] == ids[j]) return false;
+    }
+    return true;
+}
+
+bool complete_permutation(int n, std::vector<int> const& a, std::vector<int> const& b)
+{
+    std::vector<int> counts(n, 0);
+    for (int id : a) {
+        if (id >= n) return false;
+        counts[id]++;
+    }
+    for (int id : b) {
+        if (id >= n) return false;
+        counts[id]++;
+    }
+    for (int c : counts)
+        if (c != 1) return false;
+    return true;
+}
+
+// Ref: src/similie/exterior/reduction_and_reconstruction.hpp:282-304
+int permutation_sign(std::vector<int> const& a, std::vector<int> const& b)
+{
+    std::vector<int> p(a);
+    p.insert(p.end(), b.begin(), b.end());
+    bool odd = false;
+    for (std::size_t i = 0; i < p.size(); ++i)
+        for (std::size_t j = i + 1; j < p.size(); ++j) odd = (p[i] > p[j]) != odd;
+    return odd ? -1 : 1;
+}
+
+// ---------------------------------------------------------------- geometry
+
+struct Geometry
+{
+    int n;
+    silo_field const* position;  // lattice over the form dims, n comps
+    silo_field const* metric;    // lattice over the form dims, n*n comps, or nullptr
+
+    void metric_at(int64_t const* node, double* g) const
+    {
+        if (metric == nullptr) {
+            for (int i = 0; i < n * n; ++i) g[i] = 0.;
+            for (int i = 0; i < n; ++i) g[i * n + i] = 1.;
+            return;
+        }
+        int64_t local[MAXD];
+        for (int d = 0; d < n; ++d) local[d] = node[d] - metric->front[d];
+        double const* p = metric->data + offset_local(*metric, local);
+        for (int i = 0; i < n * n; ++i) g[i] = p[i * metric->comp_stride];
+    }
+
+    double pos(int64_t const* node, int comp) const
+    {
+        int64_t local[MAXD];
+        for (int d = 0; d < n; ++d) local[d] = node[d] - position->front[d];
+        return position->data[offset_local(*position, local) + comp * position->comp_stride];
+    }
+
+    // Ref: src/similie/exterior/volume.hpp:55-82
+    void edge_vector(int64_t const* node, int dim, double* v) const
+    {
+        int64_t fwd[MAXD], bwd[MAXD];
+        for (int d = 0; d < n; ++d) fwd[d] = bwd[d] = node[d];
+        fwd[dim] += 1;
+        bwd[dim] -= 1;
+        bool const has_fwd = contains_abs(*position, fwd);
+        bool const has_bwd = contains_abs(*position, bwd);
+        for (int c = 0; c < n; ++c) {
+            double const center = pos(node, c);
+            if (has_fwd) v[c] = pos(fwd, c) - center;
+            else if (has_bwd) v[c] = center - pos(bwd, c);
+            else v[c] = 0.;
+        }
+    }
+
+    // Ref: src/similie/exterior/volume.hpp:101-155
+    double simplex_volume(int64_t const* node, std::vector<int> const& ids) const
+    {
+        int const K = static_cast<int>(ids.size());
+        if (K == 0) return 1.;
+        double g[MAXN * MAXN];
+        metric_at(node, g);
+        std::vector<std::array<double, MAXN>> edges(K);
+        for (int i = 0; i < K; ++i) edge_vector(node, ids[i], edges[i].data());
+        std::vector<double> gram(K * K);
+        for (int i = 0; i < K; ++i) {
+            for (int j = i; j < K; ++j) {
+                double value = 0.;
+                for (int a = 0; a < n; ++a)
+                    for (int b = 0; b < n; ++b) value += edges[i][a] * g[a * n + b] * edges[j][b];
+                gram[i * K + j] = value;
+                gram[j * K + i] = value;
+            }
+        }
+        return std::sqrt(std::abs(determinant(gram.data(), K)));
+    }
+
+    // Ref: src/similie/exterior/reduction_and_reconstruction.hpp:324-348
+    double primal_reconstruction_diagonal(int64_t const* node, std::vector<int> const& ids) const
+    {
+        int const K = static_cast<int>(ids.size());
+        if (K == 0) return 1.;
+        std::vector<double> j(K * K);
+        for (int row = 0; row < K; ++row) {
+            for (int col = 0; col < K; ++col) {
+                double e[MAXN];
+                edge_vector(node, ids[col], e);
+                j[row * K + col] = e[ids[row]];
+            }
+        }
+        double const jac = reduction_determinant(j, K);
+        if (std::abs(jac) < 1e-14) return 0.;
+        return 1. / jac;
+    }
+
+    // Ref: src/similie/exterior/reduction_and_reconstruction.hpp:350-401 and hodge_star.hpp:396-450
+    double continuous_hodge_value(
+            int64_t const* node,
+            std::vector<int> const& source,
+            std::vector<int> const& target) const
+    {
+        int const K = static_cast<int>(source.size());
+        if (!unique_ids(n, source) || !unique_ids(n, target) || !complete_permutation(n, source, target))
+            return 0.;
+        std::vector<int> const comp = complement(n, target);
+        double g[MAXN * MAXN], gdet[MAXN * MAXN], ginv[MAXN * MAXN];
+        metric_at(node, g);
+        std::copy(g, g + n * n, gdet);
+        double const det = determinant(gdet, n);
+        if (!invert(ginv, g, n)) return 0.;
+        return std::sqrt(std::abs(det)) * static_cast<double>(permutation_sign(comp, target))
+               * submatrix_determinant(ginv, n, source, comp) / factorial(K);
+    }
+
+    // Ref: src/similie/exterior/reduction_and_reconstruction.hpp:403-432
+    double legacy_hodge_value(
+            int64_t const* node,
+            std::vector<int> const& source,
+            std::vector<int> const& target) const
+    {
+        int const K = static_cast<int>(source.size());
+        if (!unique_ids(n, source) || !unique_ids(n, target) || !complete_permutation(n, source, target))
+            return 0.;
+        double const primal_volume = simplex_volume(node, source);
+        if (primal_volume == 0.) return 0.;
+        return static_cast<double>(permutation_sign(source, target)) * simplex_volume(node, complement(n, source))
+               / (primal_volume * factorial(K));
+    }
+
+    // Reconstruction<Primal>::run: rec[t] = sum_s value(s,t) * cochain[s].
+    // Ref: src/similie/exterior/reduction_and_reconstruction.hpp:814-892
+    void reconstruct(int64_t const* node, int K, double const* cochain, double* rec) const
+    {
+        if (K == 0) {
+            rec[0] = cochain[0];
+            return;
+        }
+        int64_t const nb = binom(n, K);
+        for (int64_t t = 0; t < nb; ++t) {
+            auto const tids = combination_from_rank(n, K, t);
+            double value_sum = 0.;
+            for (int64_t s = 0; s < nb; ++s) {
+                auto const sids = combination_from_rank(n, K, s);
+                double value;
+                // Reduction<Primal>::value with source=sids, target=tids (lines 649-677).
+                std::vector<double> j(K * K);
+                for (int row = 0; row < K; ++row) {
+                    for (int col = 0; col < K; ++col) {
+                        double e[MAXN];
+                        edge_vector(node, tids[col], e);
+                        j[row * K + col] = e[sids[row]];
+                    }
+                }
+                double const reduction_value = reduction_determinant(j, K) / factorial(K);
+                if (s != t) value = 0.;
+                else if (std::abs(reduction_value) < 1e-14) value = 0.;
+                else value = 1. / (factorial(K) * reduction_value);
+                value_sum += value * cochain[s];
+            }
+            rec[t] = value_sum;
+        }
+    }
+
+    // ContinuousHodgeStar::run: contraction of the Full x Antisym tensor with
+    // the K-form over all index tuples.  Ref: src/similie/exterior/hodge_star.hpp:366-394
+    void continuous_star(int64_t const* node, int K, double const* form, double* out) const
+    {
+        int const Q = n - K;
+        int64_t const nq = binom(n, Q);
+        int64_t const ntuples = ipow(n, K);
+        for (int64_t t = 0; t < nq; ++t) {
+            auto const tids = combination_from_rank(n, Q, t);
+            double acc = 0.;
+            for (int64_t tu = 0; tu < ntuples; ++tu) {
+                std::vector<int> tuple(K);
+                int64_t r = tu;
+                for (int a = K - 1; a >= 0; --a) {
+                    tuple[a] = static_cast<int>(r % n);
+                    r /= n;
+                }
+                double const hs = continuous_hodge_value(node, tuple, tids);
+                double fv;
+                if (K == 0) {
+                    fv = form[0];
+                } else if (!unique_ids(n, tuple)) {
+                    fv = 0.;
+                } else {
+                    std::vector<int> sorted(tuple);
+                    std::sort(sorted.begin(), sorted.end());
+                    std::vector<int> none;
+                    int const sgn = permutation_sign(tuple, none);
+                    fv = sgn * form[combination_rank(n, sorted)];
+                }
+                acc += hs * fv;
+            }
+            out[t] = acc;
+        }
+    }
+
+    // Reduction<CircumcentricDual>::run (metric-aware).
+    // Ref: src/similie/exterior/reduction_and_reconstruction.hpp:535-647
+    void reduce_dual(int64_t const* node, int Q, double const* form, double* out) const
+    {
+        int const K = n - Q;
+        int64_t const nb = binom(n, Q);
+        std::vector<double> coeff(nb * nb), cinv(nb * nb), old(nb * nb);
+        for (int64_t p = 0; p < nb; ++p) {
+            auto const pids = combination_from_rank(n, K, p);
+            double const rdiag = primal_reconstruction_diagonal(node, pids);
+            for (int64_t s = 0; s < nb; ++s) {
+                auto const sids = combination_from_rank(n, Q, s);
+                coeff[s * nb + p] = continuous_hodge_value(node, pids, sids) * rdiag;
+            }
+            for (int64_t t = 0; t < nb; ++t) {
+                auto const tids = combination_from_rank(n, Q, t);
+                old[t * nb + p] = legacy_hodge_value(node, pids, tids);
+            }
+        }
+        bool const invertible = invert(cinv.data(), coeff.data(), static_cast<int>(nb));
+        for (int64_t t = 0; t < nb; ++t) {
+            double reduced = 0.;
+            for (int64_t s = 0; s < nb; ++s) {
+                double drv = 0.;
+                if (invertible) {
+                    for (int64_t p = 0; p < nb; ++p) drv += old[t * nb + p] * cinv[p * nb + s];
+                }
+                reduced += drv * form[s];
+            }
+            out[t] = reduced;
+        }
+    }
+
+    // DiscreteHodgeStar::run.  Ref: src/similie/exterior/hodge_star.hpp:227-273
+    void discrete_star(int64_t const* node, int K, double const* form, double* out) const
+    {
+        double rec[8], cont[8];
+        reconstruct(node, K, form, rec);
+        continuous_star(node, K, rec, cont);
+        reduce_dual(node, n - K, cont, out);
+    }
+};
+
+// Per-node stored Hodge tensor, DiscreteHodgeStar::value for every
+// (full source tuple, canonical target) pair.  run() depends only on the
+// canonical source, so it is evaluated once per canonical component.
+// Ref: src/similie/exterior/hodge_star.hpp:275-358, 461-494
+void fill_node(Geometry const& geo, int K, int64_t const* node, double* out, int64_t comp_stride)
+{
+    int const n = geo.n;
+    int const Q = n - K;
+    int64_t const nk = binom(n, K);
+    int64_t const nq = binom(n, Q);
+    std::vector<double> responses(nk * nq);
+    for (int64_t c = 0; c < nk; ++c) {
+        double unit[8] = {0};
+        unit[c] = 1.;
+        geo.discrete_star(node, K, unit, &responses[c * nq]);
+    }
+    int64_t const ntuples = ipow(n, K);
+    for (int64_t tu = 0; tu < ntuples; ++tu) {
+        std::vector<int> tuple(K);
+        int64_t r = tu;
+        for (int a = K - 1; a >= 0; --a) {
+            tuple[a] = static_cast<int>(r % n);
+            r /= n;
+        }
+        bool const valid = K <= 1 || unique_ids(n, tuple);
+        bool odd = false;
+        for (int i = 0; i < K; ++i)
+            for (int j = i + 1; j < K; ++j) odd = (tuple[i] > tuple[j]) != odd;
+        std::vector<int> sorted(tuple);
+        std::sort(sorted.begin(), sorted.end());
+        double const source_factor = (odd ? -1. : 1.) / factorial(K);
+        int64_t const c = K == 0 ? 0 : combination_rank(n, sorted);
+        for (int64_t t = 0; t < nq; ++t) {
+            out[(tu * nq + t) * comp_stride] = valid ? source_factor * responses[c * nq + t] : 0.;
+        }
+    }
+}
+
+// tensor_prod(out, form, hodge): out[t] = sum over tuples form.get(tuple) * hodge(tuple, t).
+// Ref: src/similie/tensor/tensor_prod.hpp:108-157
+void apply_node(int n, int K, double const* hodge, int64_t hstride, double const* form, int64_t fstride,
+                double* out, int64_t ostride)
+{
+    int const Q = n - K;
+    int64_t const nq = binom(n, Q);
+    int64_t const ntuples = ipow(n, K);
+    for (int64_t t = 0; t < nq; ++t) {
+        double acc = 0.;
+        for (int64_t tu = 0; tu < ntuples; ++tu) {
+            std::vector<int> tuple(K);
+            int64_t r = tu;
+            for (int a = K - 1; a >= 0; --a) {
+                tuple[a] = static_cast<int>(r % n);
+                r /= n;
+            }
+            double fv;
+            if (K == 0) {
+                fv = form[0];
+            } else if (!unique_ids(n, tuple)) {
+                fv = 0.;
+            } else {
+                std::vector<int> sorted(tuple);
+                std::sort(sorted.begin(), sorted.end());
+                std::vector<int> none;
+                fv = permutation_sign(tuple, none) * form[combination_rank(n, sorted) * fstride];
+            }
+            acc += fv * hodge[(tu * nq + t) * hstride];
+        }
+        out[t * ostride] = acc;
+    }
+}
+
+// Stored-Hodge lookup for a node of a field whose form dims are the first
+// `n` dims listed in `dims`.
+double const* hodge_at(silo_field const& hs, int n, int const* dims, int64_t const* abs)
+{
+    int64_t local[MAXD];
+    for (int a = 0; a < n; ++a) local[a] = abs[dims[a]] - hs.front[a];
+    return hs.data + offset_local(hs, local);
+}
+
+silo_field make_buffer(silo_field const& like, int ncomp, std::vector<double>& storage)
+{
+    silo_field f = like;
+    int64_t const nodes = num_nodes(like);
+    storage.assign(nodes * ncomp, 0.);
+    f.data = storage.data();
+    f.ncomp = ncomp;
+    f.comp_stride = 1;
+    int64_t s = ncomp;
+    for (int d = like.ndims - 1; d >= 0; --d) {
+        f.stride[d] = s;
+        s *= like.extent[d];
+    }
+    return f;
+}
+
+silo_field make_hodge_field(silo_field const& lattice, int n, int K, std::vector<double>& storage)
+{
+    silo_field f {};
+    f.ndims = n;
+    int const ncomp = static_cast<int>(ipow(n, K) * binom(n, n - K));
+    int64_t nodes = 1;
+    for (int d = 0; d < n; ++d) {
+        f.front[d] = lattice.front[d];
+        f.extent[d] = lattice.extent[d];
+        nodes *= f.extent[d];
+    }
+    storage.assign(nodes * ncomp, 0.);
+    f.data = storage.data();
+    f.ncomp = ncomp;
+    f.comp_stride = 1;
+    int64_t s = ncomp;
+    for (int d = n - 1; d >= 0; --d) {
+        f.stride[d] = s;
+        s *= f.extent[d];
+    }
+    return f;
+}
+
+int fill_impl(int n, int K, silo_field const* position, silo_field const* metric, silo_field* hodge)
+{
+    if (n < 1 || n > 3 || K < 0 || K > n) return -1;
+    if (hodge->ncomp != ipow(n, K) * binom(n, n - K)) return -1;
+    Geometry const geo {n, position, metric};
+    int64_t const total = num_nodes(*hodge);
+#pragma omp parallel for schedule(static)
+    for (int64_t flat = 0; flat < total; ++flat) {
+        int64_t local[MAXD], abs[MAXD];
+        unravel(*hodge, flat, local);
+        for (int d = 0; d < n; ++d) abs[d] = hodge->front[d] + local[d];
+        fill_node(geo, K, abs, hodge->data + offset_local(*hodge, local), hodge->comp_stride);
+    }
+    return 0;
+}
+
+// out[node] = hodge[node] . in[node] over every node of `out` (same lattice as in).
+void apply_field(int n, int const* dims, int K, silo_field const& hs, silo_field const& in, silo_field& out)
+{
+    int64_t const total = num_nodes(out);
+#pragma omp parallel for schedule(static)
+    for (int64_t flat = 0; flat < total; ++flat) {
+        int64_t local[MAXD], abs[MAXD], il[MAXD];
+        unravel(out, flat, local);
+        for (int d = 0; d < out.ndims; ++d) {
+            abs[d] = out.front[d] + local[d];
+            il[d] = abs[d] - in.front[d];
+        }
+        apply_node(n, K, hodge_at(hs, n, dims, abs), hs.comp_stride, in.data + offset_local(in, il),
+                   in.comp_stride, out.data + offset_local(out, local), out.comp_stride);
+    }
+}
+
+// dual-side kernel: sample `src` by d^T (zero outside) at each node of `out`,
+// then apply the stored Hodge tensor `hs` and the codifferential sign.
+// Ref: src/similie/exterior/codifferential.hpp:460-504; laplacian.hpp:110-152
+void transpose_star_field(int n, int const* dims, int src_rank, silo_field const& hs, silo_field const& src,
+                          silo_field& out, bool negate)
+{
+    auto const rules = face_rules(n, src_rank, true);
+    int const dual_k = src_rank + 1;
+    int64_t const total = num_nodes(out);
+#pragma omp parallel for schedule(static)
+    for (int64_t flat = 0; flat < total; ++flat) {
+        int64_t local[MAXD], abs[MAXD];
+        unravel(out, flat, local);
+        for (int d = 0; d < out.ndims; ++d) abs[d] = out.front[d] + local[d];
+        double dual_codiff[8];
+        for (std::size_t c = 0; c < rules.size(); ++c) {
+            double acc = 0.;
+            for (auto const& r : rules[c]) {
+                int64_t s[MAXD];
+                for (int d = 0; d < src.ndims; ++d) s[d] = abs[d];
+                for (int a = 0; a < n; ++a) s[dims[a]] += r.offset[a];
+                double v = 0.;
+                if (contains_abs(src, s)) {
+                    int64_t sl[MAXD];
+                    for (int d = 0; d < src.ndims; ++d) sl[d] = s[d] - src.front[d];
+                    v = src.data[offset_local(src, sl) + r.comp * src.comp_stride];
+                }
+                acc += (r.negative ? -1 : 1) * v;
+            }
+            dual_codiff[c] = -acc;
+        }
+        double* o = out.data + offset_local(out, local);
+        apply_node(n, dual_k, hodge_at(hs, n, dims, abs), hs.comp_stride, dual_codiff, 1, o, out.comp_stride);
+        if (negate) {
+            for (int c = 0; c < out.ncomp; ++c) o[c * out.comp_stride] *= -1;
+        }
+    }
+}
+
+// First kernel of codifferential_of_coboundary: clamped d then stored Hodge.
+// Ref: src/similie/exterior/laplacian.hpp:78-108
+void deriv_star_field(int n, int const* dims, int k, silo_field const& hs, silo_field const& in, silo_field& dual)
+{
+    auto const rules = face_rules(n, k, false);
+    int64_t const total = num_nodes(dual);
+#pragma omp parallel for schedule(static)
+    for (int64_t flat = 0; flat < total; ++flat) {
+        int64_t local[MAXD], abs[MAXD];
+        unravel(dual, flat, local);
+        for (int d = 0; d < dual.ndims; ++d) abs[d] = dual.front[d] + local[d];
+        double deriv[8];
+        for (std::size_t c = 0; c < rules.size(); ++c) {
+            double acc = 0.;
+            for (auto const& r : rules[c]) {
+                int64_t s[MAXD], sl[MAXD];
+                for (int d = 0; d < in.ndims; ++d) s[d] = abs[d];
+                for (int a = 0; a < n; ++a) s[dims[a]] += r.offset[a];
+                for (int d = 0; d < in.ndims; ++d) {
+                    s[d] = std::min(std::max(s[d], in.front[d]), in.front[d] + in.extent[d] - 1);
+                    sl[d] = s[d] - in.front[d];
+                }
+                acc += (r.negative ? -1 : 1) * in.data[offset_local(in, sl) + r.comp * in.comp_stride];
+            }
+            deriv[c] = acc;
+        }
+        apply_node(n, k + 1, hodge_at(hs, n, dims, abs), hs.comp_stride, deriv, 1,
+                   dual.data + offset_local(dual, local), dual.comp_stride);
+    }
+}
+
+bool sign_negative(int n, int k_plus_one)
+{
+    return (n * (k_plus_one + 1) + 1) % 2 == 1;
+}
+
+struct LaplacianHodges
+{
+    silo_field const* h[4];
+};
+
+int laplacian_impl(int n, int k, LaplacianHodges const& hs, silo_field const* in, silo_field* out)
+{
+    int dims[MAXD];
+    for (int d = 0; d < n; ++d) dims[d] = d;
+    if (in->ndims != n || out->ndims != n) return -1;
+    if (in->ncomp != binom(n, k) || out->ncomp != binom(n, k)) return -1;
+    std::vector<double> s1, s2, s3, s4;
+    if (k < n) {
+        // delta d: codifferential_of_coboundary (laplacian.hpp:27-155)
+        silo_field dual = make_buffer(*in, static_cast<int>(binom(n, n - k - 1)), s1);
+        deriv_star_field(n, dims, k, *hs.h[0], *in, dual);
+        transpose_star_field(n, dims, n - k - 1, *hs.h[1], dual, *out, sign_negative(n, k + 1));
+    }
+    if (k > 0) {
+        // d delta: StagedCodifferential::run then deriv (laplacian.hpp:614-631, 793-810)
+        silo_field dual = make_buffer(*in, static_cast<int>(binom(n, n - k)), s2);
+        apply_field(n, dims, k, *hs.h[2], *in, dual);
+        silo_field codiff = make_buffer(*in, static_cast<int>(binom(n, k - 1)), s3);
+        transpose_star_field(n, dims, n - k, *hs.h[3], dual, codiff, sign_negative(n, k));
+        if (k < n) {
+            silo_field cob = make_buffer(*out, out->ncomp, s4);
+            coboundary_impl((1u << n) - 1, k - 1, &codiff, &cob, false);
+            int64_t const total = num_nodes(*out);
+#pragma omp parallel for schedule(static)
+            for (int64_t flat = 0; flat < total; ++flat) {
+                int64_t local[MAXD];
+                unravel(*out, flat, local);
+                double* o = out->data + offset_local(*out, local);
+                double const* c = cob.data + offset_local(cob, local);
+                for (int comp = 0; comp < out->ncomp; ++comp) o[comp * out->comp_stride] += c[comp * cob.comp_stride];
+            }
+        } else {
+            coboundary_impl((1u << n) - 1, k - 1, &codiff, out, false);
+        }
+    }
+    return 0;
+}
+
+int hodge_kin(int n, int k, int which)
+{
+    switch (which) {
+    case 0: return k + 1;      // derivative Hodge: (k+1)-form -> (n-k-1)-form
+    case 1: return n - k;      // dual derivative Hodge: (n-k)-form -> k-form
+    case 2: return k;          // codifferential Hodge: k-form -> (n-k)-form
+    case 3: return n - k + 1;  // dual codifferential Hodge: (n-k+1)-form -> (k-1)-form
+    default: return -1;
+    }
+}
+
+bool hodge_needed(int n, int k, int which)
+{
+    return (which <= 1) ? (k < n) : (k > 0);
+}
+
+} // namespace
+
+extern "C" {
+
+int silo_coboundary(uint32_t form_mask, int k, const silo_field* in, silo_field* out)
+{
+    return coboundary_impl(form_mask, k, in, out, false);
+}
+
+int silo_transposed_coboundary(uint32_t form_mask, int k, const silo_field* in, silo_field* out)
+{
+    return coboundary_impl(form_mask, k, in, out, true);
+}
+
+int silo_fill_hodge_star(int n, int k_in, const silo_field* position, const silo_field* metric,
+                         silo_field* hodge)
+{
+    return fill_impl(n, k_in, position, metric, hodge);
+}
+
+int silo_apply_hodge_star(int n, int k_in, const silo_field* hodge, const silo_field* in, silo_field* out)
+{
+    int dims[MAXD];
+    for (int d = 0; d < n; ++d) dims[d] = d;
+    if (in->ncomp != binom(n, k_in) || out->ncomp != binom(n, n - k_in)) return -1;
+    apply_field(n, dims, k_in, *hodge, *in, *out);
+    return 0;
+}
+
+int silo_hodge_matrix(int n, int k_in, const silo_field* position, const silo_field* metric,
+                      const int64_t* node, double* matrix)
+{
+    if (n < 1 || n > 3 || k_in < 0 || k_in > n) return -1;
+    Geometry const geo {n, position, metric};
+    int64_t const nk = binom(n, k_in), nq = binom(n, n - k_in);
+    for (int64_t c = 0; c < nk; ++c) {
+        double unit[8] = {0}, resp[8] = {0};
+        unit[c] = 1.;
+        geo.discrete_star(node, k_in, unit, resp);
+        for (int64_t t = 0; t < nq; ++t) matrix[t * nk + c] = resp[t];
+    }
+    return 0;
+}
+
+int silo_codifferential(int n, int k, const silo_field* position, const silo_field* metric,
+                        const silo_field* in, silo_field* out)
+{
+    if (k < 1 || k > n || n > 3) return -1;
+    int dims[MAXD];
+    for (int d = 0; d < n; ++d) dims[d] = d;
+    std::vector<double> sh, sdh, sdual;
+    silo_field hs = make_hodge_field(*position, n, k, sh);
+    silo_field dhs = make_hodge_field(*position, n, n - k + 1, sdh);
+    fill_impl(n, k, position, metric, &hs);
+    fill_impl(n, n - k + 1, position, metric, &dhs);
+    silo_field dual = make_buffer(*in, static_cast<int>(binom(n, n - k)), sdual);
+    apply_field(n, dims, k, hs, *in, dual);
+    transpose_star_field(n, dims, n - k, dhs, dual, *out, sign_negative(n, k));
+    return 0;
+}
+
+int silo_laplacian_hodge_ncomp(int n, int k, int which)
+{
+    int const kin = hodge_kin(n, k, which);
+    if (kin < 0 || kin > n || !hodge_needed(n, k, which)) return 0;
+    return static_cast<int>(ipow(n, kin) * binom(n, n - kin));
+}
+
+int silo_laplacian_hodge_kin(int n, int k, int which)
+{
+    return hodge_kin(n, k, which);
+}
+
+int silo_laplacian(int n, int k, const silo_field* position, const silo_field* metric,
+                   const silo_field* in, silo_field* out)
+{
+    if (n < 1 || n > 3 || k < 0 || k > n) return -1;
+    std::vector<double> store[4];
+    silo_field fields[4];
+    LaplacianHodges hs {};
+    for (int w = 0; w < 4; ++w) {
+        if (!hodge_needed(n, k, w)) {
+            hs.h[w] = nullptr;
+            continue;
+        }
+        fields[w] = make_hodge_field(*position, n, hodge_kin(n, k, w), store[w]);
+        fill_impl(n, hodge_kin(n, k, w), position, metric, &fields[w]);
+        hs.h[w] = &fields[w];
+    }
+    return laplacian_impl(n, k, hs, in, out);
+}
+
+int silo_laplacian_prefilled(int n, int k, const silo_field* const* h, const silo_field* in, silo_field* out)
+{
+    LaplacianHodges hs {{h[0], h[1], h[2], h[3]}};
+    return laplacian_impl(n, k, hs, in, out);
+}
+
+// ------------------------------------------------------------------ magnetostatics
+
+// Ref: onelab_interface/magnetostatics_onelab.hpp:4491-4519
+void silo_mag2d_node_mu(int64_t nx, int64_t ny, const double* cell_mu, double mu0, double* node_mu)
+{
+    int64_t const ncx = nx - 1, ncy = ny - 1;
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ny; ++j) {
+        for (int64_t i = 0; i < nx; ++i) {
+            double acc = 0.;
+            int64_t count = 0;
+            for (int dj = -1; dj <= 0; ++dj) {
+                for (int di = -1; di <= 0; ++di) {
+                    int64_t const ci = i + di, cj = j + dj;
+                    if (ci < 0 || cj < 0 || ci >= ncx || cj >= ncy) continue;
+                    acc += cell_mu[ci + ncx * cj];
+                    ++count;
+                }
+            }
+            node_mu[i + nx * j] = count == 0 ? mu0 : acc / static_cast<double>(count);
+        }
+    }
+}
+
+// Ref: onelab_interface/magnetostatics_onelab.hpp:4414-4451
+void silo_mag2d_rhs(int64_t nx, int64_t ny, const double* x, const double* y, const double* cell_j, double* rhs)
+{
+    int64_t const ncx = nx - 1, ncy = ny - 1;
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ny; ++j) {
+        for (int64_t i = 0; i < nx; ++i) {
+            bool const boundary = i == 0 || j == 0 || i + 1 == nx || j + 1 == ny;
+            if (boundary) {
+                rhs[i + nx * j] = 0.;
+                continue;
+            }
+            double acc = 0.;
+            for (int dj = -1; dj <= 0; ++dj) {
+                for (int di = -1; di <= 0; ++di) {
+                    int64_t const ci = i + di, cj = j + dj;
+                    if (ci < 0 || cj < 0 || ci >= ncx || cj >= ncy) continue;
+                    double const area = (x[ci + 1] - x[ci]) * (y[cj + 1] - y[cj]);
+                    acc += 0.25 * area * cell_j[ci + ncx * cj];
+                }
+            }
+            rhs[i + nx * j] = acc;
+        }
+    }
+}
+
+namespace {
+inline double m0(int64_t nx, const double* a, int64_t i, int64_t j)
+{
+    double m = 0.;
+    m += -1. * a[i + nx * j];
+    m += 1. * a[i + nx * (j + 1)];
+    return m;
+}
+inline double m1(int64_t nx, const double* a, int64_t i, int64_t j)
+{
+    double m = 0.;
+    m += 1. * a[i + nx * j];
+    m += -1. * a[(i + 1) + nx * j];
+    return m;
+}
+} // namespace
+
+// Moments criterion (default): residual += c * (moment / mu) over the
+// interior sampled nodes whose moment stencil touches the row, in
+// ascending sampled-row order, X moments then Y moments.
+// Ref: onelab_interface/magnetostatics_onelab.hpp:1095-1258 (stencils), 1271-1426 (apply);
+//      src/similie/physics/magnetostatics/magnetostatics_quantities.hpp:100-123
+void silo_mag2d_apply(int64_t nx, int64_t ny, const double* mu, const double* a, double* y)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ny; ++j) {
+        for (int64_t i = 0; i < nx; ++i) {
+            int64_t const row = i + nx * j;
+            if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) {
+                y[row] = a[row];
+                continue;
+            }
+            double residual = 0.;
+            if (j - 1 >= 1) residual -= -1. * (m0(nx, a, i, j - 1) / mu[i + nx * (j - 1)]);
+            residual -= 1. * (m0(nx, a, i, j) / mu[row]);
+            if (i - 1 >= 1) residual -= 1. * (m1(nx, a, i - 1, j) / mu[(i - 1) + nx * j]);
+            residual -= -1. * (m1(nx, a, i, j) / mu[row]);
+            y[row] = residual;
+        }
+    }
+}
+
+void silo_mag2d_diagonal(int64_t nx, int64_t ny, const double* mu, double* diag)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ny; ++j) {
+        for (int64_t i = 0; i < nx; ++i) {
+            int64_t const row = i + nx * j;
+            if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) {
+                diag[row] = 1.;
+                continue;
+            }
+            double d = 0.;
+            if (j - 1 >= 1) d += 1. / mu[i + nx * (j - 1)];
+            d += 1. / mu[row];
+            if (i - 1 >= 1) d += 1. / mu[(i - 1) + nx * j];
+            d += 1. / mu[row];
+            diag[row] = d;
+        }
+    }
+}
+
+namespace {
+double dot(int64_t n, const double* a, const double* b)
+{
+    double s = 0.;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+} // namespace
+
+// Jacobi-preconditioned CG from x0 = 0 with the stopping rule
+// ||r_k|| <= tol * ||b|| (Ginkgo Cg + Jacobi + ResidualNorm reduction factor).
+// Ref: src/similie/solvers/minimize_strong_formulation_residual.hpp:1028-1304, 1308-1382
+int silo_mag2d_cg(int64_t nx, int64_t ny, const double* mu, const double* b, double* x, double tol,
+                  int max_iter, double* final_rel)
+{
+    int64_t const n = nx * ny;
+    std::vector<double> r(b, b + n), z(n), p(n), q(n), dinv(n);
+    silo_mag2d_diagonal(nx, ny, mu, dinv.data());
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        dinv[i] = 1. / dinv[i];
+        x[i] = 0.;
+        z[i] = dinv[i] * r[i];
+        p[i] = z[i];
+    }
+    double const bnorm = std::sqrt(dot(n, b, b));
+    double rz = dot(n, r.data(), z.data());
+    int it = 0;
+    double rnorm = bnorm;
+    if (bnorm == 0.) {
+        if (final_rel) *final_rel = 0.;
+        return 0;
+    }
+    while (it < max_iter) {
+        silo_mag2d_apply(nx, ny, mu, p.data(), q.data());
+        double const alpha = rz / dot(n, p.data(), q.data());
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * q[i];
+        }
+        ++it;
+        rnorm = std::sqrt(dot(n, r.data(), r.data()));
+        if (rnorm <= tol * bnorm) break;
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) z[i] = dinv[i] * r[i];
+        double const rz_new = dot(n, r.data(), z.data());
+        double const beta = rz_new / rz;
+        rz = rz_new;
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+    }
+    if (final_rel) *final_rel = rnorm / bnorm;
+    return it;
+}
+
+int silo_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+} // extern "C"

@@ -1,0 +1,112 @@
+/*
+ * sil_oracle.h -- CPU restatement of SimiLie's discrete-exterior-calculus
+ * operators and of its 2D magnetostatics residual solve.
+ *
+ * THIS IS TEST INFRASTRUCTURE. It is the correctness checker and the timed
+ * CPU baseline for the CUDA library in similie_b200/. Nothing in the product
+ * path links, loads or calls it.
+ *
+ * Every function follows the reference algorithm step by step (chain
+ * construction, boundary orientation, summation order, clamped / zero-outside
+ * sampling, stored per-node Hodge-star tensors, staged kernels). The file and
+ * line of the reference code each routine restates is given at its
+ * definition in sil_oracle.cpp.
+ *
+ * Field convention: a field is a strided array over up to SILO_MAX_DIMS
+ * lattice dimensions plus one component index.  `front` is the absolute
+ * lattice coordinate of element 0 along each dimension (DDC's domain front);
+ * sampling between fields is done in absolute coordinates, exactly like
+ * DDC's DiscreteElement arithmetic.  Form dimensions (those the exterior
+ * algebra acts on) are selected by a bit mask; the other dimensions are
+ * spectators (batch) and are never shifted.
+ */
+#ifndef SIL_ORACLE_H
+#define SIL_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SILO_MAX_DIMS 6
+
+typedef struct silo_field {
+    double* data;
+    int32_t ndims;
+    int32_t ncomp;
+    int64_t front[SILO_MAX_DIMS];
+    int64_t extent[SILO_MAX_DIMS];
+    int64_t stride[SILO_MAX_DIMS];
+    int64_t comp_stride;
+} silo_field;
+
+/* Coboundary d on a k-form (clamped sampling).  out has C(n,k+1) comps. */
+int silo_coboundary(uint32_t form_mask, int k, const silo_field* in, silo_field* out);
+
+/* Transposed coboundary on a k-form (zero-outside sampling, backward shift,
+ * final negation).  out has C(n,k+1) comps. */
+int silo_transposed_coboundary(uint32_t form_mask, int k, const silo_field* in, silo_field* out);
+
+/* Fill the stored per-node discrete Hodge star tensor mapping k_in-forms to
+ * (n-k_in)-forms: layout per node [n^k_in full tuples][C(n,n-k_in) comps].
+ * position: n comps per node; metric: n*n comps per node (row-major) or
+ * NULL for the identity metric.  hodge->ncomp must be n^k_in * C(n, n-k_in).
+ * The lattice of `hodge`, `position` and `metric` spans the form dims only. */
+int silo_fill_hodge_star(int n, int k_in, const silo_field* position, const silo_field* metric,
+                         silo_field* hodge);
+
+/* Apply a stored Hodge tensor at every node of `in` (k_in-form) into `out`. */
+int silo_apply_hodge_star(int n, int k_in, const silo_field* hodge, const silo_field* in,
+                          silo_field* out);
+
+/* Effective per-node Hodge matrix (C(n,n-k) x C(n,k), row-major) at one
+ * node, computed by DiscreteHodgeStar::run on unit cochains. */
+int silo_hodge_matrix(int n, int k_in, const silo_field* position, const silo_field* metric,
+                      const int64_t* node, double* matrix);
+
+/* Staged codifferential of a k-form (k >= 1): reference two-kernel structure. */
+int silo_codifferential(int n, int k, const silo_field* position, const silo_field* metric,
+                        const silo_field* in, silo_field* out);
+
+/* Staged Hodge Laplacian of a k-form (0 <= k <= n): reference kernel chain
+ * (delta d for k = 0, delta d + d delta for 0 < k < n, d delta for k = n). */
+int silo_laplacian(int n, int k, const silo_field* position, const silo_field* metric,
+                   const silo_field* in, silo_field* out);
+
+/* Same chain with the Hodge tensors supplied by the caller (setup excluded
+ * from timing).  hs[0..3] = derivative, dual-derivative, codifferential,
+ * dual-codifferential stored Hodge tensors (unused ones may be NULL). */
+int silo_laplacian_prefilled(int n, int k, const silo_field* const* hs, const silo_field* in,
+                             silo_field* out);
+
+/* Component counts of the stored Hodge tensors silo_laplacian_prefilled needs. */
+int silo_laplacian_hodge_ncomp(int n, int k, int which);
+int silo_laplacian_hodge_kin(int n, int k, int which);
+
+/* ------------------------------------------------------------------ */
+/* 2D linear magnetostatics (x-fastest flat layout row = i + nx*j).     */
+
+/* Node permeability: mean of the (up to 4) adjacent cell values. */
+void silo_mag2d_node_mu(int64_t nx, int64_t ny, const double* cell_mu, double mu0,
+                        double* node_mu);
+/* Right-hand side b_i = sum over adjacent cells of 1/4 * area * J, 0 on the boundary. */
+void silo_mag2d_rhs(int64_t nx, int64_t ny, const double* x, const double* y,
+                    const double* cell_j, double* rhs);
+/* Matrix-free residual operator (moments criterion), identity rows on the boundary. */
+void silo_mag2d_apply(int64_t nx, int64_t ny, const double* node_mu, const double* a, double* y);
+/* Diagonal of the assembled operator (Jacobi preconditioner). */
+void silo_mag2d_diagonal(int64_t nx, int64_t ny, const double* node_mu, double* diag);
+/* Jacobi-preconditioned CG from x = 0, stop when ||r|| <= tol * ||b||.
+ * Returns iterations; *final_rel receives the recurrence relative residual. */
+int silo_mag2d_cg(int64_t nx, int64_t ny, const double* node_mu, const double* rhs,
+                  double* x, double tol, int max_iter, double* final_rel);
+
+/* Threads OpenMP uses (for reporting). */
+int silo_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

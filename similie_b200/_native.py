@@ -1,0 +1,126 @@
+"""ctypes binding of libsil_b200.so (the sm_100a C ABI in include/sil_b200.h).
+
+The library is built in-tree by similie_b200/build.py.  Loading fails loudly
+when it is missing: there is no CPU implementation behind this API.
+"""
+import ctypes
+import os
+
+SIL_MAX_DIMS = 6
+SIL_OK = 0
+SIL_F64 = 0
+SIL_F32 = 1
+
+STATUS_NAMES = {
+    0: "SIL_OK", 1: "SIL_ERR_INVALID", 2: "SIL_ERR_UNSUPPORTED", 3: "SIL_ERR_CUDA",
+    4: "SIL_ERR_ALLOC", 5: "SIL_ERR_NONFINITE", 6: "SIL_ERR_STALLED", 7: "SIL_ERR_BUDGET",
+}
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsil_b200.so")
+
+
+class SilField(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("dtype", ctypes.c_int32),
+        ("ndims", ctypes.c_int32),
+        ("ncomp", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("front", ctypes.c_int64 * SIL_MAX_DIMS),
+        ("extent", ctypes.c_int64 * SIL_MAX_DIMS),
+        ("stride", ctypes.c_int64 * SIL_MAX_DIMS),
+        ("comp_stride", ctypes.c_int64),
+    ]
+
+
+class SilMag2dProblem(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int64),
+        ("ny", ctypes.c_int64),
+        ("node_mu", ctypes.c_void_p),
+        ("rhs", ctypes.c_void_p),
+        ("solution", ctypes.c_void_p),
+    ]
+
+
+class SilSolveSettings(ctypes.Structure):
+    _fields_ = [
+        ("solver", ctypes.c_int32),
+        ("max_iterations", ctypes.c_int32),
+        ("relative_tolerance", ctypes.c_double),
+        ("inner_iterations", ctypes.c_int32),
+        ("inner_tolerance", ctypes.c_double),
+    ]
+
+
+class SilSolveDiagnostics(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int32),
+        ("converged", ctypes.c_int32),
+        ("refinements", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("initial_residual_l2", ctypes.c_double),
+        ("final_residual_l2", ctypes.c_double),
+        ("final_relative_residual", ctypes.c_double),
+    ]
+
+
+class SilError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+# (name, restype, argtypes) for every symbol include/sil_b200.h declares.
+_P = ctypes.c_void_p
+_F = ctypes.POINTER(SilField)
+SIGNATURES = [
+    ("sil_status_string", ctypes.c_char_p, [ctypes.c_int]),
+    ("sil_last_error", ctypes.c_char_p, []),
+    ("sil_deriv", ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_int, _F, _F]),
+    ("sil_transposed_coboundary", ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_int, _F, _F]),
+    ("sil_geometry_create", ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+    ("sil_geometry_destroy", ctypes.c_int, [_P]),
+    ("sil_hodge_star", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_int, _F, _F]),
+    ("sil_fill_discrete_hodge_star", ctypes.c_int, [_P, _P, ctypes.c_int, _F]),
+    ("sil_codifferential", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_int, _F, _F]),
+    ("sil_laplacian_plan_create", ctypes.c_int, [ctypes.POINTER(_P), _P, ctypes.c_uint32, ctypes.c_int, _F, _F,
+                                                 ctypes.c_int]),
+    ("sil_laplacian_run", ctypes.c_int, [_P, _P, _F, _F]),
+    ("sil_laplacian_plan_destroy", ctypes.c_int, [_P]),
+    ("sil_laplacian_plan_scratch_bytes", ctypes.c_size_t, [_P]),
+    ("sil_laplacian_plan_kernel", ctypes.c_int, [_P]),
+    ("sil_laplacian_plan_status", ctypes.c_int, [_P]),
+    ("sil_laplacian", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_int, _F, _F]),
+    ("sil_mag2d_apply", ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, _P, _P]),
+    ("sil_mag2d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag2dProblem), ctypes.c_int,
+                                             ctypes.POINTER(SilSolveSettings),
+                                             ctypes.POINTER(SilSolveDiagnostics), _P]),
+]
+
+
+def lib():
+    """Load the CUDA library (building it first if sources are newer)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build as _build
+            _build.build()
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"similie_b200: CUDA library {LIB_PATH} is missing; run similie_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status, what=""):
+    if status != SIL_OK:
+        msg = lib().sil_last_error().decode(errors="replace")
+        raise SilError(status, f"{what}: {msg}" if what else msg)

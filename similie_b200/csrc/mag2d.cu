@@ -1,0 +1,636 @@
+// mag2d.cu -- 2D linear magnetostatics on the GPU: the matrix-free residual
+// operator d^T (nu d A) with identity rows on the Dirichlet boundary, and a
+// batched Jacobi-preconditioned conjugate-gradient solve (FP64, or FP32
+// inner sweeps inside FP64 iterative refinement).
+//
+// Operator (onelab_interface/magnetostatics_onelab.hpp:1271-1426 with the
+// moment stencils of magnetostatics_quantities.hpp:100-123 built at
+// 1095-1258): for an interior node (i,j), over the interior sampled nodes s
+// whose moment stencil touches the row,
+//   y = sum_s c(s->row) * moment(s) / mu(s)
+// with moment0(s) = A(s+ey) - A(s) (c = +1 at s+ey, -1 at s) and
+// moment1(s) = A(s) - A(s+ex) (c = -1 at s+ex, +1 at s); X moments first,
+// sampled nodes in ascending flat order.  Boundary rows are the identity.
+// Sampled nodes on the first row/column are excluded, as in the reference.
+//
+// Solver (minimize_strong_formulation_residual.hpp:1028-1304): CG from
+// x = 0 with the inverse diagonal as preconditioner, stopped when
+// ||r|| <= tol ||b||; the final residual is re-evaluated in FP64.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "sil_internal.cuh"
+
+namespace sil {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kNodesPerThread = 8;
+constexpr int kItemNodes = kThreads * kNodesPerThread;  // nodes per work item (one CTA)
+
+// ------------------------------------------------------------------ operator
+
+template <class T>
+__device__ __forceinline__ T mag_apply_node(T const* a, T const* nu, int64_t nx, int64_t ny, int64_t row)
+{
+    int64_t const i = row % nx, j = row / nx;
+    if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) return a[row];
+    T const a0 = a[row];
+    T residual = T(0);
+    if (j >= 2) {
+        int64_t const s = row - nx;
+        T m0 = T(0);
+        m0 = m0 - a[s];
+        m0 = m0 + a0;
+        residual = residual + m0 * nu[s];  // c = +1
+    }
+    {
+        T m0 = T(0);
+        m0 = m0 - a0;
+        m0 = m0 + a[row + nx];
+        residual = residual - m0 * nu[row];  // c = -1
+    }
+    if (i >= 2) {
+        int64_t const s = row - 1;
+        T m1 = T(0);
+        m1 = m1 + a[s];
+        m1 = m1 - a0;
+        residual = residual - m1 * nu[s];  // c = -1
+    }
+    {
+        T m1 = T(0);
+        m1 = m1 + a0;
+        m1 = m1 - a[row + 1];
+        residual = residual + m1 * nu[row];  // c = +1
+    }
+    return residual;
+}
+
+__global__ void mag_apply_kernel(double const* nu, double const* a, double* y, int64_t nx, int64_t ny)
+{
+    int64_t const row = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (row >= nx * ny) return;
+    y[row] = mag_apply_node(a, nu, nx, ny, row);
+}
+
+__global__ void reciprocal_kernel(double const* mu, double* nu, int64_t n)
+{
+    int64_t const i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i < n) nu[i] = 1.0 / mu[i];
+}
+
+// ------------------------------------------------------------------ batched CG
+
+struct Item
+{
+    int prob;
+    int index;  // item index within its problem
+    int64_t begin;
+    int64_t end;
+};
+
+template <class T>
+struct Vecs
+{
+    T* x;
+    T* r;
+    T* z;
+    T* p;
+    T* q;
+    T* dinv;
+    T* nu;
+};
+
+struct ProbInfo
+{
+    int64_t nx, ny, n;
+    int nitems;
+    int first_item;
+};
+
+struct Scalars
+{
+    double rz;        // r . z of the current iterate
+    double rr;        // r . r
+    double rr0;       // r . r at the start of the (inner) solve
+    double bb;        // b . b (outer right-hand side)
+    double alpha, beta;
+    double scale;     // outer residual norm used to scale the inner right-hand side
+    int done;         // inner / plain solve finished
+    int outer_done;   // refinement finished
+    int iters;        // iterations of the current solve
+    int total_iters;  // all inner iterations
+    int nonfinite;
+    int counter_a, counter_b, counter_c;
+};
+
+// Deterministic block sum of one double per thread.
+__device__ __forceinline__ double block_sum(double v, double* smem)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int const warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    __syncthreads();
+    if (lane == 0) smem[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < kThreads / 32; ++w) t += smem[w];
+    }
+    return t;  // valid in thread 0
+}
+
+// Last-CTA-of-the-problem reduction: returns true in the thread that must
+// finalize, with `out` holding the ordered sum of the problem's partials.
+__device__ bool finish_reduction(double partial, double* partials, int item_index, int first_item, int nitems,
+                                 int* counter, double* out)
+{
+    __shared__ bool is_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        partials[first_item + item_index] = partial;
+        __threadfence();
+        int const prev = atomicAdd(counter, 1);
+        is_last = prev == nitems - 1;
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        double s = 0.0;
+        for (int k = 0; k < nitems; ++k) s += __ldcg(partials + first_item + k);
+        *out = s;
+        *counter = 0;
+        return true;
+    }
+    return false;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) cg_init_kernel(Item const* items, ProbInfo const* info, Vecs<T> const* vecs,
+                                                           double const* const* rhs64, double const* const* r64,
+                                                           Scalars* sc, double* part_a, double* part_b, bool from_r64)
+{
+    __shared__ double red[kThreads / 32];
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->outer_done) return;
+    ProbInfo const pi = info[it.prob];
+    Vecs<T> const v = vecs[it.prob];
+    double const scale = from_r64 ? s->scale : 1.0;
+    double rz = 0.0, bb = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        double const b = from_r64 ? r64[it.prob][row] / scale : rhs64[it.prob][row];
+        T const r = static_cast<T>(b);
+        T const z = v.dinv[row] * r;
+        v.x[row] = T(0);
+        v.r[row] = r;
+        v.z[row] = z;
+        v.p[row] = z;
+        rz += static_cast<double>(r) * static_cast<double>(z);
+        bb += static_cast<double>(r) * static_cast<double>(r);
+    }
+    double const rz_b = block_sum(rz, red);
+    double const bb_b = block_sum(bb, red);
+    double tot_rz = 0.0, tot_bb = 0.0;
+    bool const last_a = finish_reduction(rz_b, part_a, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot_rz);
+    bool const last_b = finish_reduction(bb_b, part_b, it.index, pi.first_item, pi.nitems, &s->counter_b, &tot_bb);
+    (void)last_a;
+    if (last_b && threadIdx.x == 0) {
+        // Both reductions are complete once this CTA is the last of the second.
+        __threadfence();
+        double trz = 0.0;
+        for (int k = 0; k < pi.nitems; ++k) trz += __ldcg(part_a + pi.first_item + k);
+        s->rz = trz;
+        s->rr = tot_bb;
+        s->rr0 = tot_bb;
+        if (!from_r64) s->bb = tot_bb;
+        s->iters = 0;
+        s->done = (tot_bb == 0.0) ? 1 : 0;
+        s->nonfinite = 0;
+    }
+}
+
+// q = A p and the partial p.q; the problem's last CTA forms alpha = rz / (p.q).
+template <class T>
+__global__ void __launch_bounds__(kThreads) cg_apply_kernel(Item const* items, ProbInfo const* info, Vecs<T> const* vecs,
+                                                            Scalars* sc, double* part)
+{
+    __shared__ double red[kThreads / 32];
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->done || s->outer_done) return;
+    ProbInfo const pi = info[it.prob];
+    Vecs<T> const v = vecs[it.prob];
+    double pq = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        T const q = mag_apply_node(v.p, v.nu, pi.nx, pi.ny, row);
+        v.q[row] = q;
+        pq += static_cast<double>(v.p[row]) * static_cast<double>(q);
+    }
+    double const pq_b = block_sum(pq, red);
+    double tot = 0.0;
+    if (finish_reduction(pq_b, part, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot)) {
+        s->alpha = s->rz / tot;
+        if (!isfinite(s->alpha)) s->nonfinite = 1;
+    }
+}
+
+// x += alpha p, r -= alpha q, z = dinv r; partials r.z and r.r; the last CTA
+// forms beta and decides convergence.
+template <class T>
+__global__ void __launch_bounds__(kThreads) cg_update_kernel(Item const* items, ProbInfo const* info,
+                                                             Vecs<T> const* vecs, Scalars* sc, double* part_a,
+                                                             double* part_b, double tol2)
+{
+    __shared__ double red[kThreads / 32];
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->done || s->outer_done) return;
+    ProbInfo const pi = info[it.prob];
+    Vecs<T> const v = vecs[it.prob];
+    T const alpha = static_cast<T>(s->alpha);
+    double rz = 0.0, rr = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        T const x = v.x[row] + alpha * v.p[row];
+        T const r = v.r[row] - alpha * v.q[row];
+        T const z = v.dinv[row] * r;
+        v.x[row] = x;
+        v.r[row] = r;
+        v.z[row] = z;
+        rz += static_cast<double>(r) * static_cast<double>(z);
+        rr += static_cast<double>(r) * static_cast<double>(r);
+    }
+    double const rz_b = block_sum(rz, red);
+    double const rr_b = block_sum(rr, red);
+    double tot_rz = 0.0, tot_rr = 0.0;
+    finish_reduction(rz_b, part_a, it.index, pi.first_item, pi.nitems, &s->counter_b, &tot_rz);
+    if (finish_reduction(rr_b, part_b, it.index, pi.first_item, pi.nitems, &s->counter_c, &tot_rr)) {
+        __threadfence();
+        double trz = 0.0;
+        for (int k = 0; k < pi.nitems; ++k) trz += __ldcg(part_a + pi.first_item + k);
+        s->beta = trz / s->rz;
+        s->rz = trz;
+        s->rr = tot_rr;
+        s->iters += 1;
+        s->total_iters += 1;
+        if (!isfinite(tot_rr) || !isfinite(trz)) s->nonfinite = 1;
+        if (tot_rr <= tol2 * s->rr0 || s->nonfinite) s->done = 1;
+    }
+}
+
+// p = z + beta p (skipped once converged).
+template <class T>
+__global__ void __launch_bounds__(kThreads) cg_direction_kernel(Item const* items, Vecs<T> const* vecs, Scalars* sc)
+{
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->done || s->outer_done) return;
+    Vecs<T> const v = vecs[it.prob];
+    T const beta = static_cast<T>(s->beta);
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) v.p[row] = v.z[row] + beta * v.p[row];
+}
+
+// r64 = b - A x64 and its norm (outer residual, FP64); marks outer convergence.
+__global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items, ProbInfo const* info,
+                                                              double const* const* nu64, double const* const* rhs,
+                                                              double* const* x64, double* const* r64, Scalars* sc,
+                                                              double* part, double tol2, int mark)
+{
+    __shared__ double red[kThreads / 32];
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->outer_done) return;
+    ProbInfo const pi = info[it.prob];
+    double rr = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        double const ax = mag_apply_node(x64[it.prob], nu64[it.prob], pi.nx, pi.ny, row);
+        double const r = rhs[it.prob][row] - ax;
+        r64[it.prob][row] = r;
+        rr += r * r;
+    }
+    double const rr_b = block_sum(rr, red);
+    double tot = 0.0;
+    if (finish_reduction(rr_b, part, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot)) {
+        s->rr = tot;
+        s->scale = sqrt(tot);
+        if (mark && (tot <= tol2 * s->bb || !isfinite(tot))) s->outer_done = 1;
+        if (!isfinite(tot)) s->nonfinite = 1;
+    }
+}
+
+// x64 += scale * e (inner correction, promoted to FP64).
+template <class T>
+__global__ void __launch_bounds__(kThreads) refine_kernel(Item const* items, Vecs<T> const* vecs, double* const* x64,
+                                                          Scalars const* sc)
+{
+    Item const it = items[blockIdx.x];
+    Scalars const* s = sc + it.prob;
+    if (s->outer_done) return;
+    T const* e = vecs[it.prob].x;
+    double const scale = s->scale;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads)
+        x64[it.prob][row] += scale * static_cast<double>(e[row]);
+}
+
+// nu = 1/mu (FP64 and, for the inner solve, the precision T) and the
+// inverse diagonal of the operator.
+template <class T>
+__global__ void setup_kernel(Item const* items, ProbInfo const* info, double const* const* mu, double* const* nu64,
+                             Vecs<T> const* vecs)
+{
+    Item const it = items[blockIdx.x];
+    ProbInfo const pi = info[it.prob];
+    Vecs<T> const v = vecs[it.prob];
+    double const* m = mu[it.prob];
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        double const nu = 1.0 / m[row];
+        nu64[it.prob][row] = nu;
+        v.nu[row] = static_cast<T>(nu);
+        int64_t const i = row % pi.nx, j = row / pi.nx;
+        double d = 1.0;
+        if (!(i == 0 || j == 0 || i + 1 == pi.nx || j + 1 == pi.ny)) {
+            d = 0.0;
+            if (j >= 2) d += 1.0 / m[row - pi.nx];
+            d += nu;
+            if (i >= 2) d += 1.0 / m[row - 1];
+            d += nu;
+        }
+        v.dinv[row] = static_cast<T>(1.0 / d);
+    }
+}
+
+__global__ void copy_kernel(Item const* items, double const* const* src, double* const* dst, Scalars const* sc)
+{
+    Item const it = items[blockIdx.x];
+    (void)sc;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) dst[it.prob][row] = src[it.prob][row];
+}
+
+template <class T>
+__global__ void copy_from_vec_kernel(Item const* items, Vecs<T> const* vecs, double* const* dst)
+{
+    Item const it = items[blockIdx.x];
+    T const* x = vecs[it.prob].x;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) dst[it.prob][row] = static_cast<double>(x[row]);
+}
+
+// ------------------------------------------------------------------ host driver
+
+struct DeviceBuffer
+{
+    void* ptr = nullptr;
+    ~DeviceBuffer() { cudaFree(ptr); }
+};
+
+template <class T>
+sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_settings const& set, sil_solve_diagnostics* diag,
+                       cudaStream_t stream, bool mixed)
+{
+    // Work items: contiguous node ranges of kItemNodes per problem.
+    std::vector<Item> items;
+    std::vector<ProbInfo> info(np);
+    int64_t total_nodes = 0;
+    for (int p = 0; p < np; ++p) {
+        int64_t const n = probs[p].nx * probs[p].ny;
+        info[p] = {probs[p].nx, probs[p].ny, n, 0, static_cast<int>(items.size())};
+        int idx = 0;
+        for (int64_t b = 0; b < n; b += kItemNodes, ++idx) items.push_back({p, idx, b, std::min(n, b + kItemNodes)});
+        info[p].nitems = idx;
+        total_nodes += n;
+    }
+    int const nitems = static_cast<int>(items.size());
+    int const nvec = 7;  // x r z p q dinv nu in precision T
+    size_t const vec_bytes = ((total_nodes * sizeof(T) + 255) / 256) * 256;
+    size_t const d_bytes = ((total_nodes * sizeof(double) + 255) / 256) * 256;
+    size_t const ndouble_vecs = mixed ? 3 : 1;  // nu64 (+ r64, x64 when mixed)
+    size_t bytes = nvec * vec_bytes + ndouble_vecs * d_bytes;
+    bytes += sizeof(Item) * nitems + sizeof(ProbInfo) * np + sizeof(Vecs<T>) * np + sizeof(Scalars) * np
+             + 3 * sizeof(double) * nitems + 7 * sizeof(void*) * np + 4096;
+    DeviceBuffer buf;
+    SIL_CUDA_CHECK(cudaMalloc(&buf.ptr, bytes));
+    char* base = static_cast<char*>(buf.ptr);
+    auto take = [&](size_t b) {
+        char* r = base;
+        base += (b + 255) / 256 * 256;
+        return r;
+    };
+    T* vec_base[nvec];
+    for (int k = 0; k < nvec; ++k) vec_base[k] = reinterpret_cast<T*>(take(vec_bytes));
+    double* nu64_base = reinterpret_cast<double*>(take(d_bytes));
+    double* r64_base = mixed ? reinterpret_cast<double*>(take(d_bytes)) : nullptr;
+    double* x64_base = mixed ? reinterpret_cast<double*>(take(d_bytes)) : nullptr;
+    Item* d_items = reinterpret_cast<Item*>(take(sizeof(Item) * nitems));
+    ProbInfo* d_info = reinterpret_cast<ProbInfo*>(take(sizeof(ProbInfo) * np));
+    Vecs<T>* d_vecs = reinterpret_cast<Vecs<T>*>(take(sizeof(Vecs<T>) * np));
+    Scalars* d_sc = reinterpret_cast<Scalars*>(take(sizeof(Scalars) * np));
+    double* part_a = reinterpret_cast<double*>(take(sizeof(double) * nitems));
+    double* part_b = reinterpret_cast<double*>(take(sizeof(double) * nitems));
+    double* part_c = reinterpret_cast<double*>(take(sizeof(double) * nitems));
+    double const** d_mu = reinterpret_cast<double const**>(take(sizeof(void*) * np));
+    double const** d_rhs = reinterpret_cast<double const**>(take(sizeof(void*) * np));
+    double** d_nu64 = reinterpret_cast<double**>(take(sizeof(void*) * np));
+    double** d_x64 = reinterpret_cast<double**>(take(sizeof(void*) * np));
+    double** d_r64 = reinterpret_cast<double**>(take(sizeof(void*) * np));
+    double** d_sol = reinterpret_cast<double**>(take(sizeof(void*) * np));
+    double** d_scratch = reinterpret_cast<double**>(take(sizeof(void*) * np));
+
+    std::vector<Vecs<T>> vecs(np);
+    std::vector<double const*> mu(np), rhs(np);
+    std::vector<double*> nu64(np), x64(np), r64(np);
+    int64_t off = 0;
+    for (int p = 0; p < np; ++p) {
+        vecs[p] = {vec_base[0] + off, vec_base[1] + off, vec_base[2] + off, vec_base[3] + off,
+                   vec_base[4] + off, vec_base[5] + off, vec_base[6] + off};
+        mu[p] = probs[p].node_mu;
+        rhs[p] = probs[p].rhs;
+        nu64[p] = nu64_base + off;
+        x64[p] = mixed ? x64_base + off : probs[p].solution;
+        r64[p] = mixed ? r64_base + off : nullptr;
+        off += info[p].n;
+    }
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_items, items.data(), sizeof(Item) * nitems, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_info, info.data(), sizeof(ProbInfo) * np, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_vecs, vecs.data(), sizeof(Vecs<T>) * np, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_mu, mu.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_rhs, rhs.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_nu64, nu64.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_x64, x64.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_r64, r64.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, stream));
+    std::vector<double*> sol(np), scratch(np);
+    for (int p = 0; p < np; ++p) {
+        sol[p] = probs[p].solution;
+        // FP64 scratch for the final true residual: r64 when refining, else the (FP64) q vectors.
+        scratch[p] = mixed ? r64[p] : reinterpret_cast<double*>(vecs[p].q);
+    }
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_sol, sol.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_scratch, scratch.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemsetAsync(d_sc, 0, sizeof(Scalars) * np, stream));
+
+    setup_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_mu, d_nu64, d_vecs);
+    SIL_CUDA_CHECK(cudaGetLastError());
+
+    double const tol = set.relative_tolerance > 0 ? set.relative_tolerance : 1e-10;
+    int const max_iter = set.max_iterations > 0 ? set.max_iterations : 100000;
+    int const chunk = 32;
+    std::vector<Scalars> hs(np);
+
+    // One chunk of CG iterations, captured once as a CUDA graph.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto capture = [&](double tol2) -> sil_status {
+        if (exec != nullptr) {
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+        if (graph != nullptr) {
+            cudaGraphDestroy(graph);
+            graph = nullptr;
+        }
+        cudaStream_t cs;
+        SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        for (int c = 0; c < chunk && err == cudaSuccess; ++c) {
+            cg_apply_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a);
+            cg_update_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_b, part_c, tol2);
+            cg_direction_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc);
+        }
+        cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
+        if (err == cudaSuccess) err = err2;
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+        cudaStreamDestroy(cs);
+        if (err != cudaSuccess) return cuda_fail(err, "solver graph capture");
+        return SIL_OK;
+    };
+    auto run_until_done = [&](int budget, int* used) -> sil_status {
+        int spent = 0;
+        while (spent < budget) {
+            SIL_CUDA_CHECK(cudaGraphLaunch(exec, stream));
+            spent += chunk;
+            SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
+            SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+            bool all = true;
+            for (int p = 0; p < np; ++p) all = all && (hs[p].done || hs[p].outer_done);
+            if (all) break;
+        }
+        *used = spent;
+        return SIL_OK;
+    };
+
+    sil_status st = SIL_OK;
+    int refinements = 0;
+    if (!mixed) {
+        cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, d_rhs, nullptr, d_sc, part_a,
+                                                           part_b, false);
+        SIL_CUDA_CHECK(cudaGetLastError());
+        st = capture(tol * tol);
+        int used = 0;
+        if (st == SIL_OK) st = run_until_done(max_iter, &used);
+        if (st == SIL_OK) {
+            copy_from_vec_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_x64);
+        }
+    } else {
+        double const inner_tol = set.inner_tolerance > 0 ? set.inner_tolerance : 1e-4;
+        int const inner_max = set.inner_iterations > 0 ? set.inner_iterations : 4000;
+        st = capture(inner_tol * inner_tol);
+        SIL_CUDA_CHECK(cudaMemsetAsync(x64_base, 0, d_bytes, stream));
+        // bb = ||b||^2 via an init pass from the right-hand side.
+        cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, d_rhs, nullptr, d_sc, part_a,
+                                                           part_b, false);
+        int total = 0;
+        while (st == SIL_OK && total < max_iter) {
+            residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc,
+                                                               part_a, tol * tol, 1);
+            SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
+            SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+            bool all = true;
+            for (int p = 0; p < np; ++p) all = all && hs[p].outer_done;
+            if (all) break;
+            cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, nullptr, d_r64, d_sc, part_a,
+                                                               part_b, true);
+            int used = 0;
+            st = run_until_done(std::min(inner_max, max_iter - total), &used);
+            total += used;
+            refine_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_x64, d_sc);
+            ++refinements;
+        }
+        if (st == SIL_OK) copy_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_x64, d_sol, d_sc);
+    }
+    if (exec != nullptr) cudaGraphExecDestroy(exec);
+    if (graph != nullptr) cudaGraphDestroy(graph);
+    if (st != SIL_OK) return st;
+
+    // FP64 true residual ||b - A x|| of the returned solution for every problem.
+    std::vector<Scalars> hs2(np);
+    SIL_CUDA_CHECK(cudaMemcpyAsync(hs2.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
+    SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+    for (int p = 0; p < np; ++p) {
+        hs2[p].outer_done = 0;
+        hs2[p].counter_a = hs2[p].counter_b = hs2[p].counter_c = 0;
+    }
+    SIL_CUDA_CHECK(cudaMemcpyAsync(d_sc, hs2.data(), sizeof(Scalars) * np, cudaMemcpyHostToDevice, stream));
+    residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_sol, d_scratch, d_sc, part_a,
+                                                       tol * tol, 0);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
+    SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+    sil_status overall = SIL_OK;
+    for (int p = 0; p < np; ++p) {
+        sil_solve_diagnostics& d = diag[p];
+        d.iterations = mixed ? hs[p].total_iters : hs[p].iters;
+        d.refinements = refinements;
+        d.initial_residual_l2 = std::sqrt(hs[p].bb);
+        d.final_residual_l2 = std::sqrt(hs[p].rr);
+        d.final_relative_residual = hs[p].bb > 0 ? std::sqrt(hs[p].rr / hs[p].bb) : 0.0;
+        d.converged = d.final_relative_residual <= tol && !hs[p].nonfinite;
+        d.status = hs[p].nonfinite ? SIL_ERR_NONFINITE : SIL_OK;
+        if (hs[p].nonfinite) overall = SIL_ERR_NONFINITE;
+    }
+    if (overall != SIL_OK) set_error("a problem of the batch met a non-finite value");
+    return overall;
+}
+
+} // namespace
+
+} // namespace sil
+
+using namespace sil;
+
+extern "C" {
+
+sil_status sil_mag2d_apply(sil_stream stream, int64_t nx, int64_t ny, const double* node_mu, const double* a, double* y)
+{
+    if (nx < 3 || ny < 3) return fail(SIL_ERR_INVALID, "sil_mag2d_apply: need at least 3x3 nodes");
+    if (node_mu == nullptr || a == nullptr || y == nullptr) return fail(SIL_ERR_INVALID, "sil_mag2d_apply: NULL pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int64_t const n = nx * ny;
+    DeviceBuffer nu;
+    SIL_CUDA_CHECK(cudaMallocAsync(&nu.ptr, n * sizeof(double), s));
+    int const blocks = static_cast<int>((n + 255) / 256);
+    reciprocal_kernel<<<blocks, 256, 0, s>>>(node_mu, static_cast<double*>(nu.ptr), n);
+    mag_apply_kernel<<<blocks, 256, 0, s>>>(static_cast<double*>(nu.ptr), a, y, nx, ny);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    SIL_CUDA_CHECK(cudaFreeAsync(nu.ptr, s));
+    nu.ptr = nullptr;
+    return SIL_OK;
+}
+
+sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblems, const sil_solve_settings* settings,
+                                 sil_solve_diagnostics* diag, sil_stream stream)
+{
+    if (problems == nullptr || settings == nullptr || diag == nullptr || nproblems < 1)
+        return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: NULL argument or empty batch");
+    for (int p = 0; p < nproblems; ++p) {
+        sil_mag2d_problem const& q = problems[p];
+        if (q.nx < 3 || q.ny < 3) return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: each problem needs >= 3x3 nodes");
+        if (q.node_mu == nullptr || q.rhs == nullptr || q.solution == nullptr)
+            return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: NULL field pointer");
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (settings->solver == SIL_SOLVER_CG_F64) return solve_batch<double>(problems, nproblems, *settings, diag, s, false);
+    if (settings->solver == SIL_SOLVER_MIXED_IR) return solve_batch<float>(problems, nproblems, *settings, diag, s, true);
+    return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: unknown solver kind");
+}
+
+} // extern "C"

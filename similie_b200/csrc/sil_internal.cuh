@@ -1,0 +1,148 @@
+// sil_internal.cuh -- shared definitions of the sm_100a DEC library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/sil_b200.h"
+
+namespace sil {
+
+constexpr int kMaxDims = SIL_MAX_DIMS;
+constexpr int kMaxN = 4;       // form dimensions handled by d / d^T
+constexpr int kMaxNHodge = 3;  // form dimensions handled by the Hodge-star based operators
+constexpr int kMaxComp = 6;    // C(4,2)
+constexpr int kMaxFaces = 8;   // 2 (k+1) for k+1 <= 4
+
+// ---------------------------------------------------------------- errors
+
+void set_error(std::string const& msg);
+sil_status fail(sil_status status, std::string const& msg);
+sil_status cuda_fail(cudaError_t err, char const* what);
+
+#define SIL_CUDA_CHECK(call)                                 \
+    do {                                                     \
+        cudaError_t const err_ = (call);                     \
+        if (err_ != cudaSuccess) return ::sil::cuda_fail(err_, #call); \
+    } while (0)
+
+inline int64_t binom(int n, int k)
+{
+    if (k < 0 || k > n) return 0;
+    int64_t r = 1;
+    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+    return r;
+}
+
+inline int64_t ipow(int64_t b, int e)
+{
+    int64_t r = 1;
+    for (int i = 0; i < e; ++i) r *= b;
+    return r;
+}
+
+// ---------------------------------------------------------------- fields
+
+// Field as the kernels see it (plain aggregate passed by value).
+struct FieldView
+{
+    void* data;
+    int32_t ndims;
+    int32_t ncomp;
+    int64_t front[kMaxDims];
+    int64_t extent[kMaxDims];
+    int64_t stride[kMaxDims];
+    int64_t comp_stride;
+};
+
+FieldView to_view(sil_field const& f);
+int64_t node_count(sil_field const& f);
+sil_status check_field(sil_field const* f, char const* name, int expect_ncomp);
+int form_dims(uint32_t mask, int ndims, int* dims);
+
+// ---------------------------------------------------------------- chains
+
+// A face of the boundary of a basis simplex, as a sampling rule: the sample
+// is taken at node + offset, component `comp` of the lower tangent basis,
+// with sign -1 when `negative`.
+struct FaceRule
+{
+    int8_t offset[kMaxN];
+    int8_t comp;
+    int8_t negative;
+};
+
+// Sampling rules of d (clamped) or d^T (zero outside, shifted second half)
+// for a k-form over n form dims: rules[c][f] for output component c.
+struct CoboundaryRules
+{
+    int n;
+    int k;
+    int ncomp_in;
+    int ncomp_out;
+    int nfaces;
+    FaceRule rule[kMaxComp][kMaxFaces];
+};
+
+CoboundaryRules make_rules(int n, int k, bool transposed);
+
+// Diagonal Hodge star of an r-form over n dims: output component t (an
+// (n-r)-combination) reads input component src[t] (the complementary
+// r-combination) with sign sgn[t]; the factor is the product of the edge
+// lengths along `num_mask[t]` divided by those along `den_mask[t]`.
+struct StarRule
+{
+    int n;
+    int r;
+    int ncomp_out;
+    int8_t src[kMaxComp];
+    int8_t sgn[kMaxComp];
+    uint8_t num_mask[kMaxComp];
+    uint8_t den_mask[kMaxComp];
+};
+
+StarRule make_star(int n, int r);
+
+// Lexicographic combinations of {0..n-1} of size k as bit masks; index =
+// component id (matches SimiLie's antisymmetric-index memory order).
+std::vector<uint32_t> combinations(int n, int k);
+
+// ---------------------------------------------------------------- geometry
+
+struct Geometry
+{
+    int n = 0;
+    int64_t npoints[kMaxNHodge] = {0, 0, 0};
+    int64_t front[kMaxNHodge] = {0, 0, 0};
+    // Device arrays of length npoints + 2, index shifted by one: entry
+    // [p + 1] is the edge length along the axis at node p (forward
+    // difference, backward at the last node); the pads hold 1.
+    double* h[kMaxNHodge] = {nullptr, nullptr, nullptr};
+    double* inv_h[kMaxNHodge] = {nullptr, nullptr, nullptr};
+    float* h32[kMaxNHodge] = {nullptr, nullptr, nullptr};
+    float* inv_h32[kMaxNHodge] = {nullptr, nullptr, nullptr};
+    std::vector<double> host_h[kMaxNHodge];
+};
+
+// Geometry view passed to kernels.
+template <class T>
+struct GeoView
+{
+    T const* h[kMaxNHodge];
+    T const* inv_h[kMaxNHodge];
+    int64_t front[kMaxNHodge];
+    int64_t npoints[kMaxNHodge];
+};
+
+template <class T>
+GeoView<T> geo_view(Geometry const& g);
+
+} // namespace sil
+
+struct sil_geometry_s
+{
+    sil::Geometry g;
+};

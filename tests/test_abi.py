@@ -1,0 +1,81 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol the
+header declares, and rejects bad arguments on the host before any launch."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import similie_b200 as sil
+from similie_b200 import _native
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "sil_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sil_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_functions():
+    names = declared_functions()
+    assert "sil_deriv" in names and "sil_laplacian_run" in names and "sil_mag2d_solve_batch" in names
+
+
+def test_every_declared_symbol_is_exported():
+    L = ctypes.CDLL(_native.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    bound = {name for name, _, _ in _native.SIGNATURES}
+    assert set(declared_functions()) <= bound
+
+
+def test_status_strings():
+    L = sil.lib()
+    for code, name in _native.STATUS_NAMES.items():
+        assert L.sil_status_string(code).decode() == name
+
+
+def test_null_arguments_rejected_on_host():
+    L = sil.lib()
+    assert L.sil_deriv(None, 1, 0, None, None) == 1
+    assert b"NULL" in L.sil_last_error()
+    f = _native.SilField()
+    f.ndims = 0
+    assert L.sil_deriv(None, 1, 0, ctypes.byref(f), ctypes.byref(f)) == 1
+    assert L.sil_laplacian_run(None, None, None, None) == 1
+    assert L.sil_mag2d_solve_batch(None, 0, None, None, None) == 1
+    assert L.sil_geometry_create(None, 2, None, None, None) == 1
+
+
+def test_rank_and_component_checks_on_host():
+    L = sil.lib()
+    fi = _native.SilField()
+    fi.data = 16
+    fi.dtype = _native.SIL_F64
+    fi.ndims = 2
+    fi.ncomp = 3  # wrong: a 2D 1-form has 2 components
+    for d in range(2):
+        fi.extent[d] = 4
+        fi.stride[d] = 1
+    fo = _native.SilField.from_buffer_copy(fi)
+    fo.ncomp = 1
+    assert L.sil_deriv(None, 3, 1, ctypes.byref(fi), ctypes.byref(fo)) == 1
+    assert b"components" in L.sil_last_error()
+    fi.ncomp = 2
+    # d of a top-rank form is rejected
+    fo.ncomp = 1
+    fi2 = _native.SilField.from_buffer_copy(fi)
+    fi2.ncomp = 1
+    assert L.sil_deriv(None, 3, 2, ctypes.byref(fi2), ctypes.byref(fo)) == 1
+    # four form dims are fine for d, the Hodge-star operators stop at three
+    assert L.sil_laplacian(None, None, 3, 0, ctypes.byref(fi2), ctypes.byref(fi2)) == 1
+
+
+def test_field_struct_layout_matches_header():
+    # data, dtype, ndims, ncomp, reserved, front[6], extent[6], stride[6], comp_stride
+    assert ctypes.sizeof(_native.SilField) == 8 + 4 * 4 + 3 * 6 * 8 + 8
