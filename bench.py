@@ -186,6 +186,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--extras", action="store_true", help="also time the unfused chain, FP32 and the 512^2 0-form")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="warm-up + timed launches of the fused kernel only (profiling runs): no e2e, extras or CPU leg")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -253,6 +255,14 @@ def main():
     achieved = bytes_per_step / (avg_launch_ms * 1e-3) / 1e9
     traffic = ncu_traffic("lap2d_1form_tma_4096_fp64.md")
 
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": world * bytes_per_step * args.steps / (total_ms * 1e-3) / 1e9,
+                              "unit": "GB/s", "ms_per_step": ms_per_step, "kernel_only": True}))
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
     # End to end through the public API with host buffers: pinned H2D of the
     # input, the Laplacian, D2H of the result, every step.
     h_in = torch.from_numpy(w_host).pin_memory()
@@ -297,7 +307,7 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded k^-2 Gaussian random field per component)",
             "config": {"workload": WORKLOAD, "global_batch": world, "nodes_per_rank": [n, n],
                        "parallelism": f"independent fields x{world}", "l2": "inputs larger than L2 (268 MB in + 268 MB out per step)",
-                       "kernel": "lap2d_1form_tma_kernel<double>",
+                       "kernel": "lap2d_1form_tma_kernel<double>", "pipeline_variant": plan.variant,
                        "cell_updates_per_s": world * cell_updates(n) * args.steps / (total_ms * 1e-3)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",

@@ -141,6 +141,11 @@ size_t sil_laplacian_plan_scratch_bytes(sil_laplacian_plan plan);
 /* Kernel the plan runs: 0 table-driven fused (any rank / layout), 1 fused 2D
  * 0-form, 2 fused 2D 1-form with TMA-staged tiles, 3 unfused reference chain. */
 int sil_laplacian_plan_kernel(sil_laplacian_plan plan);
+/* Pipeline shape of kernel 2 chosen by the autotuner on the plan's first
+ * run (-1 before it).  The first run times each shape on the caller's fields
+ * and synchronises the stream once; SIMILIE_B200_AUTOTUNE=0 skips the tuning
+ * and uses shape 0. */
+int sil_laplacian_plan_variant(sil_laplacian_plan plan);
 /* Synchronising check of the plan's device error flag: SIL_ERR_BUDGET when a
  * bounded wait inside a kernel ran out (the kernel returned early). */
 sil_status sil_laplacian_plan_status(sil_laplacian_plan plan);

@@ -221,6 +221,10 @@ class StagedLaplacian:
         return lib().sil_laplacian_plan_kernel(self._p)
 
     @property
+    def variant(self):
+        return lib().sil_laplacian_plan_variant(self._p)
+
+    @property
     def scratch_bytes(self):
         return lib().sil_laplacian_plan_scratch_bytes(self._p)
 

@@ -1,5 +1,6 @@
 // capi.cu -- C ABI entry points of the DEC operators (see include/sil_b200.h).
 #include <algorithm>
+#include <cstdlib>
 #include <new>
 #include <string>
 
@@ -20,6 +21,7 @@ bool lap2d_layout_ok(sil_field const&, sil_field const&, int);
 bool lap2d_1form_tma_ok(sil_field const&, sil_field const&);
 sil_status launch_lap2d_0form(cudaStream_t, Geometry const&, sil_field const&, sil_field const&);
 sil_status launch_lap2d_1form_tma(cudaStream_t, Geometry const&, sil_field const&, sil_field const&, int*, int);
+sil_status autotune_lap2d_1form(cudaStream_t, Geometry const&, sil_field const&, sil_field const&, int*, int*, float*);
 
 namespace {
 
@@ -100,6 +102,8 @@ struct sil_laplacian_plan_s
     int k = 0;
     int mode = 0;
     int kernel = 0;  // 0 generic fused, 1 2D 0-form, 2 2D 1-form TMA, 3 unfused chain
+    int variant = -1;  // TMA pipeline shape picked by the autotuner (-1: not tuned yet)
+    float tuned_ms = 0.f;
     sil_field in_like {};
     sil_field out_like {};
     int* error_flag = nullptr;
@@ -299,9 +303,22 @@ sil_status sil_laplacian_run(sil_laplacian_plan plan, sil_stream stream, const s
     cudaStream_t const s = as_stream(stream);
     switch (plan->kernel) {
     case 1: return launch_lap2d_0form(s, *plan->geo, *in, *out);
-    case 2:
+    case 2: {
         if (!lap2d_1form_tma_ok(*in, *out)) return launch_fused_laplacian(s, *plan->geo, plan->mask, plan->k, *in, *out);
-        return launch_lap2d_1form_tma(s, *plan->geo, *in, *out, plan->error_flag, 0);
+        if (plan->variant < 0) {
+            // First run: time the pipeline shapes on these fields and keep the
+            // fastest (synchronises the stream once).
+            char const* env = std::getenv("SIMILIE_B200_AUTOTUNE");
+            if (env != nullptr && env[0] == '0') {
+                plan->variant = 0;
+            } else {
+                sil_status const st = autotune_lap2d_1form(s, *plan->geo, *in, *out, plan->error_flag, &plan->variant,
+                                                           &plan->tuned_ms);
+                if (st != SIL_OK) return st;
+            }
+        }
+        return launch_lap2d_1form_tma(s, *plan->geo, *in, *out, plan->error_flag, plan->variant);
+    }
     case 3: return run_unfused(*plan, s, *in, *out);
     default: return launch_fused_laplacian(s, *plan->geo, plan->mask, plan->k, *in, *out);
     }
@@ -324,6 +341,11 @@ size_t sil_laplacian_plan_scratch_bytes(sil_laplacian_plan plan)
 int sil_laplacian_plan_kernel(sil_laplacian_plan plan)
 {
     return plan == nullptr ? -1 : plan->kernel;
+}
+
+int sil_laplacian_plan_variant(sil_laplacian_plan plan)
+{
+    return plan == nullptr ? -1 : plan->variant;
 }
 
 sil_status sil_laplacian_plan_status(sil_laplacian_plan plan)

@@ -1,8 +1,14 @@
 // dec_generic.cu -- table-driven DEC kernels for any rank, 1-4 form
 // dimensions (3 for the Hodge-star based operators), any strides, spectator
-// dimensions, FP64 and FP32.  These serve every shape the specialised
-// kernels do not, and the unfused comparison chain.
+// dimensions, FP64 and FP32.  They serve every shape the specialised kernels
+// do not, and the unfused reference chain.
+//
+// Each kernel is instantiated for the field rank ND (lattice + spectator
+// dims, 1..6) so the index arithmetic unrolls; the sampling rules (faces of
+// the basis simplices, Hodge-star factors) come from tables built on the
+// host (host.cu).
 #include <algorithm>
+#include <type_traits>
 
 #include "sil_internal.cuh"
 
@@ -10,50 +16,67 @@ namespace sil {
 
 namespace {
 
-struct NodeCoords
-{
-    int64_t abs[kMaxDims];
-};
-
+template <int ND>
 __device__ __forceinline__ void unravel(FieldView const& f, int64_t flat, int64_t* local)
 {
+    if (flat < (int64_t(1) << 31)) {
+        uint32_t fl = static_cast<uint32_t>(flat);
 #pragma unroll
-    for (int d = kMaxDims - 1; d >= 0; --d) {
-        if (d < f.ndims) {
-            int64_t const e = f.extent[d];
-            local[d] = flat % e;
-            flat /= e;
+        for (int d = ND - 1; d > 0; --d) {
+            uint32_t const e = static_cast<uint32_t>(f.extent[d]);
+            local[d] = fl % e;
+            fl /= e;
         }
+        local[0] = fl;
+        return;
     }
+#pragma unroll
+    for (int d = ND - 1; d > 0; --d) {
+        int64_t const e = f.extent[d];
+        local[d] = flat % e;
+        flat /= e;
+    }
+    local[0] = flat;
 }
 
-template <class T>
+// Absolute coordinates of the output node `flat` and its element offset.
+template <int ND>
+__device__ __forceinline__ int64_t node_setup(FieldView const& out, int64_t flat, int64_t* abs)
+{
+    int64_t local[ND];
+    unravel<ND>(out, flat, local);
+    int64_t off = 0;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        abs[d] = out.front[d] + local[d];
+        off += local[d] * out.stride[d];
+    }
+    return off;
+}
+
+template <class T, int ND>
 __device__ __forceinline__ T load_at(FieldView const& f, int64_t const* abs, int comp)
 {
     int64_t off = comp * f.comp_stride;
 #pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        if (d < f.ndims) off += (abs[d] - f.front[d]) * f.stride[d];
-    }
+    for (int d = 0; d < ND; ++d) off += (abs[d] - f.front[d]) * f.stride[d];
     return static_cast<T const*>(f.data)[off];
 }
 
+template <int ND>
 __device__ __forceinline__ bool inside(FieldView const& f, int64_t const* abs)
 {
     bool in = true;
 #pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        if (d < f.ndims) in = in && abs[d] >= f.front[d] && abs[d] < f.front[d] + f.extent[d];
-    }
+    for (int d = 0; d < ND; ++d) in = in && abs[d] >= f.front[d] && abs[d] < f.front[d] + f.extent[d];
     return in;
 }
 
+template <int ND>
 __device__ __forceinline__ void clamp_to(FieldView const& f, int64_t* abs)
 {
 #pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        if (d < f.ndims) abs[d] = min(max(abs[d], f.front[d]), f.front[d] + f.extent[d] - 1);
-    }
+    for (int d = 0; d < ND; ++d) abs[d] = min(max(abs[d], f.front[d]), f.front[d] + f.extent[d] - 1);
 }
 
 struct DimMap
@@ -62,37 +85,38 @@ struct DimMap
     int dims[kMaxN];
 };
 
+template <int ND>
+__device__ __forceinline__ void offset_node(DimMap const& dm, int64_t const* abs, FaceRule const& r, int64_t* s)
+{
+#pragma unroll
+    for (int d = 0; d < ND; ++d) s[d] = abs[d];
+#pragma unroll
+    for (int a = 0; a < kMaxN; ++a) {
+        if (a < dm.n) s[dm.dims[a]] += r.offset[a];
+    }
+}
+
 // ------------------------------------------------------------------ d, d^T
 
-template <class T, bool TRANSPOSED>
+template <class T, bool TRANSPOSED, int ND>
 __global__ void coboundary_kernel(FieldView in, FieldView out, CoboundaryRules rules, DimMap dm, int64_t total)
 {
     int64_t const flat = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (flat >= total) return;
-    int64_t local[kMaxDims];
-    unravel(out, flat, local);
-    int64_t abs[kMaxDims];
-    int64_t out_off = 0;
-#pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        abs[d] = d < out.ndims ? out.front[d] + local[d] : 0;
-        if (d < out.ndims) out_off += local[d] * out.stride[d];
-    }
-    T* o = static_cast<T*>(out.data) + out_off;
+    int64_t abs[ND];
+    T* o = static_cast<T*>(out.data) + node_setup<ND>(out, flat, abs);
     for (int c = 0; c < rules.ncomp_out; ++c) {
         T acc = T(0);
         for (int f = 0; f < rules.nfaces; ++f) {
             FaceRule const r = rules.rule[c][f];
-            int64_t s[kMaxDims];
-#pragma unroll
-            for (int d = 0; d < kMaxDims; ++d) s[d] = abs[d];
-            for (int a = 0; a < dm.n; ++a) s[dm.dims[a]] += r.offset[a];
+            int64_t s[ND];
+            offset_node<ND>(dm, abs, r, s);
             T v;
             if (!TRANSPOSED) {
-                clamp_to(in, s);
-                v = load_at<T>(in, s, r.comp);
+                clamp_to<ND>(in, s);
+                v = load_at<T, ND>(in, s, r.comp);
             } else {
-                v = inside(in, s) ? load_at<T>(in, s, r.comp) : T(0);
+                v = inside<ND>(in, s) ? load_at<T, ND>(in, s, r.comp) : T(0);
             }
             // Chain-order signed sum from zero: acc + (-1)*v is acc - v exactly.
             acc = r.negative ? acc - v : acc + v;
@@ -110,54 +134,43 @@ struct GeoCtx
     DimMap dm;
 };
 
-// Product of edge lengths over `num` divided by those over `den` at a node.
+// sign * product of edge lengths over `num` * product of inverse lengths over `den`.
 template <class T>
 __device__ __forceinline__ T star_factor(GeoCtx<T> const& g, int64_t const* abs, uint32_t num, uint32_t den, int sgn)
 {
     T f = static_cast<T>(sgn);
-    for (int a = 0; a < g.dm.n; ++a) {
-        int64_t const p = abs[g.dm.dims[a]] - g.geo.front[a] + 1;
-        if (num & (1u << a)) f *= g.geo.h[a][p];
-        if (den & (1u << a)) f *= g.geo.inv_h[a][p];
+#pragma unroll
+    for (int a = 0; a < kMaxNHodge; ++a) {
+        if (a < g.dm.n) {
+            int64_t const p = abs[g.dm.dims[a]] - g.geo.front[a] + 1;
+            if (num & (1u << a)) f *= g.geo.h[a][p];
+            if (den & (1u << a)) f *= g.geo.inv_h[a][p];
+        }
     }
     return f;
 }
 
-template <class T>
+template <class T, int ND>
 __global__ void hodge_kernel(FieldView in, FieldView out, StarRule star, GeoCtx<T> g, int64_t total)
 {
     int64_t const flat = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (flat >= total) return;
-    int64_t local[kMaxDims], abs[kMaxDims];
-    unravel(out, flat, local);
-    int64_t out_off = 0;
-#pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        abs[d] = d < out.ndims ? out.front[d] + local[d] : 0;
-        if (d < out.ndims) out_off += local[d] * out.stride[d];
-    }
-    T* o = static_cast<T*>(out.data) + out_off;
+    int64_t abs[ND];
+    T* o = static_cast<T*>(out.data) + node_setup<ND>(out, flat, abs);
     for (int t = 0; t < star.ncomp_out; ++t) {
-        T const v = load_at<T>(in, abs, star.src[t]);
+        T const v = load_at<T, ND>(in, abs, star.src[t]);
         o[t * out.comp_stride] = star_factor(g, abs, star.num_mask[t], star.den_mask[t], star.sgn[t]) * v;
     }
 }
 
 // Stored per-node Hodge tensor (Full<k> x Antisym<n-k>) of the diagonal metric.
-template <class T>
+template <class T, int ND>
 __global__ void fill_hodge_kernel(FieldView out, StarRule star, GeoCtx<T> g, int k, int n, int64_t total)
 {
     int64_t const flat = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (flat >= total) return;
-    int64_t local[kMaxDims], abs[kMaxDims];
-    unravel(out, flat, local);
-    int64_t out_off = 0;
-#pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        abs[d] = d < out.ndims ? out.front[d] + local[d] : 0;
-        if (d < out.ndims) out_off += local[d] * out.stride[d];
-    }
-    T* o = static_cast<T*>(out.data) + out_off;
+    int64_t abs[ND];
+    T* o = static_cast<T*>(out.data) + node_setup<ND>(out, flat, abs);
     int ntuples = 1;
     for (int i = 0; i < k; ++i) ntuples *= n;
     double inv_fact = 1.0;
@@ -213,34 +226,26 @@ struct FusedParams
     CoboundaryRules d_km1;      // d on the (k-1)-form codifferential (clamped)
 };
 
-template <class T>
-__device__ __forceinline__ void offset_node(DimMap const& dm, int64_t const* abs, FaceRule const& r, int64_t* s)
-{
-#pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) s[d] = abs[d];
-    for (int a = 0; a < dm.n; ++a) s[dm.dims[a]] += r.offset[a];
-}
-
 // (star_k w)(q) component c, zero outside the input domain.
-template <class T>
+template <class T, int ND>
 __device__ T dual_of_input(FusedParams<T> const& P, int64_t const* q, int c)
 {
-    if (!inside(P.in, q)) return T(0);
+    if (!inside<ND>(P.in, q)) return T(0);
     return star_factor(P.g, q, P.star_k.num_mask[c], P.star_k.den_mask[c], P.star_k.sgn[c])
-           * load_at<T>(P.in, q, P.star_k.src[c]);
+           * load_at<T, ND>(P.in, q, P.star_k.src[c]);
 }
 
-// codifferential of the input at node p (inside the input domain), component t.
-template <class T>
+// Codifferential of the input at node p (inside the input domain), component t.
+template <class T, int ND>
 __device__ T codiff_at(FusedParams<T> const& P, int64_t const* p, int t)
 {
     int const c = P.star_codiff.src[t];
     T acc = T(0);
     for (int f = 0; f < P.dt_codiff.nfaces; ++f) {
         FaceRule const r = P.dt_codiff.rule[c][f];
-        int64_t s[kMaxDims];
-        offset_node<T>(P.g.dm, p, r, s);
-        T const v = dual_of_input(P, s, r.comp);
+        int64_t s[ND];
+        offset_node<ND>(P.g.dm, p, r, s);
+        T const v = dual_of_input<T, ND>(P, s, r.comp);
         acc = r.negative ? acc - v : acc + v;
     }
     T const dual_codiff = -acc;
@@ -250,37 +255,30 @@ __device__ T codiff_at(FusedParams<T> const& P, int64_t const* p, int t)
 }
 
 // (star d w)(p) component c1, zero outside the input domain; d samples are clamped.
-template <class T>
+template <class T, int ND>
 __device__ T dual_of_derivative(FusedParams<T> const& P, int64_t const* p, int c1)
 {
-    if (!inside(P.in, p)) return T(0);
+    if (!inside<ND>(P.in, p)) return T(0);
     int const c0 = P.star_dk.src[c1];
     T acc = T(0);
     for (int f = 0; f < P.d_k.nfaces; ++f) {
         FaceRule const r = P.d_k.rule[c0][f];
-        int64_t s[kMaxDims];
-        offset_node<T>(P.g.dm, p, r, s);
-        clamp_to(P.in, s);
-        T const v = load_at<T>(P.in, s, r.comp);
+        int64_t s[ND];
+        offset_node<ND>(P.g.dm, p, r, s);
+        clamp_to<ND>(P.in, s);
+        T const v = load_at<T, ND>(P.in, s, r.comp);
         acc = r.negative ? acc - v : acc + v;
     }
     return star_factor(P.g, p, P.star_dk.num_mask[c1], P.star_dk.den_mask[c1], P.star_dk.sgn[c1]) * acc;
 }
 
-template <class T, bool DELTA_D, bool D_DELTA>
+template <class T, bool DELTA_D, bool D_DELTA, int ND>
 __global__ void fused_laplacian_kernel(FusedParams<T> P, int64_t total)
 {
     int64_t const flat = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (flat >= total) return;
-    int64_t local[kMaxDims], abs[kMaxDims];
-    unravel(P.out, flat, local);
-    int64_t out_off = 0;
-#pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        abs[d] = d < P.out.ndims ? P.out.front[d] + local[d] : 0;
-        if (d < P.out.ndims) out_off += local[d] * P.out.stride[d];
-    }
-    T* o = static_cast<T*>(P.out.data) + out_off;
+    int64_t abs[ND];
+    T* o = static_cast<T*>(P.out.data) + node_setup<ND>(P.out, flat, abs);
     for (int t = 0; t < P.out.ncomp; ++t) {
         T result = T(0);
         if constexpr (DELTA_D) {
@@ -288,9 +286,9 @@ __global__ void fused_laplacian_kernel(FusedParams<T> P, int64_t total)
             T acc = T(0);
             for (int f = 0; f < P.dt_dual.nfaces; ++f) {
                 FaceRule const r = P.dt_dual.rule[c2][f];
-                int64_t s[kMaxDims];
-                offset_node<T>(P.g.dm, abs, r, s);
-                T const v = dual_of_derivative(P, s, r.comp);
+                int64_t s[ND];
+                offset_node<ND>(P.g.dm, abs, r, s);
+                T const v = dual_of_derivative<T, ND>(P, s, r.comp);
                 acc = r.negative ? acc - v : acc + v;
             }
             T const dual_codiff = -acc;
@@ -302,10 +300,10 @@ __global__ void fused_laplacian_kernel(FusedParams<T> P, int64_t total)
             T acc = T(0);
             for (int f = 0; f < P.d_km1.nfaces; ++f) {
                 FaceRule const r = P.d_km1.rule[t][f];
-                int64_t s[kMaxDims];
-                offset_node<T>(P.g.dm, abs, r, s);
-                clamp_to(P.in, s);
-                T const v = codiff_at(P, s, r.comp);
+                int64_t s[ND];
+                offset_node<ND>(P.g.dm, abs, r, s);
+                clamp_to<ND>(P.in, s);
+                T const v = codiff_at<T, ND>(P, s, r.comp);
                 acc = r.negative ? acc - v : acc + v;
             }
             result = DELTA_D ? result + acc : acc;
@@ -314,49 +312,35 @@ __global__ void fused_laplacian_kernel(FusedParams<T> P, int64_t total)
     }
 }
 
-template <class T>
+template <class T, int ND>
 __global__ void fused_codifferential_kernel(FusedParams<T> P, int64_t total)
 {
     int64_t const flat = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (flat >= total) return;
-    int64_t local[kMaxDims], abs[kMaxDims];
-    unravel(P.out, flat, local);
-    int64_t out_off = 0;
-#pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        abs[d] = d < P.out.ndims ? P.out.front[d] + local[d] : 0;
-        if (d < P.out.ndims) out_off += local[d] * P.out.stride[d];
-    }
-    T* o = static_cast<T*>(P.out.data) + out_off;
-    for (int t = 0; t < P.out.ncomp; ++t) o[t * P.out.comp_stride] = codiff_at(P, abs, t);
+    int64_t abs[ND];
+    T* o = static_cast<T*>(P.out.data) + node_setup<ND>(P.out, flat, abs);
+    for (int t = 0; t < P.out.ncomp; ++t) o[t * P.out.comp_stride] = codiff_at<T, ND>(P, abs, t);
 }
 
 // Reference kernel 1 of codifferential_of_coboundary: clamped d of an
 // r-form followed by the Hodge star of the (r+1)-form, at every node of `out`.
-template <class T>
+template <class T, int ND>
 __global__ void deriv_star_kernel(FieldView in, FieldView out, CoboundaryRules rules, StarRule star, GeoCtx<T> g,
                                   int64_t total)
 {
     int64_t const flat = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (flat >= total) return;
-    int64_t local[kMaxDims], abs[kMaxDims];
-    unravel(out, flat, local);
-    int64_t out_off = 0;
-#pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        abs[d] = d < out.ndims ? out.front[d] + local[d] : 0;
-        if (d < out.ndims) out_off += local[d] * out.stride[d];
-    }
-    T* o = static_cast<T*>(out.data) + out_off;
+    int64_t abs[ND];
+    T* o = static_cast<T*>(out.data) + node_setup<ND>(out, flat, abs);
     for (int t = 0; t < star.ncomp_out; ++t) {
         int const c0 = star.src[t];
         T acc = T(0);
         for (int f = 0; f < rules.nfaces; ++f) {
             FaceRule const r = rules.rule[c0][f];
-            int64_t s[kMaxDims];
-            offset_node<T>(g.dm, abs, r, s);
-            clamp_to(in, s);
-            T const v = load_at<T>(in, s, r.comp);
+            int64_t s[ND];
+            offset_node<ND>(g.dm, abs, r, s);
+            clamp_to<ND>(in, s);
+            T const v = load_at<T, ND>(in, s, r.comp);
             acc = r.negative ? acc - v : acc + v;
         }
         o[t * out.comp_stride] = star_factor(g, abs, star.num_mask[t], star.den_mask[t], star.sgn[t]) * acc;
@@ -365,29 +349,22 @@ __global__ void deriv_star_kernel(FieldView in, FieldView out, CoboundaryRules r
 
 // Reference kernel 2: d^T (zero outside `src`) of an r-form, Hodge star of
 // the (r+1)-form, times the codifferential sign.
-template <class T>
+template <class T, int ND>
 __global__ void transpose_star_kernel(FieldView src, FieldView out, CoboundaryRules rules, StarRule star, GeoCtx<T> g,
                                       T sign, int64_t total)
 {
     int64_t const flat = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (flat >= total) return;
-    int64_t local[kMaxDims], abs[kMaxDims];
-    unravel(out, flat, local);
-    int64_t out_off = 0;
-#pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        abs[d] = d < out.ndims ? out.front[d] + local[d] : 0;
-        if (d < out.ndims) out_off += local[d] * out.stride[d];
-    }
-    T* o = static_cast<T*>(out.data) + out_off;
+    int64_t abs[ND];
+    T* o = static_cast<T*>(out.data) + node_setup<ND>(out, flat, abs);
     for (int t = 0; t < star.ncomp_out; ++t) {
         int const c = star.src[t];
         T acc = T(0);
         for (int f = 0; f < rules.nfaces; ++f) {
             FaceRule const r = rules.rule[c][f];
-            int64_t s[kMaxDims];
-            offset_node<T>(g.dm, abs, r, s);
-            T const v = inside(src, s) ? load_at<T>(src, s, r.comp) : T(0);
+            int64_t s[ND];
+            offset_node<ND>(g.dm, abs, r, s);
+            T const v = inside<ND>(src, s) ? load_at<T, ND>(src, s, r.comp) : T(0);
             acc = r.negative ? acc - v : acc + v;
         }
         T const dual_codiff = -acc;
@@ -396,20 +373,18 @@ __global__ void transpose_star_kernel(FieldView src, FieldView out, CoboundaryRu
 }
 
 // out += add (same shape, any strides).
-template <class T>
+template <class T, int ND>
 __global__ void add_kernel(FieldView out, FieldView add, int64_t total)
 {
     int64_t const flat = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (flat >= total) return;
-    int64_t local[kMaxDims];
-    unravel(out, flat, local);
+    int64_t local[ND];
+    unravel<ND>(out, flat, local);
     int64_t oo = 0, ao = 0;
 #pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        if (d < out.ndims) {
-            oo += local[d] * out.stride[d];
-            ao += local[d] * add.stride[d];
-        }
+    for (int d = 0; d < ND; ++d) {
+        oo += local[d] * out.stride[d];
+        ao += local[d] * add.stride[d];
     }
     for (int c = 0; c < out.ncomp; ++c)
         static_cast<T*>(out.data)[oo + c * out.comp_stride] += static_cast<T const*>(add.data)[ao + c * add.comp_stride];
@@ -417,41 +392,27 @@ __global__ void add_kernel(FieldView out, FieldView add, int64_t total)
 
 constexpr int kBlock = 256;
 
-int64_t grid_for(int64_t total)
+unsigned grid_for(int64_t total)
 {
-    return (total + kBlock - 1) / kBlock;
+    return static_cast<unsigned>((total + kBlock - 1) / kBlock);
 }
 
-} // namespace
-
-// ------------------------------------------------------------------ launchers
-
-sil_status launch_coboundary(cudaStream_t stream, uint32_t mask, int k, sil_field const& in, sil_field const& out,
-                             bool transposed)
+// Call f(std::integral_constant<int, ND>{}) for the runtime rank nd (1..6).
+template <class F>
+void with_nd(int nd, F&& f)
 {
-    DimMap dm {};
-    dm.n = form_dims(mask, in.ndims, dm.dims);
-    CoboundaryRules const rules = make_rules(dm.n, k, transposed);
-    int64_t const total = node_count(out);
-    if (total == 0) return SIL_OK;
-    dim3 const grid(static_cast<unsigned>(grid_for(total)));
-    if (in.dtype == SIL_F64) {
-        if (transposed)
-            coboundary_kernel<double, true><<<grid, kBlock, 0, stream>>>(to_view(in), to_view(out), rules, dm, total);
-        else
-            coboundary_kernel<double, false><<<grid, kBlock, 0, stream>>>(to_view(in), to_view(out), rules, dm, total);
-    } else {
-        if (transposed)
-            coboundary_kernel<float, true><<<grid, kBlock, 0, stream>>>(to_view(in), to_view(out), rules, dm, total);
-        else
-            coboundary_kernel<float, false><<<grid, kBlock, 0, stream>>>(to_view(in), to_view(out), rules, dm, total);
+    switch (nd) {
+    case 1: f(std::integral_constant<int, 1>{}); break;
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 3: f(std::integral_constant<int, 3>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 5: f(std::integral_constant<int, 5>{}); break;
+    default: f(std::integral_constant<int, 6>{}); break;
     }
-    SIL_CUDA_CHECK(cudaGetLastError());
-    return SIL_OK;
 }
 
 template <class T>
-static GeoCtx<T> make_geo_ctx(Geometry const& geo, uint32_t mask, int ndims)
+GeoCtx<T> make_geo_ctx(Geometry const& geo, uint32_t mask, int ndims)
 {
     GeoCtx<T> g {};
     g.geo = geo_view<T>(geo);
@@ -459,45 +420,8 @@ static GeoCtx<T> make_geo_ctx(Geometry const& geo, uint32_t mask, int ndims)
     return g;
 }
 
-sil_status launch_hodge(cudaStream_t stream, Geometry const& geo, uint32_t mask, int k, sil_field const& in,
-                        sil_field const& out)
-{
-    int dims[kMaxDims];
-    int const n = form_dims(mask, in.ndims, dims);
-    StarRule const star = make_star(n, k);
-    int64_t const total = node_count(out);
-    if (total == 0) return SIL_OK;
-    dim3 const grid(static_cast<unsigned>(grid_for(total)));
-    if (in.dtype == SIL_F64)
-        hodge_kernel<double><<<grid, kBlock, 0, stream>>>(to_view(in), to_view(out), star,
-                                                          make_geo_ctx<double>(geo, mask, in.ndims), total);
-    else
-        hodge_kernel<float><<<grid, kBlock, 0, stream>>>(to_view(in), to_view(out), star,
-                                                         make_geo_ctx<float>(geo, mask, in.ndims), total);
-    SIL_CUDA_CHECK(cudaGetLastError());
-    return SIL_OK;
-}
-
-sil_status launch_fill_hodge(cudaStream_t stream, Geometry const& geo, int k, sil_field const& out)
-{
-    int const n = geo.n;
-    StarRule const star = make_star(n, k);
-    int64_t const total = node_count(out);
-    if (total == 0) return SIL_OK;
-    uint32_t const mask = (1u << n) - 1;
-    dim3 const grid(static_cast<unsigned>(grid_for(total)));
-    if (out.dtype == SIL_F64)
-        fill_hodge_kernel<double><<<grid, kBlock, 0, stream>>>(to_view(out), star, make_geo_ctx<double>(geo, mask, n),
-                                                               k, n, total);
-    else
-        fill_hodge_kernel<float><<<grid, kBlock, 0, stream>>>(to_view(out), star, make_geo_ctx<float>(geo, mask, n),
-                                                              k, n, total);
-    SIL_CUDA_CHECK(cudaGetLastError());
-    return SIL_OK;
-}
-
 template <class T>
-static FusedParams<T> make_fused(Geometry const& geo, uint32_t mask, int k, sil_field const& in, sil_field const& out)
+FusedParams<T> make_fused(Geometry const& geo, uint32_t mask, int k, sil_field const& in, sil_field const& out)
 {
     FusedParams<T> P {};
     P.in = to_view(in);
@@ -523,26 +447,99 @@ static FusedParams<T> make_fused(Geometry const& geo, uint32_t mask, int k, sil_
     return P;
 }
 
-sil_status launch_fused_laplacian(cudaStream_t stream, Geometry const& geo, uint32_t mask, int k, sil_field const& in,
-                                  sil_field const& out)
+template <class T>
+void launch_coboundary_t(cudaStream_t stream, CoboundaryRules const& rules, DimMap const& dm, sil_field const& in,
+                         sil_field const& out, bool transposed, int64_t total)
+{
+    with_nd(out.ndims, [&](auto ndc) {
+        constexpr int ND = decltype(ndc)::value;
+        if (transposed)
+            coboundary_kernel<T, true, ND><<<grid_for(total), kBlock, 0, stream>>>(to_view(in), to_view(out), rules, dm, total);
+        else
+            coboundary_kernel<T, false, ND><<<grid_for(total), kBlock, 0, stream>>>(to_view(in), to_view(out), rules, dm, total);
+    });
+}
+
+template <class T>
+void launch_fused_t(cudaStream_t stream, Geometry const& geo, uint32_t mask, int k, sil_field const& in,
+                    sil_field const& out, int64_t total)
+{
+    auto P = make_fused<T>(geo, mask, k, in, out);
+    bool const dd = k < P.n, dl = k > 0;
+    with_nd(out.ndims, [&](auto ndc) {
+        constexpr int ND = decltype(ndc)::value;
+        if (dd && dl) fused_laplacian_kernel<T, true, true, ND><<<grid_for(total), kBlock, 0, stream>>>(P, total);
+        else if (dd) fused_laplacian_kernel<T, true, false, ND><<<grid_for(total), kBlock, 0, stream>>>(P, total);
+        else fused_laplacian_kernel<T, false, true, ND><<<grid_for(total), kBlock, 0, stream>>>(P, total);
+    });
+}
+
+} // namespace
+
+// ------------------------------------------------------------------ launchers
+
+sil_status launch_coboundary(cudaStream_t stream, uint32_t mask, int k, sil_field const& in, sil_field const& out,
+                             bool transposed)
+{
+    DimMap dm {};
+    dm.n = form_dims(mask, in.ndims, dm.dims);
+    CoboundaryRules const rules = make_rules(dm.n, k, transposed);
+    int64_t const total = node_count(out);
+    if (total == 0) return SIL_OK;
+    if (in.dtype == SIL_F64) launch_coboundary_t<double>(stream, rules, dm, in, out, transposed, total);
+    else launch_coboundary_t<float>(stream, rules, dm, in, out, transposed, total);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+sil_status launch_hodge(cudaStream_t stream, Geometry const& geo, uint32_t mask, int k, sil_field const& in,
+                        sil_field const& out)
 {
     int dims[kMaxDims];
     int const n = form_dims(mask, in.ndims, dims);
+    StarRule const star = make_star(n, k);
     int64_t const total = node_count(out);
     if (total == 0) return SIL_OK;
-    dim3 const grid(static_cast<unsigned>(grid_for(total)));
-    bool const dd = k < n, dl = k > 0;
-    if (in.dtype == SIL_F64) {
-        auto P = make_fused<double>(geo, mask, k, in, out);
-        if (dd && dl) fused_laplacian_kernel<double, true, true><<<grid, kBlock, 0, stream>>>(P, total);
-        else if (dd) fused_laplacian_kernel<double, true, false><<<grid, kBlock, 0, stream>>>(P, total);
-        else fused_laplacian_kernel<double, false, true><<<grid, kBlock, 0, stream>>>(P, total);
-    } else {
-        auto P = make_fused<float>(geo, mask, k, in, out);
-        if (dd && dl) fused_laplacian_kernel<float, true, true><<<grid, kBlock, 0, stream>>>(P, total);
-        else if (dd) fused_laplacian_kernel<float, true, false><<<grid, kBlock, 0, stream>>>(P, total);
-        else fused_laplacian_kernel<float, false, true><<<grid, kBlock, 0, stream>>>(P, total);
-    }
+    with_nd(out.ndims, [&](auto ndc) {
+        constexpr int ND = decltype(ndc)::value;
+        if (in.dtype == SIL_F64)
+            hodge_kernel<double, ND><<<grid_for(total), kBlock, 0, stream>>>(to_view(in), to_view(out), star,
+                                                                             make_geo_ctx<double>(geo, mask, in.ndims), total);
+        else
+            hodge_kernel<float, ND><<<grid_for(total), kBlock, 0, stream>>>(to_view(in), to_view(out), star,
+                                                                            make_geo_ctx<float>(geo, mask, in.ndims), total);
+    });
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+sil_status launch_fill_hodge(cudaStream_t stream, Geometry const& geo, int k, sil_field const& out)
+{
+    int const n = geo.n;
+    StarRule const star = make_star(n, k);
+    int64_t const total = node_count(out);
+    if (total == 0) return SIL_OK;
+    uint32_t const mask = (1u << n) - 1;
+    with_nd(out.ndims, [&](auto ndc) {
+        constexpr int ND = decltype(ndc)::value;
+        if (out.dtype == SIL_F64)
+            fill_hodge_kernel<double, ND><<<grid_for(total), kBlock, 0, stream>>>(
+                    to_view(out), star, make_geo_ctx<double>(geo, mask, n), k, n, total);
+        else
+            fill_hodge_kernel<float, ND><<<grid_for(total), kBlock, 0, stream>>>(
+                    to_view(out), star, make_geo_ctx<float>(geo, mask, n), k, n, total);
+    });
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+sil_status launch_fused_laplacian(cudaStream_t stream, Geometry const& geo, uint32_t mask, int k, sil_field const& in,
+                                  sil_field const& out)
+{
+    int64_t const total = node_count(out);
+    if (total == 0) return SIL_OK;
+    if (in.dtype == SIL_F64) launch_fused_t<double>(stream, geo, mask, k, in, out, total);
+    else launch_fused_t<float>(stream, geo, mask, k, in, out, total);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
@@ -552,11 +549,15 @@ sil_status launch_codifferential(cudaStream_t stream, Geometry const& geo, uint3
 {
     int64_t const total = node_count(out);
     if (total == 0) return SIL_OK;
-    dim3 const grid(static_cast<unsigned>(grid_for(total)));
-    if (in.dtype == SIL_F64)
-        fused_codifferential_kernel<double><<<grid, kBlock, 0, stream>>>(make_fused<double>(geo, mask, k, in, out), total);
-    else
-        fused_codifferential_kernel<float><<<grid, kBlock, 0, stream>>>(make_fused<float>(geo, mask, k, in, out), total);
+    with_nd(out.ndims, [&](auto ndc) {
+        constexpr int ND = decltype(ndc)::value;
+        if (in.dtype == SIL_F64)
+            fused_codifferential_kernel<double, ND><<<grid_for(total), kBlock, 0, stream>>>(
+                    make_fused<double>(geo, mask, k, in, out), total);
+        else
+            fused_codifferential_kernel<float, ND><<<grid_for(total), kBlock, 0, stream>>>(
+                    make_fused<float>(geo, mask, k, in, out), total);
+    });
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
@@ -570,13 +571,15 @@ sil_status launch_deriv_star(cudaStream_t stream, Geometry const& geo, uint32_t 
     StarRule const star = make_star(n, r + 1);
     int64_t const total = node_count(out);
     if (total == 0) return SIL_OK;
-    dim3 const grid(static_cast<unsigned>(grid_for(total)));
-    if (in.dtype == SIL_F64)
-        deriv_star_kernel<double><<<grid, kBlock, 0, stream>>>(to_view(in), to_view(out), rules, star,
-                                                               make_geo_ctx<double>(geo, mask, in.ndims), total);
-    else
-        deriv_star_kernel<float><<<grid, kBlock, 0, stream>>>(to_view(in), to_view(out), rules, star,
-                                                              make_geo_ctx<float>(geo, mask, in.ndims), total);
+    with_nd(out.ndims, [&](auto ndc) {
+        constexpr int ND = decltype(ndc)::value;
+        if (in.dtype == SIL_F64)
+            deriv_star_kernel<double, ND><<<grid_for(total), kBlock, 0, stream>>>(
+                    to_view(in), to_view(out), rules, star, make_geo_ctx<double>(geo, mask, in.ndims), total);
+        else
+            deriv_star_kernel<float, ND><<<grid_for(total), kBlock, 0, stream>>>(
+                    to_view(in), to_view(out), rules, star, make_geo_ctx<float>(geo, mask, in.ndims), total);
+    });
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
@@ -590,15 +593,16 @@ sil_status launch_transpose_star(cudaStream_t stream, Geometry const& geo, uint3
     StarRule const star = make_star(n, r + 1);
     int64_t const total = node_count(out);
     if (total == 0) return SIL_OK;
-    dim3 const grid(static_cast<unsigned>(grid_for(total)));
-    if (src.dtype == SIL_F64)
-        transpose_star_kernel<double><<<grid, kBlock, 0, stream>>>(to_view(src), to_view(out), rules, star,
-                                                                   make_geo_ctx<double>(geo, mask, src.ndims), sign,
-                                                                   total);
-    else
-        transpose_star_kernel<float><<<grid, kBlock, 0, stream>>>(to_view(src), to_view(out), rules, star,
-                                                                  make_geo_ctx<float>(geo, mask, src.ndims),
-                                                                  static_cast<float>(sign), total);
+    with_nd(out.ndims, [&](auto ndc) {
+        constexpr int ND = decltype(ndc)::value;
+        if (src.dtype == SIL_F64)
+            transpose_star_kernel<double, ND><<<grid_for(total), kBlock, 0, stream>>>(
+                    to_view(src), to_view(out), rules, star, make_geo_ctx<double>(geo, mask, src.ndims), sign, total);
+        else
+            transpose_star_kernel<float, ND><<<grid_for(total), kBlock, 0, stream>>>(
+                    to_view(src), to_view(out), rules, star, make_geo_ctx<float>(geo, mask, src.ndims),
+                    static_cast<float>(sign), total);
+    });
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
@@ -607,11 +611,13 @@ sil_status launch_add(cudaStream_t stream, sil_field const& out, sil_field const
 {
     int64_t const total = node_count(out);
     if (total == 0) return SIL_OK;
-    dim3 const grid(static_cast<unsigned>(grid_for(total)));
-    if (out.dtype == SIL_F64)
-        add_kernel<double><<<grid, kBlock, 0, stream>>>(to_view(out), to_view(add), total);
-    else
-        add_kernel<float><<<grid, kBlock, 0, stream>>>(to_view(out), to_view(add), total);
+    with_nd(out.ndims, [&](auto ndc) {
+        constexpr int ND = decltype(ndc)::value;
+        if (out.dtype == SIL_F64)
+            add_kernel<double, ND><<<grid_for(total), kBlock, 0, stream>>>(to_view(out), to_view(add), total);
+        else
+            add_kernel<float, ND><<<grid_for(total), kBlock, 0, stream>>>(to_view(out), to_view(add), total);
+    });
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }

@@ -258,8 +258,10 @@ sil_status sil_geometry_create(sil_geometry* geometry, int n, const double* cons
         }
         g.npoints[a] = np;
         g.front[a] = front ? front[a] : 0;
-        std::vector<double> h(np + 2, 1.0), ih(np + 2, 1.0);
-        std::vector<float> h32(np + 2, 1.0f), ih32(np + 2, 1.0f);
+        // Pads: edge length 1 and inverse 0 outside the axis, so a Hodge
+        // factor evaluated one node outside the lattice vanishes.
+        std::vector<double> h(np + 2, 1.0), ih(np + 2, 0.0);
+        std::vector<float> h32(np + 2, 1.0f), ih32(np + 2, 0.0f);
         for (int64_t p = 0; p < np; ++p) {
             double const e = p + 1 < np ? coords[a][p + 1] - coords[a][p] : coords[a][p] - coords[a][p - 1];
             h[p + 1] = e;

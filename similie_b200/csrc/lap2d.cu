@@ -80,36 +80,53 @@ __global__ void __launch_bounds__(256) lap2d_0form_kernel(Lap0Params<T> P)
 
 // ------------------------------------------------------------------ 1-form, TMA
 
-constexpr int kTJ = 128;     // output columns per strip (= threads per CTA)
-constexpr int kRows = 8;     // rows per pipeline stage
-constexpr int kStages = 4;   // pipeline depth
+constexpr int kTJ = 256;                 // output columns per strip = consumer threads
+constexpr int kHalf = kTJ / 2;           // nodes per TMA box row (one half strip)
+constexpr int kConsumerWarps = kTJ / 32;
+constexpr int kThreads1 = kTJ + 32;      // consumers + one TMA producer warp
 
 template <class T>
 struct Lap1Traits;
 template <>
 struct Lap1Traits<double>
 {
-    static constexpr int kHalo = 1;  // left halo columns in the staged tile
     using Vec = double2;
 };
 template <>
 struct Lap1Traits<float>
 {
-    static constexpr int kHalo = 2;  // keeps the TMA start 16-byte aligned
     using Vec = float2;
 };
 
-template <class T>
-__host__ __device__ constexpr int tile_cols()
+// Pipeline shape: ROWS rows per stage, STAGES stages in the ring, MINB CTAs
+// per SM the register budget is sized for.  The autotuner picks one.
+//
+// Stage layout in shared memory (bytes, 128-byte aligned pieces):
+//   half A      ROWS rows x 128 nodes x 2 components (strip columns 0..127)
+//   half B      ROWS rows x 128 nodes x 2 components (strip columns 128..255)
+//   halo L      ROWS x 16 bytes: node col0-1 (FP32: the node pair col0-2, col0-1)
+//   halo R      ROWS x 16 bytes: node col0+256 (FP32: the pair col0+256, col0+257)
+//   factors     ROWS x (hx, 1/hx), written by the producer warp
+// The 2D tensor maps view a row of the field as 2*ny contiguous elements, so
+// every box row is a 2 KB (FP64) / 1 KB (FP32) contiguous run.
+template <class T, int ROWS, int STAGES, int MINB>
+struct Lap1Cfg
 {
-    return kTJ + 2 * Lap1Traits<T>::kHalo;
-}
-
-template <class T>
-__host__ __device__ constexpr int stage_bytes()
-{
-    return kRows * tile_cols<T>() * 2 * static_cast<int>(sizeof(T));
-}
+    using Vec = typename Lap1Traits<T>::Vec;
+    static constexpr int kRows = ROWS;
+    static constexpr int kStages = STAGES;
+    static constexpr int kMinBlocks = MINB;
+    static constexpr int kHalfBytes = ROWS * kHalf * 2 * static_cast<int>(sizeof(T));
+    static constexpr int kHaloBytes = ROWS * 16;
+    static constexpr int kHaloPad = (kHaloBytes + 127) / 128 * 128;
+    static constexpr int kOffB = kHalfBytes;
+    static constexpr int kOffL = 2 * kHalfBytes;
+    static constexpr int kOffR = kOffL + kHaloPad;
+    static constexpr int kOffF = kOffR + kHaloPad;
+    static constexpr int kStageStride = (kOffF + ROWS * 2 * static_cast<int>(sizeof(T)) + 127) / 128 * 128;
+    static constexpr int kTxBytes = 2 * kHalfBytes + 2 * kHaloBytes;
+    static constexpr int kSmemBytes = STAGES * kStageStride + 128;
+};
 
 template <class T>
 struct Lap1Params
@@ -121,7 +138,7 @@ struct Lap1Params
     int ox, oy;                // output front relative to the input front
     int strips;                // column strips of width kTJ over the output
     int64_t work;              // strips * mx (strip-major row items)
-    T const* hx;               // padded spacing arrays [p + 1]
+    T const* hx;               // padded spacing arrays [p + 1] (inverse pads are 0)
     T const* ihx;
     T const* hy;
     T const* ihy;
@@ -144,6 +161,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // Bounded wait on an mbarrier phase; returns false when the bound runs out.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 {
@@ -162,214 +184,262 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
     return false;
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, CUtensorMap const* map, uint64_t* bar, int c0, int c1, int c2)
+__device__ __forceinline__ void tma_load_2d(void* dst, CUtensorMap const* map, uint64_t* bar, int c0, int c1)
 {
     asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-            ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+            ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_addr(bar))
             : "memory");
 }
 
-template <class T>
-__device__ __forceinline__ void issue_stage(CUtensorMap const* map, T* tile, uint64_t* bar, int strip_col0, int row0)
+// One strip segment of the persistent work split: strip, output rows
+// [r_begin, r_end) relative to the output front.
+struct Segment
 {
-    mbar_expect_tx(bar, stage_bytes<T>());
-    if constexpr (sizeof(T) == 8) {
-        // map dims {2 comps, ny, nx}; tile columns start at strip_col0 - 1
-        tma_load_3d(tile, map, bar, 0, strip_col0 - 1, row0);
-    } else {
-        // map dims {4 (two nodes x 2 comps), ny / 2, nx}; columns start at strip_col0 - 2 (even)
-        tma_load_3d(tile, map, bar, 0, (strip_col0 - 2) / 2, row0);
-    }
+    int strip, r_begin, r_end;
+};
+
+template <class T>
+__device__ __forceinline__ Segment next_segment(Lap1Params<T> const& P, int64_t& item, int64_t end)
+{
+    Segment s;
+    s.strip = static_cast<int>(item / P.mx);
+    s.r_begin = static_cast<int>(item % P.mx);
+    int64_t const len = min(end - item, static_cast<int64_t>(P.mx - s.r_begin));
+    s.r_end = s.r_begin + static_cast<int>(len);
+    item += len;
+    return s;
 }
 
-template <class T>
-__global__ void __launch_bounds__(kTJ) lap2d_1form_tma_kernel(const __grid_constant__ CUtensorMap map, Lap1Params<T> P)
+template <class T, class C>
+__global__ void __launch_bounds__(kThreads1, C::kMinBlocks)
+lap2d_1form_tma_kernel(const __grid_constant__ CUtensorMap map_main, const __grid_constant__ CUtensorMap map_halo,
+                       Lap1Params<T> P)
 {
-    using Vec = typename Lap1Traits<T>::Vec;
-    constexpr int H = Lap1Traits<T>::kHalo;
-    constexpr int W = tile_cols<T>();
-    constexpr int kStageElems = stage_bytes<T>() / static_cast<int>(sizeof(T));
+    using Vec = typename C::Vec;
+    constexpr int R = C::kRows;
+    constexpr int S = C::kStages;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // Stage buffers start on a 128-byte boundary (the launch reserves 128 spare bytes).
-    T* tiles = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    __shared__ __align__(8) uint64_t full[kStages];
+    unsigned char* stages = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t empty[S];
+    __shared__ int abort_flag;
 
     int const tid = threadIdx.x;
+    int const warp = tid / 32, lane = tid % 32;
     if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kConsumerWarps);
+        }
+        abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
 
-    // Per-slot counts of loads issued and consumed; identical in every thread
-    // (all control flow below is block-uniform), only thread 0 issues.
-    uint32_t issued[kStages] = {0, 0, 0, 0};
-    uint32_t uses[kStages] = {0, 0, 0, 0};
-    bool ok = true;
-
     int64_t const begin = (P.work * blockIdx.x) / gridDim.x;
     int64_t const end = (P.work * (blockIdx.x + 1)) / gridDim.x;
-    int64_t item = begin;
-    while (item < end && ok) {
-        // Segment: one strip, output rows [r_begin, r_end) relative to the output front.
-        int const strip = static_cast<int>(item / P.mx);
-        int const r_begin = static_cast<int>(item % P.mx);
-        int64_t const seg_len = min(end - item, static_cast<int64_t>(P.mx - r_begin));
-        int const r_end = r_begin + static_cast<int>(seg_len);
-        item += seg_len;
+    // Element offset of node (., col) in the 2*ny-wide rows of the tensor maps.
+    constexpr int kHaloNodes = sizeof(T) == 8 ? 1 : 2;  // nodes in a 16-byte halo box
 
-        int const col0 = P.oy + strip * kTJ;  // first output column of the strip (input-relative)
-        int const j = col0 + tid;             // this thread's column (input-relative)
-        int const i_first = P.ox + r_begin;   // first output row (input-relative)
-        int const i_last = P.ox + r_end;      // one past the last output row
-        int const load_row0 = i_first - 1;    // input rows [i_first - 1, i_last] are read
-        int const nload = i_last - load_row0 + 1;
-        int const nstages = (nload + kRows - 1) / kRows;
-
-        // Column spacing factors at q = j-1, j, j+1 (padded arrays, index q + 1;
-        // columns past the output are clamped, their results are never stored).
-        int const jq = min(j, P.ny - 2);
-        T const hy_m = __ldg(P.hy + jq), ihy_m = __ldg(P.ihy + jq);
-        T const hy_0 = __ldg(P.hy + jq + 1), ihy_0 = __ldg(P.ihy + jq + 1);
-        T const hy_p = __ldg(P.hy + jq + 2), ihy_p = __ldg(P.ihy + jq + 2);
-        bool const col_m_in = j - 1 >= 0;
-        bool const store_col = j < P.oy + P.my;
-
-        if (tid == 0) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            for (int s = 0; s < kStages && s < nstages; ++s)
-                issue_stage<T>(&map, tiles + s * kStageElems, &full[s], col0, load_row0 + s * kRows);
-        }
-        for (int s = 0; s < kStages && s < nstages; ++s) issued[s] += 1;
-
-        // Window state, all at the previous row r-1 unless noted.
-        T a_m = 0, b_m = 0, a_0 = 0, b_0 = 0, a_p = 0;  // components A (x) and B (y) at columns j-1, j, j+1
-        T xy_0 = 0, xx_0 = 0, xy_p = 0, xx_p = 0;       // star of the input: xi_y, xi_x at columns j, j+1
-        T xy_p_prev = 0;                               // xi_y at row r-2, column j+1
-        T eta_prev = 0;                                // eta(r-2, j)
-        T delta_prev = 0;                              // delta(r-1, j)
-        int r = load_row0;
-
-        for (int st = 0; st < nstages; ++st) {
-            int const slot = st % kStages;
-            bool const got = mbar_wait(&full[slot], uses[slot] & 1u);
-            if (!__syncthreads_and(got)) {
-                ok = false;
-                break;
-            }
-            T const* tile = tiles + slot * kStageElems;
-            int const rows_here = min(kRows, nload - st * kRows);
-            for (int rr = 0; rr < rows_here; ++rr, ++r) {
-                Vec const* row = reinterpret_cast<Vec const*>(tile + rr * W * 2);
-                int const c = tid + H;  // tile column of j
-                Vec const vm = row[c - 1], v0 = row[c], vp = row[c + 1];
-                T const hx_r = __ldg(P.hx + r + 1), ihx_r = __ldg(P.ihx + r + 1);
-                bool const row_in = r >= 0;
-                // Star of the 1-form at row r: xi_x = (-hx/hy) B, xi_y = (hy/hx) A, zero outside.
-                T const nxx_m = (row_in && col_m_in) ? ((T(-1) * hx_r) * ihy_m) * vm.y : T(0);
-                T const nxy_0 = row_in ? ((T(1) * ihx_r) * hy_0) * v0.x : T(0);
-                T const nxx_0 = row_in ? ((T(-1) * hx_r) * ihy_0) * v0.y : T(0);
-                T const nxy_p = row_in ? ((T(1) * ihx_r) * hy_p) * vp.x : T(0);
-                T const nxx_p = row_in ? ((T(-1) * hx_r) * ihy_p) * vp.y : T(0);
-                T eta_0 = 0, eta_m = 0, delta_r = 0, delta_up = 0;
-                if (r > load_row0) {
-                    int const p = r - 1;
-                    T const ihx_p = __ldg(P.ihx + p + 1);
-                    bool const p_in = p >= 0;
-                    // eta = star(d w) at (p, j) and (p, j-1); d sums in chain order.
-                    T d0 = T(0);
-                    d0 = d0 - b_0;
-                    d0 = d0 + a_0;
-                    d0 = d0 + v0.y;
-                    d0 = d0 - a_p;
-                    eta_0 = p_in ? ((T(1) * ihx_p) * ihy_0) * d0 : T(0);
-                    T dm = T(0);
-                    dm = dm - b_m;
-                    dm = dm + a_m;
-                    dm = dm + vm.y;
-                    dm = dm - a_0;
-                    eta_m = (p_in && col_m_in) ? ((T(1) * ihx_p) * ihy_m) * dm : T(0);
-                    // delta(r, j): transposed d of xi, star, codifferential sign.
-                    T acc = T(0);
-                    acc = acc - nxy_0;
-                    acc = acc + nxx_0;
-                    acc = acc + xy_0;
-                    acc = acc - nxx_m;
-                    delta_r = T(-1) * (((T(1) * ihx_r) * ihy_0) * (-acc));
-                    // delta(r-1, j+1)
-                    T acc2 = T(0);
-                    acc2 = acc2 - xy_p;
-                    acc2 = acc2 + xx_p;
-                    acc2 = acc2 + xy_p_prev;
-                    acc2 = acc2 - xx_0;
-                    delta_up = T(-1) * (((T(1) * ihx_p) * ihy_p) * (-acc2));
-                }
-                if (r > i_first) {
-                    int const i = r - 1;  // output row
-                    T const hx_i = __ldg(P.hx + i + 1), ihx_i = __ldg(P.ihx + i + 1);
-                    // delta d: transposed d of eta, star, sign -1.
-                    T sx = T(0);
-                    sx = sx - eta_0;
-                    sx = sx + eta_prev;
-                    T sy = T(0);
-                    sy = sy - eta_0;
-                    sy = sy + eta_m;
-                    T const dcx = -sx, dcy = -sy;
-                    T const ddx = T(-1) * (((T(-1) * hx_i) * ihy_0) * dcy);
-                    T const ddy = T(-1) * (((T(1) * ihx_i) * hy_0) * dcx);
-                    // d delta: d of the codifferential.
-                    T ex = T(0);
-                    ex = ex - delta_prev;
-                    ex = ex + delta_r;
-                    T ey = T(0);
-                    ey = ey - delta_prev;
-                    ey = ey + delta_up;
-                    if (store_col) {
-                        Vec o;
-                        o.x = ddx + ex;
-                        o.y = ddy + ey;
-                        __stcs(reinterpret_cast<Vec*>(P.out + static_cast<int64_t>(i - P.ox) * P.out_row) + (j - P.oy), o);
+    if (warp == kConsumerWarps) {
+        // ---------------- producer warp: TMA loads + row factors
+        int64_t g = 0;  // stages issued so far (all segments)
+        bool ok = true;
+        int64_t item = begin;
+        while (item < end && ok) {
+            Segment const sg = next_segment(P, item, end);
+            int const col0 = P.oy + sg.strip * kTJ;
+            int const load_row0 = P.ox + sg.r_begin - 1;
+            int const nload = sg.r_end - sg.r_begin + 2;
+            int const nstages = (nload + R - 1) / R;
+            for (int st = 0; st < nstages; ++st, ++g) {
+                int const slot = static_cast<int>(g % S);
+                uint32_t const use = static_cast<uint32_t>(g / S);
+                if (use > 0) {
+                    bool const got = mbar_wait(&empty[slot], (use - 1) & 1u);
+                    if (!__all_sync(0xffffffffu, got) || *reinterpret_cast<volatile int*>(&abort_flag)) {
+                        ok = false;
+                        break;
                     }
                 }
-                if (r > load_row0) {
-                    eta_prev = eta_0;
-                    delta_prev = delta_r;
+                unsigned char* stage = stages + slot * C::kStageStride;
+                int const row0 = load_row0 + st * R;
+                if (lane < R) {
+                    int const idx = min(row0 + lane + 1, P.nx + 1);
+                    T* fac = reinterpret_cast<T*>(stage + C::kOffF);
+                    fac[2 * lane] = __ldg(P.hx + idx);
+                    fac[2 * lane + 1] = __ldg(P.ihx + idx);
                 }
-                xy_p_prev = xy_p;
-                xy_0 = nxy_0;
-                xx_0 = nxx_0;
-                xy_p = nxy_p;
-                xx_p = nxx_p;
-                a_m = vm.x;
-                b_m = vm.y;
-                a_0 = v0.x;
-                b_0 = v0.y;
-                a_p = vp.x;
-            }
-            uses[slot] += 1;
-            __syncthreads();  // every thread is done reading this slot
-            int const next = st + kStages;
-            if (next < nstages) {
-                if (tid == 0) {
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    issue_stage<T>(&map, tiles + slot * kStageElems, &full[slot], col0, load_row0 + next * kRows);
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_expect_tx(&full[slot], C::kTxBytes);
+                    tma_load_2d(stage, &map_main, &full[slot], 2 * col0, row0);
+                    tma_load_2d(stage + C::kOffB, &map_main, &full[slot], 2 * (col0 + kHalf), row0);
+                    tma_load_2d(stage + C::kOffL, &map_halo, &full[slot], 2 * (col0 - kHaloNodes), row0);
+                    tma_load_2d(stage + C::kOffR, &map_halo, &full[slot], 2 * (col0 + kTJ), row0);
                 }
-                issued[slot] += 1;
             }
         }
-    }
-    if (!ok) {
-        // Let the copies still in flight land (bounded) before the CTA exits.
-        if (tid == 0) {
-            for (int s = 0; s < kStages; ++s) {
-                while (uses[s] < issued[s]) {
-                    mbar_wait(&full[s], uses[s] & 1u);
-                    uses[s] += 1;
-                }
-            }
+        if (!ok && lane == 0) {
+            abort_flag = 1;
             atomicExch(P.error_flag, 1);
+            // Let the loads still in flight land (bounded) before the CTA exits.
+            for (int64_t q = max(g - S, int64_t(0)); q < g; ++q)
+                mbar_wait(&full[q % S], static_cast<uint32_t>(q / S) & 1u);
+        }
+        return;
+    }
+
+    // ---------------- consumer warps: one output column per thread
+    // Neighbour addressing (in Vec units from the stage base): offset of
+    // row 0 and stride between rows, for the left / own / right columns.
+    constexpr int kVecPerHalfRow = kHalf;
+    constexpr int kHaloStride = 16 / static_cast<int>(sizeof(Vec));
+    int const half = tid / kHalf, lc = tid % kHalf;
+    int const o_off = half * (C::kOffB / static_cast<int>(sizeof(Vec))) + lc;
+    int m_off, m_stride, p_off, p_stride;
+    if (tid == 0) {
+        m_off = C::kOffL / static_cast<int>(sizeof(Vec)) + (sizeof(T) == 4 ? 1 : 0);
+        m_stride = kHaloStride;
+    } else if (tid == kHalf) {
+        m_off = kHalf - 1;
+        m_stride = kVecPerHalfRow;
+    } else {
+        m_off = o_off - 1;
+        m_stride = kVecPerHalfRow;
+    }
+    if (tid == kTJ - 1) {
+        p_off = C::kOffR / static_cast<int>(sizeof(Vec));
+        p_stride = kHaloStride;
+    } else if (tid == kHalf - 1) {
+        p_off = C::kOffB / static_cast<int>(sizeof(Vec));
+        p_stride = kVecPerHalfRow;
+    } else {
+        p_off = o_off + 1;
+        p_stride = kVecPerHalfRow;
+    }
+
+    int64_t g = 0;
+    int64_t item = begin;
+    while (item < end) {
+        Segment const sg = next_segment(P, item, end);
+        int const col0 = P.oy + sg.strip * kTJ;
+        int const j = col0 + tid;
+        int const i_first = P.ox + sg.r_begin;
+        int const nload = sg.r_end - sg.r_begin + 2;
+        int const nstages = (nload + R - 1) / R;
+
+        int const jq = min(j, P.ny - 2);  // columns past the output: clamped, never stored
+        T const ihy_m = __ldg(P.ihy + jq);
+        T const hy_0 = __ldg(P.hy + jq + 1), ihy_0 = __ldg(P.ihy + jq + 1);
+        T const hy_p = __ldg(P.hy + jq + 2), ihy_p = __ldg(P.ihy + jq + 2);
+        bool const store_col = j < P.oy + P.my;
+
+        // Window state (previous row r-1 unless noted).
+        T a_m = 0, b_m = 0, a_0 = 0, b_0 = 0, a_p = 0;  // 1-form components A (x), B (y) at j-1, j, j+1
+        T xy_0 = 0, xx_0 = 0, xy_p = 0, xx_p = 0;       // star of the 1-form: xi_y, xi_x at j, j+1
+        T xy_p_prev = 0;                               // xi_y at row r-2, column j+1
+        T s0_prev = 0, sm_prev = 0, sp_prev = 0;        // 1/(hx hy) at (r-1, j), (r-1, j-1), (r-1, j+1)
+        T px0_prev = 0, qy0_prev = 0;                   // hx/hy and hy/hx at (r-1, j)
+        T eta_prev = 0;                                // eta(r-2, j)
+        T delta_prev = 0;                              // delta(r-1, j)
+        // Rows stream from i_first - 1; output row i is complete once row i + 1
+        // has arrived, so the first two streamed rows store nothing.  The eta /
+        // delta values they produce are overwritten before they are used.
+        int out_after = 2;
+        Vec* optr = reinterpret_cast<Vec*>(P.out + static_cast<int64_t>(i_first - P.ox) * P.out_row) + (j - P.oy);
+        int64_t const ostep = P.out_row / 2;  // in Vec units
+
+        auto row_step = [&](Vec const vm, Vec const v0, Vec const vp, T const hx_r, T const ihx_r) {
+            // Hodge factors at row r (zero inverse pads make every factor that
+            // reaches outside the lattice vanish).
+            T const px_m = hx_r * ihy_m;
+            T const qy_0 = ihx_r * hy_0;
+            T const px_0 = hx_r * ihy_0;
+            T const qy_p = ihx_r * hy_p;
+            T const px_p = hx_r * ihy_p;
+            T const s_0 = ihx_r * ihy_0;
+            T const s_m = ihx_r * ihy_m;
+            T const s_p = ihx_r * ihy_p;
+            // Star of the 1-form at row r: xi_x = -(hx/hy) B, xi_y = (hy/hx) A.
+            T const nxx_m = -(px_m * vm.y);
+            T const nxy_0 = qy_0 * v0.x;
+            T const nxx_0 = -(px_0 * v0.y);
+            T const nxy_p = qy_p * vp.x;
+            T const nxx_p = -(px_p * vp.y);
+            // eta = star(d w) at (r-1, j) and (r-1, j-1); chain-order sums.
+            T const d0 = (((-b_0) + a_0) + v0.y) - a_p;
+            T const eta_0 = s0_prev * d0;
+            T const dm = (((-b_m) + a_m) + vm.y) - a_0;
+            T const eta_m = sm_prev * dm;
+            // delta(r, j) and delta(r-1, j+1): transposed d of xi, star, sign.
+            T const acc = (((-nxy_0) + nxx_0) + xy_0) - nxx_m;
+            T const delta_r = s_0 * acc;
+            T const acc2 = (((-xy_p) + xx_p) + xy_p_prev) - xx_0;
+            T const delta_up = sp_prev * acc2;
+            if (out_after == 0) {
+                // Output row r - 1: delta d (transposed d of eta, star, sign) + d delta.
+                T const sx = (-eta_0) + eta_prev;
+                T const sy = (-eta_0) + eta_m;
+                T const ddx = -(px0_prev * sy);
+                T const ddy = qy0_prev * sx;
+                T const ex = (-delta_prev) + delta_r;
+                T const ey = (-delta_prev) + delta_up;
+                Vec o;
+                o.x = ddx + ex;
+                o.y = ddy + ey;
+                if (store_col) __stcs(optr, o);
+                optr += ostep;
+            } else {
+                --out_after;
+            }
+            eta_prev = eta_0;
+            delta_prev = delta_r;
+            xy_p_prev = xy_p;
+            xy_0 = nxy_0;
+            xx_0 = nxx_0;
+            xy_p = nxy_p;
+            xx_p = nxx_p;
+            s0_prev = s_0;
+            sm_prev = s_m;
+            sp_prev = s_p;
+            px0_prev = px_0;
+            qy0_prev = qy_0;
+            a_m = vm.x;
+            b_m = vm.y;
+            a_0 = v0.x;
+            b_0 = v0.y;
+            a_p = vp.x;
+        };
+
+        for (int st = 0; st < nstages; ++st, ++g) {
+            int const slot = static_cast<int>(g % S);
+            uint32_t const use = static_cast<uint32_t>(g / S);
+            if (!mbar_wait(&full[slot], use & 1u)) {
+                if (lane == 0) {
+                    abort_flag = 1;
+                    atomicExch(P.error_flag, 1);
+                }
+                return;
+            }
+            Vec const* sv = reinterpret_cast<Vec const*>(stages + slot * C::kStageStride);
+            Vec const* pm = sv + m_off;
+            Vec const* p0 = sv + o_off;
+            Vec const* pp = sv + p_off;
+            T const* fac = reinterpret_cast<T const*>(stages + slot * C::kStageStride + C::kOffF);
+            int const rows_here = min(R, nload - st * R);
+            if (rows_here == R) {
+#pragma unroll
+                for (int rr = 0; rr < R; ++rr)
+                    row_step(pm[rr * m_stride], p0[rr * kVecPerHalfRow], pp[rr * p_stride], fac[2 * rr], fac[2 * rr + 1]);
+            } else {
+                for (int rr = 0; rr < rows_here; ++rr)
+                    row_step(pm[rr * m_stride], p0[rr * kVecPerHalfRow], pp[rr * p_stride], fac[2 * rr], fac[2 * rr + 1]);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[slot]);
         }
     }
 }
@@ -392,20 +462,6 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
             fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
     });
     return fn;
-}
-
-template <class T>
-int lap1_occupancy()
-{
-    static int blocks = 0;
-    if (blocks == 0) {
-        int smem = kStages * stage_bytes<T>() + 128;
-        cudaFuncSetAttribute(lap2d_1form_tma_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lap2d_1form_tma_kernel<T>, kTJ, smem);
-        blocks = b > 0 ? b : 1;
-    }
-    return blocks;
 }
 
 int sm_count()
@@ -480,65 +536,163 @@ bool lap2d_1form_tma_ok(sil_field const& in, sil_field const& out)
     return encode_fn() != nullptr;
 }
 
-sil_status launch_lap2d_1form_tma(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
-                                  int* error_flag, int max_ctas)
+namespace {
+
+template <class T, class C>
+int lap1_occupancy()
 {
-    int64_t const mx = out.extent[0], my = out.extent[1];
-    if (mx == 0 || my == 0) return SIL_OK;
+    static int blocks = -1;
+    if (blocks < 0) {
+        cudaFuncSetAttribute(lap2d_1form_tma_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmemBytes);
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lap2d_1form_tma_kernel<T, C>, kThreads1, C::kSmemBytes);
+        blocks = b > 0 ? b : 0;
+    }
+    return blocks;
+}
+
+template <class T, class C>
+sil_status launch_variant(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
+                          int* error_flag, int ctas_per_sm)
+{
     auto encode = encode_fn();
     if (encode == nullptr) return fail(SIL_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
-    bool const f64 = in.dtype == SIL_F64;
-    CUtensorMap map;
-    cuuint64_t dims[3];
-    cuuint64_t strides[2];
-    cuuint32_t box[3];
-    cuuint32_t estr[3] = {1, 1, 1};
+    int64_t const mx = out.extent[0], my = out.extent[1];
     uint64_t const nx = in.extent[0], ny = in.extent[1];
-    if (f64) {
-        dims[0] = 2;
-        dims[1] = ny;
-        dims[2] = nx;
-        strides[0] = 2 * 8;
-        strides[1] = 2 * 8 * ny;
-        box[0] = 2;
-        box[1] = tile_cols<double>();
-        box[2] = kRows;
-    } else {
-        dims[0] = 4;
-        dims[1] = ny / 2;
-        dims[2] = nx;
-        strides[0] = 4 * 4;
-        strides[1] = 2 * 4 * ny;
-        box[0] = 4;
-        box[1] = tile_cols<float>() / 2;
-        box[2] = kRows;
-    }
-    CUresult const res = encode(&map, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
-                                in.data, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    constexpr bool f64 = sizeof(T) == 8;
+    // Rows of 2*ny contiguous elements; the main boxes cover half a strip
+    // (128 nodes), the halo boxes one 16-byte slot (1 node FP64, 2 nodes FP32).
+    cuuint64_t dims[2] = {2 * ny, nx};
+    cuuint64_t strides[1] = {2 * ny * sizeof(T)};
+    cuuint32_t box_main[2] = {2 * kHalf, static_cast<cuuint32_t>(C::kRows)};
+    cuuint32_t box_halo[2] = {16 / sizeof(T), static_cast<cuuint32_t>(C::kRows)};
+    cuuint32_t estr[2] = {1, 1};
+    auto const dt = f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUtensorMap map_main, map_halo;
+    CUresult res = encode(&map_main, dt, 2, in.data, dims, strides, box_main, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (res == CUDA_SUCCESS)
+        res = encode(&map_halo, dt, 2, in.data, dims, strides, box_halo, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (res != CUDA_SUCCESS) return fail(SIL_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    int const occ = lap1_occupancy<T, C>();
+    if (occ < 1) return fail(SIL_ERR_UNSUPPORTED, "1-form Laplacian variant does not fit on an SM");
     int const strips = static_cast<int>((my + kTJ - 1) / kTJ);
     int64_t const work = static_cast<int64_t>(strips) * mx;
-    int64_t const gx = in.front[0] - geo.front[0], gy = in.front[1] - geo.front[1];
-    int const resident = sm_count() * (f64 ? lap1_occupancy<double>() : lap1_occupancy<float>());
-    int64_t ctas = std::min<int64_t>(work, max_ctas > 0 ? std::min(max_ctas, resident) : resident);
+    int const per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, occ) : occ;
+    int64_t ctas = std::min<int64_t>(work, static_cast<int64_t>(sm_count()) * per_sm);
     if (ctas < 1) ctas = 1;
-    if (f64) {
-        Lap1Params<double> P {static_cast<double*>(out.data), out.stride[0], static_cast<int>(nx), static_cast<int>(ny),
-                              static_cast<int>(mx), static_cast<int>(my), static_cast<int>(out.front[0] - in.front[0]),
-                              static_cast<int>(out.front[1] - in.front[1]), strips, work, geo.h[0] + gx,
-                              geo.inv_h[0] + gx, geo.h[1] + gy, geo.inv_h[1] + gy, error_flag};
-        lap2d_1form_tma_kernel<double><<<static_cast<unsigned>(ctas), kTJ, kStages * stage_bytes<double>() + 128, stream>>>(map, P);
-    } else {
-        Lap1Params<float> P {static_cast<float*>(out.data), out.stride[0], static_cast<int>(nx), static_cast<int>(ny),
-                             static_cast<int>(mx), static_cast<int>(my), static_cast<int>(out.front[0] - in.front[0]),
-                             static_cast<int>(out.front[1] - in.front[1]), strips, work, geo.h32[0] + gx,
-                             geo.inv_h32[0] + gx, geo.h32[1] + gy, geo.inv_h32[1] + gy, error_flag};
-        lap2d_1form_tma_kernel<float><<<static_cast<unsigned>(ctas), kTJ, kStages * stage_bytes<float>() + 128, stream>>>(map, P);
-    }
+    int64_t const gx = in.front[0] - geo.front[0], gy = in.front[1] - geo.front[1];
+    T const* const* gh = reinterpret_cast<T const* const*>(f64 ? (void const*)geo.h : (void const*)geo.h32);
+    T const* const* gih = reinterpret_cast<T const* const*>(f64 ? (void const*)geo.inv_h : (void const*)geo.inv_h32);
+    Lap1Params<T> P {static_cast<T*>(out.data), out.stride[0], static_cast<int>(nx), static_cast<int>(ny),
+                     static_cast<int>(mx), static_cast<int>(my), static_cast<int>(out.front[0] - in.front[0]),
+                     static_cast<int>(out.front[1] - in.front[1]), strips, work, gh[0] + gx, gih[0] + gx, gh[1] + gy,
+                     gih[1] + gy, error_flag};
+    lap2d_1form_tma_kernel<T, C><<<static_cast<unsigned>(ctas), kThreads1, C::kSmemBytes, stream>>>(map_main, map_halo, P);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
+}
+
+// Candidate pipeline shapes (rows per stage, stages, CTAs per SM sized for).
+template <class T>
+struct Lap1Variants;
+template <>
+struct Lap1Variants<double>
+{
+    using V0 = Lap1Cfg<double, 4, 4, 2>;
+    using V1 = Lap1Cfg<double, 4, 6, 2>;
+    using V2 = Lap1Cfg<double, 8, 3, 2>;
+    using V3 = Lap1Cfg<double, 8, 6, 1>;
+    using V4 = Lap1Cfg<double, 2, 8, 2>;
+    using V5 = Lap1Cfg<double, 16, 3, 1>;
+};
+template <>
+struct Lap1Variants<float>
+{
+    using V0 = Lap1Cfg<float, 4, 4, 3>;
+    using V1 = Lap1Cfg<float, 4, 8, 2>;
+    using V2 = Lap1Cfg<float, 8, 4, 2>;
+    using V3 = Lap1Cfg<float, 8, 8, 1>;
+    using V4 = Lap1Cfg<float, 2, 8, 3>;
+    using V5 = Lap1Cfg<float, 16, 4, 1>;
+};
+
+constexpr int kLap1Variants = 6;
+
+template <class T>
+sil_status launch_by_index(int v, cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
+                           int* error_flag, int ctas_per_sm)
+{
+    using V = Lap1Variants<T>;
+    switch (v) {
+    case 0: return launch_variant<T, typename V::V0>(stream, geo, in, out, error_flag, ctas_per_sm);
+    case 1: return launch_variant<T, typename V::V1>(stream, geo, in, out, error_flag, ctas_per_sm);
+    case 2: return launch_variant<T, typename V::V2>(stream, geo, in, out, error_flag, ctas_per_sm);
+    case 3: return launch_variant<T, typename V::V3>(stream, geo, in, out, error_flag, ctas_per_sm);
+    case 4: return launch_variant<T, typename V::V4>(stream, geo, in, out, error_flag, ctas_per_sm);
+    default: return launch_variant<T, typename V::V5>(stream, geo, in, out, error_flag, ctas_per_sm);
+    }
+}
+
+} // namespace
+
+int lap2d_1form_variants()
+{
+    return kLap1Variants;
+}
+
+// Launch pipeline variant `variant` (0 = default) of the TMA 1-form kernel.
+sil_status launch_lap2d_1form_tma(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
+                                  int* error_flag, int variant)
+{
+    if (out.extent[0] == 0 || out.extent[1] == 0) return SIL_OK;
+    if (variant < 0 || variant >= kLap1Variants) variant = 0;
+    if (in.dtype == SIL_F64) return launch_by_index<double>(variant, stream, geo, in, out, error_flag, 0);
+    return launch_by_index<float>(variant, stream, geo, in, out, error_flag, 0);
+}
+
+// Time every variant on the caller's fields (two warm-up and three timed
+// launches each) and return the fastest.  Runs on `stream` and synchronises it.
+sil_status autotune_lap2d_1form(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
+                                int* error_flag, int* best_variant, float* best_ms)
+{
+    cudaEvent_t e0, e1;
+    SIL_CUDA_CHECK(cudaEventCreate(&e0));
+    SIL_CUDA_CHECK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_v = 0;
+    sil_status st = SIL_OK;
+    for (int v = 0; v < kLap1Variants && st == SIL_OK; ++v) {
+        sil_status const probe = launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
+        if (probe == SIL_ERR_UNSUPPORTED) continue;  // does not fit: skip
+        if (probe != SIL_OK) {
+            st = probe;
+            break;
+        }
+        launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
+        cudaEventRecord(e0, stream);
+        for (int i = 0; i < 3; ++i) launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
+        cudaEventRecord(e1, stream);
+        cudaError_t const err = cudaEventSynchronize(e1);
+        if (err != cudaSuccess) {
+            st = cuda_fail(err, "autotune");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= 3.f;
+        if (ms < best) {
+            best = ms;
+            best_v = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *best_variant = best_v;
+    *best_ms = best;
+    return st;
 }
 
 } // namespace sil

@@ -119,7 +119,8 @@ struct Geometry
     int64_t front[kMaxNHodge] = {0, 0, 0};
     // Device arrays of length npoints + 2, index shifted by one: entry
     // [p + 1] is the edge length along the axis at node p (forward
-    // difference, backward at the last node); the pads hold 1.
+    // difference, backward at the last node); the pads hold h = 1 and
+    // inv_h = 0.
     double* h[kMaxNHodge] = {nullptr, nullptr, nullptr};
     double* inv_h[kMaxNHodge] = {nullptr, nullptr, nullptr};
     float* h32[kMaxNHodge] = {nullptr, nullptr, nullptr};
