@@ -144,7 +144,7 @@ int sil_laplacian_plan_kernel(sil_laplacian_plan plan);
 /* Pipeline shape of kernel 2 chosen by the autotuner on the plan's first
  * run (-1 before it).  The first run times each shape on the caller's fields
  * and synchronises the stream once; SIMILIE_B200_AUTOTUNE=0 skips the tuning
- * and uses shape 0. */
+ * and uses shape 0, SIMILIE_B200_LAP1_VARIANT=<digit> forces a shape. */
 int sil_laplacian_plan_variant(sil_laplacian_plan plan);
 /* Synchronising check of the plan's device error flag: SIL_ERR_BUDGET when a
  * bounded wait inside a kernel ran out (the kernel returned early). */

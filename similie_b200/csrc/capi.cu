@@ -309,7 +309,10 @@ sil_status sil_laplacian_run(sil_laplacian_plan plan, sil_stream stream, const s
             // First run: time the pipeline shapes on these fields and keep the
             // fastest (synchronises the stream once).
             char const* env = std::getenv("SIMILIE_B200_AUTOTUNE");
-            if (env != nullptr && env[0] == '0') {
+            char const* forced = std::getenv("SIMILIE_B200_LAP1_VARIANT");
+            if (forced != nullptr && forced[0] >= '0' && forced[0] <= '9') {
+                plan->variant = forced[0] - '0';
+            } else if (env != nullptr && env[0] == '0') {
                 plan->variant = 0;
             } else {
                 sil_status const st = autotune_lap2d_1form(s, *plan->geo, *in, *out, plan->error_flag, &plan->variant,
