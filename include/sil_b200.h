@@ -165,6 +165,24 @@ sil_status sil_laplacian(sil_geometry geometry, sil_stream stream, uint32_t form
 sil_status sil_mag2d_apply(sil_stream stream, int64_t nx, int64_t ny, const double* node_mu,
                            const double* a, double* y);
 
+/* Allocation-free variant of sil_mag2d_apply, for callers that must not
+ * allocate device memory while they apply the operator: an operator applied
+ * inside every iteration of someone else's Krylov loop (a matrix-free linear
+ * operator wrapped by a solver library), code running under a memory pool or
+ * a device-memory cap owned by its host framework, or a real-time loop where
+ * an allocation (even a stream-ordered one, which sil_mag2d_apply makes for
+ * its 1/mu scratch) costs an unbounded wait or is not permitted.
+ * The scratch is a fixed device array inside the library of 2,097,152 doubles
+ * (16 MiB), held by every GPU that loads the library until the process exits;
+ * nx*ny above 2,097,152 is rejected with SIL_ERR_INVALID.  The first call on a
+ * device looks up that array's device address (once per device, with the
+ * device current); make that first call before any stream capture.  All calls
+ * share the one array, so calls that overlap on the GPU (e.g. on two streams
+ * at once) race; serialise them.  Same result as sil_mag2d_apply.
+ * This entry point has no counterpart in the reference. */
+sil_status sil_mag2d_apply_noalloc(sil_stream stream, int64_t nx, int64_t ny, const double* node_mu,
+                                   const double* a, double* y);
+
 typedef struct sil_mag2d_problem {
     int64_t nx, ny;          /* nodes per axis (>= 3) */
     const double* node_mu;   /* device, nx*ny: node permeability (mean of adjacent cells) */

@@ -18,6 +18,7 @@
 // ||r|| <= tol ||b||; the final residual is re-evaluated in FP64.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "sil_internal.cuh"
@@ -613,6 +614,72 @@ sil_status sil_mag2d_apply(sil_stream stream, int64_t nx, int64_t ny, const doub
     SIL_CUDA_CHECK(cudaGetLastError());
     SIL_CUDA_CHECK(cudaFreeAsync(nu.ptr, s));
     nu.ptr = nullptr;
+    return SIL_OK;
+}
+
+} // extern "C"
+
+// ------------------------------------------------------------------ allocation-free apply
+
+namespace sil {
+namespace {
+
+// Scratch of sil_mag2d_apply_noalloc: the reciprocal permeability 1/mu of
+// every node.  A fixed array in the library's device image (16 MiB of
+// doubles), so the entry point never allocates; every GPU that loads the
+// library holds it until the process exits.
+constexpr int64_t kNoAllocMaxNodes = int64_t(1) << 21;
+static __device__ __align__(256) double g_noalloc_nu[kNoAllocMaxNodes];
+
+constexpr int kNoAllocMaxDevices = 128;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  The host-side
+// name g_noalloc_nu is only a stand-in for the symbol; its device address is
+// looked up once per device, with that device current.
+sil_status noalloc_scratch(double** out)
+{
+    int dev = 0;
+    SIL_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(SIL_ERR_UNSUPPORTED, "sil_mag2d_apply_noalloc: device index too large");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        cudaError_t const err = cudaGetSymbolAddress(&p, g_noalloc_nu);
+        if (err != cudaSuccess) return cuda_fail(err, "sil_mag2d_apply_noalloc: cudaGetSymbolAddress");
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return SIL_OK;
+}
+
+} // namespace
+} // namespace sil
+
+extern "C" {
+
+sil_status sil_mag2d_apply_noalloc(sil_stream stream, int64_t nx, int64_t ny, const double* node_mu, const double* a,
+                                   double* y)
+{
+    if (nx < 3 || ny < 3) return fail(SIL_ERR_INVALID, "sil_mag2d_apply_noalloc: need at least 3x3 nodes");
+    if (node_mu == nullptr || a == nullptr || y == nullptr)
+        return fail(SIL_ERR_INVALID, "sil_mag2d_apply_noalloc: NULL pointer");
+    if (nx > kNoAllocMaxNodes || ny > kNoAllocMaxNodes || nx * ny > kNoAllocMaxNodes)
+        return fail(SIL_ERR_INVALID, "sil_mag2d_apply_noalloc: nx*ny = " + std::to_string(nx * ny)
+                                             + " exceeds the fixed scratch of " + std::to_string(kNoAllocMaxNodes)
+                                             + " nodes; use sil_mag2d_apply");
+    double* nu = nullptr;
+    sil_status const st = noalloc_scratch(&nu);
+    if (st != SIL_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int64_t const n = nx * ny;
+    int const blocks = static_cast<int>((n + 255) / 256);
+    // Every scratch entry the apply reads is written first, so nothing from a
+    // previous call needs clearing.
+    reciprocal_kernel<<<blocks, 256, 0, s>>>(node_mu, nu, n);
+    mag_apply_kernel<<<blocks, 256, 0, s>>>(nu, a, y, nx, ny);
+    SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
 
