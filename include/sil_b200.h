@@ -190,9 +190,14 @@ typedef struct sil_mag2d_problem {
     double* solution;        /* device, nx*ny: written (initial guess is 0) */
 } sil_mag2d_problem;
 
+/* Both kinds refine on the FP64 true residual r = b - A x: an inner
+ * Jacobi-preconditioned CG solve of A e = r, x += e, until
+ * ||b - A x|| <= tol ||b|| in FP64.  CG_F64 runs the inner CG in FP64 to half
+ * the tolerance (further passes only correct recurrence drift); MIXED_IR runs
+ * it in FP32 to `inner_tolerance` per pass (dot products in FP64). */
 typedef enum sil_solver_kind {
-    SIL_SOLVER_CG_F64 = 0,      /* Jacobi-preconditioned CG, all FP64 */
-    SIL_SOLVER_MIXED_IR = 1     /* FP32 inner Jacobi-CG sweeps, FP64 residual/refinement */
+    SIL_SOLVER_CG_F64 = 0,
+    SIL_SOLVER_MIXED_IR = 1
 } sil_solver_kind;
 
 typedef struct sil_solve_settings {

@@ -116,6 +116,7 @@ struct Scalars
     double rz;        // r . z of the current iterate
     double rr;        // r . r
     double rr0;       // r . r at the start of the (inner) solve
+    double inner_tol2;  // squared relative reduction the inner solve stops at
     double bb;        // b . b (outer right-hand side)
     double alpha, beta;
     double scale;     // outer residual norm used to scale the inner right-hand side
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(kThreads) cg_apply_kernel(Item const* items, P
 template <class T>
 __global__ void __launch_bounds__(kThreads) cg_update_kernel(Item const* items, ProbInfo const* info,
                                                              Vecs<T> const* vecs, Scalars* sc, double* part_a,
-                                                             double* part_b, double tol2)
+                                                             double* part_b)
 {
     __shared__ double red[kThreads / 32];
     Item const it = items[blockIdx.x];
@@ -277,7 +278,7 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(Item const* items, 
         s->iters += 1;
         s->total_iters += 1;
         if (!isfinite(tot_rr) || !isfinite(trz)) s->nonfinite = 1;
-        if (tot_rr <= tol2 * s->rr0 || s->nonfinite) s->done = 1;
+        if (tot_rr <= s->inner_tol2 * s->rr0 || s->nonfinite) s->done = 1;
     }
 }
 
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(kThreads) cg_direction_kernel(Item const* item
 __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items, ProbInfo const* info,
                                                               double const* const* nu64, double const* const* rhs,
                                                               double* const* x64, double* const* r64, Scalars* sc,
-                                                              double* part, double tol2, int mark)
+                                                              double* part, double tol2, double floor2, int mark)
 {
     __shared__ double red[kThreads / 32];
     Item const it = items[blockIdx.x];
@@ -317,6 +318,10 @@ __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items,
         s->rr = tot;
         s->scale = sqrt(tot);
         if (mark && (tot <= tol2 * s->bb || !isfinite(tot))) s->outer_done = 1;
+        // Next inner solve: reduce the (unit-scaled) residual until the outer
+        // residual would be half the tolerance, but never below the floor the
+        // inner precision can reach.
+        s->inner_tol2 = fmax(floor2, 0.25 * tol2 * s->bb / fmax(tot, 1e-300));
         if (!isfinite(tot)) s->nonfinite = 1;
     }
 }
@@ -387,7 +392,7 @@ struct DeviceBuffer
 
 template <class T>
 sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_settings const& set, sil_solve_diagnostics* diag,
-                       cudaStream_t stream, bool mixed)
+                       cudaStream_t stream)
 {
     // Work items: contiguous node ranges of kItemNodes per problem.
     std::vector<Item> items;
@@ -405,7 +410,7 @@ sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_setting
     int const nvec = 7;  // x r z p q dinv nu in precision T
     size_t const vec_bytes = ((total_nodes * sizeof(T) + 255) / 256) * 256;
     size_t const d_bytes = ((total_nodes * sizeof(double) + 255) / 256) * 256;
-    size_t const ndouble_vecs = mixed ? 3 : 1;  // nu64 (+ r64, x64 when mixed)
+    size_t const ndouble_vecs = 3;  // nu64, r64, x64
     size_t bytes = nvec * vec_bytes + ndouble_vecs * d_bytes;
     bytes += sizeof(Item) * nitems + sizeof(ProbInfo) * np + sizeof(Vecs<T>) * np + sizeof(Scalars) * np
              + 3 * sizeof(double) * nitems + 7 * sizeof(void*) * np + 4096;
@@ -420,8 +425,8 @@ sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_setting
     T* vec_base[nvec];
     for (int k = 0; k < nvec; ++k) vec_base[k] = reinterpret_cast<T*>(take(vec_bytes));
     double* nu64_base = reinterpret_cast<double*>(take(d_bytes));
-    double* r64_base = mixed ? reinterpret_cast<double*>(take(d_bytes)) : nullptr;
-    double* x64_base = mixed ? reinterpret_cast<double*>(take(d_bytes)) : nullptr;
+    double* r64_base = reinterpret_cast<double*>(take(d_bytes));
+    double* x64_base = reinterpret_cast<double*>(take(d_bytes));
     Item* d_items = reinterpret_cast<Item*>(take(sizeof(Item) * nitems));
     ProbInfo* d_info = reinterpret_cast<ProbInfo*>(take(sizeof(ProbInfo) * np));
     Vecs<T>* d_vecs = reinterpret_cast<Vecs<T>*>(take(sizeof(Vecs<T>) * np));
@@ -447,8 +452,8 @@ sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_setting
         mu[p] = probs[p].node_mu;
         rhs[p] = probs[p].rhs;
         nu64[p] = nu64_base + off;
-        x64[p] = mixed ? x64_base + off : probs[p].solution;
-        r64[p] = mixed ? r64_base + off : nullptr;
+        x64[p] = x64_base + off;
+        r64[p] = r64_base + off;
         off += info[p].n;
     }
     SIL_CUDA_CHECK(cudaMemcpyAsync(d_items, items.data(), sizeof(Item) * nitems, cudaMemcpyHostToDevice, stream));
@@ -462,8 +467,7 @@ sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_setting
     std::vector<double*> sol(np), scratch(np);
     for (int p = 0; p < np; ++p) {
         sol[p] = probs[p].solution;
-        // FP64 scratch for the final true residual: r64 when refining, else the (FP64) q vectors.
-        scratch[p] = mixed ? r64[p] : reinterpret_cast<double*>(vecs[p].q);
+        scratch[p] = r64[p];  // FP64 scratch for the final true residual
     }
     SIL_CUDA_CHECK(cudaMemcpyAsync(d_sol, sol.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, stream));
     SIL_CUDA_CHECK(cudaMemcpyAsync(d_scratch, scratch.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, stream));
@@ -480,7 +484,7 @@ sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_setting
     // One chunk of CG iterations, captured once as a CUDA graph.
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    auto capture = [&](double tol2) -> sil_status {
+    auto capture = [&](double) -> sil_status {
         if (exec != nullptr) {
             cudaGraphExecDestroy(exec);
             exec = nullptr;
@@ -494,7 +498,7 @@ sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_setting
         cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         for (int c = 0; c < chunk && err == cudaSuccess; ++c) {
             cg_apply_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a);
-            cg_update_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_b, part_c, tol2);
+            cg_update_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_b, part_c);
             cg_direction_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc);
         }
         cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
@@ -519,45 +523,40 @@ sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_setting
         return SIL_OK;
     };
 
+    // Iterative refinement on the FP64 residual: r = b - A x (FP64), an inner
+    // Jacobi-CG solve of A e = r / ||r|| in precision T, x += ||r|| e.  With
+    // T = double the inner target is adaptive (half the outer tolerance), so a
+    // single pass usually suffices and further passes only correct the drift
+    // between the CG recurrence residual and the true residual; with T =
+    // float each pass reduces the residual by about `inner_tolerance`.
     sil_status st = SIL_OK;
     int refinements = 0;
-    if (!mixed) {
-        cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, d_rhs, nullptr, d_sc, part_a,
-                                                           part_b, false);
-        SIL_CUDA_CHECK(cudaGetLastError());
-        st = capture(tol * tol);
+    bool const low = sizeof(T) < sizeof(double);
+    double const inner_tol = low ? (set.inner_tolerance > 0 ? set.inner_tolerance : 1e-4) : 0.0;
+    int const inner_max = low ? (set.inner_iterations > 0 ? set.inner_iterations : 4000) : max_iter;
+    st = capture(0.0);
+    SIL_CUDA_CHECK(cudaMemsetAsync(x64_base, 0, d_bytes, stream));
+    // bb = ||b||^2 via an init pass from the right-hand side.
+    cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, d_rhs, nullptr, d_sc, part_a, part_b,
+                                                       false);
+    int total = 0;
+    while (st == SIL_OK && total < max_iter) {
+        residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc, part_a,
+                                                           tol * tol, inner_tol * inner_tol, 1);
+        SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
+        SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+        bool all = true;
+        for (int p = 0; p < np; ++p) all = all && hs[p].outer_done;
+        if (all) break;
+        cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, nullptr, d_r64, d_sc, part_a,
+                                                           part_b, true);
         int used = 0;
-        if (st == SIL_OK) st = run_until_done(max_iter, &used);
-        if (st == SIL_OK) {
-            copy_from_vec_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_x64);
-        }
-    } else {
-        double const inner_tol = set.inner_tolerance > 0 ? set.inner_tolerance : 1e-4;
-        int const inner_max = set.inner_iterations > 0 ? set.inner_iterations : 4000;
-        st = capture(inner_tol * inner_tol);
-        SIL_CUDA_CHECK(cudaMemsetAsync(x64_base, 0, d_bytes, stream));
-        // bb = ||b||^2 via an init pass from the right-hand side.
-        cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, d_rhs, nullptr, d_sc, part_a,
-                                                           part_b, false);
-        int total = 0;
-        while (st == SIL_OK && total < max_iter) {
-            residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc,
-                                                               part_a, tol * tol, 1);
-            SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
-            SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
-            bool all = true;
-            for (int p = 0; p < np; ++p) all = all && hs[p].outer_done;
-            if (all) break;
-            cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, nullptr, d_r64, d_sc, part_a,
-                                                               part_b, true);
-            int used = 0;
-            st = run_until_done(std::min(inner_max, max_iter - total), &used);
-            total += used;
-            refine_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_x64, d_sc);
-            ++refinements;
-        }
-        if (st == SIL_OK) copy_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_x64, d_sol, d_sc);
+        st = run_until_done(std::min(inner_max, max_iter - total), &used);
+        total += used;
+        refine_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_x64, d_sc);
+        ++refinements;
     }
+    if (st == SIL_OK) copy_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_x64, d_sol, d_sc);
     if (exec != nullptr) cudaGraphExecDestroy(exec);
     if (graph != nullptr) cudaGraphDestroy(graph);
     if (st != SIL_OK) return st;
@@ -572,14 +571,14 @@ sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_setting
     }
     SIL_CUDA_CHECK(cudaMemcpyAsync(d_sc, hs2.data(), sizeof(Scalars) * np, cudaMemcpyHostToDevice, stream));
     residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_sol, d_scratch, d_sc, part_a,
-                                                       tol * tol, 0);
+                                                       tol * tol, 0.0, 0);
     SIL_CUDA_CHECK(cudaGetLastError());
     SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
     SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
     sil_status overall = SIL_OK;
     for (int p = 0; p < np; ++p) {
         sil_solve_diagnostics& d = diag[p];
-        d.iterations = mixed ? hs[p].total_iters : hs[p].iters;
+        d.iterations = hs[p].total_iters;
         d.refinements = refinements;
         d.initial_residual_l2 = std::sqrt(hs[p].bb);
         d.final_residual_l2 = std::sqrt(hs[p].rr);
@@ -695,8 +694,8 @@ sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblem
             return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: NULL field pointer");
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (settings->solver == SIL_SOLVER_CG_F64) return solve_batch<double>(problems, nproblems, *settings, diag, s, false);
-    if (settings->solver == SIL_SOLVER_MIXED_IR) return solve_batch<float>(problems, nproblems, *settings, diag, s, true);
+    if (settings->solver == SIL_SOLVER_CG_F64) return solve_batch<double>(problems, nproblems, *settings, diag, s);
+    if (settings->solver == SIL_SOLVER_MIXED_IR) return solve_batch<float>(problems, nproblems, *settings, diag, s);
     return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: unknown solver kind");
 }
 
