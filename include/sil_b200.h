@@ -227,6 +227,37 @@ sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblem
                                  const sil_solve_settings* settings, sil_solve_diagnostics* diag,
                                  sil_stream stream);
 
+/* ---------------------------------------------------------------------- */
+/* 3D linear magnetostatics: curl-curl residual operator with the Coulomb   */
+/* gauge penalty, on a rectilinear grid.  Nodes flat x fastest              */
+/* (node = i + nx*(j + ny*k)), unknown row = 3*node + c (c = x, y, z);       */
+/* identity rows on the Dirichlet boundary.                                   */
+
+typedef struct sil_mag3d_problem {
+    int64_t nx, ny, nz;      /* nodes per axis (>= 3) */
+    const double* x;         /* HOST, nx strictly increasing node coordinates */
+    const double* y;         /* HOST, ny */
+    const double* z;         /* HOST, nz */
+    const double* node_mu;   /* device, nx*ny*nz: node permeability (mean of adjacent cells) */
+    const double* rhs;       /* device, 3*nx*ny*nz: right-hand side, 0 on the boundary */
+    double* solution;        /* device, 3*nx*ny*nz: written (initial guess is 0) */
+    double gauge_penalty;    /* gamma > 0 (the reference's default is 20) */
+} sil_mag3d_problem;
+
+/* y = K a for one problem (a, y: device, 3*nx*ny*nz doubles; rhs and
+ * solution of the problem are not used).
+ * Replaces: MagnetostaticsOperator3D::apply_with_precomputed_stencils,
+ *   onelab_interface/magnetostatics_onelab.hpp:2241-2396 (Hodge factors 856-910). */
+sil_status sil_mag3d_apply(sil_stream stream, const sil_mag3d_problem* problem, const double* a, double* y);
+
+/* Batched 3D solve; same settings, diagnostics and refinement scheme as
+ * sil_mag2d_solve_batch.  Synchronous.
+ * Replaces: solvers::minimize_strong_formulation_residual for
+ *   MagnetostaticsOperator3D, minimize_strong_formulation_residual.hpp:1308-1382. */
+sil_status sil_mag3d_solve_batch(const sil_mag3d_problem* problems, int nproblems,
+                                 const sil_solve_settings* settings, sil_solve_diagnostics* diag,
+                                 sil_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,12 @@ def lib():
         _lib.silo_mag2d_diagonal.argtypes = [i64, i64, dp, dp]
         _lib.silo_mag2d_cg.argtypes = [i64, i64, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp]
         _lib.silo_num_threads.argtypes = []
+        _lib.silo_mag3d_node_mu.argtypes = [i64, i64, i64, dp, ctypes.c_double, dp]
+        _lib.silo_mag3d_rhs.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp]
+        _lib.silo_mag3d_apply.argtypes = [i64, i64, i64, dp, dp, dp, dp, ctypes.c_double, dp, dp]
+        _lib.silo_mag3d_diagonal.argtypes = [i64, i64, i64, dp, dp, dp, dp, ctypes.c_double, dp]
+        _lib.silo_mag3d_cg.argtypes = [i64, i64, i64, dp, dp, dp, dp, ctypes.c_double, dp, dp, ctypes.c_double,
+                                       ctypes.c_int, dp]
     return _lib
 
 
@@ -248,3 +254,46 @@ def mag2d_cg(nx, ny, node_mu, rhs, tol=1e-10, max_iter=100000):
 
 def num_threads():
     return lib().silo_num_threads()
+
+
+# ----------------------------------------------------------------- magnetostatics 3D
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def mag3d_node_mu(nx, ny, nz, cell_mu, mu0=1.0):
+    out = np.zeros(nx * ny * nz)
+    c = _f64(cell_mu)
+    lib().silo_mag3d_node_mu(nx, ny, nz, _ptr(c), mu0, _ptr(out))
+    return out
+
+
+def mag3d_rhs(x, y, z, cell_j):
+    x, y, z, cj = _f64(x), _f64(y), _f64(z), _f64(cell_j)
+    out = np.zeros(3 * len(x) * len(y) * len(z))
+    lib().silo_mag3d_rhs(len(x), len(y), len(z), _ptr(x), _ptr(y), _ptr(z), _ptr(cj), _ptr(out))
+    return out
+
+
+def mag3d_apply(x, y, z, node_mu, gamma, a):
+    x, y, z, mu, a = _f64(x), _f64(y), _f64(z), _f64(node_mu), _f64(a)
+    out = np.zeros_like(a)
+    lib().silo_mag3d_apply(len(x), len(y), len(z), _ptr(x), _ptr(y), _ptr(z), _ptr(mu), gamma, _ptr(a), _ptr(out))
+    return out
+
+
+def mag3d_diagonal(x, y, z, node_mu, gamma):
+    x, y, z, mu = _f64(x), _f64(y), _f64(z), _f64(node_mu)
+    out = np.zeros(3 * len(x) * len(y) * len(z))
+    lib().silo_mag3d_diagonal(len(x), len(y), len(z), _ptr(x), _ptr(y), _ptr(z), _ptr(mu), gamma, _ptr(out))
+    return out
+
+
+def mag3d_cg(x, y, z, node_mu, gamma, rhs, tol=1e-10, max_iter=100000):
+    x, y, z, mu, b = _f64(x), _f64(y), _f64(z), _f64(node_mu), _f64(rhs)
+    sol = np.zeros_like(b)
+    rel = ctypes.c_double(0.0)
+    it = lib().silo_mag3d_cg(len(x), len(y), len(z), _ptr(x), _ptr(y), _ptr(z), _ptr(mu), gamma, _ptr(b), _ptr(sol),
+                             tol, max_iter, ctypes.byref(rel))
+    return sol, it, rel.value

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <tuple>
 #include <vector>
 
 #ifdef _OPENMP
@@ -1258,6 +1259,265 @@ int silo_mag2d_cg(int64_t nx, int64_t ny, const double* mu, const double* b, dou
     if (final_rel) *final_rel = rnorm / bnorm;
     return it;
 }
+
+// ------------------------------------------------------------------ magnetostatics 3D
+
+namespace {
+
+// Reference local spacing: one-sided at the ends, central average inside.
+// Ref: onelab_interface/magnetostatics_onelab.hpp:856-870
+double local_spacing(const double* c, int64_t n, int64_t i)
+{
+    if (n < 2) return 1.0;
+    if (i == 0) return c[1] - c[0];
+    if (i + 1 == n) return c[n - 1] - c[n - 2];
+    return 0.5 * (c[i + 1] - c[i - 1]);
+}
+
+struct Grid3
+{
+    int64_t nx, ny, nz;
+    const double *x, *y, *z;
+    bool interior(int64_t i, int64_t j, int64_t k) const
+    {
+        return i > 0 && j > 0 && k > 0 && i + 1 < nx && j + 1 < ny && k + 1 < nz;
+    }
+    int64_t node(int64_t i, int64_t j, int64_t k) const { return i + nx * (j + ny * k); }
+};
+
+// One entry of a moment stencil: coefficient of A(node, comp).
+struct MomentTerm
+{
+    int64_t node;
+    int comp;
+    double coeff;
+};
+
+// Moment stencils B_m(s) = (curl A)_m at node s (m = x, y, z), as SimiLie's
+// Coboundary::value builds them for the 2-form components yz, -(xz), xy,
+// visiting the 2x2x2 block (x slowest) and the components in order and
+// dropping columns on the Dirichlet boundary.
+// Ref: onelab_interface/magnetostatics_onelab.hpp:1815-1900,
+//      src/similie/physics/magnetostatics/magnetostatics_quantities.hpp:139-196
+std::vector<MomentTerm> moment_stencil(Grid3 const& g, int64_t i, int64_t j, int64_t k, int m)
+{
+    // coefficients per (di, dj, dk, comp) of the curl component
+    double coef[2][2][2][3] = {};
+    if (m == 0) {  // B_x = -A_z(s) + A_y(s) + A_z(s+y) - A_y(s+z)
+        coef[0][0][0][2] += -1; coef[0][0][0][1] += 1; coef[0][1][0][2] += 1; coef[0][0][1][1] += -1;
+    } else if (m == 1) {  // B_y = -[-A_z(s) + A_x(s) + A_z(s+x) - A_x(s+z)]
+        coef[0][0][0][2] += 1; coef[0][0][0][0] += -1; coef[1][0][0][2] += -1; coef[0][0][1][0] += 1;
+    } else {  // B_z = -A_y(s) + A_x(s) + A_y(s+x) - A_x(s+y)
+        coef[0][0][0][1] += -1; coef[0][0][0][0] += 1; coef[1][0][0][1] += 1; coef[0][1][0][0] += -1;
+    }
+    std::vector<MomentTerm> out;
+    for (int di = 0; di < 2; ++di)
+        for (int dj = 0; dj < 2; ++dj)
+            for (int dk = 0; dk < 2; ++dk)
+                for (int c = 0; c < 3; ++c) {
+                    double const v = coef[di][dj][dk][c];
+                    if (v == 0.0) continue;
+                    int64_t const pi = i + di, pj = j + dj, pk = k + dk;
+                    if (!g.interior(pi, pj, pk)) continue;
+                    out.push_back({g.node(pi, pj, pk), c, v});
+                }
+    return out;
+}
+
+double hodge_b(Grid3 const& g, int64_t i, int64_t j, int64_t k, int m)
+{
+    double const dx = local_spacing(g.x, g.nx, i), dy = local_spacing(g.y, g.ny, j), dz = local_spacing(g.z, g.nz, k);
+    if (m == 0) return dx / (dy * dz);
+    if (m == 1) return dy / (dx * dz);
+    return dz / (dx * dy);
+}
+
+double hodge_a(Grid3 const& g, int64_t i, int64_t j, int64_t k, int c)
+{
+    double const dx = local_spacing(g.x, g.nx, i), dy = local_spacing(g.y, g.ny, j), dz = local_spacing(g.z, g.nz, k);
+    if (c == 0) return dy * dz / dx;
+    if (c == 1) return dx * dz / dy;
+    return dx * dy / dz;
+}
+
+// Transposed stencil lists of every DOF: (sampled node, moment component,
+// coefficient), built by visiting the interior sampled nodes in ascending
+// order (the reference fills them with atomics, so its order is not fixed).
+struct Transposed
+{
+    std::vector<std::vector<std::tuple<int64_t, int, double>>> rows;
+};
+
+Transposed transposed_lists(Grid3 const& g)
+{
+    Transposed t;
+    t.rows.resize(3 * g.nx * g.ny * g.nz);
+    for (int64_t k = 1; k + 1 < g.nz; ++k)
+        for (int64_t j = 1; j + 1 < g.ny; ++j)
+            for (int64_t i = 1; i + 1 < g.nx; ++i)
+                for (int m = 0; m < 3; ++m)
+                    for (auto const& term : moment_stencil(g, i, j, k, m))
+                        t.rows[3 * term.node + term.comp].push_back({g.node(i, j, k), m, term.coeff});
+    return t;
+}
+
+double moment_value(Grid3 const& g, int64_t s, int m, const double* a)
+{
+    int64_t const i = s % g.nx, j = (s / g.nx) % g.ny, k = s / (g.nx * g.ny);
+    double v = 0.0;
+    for (auto const& term : moment_stencil(g, i, j, k, m)) v += term.coeff * a[3 * term.node + term.comp];
+    return v;
+}
+
+} // namespace
+
+extern "C" {
+
+// Ref: onelab_interface/magnetostatics_onelab.hpp:5030-5067 (node mu, mean of adjacent cells)
+void silo_mag3d_node_mu(int64_t nx, int64_t ny, int64_t nz, const double* cell_mu, double mu0, double* node_mu)
+{
+    int64_t const ncx = nx - 1, ncy = ny - 1, ncz = nz - 1;
+    for (int64_t k = 0; k < nz; ++k)
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                double acc = 0.0;
+                int64_t cnt = 0;
+                for (int dk = -1; dk <= 0; ++dk)
+                    for (int dj = -1; dj <= 0; ++dj)
+                        for (int di = -1; di <= 0; ++di) {
+                            int64_t const ci = i + di, cj = j + dj, ck = k + dk;
+                            if (ci < 0 || cj < 0 || ck < 0 || ci >= ncx || cj >= ncy || ck >= ncz) continue;
+                            acc += cell_mu[ci + ncx * (cj + ncy * ck)];
+                            ++cnt;
+                        }
+                node_mu[i + nx * (j + ny * k)] = cnt == 0 ? mu0 : acc / static_cast<double>(cnt);
+            }
+}
+
+// Ref: onelab_interface/magnetostatics_onelab.hpp:4919-4975
+void silo_mag3d_rhs(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                    const double* cell_j, double* rhs)
+{
+    int64_t const ncx = nx - 1, ncy = ny - 1, ncz = nz - 1;
+    for (int64_t k = 0; k < nz; ++k)
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                int64_t const node = i + nx * (j + ny * k);
+                bool const boundary = i == 0 || j == 0 || k == 0 || i + 1 == nx || j + 1 == ny || k + 1 == nz;
+                for (int c = 0; c < 3; ++c) {
+                    double acc = 0.0;
+                    if (!boundary) {
+                        for (int dk = -1; dk <= 0; ++dk)
+                            for (int dj = -1; dj <= 0; ++dj)
+                                for (int di = -1; di <= 0; ++di) {
+                                    int64_t const ci = i + di, cj = j + dj, ck = k + dk;
+                                    if (ci < 0 || cj < 0 || ck < 0 || ci >= ncx || cj >= ncy || ck >= ncz) continue;
+                                    double const wx = x[ci + 1] - x[ci], wy = y[cj + 1] - y[cj], wz = z[ck + 1] - z[ck];
+                                    double face = wx * wy;
+                                    if (c == 0) face = wy * wz;
+                                    else if (c == 1) face = wx * wz;
+                                    acc += 0.125 * face * cell_j[3 * (ci + ncx * (cj + ncy * ck)) + c];
+                                }
+                    }
+                    rhs[3 * node + c] = acc;
+                }
+            }
+}
+
+// Ref: onelab_interface/magnetostatics_onelab.hpp:2242-2396 (precomputed-stencil apply,
+// Coulomb-gauge penalty gamma * H_A * A; y-response sign and divergence gauge at their defaults)
+void silo_mag3d_apply(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                      const double* node_mu, double gamma, const double* a, double* out)
+{
+    Grid3 const g {nx, ny, nz, x, y, z};
+    Transposed const t = transposed_lists(g);
+    int64_t const nn = nx * ny * nz;
+#pragma omp parallel for schedule(static)
+    for (int64_t node = 0; node < nn; ++node) {
+        int64_t const i = node % nx, j = (node / nx) % ny, k = node / (nx * ny);
+        for (int c = 0; c < 3; ++c) {
+            int64_t const row = 3 * node + c;
+            if (!g.interior(i, j, k)) {
+                out[row] = a[row];
+                continue;
+            }
+            double residual = 0.0;
+            for (auto const& [s, m, coeff] : t.rows[row]) {
+                int64_t const si = s % nx, sj = (s / nx) % ny, sk = s / (nx * ny);
+                residual += coeff * hodge_b(g, si, sj, sk, m) * (moment_value(g, s, m, a) / node_mu[s]);
+            }
+            double const gauge = gamma * hodge_a(g, i, j, k, c) * a[row];
+            out[row] = residual + gauge;
+        }
+    }
+}
+
+void silo_mag3d_diagonal(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                         const double* node_mu, double gamma, double* diag)
+{
+    Grid3 const g {nx, ny, nz, x, y, z};
+    Transposed const t = transposed_lists(g);
+    int64_t const nn = nx * ny * nz;
+    for (int64_t node = 0; node < nn; ++node) {
+        int64_t const i = node % nx, j = (node / nx) % ny, k = node / (nx * ny);
+        for (int c = 0; c < 3; ++c) {
+            int64_t const row = 3 * node + c;
+            if (!g.interior(i, j, k)) {
+                diag[row] = 1.0;
+                continue;
+            }
+            double d = 0.0;
+            for (auto const& [s, m, coeff] : t.rows[row]) {
+                int64_t const si = s % nx, sj = (s / nx) % ny, sk = s / (nx * ny);
+                d += coeff * coeff * hodge_b(g, si, sj, sk, m) / node_mu[s];
+            }
+            diag[row] = d + gamma * hodge_a(g, i, j, k, c);
+        }
+    }
+}
+
+int silo_mag3d_cg(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                  const double* node_mu, double gamma, const double* b, double* sol, double tol, int max_iter,
+                  double* final_rel)
+{
+    int64_t const n = 3 * nx * ny * nz;
+    std::vector<double> r(b, b + n), zv(n), p(n), q(n), dinv(n);
+    silo_mag3d_diagonal(nx, ny, nz, x, y, z, node_mu, gamma, dinv.data());
+    for (int64_t i = 0; i < n; ++i) {
+        dinv[i] = 1. / dinv[i];
+        sol[i] = 0.;
+        zv[i] = dinv[i] * r[i];
+        p[i] = zv[i];
+    }
+    double const bnorm = std::sqrt(dot(n, b, b));
+    if (bnorm == 0.) {
+        if (final_rel) *final_rel = 0.;
+        return 0;
+    }
+    double rz = dot(n, r.data(), zv.data());
+    double rnorm = bnorm;
+    int it = 0;
+    while (it < max_iter) {
+        silo_mag3d_apply(nx, ny, nz, x, y, z, node_mu, gamma, p.data(), q.data());
+        double const alpha = rz / dot(n, p.data(), q.data());
+        for (int64_t i = 0; i < n; ++i) {
+            sol[i] += alpha * p[i];
+            r[i] -= alpha * q[i];
+        }
+        ++it;
+        rnorm = std::sqrt(dot(n, r.data(), r.data()));
+        if (rnorm <= tol * bnorm) break;
+        for (int64_t i = 0; i < n; ++i) zv[i] = dinv[i] * r[i];
+        double const rz_new = dot(n, r.data(), zv.data());
+        double const beta = rz_new / rz;
+        rz = rz_new;
+        for (int64_t i = 0; i < n; ++i) p[i] = zv[i] + beta * p[i];
+    }
+    if (final_rel) *final_rel = rnorm / bnorm;
+    return it;
+}
+
+} // extern "C"
 
 int silo_num_threads(void)
 {

@@ -102,6 +102,25 @@ void silo_mag2d_diagonal(int64_t nx, int64_t ny, const double* node_mu, double* 
 int silo_mag2d_cg(int64_t nx, int64_t ny, const double* node_mu, const double* rhs,
                   double* x, double tol, int max_iter, double* final_rel);
 
+/* ------------------------------------------------------------------ */
+/* 3D linear magnetostatics, curl-curl with the gauge penalty.          */
+/* Nodes flat x fastest (node = i + nx*(j + ny*k)), DOF row = 3*node + c. */
+
+/* Node permeability: mean of the (up to 8) adjacent cell values. */
+void silo_mag3d_node_mu(int64_t nx, int64_t ny, int64_t nz, const double* cell_mu, double mu0, double* node_mu);
+/* b = sum over adjacent cells of 1/8 * dual face * J_c, zero on the boundary.
+ * cell_j holds 3 components per cell, cell = ci + ncx*(cj + ncy*ck). */
+void silo_mag3d_rhs(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                    const double* cell_j, double* rhs);
+/* y = (curl^T W curl + gamma H_A) a on interior DOFs, identity on the boundary. */
+void silo_mag3d_apply(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                      const double* node_mu, double gamma, const double* a, double* out);
+void silo_mag3d_diagonal(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                         const double* node_mu, double gamma, double* diag);
+int silo_mag3d_cg(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                  const double* node_mu, double gamma, const double* rhs, double* sol, double tol, int max_iter,
+                  double* final_rel);
+
 /* Threads OpenMP uses (for reporting). */
 int silo_num_threads(void);
 

@@ -43,6 +43,21 @@ class SilMag2dProblem(ctypes.Structure):
     ]
 
 
+class SilMag3dProblem(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int64),
+        ("ny", ctypes.c_int64),
+        ("nz", ctypes.c_int64),
+        ("x", ctypes.c_void_p),
+        ("y", ctypes.c_void_p),
+        ("z", ctypes.c_void_p),
+        ("node_mu", ctypes.c_void_p),
+        ("rhs", ctypes.c_void_p),
+        ("solution", ctypes.c_void_p),
+        ("gauge_penalty", ctypes.c_double),
+    ]
+
+
 class SilSolveSettings(ctypes.Structure):
     _fields_ = [
         ("solver", ctypes.c_int32),
@@ -99,6 +114,10 @@ SIGNATURES = [
     ("sil_mag2d_apply", ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, _P, _P]),
     ("sil_mag2d_apply_noalloc", ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, _P, _P]),
     ("sil_mag2d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag2dProblem), ctypes.c_int,
+                                             ctypes.POINTER(SilSolveSettings),
+                                             ctypes.POINTER(SilSolveDiagnostics), _P]),
+    ("sil_mag3d_apply", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dProblem), _P, _P]),
+    ("sil_mag3d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag3dProblem), ctypes.c_int,
                                              ctypes.POINTER(SilSolveSettings),
                                              ctypes.POINTER(SilSolveDiagnostics), _P]),
 ]

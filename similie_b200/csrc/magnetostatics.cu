@@ -106,10 +106,175 @@ struct Vecs
 
 struct ProbInfo
 {
-    int64_t nx, ny, n;
+    int dim;                  // 2: scalar A_z on an nx x ny grid; 3: vector A on nx x ny x nz
+    int64_t nx, ny, nz;
+    int64_t nodes;            // grid nodes
+    int64_t n;                // unknowns: nodes (2D) or 3 * nodes (3D)
+    double gamma;             // 3D gauge penalty
     int nitems;
     int first_item;
+    double const* ls64[3];    // 3D: reference local spacing per axis and its inverse
+    double const* ils64[3];
+    float const* ls32[3];
+    float const* ils32[3];
 };
+
+template <class T>
+__device__ __forceinline__ T const* spacing(ProbInfo const& pi, int axis)
+{
+    if constexpr (sizeof(T) == 8) return pi.ls64[axis];
+    else return pi.ls32[axis];
+}
+
+template <class T>
+__device__ __forceinline__ T const* inv_spacing(ProbInfo const& pi, int axis)
+{
+    if constexpr (sizeof(T) == 8) return pi.ils64[axis];
+    else return pi.ils32[axis];
+}
+
+// 3D curl-curl + gauge penalty at DOF row = 3*node + c (onelab_interface/
+// magnetostatics_onelab.hpp:2242-2396).  The moments are the curl
+// components at the interior sampled nodes s whose stencil holds the DOF,
+//   B_x(s) = A_y(s) - A_z(s) - A_y(s+z) + A_z(s+y)
+//   B_y(s) = -A_x(s) + A_z(s) + A_x(s+z) - A_z(s+x)
+//   B_z(s) = A_x(s) - A_y(s) - A_x(s+y) + A_y(s+x)
+// (boundary DOFs dropped from the stencils), weighted by the Hodge factor of
+// B (d_m / (d_a d_b), central local spacings) and 1/mu(s); the gauge term is
+// gamma * (d_a d_b / d_c) * A.  Boundary rows are the identity.
+template <class T>
+__device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_t row)
+{
+    int64_t const node = row / 3;
+    int const c = static_cast<int>(row - 3 * node);
+    int64_t const nx = pi.nx, ny = pi.ny, nz = pi.nz;
+    int64_t const i = node % nx, t = node / nx, j = t % ny, k = t / ny;
+    auto interior = [&](int64_t ii, int64_t jj, int64_t kk) {
+        return ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz;
+    };
+    if (!interior(i, j, k)) return a[row];
+    auto A = [&](int64_t ii, int64_t jj, int64_t kk, int cc) -> T {
+        return interior(ii, jj, kk) ? a[3 * (ii + nx * (jj + ny * kk)) + cc] : T(0);
+    };
+    auto bx = [&](int64_t ii, int64_t jj, int64_t kk) {
+        T m = T(0);
+        m = m + A(ii, jj, kk, 1);
+        m = m - A(ii, jj, kk, 2);
+        m = m - A(ii, jj, kk + 1, 1);
+        m = m + A(ii, jj + 1, kk, 2);
+        return m;
+    };
+    auto by = [&](int64_t ii, int64_t jj, int64_t kk) {
+        T m = T(0);
+        m = m - A(ii, jj, kk, 0);
+        m = m + A(ii, jj, kk, 2);
+        m = m + A(ii, jj, kk + 1, 0);
+        m = m - A(ii + 1, jj, kk, 2);
+        return m;
+    };
+    auto bz = [&](int64_t ii, int64_t jj, int64_t kk) {
+        T m = T(0);
+        m = m + A(ii, jj, kk, 0);
+        m = m - A(ii, jj, kk, 1);
+        m = m - A(ii, jj + 1, kk, 0);
+        m = m + A(ii + 1, jj, kk, 1);
+        return m;
+    };
+    T const* lx = spacing<T>(pi, 0);
+    T const* ly = spacing<T>(pi, 1);
+    T const* lz = spacing<T>(pi, 2);
+    T const* ilx = inv_spacing<T>(pi, 0);
+    T const* ily = inv_spacing<T>(pi, 1);
+    T const* ilz = inv_spacing<T>(pi, 2);
+    auto w = [&](int64_t ii, int64_t jj, int64_t kk, int m) -> T {
+        T const nuv = nu[ii + nx * (jj + ny * kk)];
+        if (m == 0) return lx[ii] * ily[jj] * ilz[kk] * nuv;
+        if (m == 1) return ly[jj] * ilx[ii] * ilz[kk] * nuv;
+        return lz[kk] * ilx[ii] * ily[jj] * nuv;
+    };
+    T res = T(0);
+    T ha;
+    if (c == 0) {
+        res = res - w(i, j, k, 1) * by(i, j, k);
+        if (interior(i, j, k - 1)) res = res + w(i, j, k - 1, 1) * by(i, j, k - 1);
+        res = res + w(i, j, k, 2) * bz(i, j, k);
+        if (interior(i, j - 1, k)) res = res - w(i, j - 1, k, 2) * bz(i, j - 1, k);
+        ha = ly[j] * lz[k] * ilx[i];
+    } else if (c == 1) {
+        res = res + w(i, j, k, 0) * bx(i, j, k);
+        if (interior(i, j, k - 1)) res = res - w(i, j, k - 1, 0) * bx(i, j, k - 1);
+        res = res - w(i, j, k, 2) * bz(i, j, k);
+        if (interior(i - 1, j, k)) res = res + w(i - 1, j, k, 2) * bz(i - 1, j, k);
+        ha = lx[i] * lz[k] * ily[j];
+    } else {
+        res = res - w(i, j, k, 0) * bx(i, j, k);
+        if (interior(i, j - 1, k)) res = res + w(i, j - 1, k, 0) * bx(i, j - 1, k);
+        res = res + w(i, j, k, 1) * by(i, j, k);
+        if (interior(i - 1, j, k)) res = res - w(i - 1, j, k, 1) * by(i - 1, j, k);
+        ha = lx[i] * ly[j] * ilz[k];
+    }
+    return res + static_cast<T>(pi.gamma) * ha * a[row];
+}
+
+template <class T>
+__device__ __forceinline__ T mag_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_t row)
+{
+    if (pi.dim == 2) return mag_apply_node(a, nu, pi.nx, pi.ny, row);
+    return mag3d_apply_row(a, nu, pi, row);
+}
+
+// Diagonal of the operator at a row (Jacobi preconditioner), from mu directly.
+__device__ double mag_diag_row(double const* mu, ProbInfo const& pi, int64_t row)
+{
+    if (pi.dim == 2) {
+        int64_t const i = row % pi.nx, j = row / pi.nx;
+        if (i == 0 || j == 0 || i + 1 == pi.nx || j + 1 == pi.ny) return 1.0;
+        double d = 0.0;
+        if (j >= 2) d += 1.0 / mu[row - pi.nx];
+        d += 1.0 / mu[row];
+        if (i >= 2) d += 1.0 / mu[row - 1];
+        d += 1.0 / mu[row];
+        return d;
+    }
+    int64_t const node = row / 3;
+    int const c = static_cast<int>(row - 3 * node);
+    int64_t const nx = pi.nx, ny = pi.ny, nz = pi.nz;
+    int64_t const i = node % nx, t = node / nx, j = t % ny, k = t / ny;
+    auto interior = [&](int64_t ii, int64_t jj, int64_t kk) {
+        return ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz;
+    };
+    if (!interior(i, j, k)) return 1.0;
+    double const* lx = pi.ls64[0];
+    double const* ly = pi.ls64[1];
+    double const* lz = pi.ls64[2];
+    double const* ilx = pi.ils64[0];
+    double const* ily = pi.ils64[1];
+    double const* ilz = pi.ils64[2];
+    auto w = [&](int64_t ii, int64_t jj, int64_t kk, int m) -> double {
+        double const nuv = 1.0 / mu[ii + nx * (jj + ny * kk)];
+        if (m == 0) return lx[ii] * ily[jj] * ilz[kk] * nuv;
+        if (m == 1) return ly[jj] * ilx[ii] * ilz[kk] * nuv;
+        return lz[kk] * ilx[ii] * ily[jj] * nuv;
+    };
+    double d = 0.0;
+    if (c == 0) {
+        d += w(i, j, k, 1) + w(i, j, k, 2);
+        if (interior(i, j, k - 1)) d += w(i, j, k - 1, 1);
+        if (interior(i, j - 1, k)) d += w(i, j - 1, k, 2);
+        d += pi.gamma * (ly[j] * lz[k] * ilx[i]);
+    } else if (c == 1) {
+        d += w(i, j, k, 0) + w(i, j, k, 2);
+        if (interior(i, j, k - 1)) d += w(i, j, k - 1, 0);
+        if (interior(i - 1, j, k)) d += w(i - 1, j, k, 2);
+        d += pi.gamma * (lx[i] * lz[k] * ily[j]);
+    } else {
+        d += w(i, j, k, 0) + w(i, j, k, 1);
+        if (interior(i, j - 1, k)) d += w(i, j - 1, k, 0);
+        if (interior(i - 1, j, k)) d += w(i - 1, j, k, 1);
+        d += pi.gamma * (lx[i] * ly[j] * ilz[k]);
+    }
+    return d;
+}
 
 struct Scalars
 {
@@ -227,7 +392,7 @@ __global__ void __launch_bounds__(kThreads) cg_apply_kernel(Item const* items, P
     Vecs<T> const v = vecs[it.prob];
     double pq = 0.0;
     for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-        T const q = mag_apply_node(v.p, v.nu, pi.nx, pi.ny, row);
+        T const q = mag_apply_row(v.p, v.nu, pi, row);
         v.q[row] = q;
         pq += static_cast<double>(v.p[row]) * static_cast<double>(q);
     }
@@ -307,7 +472,7 @@ __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items,
     ProbInfo const pi = info[it.prob];
     double rr = 0.0;
     for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-        double const ax = mag_apply_node(x64[it.prob], nu64[it.prob], pi.nx, pi.ny, row);
+        double const ax = mag_apply_row(x64[it.prob], nu64[it.prob], pi, row);
         double const r = rhs[it.prob][row] - ax;
         r64[it.prob][row] = r;
         rr += r * r;
@@ -340,8 +505,8 @@ __global__ void __launch_bounds__(kThreads) refine_kernel(Item const* items, Vec
         x64[it.prob][row] += scale * static_cast<double>(e[row]);
 }
 
-// nu = 1/mu (FP64 and, for the inner solve, the precision T) and the
-// inverse diagonal of the operator.
+// nu = 1/mu per node (FP64 and, for the inner solve, the precision T) and
+// the inverse diagonal of the operator per unknown.
 template <class T>
 __global__ void setup_kernel(Item const* items, ProbInfo const* info, double const* const* mu, double* const* nu64,
                              Vecs<T> const* vecs)
@@ -350,20 +515,15 @@ __global__ void setup_kernel(Item const* items, ProbInfo const* info, double con
     ProbInfo const pi = info[it.prob];
     Vecs<T> const v = vecs[it.prob];
     double const* m = mu[it.prob];
+    int const per_node = pi.dim == 2 ? 1 : 3;
     for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-        double const nu = 1.0 / m[row];
-        nu64[it.prob][row] = nu;
-        v.nu[row] = static_cast<T>(nu);
-        int64_t const i = row % pi.nx, j = row / pi.nx;
-        double d = 1.0;
-        if (!(i == 0 || j == 0 || i + 1 == pi.nx || j + 1 == pi.ny)) {
-            d = 0.0;
-            if (j >= 2) d += 1.0 / m[row - pi.nx];
-            d += nu;
-            if (i >= 2) d += 1.0 / m[row - 1];
-            d += nu;
+        if (row % per_node == 0) {
+            int64_t const node = row / per_node;
+            double const nu = 1.0 / m[node];
+            nu64[it.prob][node] = nu;
+            v.nu[node] = static_cast<T>(nu);
         }
-        v.dinv[row] = static_cast<T>(1.0 / d);
+        v.dinv[row] = static_cast<T>(1.0 / mag_diag_row(m, pi, row));
     }
 }
 
@@ -390,30 +550,76 @@ struct DeviceBuffer
     ~DeviceBuffer() { cudaFree(ptr); }
 };
 
+// One problem of a batch, 2D or 3D, as the solver driver sees it.
+struct ProblemDesc
+{
+    int dim;
+    int64_t nx, ny, nz;
+    double gamma;
+    double const* node_mu;
+    double const* rhs;
+    double* solution;
+    double const* coords[3];  // 3D: host node coordinates per axis
+};
+
+// Central local spacing of a node along one axis (one-sided at the ends),
+// the length SimiLie's magnetostatics operator uses for its Hodge factors
+// (onelab_interface/magnetostatics_onelab.hpp:856-870).
+double local_spacing(double const* c, int64_t n, int64_t i)
+{
+    if (n < 2) return 1.0;
+    if (i == 0) return c[1] - c[0];
+    if (i + 1 == n) return c[n - 1] - c[n - 2];
+    return 0.5 * (c[i + 1] - c[i - 1]);
+}
+
 template <class T>
-sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_settings const& set, sil_solve_diagnostics* diag,
+sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings const& set, sil_solve_diagnostics* diag,
                        cudaStream_t stream)
 {
-    // Work items: contiguous node ranges of kItemNodes per problem.
+    int const np = static_cast<int>(probs.size());
+    // Work items: contiguous row ranges of kItemNodes per problem.
     std::vector<Item> items;
     std::vector<ProbInfo> info(np);
-    int64_t total_nodes = 0;
+    int64_t total_rows = 0;
+    // 3D spacing tables, per problem [ls_x ls_y ls_z ils_x ils_y ils_z].
+    std::vector<double> sp64;
+    std::vector<int64_t> sp_off(np, -1);
     for (int p = 0; p < np; ++p) {
-        int64_t const n = probs[p].nx * probs[p].ny;
-        info[p] = {probs[p].nx, probs[p].ny, n, 0, static_cast<int>(items.size())};
+        ProblemDesc const& q = probs[p];
+        ProbInfo& pi = info[p];
+        pi = ProbInfo {};
+        pi.dim = q.dim;
+        pi.nx = q.nx;
+        pi.ny = q.ny;
+        pi.nz = q.dim == 3 ? q.nz : 1;
+        pi.nodes = pi.nx * pi.ny * pi.nz;
+        pi.n = q.dim == 3 ? 3 * pi.nodes : pi.nodes;
+        pi.gamma = q.gamma;
+        pi.first_item = static_cast<int>(items.size());
         int idx = 0;
-        for (int64_t b = 0; b < n; b += kItemNodes, ++idx) items.push_back({p, idx, b, std::min(n, b + kItemNodes)});
-        info[p].nitems = idx;
-        total_nodes += n;
+        for (int64_t b = 0; b < pi.n; b += kItemNodes, ++idx) items.push_back({p, idx, b, std::min(pi.n, b + kItemNodes)});
+        pi.nitems = idx;
+        total_rows += pi.n;
+        if (q.dim == 3) {
+            sp_off[p] = static_cast<int64_t>(sp64.size());
+            int64_t const len[3] = {q.nx, q.ny, q.nz};
+            for (int a = 0; a < 3; ++a)
+                for (int64_t i = 0; i < len[a]; ++i) sp64.push_back(local_spacing(q.coords[a], len[a], i));
+            for (int a = 0; a < 3; ++a)
+                for (int64_t i = 0; i < len[a]; ++i) sp64.push_back(1.0 / local_spacing(q.coords[a], len[a], i));
+        }
     }
+    std::vector<float> sp32(sp64.begin(), sp64.end());
     int const nitems = static_cast<int>(items.size());
     int const nvec = 7;  // x r z p q dinv nu in precision T
-    size_t const vec_bytes = ((total_nodes * sizeof(T) + 255) / 256) * 256;
-    size_t const d_bytes = ((total_nodes * sizeof(double) + 255) / 256) * 256;
+    size_t const vec_bytes = ((total_rows * sizeof(T) + 255) / 256) * 256;
+    size_t const d_bytes = ((total_rows * sizeof(double) + 255) / 256) * 256;
     size_t const ndouble_vecs = 3;  // nu64, r64, x64
     size_t bytes = nvec * vec_bytes + ndouble_vecs * d_bytes;
     bytes += sizeof(Item) * nitems + sizeof(ProbInfo) * np + sizeof(Vecs<T>) * np + sizeof(Scalars) * np
-             + 3 * sizeof(double) * nitems + 7 * sizeof(void*) * np + 4096;
+             + 3 * sizeof(double) * nitems + 7 * sizeof(void*) * np + sp64.size() * (sizeof(double) + sizeof(float))
+             + 20 * 256;
     DeviceBuffer buf;
     SIL_CUDA_CHECK(cudaMalloc(&buf.ptr, bytes));
     char* base = static_cast<char*>(buf.ptr);
@@ -441,6 +647,27 @@ sil_status solve_batch(sil_mag2d_problem const* probs, int np, sil_solve_setting
     double** d_r64 = reinterpret_cast<double**>(take(sizeof(void*) * np));
     double** d_sol = reinterpret_cast<double**>(take(sizeof(void*) * np));
     double** d_scratch = reinterpret_cast<double**>(take(sizeof(void*) * np));
+    double* d_sp64 = reinterpret_cast<double*>(take(sizeof(double) * sp64.size()));
+    float* d_sp32 = reinterpret_cast<float*>(take(sizeof(float) * sp32.size()));
+    for (int p = 0; p < np; ++p) {
+        if (sp_off[p] < 0) continue;
+        int64_t const len[3] = {info[p].nx, info[p].ny, info[p].nz};
+        int64_t o = sp_off[p];
+        for (int a = 0; a < 3; ++a) {
+            info[p].ls64[a] = d_sp64 + o;
+            info[p].ls32[a] = d_sp32 + o;
+            o += len[a];
+        }
+        for (int a = 0; a < 3; ++a) {
+            info[p].ils64[a] = d_sp64 + o;
+            info[p].ils32[a] = d_sp32 + o;
+            o += len[a];
+        }
+    }
+    if (!sp64.empty()) {
+        SIL_CUDA_CHECK(cudaMemcpyAsync(d_sp64, sp64.data(), sizeof(double) * sp64.size(), cudaMemcpyHostToDevice, stream));
+        SIL_CUDA_CHECK(cudaMemcpyAsync(d_sp32, sp32.data(), sizeof(float) * sp32.size(), cudaMemcpyHostToDevice, stream));
+    }
 
     std::vector<Vecs<T>> vecs(np);
     std::vector<double const*> mu(np), rhs(np);
@@ -687,16 +914,122 @@ sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblem
 {
     if (problems == nullptr || settings == nullptr || diag == nullptr || nproblems < 1)
         return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: NULL argument or empty batch");
+    std::vector<ProblemDesc> descs(nproblems);
     for (int p = 0; p < nproblems; ++p) {
         sil_mag2d_problem const& q = problems[p];
         if (q.nx < 3 || q.ny < 3) return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: each problem needs >= 3x3 nodes");
         if (q.node_mu == nullptr || q.rhs == nullptr || q.solution == nullptr)
             return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: NULL field pointer");
+        descs[p] = {2, q.nx, q.ny, 1, 0.0, q.node_mu, q.rhs, q.solution, {nullptr, nullptr, nullptr}};
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (settings->solver == SIL_SOLVER_CG_F64) return solve_batch<double>(problems, nproblems, *settings, diag, s);
-    if (settings->solver == SIL_SOLVER_MIXED_IR) return solve_batch<float>(problems, nproblems, *settings, diag, s);
+    if (settings->solver == SIL_SOLVER_CG_F64) return solve_batch<double>(descs, *settings, diag, s);
+    if (settings->solver == SIL_SOLVER_MIXED_IR) return solve_batch<float>(descs, *settings, diag, s);
     return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: unknown solver kind");
+}
+
+} // extern "C"
+
+// ------------------------------------------------------------------ 3D
+
+namespace sil {
+namespace {
+
+sil_status check_mag3d(sil_mag3d_problem const& q, char const* who, bool need_fields)
+{
+    if (q.nx < 3 || q.ny < 3 || q.nz < 3) return fail(SIL_ERR_INVALID, std::string(who) + ": need at least 3x3x3 nodes");
+    if (q.x == nullptr || q.y == nullptr || q.z == nullptr)
+        return fail(SIL_ERR_INVALID, std::string(who) + ": NULL coordinate array");
+    if (q.node_mu == nullptr) return fail(SIL_ERR_INVALID, std::string(who) + ": NULL node_mu");
+    if (need_fields && (q.rhs == nullptr || q.solution == nullptr))
+        return fail(SIL_ERR_INVALID, std::string(who) + ": NULL field pointer");
+    if (!(q.gauge_penalty > 0.0) || !std::isfinite(q.gauge_penalty))
+        return fail(SIL_ERR_INVALID, std::string(who) + ": gauge_penalty must be positive and finite");
+    double const* c[3] = {q.x, q.y, q.z};
+    int64_t const len[3] = {q.nx, q.ny, q.nz};
+    for (int a = 0; a < 3; ++a)
+        for (int64_t i = 0; i + 1 < len[a]; ++i)
+            if (!(c[a][i + 1] > c[a][i]))
+                return fail(SIL_ERR_INVALID, std::string(who) + ": node coordinates must increase strictly");
+    return SIL_OK;
+}
+
+__global__ void mag3d_apply_kernel(ProbInfo pi, double const* nu, double const* a, double* y)
+{
+    int64_t const row = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (row >= pi.n) return;
+    y[row] = mag3d_apply_row(a, nu, pi, row);
+}
+
+} // namespace
+} // namespace sil
+
+extern "C" {
+
+sil_status sil_mag3d_apply(sil_stream stream, const sil_mag3d_problem* problem, const double* a, double* y)
+{
+    if (problem == nullptr || a == nullptr || y == nullptr) return fail(SIL_ERR_INVALID, "sil_mag3d_apply: NULL pointer");
+    sil_mag3d_problem const& q = *problem;
+    sil_status const st = check_mag3d(q, "sil_mag3d_apply", false);
+    if (st != SIL_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int64_t const nodes = q.nx * q.ny * q.nz;
+    int64_t const len[3] = {q.nx, q.ny, q.nz};
+    double const* c[3] = {q.x, q.y, q.z};
+    std::vector<double> sp;
+    for (int a2 = 0; a2 < 3; ++a2)
+        for (int64_t i = 0; i < len[a2]; ++i) sp.push_back(local_spacing(c[a2], len[a2], i));
+    for (int a2 = 0; a2 < 3; ++a2)
+        for (int64_t i = 0; i < len[a2]; ++i) sp.push_back(1.0 / local_spacing(c[a2], len[a2], i));
+    size_t const nu_bytes = (nodes * sizeof(double) + 255) / 256 * 256;
+    DeviceBuffer buf;
+    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, nu_bytes + sp.size() * sizeof(double), s));
+    double* nu = static_cast<double*>(buf.ptr);
+    double* dsp = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + nu_bytes);
+    SIL_CUDA_CHECK(cudaMemcpyAsync(dsp, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    ProbInfo pi {};
+    pi.dim = 3;
+    pi.nx = q.nx;
+    pi.ny = q.ny;
+    pi.nz = q.nz;
+    pi.nodes = nodes;
+    pi.n = 3 * nodes;
+    pi.gamma = q.gauge_penalty;
+    int64_t o = 0;
+    for (int a2 = 0; a2 < 3; ++a2) {
+        pi.ls64[a2] = dsp + o;
+        o += len[a2];
+    }
+    for (int a2 = 0; a2 < 3; ++a2) {
+        pi.ils64[a2] = dsp + o;
+        o += len[a2];
+    }
+    reciprocal_kernel<<<static_cast<int>((nodes + 255) / 256), 256, 0, s>>>(q.node_mu, nu, nodes);
+    mag3d_apply_kernel<<<static_cast<int>((pi.n + 255) / 256), 256, 0, s>>>(pi, nu, a, y);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    // A copy from pageable memory has left the host table once it returns;
+    // the device buffer is freed in stream order after the apply.
+    SIL_CUDA_CHECK(cudaFreeAsync(buf.ptr, s));
+    buf.ptr = nullptr;
+    return SIL_OK;
+}
+
+sil_status sil_mag3d_solve_batch(const sil_mag3d_problem* problems, int nproblems, const sil_solve_settings* settings,
+                                 sil_solve_diagnostics* diag, sil_stream stream)
+{
+    if (problems == nullptr || settings == nullptr || diag == nullptr || nproblems < 1)
+        return fail(SIL_ERR_INVALID, "sil_mag3d_solve_batch: NULL argument or empty batch");
+    std::vector<ProblemDesc> descs(nproblems);
+    for (int p = 0; p < nproblems; ++p) {
+        sil_mag3d_problem const& q = problems[p];
+        sil_status const st = check_mag3d(q, "sil_mag3d_solve_batch", true);
+        if (st != SIL_OK) return st;
+        descs[p] = {3, q.nx, q.ny, q.nz, q.gauge_penalty, q.node_mu, q.rhs, q.solution, {q.x, q.y, q.z}};
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (settings->solver == SIL_SOLVER_CG_F64) return solve_batch<double>(descs, *settings, diag, s);
+    if (settings->solver == SIL_SOLVER_MIXED_IR) return solve_batch<float>(descs, *settings, diag, s);
+    return fail(SIL_ERR_INVALID, "sil_mag3d_solve_batch: unknown solver kind");
 }
 
 } // extern "C"

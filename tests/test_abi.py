@@ -52,6 +52,32 @@ def test_null_arguments_rejected_on_host():
     assert L.sil_geometry_create(None, 2, None, None, None) == 1
 
 
+def test_mag3d_arguments_checked_on_host():
+    import numpy as np
+    L = sil.lib()
+    x = np.linspace(0.0, 1.0, 4)
+    p = _native.SilMag3dProblem()
+    p.nx = p.ny = p.nz = 4
+    p.x = p.y = p.z = x.ctypes.data
+    p.node_mu = p.rhs = p.solution = 256  # never dereferenced: the checks fail first
+    p.gauge_penalty = 0.0
+    assert L.sil_mag3d_apply(None, ctypes.byref(p), 256, 256) == 1
+    assert b"gauge_penalty" in L.sil_last_error()
+    p.gauge_penalty = 20.0
+    p.nz = 2
+    assert L.sil_mag3d_apply(None, ctypes.byref(p), 256, 256) == 1
+    assert b"3x3x3" in L.sil_last_error()
+    p.nz = 4
+    bad = np.array([0.0, 0.5, 0.5, 1.0])
+    p.y = bad.ctypes.data
+    st = _native.SilSolveSettings()
+    diag = (_native.SilSolveDiagnostics * 1)()
+    assert L.sil_mag3d_solve_batch(ctypes.byref(p), 1, ctypes.byref(st), diag, None) == 1
+    assert b"increase" in L.sil_last_error()
+    assert L.sil_mag3d_apply(None, None, None, None) == 1
+    assert L.sil_mag3d_solve_batch(None, 0, None, None, None) == 1
+
+
 def test_rank_and_component_checks_on_host():
     L = sil.lib()
     fi = _native.SilField()

@@ -220,3 +220,45 @@ def test_mag2d_cg_converges():
     r = b - O.mag2d_apply(nx, ny, mu, sol)
     assert np.linalg.norm(r) <= 1.1e-10 * np.linalg.norm(b)
     assert it > 10
+
+
+def test_mag3d_host_setup_matches_oracle():
+    from similie_b200 import magnetostatics3d as m3
+    rng = np.random.default_rng(3)
+    p = m3.synthetic_problem(rng, 14, tube=0.15)
+    nx, ny, nz = p.shape
+    np.testing.assert_allclose(p.node_mu(), O.mag3d_node_mu(nx, ny, nz, p.cell_mu), rtol=1e-15)
+    np.testing.assert_allclose(p.rhs(), O.mag3d_rhs(p.x, p.y, p.z, p.cell_j), rtol=1e-13, atol=1e-18)
+    assert np.count_nonzero(p.cell_j) > 0
+
+
+def test_mag3d_stretched_coords():
+    from similie_b200 import magnetostatics3d as m3
+    x = m3.stretched_coords(256, 1.01)
+    h = np.diff(x)
+    assert x[0] == 0.0 and abs(x[-1] - 1.0) < 1e-15
+    np.testing.assert_allclose(h[1:] / h[:-1], 1.01, rtol=1e-12)
+
+
+def test_mag3d_oracle_operator_properties():
+    """Interior block symmetric positive definite, diagonal consistent, CG converges."""
+    from similie_b200 import magnetostatics3d as m3
+    rng = np.random.default_rng(9)
+    nx, ny, nz = 5, 6, 5
+    x, y, z = m3.stretched_coords(nx, 1.1), m3.stretched_coords(ny, 0.9), m3.stretched_coords(nz, 1.05)
+    mu = rng.uniform(1.0, 10.0, nx * ny * nz)
+    n = 3 * nx * ny * nz
+    A = np.stack([O.mag3d_apply(x, y, z, mu, 20.0, e) for e in np.eye(n)], axis=1)
+    b = np.zeros((nz, ny, nx, 3), dtype=bool)
+    b[0] = b[-1] = True
+    b[:, 0] = b[:, -1] = True
+    b[:, :, 0] = b[:, :, -1] = True
+    inner = np.flatnonzero(~b.ravel())
+    K = A[np.ix_(inner, inner)]
+    assert np.abs(K - K.T).max() <= 1e-13 * np.abs(K).max()
+    assert np.linalg.eigvalsh(K).min() > 0
+    np.testing.assert_allclose(O.mag3d_diagonal(x, y, z, mu, 20.0), np.diag(A), rtol=1e-13)
+    rhs = np.zeros(n)
+    rhs[inner] = rng.standard_normal(inner.size)
+    sol, it, rel = O.mag3d_cg(x, y, z, mu, 20.0, rhs, tol=1e-11)
+    assert rel <= 1e-11 and np.linalg.norm(A @ sol - rhs) <= 1e-10 * np.linalg.norm(rhs)
