@@ -228,6 +228,52 @@ sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblem
                                  sil_stream stream);
 
 /* ---------------------------------------------------------------------- */
+/* Learned multilevel convolutional preconditioner of the 2D solve.        */
+/* M(r) = Jacobi step, then a U-Net correction computed at half resolution  */
+/* from [r1 / rms(r1), log(nu) / log(1000)], then a Jacobi step; 32          */
+/* channels, 3x3 convolutions, BF16 activations and weights with FP32        */
+/* accumulation on the tensor cores.  Trained on (source, solution) pairs    */
+/* with the loss 1 - (u.b)^2 / ((u.K u)(x.b)), u = M(b): the K-norm error    */
+/* left after one optimally scaled preconditioned step.                       */
+/* The reference has no learned preconditioner; the entry points below are  */
+/* the sil_precond_load/train/save family of its GPU design.                 */
+
+typedef struct sil_precond_s* sil_precond;
+
+/* One node grid of a batch: nx x ny nodes, x fastest, starting at element
+ * `offset` of the batch's flat FP32 node arrays (nu = 1/mu, r, b, x, out). */
+typedef struct sil_precond_sample {
+    int32_t nx, ny;
+    int64_t offset;
+} sil_precond_sample;
+
+int64_t sil_precond_num_params(void);
+/* New network with He-normal weights drawn from `seed`. */
+sil_status sil_precond_create(sil_precond* out, uint64_t seed, sil_stream stream);
+void sil_precond_destroy(sil_precond p);
+/* Parameters as FP32 host arrays of sil_precond_num_params() values
+ * (save / load); set_params resets the optimiser state. */
+sil_status sil_precond_get_params(sil_precond p, float* host);
+sil_status sil_precond_set_params(sil_precond p, const float* host, sil_stream stream);
+/* out = M(r) for 1..64 samples (device arrays). */
+sil_status sil_precond_apply(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
+                             const float* nu, const float* r, float* out);
+/* Mean loss over the batch for right-hand sides b with solutions x, the
+ * per-sample losses (host, may be NULL) and the gradient with respect to
+ * every parameter (host FP32, may be NULL).  Synchronous. */
+sil_status sil_precond_loss_grad(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
+                                 const float* nu, const float* b, const float* x, double* loss,
+                                 double* per_sample_loss, float* grad_host);
+/* loss_grad followed by one Adam step (beta 0.9 / 0.999, eps 1e-8). */
+sil_status sil_precond_train_step(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
+                                  const float* nu, const float* b, const float* x, float learning_rate,
+                                  double* loss);
+/* Diagnostic: copy an intermediate buffer of the last batch to the host as
+ * FP32 (which: 0 h, 1 p, 2 g activations of `level`; 3 dh, 4 dg gradients;
+ * 5 input features, 6 network output, 7 M(r), 8 network-output gradient). */
+sil_status sil_precond_debug_fetch(sil_precond p, int which, int level, float* host, int64_t count);
+
+/* ---------------------------------------------------------------------- */
 /* 3D linear magnetostatics: curl-curl residual operator with the Coulomb   */
 /* gauge penalty, on a rectilinear grid.  Nodes flat x fastest              */
 /* (node = i + nx*(j + ny*k)), unknown row = 3*node + c (c = x, y, z);       */

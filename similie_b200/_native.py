@@ -58,6 +58,14 @@ class SilMag3dProblem(ctypes.Structure):
     ]
 
 
+class SilPrecondSample(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32),
+        ("ny", ctypes.c_int32),
+        ("offset", ctypes.c_int64),
+    ]
+
+
 class SilSolveSettings(ctypes.Structure):
     _fields_ = [
         ("solver", ctypes.c_int32),
@@ -116,6 +124,17 @@ SIGNATURES = [
     ("sil_mag2d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag2dProblem), ctypes.c_int,
                                              ctypes.POINTER(SilSolveSettings),
                                              ctypes.POINTER(SilSolveDiagnostics), _P]),
+    ("sil_precond_num_params", ctypes.c_int64, []),
+    ("sil_precond_create", ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_uint64, _P]),
+    ("sil_precond_destroy", None, [_P]),
+    ("sil_precond_get_params", ctypes.c_int, [_P, _P]),
+    ("sil_precond_set_params", ctypes.c_int, [_P, _P, _P]),
+    ("sil_precond_apply", ctypes.c_int, [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P]),
+    ("sil_precond_loss_grad", ctypes.c_int, [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P,
+                                             ctypes.POINTER(ctypes.c_double), _P, _P]),
+    ("sil_precond_train_step", ctypes.c_int, [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P,
+                                              ctypes.c_float, ctypes.POINTER(ctypes.c_double)]),
+    ("sil_precond_debug_fetch", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int64]),
     ("sil_mag3d_apply", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dProblem), _P, _P]),
     ("sil_mag3d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag3dProblem), ctypes.c_int,
                                              ctypes.POINTER(SilSolveSettings),

@@ -1,4 +1,4 @@
-// mag2d.cu -- 2D linear magnetostatics on the GPU: the matrix-free residual
+// magnetostatics.cu -- 2D and 3D linear magnetostatics on the GPU: the matrix-free residual
 // operator d^T (nu d A) with identity rows on the Dirichlet boundary, and a
 // batched Jacobi-preconditioned conjugate-gradient solve (FP64, or FP32
 // inner sweeps inside FP64 iterative refinement).
@@ -21,6 +21,7 @@
 #include <mutex>
 #include <vector>
 
+#include "mag_ops.cuh"
 #include "sil_internal.cuh"
 
 namespace sil {
@@ -32,42 +33,6 @@ constexpr int kNodesPerThread = 8;
 constexpr int kItemNodes = kThreads * kNodesPerThread;  // nodes per work item (one CTA)
 
 // ------------------------------------------------------------------ operator
-
-template <class T>
-__device__ __forceinline__ T mag_apply_node(T const* a, T const* nu, int64_t nx, int64_t ny, int64_t row)
-{
-    int64_t const i = row % nx, j = row / nx;
-    if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) return a[row];
-    T const a0 = a[row];
-    T residual = T(0);
-    if (j >= 2) {
-        int64_t const s = row - nx;
-        T m0 = T(0);
-        m0 = m0 - a[s];
-        m0 = m0 + a0;
-        residual = residual + m0 * nu[s];  // c = +1
-    }
-    {
-        T m0 = T(0);
-        m0 = m0 - a0;
-        m0 = m0 + a[row + nx];
-        residual = residual - m0 * nu[row];  // c = -1
-    }
-    if (i >= 2) {
-        int64_t const s = row - 1;
-        T m1 = T(0);
-        m1 = m1 + a[s];
-        m1 = m1 - a0;
-        residual = residual - m1 * nu[s];  // c = -1
-    }
-    {
-        T m1 = T(0);
-        m1 = m1 + a0;
-        m1 = m1 - a[row + 1];
-        residual = residual + m1 * nu[row];  // c = +1
-    }
-    return residual;
-}
 
 __global__ void mag_apply_kernel(double const* nu, double const* a, double* y, int64_t nx, int64_t ny)
 {

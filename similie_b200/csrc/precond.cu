@@ -1,0 +1,1673 @@
+// precond.cu -- kernels and host driver of the learned multilevel
+// convolutional preconditioner (network layout in precond_net.cuh).
+//
+// Activation storage: one buffer per level holding every image of the batch
+// that reaches that level; an image of h x w pixels is stored padded to
+// (h+2) x (w+2) pixels with a zero border, 32 channels fastest (BF16,
+// 64 bytes per pixel), so a 3x3 tap is a flat pixel offset.  Gradients of
+// activations are FP32 in the same layout.
+//
+// 32->32 convolutions run on the tensor cores as implicit GEMMs: a CTA owns
+// 128 consecutive flat pixels (M = 128), N = 32 output channels, K = 9 taps
+// x 32 input channels.  The three 130-pixel halo rows of the tile are staged
+// once in shared memory in the canonical no-swizzle UMMA layout (16-byte
+// channel chunks, pixels at 16-byte stride), so each of the 9 taps is an
+// operand descriptor at a different start address; 18 tcgen05.mma
+// (128x32x16, BF16 in, FP32 accumulate in TMEM) per tile, one commit, the
+// epilogue reads TMEM with tcgen05.ld and applies bias / ReLU / border.
+// The weight gradient runs on the tensor cores too (M = 4 taps x 32 input
+// channels from an im2col tile, N = 32, K = pixels, MN-major operands),
+// accumulating in TMEM over all tiles of a persistent CTA.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "mag_ops.cuh"
+#include "precond_net.cuh"
+#include "sil_internal.cuh"
+#include "sm100.cuh"
+
+namespace sil {
+namespace nn {
+
+using bf16 = __nv_bfloat16;
+using namespace sil::sm100;
+
+constexpr int kTilePx = 128;
+constexpr int kHalo = kTilePx + 2;
+constexpr int kChunks = kCh / 8;                 // 16-byte chunks per pixel
+constexpr int kKChunks = kTaps * kChunks;        // 36
+constexpr int kWgradParts = kBigW + kCh;         // per-CTA partial: weights + bias
+constexpr uint32_t kIdescFwd = idesc_bf16_f32(128, 32, false, false);
+constexpr uint32_t kIdescWgrad = idesc_bf16_f32(128, 32, true, true);
+
+struct Img
+{
+    int32_t h, w;     // interior pixels
+    int64_t offset;   // pixel offset of the padded image in its level buffer
+};
+
+// Images of one launch: output level and, per image, the other level the
+// input mode reads (POOL: the finer level; UPADD: the coarser level).
+struct Table
+{
+    int nimg;
+    int32_t tile_base[kMaxImages + 1];
+    Img img[kMaxImages];
+    Img aux[kMaxImages];
+};
+
+enum InMode { kPlain = 0, kPool = 1, kUpAdd = 2, kMasked = 3 };
+
+__device__ __forceinline__ void unpack8(uint4 u, float* f)
+{
+    __nv_bfloat162 const* h = reinterpret_cast<__nv_bfloat162 const*>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float2 const t = __bfloat1622float2(h[i]);
+        f[2 * i] = t.x;
+        f[2 * i + 1] = t.y;
+    }
+}
+
+__device__ __forceinline__ uint4 pack8(float const* f)
+{
+    uint4 u;
+    __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+    return u;
+}
+
+__device__ __forceinline__ uint4 ld_chunk(bf16 const* base, int64_t px, int c)
+{
+    return __ldg(reinterpret_cast<uint4 const*>(base + px * kCh) + c);
+}
+
+__device__ __forceinline__ int find_image(Table const& t, int tile)
+{
+    int lo = 0, hi = t.nimg - 1;
+    while (lo < hi) {
+        int const mid = (lo + hi + 1) / 2;
+        if (t.tile_base[mid] <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Channel chunk c (8 channels) of the convolution input at padded flat
+// pixel g of image im, per input mode.  Zero outside the padded image and
+// on its border.
+__device__ uint4 load_input(int mode, Table const& t, int im, int64_t g, int c, bf16 const* in, bf16 const* in2,
+                            float const* gin)
+{
+    Img const o = t.img[im];
+    int64_t const P = o.w + 2;
+    uint4 const zero = make_uint4(0u, 0u, 0u, 0u);
+    if (g < 0 || g >= P * (o.h + 2)) return zero;
+    if (mode == kPlain) return ld_chunk(in, o.offset + g, c);
+    int64_t const y = g / P, x = g - y * P;
+    if (y == 0 || x == 0 || y > o.h || x > o.w) return zero;
+    float f[8];
+    if (mode == kMasked) {
+        float4 const* gp = reinterpret_cast<float4 const*>(gin + (o.offset + g) * kCh + c * 8);
+        float4 const a = __ldg(gp), b = __ldg(gp + 1);
+        float act[8];
+        unpack8(ld_chunk(in2, o.offset + g, c), act);
+        float const gv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < 8; ++i) f[i] = act[i] > 0.0f ? gv[i] : 0.0f;
+        return pack8(f);
+    }
+    if (mode == kPool) {
+        Img const fi = t.aux[im];
+        int64_t const Pf = fi.w + 2;
+        int64_t const base = fi.offset + (2 * y - 1) * Pf + (2 * x - 1);
+        float a[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) f[i] = 0.0f;
+        int64_t const px[4] = {base, base + 1, base + Pf, base + Pf + 1};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            unpack8(ld_chunk(in, px[q], c), a);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) f[i] = f[i] + a[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) f[i] = f[i] * 0.25f;
+        return pack8(f);
+    }
+    // kUpAdd: skip (this level) + nearest-upsampled coarse features
+    Img const ci = t.aux[im];
+    int64_t const cpx = ci.offset + ((y - 1) / 2 + 1) * (ci.w + 2) + ((x - 1) / 2 + 1);
+    float a[8];
+    unpack8(ld_chunk(in, o.offset + g, c), f);
+    unpack8(ld_chunk(in2, cpx, c), a);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) f[i] = f[i] + a[i];
+    return pack8(f);
+}
+
+// Shared memory of the convolution kernel.
+struct ConvSmem
+{
+    uint4 w[kKChunks * kCh];           // B operand: [K chunk][output channel], 18432 B
+    uint4 halo[kChunks * 3 * kHalo];   // A operand source: [chunk][halo row][halo pixel], 24960 B
+    uint64_t bar;
+    uint32_t tmem;
+    int abort;
+};
+
+// out = act(conv3x3(input) + bias) for the interior pixels of every image of
+// the table; border pixels are written as zero.  out_f32 selects an FP32
+// output (data gradients), accumulate adds into it.
+__global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Table t, int mode, bf16 const* in,
+                                                      bf16 const* in2, float const* gin, bf16 const* wt,
+                                                      float const* bias, int relu, bf16* out, float* out_f32,
+                                                      int accumulate, int* error_flag)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    ConvSmem& s = *reinterpret_cast<ConvSmem*>(smem_raw);
+    int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < kKChunks * kCh; i += 128) {
+        int const co = i & 31, k = i >> 5;
+        s.w[k * kCh + co] = __ldg(reinterpret_cast<uint4 const*>(wt + co * (kTaps * kCh)) + k);
+    }
+    if (warp == 0) tmem_alloc(&s.tmem, 32);
+    if (tid == 0) {
+        mbar_init(&s.bar, 1);
+        s.abort = 0;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    uint32_t const tmem = s.tmem;
+    uint32_t const halo_addr = smem_u32(s.halo);
+    uint32_t const w_addr = smem_u32(s.w);
+    uint32_t phase = 0;
+    int const ntiles = t.tile_base[t.nimg];
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int const im = find_image(t, tile);
+        Img const o = t.img[im];
+        int64_t const P = o.w + 2;
+        int64_t const start = P + static_cast<int64_t>(tile - t.tile_base[im]) * kTilePx;
+        for (int i = tid; i < 3 * kHalo * kChunks; i += 128) {
+            int const c = i & 3;
+            int const j = (i >> 2) % kHalo;
+            int const r = (i >> 2) / kHalo;
+            int64_t const g = start + (r - 1) * P - 1 + j;
+            s.halo[(c * 3 + r) * kHalo + j] = load_input(mode, t, im, g, c, in, in2, gin);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            int step = 0;
+#pragma unroll 1
+            for (int tap = 0; tap < kTaps; ++tap) {
+                int const dy = tap / 3, dx = tap % 3;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    uint64_t const a = umma_desc(halo_addr + ((2 * h * 3 + dy) * kHalo + dx) * 16, 3 * kHalo * 16, 128);
+                    uint64_t const b = umma_desc(w_addr + (tap * kChunks + 2 * h) * kCh * 16, kCh * 16, 128);
+                    umma_bf16(tmem, a, b, kIdescFwd, step > 0 ? 1u : 0u);
+                    ++step;
+                }
+            }
+            umma_commit(&s.bar);
+        }
+        __syncwarp();
+        bool const done = mbar_wait(&s.bar, phase);
+        phase ^= 1u;
+        if (!done) s.abort = 1;
+        __syncthreads();
+        if (s.abort) break;
+        tc_fence_after();
+        float acc[32];
+        tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16), acc);
+        int64_t const g = start + warp * 32 + lane;
+        if (g < P * (o.h + 1)) {
+            int64_t const x = g % P;
+            bool const border = x == 0 || x == P - 1;
+            if (border) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) acc[i] = 0.0f;
+            } else {
+                if (bias != nullptr) {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) acc[i] = acc[i] + __ldg(bias + i);
+                }
+                if (relu) {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) acc[i] = fmaxf(acc[i], 0.0f);
+                }
+            }
+            int64_t const px = o.offset + g;
+            if (out_f32 != nullptr) {
+                float4* dst = reinterpret_cast<float4*>(out_f32 + px * kCh);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    float4 v = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+                    if (accumulate) {
+                        float4 const o4 = dst[q];
+                        v.x = v.x + o4.x;
+                        v.y = v.y + o4.y;
+                        v.z = v.z + o4.z;
+                        v.w = v.w + o4.w;
+                    }
+                    dst[q] = v;
+                }
+            } else {
+                uint4* dst = reinterpret_cast<uint4*>(out + px * kCh);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) dst[q] = pack8(acc + 8 * q);
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (s.abort && tid == 0) atomicExch(error_flag, 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, 32);
+}
+
+// Shared memory of the weight-gradient kernel.  The im2col tile is followed
+// by the other buffers so that the third M tile (taps 8..11, of which only
+// tap 8 exists) reads in-bounds shared memory for the missing taps.
+struct WgradSmem
+{
+    uint4 col[kKChunks * kTilePx];     // A operand: [K-row chunk (tap, ci/8)][pixel], 73728 B
+    uint4 dz[kChunks * kTilePx];       // B operand: [output-channel chunk][pixel], 8192 B
+    uint4 halo[kChunks * 3 * kHalo];   // 24960 B
+    uint64_t bar;
+    uint32_t tmem;
+    int abort;
+};
+static_assert(sizeof(uint4) * (kKChunks * kTilePx + kChunks * kTilePx + kChunks * 3 * kHalo)
+                      >= sizeof(uint4) * 48 * kTilePx,
+              "the third M tile must stay inside the shared-memory block");
+
+// Per-CTA partial weight and bias gradients of one 32->32 convolution:
+// dW[co][tap][ci] = sum_p dz[p][co] * in[p + tap][ci], db[co] = sum_p dz[p][co]
+// with dz = dy * (y > 0).
+__global__ void __launch_bounds__(128) wgrad_kernel(const __grid_constant__ Table t, int mode, bf16 const* in,
+                                                    bf16 const* in2, float const* dy, bf16 const* y, float* part,
+                                                    int* error_flag)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    WgradSmem& s = *reinterpret_cast<WgradSmem*>(smem_raw);
+    int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) tmem_alloc(&s.tmem, 128);
+    if (tid == 0) {
+        mbar_init(&s.bar, 1);
+        s.abort = 0;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    uint32_t const tmem = s.tmem;
+    uint32_t const col_addr = smem_u32(s.col);
+    uint32_t const dz_addr = smem_u32(s.dz);
+    uint32_t phase = 0;
+    float db = 0.0f;  // thread co = tid (< 32) accumulates the bias gradient
+    bool any = false;
+    int const ntiles = t.tile_base[t.nimg];
+    Table tz = t;  // masked-mode view of the gradient tile (same images)
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int const im = find_image(t, tile);
+        Img const o = t.img[im];
+        int64_t const P = o.w + 2;
+        int64_t const start = P + static_cast<int64_t>(tile - t.tile_base[im]) * kTilePx;
+        for (int i = tid; i < 3 * kHalo * kChunks; i += 128) {
+            int const c = i & 3;
+            int const j = (i >> 2) % kHalo;
+            int const r = (i >> 2) / kHalo;
+            int64_t const g = start + (r - 1) * P - 1 + j;
+            s.halo[(c * 3 + r) * kHalo + j] = load_input(mode, t, im, g, c, in, in2, nullptr);
+        }
+        for (int i = tid; i < kTilePx * kChunks; i += 128) {
+            int const c = i & 3, m = i >> 2;
+            int64_t const g = start + m;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (g < P * (o.h + 1)) v = load_input(kMasked, tz, im, g, c, y, y, dy);
+            s.dz[c * kTilePx + m] = v;
+        }
+        __syncthreads();
+        for (int i = tid; i < kKChunks * kTilePx; i += 128) {
+            int const m = i % kTilePx, kc = i / kTilePx;
+            int const tap = kc / kChunks, c = kc % kChunks;
+            int const dyy = tap / 3, dxx = tap % 3;
+            s.col[kc * kTilePx + m] = s.halo[(c * 3 + dyy) * kHalo + m + dxx];
+        }
+        if (tid < kCh) {
+            int const c = tid / 8, e = tid % 8;
+            float f[8];
+            for (int m = 0; m < kTilePx; ++m) {
+                unpack8(s.dz[c * kTilePx + m], f);
+                db = db + f[e];
+            }
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll 1
+            for (int mt = 0; mt < 3; ++mt) {
+#pragma unroll
+                for (int kk = 0; kk < kTilePx / 16; ++kk) {
+                    uint64_t const a = umma_desc(col_addr + (16 * mt * kTilePx + kk * 16) * 16, 128, kTilePx * 16);
+                    uint64_t const b = umma_desc(dz_addr + kk * 16 * 16, 128, kTilePx * 16);
+                    umma_bf16(tmem + mt * 32, a, b, kIdescWgrad, (any || kk > 0) ? 1u : 0u);
+                }
+            }
+            umma_commit(&s.bar);
+        }
+        any = true;
+        __syncwarp();
+        bool const done = mbar_wait(&s.bar, phase);
+        phase ^= 1u;
+        if (!done) s.abort = 1;
+        __syncthreads();
+        if (s.abort) break;
+        tc_fence_before();
+        __syncthreads();
+    }
+    float* dst = part + static_cast<int64_t>(blockIdx.x) * kWgradParts;
+    if (!s.abort) {
+        tc_fence_after();
+        for (int mt = 0; mt < 3; ++mt) {
+            float acc[32];
+            tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + mt * 32, acc);
+            int const tap = 4 * mt + warp;
+            if (tap < kTaps) {
+                for (int co = 0; co < kCh; ++co) dst[co * (kTaps * kCh) + tap * kCh + lane] = any ? acc[co] : 0.0f;
+            }
+        }
+        if (tid < kCh) dst[kBigW + tid] = db;
+    } else if (tid == 0) {
+        atomicExch(error_flag, 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, 128);
+}
+
+// grad[i] += sum over parts p of part[p][i] (fixed order).
+__global__ void reduce_parts_kernel(float const* part, int nparts, int n, float* grad)
+{
+    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float sacc = 0.0f;
+    for (int p = 0; p < nparts; ++p) sacc = sacc + part[static_cast<int64_t>(p) * n + i];
+    grad[i] = grad[i] + sacc;
+}
+
+// BF16 weights of the 32->32 convolutions: forward [co][tap][ci] and, for
+// the data gradient, transposed and flipped [ci][8 - tap][co].
+__global__ void convert_weights_kernel(float const* params, bf16* wf, bf16* wt)
+{
+    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kNumBig * kBigW) return;
+    int const j = i / kBigW, r = i % kBigW;
+    int const co = r / (kTaps * kCh), tap = (r / kCh) % kTaps, ci = r % kCh;
+    bf16 const v = __float2bfloat16_rn(params[kOffBig + j * kBigParams + r]);
+    wf[i] = v;
+    wt[j * kBigW + ci * (kTaps * kCh) + (kTaps - 1 - tap) * kCh + co] = v;
+}
+
+// ------------------------------------------------------------------ thin layers (CUDA cores)
+
+// Input convolution 2 -> 32 (+ bias, ReLU) from the FP32 2-channel feature image.
+__global__ void inc_forward_kernel(const __grid_constant__ Table t, float const* feat, float const* params, bf16* out)
+{
+    int const im = blockIdx.y;
+    if (im >= t.nimg) return;
+    Img const o = t.img[im];
+    int64_t const P = o.w + 2, npx = P * (o.h + 2);
+    int64_t const g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= npx) return;
+    int64_t const y = g / P, x = g - y * P;
+    float acc[kCh];
+    bool const border = y == 0 || x == 0 || y > o.h || x > o.w;
+    if (border) {
+        for (int i = 0; i < kCh; ++i) acc[i] = 0.0f;
+    } else {
+        float in[kTaps][2];
+        for (int tap = 0; tap < kTaps; ++tap) {
+            int64_t const q = o.offset + g + (tap / 3 - 1) * P + (tap % 3 - 1);
+            in[tap][0] = feat[2 * q];
+            in[tap][1] = feat[2 * q + 1];
+        }
+        float const* w = params + kOffIn;
+        for (int co = 0; co < kCh; ++co) {
+            float a = 0.0f;
+            for (int tap = 0; tap < kTaps; ++tap)
+                for (int ci = 0; ci < 2; ++ci) a = a + w[(co * kTaps + tap) * 2 + ci] * in[tap][ci];
+            a = a + w[kInW + co];
+            acc[co] = fmaxf(a, 0.0f);
+        }
+    }
+    uint4* dst = reinterpret_cast<uint4*>(out + (o.offset + g) * kCh);
+    for (int q = 0; q < 4; ++q) dst[q] = pack8(acc + 8 * q);
+}
+
+// Output convolution 32 -> 1 (+ bias), FP32 out, zero border.
+__global__ void out_forward_kernel(const __grid_constant__ Table t, bf16 const* in, float const* params, float* out)
+{
+    int const im = blockIdx.y;
+    if (im >= t.nimg) return;
+    Img const o = t.img[im];
+    int64_t const P = o.w + 2, npx = P * (o.h + 2);
+    int64_t const g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= npx) return;
+    int64_t const y = g / P, x = g - y * P;
+    float a = 0.0f;
+    if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
+        float const* w = params + kOffOut;
+        for (int tap = 0; tap < kTaps; ++tap) {
+            int64_t const q = o.offset + g + (tap / 3 - 1) * P + (tap % 3 - 1);
+            float f[8];
+            for (int c = 0; c < kChunks; ++c) {
+                unpack8(ld_chunk(in, q, c), f);
+                for (int e = 0; e < 8; ++e) a = a + w[tap * kCh + c * 8 + e] * f[e];
+            }
+        }
+        a = a + w[kOutW];
+    }
+    out[o.offset + g] = a;
+}
+
+// Data gradient of the output convolution: dg[p][ci] = sum_tap du[p - tap] w[tap][ci].
+__global__ void out_backward_data_kernel(const __grid_constant__ Table t, float const* du, float const* params, float* dg)
+{
+    int const im = blockIdx.y;
+    if (im >= t.nimg) return;
+    Img const o = t.img[im];
+    int64_t const P = o.w + 2, npx = P * (o.h + 2);
+    int64_t const g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= npx) return;
+    int64_t const y = g / P, x = g - y * P;
+    float acc[kCh];
+    for (int i = 0; i < kCh; ++i) acc[i] = 0.0f;
+    if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
+        float const* w = params + kOffOut;
+        for (int tap = 0; tap < kTaps; ++tap) {
+            float const d = du[o.offset + g - (tap / 3 - 1) * P - (tap % 3 - 1)];
+            for (int ci = 0; ci < kCh; ++ci) acc[ci] = acc[ci] + d * w[tap * kCh + ci];
+        }
+    }
+    float4* dst = reinterpret_cast<float4*>(dg + (o.offset + g) * kCh);
+    for (int q = 0; q < 8; ++q) dst[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+}
+
+constexpr int kThinBlock = 256;
+constexpr int kThinPx = 1024;  // pixels per block of the thin weight-gradient kernels
+
+// Image of a flat pixel of the concatenated padded images of a table.
+__device__ __forceinline__ int image_of_pixel(Table const& t, int64_t p)
+{
+    int lo = 0, hi = t.nimg - 1;
+    while (lo < hi) {
+        int const mid = (lo + hi + 1) / 2;
+        if (t.img[mid].offset <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+constexpr int kThinPerThread = 3;  // parameters per thread (608 <= 3 * 256)
+
+// Weight gradient of the output convolution, per-block partials:
+// part[b][tap*32 + ci] = sum_p du[p] in[p + tap][ci], part[b][288] = sum_p du[p],
+// block b covering the flat pixels [b*kThinPx, (b+1)*kThinPx) of the table's images.
+__global__ void __launch_bounds__(kThinBlock) out_wgrad_kernel(const __grid_constant__ Table t, float const* du,
+                                                               bf16 const* in, float* part, int64_t total_px)
+{
+    int const n = kOutW + 1;
+    float acc[kThinPerThread] = {0.0f, 0.0f, 0.0f};
+    int64_t const p0 = static_cast<int64_t>(blockIdx.x) * kThinPx;
+    for (int64_t p = p0; p < p0 + kThinPx && p < total_px; ++p) {
+        Img const o = t.img[image_of_pixel(t, p)];
+        int64_t const g = p - o.offset;
+        int64_t const P = o.w + 2;
+        int64_t const y = g / P, x = g - y * P;
+        if (y == 0 || x == 0 || y > o.h || x > o.w) continue;
+        float const d = du[p];
+#pragma unroll
+        for (int r = 0; r < kThinPerThread; ++r) {
+            int const k = threadIdx.x + r * kThinBlock;
+            if (k > kOutW) continue;
+            if (k == kOutW) {
+                acc[r] = acc[r] + d;
+            } else {
+                int const tap = k / kCh, ci = k % kCh;
+                int64_t const q = p + (tap / 3 - 1) * P + (tap % 3 - 1);
+                acc[r] = acc[r] + d * __bfloat162float(in[q * kCh + ci]);
+            }
+        }
+    }
+    float* dst = part + static_cast<int64_t>(blockIdx.x) * n;
+    for (int r = 0; r < kThinPerThread; ++r) {
+        int const k = threadIdx.x + r * kThinBlock;
+        if (k < n) dst[k] = acc[r];
+    }
+}
+
+// Weight gradient of the input convolution, per-block partials over
+// dz = dh * (h > 0): part[b][(co*9 + tap)*2 + ci], then 32 bias entries.
+__global__ void __launch_bounds__(kThinBlock) inc_wgrad_kernel(const __grid_constant__ Table t, float const* dh,
+                                                               bf16 const* h, float const* feat, float* part,
+                                                               int64_t total_px)
+{
+    int const n = kInW + kCh;
+    float acc[kThinPerThread] = {0.0f, 0.0f, 0.0f};
+    int64_t const p0 = static_cast<int64_t>(blockIdx.x) * kThinPx;
+    for (int64_t p = p0; p < p0 + kThinPx && p < total_px; ++p) {
+        Img const o = t.img[image_of_pixel(t, p)];
+        int64_t const g = p - o.offset;
+        int64_t const P = o.w + 2;
+        int64_t const y = g / P, x = g - y * P;
+        if (y == 0 || x == 0 || y > o.h || x > o.w) continue;
+#pragma unroll
+        for (int r = 0; r < kThinPerThread; ++r) {
+            int const k = threadIdx.x + r * kThinBlock;
+            if (k >= n) continue;
+            int const co = k < kInW ? k / (kTaps * 2) : k - kInW;
+            float const hv = __bfloat162float(h[p * kCh + co]);
+            if (!(hv > 0.0f)) continue;
+            float const d = dh[p * kCh + co];
+            if (k >= kInW) {
+                acc[r] = acc[r] + d;
+            } else {
+                int const tap = (k / 2) % kTaps, ci = k % 2;
+                int64_t const q = p + (tap / 3 - 1) * P + (tap % 3 - 1);
+                acc[r] = acc[r] + d * feat[2 * q + ci];
+            }
+        }
+    }
+    float* dst = part + static_cast<int64_t>(blockIdx.x) * n;
+    for (int r = 0; r < kThinPerThread; ++r) {
+        int const k = threadIdx.x + r * kThinBlock;
+        if (k < n) dst[k] = acc[r];
+    }
+}
+
+// ------------------------------------------------------------------ level adjoints
+
+// dfine[p] += 0.25 * dcoarse[parent(p)] (adjoint of the 2x2 average pool).
+__global__ void pool_adjoint_kernel(const __grid_constant__ Table t, float const* dcoarse, float* dfine)
+{
+    // t.img: fine level; t.aux: coarse level
+    int const im = blockIdx.y;
+    if (im >= t.nimg) return;
+    Img const f = t.img[im], c = t.aux[im];
+    int64_t const P = f.w + 2;
+    int64_t const idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    int64_t const g = idx / 8;
+    int const ch = static_cast<int>(idx % 8) * 4;
+    if (g >= P * (f.h + 2)) return;
+    int64_t const y = g / P, x = g - y * P;
+    if (y == 0 || x == 0 || y > f.h || x > f.w) return;
+    int64_t const cp = c.offset + ((y - 1) / 2 + 1) * (c.w + 2) + ((x - 1) / 2 + 1);
+    float4 const d = *reinterpret_cast<float4 const*>(dcoarse + cp * kCh + ch);
+    float4* o = reinterpret_cast<float4*>(dfine + (f.offset + g) * kCh + ch);
+    float4 v = *o;
+    v.x = v.x + 0.25f * d.x;
+    v.y = v.y + 0.25f * d.y;
+    v.z = v.z + 0.25f * d.z;
+    v.w = v.w + 0.25f * d.w;
+    *o = v;
+}
+
+// Adjoint of skip + up(coarse): dskip[p] += dx[p]; dcoarse[q] += sum of dx over q's children.
+__global__ void upadd_adjoint_skip_kernel(const __grid_constant__ Table t, float const* dx, float* dskip)
+{
+    int const im = blockIdx.y;
+    if (im >= t.nimg) return;
+    Img const f = t.img[im];
+    int64_t const P = f.w + 2;
+    int64_t const idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    int64_t const g = idx / 8;
+    int const ch = static_cast<int>(idx % 8) * 4;
+    if (g >= P * (f.h + 2)) return;
+    int64_t const q = (f.offset + g) * kCh + ch;
+    float4 const d = *reinterpret_cast<float4 const*>(dx + q);
+    float4* o = reinterpret_cast<float4*>(dskip + q);
+    float4 v = *o;
+    v.x = v.x + d.x;
+    v.y = v.y + d.y;
+    v.z = v.z + d.z;
+    v.w = v.w + d.w;
+    *o = v;
+}
+
+__global__ void upadd_adjoint_coarse_kernel(const __grid_constant__ Table t, float const* dx, float* dcoarse)
+{
+    // t.img: coarse level; t.aux: fine level
+    int const im = blockIdx.y;
+    if (im >= t.nimg) return;
+    Img const c = t.img[im], f = t.aux[im];
+    int64_t const P = c.w + 2;
+    int64_t const idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    int64_t const g = idx / 8;
+    int const ch = static_cast<int>(idx % 8) * 4;
+    if (g >= P * (c.h + 2)) return;
+    int64_t const y = g / P, x = g - y * P;
+    if (y == 0 || x == 0 || y > c.h || x > c.w) return;
+    int64_t const Pf = f.w + 2;
+    float4 sacc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            int64_t const fy = 2 * (y - 1) + a, fx = 2 * (x - 1) + b;  // interior coordinates
+            if (fy >= f.h || fx >= f.w) continue;
+            float4 const d = *reinterpret_cast<float4 const*>(dx + (f.offset + (fy + 1) * Pf + fx + 1) * kCh + ch);
+            sacc.x = sacc.x + d.x;
+            sacc.y = sacc.y + d.y;
+            sacc.z = sacc.z + d.z;
+            sacc.w = sacc.w + d.w;
+        }
+    float4* o = reinterpret_cast<float4*>(dcoarse + (c.offset + g) * kCh + ch);
+    float4 v = *o;
+    v.x = v.x + sacc.x;
+    v.y = v.y + sacc.y;
+    v.z = v.z + sacc.z;
+    v.w = v.w + sacc.w;
+    *o = v;
+}
+
+// ------------------------------------------------------------------ node-level wrapper (FP32)
+
+struct Samples
+{
+    int n;
+    Sample s[kMaxImages];
+    Img top[kMaxImages];   // level-0 network image of each sample
+};
+
+__device__ __forceinline__ bool node_of(Samples const& ss, int64_t& row, Sample& sm)
+{
+    sm = ss.s[blockIdx.y];
+    row = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    return row < static_cast<int64_t>(sm.nx) * sm.ny;
+}
+
+// dinv = 1 / diag(K) (identity on the boundary); nu given per node.
+__global__ void dinv_kernel(const __grid_constant__ Samples ss, float const* nu, float* dinv)
+{
+    int64_t row;
+    Sample sm;
+    if (!node_of(ss, row, sm)) return;
+    int64_t const nx = sm.nx, ny = sm.ny;
+    int64_t const i = row % nx, j = row / nx;
+    float const* v = nu + sm.offset;
+    float d = 1.0f;
+    if (!(i == 0 || j == 0 || i + 1 == nx || j + 1 == ny)) {
+        d = 0.0f;
+        if (j >= 2) d = d + v[row - nx];
+        d = d + v[row];
+        if (i >= 2) d = d + v[row - 1];
+        d = d + v[row];
+    }
+    dinv[sm.offset + row] = 1.0f / d;
+}
+
+// y = alpha * x + beta * dinv (b - K e)   with optional K e: general Jacobi-type update
+// out = base + w * dinv * (b - K e)
+__global__ void jacobi_kernel(const __grid_constant__ Samples ss, float const* nu, float const* dinv, float const* b,
+                              float const* e, float const* base, float w, float* out)
+{
+    int64_t row;
+    Sample sm;
+    if (!node_of(ss, row, sm)) return;
+    int64_t const o = sm.offset;
+    float const ke = e != nullptr ? mag_apply_node(e + o, nu + o, sm.nx, sm.ny, row) : 0.0f;
+    float const r = b[o + row] - ke;
+    float const bv = base != nullptr ? base[o + row] : 0.0f;
+    out[o + row] = bv + w * (dinv[o + row] * r);
+}
+
+// out = b - K e
+__global__ void residual_kernel(const __grid_constant__ Samples ss, float const* nu, float const* b, float const* e,
+                                float* out)
+{
+    int64_t row;
+    Sample sm;
+    if (!node_of(ss, row, sm)) return;
+    int64_t const o = sm.offset;
+    out[o + row] = b[o + row] - mag_apply_node(e + o, nu + o, sm.nx, sm.ny, row);
+}
+
+// out = K e
+__global__ void kapply_kernel(const __grid_constant__ Samples ss, float const* nu, float const* e, float* out)
+{
+    int64_t row;
+    Sample sm;
+    if (!node_of(ss, row, sm)) return;
+    int64_t const o = sm.offset;
+    out[o + row] = mag_apply_node(e + o, nu + o, sm.nx, sm.ny, row);
+}
+
+constexpr int kDotBlock = 256;
+
+// Per-sample partial sums of up to three products a1.b1, a2.b2, a3.b3 (FP64).
+__global__ void dots_kernel(const __grid_constant__ Samples ss, float const* a1, float const* b1, float const* a2,
+                            float const* b2, float const* a3, float const* b3, double* part, int nblocks_x)
+{
+    __shared__ double red[3][kDotBlock / 32];
+    Sample const sm = ss.s[blockIdx.y];
+    int64_t const n = static_cast<int64_t>(sm.nx) * sm.ny;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int64_t row = static_cast<int64_t>(blockIdx.x) * kDotBlock + threadIdx.x; row < n;
+         row += static_cast<int64_t>(nblocks_x) * kDotBlock) {
+        int64_t const q = sm.offset + row;
+        acc[0] += static_cast<double>(a1[q]) * static_cast<double>(b1[q]);
+        if (a2 != nullptr) acc[1] += static_cast<double>(a2[q]) * static_cast<double>(b2[q]);
+        if (a3 != nullptr) acc[2] += static_cast<double>(a3[q]) * static_cast<double>(b3[q]);
+    }
+    for (int k = 0; k < 3; ++k) {
+        double v = acc[k];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 0.0;
+        for (int w = 0; w < kDotBlock / 32; ++w) v += red[threadIdx.x][w];
+        part[(static_cast<int64_t>(blockIdx.y) * nblocks_x + blockIdx.x) * 3 + threadIdx.x] = v;
+    }
+}
+
+// dots[s][k] = sum over blocks (fixed order).
+__global__ void dots_finish_kernel(double const* part, int nsamples, int nblocks_x, double* dots)
+{
+    int const i = threadIdx.x;
+    if (i >= nsamples * 3) return;
+    int const s = i / 3, k = i % 3;
+    double v = 0.0;
+    for (int b = 0; b < nblocks_x; ++b) v += part[(static_cast<int64_t>(s) * nblocks_x + b) * 3 + k];
+    dots[i] = v;
+}
+
+// Feature image of the network's top level: 2x2 average of [r1 / s, log(nu)/log(1000)]
+// over the nodes of each half-resolution pixel (nodes outside the grid count as zero).
+__global__ void features_kernel(const __grid_constant__ Samples ss, float const* r1, float const* nu,
+                                double const* dots, float* feat)
+{
+    int const sidx = blockIdx.y;
+    Sample const sm = ss.s[sidx];
+    Img const o = ss.top[sidx];
+    int64_t const P = o.w + 2, npx = P * (o.h + 2);
+    int64_t const g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= npx) return;
+    int64_t const y = g / P, x = g - y * P;
+    float f0 = 0.0f, f1 = 0.0f;
+    if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
+        double const n = static_cast<double>(sm.nx) * sm.ny;
+        double const ms = dots[sidx * 3] / n;
+        float const inv_s = ms > 0.0 ? static_cast<float>(1.0 / sqrt(ms)) : 0.0f;
+        float const inv_l = static_cast<float>(1.0 / log(1000.0));
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                int64_t const j = 2 * (y - 1) + a, i = 2 * (x - 1) + b;
+                if (j >= sm.ny || i >= sm.nx) continue;
+                int64_t const q = sm.offset + j * sm.nx + i;
+                f0 = f0 + r1[q] * inv_s;
+                f1 = f1 + logf(nu[q]) * inv_l;
+            }
+        f0 = f0 * 0.25f;
+        f1 = f1 * 0.25f;
+    }
+    feat[2 * (o.offset + g)] = f0;
+    feat[2 * (o.offset + g) + 1] = f1;
+}
+
+// e2 = e1 + s * up(u_net), zero on the Dirichlet boundary.
+__global__ void correction_kernel(const __grid_constant__ Samples ss, float const* e1, float const* unet,
+                                  double const* dots, float* e2)
+{
+    int64_t row;
+    Sample sm;
+    if (!node_of(ss, row, sm)) return;
+    Img const o = ss.top[blockIdx.y];
+    int64_t const nx = sm.nx, ny = sm.ny;
+    int64_t const i = row % nx, j = row / nx;
+    float v = 0.0f;
+    if (!(i == 0 || j == 0 || i + 1 == nx || j + 1 == ny)) {
+        double const ms = dots[blockIdx.y * 3] / (static_cast<double>(nx) * ny);
+        float const s = static_cast<float>(sqrt(ms));
+        v = s * unet[o.offset + (j / 2 + 1) * (o.w + 2) + (i / 2 + 1)];
+    }
+    e2[sm.offset + row] = e1[sm.offset + row] + v;
+}
+
+// Gradient of the loss with respect to u:
+// g = -(2 ub uKu b - 2 ub^2 Ku) / (uKu^2 xb) / nsamples.
+__global__ void loss_grad_u_kernel(const __grid_constant__ Samples ss, float const* b, float const* ku,
+                                   double const* dots_u, double const* dots_x, float* gu)
+{
+    int64_t row;
+    Sample sm;
+    if (!node_of(ss, row, sm)) return;
+    double const ub = dots_u[blockIdx.y * 3], uku = dots_u[blockIdx.y * 3 + 1], xb = dots_x[blockIdx.y * 3];
+    double const den = uku * uku * xb * ss.n;
+    double const cb = den > 0 ? -2.0 * ub * uku / den : 0.0;
+    double const ck = den > 0 ? 2.0 * ub * ub / den : 0.0;
+    int64_t const q = sm.offset + row;
+    gu[q] = static_cast<float>(cb * b[q] + ck * ku[q]);
+}
+
+// g_net[top pixel] = s * sum over interior child nodes of g_e2.
+__global__ void net_grad_kernel(const __grid_constant__ Samples ss, float const* ge2, double const* dots, float* gnet)
+{
+    int const sidx = blockIdx.y;
+    Sample const sm = ss.s[sidx];
+    Img const o = ss.top[sidx];
+    int64_t const P = o.w + 2, npx = P * (o.h + 2);
+    int64_t const g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= npx) return;
+    int64_t const y = g / P, x = g - y * P;
+    float v = 0.0f;
+    if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
+        double const ms = dots[sidx * 3] / (static_cast<double>(sm.nx) * sm.ny);
+        float const s = static_cast<float>(sqrt(ms));
+        float acc = 0.0f;
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                int64_t const j = 2 * (y - 1) + a, i = 2 * (x - 1) + b;
+                if (j >= sm.ny || i >= sm.nx) continue;
+                if (i == 0 || j == 0 || i + 1 == sm.nx || j + 1 == sm.ny) continue;
+                acc = acc + ge2[sm.offset + j * sm.nx + i];
+            }
+        v = s * acc;
+    }
+    gnet[o.offset + g] = v;
+}
+
+// out = a x + b y
+__global__ void axpby_kernel(const __grid_constant__ Samples ss, float a, float const* x, float b, float const* y,
+                             float* out)
+{
+    int64_t row;
+    Sample sm;
+    if (!node_of(ss, row, sm)) return;
+    int64_t const q = sm.offset + row;
+    out[q] = a * x[q] + b * y[q];
+}
+
+__global__ void adam_kernel(float* p, float const* g, float* m, float* v, int n, float lr, float b1t, float b2t)
+{
+    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float const gi = g[i];
+    float const mi = 0.9f * m[i] + 0.1f * gi;
+    float const vi = 0.999f * v[i] + 0.001f * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    float const mh = mi / b1t, vh = vi / b2t;
+    p[i] = p[i] - lr * mh / (sqrtf(vh) + 1e-8f);
+}
+
+// ------------------------------------------------------------------ host side
+
+struct DevBuf
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { cudaFree(p); }
+    sil_status alloc(size_t b)
+    {
+        if (b <= bytes) return SIL_OK;
+        cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t const e = cudaMalloc(&p, std::max<size_t>(b, 256));
+        if (e != cudaSuccess) return cuda_fail(e, "precond workspace");
+        bytes = b;
+        return SIL_OK;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Geometry of one network level for the images that reach it.
+struct Level
+{
+    std::vector<int> images;       // sample indices present
+    std::vector<Img> img;          // per present image (same order)
+    int64_t npx = 0;               // padded pixels of the level buffer
+    int ntiles = 0;
+};
+
+class Workspace
+{
+public:
+    std::vector<Sample> samples;
+    int64_t nodes = 0;
+    std::vector<Level> levels;
+    std::vector<int> depth;        // levels per sample
+    Samples ss {};
+    // node-level FP32 vectors
+    DevBuf dinv, e1, r1, e2, u, ku, tmp, gu, ge2, fnu;
+    DevBuf dparts;                 // per-sample dot partials
+    DevBuf dots;                   // [3 sets][nsamples][3]
+    int dot_blocks = 0;
+    // network buffers per level
+    std::vector<DevBuf> h, p, g, dh, dg, dx;
+    DevBuf feat, unet, gnet;
+    DevBuf wparts;                 // weight-gradient partials
+    int wgrad_grid = 0;
+    int64_t max_node_per_sample = 0;
+
+    sil_status build(std::vector<Sample> const& s);
+    Table table(int level, int aux_level, bool aux_is_finer) const;
+};
+
+static int depth_of(int h, int w)
+{
+    int d = 1;
+    while (std::min(h, w) >= 16) {
+        h = (h + 1) / 2;
+        w = (w + 1) / 2;
+        ++d;
+    }
+    return d;
+}
+
+sil_status Workspace::build(std::vector<Sample> const& s)
+{
+    samples = s;
+    int const n = static_cast<int>(s.size());
+    if (n < 1 || n > kMaxImages) return fail(SIL_ERR_INVALID, "precond: 1 to 64 samples per batch");
+    nodes = 0;
+    max_node_per_sample = 0;
+    depth.assign(n, 0);
+    int maxd = 0;
+    ss = Samples {};
+    ss.n = n;
+    for (int i = 0; i < n; ++i) {
+        if (s[i].nx < 3 || s[i].ny < 3) return fail(SIL_ERR_INVALID, "precond: grids need at least 3x3 nodes");
+        ss.s[i] = s[i];
+        nodes = std::max<int64_t>(nodes, s[i].offset + static_cast<int64_t>(s[i].nx) * s[i].ny);
+        max_node_per_sample = std::max<int64_t>(max_node_per_sample, static_cast<int64_t>(s[i].nx) * s[i].ny);
+        depth[i] = depth_of((s[i].ny + 1) / 2, (s[i].nx + 1) / 2);
+        maxd = std::max(maxd, depth[i]);
+    }
+    levels.assign(maxd, Level {});
+    for (int l = 0; l < maxd; ++l) {
+        Level& L = levels[l];
+        for (int i = 0; i < n; ++i) {
+            if (depth[i] <= l) continue;
+            int hh = (s[i].ny + 1) / 2, ww = (s[i].nx + 1) / 2;
+            for (int k = 0; k < l; ++k) {
+                hh = (hh + 1) / 2;
+                ww = (ww + 1) / 2;
+            }
+            L.images.push_back(i);
+            L.img.push_back({hh, ww, L.npx});
+            L.npx += static_cast<int64_t>(hh + 2) * (ww + 2);
+            L.ntiles += static_cast<int>((static_cast<int64_t>(ww + 2) * hh + kTilePx - 1) / kTilePx);
+        }
+    }
+    for (int i = 0; i < n; ++i) ss.top[i] = levels[0].img[i];
+    size_t const nb = static_cast<size_t>(nodes) * sizeof(float);
+    for (DevBuf* b : {&dinv, &e1, &r1, &e2, &u, &ku, &tmp, &gu, &ge2, &fnu}) {
+        sil_status const st = b->alloc(nb);
+        if (st != SIL_OK) return st;
+    }
+    dot_blocks = static_cast<int>(std::min<int64_t>(64, (max_node_per_sample + kDotBlock - 1) / kDotBlock));
+    if (sil_status st = dparts.alloc(sizeof(double) * 3 * n * dot_blocks); st != SIL_OK) return st;
+    if (sil_status st = dots.alloc(sizeof(double) * 3 * 3 * n); st != SIL_OK) return st;
+    h.resize(maxd);
+    p.resize(maxd);
+    g.resize(maxd);
+    dh.resize(maxd);
+    dg.resize(maxd);
+    dx.resize(maxd);
+    // Every level buffer starts zeroed: no kernel writes the top and bottom
+    // border rows of an image, which must read as zero.
+    for (int l = 0; l < maxd; ++l) {
+        size_t const a = static_cast<size_t>(levels[l].npx) * kCh;
+        for (DevBuf* b : {&h[l], &p[l], &g[l]}) {
+            if (sil_status st = b->alloc(a * sizeof(bf16)); st != SIL_OK) return st;
+            SIL_CUDA_CHECK(cudaMemset(b->p, 0, a * sizeof(bf16)));
+        }
+        for (DevBuf* b : {&dh[l], &dg[l], &dx[l]}) {
+            if (sil_status st = b->alloc(a * sizeof(float)); st != SIL_OK) return st;
+            SIL_CUDA_CHECK(cudaMemset(b->p, 0, a * sizeof(float)));
+        }
+    }
+    int64_t const top = levels[0].npx;
+    if (sil_status st = feat.alloc(top * 2 * sizeof(float)); st != SIL_OK) return st;
+    if (sil_status st = unet.alloc(top * sizeof(float)); st != SIL_OK) return st;
+    if (sil_status st = gnet.alloc(top * sizeof(float)); st != SIL_OK) return st;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    wgrad_grid = 2 * sms;
+    int64_t const thin_blocks = (top + kThinPx - 1) / kThinPx;
+    size_t const wp = std::max<size_t>(static_cast<size_t>(wgrad_grid) * kWgradParts,
+                                       static_cast<size_t>(thin_blocks) * (kInW + kCh));
+    if (sil_status st = wparts.alloc(wp * sizeof(float)); st != SIL_OK) return st;
+    return SIL_OK;
+}
+
+// Table of `level`; aux entries describe the same images at aux_level.
+Table Workspace::table(int level, int aux_level, bool) const
+{
+    Table t {};
+    Level const& L = levels[level];
+    t.nimg = static_cast<int>(L.images.size());
+    t.tile_base[0] = 0;
+    for (int k = 0; k < t.nimg; ++k) {
+        t.img[k] = L.img[k];
+        int64_t const tiles = (static_cast<int64_t>(L.img[k].w + 2) * L.img[k].h + kTilePx - 1) / kTilePx;
+        t.tile_base[k + 1] = t.tile_base[k] + static_cast<int32_t>(tiles);
+        if (aux_level >= 0) {
+            Level const& A = levels[aux_level];
+            int const sidx = L.images[k];
+            auto it = std::find(A.images.begin(), A.images.end(), sidx);
+            t.aux[k] = it != A.images.end() ? A.img[it - A.images.begin()] : Img {0, 0, 0};
+        }
+    }
+    return t;
+}
+
+namespace {
+
+size_t conv_smem() { return sizeof(ConvSmem) + 1024; }
+size_t wgrad_smem() { return sizeof(WgradSmem) + 1024; }
+
+bool g_attr_done = false;
+
+sil_status ensure_attributes()
+{
+    if (g_attr_done) return SIL_OK;
+    SIL_CUDA_CHECK(cudaFuncSetAttribute(conv3x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(conv_smem())));
+    SIL_CUDA_CHECK(cudaFuncSetAttribute(wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(wgrad_smem())));
+    g_attr_done = true;
+    return SIL_OK;
+}
+
+int conv_grid(int ntiles)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, std::min(ntiles, 4 * sms));
+}
+
+// 1024-byte aligned dynamic shared memory: the kernels index from the start
+// of the dynamic block, which the runtime aligns to at least 1024 bytes when
+// the kernel declares it so.
+sil_status launch_conv(cudaStream_t st, Table const& t, int mode, bf16 const* in, bf16 const* in2, float const* gin,
+                       bf16 const* w, float const* bias, int relu, bf16* out, float* out_f32, int accumulate,
+                       int* err)
+{
+    if (t.nimg == 0 || t.tile_base[t.nimg] == 0) return SIL_OK;
+    conv3x3_kernel<<<conv_grid(t.tile_base[t.nimg]), 128, conv_smem(), st>>>(t, mode, in, in2, gin, w, bias, relu, out,
+                                                                             out_f32, accumulate, err);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+template <class K>
+dim3 image_grid(Table const& t, int per_px, K)
+{
+    int64_t maxpx = 0;
+    for (int k = 0; k < t.nimg; ++k) maxpx = std::max<int64_t>(maxpx, static_cast<int64_t>(t.img[k].h + 2) * (t.img[k].w + 2));
+    return dim3(static_cast<unsigned>((maxpx * per_px + 255) / 256), static_cast<unsigned>(t.nimg));
+}
+
+} // namespace
+
+Net::Net() = default;
+
+Net::~Net()
+{
+    cudaFree(params);
+    cudaFree(grad);
+    cudaFree(adam_m);
+    cudaFree(adam_v);
+    cudaFree(wbf);
+    cudaFree(wbf_t);
+    cudaFree(error_flag);
+}
+
+sil_status Net::init(uint64_t seed, cudaStream_t stream)
+{
+    if (params == nullptr) {
+        SIL_CUDA_CHECK(cudaMalloc(&params, sizeof(float) * kNumParams));
+        SIL_CUDA_CHECK(cudaMalloc(&grad, sizeof(float) * kNumParams));
+        SIL_CUDA_CHECK(cudaMalloc(&adam_m, sizeof(float) * kNumParams));
+        SIL_CUDA_CHECK(cudaMalloc(&adam_v, sizeof(float) * kNumParams));
+        SIL_CUDA_CHECK(cudaMalloc(&wbf, sizeof(bf16) * kNumBig * kBigW));
+        SIL_CUDA_CHECK(cudaMalloc(&wbf_t, sizeof(bf16) * kNumBig * kBigW));
+        SIL_CUDA_CHECK(cudaMalloc(&error_flag, sizeof(int)));
+        SIL_CUDA_CHECK(cudaMemsetAsync(error_flag, 0, sizeof(int), stream));
+    }
+    // He-normal weights, zero biases (host RNG, reproducible per seed).
+    std::vector<float> h(kNumParams, 0.0f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int off, int count, int fan_in) {
+        std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / static_cast<float>(fan_in)));
+        for (int i = 0; i < count; ++i) h[off + i] = nd(rng);
+    };
+    fill(kOffIn, kInW, kTaps * 2);
+    for (int j = 0; j < kNumBig; ++j) fill(kOffBig + j * kBigParams, kBigW, kTaps * kCh);
+    fill(kOffOut, kOutW, kTaps * kCh);
+    for (int i = 0; i < kOutW; ++i) h[kOffOut + i] *= 0.5f;
+    return set_params(h.data(), stream);
+}
+
+sil_status Net::set_params(float const* host, cudaStream_t stream)
+{
+    if (params == nullptr) {
+        sil_status const st = init(0, stream);
+        if (st != SIL_OK) return st;
+    }
+    SIL_CUDA_CHECK(cudaMemcpyAsync(params, host, sizeof(float) * kNumParams, cudaMemcpyHostToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemsetAsync(adam_m, 0, sizeof(float) * kNumParams, stream));
+    SIL_CUDA_CHECK(cudaMemsetAsync(adam_v, 0, sizeof(float) * kNumParams, stream));
+    adam_t = 0;
+    return refresh(stream);
+}
+
+sil_status Net::get_params(float* host, cudaStream_t stream)
+{
+    SIL_CUDA_CHECK(cudaMemcpyAsync(host, params, sizeof(float) * kNumParams, cudaMemcpyDeviceToHost, stream));
+    SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+    return SIL_OK;
+}
+
+sil_status Net::refresh(cudaStream_t stream)
+{
+    int const n = kNumBig * kBigW;
+    convert_weights_kernel<<<(n + 255) / 256, 256, 0, stream>>>(params, static_cast<bf16*>(wbf), static_cast<bf16*>(wbf_t));
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+Workspace* Net::workspace(std::vector<Sample> const& samples, cudaStream_t stream, sil_status* st)
+{
+    (void)stream;
+    for (auto& w : cache_) {
+        if (w->samples.size() != samples.size()) continue;
+        bool same = true;
+        for (size_t i = 0; i < samples.size() && same; ++i)
+            same = w->samples[i].nx == samples[i].nx && w->samples[i].ny == samples[i].ny
+                   && w->samples[i].offset == samples[i].offset;
+        if (same) {
+            *st = SIL_OK;
+            return w.get();
+        }
+    }
+    if (cache_.size() >= 4) cache_.erase(cache_.begin());
+    auto w = std::make_unique<Workspace>();
+    *st = w->build(samples);
+    if (*st != SIL_OK) return nullptr;
+    cache_.push_back(std::move(w));
+    return cache_.back().get();
+}
+
+namespace {
+
+bf16 const* big_w(Net const& net, int kind, int wl) { return static_cast<bf16 const*>(net.wbf) + big_index(kind, wl) * kBigW; }
+bf16 const* big_wt(Net const& net, int kind, int wl) { return static_cast<bf16 const*>(net.wbf_t) + big_index(kind, wl) * kBigW; }
+float const* big_b(Net const& net, int kind, int wl) { return net.params + kOffBig + big_index(kind, wl) * kBigParams + kBigW; }
+float* big_grad(Net& net, int kind, int wl) { return net.grad + kOffBig + big_index(kind, wl) * kBigParams; }
+int weight_level_enc(int l) { return std::min(l - 1, 2); }   // encoder convs of level l >= 1
+int weight_level_dec(int l) { return std::min(l, 2); }       // decoder conv producing level l
+
+dim3 node_grid(Workspace const& w)
+{
+    return dim3(static_cast<unsigned>((w.max_node_per_sample + 255) / 256), static_cast<unsigned>(w.samples.size()));
+}
+
+dim3 top_grid(Workspace const& w)
+{
+    int64_t m = 0;
+    for (Img const& i : w.levels[0].img) m = std::max<int64_t>(m, static_cast<int64_t>(i.h + 2) * (i.w + 2));
+    return dim3(static_cast<unsigned>((m + 255) / 256), static_cast<unsigned>(w.samples.size()));
+}
+
+sil_status dots(Workspace& w, cudaStream_t st, int set, float const* a1, float const* b1, float const* a2,
+                float const* b2, float const* a3, float const* b3)
+{
+    int const n = static_cast<int>(w.samples.size());
+    dots_kernel<<<dim3(w.dot_blocks, n), kDotBlock, 0, st>>>(w.ss, a1, b1, a2, b2, a3, b3, w.dparts.as<double>(),
+                                                             w.dot_blocks);
+    dots_finish_kernel<<<1, std::max(32, ((3 * n + 31) / 32) * 32), 0, st>>>(w.dparts.as<double>(), n, w.dot_blocks,
+                                                                            w.dots.as<double>() + set * 3 * n);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+// Network forward on the feature image in w.feat; result in w.unet.
+sil_status net_forward(Net& net, Workspace& w, cudaStream_t st)
+{
+    int const D = static_cast<int>(w.levels.size());
+    int* err = net.error_flag;
+    {
+        Table const t = w.table(0, -1, false);
+        inc_forward_kernel<<<image_grid(t, 1, 0), 256, 0, st>>>(t, w.feat.as<float>(), net.params, w.h[0].as<bf16>());
+        SIL_CUDA_CHECK(cudaGetLastError());
+    }
+    for (int l = 1; l < D; ++l) {
+        int const wl = weight_level_enc(l);
+        Table const t = w.table(l, l - 1, true);
+        sil_status s = launch_conv(st, t, kPool, w.h[l - 1].as<bf16>(), nullptr, nullptr, big_w(net, kDown, wl),
+                                   big_b(net, kDown, wl), 1, w.p[l].as<bf16>(), nullptr, 0, err);
+        if (s != SIL_OK) return s;
+        Table const t2 = w.table(l, -1, false);
+        s = launch_conv(st, t2, kPlain, w.p[l].as<bf16>(), nullptr, nullptr, big_w(net, kEnc, wl), big_b(net, kEnc, wl),
+                        1, w.h[l].as<bf16>(), nullptr, 0, err);
+        if (s != SIL_OK) return s;
+    }
+    // g at each image's deepest level is its h.
+    for (size_t i = 0; i < w.samples.size(); ++i) {
+        int const l = w.depth[i] - 1;
+        Level const& L = w.levels[l];
+        int const k = static_cast<int>(std::find(L.images.begin(), L.images.end(), static_cast<int>(i)) - L.images.begin());
+        int64_t const px = static_cast<int64_t>(L.img[k].h + 2) * (L.img[k].w + 2);
+        SIL_CUDA_CHECK(cudaMemcpyAsync(w.g[l].as<bf16>() + L.img[k].offset * kCh, w.h[l].as<bf16>() + L.img[k].offset * kCh,
+                                       px * kCh * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
+    }
+    for (int l = D - 2; l >= 0; --l) {
+        int const wl = weight_level_dec(l);
+        // images at level l that also have level l+1
+        Table t = w.table(l, l + 1, false);
+        Table tt {};
+        tt.nimg = 0;
+        tt.tile_base[0] = 0;
+        for (int k = 0; k < t.nimg; ++k) {
+            if (t.aux[k].h == 0) continue;
+            int const q = tt.nimg++;
+            tt.img[q] = t.img[k];
+            tt.aux[q] = t.aux[k];
+            tt.tile_base[q + 1] = tt.tile_base[q] + (t.tile_base[k + 1] - t.tile_base[k]);
+        }
+        sil_status const s = launch_conv(st, tt, kUpAdd, w.h[l].as<bf16>(), w.g[l + 1].as<bf16>(), nullptr,
+                                         big_w(net, kDec, wl), big_b(net, kDec, wl), 1, w.g[l].as<bf16>(), nullptr, 0, err);
+        if (s != SIL_OK) return s;
+    }
+    {
+        Table const t = w.table(0, -1, false);
+        out_forward_kernel<<<image_grid(t, 1, 0), 256, 0, st>>>(t, w.g[0].as<bf16>(), net.params, w.unet.as<float>());
+        SIL_CUDA_CHECK(cudaGetLastError());
+    }
+    return SIL_OK;
+}
+
+// Images of level l that have level l+1 (the decoder's images).
+Table dec_table(Workspace const& w, int l)
+{
+    Table t = w.table(l, l + 1, false);
+    Table tt {};
+    tt.tile_base[0] = 0;
+    for (int k = 0; k < t.nimg; ++k) {
+        if (t.aux[k].h == 0) continue;
+        int const q = tt.nimg++;
+        tt.img[q] = t.img[k];
+        tt.aux[q] = t.aux[k];
+        tt.tile_base[q + 1] = tt.tile_base[q] + (t.tile_base[k + 1] - t.tile_base[k]);
+    }
+    return tt;
+}
+
+sil_status wgrad(Net& net, Workspace& w, cudaStream_t st, Table const& t, int mode, bf16 const* in, bf16 const* in2,
+                 float const* dy, bf16 const* y, float* grad_out)
+{
+    if (t.nimg == 0 || t.tile_base[t.nimg] == 0) return SIL_OK;
+    int const grid = std::min(w.wgrad_grid, t.tile_base[t.nimg]);
+    wgrad_kernel<<<grid, 128, wgrad_smem(), st>>>(t, mode, in, in2, dy, y, w.wparts.as<float>(), net.error_flag);
+    reduce_parts_kernel<<<(kWgradParts + 255) / 256, 256, 0, st>>>(w.wparts.as<float>(), grid, kWgradParts, grad_out);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+// Network backward from the gradient in w.gnet: accumulates into net.grad.
+sil_status net_backward(Net& net, Workspace& w, cudaStream_t st)
+{
+    int const D = static_cast<int>(w.levels.size());
+    int* err = net.error_flag;
+    for (int l = 0; l < D; ++l) {
+        size_t const a = static_cast<size_t>(w.levels[l].npx) * kCh * sizeof(float);
+        SIL_CUDA_CHECK(cudaMemsetAsync(w.dh[l].p, 0, a, st));
+        SIL_CUDA_CHECK(cudaMemsetAsync(w.dg[l].p, 0, a, st));
+    }
+    Table const t0 = w.table(0, -1, false);
+    int64_t const top = w.levels[0].npx;
+    int const thin_blocks = static_cast<int>((top + kThinPx - 1) / kThinPx);
+    // output convolution
+    out_backward_data_kernel<<<image_grid(t0, 1, 0), 256, 0, st>>>(t0, w.gnet.as<float>(), net.params, w.dg[0].as<float>());
+    out_wgrad_kernel<<<thin_blocks, kThinBlock, 0, st>>>(t0, w.gnet.as<float>(), w.g[0].as<bf16>(), w.wparts.as<float>(), top);
+    reduce_parts_kernel<<<(kOutW + 1 + 255) / 256, 256, 0, st>>>(w.wparts.as<float>(), thin_blocks, kOutW + 1,
+                                                                 net.grad + kOffOut);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    // decoder, top-down
+    for (int l = 0; l <= D - 2; ++l) {
+        int const wl = weight_level_dec(l);
+        Table const t = dec_table(w, l);
+        if (t.nimg == 0) continue;
+        sil_status s = wgrad(net, w, st, t, kUpAdd, w.h[l].as<bf16>(), w.g[l + 1].as<bf16>(), w.dg[l].as<float>(),
+                             w.g[l].as<bf16>(), big_grad(net, kDec, wl));
+        if (s != SIL_OK) return s;
+        s = launch_conv(st, t, kMasked, w.g[l].as<bf16>(), w.g[l].as<bf16>(), w.dg[l].as<float>(), big_wt(net, kDec, wl),
+                        nullptr, 0, nullptr, w.dx[l].as<float>(), 0, err);
+        if (s != SIL_OK) return s;
+        upadd_adjoint_skip_kernel<<<image_grid(t, 8, 0), 256, 0, st>>>(t, w.dx[l].as<float>(), w.dh[l].as<float>());
+        // coarse part: table over level l+1 with aux = level l
+        Table tc {};
+        tc.nimg = t.nimg;
+        for (int k = 0; k < t.nimg; ++k) {
+            tc.img[k] = t.aux[k];
+            tc.aux[k] = t.img[k];
+        }
+        upadd_adjoint_coarse_kernel<<<image_grid(tc, 8, 0), 256, 0, st>>>(tc, w.dx[l].as<float>(), w.dg[l + 1].as<float>());
+        SIL_CUDA_CHECK(cudaGetLastError());
+    }
+    // deepest level of each image: g = h
+    for (size_t i = 0; i < w.samples.size(); ++i) {
+        int const l = w.depth[i] - 1;
+        Level const& L = w.levels[l];
+        int const k = static_cast<int>(std::find(L.images.begin(), L.images.end(), static_cast<int>(i)) - L.images.begin());
+        Table t {};
+        t.nimg = 1;
+        t.img[0] = L.img[k];
+        t.aux[0] = L.img[k];
+        // dh += dg over this image (reuse the skip adjoint kernel)
+        upadd_adjoint_skip_kernel<<<image_grid(t, 8, 0), 256, 0, st>>>(t, w.dg[l].as<float>(), w.dh[l].as<float>());
+        SIL_CUDA_CHECK(cudaGetLastError());
+    }
+    // encoder, bottom-up
+    for (int l = D - 1; l >= 1; --l) {
+        int const wl = weight_level_enc(l);
+        Table const t = w.table(l, -1, false);
+        sil_status s = wgrad(net, w, st, t, kPlain, w.p[l].as<bf16>(), nullptr, w.dh[l].as<float>(), w.h[l].as<bf16>(),
+                             big_grad(net, kEnc, wl));
+        if (s != SIL_OK) return s;
+        s = launch_conv(st, t, kMasked, w.h[l].as<bf16>(), w.h[l].as<bf16>(), w.dh[l].as<float>(), big_wt(net, kEnc, wl),
+                        nullptr, 0, nullptr, w.dx[l].as<float>(), 0, err);
+        if (s != SIL_OK) return s;
+        Table const tp = w.table(l, l - 1, true);
+        s = wgrad(net, w, st, tp, kPool, w.h[l - 1].as<bf16>(), nullptr, w.dx[l].as<float>(), w.p[l].as<bf16>(),
+                  big_grad(net, kDown, wl));
+        if (s != SIL_OK) return s;
+        // data gradient of the down convolution into dg[l] (scratch), then pool adjoint into dh[l-1]
+        s = launch_conv(st, t, kMasked, w.p[l].as<bf16>(), w.p[l].as<bf16>(), w.dx[l].as<float>(),
+                        big_wt(net, kDown, wl), nullptr, 0, nullptr, w.dg[l].as<float>(), 0, err);
+        if (s != SIL_OK) return s;
+        Table tf {};
+        tf.nimg = tp.nimg;
+        for (int k = 0; k < tp.nimg; ++k) {
+            tf.img[k] = tp.aux[k];   // fine level l-1
+            tf.aux[k] = tp.img[k];   // coarse level l
+        }
+        pool_adjoint_kernel<<<image_grid(tf, 8, 0), 256, 0, st>>>(tf, w.dg[l].as<float>(), w.dh[l - 1].as<float>());
+        SIL_CUDA_CHECK(cudaGetLastError());
+    }
+    // input convolution
+    inc_wgrad_kernel<<<thin_blocks, kThinBlock, 0, st>>>(t0, w.dh[0].as<float>(), w.h[0].as<bf16>(), w.feat.as<float>(),
+                                                         w.wparts.as<float>(), top);
+    reduce_parts_kernel<<<(kInW + kCh + 255) / 256, 256, 0, st>>>(w.wparts.as<float>(), thin_blocks, kInW + kCh,
+                                                                  net.grad + kOffIn);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+// Preconditioner forward: w.u = M(b).  nu is read from w.fnu.
+sil_status precond_forward(Net& net, Workspace& w, float const* b, cudaStream_t st)
+{
+    dim3 const ng = node_grid(w);
+    float const* nu = w.fnu.as<float>();
+    dinv_kernel<<<ng, 256, 0, st>>>(w.ss, nu, w.dinv.as<float>());
+    jacobi_kernel<<<ng, 256, 0, st>>>(w.ss, nu, w.dinv.as<float>(), b, nullptr, nullptr, kOmega, w.e1.as<float>());
+    residual_kernel<<<ng, 256, 0, st>>>(w.ss, nu, b, w.e1.as<float>(), w.r1.as<float>());
+    SIL_CUDA_CHECK(cudaGetLastError());
+    sil_status s = dots(w, st, 0, w.r1.as<float>(), w.r1.as<float>(), nullptr, nullptr, nullptr, nullptr);
+    if (s != SIL_OK) return s;
+    features_kernel<<<top_grid(w), 256, 0, st>>>(w.ss, w.r1.as<float>(), nu, w.dots.as<double>(), w.feat.as<float>());
+    SIL_CUDA_CHECK(cudaGetLastError());
+    s = net_forward(net, w, st);
+    if (s != SIL_OK) return s;
+    correction_kernel<<<ng, 256, 0, st>>>(w.ss, w.e1.as<float>(), w.unet.as<float>(), w.dots.as<double>(), w.e2.as<float>());
+    jacobi_kernel<<<ng, 256, 0, st>>>(w.ss, nu, w.dinv.as<float>(), b, w.e2.as<float>(), w.e2.as<float>(), kOmega,
+                                      w.u.as<float>());
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+sil_status check_samples(std::vector<Sample> const& samples)
+{
+    if (samples.empty() || samples.size() > kMaxImages) return fail(SIL_ERR_INVALID, "precond: 1 to 64 samples per batch");
+    for (Sample const& s : samples)
+        if (s.nx < 3 || s.ny < 3 || s.offset < 0) return fail(SIL_ERR_INVALID, "precond: bad sample geometry");
+    return SIL_OK;
+}
+
+} // namespace
+
+sil_status Net::apply(std::vector<Sample> const& samples, float const* nu, float const* r, float* out, cudaStream_t stream)
+{
+    if (sil_status s = check_samples(samples); s != SIL_OK) return s;
+    if (sil_status s = ensure_attributes(); s != SIL_OK) return s;
+    sil_status st = SIL_OK;
+    Workspace* w = workspace(samples, stream, &st);
+    if (w == nullptr) return st;
+    SIL_CUDA_CHECK(cudaMemcpyAsync(w->fnu.p, nu, sizeof(float) * w->nodes, cudaMemcpyDeviceToDevice, stream));
+    st = precond_forward(*this, *w, r, stream);
+    if (st != SIL_OK) return st;
+    SIL_CUDA_CHECK(cudaMemcpyAsync(out, w->u.p, sizeof(float) * w->nodes, cudaMemcpyDeviceToDevice, stream));
+    return SIL_OK;
+}
+
+sil_status Net::loss_grad(std::vector<Sample> const& samples, float const* nu, float const* b, float const* x,
+                          double* loss, std::vector<double>* per_sample, cudaStream_t stream)
+{
+    if (sil_status s = check_samples(samples); s != SIL_OK) return s;
+    if (sil_status s = ensure_attributes(); s != SIL_OK) return s;
+    sil_status st = SIL_OK;
+    Workspace* w = workspace(samples, stream, &st);
+    if (w == nullptr) return st;
+    int const n = static_cast<int>(samples.size());
+    SIL_CUDA_CHECK(cudaMemcpyAsync(w->fnu.p, nu, sizeof(float) * w->nodes, cudaMemcpyDeviceToDevice, stream));
+    SIL_CUDA_CHECK(cudaMemsetAsync(grad, 0, sizeof(float) * kNumParams, stream));
+    st = precond_forward(*this, *w, b, stream);
+    if (st != SIL_OK) return st;
+    dim3 const ng = node_grid(*w);
+    float const* fnu = w->fnu.as<float>();
+    kapply_kernel<<<ng, 256, 0, stream>>>(w->ss, fnu, w->u.as<float>(), w->ku.as<float>());
+    SIL_CUDA_CHECK(cudaGetLastError());
+    // set 1: u.b, u.Ku ; set 2: x.b
+    if (sil_status s = dots(*w, stream, 1, w->u.as<float>(), b, w->u.as<float>(), w->ku.as<float>(), nullptr, nullptr);
+        s != SIL_OK)
+        return s;
+    if (sil_status s = dots(*w, stream, 2, x, b, nullptr, nullptr, nullptr, nullptr); s != SIL_OK) return s;
+    double const* d = w->dots.as<double>();
+    loss_grad_u_kernel<<<ng, 256, 0, stream>>>(w->ss, b, w->ku.as<float>(), d + 3 * n, d + 6 * n, w->gu.as<float>());
+    // g_e2 = g_u - w K (dinv g_u)
+    jacobi_kernel<<<ng, 256, 0, stream>>>(w->ss, fnu, w->dinv.as<float>(), w->gu.as<float>(), nullptr, nullptr, 1.0f,
+                                          w->tmp.as<float>());
+    kapply_kernel<<<ng, 256, 0, stream>>>(w->ss, fnu, w->tmp.as<float>(), w->ge2.as<float>());
+    axpby_kernel<<<ng, 256, 0, stream>>>(w->ss, 1.0f, w->gu.as<float>(), -kOmega, w->ge2.as<float>(), w->ge2.as<float>());
+    net_grad_kernel<<<top_grid(*w), 256, 0, stream>>>(w->ss, w->ge2.as<float>(), d, w->gnet.as<float>());
+    SIL_CUDA_CHECK(cudaGetLastError());
+    st = net_backward(*this, *w, stream);
+    if (st != SIL_OK) return st;
+    std::vector<double> hd(9 * n);
+    SIL_CUDA_CHECK(cudaMemcpyAsync(hd.data(), d, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, stream));
+    int herr = 0;
+    SIL_CUDA_CHECK(cudaMemcpyAsync(&herr, error_flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (herr != 0) return fail(SIL_ERR_BUDGET, "precond: a tensor-core wait ran out of its bound");
+    double total = 0.0;
+    if (per_sample != nullptr) per_sample->assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        double const ub = hd[3 * n + 3 * i], uku = hd[3 * n + 3 * i + 1], xb = hd[6 * n + 3 * i];
+        double const li = (uku > 0 && xb > 0) ? 1.0 - ub * ub / (uku * xb) : 1.0;
+        total += li;
+        if (per_sample != nullptr) (*per_sample)[i] = li;
+    }
+    *loss = total / n;
+    return SIL_OK;
+}
+
+sil_status Net::adam_step(float lr, cudaStream_t stream)
+{
+    ++adam_t;
+    float const b1t = 1.0f - std::pow(0.9f, static_cast<float>(adam_t));
+    float const b2t = 1.0f - std::pow(0.999f, static_cast<float>(adam_t));
+    adam_kernel<<<(kNumParams + 255) / 256, 256, 0, stream>>>(params, grad, adam_m, adam_v, kNumParams, lr, b1t, b2t);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return refresh(stream);
+}
+
+sil_status Net::debug_fetch(int which, int level, float* host, int64_t count, cudaStream_t stream)
+{
+    if (cache_.empty()) return fail(SIL_ERR_INVALID, "precond: no workspace yet");
+    Workspace& w = *cache_.back();
+    if (level < 0 || level >= static_cast<int>(w.levels.size())) return fail(SIL_ERR_INVALID, "precond: bad level");
+    int64_t const n = w.levels[level].npx * kCh;
+    std::vector<uint16_t> tmp;
+    auto get_bf = [&](DevBuf const& b) -> sil_status {
+        if (count < n) return fail(SIL_ERR_INVALID, "precond: host buffer too small");
+        tmp.resize(n);
+        SIL_CUDA_CHECK(cudaMemcpyAsync(tmp.data(), b.p, n * 2, cudaMemcpyDeviceToHost, stream));
+        SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+        for (int64_t i = 0; i < n; ++i) {
+            uint32_t const u = static_cast<uint32_t>(tmp[i]) << 16;
+            std::memcpy(host + i, &u, 4);
+        }
+        return SIL_OK;
+    };
+    auto get_f = [&](void const* p, int64_t m) -> sil_status {
+        if (count < m) return fail(SIL_ERR_INVALID, "precond: host buffer too small");
+        SIL_CUDA_CHECK(cudaMemcpyAsync(host, p, m * 4, cudaMemcpyDeviceToHost, stream));
+        SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+        return SIL_OK;
+    };
+    switch (which) {
+    case 0: return get_bf(w.h[level]);
+    case 1: return get_bf(w.p[level]);
+    case 2: return get_bf(w.g[level]);
+    case 3: return get_f(w.dh[level].p, n);
+    case 4: return get_f(w.dg[level].p, n);
+    case 5: return get_f(w.feat.p, w.levels[0].npx * 2);
+    case 6: return get_f(w.unet.p, w.levels[0].npx);
+    case 7: return get_f(w.u.p, w.nodes);
+    case 8: return get_f(w.gnet.p, w.levels[0].npx);
+    default: return fail(SIL_ERR_INVALID, "precond: unknown debug tensor");
+    }
+}
+
+} // namespace nn
+} // namespace sil
+
+// ------------------------------------------------------------------ C API
+
+using sil::nn::Sample;
+
+namespace {
+
+sil_status to_samples(sil_precond_sample const* in, int n, std::vector<Sample>* out)
+{
+    if (in == nullptr || n < 1 || n > sil::nn::kMaxImages) return sil::fail(SIL_ERR_INVALID, "precond: 1 to 64 samples");
+    out->resize(n);
+    for (int i = 0; i < n; ++i) (*out)[i] = {in[i].nx, in[i].ny, in[i].offset};
+    return SIL_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int64_t sil_precond_num_params(void) { return sil::nn::kNumParams; }
+
+sil_status sil_precond_create(sil_precond* out, uint64_t seed, sil_stream stream)
+{
+    if (out == nullptr) return sil::fail(SIL_ERR_INVALID, "sil_precond_create: NULL");
+    auto* p = new (std::nothrow) sil_precond_s;
+    if (p == nullptr) return sil::fail(SIL_ERR_ALLOC, "sil_precond_create");
+    sil_status const st = p->net.init(seed, static_cast<cudaStream_t>(stream));
+    if (st != SIL_OK) {
+        delete p;
+        return st;
+    }
+    *out = p;
+    return SIL_OK;
+}
+
+void sil_precond_destroy(sil_precond p) { delete p; }
+
+sil_status sil_precond_get_params(sil_precond p, float* host)
+{
+    if (p == nullptr || host == nullptr) return sil::fail(SIL_ERR_INVALID, "sil_precond_get_params: NULL");
+    return p->net.get_params(host, nullptr);
+}
+
+sil_status sil_precond_set_params(sil_precond p, const float* host, sil_stream stream)
+{
+    if (p == nullptr || host == nullptr) return sil::fail(SIL_ERR_INVALID, "sil_precond_set_params: NULL");
+    return p->net.set_params(host, static_cast<cudaStream_t>(stream));
+}
+
+sil_status sil_precond_apply(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
+                             const float* nu, const float* r, float* out)
+{
+    if (p == nullptr || nu == nullptr || r == nullptr || out == nullptr)
+        return sil::fail(SIL_ERR_INVALID, "sil_precond_apply: NULL");
+    std::vector<Sample> s;
+    if (sil_status st = to_samples(samples, n, &s); st != SIL_OK) return st;
+    return p->net.apply(s, nu, r, out, static_cast<cudaStream_t>(stream));
+}
+
+sil_status sil_precond_loss_grad(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
+                                 const float* nu, const float* b, const float* x, double* loss,
+                                 double* per_sample_loss, float* grad_host)
+{
+    if (p == nullptr || nu == nullptr || b == nullptr || x == nullptr || loss == nullptr)
+        return sil::fail(SIL_ERR_INVALID, "sil_precond_loss_grad: NULL");
+    std::vector<Sample> s;
+    if (sil_status st = to_samples(samples, n, &s); st != SIL_OK) return st;
+    std::vector<double> ps;
+    cudaStream_t const cs = static_cast<cudaStream_t>(stream);
+    sil_status st = p->net.loss_grad(s, nu, b, x, loss, &ps, cs);
+    if (st != SIL_OK) return st;
+    if (per_sample_loss != nullptr) std::copy(ps.begin(), ps.end(), per_sample_loss);
+    if (grad_host != nullptr) {
+        SIL_CUDA_CHECK(cudaMemcpyAsync(grad_host, p->net.grad, sizeof(float) * sil::nn::kNumParams,
+                                       cudaMemcpyDeviceToHost, cs));
+        SIL_CUDA_CHECK(cudaStreamSynchronize(cs));
+    }
+    return SIL_OK;
+}
+
+sil_status sil_precond_train_step(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
+                                  const float* nu, const float* b, const float* x, float learning_rate, double* loss)
+{
+    if (p == nullptr || nu == nullptr || b == nullptr || x == nullptr || loss == nullptr || !(learning_rate > 0.0f))
+        return sil::fail(SIL_ERR_INVALID, "sil_precond_train_step: bad argument");
+    std::vector<Sample> s;
+    if (sil_status st = to_samples(samples, n, &s); st != SIL_OK) return st;
+    cudaStream_t const cs = static_cast<cudaStream_t>(stream);
+    sil_status st = p->net.loss_grad(s, nu, b, x, loss, nullptr, cs);
+    if (st != SIL_OK) return st;
+    return p->net.adam_step(learning_rate, cs);
+}
+
+sil_status sil_precond_debug_fetch(sil_precond p, int which, int level, float* host, int64_t count)
+{
+    if (p == nullptr || host == nullptr) return sil::fail(SIL_ERR_INVALID, "sil_precond_debug_fetch: NULL");
+    return p->net.debug_fetch(which, level, host, count, nullptr);
+}
+
+} // extern "C"

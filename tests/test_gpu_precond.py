@@ -1,0 +1,107 @@
+"""GPU learned preconditioner: forward pass, loss and parameter gradients of
+the tensor-core network against the CPU oracle (BF16 storage emulated), and
+training on the GPU lowering the loss."""
+import numpy as np
+import pytest
+
+from oracle import precond_oracle as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+@pytest.fixture(scope="module")
+def pc():
+    import similie_b200.precond as m
+    return m
+
+
+def make_batch(shapes, seed, solution_noise=0.0):
+    import similie_b200.magnetostatics as mag
+    import oracle as O
+    rng = np.random.default_rng(seed)
+    out = []
+    for nx, ny in shapes:
+        n = max(nx, ny)
+        pr = mag.synthetic_problem(rng, n)
+        nu = (1.0 / pr.node_mu()).reshape(n, n)[:ny, :nx].copy()
+        b = pr.rhs().reshape(n, n)[:ny, :nx].copy()
+        b[0] = b[-1] = 0
+        b[:, 0] = b[:, -1] = 0
+        if not np.any(b):
+            b[ny // 2, nx // 2] = 1e-3
+        mu = 1.0 / nu
+        x, _, _ = O.mag2d_cg(nx, ny, mu.ravel(), b.ravel(), tol=1e-12)
+        out.append((nu, b, x.reshape(ny, nx)))
+    return out
+
+
+def flat(torch, arrs):
+    return torch.from_numpy(np.concatenate([a.ravel() for a in arrs]).astype(np.float32)).cuda()
+
+
+SHAPES = [(130, 130), (70, 50), (33, 41)]
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_forward_matches_oracle(torch, pc):
+    batch = make_batch(SHAPES, 3)
+    params = P.init_params(5)
+    net = pc.LearnedPreconditioner(seed=0)
+    net.set_params(params)
+    nu = flat(torch, [s[0] for s in batch])
+    r = flat(torch, [s[1] for s in batch])
+    out = torch.zeros_like(r)
+    net.apply(SHAPES, nu, r, out)
+    got = out.cpu().numpy()
+    off = 0
+    for (nx, ny), (nub, b, _) in zip(SHAPES, batch):
+        ref = P.precond(params, nub.astype(np.float32), b.astype(np.float32), emulate=True)
+        g = got[off:off + nx * ny].reshape(ny, nx)
+        off += nx * ny
+        assert rel(g, ref) < 2e-2, ((nx, ny), rel(g, ref))
+
+
+def test_gradient_matches_oracle(torch, pc):
+    batch = make_batch(SHAPES, 4)
+    params = P.init_params(6)
+    net = pc.LearnedPreconditioner(seed=0)
+    net.set_params(params)
+    nu = flat(torch, [s[0] for s in batch])
+    b = flat(torch, [s[1] for s in batch])
+    x = flat(torch, [s[2] for s in batch])
+    loss, per, g = net.loss_grad(SHAPES, nu, b, x)
+    f32 = [(s[0].astype(np.float32), s[1].astype(np.float32), s[2].astype(np.float32)) for s in batch]
+    lref, pref, gref = P.loss_and_grad(params, f32, emulate=True)
+    assert abs(loss - lref) < 2e-3 * max(1.0, abs(lref)), (loss, lref)
+    np.testing.assert_allclose(per, pref, rtol=2e-2, atol=2e-3)
+    blocks = [(P.OFF_IN, P.OFF_BIG)] + [(P.OFF_BIG + j * P.BIG_P, P.OFF_BIG + (j + 1) * P.BIG_P) for j in range(9)] \
+        + [(P.OFF_OUT, P.NUM_PARAMS)]
+    for a, e in blocks:
+        if np.linalg.norm(gref[a:e]) == 0:
+            continue
+        assert rel(g[a:e], gref[a:e]) < 5e-2, (a, rel(g[a:e], gref[a:e]))
+    cos = float(g @ gref / (np.linalg.norm(g) * np.linalg.norm(gref)))
+    assert cos > 0.999, cos
+
+
+def test_training_lowers_loss(torch, pc):
+    shapes = [(66, 66)] * 4
+    batch = make_batch(shapes, 8)
+    net = pc.LearnedPreconditioner(seed=3)
+    nu = flat(torch, [s[0] for s in batch])
+    b = flat(torch, [s[1] for s in batch])
+    x = flat(torch, [s[2] for s in batch])
+    first = net.train_step(shapes, nu, b, x, 1e-3)
+    for _ in range(40):
+        last = net.train_step(shapes, nu, b, x, 1e-3)
+    assert np.isfinite(last) and last < first, (first, last)
