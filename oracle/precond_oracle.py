@@ -6,8 +6,8 @@ loss and parameter gradients.  Nothing in the product path imports it.
 The reference (SimiLie) has no learned preconditioner; this file restates
 the network the GPU library defines (similie_b200/csrc/precond_net.cuh):
 
-  M(r): e1 = w D^-1 r; r1 = r - K e1; s = rms(r1);
-        x = pool2x2([r1/s, log(nu)/log(1000)]);  v = s up2x2(net(x)) (0 on the boundary);
+  M(r): e1 = w D^-1 r; r1 = r - K e1; s = rms(D^-1/2 r1);
+        x = pool2x2([D^-1/2 r1/s, log(nu)/log(1000)]);  v = s D^-1/2 up2x2(net(x)) (0 on the boundary);
         e2 = e1 + v;  M(r) = e2 + w D^-1 (r - K e2),  w = 0.8
   net:  h0 = relu(inc(x));  per level l >= 1: p_l = relu(down(pool(h_{l-1}))), h_l = relu(enc(p_l));
         g_{D-1} = h_{D-1};  g_l = relu(dec(h_l + up(g_{l+1})));  out = outc(g_0)
@@ -15,8 +15,10 @@ the network the GPU library defines (similie_b200/csrc/precond_net.cuh):
 
 Images are stored padded with a zero border ((h+2) x (w+2) pixels, channels
 last).  With `emulate=True` every value the GPU stores in BF16 (activations,
-tensor-core operands, the 32->32 weights) is rounded to BF16 here at the same
-point, so the GPU's results differ only by FP32 summation order; with
+pooled inputs, masked gradients fed to the tensor cores, the 32->32 weights)
+is rounded to BF16 here at the same point (the decoder input skip +
+up(coarse) is a sum of two BF16 tensors that the tensor core accumulates in
+FP32, so it is not rounded), so the GPU's results differ only by FP32 summation order; with
 `emulate=False` the whole computation is float64, which the finite-difference
 test uses to pin the backward pass.
 """
@@ -160,7 +162,8 @@ def net_forward(params, featp, emulate=True):
     for l in range(D - 2, -1, -1):
         wl = min(l, 2)
         Hl, Wl = hs[l].shape[0] - 2, hs[l].shape[1] - 2
-        uin = pad(rnd(hs[l][1:-1, 1:-1] + up(gs[l + 1], Hl, Wl)))
+        # the tensor core sums conv(skip) + conv(up(coarse)): no rounding of the sum
+        uin = pad(hs[l][1:-1, 1:-1] + up(gs[l + 1], Hl, Wl))
         w, b = big[DEC][wl]
         gs[l] = pad(rnd(np.maximum(conv(uin, w, b), 0.0)))
         uins[l] = uin
@@ -279,12 +282,13 @@ def precond(params, nu, r, emulate=True, keep=False):
     dinv = dinv_of(nu)
     e1 = OMEGA * dinv * r
     r1 = r - k_apply(e1, nu)
-    s = math.sqrt(np.mean(r1 * r1))
+    sq = np.sqrt(dinv)
+    s = math.sqrt(np.mean(dinv * r1 * r1))
     inv_s = 1.0 / s if s > 0 else 0.0
-    f = np.stack([r1 * inv_s, np.log(nu) / math.log(1000.0)], axis=-1)
+    f = np.stack([sq * r1 * inv_s, np.log(nu) / math.log(1000.0)], axis=-1)
     featp = pad(pool(pad(f)))
     out, cache = net_forward(params, featp, emulate)
-    v = s * up(pad(out), ny, nx) * interior_mask(ny, nx)
+    v = s * sq * up(pad(out), ny, nx) * interior_mask(ny, nx)
     e2 = e1 + v
     u = e2 + OMEGA * dinv * (r - k_apply(e2, nu))
     if keep:
@@ -310,7 +314,7 @@ def loss_and_grad(params, samples, emulate=True):
         ge2 = gu - OMEGA * k_apply(aux["dinv"] * gu, nu)
         ny, nx = b.shape
         hc, wc = aux["out"].shape
-        gnet = aux["s"] * up_adjoint(ge2 * interior_mask(ny, nx), hc, wc)
+        gnet = aux["s"] * up_adjoint(np.sqrt(aux["dinv"]) * ge2 * interior_mask(ny, nx), hc, wc)
         grad += net_backward(params, aux["cache"], gnet, emulate)
     return float(np.mean(losses)), losses, grad
 

@@ -61,7 +61,12 @@ struct Table
     Img aux[kMaxImages];
 };
 
-enum InMode { kPlain = 0, kPool = 1, kUpAdd = 2, kMasked = 3 };
+// Convolution inputs: kPlain the level's own tensor; kUpAdd skip + nearest
+// upsampled coarse tensor (two operands summed by the tensor core); kMasked a
+// FP32 gradient masked by ReLU activity (data and weight gradients);
+// kUpOnly the upsampled coarse tensor alone (second pass of kUpAdd's weight
+// gradient); kPool a 2x2 average of the finer level.
+enum InMode { kPlain = 0, kPool = 1, kUpAdd = 2, kMasked = 3, kUpOnly = 4 };
 
 __device__ __forceinline__ void unpack8(uint4 u, float* f)
 {
@@ -99,76 +104,175 @@ __device__ __forceinline__ int find_image(Table const& t, int tile)
     return lo;
 }
 
-// Channel chunk c (8 channels) of the convolution input at padded flat
-// pixel g of image im, per input mode.  Zero outside the padded image and
-// on its border.
-__device__ uint4 load_input(int mode, Table const& t, int im, int64_t g, int c, bf16 const* in, bf16 const* in2,
-                            float const* gin)
+// The 32 channels (four 16-byte chunks) of the convolution input at padded
+// flat pixel g of image im, per input mode.  Zero outside the padded image
+// and on its border.  32-bit pixel arithmetic (images below 2^31 pixels).
+__device__ __forceinline__ void load_pixel(int mode, Table const& t, int im, int g, bf16 const* in, bf16 const* in2,
+                                           float const* gin, uint4 (&v)[kChunks])
 {
     Img const o = t.img[im];
-    int64_t const P = o.w + 2;
+    int const P = o.w + 2;
     uint4 const zero = make_uint4(0u, 0u, 0u, 0u);
-    if (g < 0 || g >= P * (o.h + 2)) return zero;
-    if (mode == kPlain) return ld_chunk(in, o.offset + g, c);
-    int64_t const y = g / P, x = g - y * P;
-    if (y == 0 || x == 0 || y > o.h || x > o.w) return zero;
-    float f[8];
-    if (mode == kMasked) {
-        float4 const* gp = reinterpret_cast<float4 const*>(gin + (o.offset + g) * kCh + c * 8);
-        float4 const a = __ldg(gp), b = __ldg(gp + 1);
-        float act[8];
-        unpack8(ld_chunk(in2, o.offset + g, c), act);
-        float const gv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-        for (int i = 0; i < 8; ++i) f[i] = act[i] > 0.0f ? gv[i] : 0.0f;
-        return pack8(f);
+    for (int c = 0; c < kChunks; ++c) v[c] = zero;
+    if (g < 0 || g >= P * (o.h + 2)) return;
+    if (mode == kPlain) {
+        uint4 const* src = reinterpret_cast<uint4 const*>(in) + (o.offset + g) * kChunks;
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) v[c] = __ldg(src + c);
+        return;
+    }
+    int const y = g / P, x = g - y * P;
+    if (y == 0 || x == 0 || y > o.h || x > o.w) return;
+    if (mode == kMasked) {
+        float4 const* gp = reinterpret_cast<float4 const*>(gin + (o.offset + g) * kCh);
+        uint4 const* ap = reinterpret_cast<uint4 const*>(in2) + (o.offset + g) * kChunks;
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            float4 const a = __ldg(gp + 2 * c), b = __ldg(gp + 2 * c + 1);
+            float act[8];
+            unpack8(__ldg(ap + c), act);
+            float const gv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+            float f[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) f[i] = act[i] > 0.0f ? gv[i] : 0.0f;
+            v[c] = pack8(f);
+        }
+        return;
     }
     if (mode == kPool) {
         Img const fi = t.aux[im];
-        int64_t const Pf = fi.w + 2;
-        int64_t const base = fi.offset + (2 * y - 1) * Pf + (2 * x - 1);
-        float a[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) f[i] = 0.0f;
+        int const Pf = fi.w + 2;
+        int64_t const base = fi.offset + static_cast<int64_t>(2 * y - 1) * Pf + (2 * x - 1);
         int64_t const px[4] = {base, base + 1, base + Pf, base + Pf + 1};
+        uint4 const* src = reinterpret_cast<uint4 const*>(in);
+        uint4 raw[4][kChunks];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            unpack8(ld_chunk(in, px[q], c), a);
+        for (int q = 0; q < 4; ++q)
 #pragma unroll
-            for (int i = 0; i < 8; ++i) f[i] = f[i] + a[i];
+            for (int c = 0; c < kChunks; ++c) raw[q][c] = __ldg(src + px[q] * kChunks + c);
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            float f[8], a[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) f[i] = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                unpack8(raw[q][c], a);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) f[i] = f[i] + a[i];
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) f[i] = f[i] * 0.25f;
+            v[c] = pack8(f);
         }
+        return;
+    }
+    Img const ci = t.aux[im];
+    int64_t const cpx = ci.offset + static_cast<int64_t>((y - 1) / 2 + 1) * (ci.w + 2) + ((x - 1) / 2 + 1);
+    if (mode == kUpOnly) {
+        uint4 const* cp = reinterpret_cast<uint4 const*>(in2) + cpx * kChunks;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) f[i] = f[i] * 0.25f;
-        return pack8(f);
+        for (int c = 0; c < kChunks; ++c) v[c] = __ldg(cp + c);
+        return;
     }
     // kUpAdd: skip (this level) + nearest-upsampled coarse features
-    Img const ci = t.aux[im];
-    int64_t const cpx = ci.offset + ((y - 1) / 2 + 1) * (ci.w + 2) + ((x - 1) / 2 + 1);
-    float a[8];
-    unpack8(ld_chunk(in, o.offset + g, c), f);
-    unpack8(ld_chunk(in2, cpx, c), a);
+    uint4 const* sp = reinterpret_cast<uint4 const*>(in) + (o.offset + g) * kChunks;
+    uint4 const* cp = reinterpret_cast<uint4 const*>(in2) + cpx * kChunks;
+    uint4 a4[kChunks], b4[kChunks];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) f[i] = f[i] + a[i];
-    return pack8(f);
+    for (int c = 0; c < kChunks; ++c) {
+        a4[c] = __ldg(sp + c);
+        b4[c] = __ldg(cp + c);
+    }
+#pragma unroll
+    for (int c = 0; c < kChunks; ++c) {
+        float f[8], a[8];
+        unpack8(a4[c], f);
+        unpack8(b4[c], a);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) f[i] = f[i] + a[i];
+        v[c] = pack8(f);
+    }
 }
 
-// Shared memory of the convolution kernel.
+// Stage the three 130-pixel halo rows of the tile starting at flat pixel
+// `start` into smem (layout [chunk][row][pixel], 16 bytes per entry).
+__device__ __forceinline__ void load_halo(uint4* halo, int mode, Table const& t, int im, int start, int P,
+                                          bf16 const* in, bf16 const* in2, float const* gin)
+{
+    for (int i = threadIdx.x; i < 3 * kHalo; i += blockDim.x) {
+        int const r = i / kHalo, j = i - r * kHalo;
+        int const g = start + (r - 1) * P - 1 + j;
+        uint4 v[kChunks];
+        load_pixel(mode, t, im, g, in, in2, gin, v);
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) halo[(c * 3 + r) * kHalo + j] = v[c];
+    }
+}
+
+__device__ __forceinline__ void cp_async16(uint4* dst, void const* src, bool valid)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Asynchronous halo staging: the level's own tensor (up = false) or the
+// nearest-upsampled coarse tensor gathered to this level (up = true); pixels
+// outside the image (and, for the gather, its border) are zero-filled.
+__device__ __forceinline__ void stage_halo(uint4* halo, Table const& t, int im, int start, int P, bf16 const* src,
+                                           bool up)
+{
+    Img const o = t.img[im];
+    int const npx = P * (o.h + 2);
+    Img const ci = t.aux[im];
+    uint4 const* base = reinterpret_cast<uint4 const*>(src);
+    for (int i = threadIdx.x; i < 3 * kHalo; i += blockDim.x) {
+        int const r = i / kHalo, j = i - r * kHalo;
+        int const g = start + (r - 1) * P - 1 + j;
+        bool valid = g >= 0 && g < npx;
+        int64_t px = 0;
+        if (valid) {
+            if (up) {
+                int const y = g / P, x = g - y * P;
+                valid = !(y == 0 || x == 0 || y > o.h || x > o.w);
+                px = ci.offset + static_cast<int64_t>((y - 1) / 2 + 1) * (ci.w + 2) + ((x - 1) / 2 + 1);
+            } else {
+                px = o.offset + g;
+            }
+        }
+        uint4 const* p = valid ? base + px * kChunks : base;
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) cp_async16(&halo[(c * 3 + r) * kHalo + j], p + c, valid);
+    }
+}
+
+// Shared memory of the convolution kernel.  The second halo (used by kUpAdd
+// only) comes last, so the other modes launch with the shorter block and fit
+// more CTAs per multiprocessor.
 struct ConvSmem
 {
-    uint4 w[kKChunks * kCh];           // B operand: [K chunk][output channel], 18432 B
-    uint4 halo[kChunks * 3 * kHalo];   // A operand source: [chunk][halo row][halo pixel], 24960 B
+    uint4 w[kKChunks * kCh];              // B operand: [K chunk][output channel], 18432 B
+    float wout[kOutW];                    // output-convolution weights (tap partials)
     uint64_t bar;
     uint32_t tmem;
     int abort;
+    uint4 halo[2][kChunks * 3 * kHalo];   // A operand sources: [chunk][halo row][halo pixel], 2 x 24960 B
 };
 
 // out = act(conv3x3(input) + bias) for the interior pixels of every image of
-// the table; border pixels are written as zero.  out_f32 selects an FP32
-// output (data gradients), accumulate adds into it.
+// the table; border pixels are written as zero.  out (BF16) may be NULL;
+// out_f32 selects an FP32 output (data gradients), accumulate adds into it;
+// out_taps (with wout) writes the nine partial sums of the 32 -> 1 output
+// convolution per pixel, taps[tap][pixel], for a separate gather.
 __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Table t, int mode, bf16 const* in,
                                                       bf16 const* in2, float const* gin, bf16 const* wt,
                                                       float const* bias, int relu, bf16* out, float* out_f32,
-                                                      int accumulate, int* error_flag)
+                                                      int accumulate, float* out_taps, float const* wout,
+                                                      int64_t taps_stride, int* error_flag)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     ConvSmem& s = *reinterpret_cast<ConvSmem*>(smem_raw);
@@ -177,6 +281,8 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
         int const co = i & 31, k = i >> 5;
         s.w[k * kCh + co] = __ldg(reinterpret_cast<uint4 const*>(wt + co * (kTaps * kCh)) + k);
     }
+    if (out_taps != nullptr)
+        for (int i = tid; i < kOutW; i += 128) s.wout[i] = wout[i];
     if (warp == 0) tmem_alloc(&s.tmem, 32);
     if (tid == 0) {
         mbar_init(&s.bar, 1);
@@ -186,21 +292,22 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
     __syncthreads();
     tc_fence_after();
     uint32_t const tmem = s.tmem;
-    uint32_t const halo_addr = smem_u32(s.halo);
+    uint32_t const halo_addr[2] = {smem_u32(s.halo[0]), smem_u32(s.halo[1])};
     uint32_t const w_addr = smem_u32(s.w);
+    int const nops = mode == kUpAdd ? 2 : 1;
     uint32_t phase = 0;
     int const ntiles = t.tile_base[t.nimg];
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         int const im = find_image(t, tile);
         Img const o = t.img[im];
-        int64_t const P = o.w + 2;
-        int64_t const start = P + static_cast<int64_t>(tile - t.tile_base[im]) * kTilePx;
-        for (int i = tid; i < 3 * kHalo * kChunks; i += 128) {
-            int const c = i & 3;
-            int const j = (i >> 2) % kHalo;
-            int const r = (i >> 2) / kHalo;
-            int64_t const g = start + (r - 1) * P - 1 + j;
-            s.halo[(c * 3 + r) * kHalo + j] = load_input(mode, t, im, g, c, in, in2, gin);
+        int const P = o.w + 2;
+        int const start = P + (tile - t.tile_base[im]) * kTilePx;
+        if (mode == kPlain || mode == kUpAdd) {
+            stage_halo(s.halo[0], t, im, start, P, in, false);
+            if (mode == kUpAdd) stage_halo(s.halo[1], t, im, start, P, in2, true);
+            cp_async_wait_all();
+        } else {
+            load_halo(s.halo[0], mode, t, im, start, P, in, in2, gin);
         }
         fence_async_smem();
         __syncthreads();
@@ -208,14 +315,18 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
             tc_fence_after();
             int step = 0;
 #pragma unroll 1
-            for (int tap = 0; tap < kTaps; ++tap) {
-                int const dy = tap / 3, dx = tap % 3;
+            for (int op = 0; op < nops; ++op) {
+#pragma unroll 1
+                for (int tap = 0; tap < kTaps; ++tap) {
+                    int const dy = tap / 3, dx = tap % 3;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    uint64_t const a = umma_desc(halo_addr + ((2 * h * 3 + dy) * kHalo + dx) * 16, 3 * kHalo * 16, 128);
-                    uint64_t const b = umma_desc(w_addr + (tap * kChunks + 2 * h) * kCh * 16, kCh * 16, 128);
-                    umma_bf16(tmem, a, b, kIdescFwd, step > 0 ? 1u : 0u);
-                    ++step;
+                    for (int h = 0; h < 2; ++h) {
+                        uint64_t const a =
+                                umma_desc(halo_addr[op] + ((2 * h * 3 + dy) * kHalo + dx) * 16, 3 * kHalo * 16, 128);
+                        uint64_t const b = umma_desc(w_addr + (tap * kChunks + 2 * h) * kCh * 16, kCh * 16, 128);
+                        umma_bf16(tmem, a, b, kIdescFwd, step > 0 ? 1u : 0u);
+                        ++step;
+                    }
                 }
             }
             umma_commit(&s.bar);
@@ -229,9 +340,9 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
         tc_fence_after();
         float acc[32];
         tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16), acc);
-        int64_t const g = start + warp * 32 + lane;
+        int const g = start + warp * 32 + lane;
         if (g < P * (o.h + 1)) {
-            int64_t const x = g % P;
+            int const x = g % P;
             bool const border = x == 0 || x == P - 1;
             if (border) {
 #pragma unroll
@@ -261,10 +372,29 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
                     }
                     dst[q] = v;
                 }
-            } else {
-                uint4* dst = reinterpret_cast<uint4*>(out + px * kCh);
+            }
+            if (out != nullptr || out_taps != nullptr) {
+                uint4 packed[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) dst[q] = pack8(acc + 8 * q);
+                for (int q = 0; q < 4; ++q) packed[q] = pack8(acc + 8 * q);
+                if (out != nullptr) {
+                    uint4* dst = reinterpret_cast<uint4*>(out + px * kCh);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) dst[q] = packed[q];
+                }
+                if (out_taps != nullptr) {
+                    // partials of the output convolution from the BF16-rounded activations
+                    float f[32];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) unpack8(packed[q], f + 8 * q);
+#pragma unroll 1
+                    for (int tap = 0; tap < kTaps; ++tap) {
+                        float a = 0.0f;
+#pragma unroll
+                        for (int ci = 0; ci < 32; ++ci) a = __fmaf_rn(s.wout[tap * kCh + ci], f[ci], a);
+                        out_taps[tap * taps_stride + px] = a;
+                    }
+                }
             }
         }
         tc_fence_before();
@@ -275,6 +405,43 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
     __syncthreads();
     tc_fence_after();
     if (warp == 0) tmem_dealloc(tmem, 32);
+}
+
+// Output convolution from the tap partials: out[p] = b + sum_tap taps[tap][p + tap] (zero border).
+__global__ void out_gather_kernel(const __grid_constant__ Table t, float const* taps, int64_t taps_stride,
+                                  float const* params, float* out)
+{
+    int const im = blockIdx.y;
+    if (im >= t.nimg) return;
+    Img const o = t.img[im];
+    int const P = o.w + 2, npx = P * (o.h + 2);
+    int const g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= npx) return;
+    int const y = g / P, x = g - y * P;
+    float a = 0.0f;
+    if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
+        a = params[kOffOut + kOutW];
+        int64_t const base = o.offset + g;
+#pragma unroll
+        for (int tap = 0; tap < kTaps; ++tap) a = a + taps[tap * taps_stride + base + (tap / 3 - 1) * P + (tap % 3 - 1)];
+    }
+    out[o.offset + g] = a;
+}
+
+// Coarse tensor = 2x2 average of the finer level (t.img coarse, t.aux fine), BF16.
+__global__ void pool_kernel(const __grid_constant__ Table t, bf16 const* fine, bf16* coarse)
+{
+    int const im = blockIdx.y;
+    if (im >= t.nimg) return;
+    Img const o = t.img[im];
+    int const P = o.w + 2, npx = P * (o.h + 2);
+    int const g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= npx) return;
+    uint4 v[kChunks];
+    load_pixel(kPool, t, im, g, fine, nullptr, nullptr, v);
+    uint4* dst = reinterpret_cast<uint4*>(coarse) + (o.offset + g) * kChunks;
+#pragma unroll
+    for (int c = 0; c < kChunks; ++c) dst[c] = v[c];
 }
 
 // Shared memory of the weight-gradient kernel.  The im2col tile is followed
@@ -324,59 +491,61 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const __grid_constant__ Tabl
         Img const o = t.img[im];
         int64_t const P = o.w + 2;
         int64_t const start = P + static_cast<int64_t>(tile - t.tile_base[im]) * kTilePx;
-        for (int i = tid; i < 3 * kHalo * kChunks; i += 128) {
-            int const c = i & 3;
-            int const j = (i >> 2) % kHalo;
-            int const r = (i >> 2) / kHalo;
-            int64_t const g = start + (r - 1) * P - 1 + j;
-            s.halo[(c * 3 + r) * kHalo + j] = load_input(mode, t, im, g, c, in, in2, nullptr);
-        }
-        for (int i = tid; i < kTilePx * kChunks; i += 128) {
-            int const c = i & 3, m = i >> 2;
-            int64_t const g = start + m;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (g < P * (o.h + 1)) v = load_input(kMasked, tz, im, g, c, y, y, dy);
-            s.dz[c * kTilePx + m] = v;
-        }
-        __syncthreads();
-        for (int i = tid; i < kKChunks * kTilePx; i += 128) {
-            int const m = i % kTilePx, kc = i / kTilePx;
-            int const tap = kc / kChunks, c = kc % kChunks;
-            int const dyy = tap / 3, dxx = tap % 3;
-            s.col[kc * kTilePx + m] = s.halo[(c * 3 + dyy) * kHalo + m + dxx];
-        }
-        if (tid < kCh) {
-            int const c = tid / 8, e = tid % 8;
-            float f[8];
-            for (int m = 0; m < kTilePx; ++m) {
-                unpack8(s.dz[c * kTilePx + m], f);
-                db = db + f[e];
-            }
-        }
-        fence_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            tc_fence_after();
-#pragma unroll 1
-            for (int mt = 0; mt < 3; ++mt) {
+        {
+            int const m = tid;
+            int const g = static_cast<int>(start) + m;
+            uint4 v[kChunks];
+            load_pixel(kMasked, tz, im, g < P * (o.h + 1) ? g : -1, y, y, dy, v);
 #pragma unroll
-                for (int kk = 0; kk < kTilePx / 16; ++kk) {
-                    uint64_t const a = umma_desc(col_addr + (16 * mt * kTilePx + kk * 16) * 16, 128, kTilePx * 16);
-                    uint64_t const b = umma_desc(dz_addr + kk * 16 * 16, 128, kTilePx * 16);
-                    umma_bf16(tmem + mt * 32, a, b, kIdescWgrad, (any || kk > 0) ? 1u : 0u);
+            for (int c = 0; c < kChunks; ++c) s.dz[c * kTilePx + m] = v[c];
+        }
+        // kUpAdd: the two summands of the input in two passes (skip, then the
+        // upsampled coarse tensor), both accumulated into TMEM.
+        int const npass = mode == kUpAdd ? 2 : 1;
+        for (int pass = 0; pass < npass; ++pass) {
+            int const lmode = mode == kUpAdd ? (pass == 0 ? kPlain : kUpOnly) : mode;
+            load_halo(s.halo, lmode, t, im, static_cast<int>(start), static_cast<int>(P), in, in2, nullptr);
+            __syncthreads();
+            for (int i = tid; i < kKChunks * kTilePx; i += 128) {
+                int const m = i % kTilePx, kc = i / kTilePx;
+                int const tap = kc / kChunks, c = kc % kChunks;
+                int const dyy = tap / 3, dxx = tap % 3;
+                s.col[kc * kTilePx + m] = s.halo[(c * 3 + dyy) * kHalo + m + dxx];
+            }
+            if (pass == 0 && tid < kCh) {
+                int const c = tid / 8, e = tid % 8;
+                float f[8];
+                for (int m = 0; m < kTilePx; ++m) {
+                    unpack8(s.dz[c * kTilePx + m], f);
+                    db = db + f[e];
                 }
             }
-            umma_commit(&s.bar);
+            fence_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+#pragma unroll 1
+                for (int mt = 0; mt < 3; ++mt) {
+#pragma unroll
+                    for (int kk = 0; kk < kTilePx / 16; ++kk) {
+                        uint64_t const a = umma_desc(col_addr + (16 * mt * kTilePx + kk * 16) * 16, 128, kTilePx * 16);
+                        uint64_t const b = umma_desc(dz_addr + kk * 16 * 16, 128, kTilePx * 16);
+                        umma_bf16(tmem + mt * 32, a, b, kIdescWgrad, (any || kk > 0) ? 1u : 0u);
+                    }
+                }
+                umma_commit(&s.bar);
+            }
+            any = true;
+            __syncwarp();
+            bool const done = mbar_wait(&s.bar, phase);
+            phase ^= 1u;
+            if (!done) s.abort = 1;
+            __syncthreads();
+            if (s.abort) break;
+            tc_fence_before();
+            __syncthreads();
         }
-        any = true;
-        __syncwarp();
-        bool const done = mbar_wait(&s.bar, phase);
-        phase ^= 1u;
-        if (!done) s.abort = 1;
-        __syncthreads();
         if (s.abort) break;
-        tc_fence_before();
-        __syncthreads();
     }
     float* dst = part + static_cast<int64_t>(blockIdx.x) * kWgradParts;
     if (!s.abort) {
@@ -424,62 +593,79 @@ __global__ void convert_weights_kernel(float const* params, bf16* wf, bf16* wt)
 
 // ------------------------------------------------------------------ thin layers (CUDA cores)
 
-// Input convolution 2 -> 32 (+ bias, ReLU) from the FP32 2-channel feature image.
-__global__ void inc_forward_kernel(const __grid_constant__ Table t, float const* feat, float const* params, bf16* out)
+// Input convolution 2 -> 32 (+ bias, ReLU) from the FP32 2-channel feature
+// image; weights staged in shared memory, one pixel per thread.
+__global__ void __launch_bounds__(256) inc_forward_kernel(const __grid_constant__ Table t, float const* feat,
+                                                          float const* params, bf16* out)
 {
+    __shared__ float w[kInW + kCh];
+    for (int i = threadIdx.x; i < kInW + kCh; i += blockDim.x) w[i] = params[kOffIn + i];
+    __syncthreads();
     int const im = blockIdx.y;
     if (im >= t.nimg) return;
     Img const o = t.img[im];
-    int64_t const P = o.w + 2, npx = P * (o.h + 2);
-    int64_t const g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    int const P = o.w + 2, npx = P * (o.h + 2);
+    int const g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= npx) return;
-    int64_t const y = g / P, x = g - y * P;
+    int const y = g / P, x = g - y * P;
     float acc[kCh];
-    bool const border = y == 0 || x == 0 || y > o.h || x > o.w;
-    if (border) {
+    if (y == 0 || x == 0 || y > o.h || x > o.w) {
+#pragma unroll
         for (int i = 0; i < kCh; ++i) acc[i] = 0.0f;
     } else {
-        float in[kTaps][2];
+        float in[kTaps * 2];
+        float2 const* f2 = reinterpret_cast<float2 const*>(feat) + o.offset;
+#pragma unroll
         for (int tap = 0; tap < kTaps; ++tap) {
-            int64_t const q = o.offset + g + (tap / 3 - 1) * P + (tap % 3 - 1);
-            in[tap][0] = feat[2 * q];
-            in[tap][1] = feat[2 * q + 1];
+            float2 const v = f2[g + (tap / 3 - 1) * P + (tap % 3 - 1)];
+            in[2 * tap] = v.x;
+            in[2 * tap + 1] = v.y;
         }
-        float const* w = params + kOffIn;
+#pragma unroll 4
         for (int co = 0; co < kCh; ++co) {
-            float a = 0.0f;
-            for (int tap = 0; tap < kTaps; ++tap)
-                for (int ci = 0; ci < 2; ++ci) a = a + w[(co * kTaps + tap) * 2 + ci] * in[tap][ci];
-            a = a + w[kInW + co];
+            float a = w[kInW + co];
+#pragma unroll
+            for (int k = 0; k < kTaps * 2; ++k) a = __fmaf_rn(w[co * kTaps * 2 + k], in[k], a);
             acc[co] = fmaxf(a, 0.0f);
         }
     }
     uint4* dst = reinterpret_cast<uint4*>(out + (o.offset + g) * kCh);
+#pragma unroll
     for (int q = 0; q < 4; ++q) dst[q] = pack8(acc + 8 * q);
 }
 
 // Output convolution 32 -> 1 (+ bias), FP32 out, zero border.
-__global__ void out_forward_kernel(const __grid_constant__ Table t, bf16 const* in, float const* params, float* out)
+__global__ void __launch_bounds__(256) out_forward_kernel(const __grid_constant__ Table t, bf16 const* in,
+                                                          float const* params, float* out)
 {
+    __shared__ float w[kOutW + 1];
+    for (int i = threadIdx.x; i < kOutW + 1; i += blockDim.x) w[i] = params[kOffOut + i];
+    __syncthreads();
     int const im = blockIdx.y;
     if (im >= t.nimg) return;
     Img const o = t.img[im];
-    int64_t const P = o.w + 2, npx = P * (o.h + 2);
-    int64_t const g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    int const P = o.w + 2, npx = P * (o.h + 2);
+    int const g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= npx) return;
-    int64_t const y = g / P, x = g - y * P;
+    int const y = g / P, x = g - y * P;
     float a = 0.0f;
     if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
-        float const* w = params + kOffOut;
+        a = w[kOutW];
+        uint4 const* src = reinterpret_cast<uint4 const*>(in) + o.offset * kChunks;
+#pragma unroll 3
         for (int tap = 0; tap < kTaps; ++tap) {
-            int64_t const q = o.offset + g + (tap / 3 - 1) * P + (tap % 3 - 1);
-            float f[8];
+            int const q = g + (tap / 3 - 1) * P + (tap % 3 - 1);
+            uint4 v[kChunks];
+#pragma unroll
+            for (int c = 0; c < kChunks; ++c) v[c] = __ldg(src + static_cast<int64_t>(q) * kChunks + c);
+#pragma unroll
             for (int c = 0; c < kChunks; ++c) {
-                unpack8(ld_chunk(in, q, c), f);
-                for (int e = 0; e < 8; ++e) a = a + w[tap * kCh + c * 8 + e] * f[e];
+                float f[8];
+                unpack8(v[c], f);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) a = __fmaf_rn(w[tap * kCh + c * 8 + e], f[e], a);
             }
         }
-        a = a + w[kOutW];
     }
     out[o.offset + g] = a;
 }
@@ -682,13 +868,26 @@ __global__ void upadd_adjoint_coarse_kernel(const __grid_constant__ Table t, flo
     *o = v;
 }
 
+// dst = src over every pixel of the table's images (16 bytes per thread).
+__global__ void copy_act_kernel(const __grid_constant__ Table t, bf16 const* src, bf16* dst)
+{
+    int const im = blockIdx.y;
+    if (im >= t.nimg) return;
+    Img const f = t.img[im];
+    int64_t const idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= static_cast<int64_t>(f.h + 2) * (f.w + 2) * kChunks) return;
+    int64_t const q = f.offset * kChunks + idx;
+    reinterpret_cast<uint4*>(dst)[q] = reinterpret_cast<uint4 const*>(src)[q];
+}
+
 // ------------------------------------------------------------------ node-level wrapper (FP32)
 
 struct Samples
 {
     int n;
     Sample s[kMaxImages];
-    Img top[kMaxImages];   // level-0 network image of each sample
+    Img top[kMaxImages];                 // level-0 network image of each sample
+    int32_t item_base[kMaxImages + 1];   // first fused-wrapper work item of each sample
 };
 
 __device__ __forceinline__ bool node_of(Samples const& ss, int64_t& row, Sample& sm)
@@ -795,10 +994,11 @@ __global__ void dots_finish_kernel(double const* part, int nsamples, int nblocks
     dots[i] = v;
 }
 
-// Feature image of the network's top level: 2x2 average of [r1 / s, log(nu)/log(1000)]
-// over the nodes of each half-resolution pixel (nodes outside the grid count as zero).
+// Feature image of the network's top level: 2x2 average of
+// [D^-1/2 r1 / s, log(nu)/log(1000)] over the nodes of each half-resolution
+// pixel (nodes outside the grid count as zero), s = rms(D^-1/2 r1).
 __global__ void features_kernel(const __grid_constant__ Samples ss, float const* r1, float const* nu,
-                                double const* dots, float* feat)
+                                float const* dinv, double const* dots, float* feat)
 {
     int const sidx = blockIdx.y;
     Sample const sm = ss.s[sidx];
@@ -818,7 +1018,7 @@ __global__ void features_kernel(const __grid_constant__ Samples ss, float const*
                 int64_t const j = 2 * (y - 1) + a, i = 2 * (x - 1) + b;
                 if (j >= sm.ny || i >= sm.nx) continue;
                 int64_t const q = sm.offset + j * sm.nx + i;
-                f0 = f0 + r1[q] * inv_s;
+                f0 = f0 + r1[q] * sqrtf(dinv[q]) * inv_s;
                 f1 = f1 + logf(nu[q]) * inv_l;
             }
         f0 = f0 * 0.25f;
@@ -863,8 +1063,9 @@ __global__ void loss_grad_u_kernel(const __grid_constant__ Samples ss, float con
     gu[q] = static_cast<float>(cb * b[q] + ck * ku[q]);
 }
 
-// g_net[top pixel] = s * sum over interior child nodes of g_e2.
-__global__ void net_grad_kernel(const __grid_constant__ Samples ss, float const* ge2, double const* dots, float* gnet)
+// g_net[top pixel] = s * sum over interior child nodes of D^-1/2 g_e2.
+__global__ void net_grad_kernel(const __grid_constant__ Samples ss, float const* ge2, float const* dinv,
+                                double const* dots, float* gnet)
 {
     int const sidx = blockIdx.y;
     Sample const sm = ss.s[sidx];
@@ -883,7 +1084,8 @@ __global__ void net_grad_kernel(const __grid_constant__ Samples ss, float const*
                 int64_t const j = 2 * (y - 1) + a, i = 2 * (x - 1) + b;
                 if (j >= sm.ny || i >= sm.nx) continue;
                 if (i == 0 || j == 0 || i + 1 == sm.nx || j + 1 == sm.ny) continue;
-                acc = acc + ge2[sm.offset + j * sm.nx + i];
+                int64_t const q = sm.offset + j * sm.nx + i;
+                acc = acc + sqrtf(dinv[q]) * ge2[q];
             }
         v = s * acc;
     }
@@ -899,6 +1101,114 @@ __global__ void axpby_kernel(const __grid_constant__ Samples ss, float a, float 
     if (!node_of(ss, row, sm)) return;
     int64_t const q = sm.offset + row;
     out[q] = a * x[q] + b * y[q];
+}
+
+// ------------------------------------------------------------------ fused wrapper passes
+//
+// Work items of kWrapRows consecutive nodes of one sample, so no block idles
+// on the small grids of a batch of uneven sizes; 32-bit index arithmetic.
+
+constexpr int kWrapRows = 2048;
+
+struct WrapItem
+{
+    int32_t sample, begin, end, index;   // index: item number within its sample
+};
+
+// K e at interior node (i, j) of an nx-wide grid for an e given by a functor.
+template <class E>
+__device__ __forceinline__ float k_row(E const& e, float const* nu, int nx, int row, int i, int j)
+{
+    float const a0 = e(row);
+    float res = 0.0f;
+    if (j >= 2) res = res + (a0 - e(row - nx)) * nu[row - nx];
+    res = res + (a0 - e(row + nx)) * nu[row];
+    if (i >= 2) res = res + (a0 - e(row - 1)) * nu[row - 1];
+    res = res + (a0 - e(row + 1)) * nu[row];
+    return res;
+}
+
+__device__ __forceinline__ double block_sum_d(double v, double* red)
+{
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < static_cast<int>(blockDim.x) / 32; ++w) t += red[w];
+    return t;
+}
+
+// e1 = w D^-1 r, r1 = r - K e1 (boundary rows: r1 = r - e1), and the partial
+// sums of |D^-1/2 r1|^2 per item.
+__global__ void __launch_bounds__(256) wrap_pre_kernel(const __grid_constant__ Samples ss, WrapItem const* items,
+                                                       float const* nu, float const* dinv, float const* r, float* e1,
+                                                       float* r1, double* part)
+{
+    __shared__ double red[8];
+    WrapItem const it = items[blockIdx.x];
+    Sample const sm = ss.s[it.sample];
+    int const nx = sm.nx, ny = sm.ny;
+    float const* nu_s = nu + sm.offset;
+    float const* d_s = dinv + sm.offset;
+    float const* r_s = r + sm.offset;
+    auto e = [&](int q) { return kOmega * (d_s[q] * r_s[q]); };
+    double acc = 0.0;
+    for (int row = it.begin + threadIdx.x; row < it.end; row += blockDim.x) {
+        int const j = row / nx, i = row - j * nx;
+        float const ev = e(row);
+        float v;
+        if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) v = r_s[row] - ev;
+        else v = r_s[row] - k_row(e, nu_s, nx, row, i, j);
+        e1[sm.offset + row] = ev;
+        r1[sm.offset + row] = v;
+        acc += static_cast<double>(d_s[row]) * static_cast<double>(v) * static_cast<double>(v);
+    }
+    double const t = block_sum_d(acc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// dots[s*3] = sum of the sample's item partials (fixed order).
+__global__ void wrap_finish_kernel(const __grid_constant__ Samples ss, double const* part, double* dots)
+{
+    int const sidx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sidx >= ss.n) return;
+    double t = 0.0;
+    for (int k = ss.item_base[sidx]; k < ss.item_base[sidx + 1]; ++k) t += part[k];
+    dots[sidx * 3] = t;
+}
+
+// M(r) = e2 + w D^-1 (r - K e2), e2 = e1 + s D^-1/2 up(unet) (zero correction on the boundary).
+__global__ void __launch_bounds__(256) wrap_post_kernel(const __grid_constant__ Samples ss, WrapItem const* items,
+                                                        float const* nu, float const* dinv, float const* r,
+                                                        float const* e1, float const* unet, double const* dots,
+                                                        float* out)
+{
+    WrapItem const it = items[blockIdx.x];
+    Sample const sm = ss.s[it.sample];
+    Img const o = ss.top[it.sample];
+    int const nx = sm.nx, ny = sm.ny;
+    int const P = o.w + 2;
+    float const s = static_cast<float>(sqrt(dots[it.sample * 3] / (static_cast<double>(nx) * ny)));
+    float const* nu_s = nu + sm.offset;
+    float const* e1_s = e1 + sm.offset;
+    float const* d_s = dinv + sm.offset;
+    float const* un = unet + o.offset;
+    auto e = [&](int q) {
+        int const jj = q / nx, ii = q - jj * nx;
+        float v = e1_s[q];
+        if (!(ii == 0 || jj == 0 || ii + 1 == nx || jj + 1 == ny))
+            v = v + s * sqrtf(d_s[q]) * un[(jj / 2 + 1) * P + (ii / 2 + 1)];
+        return v;
+    };
+    for (int row = it.begin + threadIdx.x; row < it.end; row += blockDim.x) {
+        int const j = row / nx, i = row - j * nx;
+        float const e0 = e(row);
+        float const ke = (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) ? e0 : k_row(e, nu_s, nx, row, i, j);
+        int64_t const q = sm.offset + row;
+        out[q] = e0 + kOmega * (dinv[q] * (r[q] - ke));
+    }
 }
 
 __global__ void adam_kernel(float* p, float const* g, float* m, float* v, int n, float lr, float b1t, float b2t)
@@ -954,13 +1264,16 @@ public:
     std::vector<int> depth;        // levels per sample
     Samples ss {};
     // node-level FP32 vectors
-    DevBuf dinv, e1, r1, e2, u, ku, tmp, gu, ge2, fnu;
+    DevBuf dinv, e1, r1, e2, u, ku, tmp, gu, ge2;
     DevBuf dparts;                 // per-sample dot partials
     DevBuf dots;                   // [3 sets][nsamples][3]
     int dot_blocks = 0;
     // network buffers per level
-    std::vector<DevBuf> h, p, g, dh, dg, dx;
+    std::vector<DevBuf> h, p, g, pin, dh, dg, dx;
+    DevBuf taps;                   // 9 x level-0 pixels: output-convolution partials
     DevBuf feat, unet, gnet;
+    DevBuf witems, wpart;          // fused wrapper work items and their partial sums
+    int nwitems = 0;
     DevBuf wparts;                 // weight-gradient partials
     int wgrad_grid = 0;
     int64_t max_node_per_sample = 0;
@@ -993,6 +1306,8 @@ sil_status Workspace::build(std::vector<Sample> const& s)
     ss.n = n;
     for (int i = 0; i < n; ++i) {
         if (s[i].nx < 3 || s[i].ny < 3) return fail(SIL_ERR_INVALID, "precond: grids need at least 3x3 nodes");
+        if (static_cast<int64_t>(s[i].nx) * s[i].ny >= (int64_t(1) << 31))
+            return fail(SIL_ERR_INVALID, "precond: a grid must have fewer than 2^31 nodes");
         ss.s[i] = s[i];
         nodes = std::max<int64_t>(nodes, s[i].offset + static_cast<int64_t>(s[i].nx) * s[i].ny);
         max_node_per_sample = std::max<int64_t>(max_node_per_sample, static_cast<int64_t>(s[i].nx) * s[i].ny);
@@ -1017,7 +1332,7 @@ sil_status Workspace::build(std::vector<Sample> const& s)
     }
     for (int i = 0; i < n; ++i) ss.top[i] = levels[0].img[i];
     size_t const nb = static_cast<size_t>(nodes) * sizeof(float);
-    for (DevBuf* b : {&dinv, &e1, &r1, &e2, &u, &ku, &tmp, &gu, &ge2, &fnu}) {
+    for (DevBuf* b : {&dinv, &e1, &r1, &e2, &u, &ku, &tmp, &gu, &ge2}) {
         sil_status const st = b->alloc(nb);
         if (st != SIL_OK) return st;
     }
@@ -1025,6 +1340,7 @@ sil_status Workspace::build(std::vector<Sample> const& s)
     if (sil_status st = dparts.alloc(sizeof(double) * 3 * n * dot_blocks); st != SIL_OK) return st;
     if (sil_status st = dots.alloc(sizeof(double) * 3 * 3 * n); st != SIL_OK) return st;
     h.resize(maxd);
+    pin.resize(maxd);
     p.resize(maxd);
     g.resize(maxd);
     dh.resize(maxd);
@@ -1034,7 +1350,7 @@ sil_status Workspace::build(std::vector<Sample> const& s)
     // border rows of an image, which must read as zero.
     for (int l = 0; l < maxd; ++l) {
         size_t const a = static_cast<size_t>(levels[l].npx) * kCh;
-        for (DevBuf* b : {&h[l], &p[l], &g[l]}) {
+        for (DevBuf* b : {&h[l], &p[l], &g[l], &pin[l]}) {
             if (sil_status st = b->alloc(a * sizeof(bf16)); st != SIL_OK) return st;
             SIL_CUDA_CHECK(cudaMemset(b->p, 0, a * sizeof(bf16)));
         }
@@ -1043,7 +1359,23 @@ sil_status Workspace::build(std::vector<Sample> const& s)
             SIL_CUDA_CHECK(cudaMemset(b->p, 0, a * sizeof(float)));
         }
     }
+    {
+        std::vector<WrapItem> wi;
+        for (int i = 0; i < n; ++i) {
+            int const rows = s[i].nx * s[i].ny;
+            int idx = 0;
+            ss.item_base[i] = static_cast<int32_t>(wi.size());
+            for (int b = 0; b < rows; b += kWrapRows, ++idx) wi.push_back({i, b, std::min(rows, b + kWrapRows), idx});
+        }
+        ss.item_base[n] = static_cast<int32_t>(wi.size());
+        nwitems = static_cast<int>(wi.size());
+        if (sil_status st = witems.alloc(sizeof(WrapItem) * wi.size()); st != SIL_OK) return st;
+        if (sil_status st = wpart.alloc(sizeof(double) * wi.size()); st != SIL_OK) return st;
+        SIL_CUDA_CHECK(cudaMemcpy(witems.p, wi.data(), sizeof(WrapItem) * wi.size(), cudaMemcpyHostToDevice));
+    }
     int64_t const top = levels[0].npx;
+    if (sil_status st = taps.alloc(top * kTaps * sizeof(float)); st != SIL_OK) return st;
+    SIL_CUDA_CHECK(cudaMemset(taps.p, 0, top * kTaps * sizeof(float)));
     if (sil_status st = feat.alloc(top * 2 * sizeof(float)); st != SIL_OK) return st;
     if (sil_status st = unet.alloc(top * sizeof(float)); st != SIL_OK) return st;
     if (sil_status st = gnet.alloc(top * sizeof(float)); st != SIL_OK) return st;
@@ -1081,14 +1413,21 @@ Table Workspace::table(int level, int aux_level, bool) const
 
 namespace {
 
-size_t conv_smem() { return sizeof(ConvSmem) + 1024; }
+size_t conv_smem(int mode = kUpAdd)
+{
+    return sizeof(ConvSmem) - (mode == kUpAdd ? 0 : sizeof(uint4) * kChunks * 3 * kHalo);
+}
 size_t wgrad_smem() { return sizeof(WgradSmem) + 1024; }
 
 bool g_attr_done = false;
+int g_sms = 0;  // multiprocessor count, read once (outside any stream capture)
 
 sil_status ensure_attributes()
 {
     if (g_attr_done) return SIL_OK;
+    int dev = 0;
+    SIL_CUDA_CHECK(cudaGetDevice(&dev));
+    SIL_CUDA_CHECK(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev));
     SIL_CUDA_CHECK(cudaFuncSetAttribute(conv3x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(conv_smem())));
     SIL_CUDA_CHECK(cudaFuncSetAttribute(wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1099,10 +1438,7 @@ sil_status ensure_attributes()
 
 int conv_grid(int ntiles)
 {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return std::max(1, std::min(ntiles, 4 * sms));
+    return std::max(1, std::min(ntiles, 4 * (g_sms > 0 ? g_sms : 148)));
 }
 
 // 1024-byte aligned dynamic shared memory: the kernels index from the start
@@ -1110,11 +1446,11 @@ int conv_grid(int ntiles)
 // the kernel declares it so.
 sil_status launch_conv(cudaStream_t st, Table const& t, int mode, bf16 const* in, bf16 const* in2, float const* gin,
                        bf16 const* w, float const* bias, int relu, bf16* out, float* out_f32, int accumulate,
-                       int* err)
+                       int* err, float* out_taps = nullptr, float const* wout = nullptr, int64_t taps_stride = 0)
 {
     if (t.nimg == 0 || t.tile_base[t.nimg] == 0) return SIL_OK;
-    conv3x3_kernel<<<conv_grid(t.tile_base[t.nimg]), 128, conv_smem(), st>>>(t, mode, in, in2, gin, w, bias, relu, out,
-                                                                             out_f32, accumulate, err);
+    conv3x3_kernel<<<conv_grid(t.tile_base[t.nimg]), 128, conv_smem(mode), st>>>(
+            t, mode, in, in2, gin, w, bias, relu, out, out_f32, accumulate, out_taps, wout, taps_stride, err);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
@@ -1251,8 +1587,13 @@ sil_status dots(Workspace& w, cudaStream_t st, int set, float const* a1, float c
     return SIL_OK;
 }
 
-// Network forward on the feature image in w.feat; result in w.unet.
-sil_status net_forward(Net& net, Workspace& w, cudaStream_t st)
+Table deepest_table(Workspace const& w, int l);
+Table dec_table(Workspace const& w, int l);
+
+// Network forward on the feature image in w.feat; result in w.unet.  With
+// `keep` every activation the backward pass reads is stored; without it the
+// output convolution is folded into the last decoder convolution.
+sil_status net_forward(Net& net, Workspace& w, cudaStream_t st, bool keep)
 {
     int const D = static_cast<int>(w.levels.size());
     int* err = net.error_flag;
@@ -1264,46 +1605,46 @@ sil_status net_forward(Net& net, Workspace& w, cudaStream_t st)
     for (int l = 1; l < D; ++l) {
         int const wl = weight_level_enc(l);
         Table const t = w.table(l, l - 1, true);
-        sil_status s = launch_conv(st, t, kPool, w.h[l - 1].as<bf16>(), nullptr, nullptr, big_w(net, kDown, wl),
+        pool_kernel<<<image_grid(t, 1, 0), 256, 0, st>>>(t, w.h[l - 1].as<bf16>(), w.pin[l].as<bf16>());
+        SIL_CUDA_CHECK(cudaGetLastError());
+        Table const t2 = w.table(l, -1, false);
+        sil_status s = launch_conv(st, t2, kPlain, w.pin[l].as<bf16>(), nullptr, nullptr, big_w(net, kDown, wl),
                                    big_b(net, kDown, wl), 1, w.p[l].as<bf16>(), nullptr, 0, err);
         if (s != SIL_OK) return s;
-        Table const t2 = w.table(l, -1, false);
         s = launch_conv(st, t2, kPlain, w.p[l].as<bf16>(), nullptr, nullptr, big_w(net, kEnc, wl), big_b(net, kEnc, wl),
                         1, w.h[l].as<bf16>(), nullptr, 0, err);
         if (s != SIL_OK) return s;
     }
     // g at each image's deepest level is its h.
-    for (size_t i = 0; i < w.samples.size(); ++i) {
-        int const l = w.depth[i] - 1;
-        Level const& L = w.levels[l];
-        int const k = static_cast<int>(std::find(L.images.begin(), L.images.end(), static_cast<int>(i)) - L.images.begin());
-        int64_t const px = static_cast<int64_t>(L.img[k].h + 2) * (L.img[k].w + 2);
-        SIL_CUDA_CHECK(cudaMemcpyAsync(w.g[l].as<bf16>() + L.img[k].offset * kCh, w.h[l].as<bf16>() + L.img[k].offset * kCh,
-                                       px * kCh * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
-    }
-    for (int l = D - 2; l >= 0; --l) {
-        int const wl = weight_level_dec(l);
-        // images at level l that also have level l+1
-        Table t = w.table(l, l + 1, false);
-        Table tt {};
-        tt.nimg = 0;
-        tt.tile_base[0] = 0;
-        for (int k = 0; k < t.nimg; ++k) {
-            if (t.aux[k].h == 0) continue;
-            int const q = tt.nimg++;
-            tt.img[q] = t.img[k];
-            tt.aux[q] = t.aux[k];
-            tt.tile_base[q + 1] = tt.tile_base[q] + (t.tile_base[k + 1] - t.tile_base[k]);
-        }
-        sil_status const s = launch_conv(st, tt, kUpAdd, w.h[l].as<bf16>(), w.g[l + 1].as<bf16>(), nullptr,
-                                         big_w(net, kDec, wl), big_b(net, kDec, wl), 1, w.g[l].as<bf16>(), nullptr, 0, err);
-        if (s != SIL_OK) return s;
-    }
-    {
-        Table const t = w.table(0, -1, false);
-        out_forward_kernel<<<image_grid(t, 1, 0), 256, 0, st>>>(t, w.g[0].as<bf16>(), net.params, w.unet.as<float>());
+    for (int l = 0; l < D; ++l) {
+        Table const t = deepest_table(w, l);
+        if (t.nimg == 0) continue;
+        copy_act_kernel<<<image_grid(t, 4, 0), 256, 0, st>>>(t, w.h[l].as<bf16>(), w.g[l].as<bf16>());
         SIL_CUDA_CHECK(cudaGetLastError());
     }
+    int64_t const top = w.levels[0].npx;
+    for (int l = D - 2; l >= 0; --l) {
+        int const wl = weight_level_dec(l);
+        Table const tt = dec_table(w, l);
+        bool const fold = l == 0 && !keep;
+        sil_status const s = launch_conv(st, tt, kUpAdd, w.h[l].as<bf16>(), w.g[l + 1].as<bf16>(), nullptr,
+                                         big_w(net, kDec, wl), big_b(net, kDec, wl), 1, fold ? nullptr : w.g[l].as<bf16>(),
+                                         nullptr, 0, err, fold ? w.taps.as<float>() : nullptr, net.params + kOffOut, top);
+        if (s != SIL_OK) return s;
+    }
+    if (keep) {
+        Table const t = w.table(0, -1, false);
+        out_forward_kernel<<<image_grid(t, 1, 0), 256, 0, st>>>(t, w.g[0].as<bf16>(), net.params, w.unet.as<float>());
+    } else {
+        Table const td = dec_table(w, 0);
+        if (td.nimg > 0)
+            out_gather_kernel<<<image_grid(td, 1, 0), 256, 0, st>>>(td, w.taps.as<float>(), top, net.params,
+                                                                   w.unet.as<float>());
+        Table const t1 = deepest_table(w, 0);  // single-level images: no decoder
+        if (t1.nimg > 0)
+            out_forward_kernel<<<image_grid(t1, 1, 0), 256, 0, st>>>(t1, w.g[0].as<bf16>(), net.params, w.unet.as<float>());
+    }
+    SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
 
@@ -1321,6 +1662,21 @@ Table dec_table(Workspace const& w, int l)
         tt.tile_base[q + 1] = tt.tile_base[q] + (t.tile_base[k + 1] - t.tile_base[k]);
     }
     return tt;
+}
+
+// Images whose deepest level is l.
+Table deepest_table(Workspace const& w, int l)
+{
+    Table t {};
+    Level const& L = w.levels[l];
+    for (size_t k = 0; k < L.images.size(); ++k) {
+        if (w.depth[L.images[k]] - 1 != l) continue;
+        int const q = t.nimg++;
+        t.img[q] = L.img[k];
+        t.aux[q] = L.img[k];
+        t.tile_base[q + 1] = t.tile_base[q];
+    }
+    return t;
 }
 
 sil_status wgrad(Net& net, Workspace& w, cudaStream_t st, Table const& t, int mode, bf16 const* in, bf16 const* in2,
@@ -1376,15 +1732,9 @@ sil_status net_backward(Net& net, Workspace& w, cudaStream_t st)
         SIL_CUDA_CHECK(cudaGetLastError());
     }
     // deepest level of each image: g = h
-    for (size_t i = 0; i < w.samples.size(); ++i) {
-        int const l = w.depth[i] - 1;
-        Level const& L = w.levels[l];
-        int const k = static_cast<int>(std::find(L.images.begin(), L.images.end(), static_cast<int>(i)) - L.images.begin());
-        Table t {};
-        t.nimg = 1;
-        t.img[0] = L.img[k];
-        t.aux[0] = L.img[k];
-        // dh += dg over this image (reuse the skip adjoint kernel)
+    for (int l = 0; l < D; ++l) {
+        Table const t = deepest_table(w, l);
+        if (t.nimg == 0) continue;
         upadd_adjoint_skip_kernel<<<image_grid(t, 8, 0), 256, 0, st>>>(t, w.dg[l].as<float>(), w.dh[l].as<float>());
         SIL_CUDA_CHECK(cudaGetLastError());
     }
@@ -1399,7 +1749,7 @@ sil_status net_backward(Net& net, Workspace& w, cudaStream_t st)
                         nullptr, 0, nullptr, w.dx[l].as<float>(), 0, err);
         if (s != SIL_OK) return s;
         Table const tp = w.table(l, l - 1, true);
-        s = wgrad(net, w, st, tp, kPool, w.h[l - 1].as<bf16>(), nullptr, w.dx[l].as<float>(), w.p[l].as<bf16>(),
+        s = wgrad(net, w, st, t, kPlain, w.pin[l].as<bf16>(), nullptr, w.dx[l].as<float>(), w.p[l].as<bf16>(),
                   big_grad(net, kDown, wl));
         if (s != SIL_OK) return s;
         // data gradient of the down convolution into dg[l] (scratch), then pool adjoint into dh[l-1]
@@ -1424,24 +1774,27 @@ sil_status net_backward(Net& net, Workspace& w, cudaStream_t st)
     return SIL_OK;
 }
 
-// Preconditioner forward: w.u = M(b).  nu is read from w.fnu.
-sil_status precond_forward(Net& net, Workspace& w, float const* b, cudaStream_t st)
+// Preconditioner forward: out = M(b) for the batch of w (nu per node).
+// dinv: the inverse operator diagonal, or NULL to compute it here.
+sil_status precond_forward(Net& net, Workspace& w, float const* nu, float const* dinv, float const* b, float* out,
+                           cudaStream_t st, bool keep = false)
 {
-    dim3 const ng = node_grid(w);
-    float const* nu = w.fnu.as<float>();
-    dinv_kernel<<<ng, 256, 0, st>>>(w.ss, nu, w.dinv.as<float>());
-    jacobi_kernel<<<ng, 256, 0, st>>>(w.ss, nu, w.dinv.as<float>(), b, nullptr, nullptr, kOmega, w.e1.as<float>());
-    residual_kernel<<<ng, 256, 0, st>>>(w.ss, nu, b, w.e1.as<float>(), w.r1.as<float>());
+    if (dinv == nullptr) {
+        dinv_kernel<<<node_grid(w), 256, 0, st>>>(w.ss, nu, w.dinv.as<float>());
+        dinv = w.dinv.as<float>();
+    }
+    WrapItem const* items = w.witems.as<WrapItem>();
+    wrap_pre_kernel<<<w.nwitems, 256, 0, st>>>(w.ss, items, nu, dinv, b, w.e1.as<float>(), w.r1.as<float>(),
+                                               w.wpart.as<double>());
+    wrap_finish_kernel<<<1, 64, 0, st>>>(w.ss, w.wpart.as<double>(), w.dots.as<double>());
     SIL_CUDA_CHECK(cudaGetLastError());
-    sil_status s = dots(w, st, 0, w.r1.as<float>(), w.r1.as<float>(), nullptr, nullptr, nullptr, nullptr);
-    if (s != SIL_OK) return s;
-    features_kernel<<<top_grid(w), 256, 0, st>>>(w.ss, w.r1.as<float>(), nu, w.dots.as<double>(), w.feat.as<float>());
+    features_kernel<<<top_grid(w), 256, 0, st>>>(w.ss, w.r1.as<float>(), nu, dinv, w.dots.as<double>(),
+                                                 w.feat.as<float>());
     SIL_CUDA_CHECK(cudaGetLastError());
-    s = net_forward(net, w, st);
+    sil_status s = net_forward(net, w, st, keep);
     if (s != SIL_OK) return s;
-    correction_kernel<<<ng, 256, 0, st>>>(w.ss, w.e1.as<float>(), w.unet.as<float>(), w.dots.as<double>(), w.e2.as<float>());
-    jacobi_kernel<<<ng, 256, 0, st>>>(w.ss, nu, w.dinv.as<float>(), b, w.e2.as<float>(), w.e2.as<float>(), kOmega,
-                                      w.u.as<float>());
+    wrap_post_kernel<<<w.nwitems, 256, 0, st>>>(w.ss, items, nu, dinv, b, w.e1.as<float>(), w.unet.as<float>(),
+                                                w.dots.as<double>(), out);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
@@ -1463,11 +1816,22 @@ sil_status Net::apply(std::vector<Sample> const& samples, float const* nu, float
     sil_status st = SIL_OK;
     Workspace* w = workspace(samples, stream, &st);
     if (w == nullptr) return st;
-    SIL_CUDA_CHECK(cudaMemcpyAsync(w->fnu.p, nu, sizeof(float) * w->nodes, cudaMemcpyDeviceToDevice, stream));
-    st = precond_forward(*this, *w, r, stream);
-    if (st != SIL_OK) return st;
-    SIL_CUDA_CHECK(cudaMemcpyAsync(out, w->u.p, sizeof(float) * w->nodes, cudaMemcpyDeviceToDevice, stream));
-    return SIL_OK;
+    return precond_forward(*this, *w, nu, nullptr, r, out, stream);
+}
+
+sil_status Net::prepare(std::vector<Sample> const& samples, cudaStream_t stream, Workspace** out)
+{
+    if (sil_status s = check_samples(samples); s != SIL_OK) return s;
+    if (sil_status s = ensure_attributes(); s != SIL_OK) return s;
+    sil_status st = SIL_OK;
+    *out = workspace(samples, stream, &st);
+    return *out == nullptr ? st : SIL_OK;
+}
+
+sil_status Net::forward(Workspace* w, float const* nu, float const* dinv, float const* r, float* out,
+                        cudaStream_t stream)
+{
+    return precond_forward(*this, *w, nu, dinv, r, out, stream);
 }
 
 sil_status Net::loss_grad(std::vector<Sample> const& samples, float const* nu, float const* b, float const* x,
@@ -1479,12 +1843,11 @@ sil_status Net::loss_grad(std::vector<Sample> const& samples, float const* nu, f
     Workspace* w = workspace(samples, stream, &st);
     if (w == nullptr) return st;
     int const n = static_cast<int>(samples.size());
-    SIL_CUDA_CHECK(cudaMemcpyAsync(w->fnu.p, nu, sizeof(float) * w->nodes, cudaMemcpyDeviceToDevice, stream));
     SIL_CUDA_CHECK(cudaMemsetAsync(grad, 0, sizeof(float) * kNumParams, stream));
-    st = precond_forward(*this, *w, b, stream);
+    st = precond_forward(*this, *w, nu, nullptr, b, w->u.as<float>(), stream, true);
     if (st != SIL_OK) return st;
     dim3 const ng = node_grid(*w);
-    float const* fnu = w->fnu.as<float>();
+    float const* fnu = nu;
     kapply_kernel<<<ng, 256, 0, stream>>>(w->ss, fnu, w->u.as<float>(), w->ku.as<float>());
     SIL_CUDA_CHECK(cudaGetLastError());
     // set 1: u.b, u.Ku ; set 2: x.b
@@ -1499,7 +1862,8 @@ sil_status Net::loss_grad(std::vector<Sample> const& samples, float const* nu, f
                                           w->tmp.as<float>());
     kapply_kernel<<<ng, 256, 0, stream>>>(w->ss, fnu, w->tmp.as<float>(), w->ge2.as<float>());
     axpby_kernel<<<ng, 256, 0, stream>>>(w->ss, 1.0f, w->gu.as<float>(), -kOmega, w->ge2.as<float>(), w->ge2.as<float>());
-    net_grad_kernel<<<top_grid(*w), 256, 0, stream>>>(w->ss, w->ge2.as<float>(), d, w->gnet.as<float>());
+    net_grad_kernel<<<top_grid(*w), 256, 0, stream>>>(w->ss, w->ge2.as<float>(), w->dinv.as<float>(), d,
+                                                      w->gnet.as<float>());
     SIL_CUDA_CHECK(cudaGetLastError());
     st = net_backward(*this, *w, stream);
     if (st != SIL_OK) return st;

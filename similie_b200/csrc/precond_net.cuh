@@ -5,9 +5,12 @@
 // Preconditioner M(r) for a batch of residuals (FP32, node grids x fastest):
 //   e1 = w D^-1 r                      (Jacobi step, w = 0.8)
 //   r1 = r - K e1
-//   s  = rms(r1)
-//   x  = pool2x2([r1 / s, log(nu) / log(1000)])      (2-channel image, half resolution)
-//   v  = s * up2x2(net(x)), zero on the Dirichlet boundary
+//   s  = rms(D^-1/2 r1)
+//   x  = pool2x2([D^-1/2 r1 / s, log(nu) / log(1000)])   (2-channel image, half resolution)
+//   v  = s * D^-1/2 up2x2(net(x)), zero on the Dirichlet boundary
+// The symmetric diagonal scaling carries the 1/nu amplitude of the error in
+// low-reluctivity (high-permeability) regions, so the network sees an
+// operator of much lower contrast.
 //   e2 = e1 + v
 //   M(r) = e2 + w D^-1 (r - K e2)      (Jacobi step)
 // The network is a U-Net over levels of halving resolution down to a
@@ -72,6 +75,12 @@ public:
     // Refresh the BF16 copies after the master weights changed.
     sil_status refresh(cudaStream_t stream);
 
+    // Workspace of a batch geometry (allocated once, before any stream capture).
+    sil_status prepare(std::vector<Sample> const& samples, cudaStream_t stream, Workspace** out);
+    // out = M(r) on a prepared workspace: kernel launches only (capturable).
+    // dinv: inverse operator diagonal per node (FP32), or NULL.
+    sil_status forward(Workspace* w, float const* nu, float const* dinv, float const* r, float* out,
+                       cudaStream_t stream);
     // out = M(r) for a batch (device FP32 node arrays, nu FP32 per node).
     sil_status apply(std::vector<Sample> const& samples, float const* nu, float const* r, float* out, cudaStream_t stream);
     // Loss 1 - (u.b)^2 / ((u.K u)(x.b)) with u = M(b), mean over the batch,
