@@ -190,32 +190,43 @@ typedef struct sil_mag2d_problem {
     double* solution;        /* device, nx*ny: written (initial guess is 0) */
 } sil_mag2d_problem;
 
-/* Both kinds refine on the FP64 true residual r = b - A x: an inner
- * Jacobi-preconditioned CG solve of A e = r, x += e, until
- * ||b - A x|| <= tol ||b|| in FP64.  CG_F64 runs the inner CG in FP64 to half
- * the tolerance (further passes only correct recurrence drift); MIXED_IR runs
- * it in FP32 to `inner_tolerance` per pass (dot products in FP64). */
+/* Every kind refines on the FP64 true residual r = b - A x: an inner solve
+ * of A e = r, x += e, until ||b - A x|| <= tol ||b|| in FP64.  CG_F64 runs a
+ * Jacobi-preconditioned CG in FP64 to half the tolerance (further passes only
+ * correct recurrence drift); MIXED_IR runs it in FP32 to `inner_tolerance`
+ * per pass (dot products in FP64).  LEARNED (2D only, at most 64 problems per call) runs a flexible CG in FP32
+ * preconditioned by the learned network (`preconditioner`) inside FP64
+ * refinement passes, and hands a problem to the MIXED_IR solver when its
+ * preconditioned residual stalls (less than a 10x reduction over
+ * `stall_window` iterations) or its inner solve runs out of iterations. */
 typedef enum sil_solver_kind {
     SIL_SOLVER_CG_F64 = 0,
-    SIL_SOLVER_MIXED_IR = 1
+    SIL_SOLVER_MIXED_IR = 1,
+    SIL_SOLVER_LEARNED = 2
 } sil_solver_kind;
+
+typedef struct sil_precond_s* sil_precond;
 
 typedef struct sil_solve_settings {
     int32_t solver;              /* sil_solver_kind */
     int32_t max_iterations;      /* total inner iterations per problem */
     double relative_tolerance;   /* stop when ||b - A x|| <= tol * ||b|| */
-    int32_t inner_iterations;    /* mixed: inner iterations per refinement step */
-    double inner_tolerance;      /* mixed: inner relative reduction per step */
+    int32_t inner_iterations;    /* MIXED_IR / LEARNED: inner iterations per refinement pass */
+    double inner_tolerance;      /* MIXED_IR / LEARNED: inner relative reduction per pass */
+    sil_precond preconditioner;  /* LEARNED: the trained network */
+    int32_t stall_window;        /* LEARNED: iterations per stall check (0: 100) */
 } sil_solve_settings;
 
 typedef struct sil_solve_diagnostics {
-    int32_t iterations;
+    int32_t iterations;          /* inner iterations, all stages together */
     int32_t converged;
-    int32_t refinements;
+    int32_t refinements;         /* FP64 refinement passes */
     int32_t status;              /* sil_status of this problem */
     double initial_residual_l2;
     double final_residual_l2;
     double final_relative_residual;
+    int32_t learned_iterations;  /* LEARNED: iterations of the preconditioned solve */
+    int32_t fallback;            /* LEARNED: 1 if the plain solver finished the problem */
 } sil_solve_diagnostics;
 
 /* Solve a batch of independent problems on one device stream.  Writes one
@@ -238,7 +249,7 @@ sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblem
 /* The reference has no learned preconditioner; the entry points below are  */
 /* the sil_precond_load/train/save family of its GPU design.                 */
 
-typedef struct sil_precond_s* sil_precond;
+/* (sil_precond is declared with the solver settings above.) */
 
 /* One node grid of a batch: nx x ny nodes, x fastest, starting at element
  * `offset` of the batch's flat FP32 node arrays (nu = 1/mu, r, b, x, out). */

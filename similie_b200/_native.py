@@ -73,6 +73,8 @@ class SilSolveSettings(ctypes.Structure):
         ("relative_tolerance", ctypes.c_double),
         ("inner_iterations", ctypes.c_int32),
         ("inner_tolerance", ctypes.c_double),
+        ("preconditioner", ctypes.c_void_p),
+        ("stall_window", ctypes.c_int32),
     ]
 
 
@@ -85,6 +87,8 @@ class SilSolveDiagnostics(ctypes.Structure):
         ("initial_residual_l2", ctypes.c_double),
         ("final_residual_l2", ctypes.c_double),
         ("final_relative_residual", ctypes.c_double),
+        ("learned_iterations", ctypes.c_int32),
+        ("fallback", ctypes.c_int32),
     ]
 
 

@@ -18,10 +18,13 @@
 // ||r|| <= tol ||b||; the final residual is re-evaluated in FP64.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <type_traits>
 #include <mutex>
 #include <vector>
 
 #include "mag_ops.cuh"
+#include "precond_net.cuh"
 #include "sil_internal.cuh"
 
 namespace sil {
@@ -256,6 +259,12 @@ struct Scalars
     int total_iters;  // all inner iterations
     int nonfinite;
     int counter_a, counter_b, counter_c;
+    // flexible CG with the learned preconditioner
+    double pq;        // p . q of the current direction
+    double win_rr;    // r . r at the start of the stall window
+    int win_iters;    // iterations into the stall window
+    int fallback;     // 1: the plain solver takes over this problem
+    int learned_iters;
 };
 
 // Deterministic block sum of one double per thread.
@@ -424,6 +433,160 @@ __global__ void __launch_bounds__(kThreads) cg_direction_kernel(Item const* item
     for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) v.p[row] = v.z[row] + beta * v.p[row];
 }
 
+// ------------------------------------------------------------------ flexible CG (learned preconditioner)
+//
+// Notay's flexible CG with one-step truncation: alpha = (p.r)/(p.q),
+// beta = -(z.q)/(p.q), z = M(r) from the learned preconditioner, which is not
+// a fixed linear operator.  A problem whose residual has not dropped 10x over
+// `window` iterations is marked for the plain solver.
+
+// x = 0, r = r64 / scale (precision T), rr0 = r.r; stall window reset.
+// Problems already handed to the plain solver get a zero correction.
+template <class T>
+__global__ void __launch_bounds__(kThreads) fcg_init_kernel(Item const* items, ProbInfo const* info,
+                                                            Vecs<T> const* vecs, double const* const* r64,
+                                                            Scalars* sc, double* part)
+{
+    __shared__ double red[kThreads / 32];
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->outer_done) return;
+    Vecs<T> const v = vecs[it.prob];
+    if (s->fallback) {
+        for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) v.x[row] = T(0);
+        return;
+    }
+    ProbInfo const pi = info[it.prob];
+    double const scale = s->scale;
+    double rr = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        T const r = static_cast<T>(r64[it.prob][row] / scale);
+        v.x[row] = T(0);
+        v.r[row] = r;
+        rr += static_cast<double>(r) * static_cast<double>(r);
+    }
+    double const rr_b = block_sum(rr, red);
+    double tot = 0.0;
+    if (finish_reduction(rr_b, part, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot)) {
+        s->rr = tot;
+        s->rr0 = tot;
+        s->win_rr = tot;
+        s->win_iters = 0;
+        s->iters = 0;
+        s->done = (tot == 0.0) ? 1 : 0;
+        s->nonfinite = 0;
+    }
+}
+
+// p = z for the first direction.
+template <class T>
+__global__ void __launch_bounds__(kThreads) fcg_first_direction_kernel(Item const* items, Vecs<T> const* vecs,
+                                                                       Scalars const* sc)
+{
+    Item const it = items[blockIdx.x];
+    Scalars const* s = sc + it.prob;
+    if (s->done || s->outer_done || s->fallback) return;
+    Vecs<T> const v = vecs[it.prob];
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) v.p[row] = v.z[row];
+}
+
+// q = A p, partials p.q and p.r; the last CTA forms alpha.
+template <class T>
+__global__ void __launch_bounds__(kThreads) fcg_apply_kernel(Item const* items, ProbInfo const* info,
+                                                             Vecs<T> const* vecs, Scalars* sc, double* part_a,
+                                                             double* part_b)
+{
+    __shared__ double red[kThreads / 32];
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->done || s->outer_done || s->fallback) return;
+    ProbInfo const pi = info[it.prob];
+    Vecs<T> const v = vecs[it.prob];
+    double pq = 0.0, pr = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        T const q = mag_apply_row(v.p, v.nu, pi, row);
+        v.q[row] = q;
+        double const pv = static_cast<double>(v.p[row]);
+        pq += pv * static_cast<double>(q);
+        pr += pv * static_cast<double>(v.r[row]);
+    }
+    double const pq_b = block_sum(pq, red);
+    double const pr_b = block_sum(pr, red);
+    double tot_pq = 0.0, tot_pr = 0.0;
+    finish_reduction(pq_b, part_a, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot_pq);
+    if (finish_reduction(pr_b, part_b, it.index, pi.first_item, pi.nitems, &s->counter_b, &tot_pr)) {
+        __threadfence();
+        double tpq = 0.0;
+        for (int k = 0; k < pi.nitems; ++k) tpq += __ldcg(part_a + pi.first_item + k);
+        s->pq = tpq;
+        s->alpha = tot_pr / tpq;
+        if (!isfinite(s->alpha)) s->nonfinite = 1;
+    }
+}
+
+// x += alpha p, r -= alpha q, partial r.r; the last CTA checks convergence
+// and the stall window.
+template <class T>
+__global__ void __launch_bounds__(kThreads) fcg_update_kernel(Item const* items, ProbInfo const* info,
+                                                              Vecs<T> const* vecs, Scalars* sc, double* part,
+                                                              int window)
+{
+    __shared__ double red[kThreads / 32];
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->done || s->outer_done || s->fallback) return;
+    ProbInfo const pi = info[it.prob];
+    Vecs<T> const v = vecs[it.prob];
+    T const alpha = static_cast<T>(s->alpha);
+    double rr = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        T const r = v.r[row] - alpha * v.q[row];
+        v.x[row] = v.x[row] + alpha * v.p[row];
+        v.r[row] = r;
+        rr += static_cast<double>(r) * static_cast<double>(r);
+    }
+    double const rr_b = block_sum(rr, red);
+    double tot = 0.0;
+    if (finish_reduction(rr_b, part, it.index, pi.first_item, pi.nitems, &s->counter_c, &tot)) {
+        s->rr = tot;
+        s->iters += 1;
+        s->total_iters += 1;
+        s->learned_iters += 1;
+        if (!isfinite(tot)) s->nonfinite = 1;
+        if (tot <= s->inner_tol2 * s->rr0 || s->nonfinite) s->done = 1;
+        if (++s->win_iters >= window) {
+            if (!(tot <= 0.01 * s->win_rr)) {
+                s->fallback = 1;
+                s->done = 1;
+            }
+            s->win_rr = tot;
+            s->win_iters = 0;
+        }
+    }
+}
+
+// Partial z.q; the last CTA forms beta = -(z.q)/(p.q).
+template <class T>
+__global__ void __launch_bounds__(kThreads) fcg_beta_kernel(Item const* items, ProbInfo const* info,
+                                                            Vecs<T> const* vecs, Scalars* sc, double* part)
+{
+    __shared__ double red[kThreads / 32];
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->done || s->outer_done || s->fallback) return;
+    ProbInfo const pi = info[it.prob];
+    Vecs<T> const v = vecs[it.prob];
+    double zq = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads)
+        zq += static_cast<double>(v.z[row]) * static_cast<double>(v.q[row]);
+    double const zq_b = block_sum(zq, red);
+    double tot = 0.0;
+    if (finish_reduction(zq_b, part, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot)) {
+        s->beta = -tot / s->pq;
+        if (!isfinite(s->beta)) s->nonfinite = 1;
+    }
+}
+
 // r64 = b - A x64 and its norm (outer residual, FP64); marks outer convergence.
 __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items, ProbInfo const* info,
                                                               double const* const* nu64, double const* const* rhs,
@@ -540,7 +703,7 @@ double local_spacing(double const* c, int64_t n, int64_t i)
 
 template <class T>
 sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings const& set, sil_solve_diagnostics* diag,
-                       cudaStream_t stream)
+                       cudaStream_t stream, nn::Net* learned = nullptr)
 {
     int const np = static_cast<int>(probs.size());
     // Work items: contiguous row ranges of kItemNodes per problem.
@@ -700,11 +863,11 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         if (err != cudaSuccess) return cuda_fail(err, "solver graph capture");
         return SIL_OK;
     };
-    auto run_until_done = [&](int budget, int* used) -> sil_status {
+    auto run_graph_until_done = [&](cudaGraphExec_t gexec, int gchunk, int budget, int* used) -> sil_status {
         int spent = 0;
         while (spent < budget) {
-            SIL_CUDA_CHECK(cudaGraphLaunch(exec, stream));
-            spent += chunk;
+            SIL_CUDA_CHECK(cudaGraphLaunch(gexec, stream));
+            spent += gchunk;
             SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
             SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
             bool all = true;
@@ -713,6 +876,9 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         }
         *used = spent;
         return SIL_OK;
+    };
+    auto run_until_done = [&](int budget, int* used) -> sil_status {
+        return run_graph_until_done(exec, chunk, budget, used);
     };
 
     // Iterative refinement on the FP64 residual: r = b - A x (FP64), an inner
@@ -728,10 +894,97 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     int const inner_max = low ? (set.inner_iterations > 0 ? set.inner_iterations : 4000) : max_iter;
     st = capture(0.0);
     SIL_CUDA_CHECK(cudaMemsetAsync(x64_base, 0, d_bytes, stream));
+
+    // Refinement passes whose inner solve is the flexible CG preconditioned by
+    // the learned network, until every problem has converged or been handed to
+    // the plain solver (stall or budget).
+    auto learned_stage = [&](nn::Net* net, int* total_out, int* refinements_out) -> sil_status {
+        if constexpr (!std::is_same_v<T, float>) {
+            return fail(SIL_ERR_UNSUPPORTED, "learned solve runs in FP32");
+        } else {
+            std::vector<nn::Sample> samples(np);
+            int64_t o = 0;
+            for (int p = 0; p < np; ++p) {
+                if (info[p].dim != 2) return fail(SIL_ERR_UNSUPPORTED, "learned solve: 2D problems only");
+                samples[p] = {static_cast<int32_t>(info[p].nx), static_cast<int32_t>(info[p].ny), o};
+                o += info[p].n;
+            }
+            nn::Workspace* ws = nullptr;
+            sil_status lst = net->prepare(samples, stream, &ws);
+            if (lst != SIL_OK) return lst;
+            float const* nuf = vec_base[6];
+            float const* dv = vec_base[5];
+            float* rv = vec_base[1];
+            float* zv = vec_base[2];
+            int const window = set.stall_window > 0 ? set.stall_window : 100;
+            double const ltol = set.inner_tolerance > 0 ? set.inner_tolerance : 1e-5;
+            int const lmax = set.inner_iterations > 0 ? set.inner_iterations : 4000;
+            int const lchunk = 8;
+            cudaGraph_t lgraph = nullptr;
+            cudaGraphExec_t lexec = nullptr;
+            {
+                cudaStream_t cs;
+                SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+                cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+                for (int c = 0; c < lchunk && err == cudaSuccess && lst == SIL_OK; ++c) {
+                    fcg_apply_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a, part_b);
+                    fcg_update_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_c, window);
+                    lst = net->forward(ws, nuf, dv, rv, zv, cs);
+                    fcg_beta_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a);
+                    cg_direction_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc);
+                }
+                cudaError_t const err2 = cudaStreamEndCapture(cs, &lgraph);
+                if (err == cudaSuccess) err = err2;
+                if (err == cudaSuccess && lst == SIL_OK) err = cudaGraphInstantiate(&lexec, lgraph, 0);
+                cudaStreamDestroy(cs);
+                if (lst == SIL_OK && err != cudaSuccess) lst = cuda_fail(err, "learned solver graph capture");
+            }
+            int tot = 0;
+            while (lst == SIL_OK && tot < max_iter) {
+                residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc,
+                                                                   part_a, tol * tol, ltol * ltol, 1);
+                SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
+                SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+                bool active = false;
+                for (int p = 0; p < np; ++p) active = active || (!hs[p].outer_done && !hs[p].fallback);
+                if (!active) break;
+                fcg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, d_r64, d_sc, part_a);
+                lst = net->forward(ws, nuf, dv, rv, zv, stream);
+                if (lst != SIL_OK) break;
+                fcg_first_direction_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_sc);
+                SIL_CUDA_CHECK(cudaGetLastError());
+                int used = 0;
+                lst = run_graph_until_done(lexec, lchunk, std::min(lmax, max_iter - tot), &used);
+                tot += used;
+                // A problem still unconverged after a full inner budget goes to the plain solver.
+                SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
+                SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+                bool flagged = false;
+                for (int p = 0; p < np; ++p) {
+                    if (!hs[p].outer_done && !hs[p].fallback && !hs[p].done) {
+                        hs[p].fallback = 1;
+                        flagged = true;
+                    }
+                }
+                refine_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_x64, d_sc);
+                if (flagged) {
+                    SIL_CUDA_CHECK(cudaMemcpyAsync(d_sc, hs.data(), sizeof(Scalars) * np, cudaMemcpyHostToDevice, stream));
+                }
+                ++*refinements_out;
+            }
+            if (lexec != nullptr) cudaGraphExecDestroy(lexec);
+            if (lgraph != nullptr) cudaGraphDestroy(lgraph);
+            *total_out = tot;
+            return lst;
+        }
+    };
     // bb = ||b||^2 via an init pass from the right-hand side.
     cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, d_rhs, nullptr, d_sc, part_a, part_b,
                                                        false);
     int total = 0;
+    if constexpr (std::is_same_v<T, float>) {
+        if (learned != nullptr && st == SIL_OK) st = learned_stage(learned, &total, &refinements);
+    }
     while (st == SIL_OK && total < max_iter) {
         residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc, part_a,
                                                            tol * tol, inner_tol * inner_tol, 1);
@@ -777,6 +1030,8 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         d.final_relative_residual = hs[p].bb > 0 ? std::sqrt(hs[p].rr / hs[p].bb) : 0.0;
         d.converged = d.final_relative_residual <= tol && !hs[p].nonfinite;
         d.status = hs[p].nonfinite ? SIL_ERR_NONFINITE : SIL_OK;
+        d.learned_iterations = hs[p].learned_iters;
+        d.fallback = hs[p].fallback;
         if (hs[p].nonfinite) overall = SIL_ERR_NONFINITE;
     }
     if (overall != SIL_OK) set_error("a problem of the batch met a non-finite value");
@@ -888,8 +1143,16 @@ sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblem
         descs[p] = {2, q.nx, q.ny, 1, 0.0, q.node_mu, q.rhs, q.solution, {nullptr, nullptr, nullptr}};
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::memset(diag, 0, sizeof(sil_solve_diagnostics) * nproblems);
     if (settings->solver == SIL_SOLVER_CG_F64) return solve_batch<double>(descs, *settings, diag, s);
     if (settings->solver == SIL_SOLVER_MIXED_IR) return solve_batch<float>(descs, *settings, diag, s);
+    if (settings->solver == SIL_SOLVER_LEARNED) {
+        if (settings->preconditioner == nullptr)
+            return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: the learned solver needs a preconditioner");
+        if (nproblems > nn::kMaxImages)
+            return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: the learned solver takes at most 64 problems per call");
+        return solve_batch<float>(descs, *settings, diag, s, &settings->preconditioner->net);
+    }
     return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: unknown solver kind");
 }
 
@@ -992,9 +1255,10 @@ sil_status sil_mag3d_solve_batch(const sil_mag3d_problem* problems, int nproblem
         descs[p] = {3, q.nx, q.ny, q.nz, q.gauge_penalty, q.node_mu, q.rhs, q.solution, {q.x, q.y, q.z}};
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::memset(diag, 0, sizeof(sil_solve_diagnostics) * nproblems);
     if (settings->solver == SIL_SOLVER_CG_F64) return solve_batch<double>(descs, *settings, diag, s);
     if (settings->solver == SIL_SOLVER_MIXED_IR) return solve_batch<float>(descs, *settings, diag, s);
-    return fail(SIL_ERR_INVALID, "sil_mag3d_solve_batch: unknown solver kind");
+    return fail(SIL_ERR_INVALID, "sil_mag3d_solve_batch: unknown solver kind (the learned solver is 2D only)");
 }
 
 } // extern "C"

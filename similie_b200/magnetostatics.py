@@ -24,7 +24,7 @@ import numpy as np
 from . import _native
 from ._native import check, lib
 
-SOLVERS = {"cg": 0, "mixed": 1}
+SOLVERS = {"cg": 0, "mixed": 1, "learned": 2}
 
 
 def node_mu(nx, ny, cell_mu, mu0=1.0):
@@ -130,14 +130,20 @@ class Diagnostics:
     initial_residual_l2: float
     final_residual_l2: float
     final_relative_residual: float
+    learned_iterations: int = 0
+    fallback: bool = False
 
 
 def solve_batch(mus, rhss, sols, shapes, solver="cg", tol=1e-10, max_iterations=200000, inner_iterations=4000,
-                inner_tolerance=1e-4, stream=None):
+                inner_tolerance=1e-4, stream=None, preconditioner=None, stall_window=100):
     """minimize_strong_formulation_residual for a batch of linear problems.
 
     mus, rhss, sols: lists of torch CUDA float64 tensors (flat nx*ny);
-    shapes: list of (nx, ny).  Returns one Diagnostics per problem."""
+    shapes: list of (nx, ny).  solver: "cg" (FP64), "mixed" (FP32 inner CG
+    inside FP64 refinement) or "learned" (flexible CG with `preconditioner`, a
+    similie_b200.precond.LearnedPreconditioner, at most 64 problems, then the
+    mixed solver for problems whose preconditioned residual stalls).
+    Returns one Diagnostics per problem."""
     import torch
     n = len(shapes)
     probs = (_native.SilMag2dProblem * n)()
@@ -152,10 +158,14 @@ def solve_batch(mus, rhss, sols, shapes, solver="cg", tol=1e-10, max_iterations=
     st.relative_tolerance = tol
     st.inner_iterations = inner_iterations
     st.inner_tolerance = inner_tolerance
+    st.stall_window = stall_window
+    if preconditioner is not None:
+        st.preconditioner = preconditioner._h.value
     diag = (_native.SilSolveDiagnostics * n)()
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
     rc = lib().sil_mag2d_solve_batch(probs, n, ctypes.byref(st), diag, s)
     out = [Diagnostics(d.iterations, bool(d.converged), d.refinements, d.status, d.initial_residual_l2,
-                       d.final_residual_l2, d.final_relative_residual) for d in diag]
+                       d.final_residual_l2, d.final_relative_residual, d.learned_iterations, bool(d.fallback))
+           for d in diag]
     check(rc, "mag2d_solve_batch")
     return out

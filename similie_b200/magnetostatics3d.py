@@ -191,6 +191,7 @@ def solve_batch(coords, mus, rhss, sols, gammas=None, solver="cg", tol=1e-10, ma
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
     rc = lib().sil_mag3d_solve_batch(probs, n, ctypes.byref(st), diag, s)
     out = [Diagnostics(d.iterations, bool(d.converged), d.refinements, d.status, d.initial_residual_l2,
-                       d.final_residual_l2, d.final_relative_residual) for d in diag]
+                       d.final_residual_l2, d.final_relative_residual, d.learned_iterations, bool(d.fallback))
+           for d in diag]
     check(rc, "mag3d_solve_batch")
     return out
