@@ -13,14 +13,16 @@
 namespace sil {
 
 template <class T>
-__device__ __forceinline__ T mag_apply_node(T const* a, T const* nu, int64_t nx, int64_t ny, int64_t row)
+__device__ __forceinline__ T mag_apply_node(T const* a, T const* nu, int64_t nx64, int64_t ny64, int64_t row64)
 {
-    int64_t const i = row % nx, j = row / nx;
+    // problems hold fewer than 2^31 nodes (checked by the entry points): 32-bit index arithmetic
+    int const nx = static_cast<int>(nx64), ny = static_cast<int>(ny64), row = static_cast<int>(row64);
+    int const j = row / nx, i = row - j * nx;
     if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) return a[row];
     T const a0 = a[row];
     T residual = T(0);
     if (j >= 2) {
-        int64_t const s = row - nx;
+        int const s = row - nx;
         T m0 = T(0);
         m0 = m0 - a[s];
         m0 = m0 + a0;
@@ -33,7 +35,7 @@ __device__ __forceinline__ T mag_apply_node(T const* a, T const* nu, int64_t nx,
         residual = residual - m0 * nu[row];  // c = -1
     }
     if (i >= 2) {
-        int64_t const s = row - 1;
+        int const s = row - 1;
         T m1 = T(0);
         m1 = m1 + a[s];
         m1 = m1 - a0;

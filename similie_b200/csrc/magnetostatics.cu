@@ -111,41 +111,46 @@ __device__ __forceinline__ T const* inv_spacing(ProbInfo const& pi, int axis)
 // B (d_m / (d_a d_b), central local spacings) and 1/mu(s); the gauge term is
 // gamma * (d_a d_b / d_c) * A.  Boundary rows are the identity.
 template <class T>
-__device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_t row)
+__device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_t row64)
 {
-    int64_t const node = row / 3;
-    int const c = static_cast<int>(row - 3 * node);
-    int64_t const nx = pi.nx, ny = pi.ny, nz = pi.nz;
-    int64_t const i = node % nx, t = node / nx, j = t % ny, k = t / ny;
-    auto interior = [&](int64_t ii, int64_t jj, int64_t kk) {
+    // fewer than 2^31 unknowns per problem (checked by the entry points)
+    int const row = static_cast<int>(row64);
+    int const node = row / 3;
+    int const c = row - 3 * node;
+    int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
+    int const t = node / nx, i = node - t * nx, k = t / ny, j = t - k * ny;
+    auto interior = [&](int ii, int jj, int kk) {
         return ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz;
     };
     if (!interior(i, j, k)) return a[row];
-    auto A = [&](int64_t ii, int64_t jj, int64_t kk, int cc) -> T {
-        return interior(ii, jj, kk) ? a[3 * (ii + nx * (jj + ny * kk)) + cc] : T(0);
+    int const sy = 3 * nx, sz = 3 * nx * ny;
+    // A at node (i, j, k) + offset, component cc; zero on the Dirichlet boundary
+    auto A = [&](int di, int dj, int dk, int cc) -> T {
+        return interior(i + di, j + dj, k + dk) ? a[row - c + 3 * di + sy * dj + sz * dk + cc] : T(0);
     };
-    auto bx = [&](int64_t ii, int64_t jj, int64_t kk) {
+    // curl moments at the sampled node (i, j, k) + (oi, oj, ok)
+    auto bx = [&](int oi, int oj, int ok) {
         T m = T(0);
-        m = m + A(ii, jj, kk, 1);
-        m = m - A(ii, jj, kk, 2);
-        m = m - A(ii, jj, kk + 1, 1);
-        m = m + A(ii, jj + 1, kk, 2);
+        m = m + A(oi, oj, ok, 1);
+        m = m - A(oi, oj, ok, 2);
+        m = m - A(oi, oj, ok + 1, 1);
+        m = m + A(oi, oj + 1, ok, 2);
         return m;
     };
-    auto by = [&](int64_t ii, int64_t jj, int64_t kk) {
+    auto by = [&](int oi, int oj, int ok) {
         T m = T(0);
-        m = m - A(ii, jj, kk, 0);
-        m = m + A(ii, jj, kk, 2);
-        m = m + A(ii, jj, kk + 1, 0);
-        m = m - A(ii + 1, jj, kk, 2);
+        m = m - A(oi, oj, ok, 0);
+        m = m + A(oi, oj, ok, 2);
+        m = m + A(oi, oj, ok + 1, 0);
+        m = m - A(oi + 1, oj, ok, 2);
         return m;
     };
-    auto bz = [&](int64_t ii, int64_t jj, int64_t kk) {
+    auto bz = [&](int oi, int oj, int ok) {
         T m = T(0);
-        m = m + A(ii, jj, kk, 0);
-        m = m - A(ii, jj, kk, 1);
-        m = m - A(ii, jj + 1, kk, 0);
-        m = m + A(ii + 1, jj, kk, 1);
+        m = m + A(oi, oj, ok, 0);
+        m = m - A(oi, oj, ok, 1);
+        m = m - A(oi, oj + 1, ok, 0);
+        m = m + A(oi + 1, oj, ok, 1);
         return m;
     };
     T const* lx = spacing<T>(pi, 0);
@@ -154,31 +159,32 @@ __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_
     T const* ilx = inv_spacing<T>(pi, 0);
     T const* ily = inv_spacing<T>(pi, 1);
     T const* ilz = inv_spacing<T>(pi, 2);
-    auto w = [&](int64_t ii, int64_t jj, int64_t kk, int m) -> T {
-        T const nuv = nu[ii + nx * (jj + ny * kk)];
-        if (m == 0) return lx[ii] * ily[jj] * ilz[kk] * nuv;
-        if (m == 1) return ly[jj] * ilx[ii] * ilz[kk] * nuv;
-        return lz[kk] * ilx[ii] * ily[jj] * nuv;
+    int const nd = node;
+    auto w = [&](int oi, int oj, int ok, int m) -> T {
+        T const nuv = nu[nd + oi + nx * oj + nx * ny * ok];
+        if (m == 0) return lx[i + oi] * ily[j + oj] * ilz[k + ok] * nuv;
+        if (m == 1) return ly[j + oj] * ilx[i + oi] * ilz[k + ok] * nuv;
+        return lz[k + ok] * ilx[i + oi] * ily[j + oj] * nuv;
     };
     T res = T(0);
     T ha;
     if (c == 0) {
-        res = res - w(i, j, k, 1) * by(i, j, k);
-        if (interior(i, j, k - 1)) res = res + w(i, j, k - 1, 1) * by(i, j, k - 1);
-        res = res + w(i, j, k, 2) * bz(i, j, k);
-        if (interior(i, j - 1, k)) res = res - w(i, j - 1, k, 2) * bz(i, j - 1, k);
+        res = res - w(0, 0, 0, 1) * by(0, 0, 0);
+        if (interior(i, j, k - 1)) res = res + w(0, 0, -1, 1) * by(0, 0, -1);
+        res = res + w(0, 0, 0, 2) * bz(0, 0, 0);
+        if (interior(i, j - 1, k)) res = res - w(0, -1, 0, 2) * bz(0, -1, 0);
         ha = ly[j] * lz[k] * ilx[i];
     } else if (c == 1) {
-        res = res + w(i, j, k, 0) * bx(i, j, k);
-        if (interior(i, j, k - 1)) res = res - w(i, j, k - 1, 0) * bx(i, j, k - 1);
-        res = res - w(i, j, k, 2) * bz(i, j, k);
-        if (interior(i - 1, j, k)) res = res + w(i - 1, j, k, 2) * bz(i - 1, j, k);
+        res = res + w(0, 0, 0, 0) * bx(0, 0, 0);
+        if (interior(i, j, k - 1)) res = res - w(0, 0, -1, 0) * bx(0, 0, -1);
+        res = res - w(0, 0, 0, 2) * bz(0, 0, 0);
+        if (interior(i - 1, j, k)) res = res + w(-1, 0, 0, 2) * bz(-1, 0, 0);
         ha = lx[i] * lz[k] * ily[j];
     } else {
-        res = res - w(i, j, k, 0) * bx(i, j, k);
-        if (interior(i, j - 1, k)) res = res + w(i, j - 1, k, 0) * bx(i, j - 1, k);
-        res = res + w(i, j, k, 1) * by(i, j, k);
-        if (interior(i - 1, j, k)) res = res - w(i - 1, j, k, 1) * by(i - 1, j, k);
+        res = res - w(0, 0, 0, 0) * bx(0, 0, 0);
+        if (interior(i, j - 1, k)) res = res + w(0, -1, 0, 0) * bx(0, -1, 0);
+        res = res + w(0, 0, 0, 1) * by(0, 0, 0);
+        if (interior(i - 1, j, k)) res = res - w(-1, 0, 0, 1) * by(-1, 0, 0);
         ha = lx[i] * ly[j] * ilz[k];
     }
     return res + static_cast<T>(pi.gamma) * ha * a[row];
@@ -282,30 +288,42 @@ __device__ __forceinline__ double block_sum(double v, double* smem)
     return t;  // valid in thread 0
 }
 
-// Last-CTA-of-the-problem reduction: returns true in the thread that must
-// finalize, with `out` holding the ordered sum of the problem's partials.
-__device__ bool finish_reduction(double partial, double* partials, int item_index, int first_item, int nitems,
-                                 int* counter, double* out)
+// Last-CTA-of-the-problem reduction of K sums: every CTA publishes its
+// partials (thread 0's vals) and counts in; the last CTA of the problem sums
+// all partials with the whole block, in a fixed order (deterministic), and
+// returns true in its thread 0 with `out` holding the K totals.
+template <int K>
+__device__ bool finish_reduction_k(double const* vals, double* const* parts, int item_index, int first_item, int nitems,
+                                   int* counter, double* out)
 {
-    __shared__ bool is_last;
+    __shared__ int is_last;
+    __shared__ double red[kThreads / 32];
     __syncthreads();
     if (threadIdx.x == 0) {
-        partials[first_item + item_index] = partial;
+        for (int k = 0; k < K; ++k) parts[k][first_item + item_index] = vals[k];
         __threadfence();
-        int const prev = atomicAdd(counter, 1);
-        is_last = prev == nitems - 1;
+        is_last = atomicAdd(counter, 1) == nitems - 1;
     }
     __syncthreads();
     if (!is_last) return false;
+    __threadfence();
+    for (int k = 0; k < K; ++k) {
+        double v = 0.0;
+        for (int j = threadIdx.x; j < nitems; j += kThreads) v += __ldcg(parts[k] + first_item + j);
+        out[k] = block_sum(v, red);
+    }
     if (threadIdx.x == 0) {
-        __threadfence();
-        double s = 0.0;
-        for (int k = 0; k < nitems; ++k) s += __ldcg(partials + first_item + k);
-        *out = s;
         *counter = 0;
         return true;
     }
     return false;
+}
+
+__device__ bool finish_reduction(double partial, double* partials, int item_index, int first_item, int nitems,
+                                 int* counter, double* out)
+{
+    double* parts[1] = {partials};
+    return finish_reduction_k<1>(&partial, parts, item_index, first_item, nitems, counter, out);
 }
 
 template <class T>
@@ -334,15 +352,11 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(Item const* items, Pr
     }
     double const rz_b = block_sum(rz, red);
     double const bb_b = block_sum(bb, red);
-    double tot_rz = 0.0, tot_bb = 0.0;
-    bool const last_a = finish_reduction(rz_b, part_a, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot_rz);
-    bool const last_b = finish_reduction(bb_b, part_b, it.index, pi.first_item, pi.nitems, &s->counter_b, &tot_bb);
-    (void)last_a;
-    if (last_b && threadIdx.x == 0) {
-        // Both reductions are complete once this CTA is the last of the second.
-        __threadfence();
-        double trz = 0.0;
-        for (int k = 0; k < pi.nitems; ++k) trz += __ldcg(part_a + pi.first_item + k);
+    double const vals[2] = {rz_b, bb_b};
+    double* parts[2] = {part_a, part_b};
+    double tot[2];
+    if (finish_reduction_k<2>(vals, parts, it.index, pi.first_item, pi.nitems, &s->counter_a, tot)) {
+        double const trz = tot[0], tot_bb = tot[1];
         s->rz = trz;
         s->rr = tot_bb;
         s->rr0 = tot_bb;
@@ -405,12 +419,11 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(Item const* items, 
     }
     double const rz_b = block_sum(rz, red);
     double const rr_b = block_sum(rr, red);
-    double tot_rz = 0.0, tot_rr = 0.0;
-    finish_reduction(rz_b, part_a, it.index, pi.first_item, pi.nitems, &s->counter_b, &tot_rz);
-    if (finish_reduction(rr_b, part_b, it.index, pi.first_item, pi.nitems, &s->counter_c, &tot_rr)) {
-        __threadfence();
-        double trz = 0.0;
-        for (int k = 0; k < pi.nitems; ++k) trz += __ldcg(part_a + pi.first_item + k);
+    double const vals[2] = {rz_b, rr_b};
+    double* parts[2] = {part_a, part_b};
+    double tot[2];
+    if (finish_reduction_k<2>(vals, parts, it.index, pi.first_item, pi.nitems, &s->counter_b, tot)) {
+        double const trz = tot[0], tot_rr = tot[1];
         s->beta = trz / s->rz;
         s->rz = trz;
         s->rr = tot_rr;
@@ -512,12 +525,11 @@ __global__ void __launch_bounds__(kThreads) fcg_apply_kernel(Item const* items, 
     }
     double const pq_b = block_sum(pq, red);
     double const pr_b = block_sum(pr, red);
-    double tot_pq = 0.0, tot_pr = 0.0;
-    finish_reduction(pq_b, part_a, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot_pq);
-    if (finish_reduction(pr_b, part_b, it.index, pi.first_item, pi.nitems, &s->counter_b, &tot_pr)) {
-        __threadfence();
-        double tpq = 0.0;
-        for (int k = 0; k < pi.nitems; ++k) tpq += __ldcg(part_a + pi.first_item + k);
+    double const vals[2] = {pq_b, pr_b};
+    double* parts[2] = {part_a, part_b};
+    double tot[2];
+    if (finish_reduction_k<2>(vals, parts, it.index, pi.first_item, pi.nitems, &s->counter_a, tot)) {
+        double const tpq = tot[0], tot_pr = tot[1];
         s->pq = tpq;
         s->alpha = tot_pr / tpq;
         if (!isfinite(s->alpha)) s->nonfinite = 1;
@@ -1049,6 +1061,7 @@ extern "C" {
 sil_status sil_mag2d_apply(sil_stream stream, int64_t nx, int64_t ny, const double* node_mu, const double* a, double* y)
 {
     if (nx < 3 || ny < 3) return fail(SIL_ERR_INVALID, "sil_mag2d_apply: need at least 3x3 nodes");
+    if (nx * ny >= (int64_t(1) << 31)) return fail(SIL_ERR_INVALID, "sil_mag2d_apply: fewer than 2^31 nodes supported");
     if (node_mu == nullptr || a == nullptr || y == nullptr) return fail(SIL_ERR_INVALID, "sil_mag2d_apply: NULL pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int64_t const n = nx * ny;
@@ -1138,6 +1151,8 @@ sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblem
     for (int p = 0; p < nproblems; ++p) {
         sil_mag2d_problem const& q = problems[p];
         if (q.nx < 3 || q.ny < 3) return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: each problem needs >= 3x3 nodes");
+        if (q.nx * q.ny >= (int64_t(1) << 31))
+            return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: a problem must have fewer than 2^31 nodes");
         if (q.node_mu == nullptr || q.rhs == nullptr || q.solution == nullptr)
             return fail(SIL_ERR_INVALID, "sil_mag2d_solve_batch: NULL field pointer");
         descs[p] = {2, q.nx, q.ny, 1, 0.0, q.node_mu, q.rhs, q.solution, {nullptr, nullptr, nullptr}};
@@ -1166,6 +1181,8 @@ namespace {
 sil_status check_mag3d(sil_mag3d_problem const& q, char const* who, bool need_fields)
 {
     if (q.nx < 3 || q.ny < 3 || q.nz < 3) return fail(SIL_ERR_INVALID, std::string(who) + ": need at least 3x3x3 nodes");
+    if (3 * q.nx * q.ny * q.nz >= (int64_t(1) << 31))
+        return fail(SIL_ERR_INVALID, std::string(who) + ": fewer than 2^31 unknowns per problem supported");
     if (q.x == nullptr || q.y == nullptr || q.z == nullptr)
         return fail(SIL_ERR_INVALID, std::string(who) + ": NULL coordinate array");
     if (q.node_mu == nullptr) return fail(SIL_ERR_INVALID, std::string(who) + ": NULL node_mu");
