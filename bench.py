@@ -195,7 +195,14 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--extras", action="store_true", help="also time the unfused chain, FP32 and the 512^2 0-form")
-    ap.add_argument("--workload", default="laplacian", choices=["laplacian", "solve", "mag3d"])
+    ap.add_argument("--workload", default="laplacian", choices=["laplacian", "solve", "mag3d", "precond"])
+    ap.add_argument("--solvers", default="cg,mixed,learned", help="solve / mag3d: solver kinds to time")
+    ap.add_argument("--max-iterations", type=int, default=200000, help="solve / mag3d: iteration budget")
+    ap.add_argument("--shapes", default=None, help="precond: NxC (C grids of N^2 nodes); default the 64-problem batch")
+    ap.add_argument("--sizes", default=None, help="solve: comma-separated grid sizes drawn from (default 128..1024)")
+    ap.add_argument("--seed", type=int, default=7, help="solve: problem seed")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="solve / mag3d: also time the oracle's FP64 CPU CG on this many problems of the batch")
     ap.add_argument("--count", type=int, default=None, help="solve / mag3d: problems per batch (64 / 8)")
     ap.add_argument("--n3d", type=int, default=256, help="mag3d: nodes per axis")
     ap.add_argument("--kernel-only", action="store_true",
@@ -209,6 +216,9 @@ def main():
         return
     if args.workload == "mag3d":
         run_mag3d_workload(args)
+        return
+    if args.workload == "precond":
+        run_precond_workload(args)
         return
 
     import torch
@@ -290,26 +300,52 @@ def main():
             pg.destroy_process_group()
         return
 
-    # End to end through the public API with host buffers: pinned H2D of the
-    # input, the Laplacian, D2H of the result, every step.
+    # End to end through the public API with host buffers: every step copies
+    # its input from pinned host memory, runs the Laplacian and copies the
+    # result back.  Steps are pipelined over three streams (H2D, compute,
+    # D2H) with two device buffers each, so step s+1's upload and step s-1's
+    # download overlap step s's kernel; events order each buffer's reuse.
     h_in = torch.from_numpy(w_host).pin_memory()
-    h_out = torch.empty((n - 1, n - 1, 2), dtype=torch.float64).pin_memory()
-    d_in = torch.empty_like(inp)
-    d_out = torch.empty_like(out)
-    e2e_steps = max(3, min(args.steps, 10))
-    for _ in range(2):
-        d_in.copy_(h_in, non_blocking=True)
-        plan.run(d_out, d_in)
-        h_out.copy_(d_out, non_blocking=True)
+    h_out = [torch.empty((n - 1, n - 1, 2), dtype=torch.float64).pin_memory() for _ in range(2)]
+    d_in = [torch.empty_like(inp) for _ in range(2)]
+    d_out = [torch.empty_like(out) for _ in range(2)]
+    s_up, s_run, s_down = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    ev_up = [torch.cuda.Event() for _ in range(2)]
+    ev_run = [torch.cuda.Event() for _ in range(2)]
+    ev_down = [torch.cuda.Event() for _ in range(2)]
+    ev_in_free = [torch.cuda.Event() for _ in range(2)]
+
+    def e2e_steps_run(count):
+        for st in range(count):
+            b = st % 2
+            with torch.cuda.stream(s_up):
+                if st >= 2:
+                    s_up.wait_event(ev_in_free[b])
+                d_in[b].copy_(h_in, non_blocking=True)
+                ev_up[b].record(s_up)
+            s_run.wait_event(ev_up[b])
+            if st >= 2:
+                s_run.wait_event(ev_down[b])
+            plan.run(d_out[b], d_in[b], stream=s_run)
+            ev_run[b].record(s_run)
+            ev_in_free[b].record(s_run)
+            with torch.cuda.stream(s_down):
+                s_down.wait_event(ev_run[b])
+                h_out[b].copy_(d_out[b], non_blocking=True)
+                ev_down[b].record(s_down)
+
+    e2e_steps = max(4, min(args.steps, 20))
+    e2e_steps_run(4)
     torch.cuda.synchronize()
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(e2e_steps):
-        d_in.copy_(h_in, non_blocking=True)
-        plan.run(d_out, d_in)
-        h_out.copy_(d_out, non_blocking=True)
+    for sx in (s_up, s_run, s_down):
+        sx.wait_event(e0)
+    e2e_steps_run(e2e_steps)
+    for sx in (s_up, s_run, s_down):
+        stream.wait_stream(sx)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -343,7 +379,8 @@ def main():
             "cpu_baseline": cb,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": int(n * n * 2 * 8),
                     "d2h_bytes_per_step": int((n - 1) * (n - 1) * 2 * 8), "steps": e2e_steps,
-                    "ms_per_step": e2e_ms / e2e_steps},
+                    "ms_per_step": e2e_ms / e2e_steps,
+                    "pipelining": "H2D, kernel and D2H of consecutive steps on three streams, two buffers each"},
             "gpu_launches": args.steps,
             "clocks": dict(clocks.summary() or {}, window="1 s preheat on the same kernel + warm-up + timed region"),
         }
@@ -410,7 +447,10 @@ def run_solve_workload(args):
         import torch.distributed as tdist
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     count = args.count or 64
-    allp = mag.synthetic_batch(seed=7, count=count)
+    if args.sizes:
+        allp = mag.synthetic_batch(seed=args.seed, count=count, sizes=tuple(int(v) for v in args.sizes.split(",")))
+    else:
+        allp = mag.synthetic_batch(seed=args.seed, count=count)
     # problems shard across ranks by work (nodes), no collective on the data path
     mine = sd.shard_by_work([p.nx * p.ny for p in allp], world)[rank]
     probs = [allp[i] for i in mine]
@@ -419,11 +459,11 @@ def run_solve_workload(args):
     rhss = [torch.from_numpy(p.rhs()).cuda() for p in probs]
     weights = os.path.join(ROOT, "similie_b200", "data", "precond_2d.npy")
     net = None
-    if os.path.exists(weights) and len(probs) <= 64:
+    if os.path.exists(weights):
         net = LearnedPreconditioner(seed=0)
         net.load(weights)
     results = {}
-    kinds = ["cg", "mixed"] + (["learned"] if net is not None else [])
+    kinds = [k for k in args.solvers.split(",") if k in ("cg", "mixed") or (k == "learned" and net is not None)]
     with ClockSampler(local) as clocks:
         for kind in kinds:
             sols = [torch.zeros_like(r) for r in rhss]
@@ -432,8 +472,12 @@ def run_solve_workload(args):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            d = mag.solve_batch(mus, rhss, sols, shapes, solver=kind, tol=1e-10,
-                                preconditioner=net if kind == "learned" else None)
+            d = []
+            for c0 in range(0, len(probs), 64):  # the learned solver takes 64 problems per call
+                sl = slice(c0, c0 + 64)
+                d += mag.solve_batch(mus[sl], rhss[sl], sols[sl], shapes[sl], solver=kind, tol=1e-10,
+                                     max_iterations=args.max_iterations, inner_iterations=min(4000, args.max_iterations),
+                                     preconditioner=net if kind == "learned" else None)
             e1.record()
             torch.cuda.synchronize()
             wall = time.perf_counter() - t0
@@ -447,6 +491,8 @@ def run_solve_workload(args):
             results[kind] = {"seconds": sec, "wall_seconds": wall, "solves_per_s": len(allp) / sec,
                              "converged": sum(x.converged for x in d), "max_iterations": max(x.iterations for x in d),
                              "fallbacks": sum(x.fallback for x in d),
+                             "median_iterations": float(np.median([x.iterations for x in d])),
+                             "median_learned_iterations": float(np.median([x.learned_iterations for x in d])),
                              "max_rel_residual_gpu": max(x.final_relative_residual for x in d),
                              "max_rel_residual_oracle_sampled": worst}
     gathered = sd.gather_to_rank0(results)
@@ -461,16 +507,28 @@ def run_solve_workload(args):
         results[kind]["fallbacks"] = sum(g[kind]["fallbacks"] for g in gathered)
         results[kind]["max_iterations"] = max(g[kind]["max_iterations"] for g in gathered)
         results[kind]["max_rel_residual_gpu"] = max(g[kind]["max_rel_residual_gpu"] for g in gathered)
-    base = results["cg"]["seconds"]
+    cpu = None
+    if args.cpu_sample > 0:
+        sample = allp[:args.cpu_sample]
+        t0 = time.perf_counter()
+        for p in sample:
+            O.mag2d_cg(p.nx, p.ny, p.node_mu(), p.rhs(), tol=1e-10, max_iter=200000)
+        sec = time.perf_counter() - t0
+        nodes = sum(p.nx * p.ny for p in sample)
+        cpu = {"value": len(sample) / sec, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"first {len(sample)} problems of the batch ({nodes} nodes), FP64 Jacobi-CG to 1e-10",
+               "seconds": sec}
+    base = results[kinds[0]]["seconds"]
     best = min(results, key=lambda k: results[k]["seconds"])
     line = {"metric": "time-to-1e-10 residual, batch of 2D magnetostatics problems (plain FP64 solve vs mixed vs learned)",
             "value": results[best]["solves_per_s"], "unit": "solves/s", "n_gpus": world, "steps": 1, "warmup": 0,
             "ms_per_step": results[best]["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 outer / f32 inner",
             "data": "synthetic (seeded coils and permeability-1000 rectangles)",
-            "config": {"workload": f"{count} problems, sizes {{128..1024}}^2 (seed 7), tol 1e-10", "best": best},
+            "config": {"workload": f"{count} problems, sizes {args.sizes or '128..1024'} squared (seed {args.seed}), "
+                                   f"tol 1e-10, solved 64 per call", "best": best},
             "solvers": results, "speedup_vs_plain_fp64": {k: base / v["seconds"] for k, v in results.items()},
-            "clocks": clocks.summary()}
+            "cpu_baseline": cpu, "clocks": clocks.summary()}
     print(json.dumps(line))
 
 
@@ -487,13 +545,13 @@ def run_mag3d_workload(args):
     setup = time.perf_counter() - t0
     results = {}
     with ClockSampler(0) as clocks:
-        for kind in ("cg", "mixed"):
+        for kind in [k for k in args.solvers.split(",") if k in ("cg", "mixed")]:
             sols = [torch.zeros_like(r) for r in rhss]
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            d = m3.solve_batch(coords, mus, rhss, sols, solver=kind, tol=1e-10)
+            d = m3.solve_batch(coords, mus, rhss, sols, solver=kind, tol=1e-10, max_iterations=args.max_iterations)
             e1.record()
             torch.cuda.synchronize()
             sec = e0.elapsed_time(e1) / 1e3
@@ -502,6 +560,7 @@ def run_mag3d_workload(args):
                              "max_rel_residual_gpu": max(x.final_relative_residual for x in d)}
     best = min(results, key=lambda k: results[k]["seconds"])
     n = args.n3d
+    hodge = hodge3d_gbs(torch, probs[0].x, probs[0].y, probs[0].z)
     line = {"metric": f"time-to-1e-10 residual, batch of {len(probs)} 3D curl-curl problems {n}^3",
             "value": results[best]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": 0,
             "ms_per_step": results[best]["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -509,8 +568,73 @@ def run_mag3d_workload(args):
             "data": "synthetic (seeded toroidal loops, ratio-1.01 stretched grid)",
             "config": {"workload": f"{len(probs)} x {n}^3 nodes x 3 components, gamma 20", "host_setup_s": setup,
                        "best": best},
-            "solvers": results, "clocks": clocks.summary()}
+            "solvers": results, "hodge_star_1_to_2_form": hodge, "clocks": clocks.summary()}
     print(json.dumps(line))
+
+
+def hodge3d_gbs(torch, x, y, z, steps=20):
+    """Hodge star of a 3D 1-form into a 2-form on the stretched grid (FP64, DDC layout
+    [x][y][z][component]): 48 algorithmic bytes per node (3 components in, 3 out)."""
+    import similie_b200 as sil
+    geo = sil.Geometry([x, y, z])
+    n = (len(x), len(y), len(z))
+    g = torch.Generator(device="cuda").manual_seed(3)
+    w = torch.randn(*n, 3, dtype=torch.float64, device="cuda", generator=g)
+    out = torch.empty_like(w)
+    for _ in range(3):
+        sil.hodge_star(geo, out, w, 1)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        sil.hodge_star(geo, out, w, 1)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    nodes = n[0] * n[1] * n[2]
+    peak, kind = measured_peaks()
+    gbs = nodes * 48 / (ms * 1e-3) / 1e9
+    return {"ms": ms, "GB/s_algorithmic": gbs, "frac_of_peak": gbs / peak, "peak_source": kind,
+            "bytes_per_node": 48, "nodes": nodes}
+
+
+def run_precond_workload(args):
+    """Learned-preconditioner applies M(r) on a batch of node grids (device-resident FP32)."""
+    import torch
+    from similie_b200.precond import LearnedPreconditioner
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(7)
+    if args.shapes:
+        n, c = (int(v) for v in args.shapes.split("x"))
+        sizes = [n] * c
+    else:
+        sizes = [int(rng.choice([128, 256, 384, 512, 768, 1024])) for _ in range(64)]
+    shapes = [(n, n) for n in sizes]
+    tot = sum(n * n for n in sizes)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    nu = torch.rand(tot, device="cuda", generator=g) * 0.9 + 0.1
+    r = torch.randn(tot, device="cuda", generator=g)
+    out = torch.zeros_like(r)
+    net = LearnedPreconditioner(seed=1)
+    weights = os.path.join(ROOT, "similie_b200", "data", "precond_2d.npy")
+    if os.path.exists(weights):
+        net.load(weights)
+    for _ in range(args.warmup):
+        net.apply(shapes, nu, r, out)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        net.apply(shapes, nu, r, out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    top = sum(((n + 1) // 2) ** 2 for n in sizes)
+    print(json.dumps({"metric": "learned preconditioner apply", "value": ms, "unit": "ms", "higher_is_better": False,
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "config": {"workload": f"{len(sizes)} grids, {tot} nodes, {top} top-level pixels"}}))
 
 
 if __name__ == "__main__":

@@ -107,6 +107,26 @@ sil_status sil_hodge_star(sil_geometry geometry, sil_stream stream, uint32_t for
 sil_status sil_fill_discrete_hodge_star(sil_geometry geometry, sil_stream stream, int k_in,
                                         sil_field* hodge);
 
+/* General (per-node, dense) metric: fill the stored Hodge tensor from a
+ * position field (n components per node) and a metric field (n*n
+ * components per node, row-major; NULL for the identity), all FP64 device
+ * fields whose lattice spans exactly the n <= 3 form dimensions.  The hodge
+ * lattice must lie inside the position and metric lattices (edge vectors are
+ * forward differences, backward at the last node of the position field).
+ * Same tensor layout as sil_fill_discrete_hodge_star.
+ * Replaces: fill_discrete_hodge_star<Idx1, Idx2, CircumcentricDual>(exec, hodge, metric, position),
+ *   src/similie/exterior/hodge_star.hpp:453-494 (DiscreteHodgeStar 222-359). */
+sil_status sil_fill_discrete_hodge_star_metric(sil_stream stream, int n, int k_in, const sil_field* position,
+                                               const sil_field* metric, sil_field* hodge);
+
+/* Apply a stored Hodge tensor (from either fill) to a k-form at every node
+ * of `out`: out[t] = sum over index tuples of in(tuple) * hodge(tuple, t).
+ * FP64, lattices over the n form dimensions.
+ * Replaces: tensor_prod(out, in, hodge), src/similie/tensor/tensor_prod.hpp:108-157,
+ *   as the staged operators use it (codifferential.hpp:460-504). */
+sil_status sil_hodge_star_stored(sil_stream stream, int n, int k_in, const sil_field* hodge, const sil_field* in,
+                                 sil_field* out);
+
 /* Codifferential of a k-form (k >= 1), one fused kernel (star, transposed d,
  * star, sign (-1)^{n(k+1)+1}).
  * Replaces: codifferential / StagedCodifferential::run,

@@ -165,6 +165,32 @@ def hodge_star(geometry, out, inp, k, form_dims=None, comp_axis=-1, in_front=Non
     return out
 
 
+def fill_discrete_hodge_star_metric(hodge, position, k_in, metric=None, fronts=None, stream=None):
+    """Stored Hodge tensor of a general metric: hodge (*lattice, n**k_in * C(n, n-k_in)),
+    position (*lattice, n), metric (*lattice, n*n) or None for the identity (FP64 CUDA tensors).
+    fronts: optional dict of lattice fronts for 'hodge', 'position', 'metric'."""
+    fronts = fronts or {}
+    n = position.shape[-1]
+    fh = field_struct(hodge, -1, fronts.get("hodge"))
+    fp = field_struct(position, -1, fronts.get("position"))
+    fm = field_struct(metric, -1, fronts.get("metric")) if metric is not None else None
+    check(lib().sil_fill_discrete_hodge_star_metric(_stream(stream), n, k_in, ctypes.byref(fp),
+                                                     ctypes.byref(fm) if fm is not None else None,
+                                                     ctypes.byref(fh)), "fill_discrete_hodge_star_metric")
+    return hodge
+
+
+def hodge_star_stored(hodge, out, inp, n, k_in, fronts=None, stream=None):
+    """out = tensor_prod(inp, hodge): apply a stored Hodge tensor to a k-form (FP64 CUDA tensors)."""
+    fronts = fronts or {}
+    fh = field_struct(hodge, -1, fronts.get("hodge"))
+    fi = field_struct(inp, -1, fronts.get("in"))
+    fo = field_struct(out, -1, fronts.get("out"))
+    check(lib().sil_hodge_star_stored(_stream(stream), n, k_in, ctypes.byref(fh), ctypes.byref(fi),
+                                      ctypes.byref(fo)), "hodge_star_stored")
+    return out
+
+
 def fill_discrete_hodge_star(geometry, hodge, k_in, front=None, stream=None):
     """Stored per-node Hodge tensor, shape (*lattice, n**k_in * C(n, n-k_in))."""
     fh = field_struct(hodge, -1, front)

@@ -128,6 +128,8 @@ SIGNATURES = [
     ("sil_mag2d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag2dProblem), ctypes.c_int,
                                              ctypes.POINTER(SilSolveSettings),
                                              ctypes.POINTER(SilSolveDiagnostics), _P]),
+    ("sil_fill_discrete_hodge_star_metric", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _F, _F, _F]),
+    ("sil_hodge_star_stored", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _F, _F, _F]),
     ("sil_precond_num_params", ctypes.c_int64, []),
     ("sil_precond_create", ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_uint64, _P]),
     ("sil_precond_destroy", None, [_P]),

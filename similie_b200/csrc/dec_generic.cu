@@ -163,6 +163,41 @@ __global__ void hodge_kernel(FieldView in, FieldView out, StarRule star, GeoCtx<
     }
 }
 
+// Dense 3D fast path of the Hodge star: a contiguous [x][y][z][component]
+// field over the three form dimensions (no spectators), input and output on
+// the same box.  One block covers a run of z along one (x, y) row, so the
+// per-node index arithmetic is one add; the factors are formed in the same
+// order as star_factor (sign, then h / inv_h per axis), so the result is the
+// table-driven kernel's bit for bit.
+template <class T>
+__global__ void __launch_bounds__(256) hodge3d_dense_kernel(T const* in, T* out, int ncin, int ncout, StarRule star,
+                                                            GeoView<T> geo, int64_t fx, int64_t fy, int64_t fz,
+                                                            int nx, int ny, int nz, int zchunks)
+{
+    int const row = blockIdx.x / zchunks;
+    int const z = (blockIdx.x - row * zchunks) * blockDim.x + threadIdx.x;
+    if (z >= nz) return;
+    int const y = row % ny, x = row / ny;
+    int64_t const node = (static_cast<int64_t>(row)) * nz + z;
+    int64_t const p[3] = {fx + x - geo.front[0] + 1, fy + y - geo.front[1] + 1, fz + z - geo.front[2] + 1};
+    T const* src = in + node * ncin;
+    T v[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = c < ncin ? src[c] : T(0);
+    T* dst = out + node * ncout;
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        if (t >= ncout) break;
+        T f = static_cast<T>(star.sgn[t]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (star.num_mask[t] & (1u << a)) f *= geo.h[a][p[a]];
+            if (star.den_mask[t] & (1u << a)) f *= geo.inv_h[a][p[a]];
+        }
+        dst[t] = f * v[star.src[t]];
+    }
+}
+
 // Stored per-node Hodge tensor (Full<k> x Antisym<n-k>) of the diagonal metric.
 template <class T, int ND>
 __global__ void fill_hodge_kernel(FieldView out, StarRule star, GeoCtx<T> g, int k, int n, int64_t total)
@@ -500,6 +535,32 @@ sil_status launch_hodge(cudaStream_t stream, Geometry const& geo, uint32_t mask,
     StarRule const star = make_star(n, k);
     int64_t const total = node_count(out);
     if (total == 0) return SIL_OK;
+    // dense 3D fields (the 3D magnetostatics / curl-curl layout): row kernel
+    auto dense = [](sil_field const& f) {
+        return f.ndims == 3 && f.comp_stride == 1 && f.stride[2] == f.ncomp && f.stride[1] == f.extent[2] * f.ncomp
+               && f.stride[0] == f.extent[1] * f.extent[2] * f.ncomp;
+    };
+    bool same_box = in.ndims == 3 && out.ndims == 3;
+    for (int d = 0; d < 3 && same_box; ++d) same_box = in.front[d] == out.front[d] && in.extent[d] == out.extent[d];
+    if (n == 3 && mask == 7u && same_box && dense(in) && dense(out) && out.extent[0] * out.extent[1] < (int64_t(1) << 30)
+        && out.extent[2] < (int64_t(1) << 30)) {
+        int const nx = static_cast<int>(out.extent[0]), ny = static_cast<int>(out.extent[1]);
+        int const nz = static_cast<int>(out.extent[2]);
+        int const zchunks = (nz + 255) / 256;
+        int64_t const blocks = static_cast<int64_t>(nx) * ny * zchunks;
+        if (blocks < (int64_t(1) << 31)) {
+            if (in.dtype == SIL_F64)
+                hodge3d_dense_kernel<double><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
+                        static_cast<double const*>(in.data), static_cast<double*>(out.data), in.ncomp, out.ncomp, star,
+                        geo_view<double>(geo), out.front[0], out.front[1], out.front[2], nx, ny, nz, zchunks);
+            else
+                hodge3d_dense_kernel<float><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
+                        static_cast<float const*>(in.data), static_cast<float*>(out.data), in.ncomp, out.ncomp, star,
+                        geo_view<float>(geo), out.front[0], out.front[1], out.front[2], nx, ny, nz, zchunks);
+            SIL_CUDA_CHECK(cudaGetLastError());
+            return SIL_OK;
+        }
+    }
     with_nd(out.ndims, [&](auto ndc) {
         constexpr int ND = decltype(ndc)::value;
         if (in.dtype == SIL_F64)

@@ -44,6 +44,7 @@ def host(t):
 # ----------------------------------------------------------------- coboundary
 
 DER = load_golden("derivative_kat.json")
+EXT = load_golden("exterior_kat.json")
 
 
 @pytest.mark.parametrize("case", [t for t in DER["tests"] if "spectators" not in t],
@@ -152,6 +153,75 @@ def test_hodge_star_vs_oracle(torch, sil, n):
         out = torch.zeros(shape + (comb(n, n - k),), device="cuda", dtype=torch.float64)
         sil.hodge_star(geo, out, dev(torch, inp), k)
         assert rel_err(host(out), ref) <= TOL, (n, k)
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_hodge_star_dense_3d_path_matches_table_driven(torch, sil, dtype):
+    """Dense [x][y][z][c] fields take the row kernel; a strided view of the same
+    data takes the table-driven kernel; both must agree bit for bit."""
+    rng = np.random.default_rng(77)
+    shape = (9, 7, 300)
+    coords = _coords(rng, shape)
+    geo = _geometry(sil, coords)
+    dt = getattr(torch, dtype)
+    for k in range(4):
+        inp = torch.from_numpy(rng.standard_normal(shape + (comb(3, k),))).to(dt).cuda()
+        dense = torch.zeros(shape + (comb(3, 3 - k),), device="cuda", dtype=dt)
+        sil.hodge_star(geo, dense, inp, k)
+        big = torch.zeros(shape + (comb(3, 3 - k) + 1,), device="cuda", dtype=dt)
+        strided = big[..., : comb(3, 3 - k)]            # comp stride 1, node stride ncomp + 1: not dense
+        sil.hodge_star(geo, strided, inp, k)
+        assert torch.equal(dense, strided), k
+
+
+@pytest.mark.parametrize("n", [1, 2, 3])
+def test_fill_hodge_star_general_metric_vs_oracle(torch, sil, n):
+    """Dense per-node SPD metric on a perturbed (non-orthogonal) lattice: the GPU
+    restatement of fill_discrete_hodge_star matches the oracle for every rank,
+    and the stored tensor applied on the GPU matches the oracle's tensor_prod."""
+    rng = np.random.default_rng(90 + n)
+    shape = tuple(int(s) for s in rng.integers(3, 6, size=n))
+    coords = _coords(rng, shape)
+    pos = O.position_from_coords(coords) + 0.02 * rng.standard_normal(shape + (n,))
+    a = rng.standard_normal(shape + (n, n)) * 0.3
+    met = np.einsum("...ij,...kj->...ik", a, a) + np.eye(n)
+    met = np.ascontiguousarray(met.reshape(shape + (n * n,)))
+    for k in range(n + 1):
+        ref = O.fill_hodge_star(n, k, pos, met)
+        out = torch.full(ref.shape, float("nan"), device="cuda", dtype=torch.float64)
+        sil.fill_discrete_hodge_star_metric(out, dev(torch, pos), k, metric=dev(torch, met))
+        assert rel_err(host(out), ref) <= TOL, (n, k)
+        form = rng.standard_normal(shape + (comb(n, k),))
+        dref = O.apply_hodge_star(n, k, ref, form)
+        dgpu = torch.zeros(shape + (comb(n, n - k),), device="cuda", dtype=torch.float64)
+        sil.hodge_star_stored(out, dgpu, dev(torch, form), n, k)
+        assert rel_err(host(dgpu), dref) <= TOL, (n, k)
+
+
+def test_hodge_star_dense_metric_kat_gpu(torch, sil):
+    """hodge_star.cpp:66-181 on the GPU: star(3 dx^dy)_z = 1.5 sqrt(6/19) with the
+    test's dense metric, and back to 3, within the reference's 4 ULP."""
+    kat = EXT["hodge_star_3d_metric"]
+    m = kat["metric"]
+    g = np.array([[m["XX"], m["XY"], m["XZ"]], [m["XY"], m["YY"], m["YZ"]], [m["XZ"], m["YZ"], m["ZZ"]]])
+    xs = np.linspace(kat["lower"], kat["upper"], kat["points"])
+    pos = O.position_from_coords([xs, xs, xs])
+    met = np.ascontiguousarray(np.broadcast_to(g.reshape(9), pos.shape[:-1] + (9,)))
+    form = np.zeros(pos.shape[:-1] + (3,))
+    form[..., 0] = kat["form_xy"]
+    shape = pos.shape[:-1]
+    h2 = torch.zeros(shape + (9 * 3,), device="cuda", dtype=torch.float64)
+    sil.fill_discrete_hodge_star_metric(h2, dev(torch, pos), 2, metric=dev(torch, met))
+    dual = torch.zeros(shape + (3,), device="cuda", dtype=torch.float64)
+    sil.hodge_star_stored(h2, dual, dev(torch, form), 3, 2)
+    d = host(dual)
+    ulp = np.spacing(kat["expected_dual_z"])
+    assert np.all(np.abs(d[..., 2] - kat["expected_dual_z"]) <= kat["tolerance_ulps"] * ulp)
+    h1 = torch.zeros(shape + (3 * 3,), device="cuda", dtype=torch.float64)
+    sil.fill_discrete_hodge_star_metric(h1, dev(torch, pos), 1, metric=dev(torch, met))
+    back = torch.zeros(shape + (3,), device="cuda", dtype=torch.float64)
+    sil.hodge_star_stored(h1, back, dual, 3, 1)
+    assert np.all(np.abs(host(back)[..., 0] - kat["expected_round_trip_xy"]) <= kat["tolerance_ulps"] * np.spacing(3.0))
 
 
 @pytest.mark.parametrize("n", [1, 2, 3])
