@@ -195,7 +195,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--extras", action="store_true", help="also time the unfused chain, FP32 and the 512^2 0-form")
-    ap.add_argument("--workload", default="laplacian", choices=["laplacian", "solve", "mag3d", "precond"])
+    ap.add_argument("--workload", default="laplacian", choices=["laplacian", "solve", "mag3d", "precond", "hodge3d"])
     ap.add_argument("--solvers", default="cg,mixed,learned", help="solve / mag3d: solver kinds to time")
     ap.add_argument("--max-iterations", type=int, default=200000, help="solve / mag3d: iteration budget")
     ap.add_argument("--shapes", default=None, help="precond: NxC (C grids of N^2 nodes); default the 64-problem batch")
@@ -219,6 +219,14 @@ def main():
         return
     if args.workload == "precond":
         run_precond_workload(args)
+        return
+    if args.workload == "hodge3d":
+        import torch
+        import similie_b200.magnetostatics3d as m3
+        torch.cuda.set_device(0)
+        x = m3.stretched_coords(args.n3d, 1.01)
+        print(json.dumps({"metric": f"3D Hodge star 1-form -> 2-form, {args.n3d}^3, FP64",
+                          "hodge": hodge3d_gbs(torch, x, x.copy(), x.copy(), steps=args.steps)}))
         return
 
     import torch

@@ -198,6 +198,43 @@ __global__ void __launch_bounds__(256) hodge3d_dense_kernel(T const* in, T* out,
     }
 }
 
+// Paired variant of the dense 3D row kernel for FP64 fields with three
+// components in and out: each thread owns two consecutive nodes along z, so
+// its 48 bytes in and out move as three 16-byte vector accesses.
+__global__ void __launch_bounds__(256) hodge3d_dense_pair_kernel(double const* in, double* out, StarRule star,
+                                                                 GeoView<double> geo, int64_t fx, int64_t fy,
+                                                                 int64_t fz, int nx, int ny, int nz, int zchunks)
+{
+    int const row = blockIdx.x / zchunks;
+    int const z0 = 2 * ((blockIdx.x - row * zchunks) * blockDim.x + threadIdx.x);
+    if (z0 >= nz) return;
+    int const y = row % ny, x = row / ny;
+    int64_t const node = static_cast<int64_t>(row) * nz + z0;
+    double2 const* src = reinterpret_cast<double2 const*>(in + node * 3);
+    double2 const a = src[0], b = src[1], c = src[2];
+    double const v[2][3] = {{a.x, a.y, b.x}, {b.y, c.x, c.y}};
+    int64_t const px = fx + x - geo.front[0] + 1, py = fy + y - geo.front[1] + 1;
+    double r[2][3];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        int64_t const p[3] = {px, py, fz + z0 + q - geo.front[2] + 1};
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            double f = static_cast<double>(star.sgn[t]);
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+                if (star.num_mask[t] & (1u << ax)) f *= geo.h[ax][p[ax]];
+                if (star.den_mask[t] & (1u << ax)) f *= geo.inv_h[ax][p[ax]];
+            }
+            r[q][t] = f * v[q][star.src[t]];
+        }
+    }
+    double2* dst = reinterpret_cast<double2*>(out + node * 3);
+    dst[0] = make_double2(r[0][0], r[0][1]);
+    dst[1] = make_double2(r[0][2], r[1][0]);
+    dst[2] = make_double2(r[1][1], r[1][2]);
+}
+
 // Stored per-node Hodge tensor (Full<k> x Antisym<n-k>) of the diagonal metric.
 template <class T, int ND>
 __global__ void fill_hodge_kernel(FieldView out, StarRule star, GeoCtx<T> g, int k, int n, int64_t total)
@@ -548,6 +585,20 @@ sil_status launch_hodge(cudaStream_t stream, Geometry const& geo, uint32_t mask,
         int const nz = static_cast<int>(out.extent[2]);
         int const zchunks = (nz + 255) / 256;
         int64_t const blocks = static_cast<int64_t>(nx) * ny * zchunks;
+        bool const pairable = in.dtype == SIL_F64 && in.ncomp == 3 && out.ncomp == 3 && nz % 2 == 0
+                              && reinterpret_cast<uintptr_t>(in.data) % 16 == 0
+                              && reinterpret_cast<uintptr_t>(out.data) % 16 == 0;
+        if (pairable) {
+            int const zc2 = (nz / 2 + 255) / 256;
+            int64_t const b2 = static_cast<int64_t>(nx) * ny * zc2;
+            if (b2 < (int64_t(1) << 31)) {
+                hodge3d_dense_pair_kernel<<<static_cast<unsigned>(b2), 256, 0, stream>>>(
+                        static_cast<double const*>(in.data), static_cast<double*>(out.data), star, geo_view<double>(geo),
+                        out.front[0], out.front[1], out.front[2], nx, ny, nz, zc2);
+                SIL_CUDA_CHECK(cudaGetLastError());
+                return SIL_OK;
+            }
+        }
         if (blocks < (int64_t(1) << 31)) {
             if (in.dtype == SIL_F64)
                 hodge3d_dense_kernel<double><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(

@@ -190,6 +190,94 @@ __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_
     return res + static_cast<T>(pi.gamma) * ha * a[row];
 }
 
+// All three rows of a node at once (the curl moments shared between the
+// components are formed once); each component sums its terms in the order of
+// mag3d_apply_row, so the values are the same.
+template <class T>
+__device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, int node, T* out)
+{
+    int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
+    int const t = node / nx, i = node - t * nx, k = t / ny, j = t - k * ny;
+    int const row0 = 3 * node;
+    auto interior = [&](int ii, int jj, int kk) {
+        return ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz;
+    };
+    if (!interior(i, j, k)) {
+        out[0] = a[row0];
+        out[1] = a[row0 + 1];
+        out[2] = a[row0 + 2];
+        return;
+    }
+    int const sy = 3 * nx, sz = 3 * nx * ny;
+    auto A = [&](int di, int dj, int dk, int cc) -> T {
+        return interior(i + di, j + dj, k + dk) ? a[row0 + 3 * di + sy * dj + sz * dk + cc] : T(0);
+    };
+    auto bx = [&](int oi, int oj, int ok) {
+        T m = T(0);
+        m = m + A(oi, oj, ok, 1);
+        m = m - A(oi, oj, ok, 2);
+        m = m - A(oi, oj, ok + 1, 1);
+        m = m + A(oi, oj + 1, ok, 2);
+        return m;
+    };
+    auto by = [&](int oi, int oj, int ok) {
+        T m = T(0);
+        m = m - A(oi, oj, ok, 0);
+        m = m + A(oi, oj, ok, 2);
+        m = m + A(oi, oj, ok + 1, 0);
+        m = m - A(oi + 1, oj, ok, 2);
+        return m;
+    };
+    auto bz = [&](int oi, int oj, int ok) {
+        T m = T(0);
+        m = m + A(oi, oj, ok, 0);
+        m = m - A(oi, oj, ok, 1);
+        m = m - A(oi, oj + 1, ok, 0);
+        m = m + A(oi + 1, oj, ok, 1);
+        return m;
+    };
+    T const* lx = spacing<T>(pi, 0);
+    T const* ly = spacing<T>(pi, 1);
+    T const* lz = spacing<T>(pi, 2);
+    T const* ilx = inv_spacing<T>(pi, 0);
+    T const* ily = inv_spacing<T>(pi, 1);
+    T const* ilz = inv_spacing<T>(pi, 2);
+    auto w = [&](int oi, int oj, int ok, int m) -> T {
+        T const nuv = nu[node + oi + nx * oj + nx * ny * ok];
+        if (m == 0) return lx[i + oi] * ily[j + oj] * ilz[k + ok] * nuv;
+        if (m == 1) return ly[j + oj] * ilx[i + oi] * ilz[k + ok] * nuv;
+        return lz[k + ok] * ilx[i + oi] * ily[j + oj] * nuv;
+    };
+    bool const in_k = interior(i, j, k - 1), in_j = interior(i, j - 1, k), in_i = interior(i - 1, j, k);
+    T const Bx = bx(0, 0, 0), By = by(0, 0, 0), Bz = bz(0, 0, 0);
+    T const Wx = w(0, 0, 0, 0), Wy = w(0, 0, 0, 1), Wz = w(0, 0, 0, 2);
+    T const g = static_cast<T>(pi.gamma);
+    {
+        T res = T(0);
+        res = res - Wy * By;
+        if (in_k) res = res + w(0, 0, -1, 1) * by(0, 0, -1);
+        res = res + Wz * Bz;
+        if (in_j) res = res - w(0, -1, 0, 2) * bz(0, -1, 0);
+        out[0] = res + g * (ly[j] * lz[k] * ilx[i]) * a[row0];
+    }
+    {
+        T res = T(0);
+        res = res + Wx * Bx;
+        if (in_k) res = res - w(0, 0, -1, 0) * bx(0, 0, -1);
+        res = res - Wz * Bz;
+        if (in_i) res = res + w(-1, 0, 0, 2) * bz(-1, 0, 0);
+        out[1] = res + g * (lx[i] * lz[k] * ily[j]) * a[row0 + 1];
+    }
+    {
+        T res = T(0);
+        res = res - Wx * Bx;
+        if (in_j) res = res + w(0, -1, 0, 0) * bx(0, -1, 0);
+        res = res + Wy * By;
+        if (in_i) res = res - w(-1, 0, 0, 1) * by(-1, 0, 0);
+        out[2] = res + g * (lx[i] * ly[j] * ilz[k]) * a[row0 + 2];
+    }
+}
+
 template <class T>
 __device__ __forceinline__ T mag_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_t row)
 {
@@ -379,10 +467,21 @@ __global__ void __launch_bounds__(kThreads) cg_apply_kernel(Item const* items, P
     ProbInfo const pi = info[it.prob];
     Vecs<T> const v = vecs[it.prob];
     double pq = 0.0;
-    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-        T const q = mag_apply_row(v.p, v.nu, pi, row);
-        v.q[row] = q;
-        pq += static_cast<double>(v.p[row]) * static_cast<double>(q);
+    if (pi.dim == 3) {
+        for (int64_t node = it.begin / 3 + threadIdx.x; node < it.end / 3; node += kThreads) {
+            T q[3];
+            mag3d_apply_node(v.p, v.nu, pi, static_cast<int>(node), q);
+            for (int c = 0; c < 3; ++c) {
+                v.q[3 * node + c] = q[c];
+                pq += static_cast<double>(v.p[3 * node + c]) * static_cast<double>(q[c]);
+            }
+        }
+    } else {
+        for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+            T const q = mag_apply_row(v.p, v.nu, pi, row);
+            v.q[row] = q;
+            pq += static_cast<double>(v.p[row]) * static_cast<double>(q);
+        }
     }
     double const pq_b = block_sum(pq, red);
     double tot = 0.0;
@@ -611,11 +710,23 @@ __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items,
     if (s->outer_done) return;
     ProbInfo const pi = info[it.prob];
     double rr = 0.0;
-    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-        double const ax = mag_apply_row(x64[it.prob], nu64[it.prob], pi, row);
-        double const r = rhs[it.prob][row] - ax;
-        r64[it.prob][row] = r;
-        rr += r * r;
+    if (pi.dim == 3) {
+        for (int64_t node = it.begin / 3 + threadIdx.x; node < it.end / 3; node += kThreads) {
+            double ax[3];
+            mag3d_apply_node(x64[it.prob], nu64[it.prob], pi, static_cast<int>(node), ax);
+            for (int c = 0; c < 3; ++c) {
+                double const r = rhs[it.prob][3 * node + c] - ax[c];
+                r64[it.prob][3 * node + c] = r;
+                rr += r * r;
+            }
+        }
+    } else {
+        for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+            double const ax = mag_apply_row(x64[it.prob], nu64[it.prob], pi, row);
+            double const r = rhs[it.prob][row] - ax;
+            r64[it.prob][row] = r;
+            rr += r * r;
+        }
     }
     double const rr_b = block_sum(rr, red);
     double tot = 0.0;
@@ -738,7 +849,9 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         pi.gamma = q.gamma;
         pi.first_item = static_cast<int>(items.size());
         int idx = 0;
-        for (int64_t b = 0; b < pi.n; b += kItemNodes, ++idx) items.push_back({p, idx, b, std::min(pi.n, b + kItemNodes)});
+        // 3D items hold whole nodes (3 rows each) so the apply can work per node
+        int64_t const step = q.dim == 3 ? (kItemNodes / 3) * 3 : kItemNodes;
+        for (int64_t b = 0; b < pi.n; b += step, ++idx) items.push_back({p, idx, b, std::min(pi.n, b + step)});
         pi.nitems = idx;
         total_rows += pi.n;
         if (q.dim == 3) {
@@ -1201,9 +1314,11 @@ sil_status check_mag3d(sil_mag3d_problem const& q, char const* who, bool need_fi
 
 __global__ void mag3d_apply_kernel(ProbInfo pi, double const* nu, double const* a, double* y)
 {
-    int64_t const row = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (row >= pi.n) return;
-    y[row] = mag3d_apply_row(a, nu, pi, row);
+    int64_t const node = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (node >= pi.nodes) return;
+    double out[3];
+    mag3d_apply_node(a, nu, pi, static_cast<int>(node), out);
+    for (int c = 0; c < 3; ++c) y[3 * node + c] = out[c];
 }
 
 } // namespace
@@ -1250,7 +1365,7 @@ sil_status sil_mag3d_apply(sil_stream stream, const sil_mag3d_problem* problem, 
         o += len[a2];
     }
     reciprocal_kernel<<<static_cast<int>((nodes + 255) / 256), 256, 0, s>>>(q.node_mu, nu, nodes);
-    mag3d_apply_kernel<<<static_cast<int>((pi.n + 255) / 256), 256, 0, s>>>(pi, nu, a, y);
+    mag3d_apply_kernel<<<static_cast<int>((nodes + 255) / 256), 256, 0, s>>>(pi, nu, a, y);
     SIL_CUDA_CHECK(cudaGetLastError());
     // A copy from pageable memory has left the host table once it returns;
     // the device buffer is freed in stream order after the apply.
