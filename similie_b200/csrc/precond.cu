@@ -219,6 +219,8 @@ __device__ __forceinline__ void cp_async16(uint4* dst, void const* src, bool val
 }
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_group1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // Asynchronous halo staging: the level's own tensor (up = false) or the
 // nearest-upsampled coarse tensor gathered to this level (up = true); pixels
@@ -295,16 +297,41 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
     uint32_t const halo_addr[2] = {smem_u32(s.halo[0]), smem_u32(s.halo[1])};
     uint32_t const w_addr = smem_u32(s.w);
     int const nops = mode == kUpAdd ? 2 : 1;
+    // kPlain runs a two-stage ring over the two halo buffers: the next tile's
+    // cp.async loads are in flight while this tile's MMAs and epilogue run.
+    bool const ring = mode == kPlain;
+    float bias_r[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) bias_r[i] = bias != nullptr ? __ldg(bias + i) : 0.0f;
     uint32_t phase = 0;
     int const ntiles = t.tile_base[t.nimg];
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    auto stage = [&](int tl, int buf) {
+        int const im2 = find_image(t, tl);
+        int const P2 = t.img[im2].w + 2;
+        int const start2 = P2 + (tl - t.tile_base[im2]) * kTilePx;
+        stage_halo(s.halo[buf], t, im2, start2, P2, in, false);
+        cp_async_commit();
+    };
+    if (ring && static_cast<int>(blockIdx.x) < ntiles) stage(blockIdx.x, 0);
+    int iter = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++iter) {
         int const im = find_image(t, tile);
         Img const o = t.img[im];
         int const P = o.w + 2;
         int const start = P + (tile - t.tile_base[im]) * kTilePx;
-        if (mode == kPlain || mode == kUpAdd) {
+        int cur = 0;
+        if (ring) {
+            cur = iter & 1;
+            int const nxt = tile + static_cast<int>(gridDim.x);
+            if (nxt < ntiles) {
+                stage(nxt, cur ^ 1);
+                cp_async_wait_group1();
+            } else {
+                cp_async_wait_all();
+            }
+        } else if (mode == kUpAdd) {
             stage_halo(s.halo[0], t, im, start, P, in, false);
-            if (mode == kUpAdd) stage_halo(s.halo[1], t, im, start, P, in2, true);
+            stage_halo(s.halo[1], t, im, start, P, in2, true);
             cp_async_wait_all();
         } else {
             load_halo(s.halo[0], mode, t, im, start, P, in, in2, gin);
@@ -321,8 +348,8 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
                     int const dy = tap / 3, dx = tap % 3;
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
-                        uint64_t const a =
-                                umma_desc(halo_addr[op] + ((2 * h * 3 + dy) * kHalo + dx) * 16, 3 * kHalo * 16, 128);
+                        uint64_t const a = umma_desc(halo_addr[ring ? cur : op] + ((2 * h * 3 + dy) * kHalo + dx) * 16,
+                                                     3 * kHalo * 16, 128);
                         uint64_t const b = umma_desc(w_addr + (tap * kChunks + 2 * h) * kCh * 16, kCh * 16, 128);
                         umma_bf16(tmem, a, b, kIdescFwd, step > 0 ? 1u : 0u);
                         ++step;
@@ -350,7 +377,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
             } else {
                 if (bias != nullptr) {
 #pragma unroll
-                    for (int i = 0; i < 32; ++i) acc[i] = acc[i] + __ldg(bias + i);
+                    for (int i = 0; i < 32; ++i) acc[i] = acc[i] + bias_r[i];
                 }
                 if (relu) {
 #pragma unroll
@@ -400,6 +427,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
         tc_fence_before();
         __syncthreads();
     }
+    cp_async_wait_all();  // no copy may still target this CTA's shared memory at exit
     if (s.abort && tid == 0) atomicExch(error_flag, 1);
     tc_fence_before();
     __syncthreads();
@@ -1116,15 +1144,16 @@ struct WrapItem
 };
 
 // K e at interior node (i, j) of an nx-wide grid for an e given by a functor.
+// e(q, i, j) gets the node's coordinates, so no index division per neighbour.
 template <class E>
 __device__ __forceinline__ float k_row(E const& e, float const* nu, int nx, int row, int i, int j)
 {
-    float const a0 = e(row);
+    float const a0 = e(row, i, j);
     float res = 0.0f;
-    if (j >= 2) res = res + (a0 - e(row - nx)) * nu[row - nx];
-    res = res + (a0 - e(row + nx)) * nu[row];
-    if (i >= 2) res = res + (a0 - e(row - 1)) * nu[row - 1];
-    res = res + (a0 - e(row + 1)) * nu[row];
+    if (j >= 2) res = res + (a0 - e(row - nx, i, j - 1)) * nu[row - nx];
+    res = res + (a0 - e(row + nx, i, j + 1)) * nu[row];
+    if (i >= 2) res = res + (a0 - e(row - 1, i - 1, j)) * nu[row - 1];
+    res = res + (a0 - e(row + 1, i + 1, j)) * nu[row];
     return res;
 }
 
@@ -1153,11 +1182,11 @@ __global__ void __launch_bounds__(256) wrap_pre_kernel(const __grid_constant__ S
     float const* nu_s = nu + sm.offset;
     float const* d_s = dinv + sm.offset;
     float const* r_s = r + sm.offset;
-    auto e = [&](int q) { return kOmega * (d_s[q] * r_s[q]); };
+    auto e = [&](int q, int, int) { return kOmega * (d_s[q] * r_s[q]); };
     double acc = 0.0;
     for (int row = it.begin + threadIdx.x; row < it.end; row += blockDim.x) {
         int const j = row / nx, i = row - j * nx;
-        float const ev = e(row);
+        float const ev = e(row, i, j);
         float v;
         if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) v = r_s[row] - ev;
         else v = r_s[row] - k_row(e, nu_s, nx, row, i, j);
@@ -1195,8 +1224,7 @@ __global__ void __launch_bounds__(256) wrap_post_kernel(const __grid_constant__ 
     float const* e1_s = e1 + sm.offset;
     float const* d_s = dinv + sm.offset;
     float const* un = unet + o.offset;
-    auto e = [&](int q) {
-        int const jj = q / nx, ii = q - jj * nx;
+    auto e = [&](int q, int ii, int jj) {
         float v = e1_s[q];
         if (!(ii == 0 || jj == 0 || ii + 1 == nx || jj + 1 == ny))
             v = v + s * sqrtf(d_s[q]) * un[(jj / 2 + 1) * P + (ii / 2 + 1)];
@@ -1204,7 +1232,7 @@ __global__ void __launch_bounds__(256) wrap_post_kernel(const __grid_constant__ 
     };
     for (int row = it.begin + threadIdx.x; row < it.end; row += blockDim.x) {
         int const j = row / nx, i = row - j * nx;
-        float const e0 = e(row);
+        float const e0 = e(row, i, j);
         float const ke = (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) ? e0 : k_row(e, nu_s, nx, row, i, j);
         int64_t const q = sm.offset + row;
         out[q] = e0 + kOmega * (dinv[q] * (r[q] - ke));
@@ -1415,12 +1443,14 @@ namespace {
 
 size_t conv_smem(int mode = kUpAdd)
 {
-    return sizeof(ConvSmem) - (mode == kUpAdd ? 0 : sizeof(uint4) * kChunks * 3 * kHalo);
+    // kPlain and kUpAdd use both halo buffers (ring stages / two operands)
+    return sizeof(ConvSmem) - (mode == kUpAdd || mode == kPlain ? 0 : sizeof(uint4) * kChunks * 3 * kHalo);
 }
 size_t wgrad_smem() { return sizeof(WgradSmem) + 1024; }
 
 bool g_attr_done = false;
 int g_sms = 0;  // multiprocessor count, read once (outside any stream capture)
+int g_conv_per_sm[5] = {0, 0, 0, 0, 0};  // resident conv CTAs per SM, by input mode
 
 sil_status ensure_attributes()
 {
@@ -1430,15 +1460,36 @@ sil_status ensure_attributes()
     SIL_CUDA_CHECK(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev));
     SIL_CUDA_CHECK(cudaFuncSetAttribute(conv3x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(conv_smem())));
+    // all of the unified L1 / shared storage as shared memory, so several
+    // CTAs of these shared-memory-heavy kernels fit on one multiprocessor
+    SIL_CUDA_CHECK(cudaFuncSetAttribute(conv3x3_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared));
+    SIL_CUDA_CHECK(cudaFuncSetAttribute(wgrad_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared));
+    // resident CTAs per multiprocessor from the kernel's registers and each
+    // mode's shared memory (1 KB per CTA reserved by the runtime)
+    cudaFuncAttributes fa {};
+    SIL_CUDA_CHECK(cudaFuncGetAttributes(&fa, conv3x3_kernel));
+    int smem_sm = 0, regs_sm = 0;
+    SIL_CUDA_CHECK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    SIL_CUDA_CHECK(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+    for (int m = 0; m < 5; ++m) {
+        int const by_smem = smem_sm / static_cast<int>(conv_smem(m) + 1024);
+        int const by_regs = regs_sm / std::max(1, fa.numRegs * 128);
+        g_conv_per_sm[m] = std::max(1, std::min(std::min(by_smem, by_regs), 8));
+    }
     SIL_CUDA_CHECK(cudaFuncSetAttribute(wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(wgrad_smem())));
     g_attr_done = true;
     return SIL_OK;
 }
 
-int conv_grid(int ntiles)
+// Persistent grid: every CTA resident in one wave (a second wave would
+// serialise behind the first).
+int conv_grid(int ntiles, int mode)
 {
-    return std::max(1, std::min(ntiles, 4 * (g_sms > 0 ? g_sms : 148)));
+    int const per_sm = g_conv_per_sm[mode] > 0 ? g_conv_per_sm[mode] : 1;
+    return std::max(1, std::min(ntiles, per_sm * (g_sms > 0 ? g_sms : 148)));
 }
 
 // 1024-byte aligned dynamic shared memory: the kernels index from the start
@@ -1449,7 +1500,7 @@ sil_status launch_conv(cudaStream_t st, Table const& t, int mode, bf16 const* in
                        int* err, float* out_taps = nullptr, float const* wout = nullptr, int64_t taps_stride = 0)
 {
     if (t.nimg == 0 || t.tile_base[t.nimg] == 0) return SIL_OK;
-    conv3x3_kernel<<<conv_grid(t.tile_base[t.nimg]), 128, conv_smem(mode), st>>>(
+    conv3x3_kernel<<<conv_grid(t.tile_base[t.nimg], mode), 128, conv_smem(mode), st>>>(
             t, mode, in, in2, gin, w, bias, relu, out, out_f32, accumulate, out_taps, wout, taps_stride, err);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
