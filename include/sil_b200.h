@@ -234,7 +234,8 @@ typedef struct sil_solve_settings {
     int32_t inner_iterations;    /* MIXED_IR / LEARNED: inner iterations per refinement pass */
     double inner_tolerance;      /* MIXED_IR / LEARNED: inner relative reduction per pass */
     sil_precond preconditioner;  /* LEARNED: the trained network */
-    int32_t stall_window;        /* LEARNED: iterations per stall check (0: 100) */
+    int32_t stall_window;        /* LEARNED: iterations per stall check (0: 200) */
+    int32_t flexible_directions; /* LEARNED: directions the flexible CG keeps, 1..16 (0: 8) */
 } sil_solve_settings;
 
 typedef struct sil_solve_diagnostics {
@@ -289,6 +290,11 @@ sil_status sil_precond_set_params(sil_precond p, const float* host, sil_stream s
 /* out = M(r) for 1..64 samples (device arrays). */
 sil_status sil_precond_apply(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
                              const float* nu, const float* r, float* out);
+/* The same for the samples whose entry of `active` (device, one int32 per
+ * sample, read when the kernels run) is nonzero; the others are neither read
+ * nor written, so a batched Krylov loop pays only for unconverged samples. */
+sil_status sil_precond_apply_active(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
+                                    const float* nu, const float* r, const int32_t* active, float* out);
 /* Mean loss over the batch for right-hand sides b with solutions x, the
  * per-sample losses (host, may be NULL) and the gradient with respect to
  * every parameter (host FP32, may be NULL).  Synchronous. */

@@ -75,6 +75,7 @@ class SilSolveSettings(ctypes.Structure):
         ("inner_tolerance", ctypes.c_double),
         ("preconditioner", ctypes.c_void_p),
         ("stall_window", ctypes.c_int32),
+        ("flexible_directions", ctypes.c_int32),
     ]
 
 
@@ -136,6 +137,8 @@ SIGNATURES = [
     ("sil_precond_get_params", ctypes.c_int, [_P, _P]),
     ("sil_precond_set_params", ctypes.c_int, [_P, _P, _P]),
     ("sil_precond_apply", ctypes.c_int, [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P]),
+    ("sil_precond_apply_active", ctypes.c_int,
+     [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P, _P]),
     ("sil_precond_loss_grad", ctypes.c_int, [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P,
                                              ctypes.POINTER(ctypes.c_double), _P, _P]),
     ("sil_precond_train_step", ctypes.c_int, [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P,

@@ -52,6 +52,9 @@ __global__ void reciprocal_kernel(double const* mu, double* nu, int64_t n)
 
 // ------------------------------------------------------------------ batched CG
 
+// Directions the flexible CG keeps at most.
+constexpr int kMaxDirs = 16;
+
 struct Item
 {
     int prob;
@@ -70,6 +73,8 @@ struct Vecs
     T* q;
     T* dinv;
     T* nu;
+    T* ph;  // flexible CG: m stored directions p_j at ph + j * hstride
+    T* qh;  // and their images q_j = A p_j
 };
 
 struct ProbInfo
@@ -354,11 +359,12 @@ struct Scalars
     int nonfinite;
     int counter_a, counter_b, counter_c;
     // flexible CG with the learned preconditioner
-    double pq;        // p . q of the current direction
     double win_rr;    // r . r at the start of the stall window
     int win_iters;    // iterations into the stall window
     int fallback;     // 1: the plain solver takes over this problem
     int learned_iters;
+    double pq_hist[kMaxDirs];  // p_j . q_j of the stored directions
+    double coef[kMaxDirs];     // (z . q_j) / (p_j . q_j) of the current z
 };
 
 // Deterministic block sum of one double per thread.
@@ -547,10 +553,19 @@ __global__ void __launch_bounds__(kThreads) cg_direction_kernel(Item const* item
 
 // ------------------------------------------------------------------ flexible CG (learned preconditioner)
 //
-// Notay's flexible CG with one-step truncation: alpha = (p.r)/(p.q),
-// beta = -(z.q)/(p.q), z = M(r) from the learned preconditioner, which is not
-// a fixed linear operator.  A problem whose residual has not dropped 10x over
-// `window` iterations is marked for the plain solver.
+// Notay's truncated flexible CG, FCG(m): z = M(r) from the learned
+// preconditioner, which is not a fixed linear operator, is made A-orthogonal
+// to the last m directions, p = z - sum_j (z.q_j)/(p_j.q_j) p_j with
+// q_j = A p_j, then alpha = (p.r)/(p.q).  Directions live in a ring of m
+// slots; iteration k writes slot k mod m.  m = 1 is the one-step truncation
+// p = z + beta p.  A problem whose residual has not dropped 10x over `window`
+// iterations is marked for the plain solver.
+
+template <class T>
+__device__ __forceinline__ T* fcg_slot(T* base, int64_t hstride, int slot)
+{
+    return base + static_cast<int64_t>(slot) * hstride;
+}
 
 // x = 0, r = r64 / scale (precision T), rr0 = r.r; stall window reset.
 // Problems already handed to the plain solver get a zero correction.
@@ -590,23 +605,81 @@ __global__ void __launch_bounds__(kThreads) fcg_init_kernel(Item const* items, P
     }
 }
 
-// p = z for the first direction.
-template <class T>
-__global__ void __launch_bounds__(kThreads) fcg_first_direction_kernel(Item const* items, Vecs<T> const* vecs,
-                                                                       Scalars const* sc)
+// Partials z.q_j over the stored directions (the first min(iters, m)); the
+// last CTA forms coef_j = (z.q_j)/(p_j.q_j).  M >= m is the compile-time bound.
+template <class T, int M>
+__global__ void __launch_bounds__(kThreads) fcg_orth_kernel(Item const* items, ProbInfo const* info,
+                                                            Vecs<T> const* vecs, Scalars* sc, double* parts_base,
+                                                            int64_t hstride, int m)
+{
+    __shared__ double red[kThreads / 32];
+    __shared__ double vals[M];
+    Item const it = items[blockIdx.x];
+    Scalars* s = sc + it.prob;
+    if (s->done || s->outer_done || s->fallback) return;
+    ProbInfo const pi = info[it.prob];
+    Vecs<T> const v = vecs[it.prob];
+    int const nvalid = min(s->iters, m);
+    if (nvalid == 0) return;
+    double acc[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) acc[j] = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        double const z = static_cast<double>(v.z[row]);
+#pragma unroll
+        for (int j = 0; j < M; ++j)
+            if (j < nvalid) acc[j] += z * static_cast<double>(fcg_slot(v.qh, hstride, j)[row]);
+    }
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+        double const t = block_sum(acc[j], red);
+        if (threadIdx.x == 0) vals[j] = t;
+    }
+    __syncthreads();
+    double* parts[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) parts[j] = parts_base + static_cast<int64_t>(j) * gridDim.x;
+    double tot[M];
+    if (finish_reduction_k<M>(vals, parts, it.index, pi.first_item, pi.nitems, &s->counter_a, tot)) {
+        for (int j = 0; j < nvalid; ++j) {
+            s->coef[j] = tot[j] / s->pq_hist[j];
+            if (!isfinite(s->coef[j])) s->nonfinite = 1;
+        }
+    }
+}
+
+// p_slot = z - sum_j coef_j p_j, slot = iters mod m.  When the ring is full
+// the slot being written is also the oldest term of the sum; each thread
+// reads its element of every p_j before writing.
+template <class T, int M>
+__global__ void __launch_bounds__(kThreads) fcg_direction_kernel(Item const* items, Vecs<T> const* vecs,
+                                                                 Scalars const* sc, int64_t hstride, int m)
 {
     Item const it = items[blockIdx.x];
     Scalars const* s = sc + it.prob;
     if (s->done || s->outer_done || s->fallback) return;
     Vecs<T> const v = vecs[it.prob];
-    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) v.p[row] = v.z[row];
+    int const nvalid = min(s->iters, m);
+    int const slot = s->iters % m;
+    T c[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) c[j] = j < nvalid ? static_cast<T>(s->coef[j]) : T(0);
+    T* const out = fcg_slot(v.ph, hstride, slot);
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        T p = v.z[row];
+#pragma unroll
+        for (int j = 0; j < M; ++j)
+            if (j < nvalid) p -= c[j] * fcg_slot(v.ph, hstride, j)[row];
+        out[row] = p;
+    }
 }
 
-// q = A p, partials p.q and p.r; the last CTA forms alpha.
+// q_slot = A p_slot, partials p.q and p.r; the last CTA stores p.q for the
+// slot and forms alpha.
 template <class T>
 __global__ void __launch_bounds__(kThreads) fcg_apply_kernel(Item const* items, ProbInfo const* info,
                                                              Vecs<T> const* vecs, Scalars* sc, double* part_a,
-                                                             double* part_b)
+                                                             double* part_b, int64_t hstride, int m)
 {
     __shared__ double red[kThreads / 32];
     Item const it = items[blockIdx.x];
@@ -614,11 +687,14 @@ __global__ void __launch_bounds__(kThreads) fcg_apply_kernel(Item const* items, 
     if (s->done || s->outer_done || s->fallback) return;
     ProbInfo const pi = info[it.prob];
     Vecs<T> const v = vecs[it.prob];
+    int const slot = s->iters % m;
+    T const* const p = fcg_slot(v.ph, hstride, slot);
+    T* const qo = fcg_slot(v.qh, hstride, slot);
     double pq = 0.0, pr = 0.0;
     for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-        T const q = mag_apply_row(v.p, v.nu, pi, row);
-        v.q[row] = q;
-        double const pv = static_cast<double>(v.p[row]);
+        T const q = mag_apply_row(p, v.nu, pi, row);
+        qo[row] = q;
+        double const pv = static_cast<double>(p[row]);
         pq += pv * static_cast<double>(q);
         pr += pv * static_cast<double>(v.r[row]);
     }
@@ -629,18 +705,18 @@ __global__ void __launch_bounds__(kThreads) fcg_apply_kernel(Item const* items, 
     double tot[2];
     if (finish_reduction_k<2>(vals, parts, it.index, pi.first_item, pi.nitems, &s->counter_a, tot)) {
         double const tpq = tot[0], tot_pr = tot[1];
-        s->pq = tpq;
+        s->pq_hist[slot] = tpq;
         s->alpha = tot_pr / tpq;
         if (!isfinite(s->alpha)) s->nonfinite = 1;
     }
 }
 
-// x += alpha p, r -= alpha q, partial r.r; the last CTA checks convergence
-// and the stall window.
+// x += alpha p_slot, r -= alpha q_slot, partial r.r; the last CTA advances
+// the iteration (and so the slot) and checks convergence and the stall window.
 template <class T>
 __global__ void __launch_bounds__(kThreads) fcg_update_kernel(Item const* items, ProbInfo const* info,
                                                               Vecs<T> const* vecs, Scalars* sc, double* part,
-                                                              int window)
+                                                              int window, int64_t hstride, int m)
 {
     __shared__ double red[kThreads / 32];
     Item const it = items[blockIdx.x];
@@ -648,11 +724,14 @@ __global__ void __launch_bounds__(kThreads) fcg_update_kernel(Item const* items,
     if (s->done || s->outer_done || s->fallback) return;
     ProbInfo const pi = info[it.prob];
     Vecs<T> const v = vecs[it.prob];
+    int const slot = s->iters % m;
+    T const* const p = fcg_slot(v.ph, hstride, slot);
+    T const* const q = fcg_slot(v.qh, hstride, slot);
     T const alpha = static_cast<T>(s->alpha);
     double rr = 0.0;
     for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-        T const r = v.r[row] - alpha * v.q[row];
-        v.x[row] = v.x[row] + alpha * v.p[row];
+        T const r = v.r[row] - alpha * q[row];
+        v.x[row] = v.x[row] + alpha * p[row];
         v.r[row] = r;
         rr += static_cast<double>(r) * static_cast<double>(r);
     }
@@ -676,26 +755,14 @@ __global__ void __launch_bounds__(kThreads) fcg_update_kernel(Item const* items,
     }
 }
 
-// Partial z.q; the last CTA forms beta = -(z.q)/(p.q).
-template <class T>
-__global__ void __launch_bounds__(kThreads) fcg_beta_kernel(Item const* items, ProbInfo const* info,
-                                                            Vecs<T> const* vecs, Scalars* sc, double* part)
+// active[p] = 1 while problem p's flexible CG still iterates; the network
+// skips the others.
+__global__ void fcg_active_kernel(Scalars const* sc, int np, int* active)
 {
-    __shared__ double red[kThreads / 32];
-    Item const it = items[blockIdx.x];
-    Scalars* s = sc + it.prob;
-    if (s->done || s->outer_done || s->fallback) return;
-    ProbInfo const pi = info[it.prob];
-    Vecs<T> const v = vecs[it.prob];
-    double zq = 0.0;
-    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads)
-        zq += static_cast<double>(v.z[row]) * static_cast<double>(v.q[row]);
-    double const zq_b = block_sum(zq, red);
-    double tot = 0.0;
-    if (finish_reduction(zq_b, part, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot)) {
-        s->beta = -tot / s->pq;
-        if (!isfinite(s->beta)) s->nonfinite = 1;
-    }
+    int const p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    Scalars const& s = sc[p];
+    active[p] = (s.done || s.outer_done || s.fallback) ? 0 : 1;
 }
 
 // r64 = b - A x64 and its norm (outer residual, FP64); marks outer convergence.
@@ -869,10 +936,14 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     size_t const vec_bytes = ((total_rows * sizeof(T) + 255) / 256) * 256;
     size_t const d_bytes = ((total_rows * sizeof(double) + 255) / 256) * 256;
     size_t const ndouble_vecs = 3;  // nu64, r64, x64
-    size_t bytes = nvec * vec_bytes + ndouble_vecs * d_bytes;
+    // Flexible CG ring: m stored directions and their images; m = 1 reuses p and q.
+    int const fdirs = learned != nullptr ? (set.flexible_directions > 0 ? set.flexible_directions : 8) : 1;
+    if (fdirs > kMaxDirs) return fail(SIL_ERR_INVALID, "flexible_directions exceeds 16");
+    int const nhist = fdirs > 1 ? 2 * fdirs : 0;
+    size_t bytes = (nvec + nhist) * vec_bytes + ndouble_vecs * d_bytes;
     bytes += sizeof(Item) * nitems + sizeof(ProbInfo) * np + sizeof(Vecs<T>) * np + sizeof(Scalars) * np
-             + 3 * sizeof(double) * nitems + 7 * sizeof(void*) * np + sp64.size() * (sizeof(double) + sizeof(float))
-             + 20 * 256;
+             + (3 + kMaxDirs) * sizeof(double) * nitems + 7 * sizeof(void*) * np
+             + sp64.size() * (sizeof(double) + sizeof(float)) + sizeof(int) * np + 22 * 256;
     DeviceBuffer buf;
     SIL_CUDA_CHECK(cudaMalloc(&buf.ptr, bytes));
     char* base = static_cast<char*>(buf.ptr);
@@ -883,6 +954,8 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     };
     T* vec_base[nvec];
     for (int k = 0; k < nvec; ++k) vec_base[k] = reinterpret_cast<T*>(take(vec_bytes));
+    T* hist_base = nhist > 0 ? reinterpret_cast<T*>(take(nhist * vec_bytes)) : nullptr;
+    int64_t const hstride = static_cast<int64_t>(vec_bytes / sizeof(T));
     double* nu64_base = reinterpret_cast<double*>(take(d_bytes));
     double* r64_base = reinterpret_cast<double*>(take(d_bytes));
     double* x64_base = reinterpret_cast<double*>(take(d_bytes));
@@ -893,6 +966,8 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     double* part_a = reinterpret_cast<double*>(take(sizeof(double) * nitems));
     double* part_b = reinterpret_cast<double*>(take(sizeof(double) * nitems));
     double* part_c = reinterpret_cast<double*>(take(sizeof(double) * nitems));
+    double* part_h = reinterpret_cast<double*>(take(sizeof(double) * kMaxDirs * nitems));
+    int* d_active = reinterpret_cast<int*>(take(sizeof(int) * np));
     double const** d_mu = reinterpret_cast<double const**>(take(sizeof(void*) * np));
     double const** d_rhs = reinterpret_cast<double const**>(take(sizeof(void*) * np));
     double** d_nu64 = reinterpret_cast<double**>(take(sizeof(void*) * np));
@@ -928,7 +1003,9 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     int64_t off = 0;
     for (int p = 0; p < np; ++p) {
         vecs[p] = {vec_base[0] + off, vec_base[1] + off, vec_base[2] + off, vec_base[3] + off,
-                   vec_base[4] + off, vec_base[5] + off, vec_base[6] + off};
+                   vec_base[4] + off, vec_base[5] + off, vec_base[6] + off,
+                   nhist > 0 ? hist_base + off : vec_base[3] + off,
+                   nhist > 0 ? hist_base + fdirs * hstride + off : vec_base[4] + off};
         mu[p] = probs[p].node_mu;
         rhs[p] = probs[p].rhs;
         nu64[p] = nu64_base + off;
@@ -1041,10 +1118,26 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
             float const* dv = vec_base[5];
             float* rv = vec_base[1];
             float* zv = vec_base[2];
-            int const window = set.stall_window > 0 ? set.stall_window : 100;
+            int const window = set.stall_window > 0 ? set.stall_window : 200;
             double const ltol = set.inner_tolerance > 0 ? set.inner_tolerance : 1e-5;
             int const lmax = set.inner_iterations > 0 ? set.inner_iterations : 4000;
             int const lchunk = 8;
+            // z -> A-orthogonal direction in the next ring slot.
+            auto new_direction = [&](cudaStream_t cs) {
+                if (fdirs <= 1) {
+                    fcg_orth_kernel<T, 1><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_h, hstride, fdirs);
+                    fcg_direction_kernel<T, 1><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc, hstride, fdirs);
+                } else if (fdirs <= 4) {
+                    fcg_orth_kernel<T, 4><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_h, hstride, fdirs);
+                    fcg_direction_kernel<T, 4><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc, hstride, fdirs);
+                } else if (fdirs <= 8) {
+                    fcg_orth_kernel<T, 8><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_h, hstride, fdirs);
+                    fcg_direction_kernel<T, 8><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc, hstride, fdirs);
+                } else {
+                    fcg_orth_kernel<T, 16><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_h, hstride, fdirs);
+                    fcg_direction_kernel<T, 16><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc, hstride, fdirs);
+                }
+            };
             cudaGraph_t lgraph = nullptr;
             cudaGraphExec_t lexec = nullptr;
             {
@@ -1052,11 +1145,13 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
                 SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
                 cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
                 for (int c = 0; c < lchunk && err == cudaSuccess && lst == SIL_OK; ++c) {
-                    fcg_apply_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a, part_b);
-                    fcg_update_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_c, window);
-                    lst = net->forward(ws, nuf, dv, rv, zv, cs);
-                    fcg_beta_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a);
-                    cg_direction_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc);
+                    fcg_apply_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a, part_b,
+                                                                     hstride, fdirs);
+                    fcg_update_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_c, window,
+                                                                      hstride, fdirs);
+                    fcg_active_kernel<<<(np + 63) / 64, 64, 0, cs>>>(d_sc, np, d_active);
+                    lst = net->forward(ws, nuf, dv, rv, zv, cs, d_active);
+                    new_direction(cs);
                 }
                 cudaError_t const err2 = cudaStreamEndCapture(cs, &lgraph);
                 if (err == cudaSuccess) err = err2;
@@ -1074,9 +1169,10 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
                 for (int p = 0; p < np; ++p) active = active || (!hs[p].outer_done && !hs[p].fallback);
                 if (!active) break;
                 fcg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, d_r64, d_sc, part_a);
-                lst = net->forward(ws, nuf, dv, rv, zv, stream);
+                fcg_active_kernel<<<(np + 63) / 64, 64, 0, stream>>>(d_sc, np, d_active);
+                lst = net->forward(ws, nuf, dv, rv, zv, stream, d_active);
                 if (lst != SIL_OK) break;
-                fcg_first_direction_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_sc);
+                new_direction(stream);
                 SIL_CUDA_CHECK(cudaGetLastError());
                 int used = 0;
                 lst = run_graph_until_done(lexec, lchunk, std::min(lmax, max_iter - tot), &used);

@@ -59,7 +59,15 @@ struct Table
     int32_t tile_base[kMaxImages + 1];
     Img img[kMaxImages];
     Img aux[kMaxImages];
+    int32_t sample[kMaxImages];   // batch sample of each image
+    int const* active;            // per batch sample: 0 = skip its images (NULL: all run)
 };
+
+// An image whose sample is switched off is neither read nor written.
+__device__ __forceinline__ bool image_active(Table const& t, int im)
+{
+    return t.active == nullptr || __ldg(t.active + t.sample[im]) != 0;
+}
 
 // Convolution inputs: kPlain the level's own tensor; kUpAdd skip + nearest
 // upsampled coarse tensor (two operands summed by the tensor core); kMasked a
@@ -102,6 +110,21 @@ __device__ __forceinline__ int find_image(Table const& t, int tile)
         else hi = mid - 1;
     }
     return lo;
+}
+
+// First tile >= tile in this CTA's round-robin sequence (tile, tile + G, ...)
+// whose image is active; ntiles when there is none.  Inactive images are
+// stepped over whole.
+__device__ __forceinline__ int next_active_tile(Table const& t, int tile, int ntiles)
+{
+    int const G = static_cast<int>(gridDim.x);
+    while (tile < ntiles) {
+        int const im = find_image(t, tile);
+        if (image_active(t, im)) return tile;
+        int const end = t.tile_base[im + 1];
+        tile += ((end - tile + G - 1) / G) * G;
+    }
+    return ntiles;
 }
 
 // The 32 channels (four 16-byte chunks) of the convolution input at padded
@@ -312,17 +335,18 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
         stage_halo(s.halo[buf], t, im2, start2, P2, in, false);
         cp_async_commit();
     };
-    if (ring && static_cast<int>(blockIdx.x) < ntiles) stage(blockIdx.x, 0);
+    int tile = next_active_tile(t, blockIdx.x, ntiles);
+    if (ring && tile < ntiles) stage(tile, 0);
     int iter = 0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++iter) {
+    for (; tile < ntiles; ++iter) {
         int const im = find_image(t, tile);
         Img const o = t.img[im];
         int const P = o.w + 2;
         int const start = P + (tile - t.tile_base[im]) * kTilePx;
+        int const nxt = next_active_tile(t, tile + static_cast<int>(gridDim.x), ntiles);
         int cur = 0;
         if (ring) {
             cur = iter & 1;
-            int const nxt = tile + static_cast<int>(gridDim.x);
             if (nxt < ntiles) {
                 stage(nxt, cur ^ 1);
                 cp_async_wait_group1();
@@ -426,6 +450,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
         }
         tc_fence_before();
         __syncthreads();
+        tile = nxt;
     }
     cp_async_wait_all();  // no copy may still target this CTA's shared memory at exit
     if (s.abort && tid == 0) atomicExch(error_flag, 1);
@@ -440,7 +465,7 @@ __global__ void out_gather_kernel(const __grid_constant__ Table t, float const* 
                                   float const* params, float* out)
 {
     int const im = blockIdx.y;
-    if (im >= t.nimg) return;
+    if (im >= t.nimg || !image_active(t, im)) return;
     Img const o = t.img[im];
     int const P = o.w + 2, npx = P * (o.h + 2);
     int const g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -460,7 +485,7 @@ __global__ void out_gather_kernel(const __grid_constant__ Table t, float const* 
 __global__ void pool_kernel(const __grid_constant__ Table t, bf16 const* fine, bf16* coarse)
 {
     int const im = blockIdx.y;
-    if (im >= t.nimg) return;
+    if (im >= t.nimg || !image_active(t, im)) return;
     Img const o = t.img[im];
     int const P = o.w + 2, npx = P * (o.h + 2);
     int const g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -630,7 +655,7 @@ __global__ void __launch_bounds__(256) inc_forward_kernel(const __grid_constant_
     for (int i = threadIdx.x; i < kInW + kCh; i += blockDim.x) w[i] = params[kOffIn + i];
     __syncthreads();
     int const im = blockIdx.y;
-    if (im >= t.nimg) return;
+    if (im >= t.nimg || !image_active(t, im)) return;
     Img const o = t.img[im];
     int const P = o.w + 2, npx = P * (o.h + 2);
     int const g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -670,7 +695,7 @@ __global__ void __launch_bounds__(256) out_forward_kernel(const __grid_constant_
     for (int i = threadIdx.x; i < kOutW + 1; i += blockDim.x) w[i] = params[kOffOut + i];
     __syncthreads();
     int const im = blockIdx.y;
-    if (im >= t.nimg) return;
+    if (im >= t.nimg || !image_active(t, im)) return;
     Img const o = t.img[im];
     int const P = o.w + 2, npx = P * (o.h + 2);
     int const g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -900,7 +925,7 @@ __global__ void upadd_adjoint_coarse_kernel(const __grid_constant__ Table t, flo
 __global__ void copy_act_kernel(const __grid_constant__ Table t, bf16 const* src, bf16* dst)
 {
     int const im = blockIdx.y;
-    if (im >= t.nimg) return;
+    if (im >= t.nimg || !image_active(t, im)) return;
     Img const f = t.img[im];
     int64_t const idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= static_cast<int64_t>(f.h + 2) * (f.w + 2) * kChunks) return;
@@ -916,7 +941,13 @@ struct Samples
     Sample s[kMaxImages];
     Img top[kMaxImages];                 // level-0 network image of each sample
     int32_t item_base[kMaxImages + 1];   // first fused-wrapper work item of each sample
+    int const* active;                   // per sample: 0 = skip (NULL: all run)
 };
+
+__device__ __forceinline__ bool sample_active(Samples const& ss, int i)
+{
+    return ss.active == nullptr || __ldg(ss.active + i) != 0;
+}
 
 __device__ __forceinline__ bool node_of(Samples const& ss, int64_t& row, Sample& sm)
 {
@@ -1029,6 +1060,7 @@ __global__ void features_kernel(const __grid_constant__ Samples ss, float const*
                                 float const* dinv, double const* dots, float* feat)
 {
     int const sidx = blockIdx.y;
+    if (!sample_active(ss, sidx)) return;
     Sample const sm = ss.s[sidx];
     Img const o = ss.top[sidx];
     int64_t const P = o.w + 2, npx = P * (o.h + 2);
@@ -1177,6 +1209,7 @@ __global__ void __launch_bounds__(256) wrap_pre_kernel(const __grid_constant__ S
 {
     __shared__ double red[8];
     WrapItem const it = items[blockIdx.x];
+    if (!sample_active(ss, it.sample)) return;
     Sample const sm = ss.s[it.sample];
     int const nx = sm.nx, ny = sm.ny;
     float const* nu_s = nu + sm.offset;
@@ -1202,7 +1235,7 @@ __global__ void __launch_bounds__(256) wrap_pre_kernel(const __grid_constant__ S
 __global__ void wrap_finish_kernel(const __grid_constant__ Samples ss, double const* part, double* dots)
 {
     int const sidx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sidx >= ss.n) return;
+    if (sidx >= ss.n || !sample_active(ss, sidx)) return;
     double t = 0.0;
     for (int k = ss.item_base[sidx]; k < ss.item_base[sidx + 1]; ++k) t += part[k];
     dots[sidx * 3] = t;
@@ -1215,6 +1248,7 @@ __global__ void __launch_bounds__(256) wrap_post_kernel(const __grid_constant__ 
                                                         float* out)
 {
     WrapItem const it = items[blockIdx.x];
+    if (!sample_active(ss, it.sample)) return;
     Sample const sm = ss.s[it.sample];
     Img const o = ss.top[it.sample];
     int const nx = sm.nx, ny = sm.ny;
@@ -1305,6 +1339,7 @@ public:
     DevBuf wparts;                 // weight-gradient partials
     int wgrad_grid = 0;
     int64_t max_node_per_sample = 0;
+    int const* active = nullptr;   // per-sample switch of the current forward (NULL: all)
 
     sil_status build(std::vector<Sample> const& s);
     Table table(int level, int aux_level, bool aux_is_finer) const;
@@ -1425,8 +1460,10 @@ Table Workspace::table(int level, int aux_level, bool) const
     Level const& L = levels[level];
     t.nimg = static_cast<int>(L.images.size());
     t.tile_base[0] = 0;
+    t.active = active;
     for (int k = 0; k < t.nimg; ++k) {
         t.img[k] = L.img[k];
+        t.sample[k] = L.images[k];
         int64_t const tiles = (static_cast<int64_t>(L.img[k].w + 2) * L.img[k].h + kTilePx - 1) / kTilePx;
         t.tile_base[k + 1] = t.tile_base[k] + static_cast<int32_t>(tiles);
         if (aux_level >= 0) {
@@ -1704,12 +1741,14 @@ Table dec_table(Workspace const& w, int l)
 {
     Table t = w.table(l, l + 1, false);
     Table tt {};
+    tt.active = t.active;
     tt.tile_base[0] = 0;
     for (int k = 0; k < t.nimg; ++k) {
         if (t.aux[k].h == 0) continue;
         int const q = tt.nimg++;
         tt.img[q] = t.img[k];
         tt.aux[q] = t.aux[k];
+        tt.sample[q] = t.sample[k];
         tt.tile_base[q + 1] = tt.tile_base[q] + (t.tile_base[k + 1] - t.tile_base[k]);
     }
     return tt;
@@ -1719,12 +1758,14 @@ Table dec_table(Workspace const& w, int l)
 Table deepest_table(Workspace const& w, int l)
 {
     Table t {};
+    t.active = w.active;
     Level const& L = w.levels[l];
     for (size_t k = 0; k < L.images.size(); ++k) {
         if (w.depth[L.images[k]] - 1 != l) continue;
         int const q = t.nimg++;
         t.img[q] = L.img[k];
         t.aux[q] = L.img[k];
+        t.sample[q] = L.images[k];
         t.tile_base[q + 1] = t.tile_base[q];
     }
     return t;
@@ -1828,8 +1869,10 @@ sil_status net_backward(Net& net, Workspace& w, cudaStream_t st)
 // Preconditioner forward: out = M(b) for the batch of w (nu per node).
 // dinv: the inverse operator diagonal, or NULL to compute it here.
 sil_status precond_forward(Net& net, Workspace& w, float const* nu, float const* dinv, float const* b, float* out,
-                           cudaStream_t st, bool keep = false)
+                           cudaStream_t st, bool keep = false, int const* active = nullptr)
 {
+    w.active = active;
+    w.ss.active = active;
     if (dinv == nullptr) {
         dinv_kernel<<<node_grid(w), 256, 0, st>>>(w.ss, nu, w.dinv.as<float>());
         dinv = w.dinv.as<float>();
@@ -1860,14 +1903,15 @@ sil_status check_samples(std::vector<Sample> const& samples)
 
 } // namespace
 
-sil_status Net::apply(std::vector<Sample> const& samples, float const* nu, float const* r, float* out, cudaStream_t stream)
+sil_status Net::apply(std::vector<Sample> const& samples, float const* nu, float const* r, float* out, cudaStream_t stream,
+                      int const* active)
 {
     if (sil_status s = check_samples(samples); s != SIL_OK) return s;
     if (sil_status s = ensure_attributes(); s != SIL_OK) return s;
     sil_status st = SIL_OK;
     Workspace* w = workspace(samples, stream, &st);
     if (w == nullptr) return st;
-    return precond_forward(*this, *w, nu, nullptr, r, out, stream);
+    return precond_forward(*this, *w, nu, nullptr, r, out, stream, false, active);
 }
 
 sil_status Net::prepare(std::vector<Sample> const& samples, cudaStream_t stream, Workspace** out)
@@ -1880,9 +1924,9 @@ sil_status Net::prepare(std::vector<Sample> const& samples, cudaStream_t stream,
 }
 
 sil_status Net::forward(Workspace* w, float const* nu, float const* dinv, float const* r, float* out,
-                        cudaStream_t stream)
+                        cudaStream_t stream, int const* active)
 {
-    return precond_forward(*this, *w, nu, dinv, r, out, stream);
+    return precond_forward(*this, *w, nu, dinv, r, out, stream, false, active);
 }
 
 sil_status Net::loss_grad(std::vector<Sample> const& samples, float const* nu, float const* b, float const* x,
@@ -2043,6 +2087,16 @@ sil_status sil_precond_apply(sil_precond p, sil_stream stream, const sil_precond
     std::vector<Sample> s;
     if (sil_status st = to_samples(samples, n, &s); st != SIL_OK) return st;
     return p->net.apply(s, nu, r, out, static_cast<cudaStream_t>(stream));
+}
+
+sil_status sil_precond_apply_active(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
+                                    const float* nu, const float* r, const int32_t* active, float* out)
+{
+    if (p == nullptr || nu == nullptr || r == nullptr || out == nullptr || active == nullptr)
+        return sil::fail(SIL_ERR_INVALID, "sil_precond_apply_active: NULL");
+    std::vector<Sample> s;
+    if (sil_status st = to_samples(samples, n, &s); st != SIL_OK) return st;
+    return p->net.apply(s, nu, r, out, static_cast<cudaStream_t>(stream), active);
 }
 
 sil_status sil_precond_loss_grad(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,

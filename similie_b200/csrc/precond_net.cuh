@@ -78,11 +78,14 @@ public:
     // Workspace of a batch geometry (allocated once, before any stream capture).
     sil_status prepare(std::vector<Sample> const& samples, cudaStream_t stream, Workspace** out);
     // out = M(r) on a prepared workspace: kernel launches only (capturable).
-    // dinv: inverse operator diagonal per node (FP32), or NULL.
+    // dinv: inverse operator diagonal per node (FP32), or NULL.  active
+    // (device, one int per sample, or NULL): samples whose entry is 0 at
+    // launch time are skipped, their out left unwritten.
     sil_status forward(Workspace* w, float const* nu, float const* dinv, float const* r, float* out,
-                       cudaStream_t stream);
+                       cudaStream_t stream, int const* active = nullptr);
     // out = M(r) for a batch (device FP32 node arrays, nu FP32 per node).
-    sil_status apply(std::vector<Sample> const& samples, float const* nu, float const* r, float* out, cudaStream_t stream);
+    sil_status apply(std::vector<Sample> const& samples, float const* nu, float const* r, float* out, cudaStream_t stream,
+                     int const* active = nullptr);
     // Loss 1 - (u.b)^2 / ((u.K u)(x.b)) with u = M(b), mean over the batch,
     // and its gradient with respect to every parameter (into grad, device).
     sil_status loss_grad(std::vector<Sample> const& samples, float const* nu, float const* b, float const* x,

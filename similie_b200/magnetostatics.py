@@ -135,14 +135,15 @@ class Diagnostics:
 
 
 def solve_batch(mus, rhss, sols, shapes, solver="cg", tol=1e-10, max_iterations=200000, inner_iterations=4000,
-                inner_tolerance=1e-4, stream=None, preconditioner=None, stall_window=100):
+                inner_tolerance=1e-4, stream=None, preconditioner=None, stall_window=200, flexible_directions=8):
     """minimize_strong_formulation_residual for a batch of linear problems.
 
     mus, rhss, sols: lists of torch CUDA float64 tensors (flat nx*ny);
     shapes: list of (nx, ny).  solver: "cg" (FP64), "mixed" (FP32 inner CG
     inside FP64 refinement) or "learned" (flexible CG with `preconditioner`, a
-    similie_b200.precond.LearnedPreconditioner, at most 64 problems, then the
-    mixed solver for problems whose preconditioned residual stalls).
+    similie_b200.precond.LearnedPreconditioner, at most 64 problems, keeping
+    `flexible_directions` (1..16) A-orthogonal directions, then the mixed
+    solver for problems whose preconditioned residual stalls).
     Returns one Diagnostics per problem."""
     import torch
     n = len(shapes)
@@ -159,6 +160,7 @@ def solve_batch(mus, rhss, sols, shapes, solver="cg", tol=1e-10, max_iterations=
     st.inner_iterations = inner_iterations
     st.inner_tolerance = inner_tolerance
     st.stall_window = stall_window
+    st.flexible_directions = flexible_directions
     if preconditioner is not None:
         st.preconditioner = preconditioner._h.value
     diag = (_native.SilSolveDiagnostics * n)()

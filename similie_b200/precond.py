@@ -63,11 +63,18 @@ class LearnedPreconditioner:
     def load(self, path):
         self.set_params(np.load(path))
 
-    def apply(self, shapes, nu, r, out, stream=None):
-        """out = M(r); nu, r, out: flat torch CUDA float32 tensors laid out as pack_samples(shapes)."""
+    def apply(self, shapes, nu, r, out, stream=None, active=None):
+        """out = M(r); nu, r, out: flat torch CUDA float32 tensors laid out as pack_samples(shapes).
+        active: optional torch CUDA int32 tensor, one entry per sample; samples
+        whose entry is 0 are skipped (their part of out is left as it was)."""
         arr, n, _ = pack_samples(shapes)
-        check(lib().sil_precond_apply(self._h, _stream(stream), arr, len(shapes), nu.data_ptr(), r.data_ptr(),
-                                      out.data_ptr()), "precond_apply")
+        if active is None:
+            check(lib().sil_precond_apply(self._h, _stream(stream), arr, len(shapes), nu.data_ptr(), r.data_ptr(),
+                                          out.data_ptr()), "precond_apply")
+        else:
+            check(lib().sil_precond_apply_active(self._h, _stream(stream), arr, len(shapes), nu.data_ptr(),
+                                                 r.data_ptr(), active.data_ptr(), out.data_ptr()),
+                  "precond_apply_active")
         return out
 
     def loss_grad(self, shapes, nu, b, x, want_grad=True, stream=None):

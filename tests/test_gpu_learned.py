@@ -82,3 +82,35 @@ def test_stall_hands_problems_to_the_plain_solver(torch, mods):
     _check(probs, sols, d)
     assert any(x.fallback for x in d)
     assert all(x.iterations > x.learned_iterations for x in d if x.fallback)
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="trained weights not present")
+def test_more_flexible_directions_cut_iterations_on_inclusions(torch, mods):
+    """FCG(m): keeping 8 A-orthogonal directions instead of one takes the
+    preconditioned solve of inclusion problems (where the network's correction
+    varies most from step to step) to 1e-10 in markedly fewer iterations."""
+    mag, pc = mods
+    probs, mus, rhss = _batch(mag, torch, 33, (256, 384), cores=2)
+    shapes = [(p.nx, p.ny) for p in probs]
+    net = pc.LearnedPreconditioner(seed=0)
+    net.load(WEIGHTS)
+    its = {}
+    for m in (1, 4, 8, 16):
+        sols = [torch.zeros_like(r) for r in rhss]
+        d = mag.solve_batch(mus, rhss, sols, shapes, solver="learned", preconditioner=net, stall_window=100000,
+                            inner_iterations=20000, flexible_directions=m)
+        _check(probs, sols, d)
+        assert not any(x.fallback for x in d)
+        its[m] = sum(x.learned_iterations for x in d)
+    assert 3 * its[8] < 2 * its[1], its
+    assert its[16] <= its[4], its
+
+
+def test_flexible_directions_above_the_ring_size_are_rejected(torch, mods):
+    mag, pc = mods
+    probs, mus, rhss = _batch(mag, torch, 34, (64,), cores=0)
+    net = pc.LearnedPreconditioner(seed=0)
+    sols = [torch.zeros_like(r) for r in rhss]
+    from similie_b200._native import SilError
+    with pytest.raises(SilError, match="flexible_directions"):
+        mag.solve_batch(mus, rhss, sols, [(64, 64)], solver="learned", preconditioner=net, flexible_directions=17)

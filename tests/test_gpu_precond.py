@@ -71,6 +71,30 @@ def test_forward_matches_oracle(torch, pc):
         assert rel(g, ref) < 2e-2, ((nx, ny), rel(g, ref))
 
 
+def test_inactive_samples_are_skipped(torch, pc):
+    """apply with a per-sample switch: switched-on samples get exactly the
+    output of the full apply, switched-off samples are left untouched."""
+    batch = make_batch(SHAPES, 6)
+    net = pc.LearnedPreconditioner(seed=0)
+    net.set_params(P.init_params(6))
+    nu = flat(torch, [s[0] for s in batch])
+    r = flat(torch, [s[1] for s in batch])
+    full = torch.zeros_like(r)
+    net.apply(SHAPES, nu, r, full)
+    sizes = [nx * ny for nx, ny in SHAPES]
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    for mask in ([1, 0, 1], [0, 1, 0], [0, 0, 0], [1, 1, 1]):
+        out = torch.full_like(r, 7.0)
+        net.apply(SHAPES, nu, r, out, active=torch.tensor(mask, dtype=torch.int32, device="cuda"))
+        got, ref = out.cpu().numpy(), full.cpu().numpy()
+        for k, on in enumerate(mask):
+            sl = slice(offs[k], offs[k + 1])
+            if on:
+                assert np.array_equal(got[sl], ref[sl]), (mask, k)
+            else:
+                assert np.all(got[sl] == 7.0), (mask, k)
+
+
 def test_gradient_matches_oracle(torch, pc):
     batch = make_batch(SHAPES, 4)
     params = P.init_params(6)
