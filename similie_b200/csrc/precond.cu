@@ -61,6 +61,7 @@ struct Table
     Img aux[kMaxImages];
     int32_t sample[kMaxImages];   // batch sample of each image
     int const* active;            // per batch sample: 0 = skip its images (NULL: all run)
+    int64_t px_base[kMaxImages + 1];  // prefix of padded pixels: the images as one flat range
 };
 
 // An image whose sample is switched off is neither read nor written.
@@ -112,19 +113,83 @@ __device__ __forceinline__ int find_image(Table const& t, int tile)
     return lo;
 }
 
-// First tile >= tile in this CTA's round-robin sequence (tile, tile + G, ...)
-// whose image is active; ntiles when there is none.  Inactive images are
-// stepped over whole.
-__device__ __forceinline__ int next_active_tile(Table const& t, int tile, int ntiles)
+// Work of a launch is counted in units (tiles, pixels, wrapper items) per
+// image; only the units of active images are handed out.  scan_active
+// forms, in shared memory, the exclusive prefix pre[0..n] over the n <= 64
+// images of count(k) (0 for an inactive image): warp 0 scans two images per
+// lane.  Every thread of the block must call it; it ends with a barrier.
+static_assert(kMaxImages <= 64, "scan_active covers 64 images");
+template <class C>
+__device__ __forceinline__ void scan_active(int n, C const& count, int64_t* pre)
 {
-    int const G = static_cast<int>(gridDim.x);
-    while (tile < ntiles) {
-        int const im = find_image(t, tile);
-        if (image_active(t, im)) return tile;
-        int const end = t.tile_base[im + 1];
-        tile += ((end - tile + G - 1) / G) * G;
+    if (threadIdx.x < 32) {
+        int const lane = threadIdx.x;
+        int64_t const a = 2 * lane < n ? count(2 * lane) : 0;
+        int64_t const b = 2 * lane + 1 < n ? count(2 * lane + 1) : 0;
+        int64_t v = a + b;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int64_t const y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        int64_t const excl = v - a - b;
+        if (2 * lane < n) pre[2 * lane] = excl;
+        if (2 * lane + 1 < n) pre[2 * lane + 1] = excl + a;
+        if (lane == 31) pre[n] = v;
     }
-    return ntiles;
+    __syncthreads();
+}
+
+// Image of active unit u (u < pre[n]): the largest k with pre[k] <= u.  An
+// inactive image has pre[k] == pre[k + 1], so the search never stops on one.
+__device__ __forceinline__ int find_unit(int64_t const* pre, int n, int64_t u)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int const mid = (lo + hi + 1) / 2;
+        if (pre[mid] <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Walk of a compacted range of `total` = pre[n] * per elements: each block
+// takes one contiguous slice (a multiple of blockDim.x long), each thread
+// every blockDim.x-th element of it, and the image index advances as the
+// walk crosses image ends (zero-length inactive images are passed over), so
+// an element costs one compare beyond f(k, q), q the element's index within
+// image k.  No barrier may sit inside f.
+template <class F>
+__device__ __forceinline__ void walk_range(int64_t const* pre, int n, int per, F const& f)
+{
+    int64_t const B = blockDim.x, G = gridDim.x;
+    int64_t const total = pre[n] * per;
+    int64_t const slice = ((total + G - 1) / G + B - 1) / B * B;
+    int64_t e = static_cast<int64_t>(blockIdx.x) * slice + threadIdx.x;
+    int64_t const stop = min(total, static_cast<int64_t>(blockIdx.x + 1) * slice);
+    if (e >= stop) return;
+    int k = find_unit(pre, n, e / per);
+    int64_t base = pre[k] * per, end = pre[k + 1] * per;
+    for (; e < stop; e += B) {
+        while (e >= end) {
+            ++k;
+            base = end;
+            end = pre[k + 1] * per;
+        }
+        f(k, static_cast<int>(e - base));
+    }
+}
+
+// Elementwise kernels: the padded pixels of the table's active images, `per`
+// elements per pixel, as one compacted range; f(im, q) for element q of
+// image im (q < npx(im) * per).  The cost follows the active pixels,
+// whatever the number of inactive images.
+template <class F>
+__device__ __forceinline__ void walk_active(Table const& t, int64_t* pre, int per, F const& f)
+{
+    scan_active(
+        t.nimg, [&](int k) { return image_active(t, k) ? t.px_base[k + 1] - t.px_base[k] : int64_t(0); }, pre);
+    walk_range(pre, t.nimg, per, f);
 }
 
 // The 32 channels (four 16-byte chunks) of the convolution input at padded
@@ -285,6 +350,7 @@ struct ConvSmem
     uint64_t bar;
     uint32_t tmem;
     int abort;
+    int64_t pre[kMaxImages + 1];          // prefix of the active images' tiles
     uint4 halo[2][kChunks * 3 * kHalo];   // A operand sources: [chunk][halo row][halo pixel], 2 x 24960 B
 };
 
@@ -308,6 +374,9 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
     }
     if (out_taps != nullptr)
         for (int i = tid; i < kOutW; i += 128) s.wout[i] = wout[i];
+    scan_active(
+        t.nimg, [&](int k) { return image_active(t, k) ? int64_t(t.tile_base[k + 1] - t.tile_base[k]) : int64_t(0); },
+        s.pre);
     if (warp == 0) tmem_alloc(&s.tmem, 32);
     if (tid == 0) {
         mbar_init(&s.bar, 1);
@@ -335,15 +404,22 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
         stage_halo(s.halo[buf], t, im2, start2, P2, in, false);
         cp_async_commit();
     };
-    int tile = next_active_tile(t, blockIdx.x, ntiles);
+    // active tiles handed out round-robin; unit a is tile tile_of(a)
+    int const nact = static_cast<int>(s.pre[t.nimg]);
+    auto tile_of = [&](int a) {
+        int const k = find_unit(s.pre, t.nimg, a);
+        return t.tile_base[k] + (a - static_cast<int>(s.pre[k]));
+    };
+    int tile = static_cast<int>(blockIdx.x) < nact ? tile_of(blockIdx.x) : ntiles;
     if (ring && tile < ntiles) stage(tile, 0);
     int iter = 0;
-    for (; tile < ntiles; ++iter) {
+    for (int a = blockIdx.x; a < nact; a += gridDim.x, ++iter) {
         int const im = find_image(t, tile);
         Img const o = t.img[im];
         int const P = o.w + 2;
         int const start = P + (tile - t.tile_base[im]) * kTilePx;
-        int const nxt = next_active_tile(t, tile + static_cast<int>(gridDim.x), ntiles);
+        int const an = a + static_cast<int>(gridDim.x);
+        int const nxt = an < nact ? tile_of(an) : ntiles;
         int cur = 0;
         if (ring) {
             cur = iter & 1;
@@ -464,37 +540,35 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
 __global__ void out_gather_kernel(const __grid_constant__ Table t, float const* taps, int64_t taps_stride,
                                   float const* params, float* out)
 {
-    int const im = blockIdx.y;
-    if (im >= t.nimg || !image_active(t, im)) return;
-    Img const o = t.img[im];
-    int const P = o.w + 2, npx = P * (o.h + 2);
-    int const g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= npx) return;
-    int const y = g / P, x = g - y * P;
-    float a = 0.0f;
-    if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
-        a = params[kOffOut + kOutW];
-        int64_t const base = o.offset + g;
+    __shared__ int64_t pre[kMaxImages + 1];
+    float const bias = params[kOffOut + kOutW];
+    walk_active(t, pre, 1, [&](int im, int g) {
+        Img const o = t.img[im];
+        int const P = o.w + 2;
+        int const y = g / P, x = g - y * P;
+        float a = 0.0f;
+        if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
+            a = bias;
+            int64_t const base = o.offset + g;
 #pragma unroll
-        for (int tap = 0; tap < kTaps; ++tap) a = a + taps[tap * taps_stride + base + (tap / 3 - 1) * P + (tap % 3 - 1)];
-    }
-    out[o.offset + g] = a;
+            for (int tap = 0; tap < kTaps; ++tap)
+                a = a + taps[tap * taps_stride + base + (tap / 3 - 1) * P + (tap % 3 - 1)];
+        }
+        out[o.offset + g] = a;
+    });
 }
 
 // Coarse tensor = 2x2 average of the finer level (t.img coarse, t.aux fine), BF16.
 __global__ void pool_kernel(const __grid_constant__ Table t, bf16 const* fine, bf16* coarse)
 {
-    int const im = blockIdx.y;
-    if (im >= t.nimg || !image_active(t, im)) return;
-    Img const o = t.img[im];
-    int const P = o.w + 2, npx = P * (o.h + 2);
-    int const g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= npx) return;
-    uint4 v[kChunks];
-    load_pixel(kPool, t, im, g, fine, nullptr, nullptr, v);
-    uint4* dst = reinterpret_cast<uint4*>(coarse) + (o.offset + g) * kChunks;
+    __shared__ int64_t pre[kMaxImages + 1];
+    walk_active(t, pre, 1, [&](int im, int g) {
+        uint4 v[kChunks];
+        load_pixel(kPool, t, im, g, fine, nullptr, nullptr, v);
+        uint4* dst = reinterpret_cast<uint4*>(coarse) + (t.img[im].offset + g) * kChunks;
 #pragma unroll
-    for (int c = 0; c < kChunks; ++c) dst[c] = v[c];
+        for (int c = 0; c < kChunks; ++c) dst[c] = v[c];
+    });
 }
 
 // Shared memory of the weight-gradient kernel.  The im2col tile is followed
@@ -651,21 +725,25 @@ __global__ void convert_weights_kernel(float const* params, bf16* wf, bf16* wt)
 __global__ void __launch_bounds__(256) inc_forward_kernel(const __grid_constant__ Table t, float const* feat,
                                                           float const* params, bf16* out)
 {
-    __shared__ float w[kInW + kCh];
-    for (int i = threadIdx.x; i < kInW + kCh; i += blockDim.x) w[i] = params[kOffIn + i];
-    __syncthreads();
-    int const im = blockIdx.y;
-    if (im >= t.nimg || !image_active(t, im)) return;
-    Img const o = t.img[im];
-    int const P = o.w + 2, npx = P * (o.h + 2);
-    int const g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= npx) return;
-    int const y = g / P, x = g - y * P;
-    float acc[kCh];
-    if (y == 0 || x == 0 || y > o.h || x > o.w) {
+    // weights transposed to [input k][output channel], four channels per float4
+    __shared__ float4 w4[kTaps * 2][kCh / 4];
+    __shared__ float4 b4[kCh / 4];
+    __shared__ int64_t pre[kMaxImages + 1];
+    for (int i = threadIdx.x; i < kInW; i += blockDim.x) {
+        int const k = i / kCh, co = i - k * kCh;
+        reinterpret_cast<float*>(w4[k])[co] = params[kOffIn + co * kTaps * 2 + k];
+    }
+    for (int i = threadIdx.x; i < kCh; i += blockDim.x) reinterpret_cast<float*>(b4)[i] = params[kOffIn + kInW + i];
+    walk_active(t, pre, 1, [&](int im, int g) {
+        Img const o = t.img[im];
+        int const P = o.w + 2;
+        int const y = g / P, x = g - y * P;
+        uint4* dst = reinterpret_cast<uint4*>(out + (o.offset + g) * kCh);
+        if (y == 0 || x == 0 || y > o.h || x > o.w) {
 #pragma unroll
-        for (int i = 0; i < kCh; ++i) acc[i] = 0.0f;
-    } else {
+            for (int q = 0; q < 4; ++q) dst[q] = make_uint4(0u, 0u, 0u, 0u);
+            return;
+        }
         float in[kTaps * 2];
         float2 const* f2 = reinterpret_cast<float2 const*>(feat) + o.offset;
 #pragma unroll
@@ -674,17 +752,31 @@ __global__ void __launch_bounds__(256) inc_forward_kernel(const __grid_constant_
             in[2 * tap] = v.x;
             in[2 * tap + 1] = v.y;
         }
-#pragma unroll 4
-        for (int co = 0; co < kCh; ++co) {
-            float a = w[kInW + co];
+        // eight output channels at a time: bias, then the 18 inputs in order
+#pragma unroll 1
+        for (int q = 0; q < 4; ++q) {
+            float a[8];
+            float4 const b0 = b4[2 * q], b1 = b4[2 * q + 1];
+            a[0] = b0.x; a[1] = b0.y; a[2] = b0.z; a[3] = b0.w;
+            a[4] = b1.x; a[5] = b1.y; a[6] = b1.z; a[7] = b1.w;
 #pragma unroll
-            for (int k = 0; k < kTaps * 2; ++k) a = __fmaf_rn(w[co * kTaps * 2 + k], in[k], a);
-            acc[co] = fmaxf(a, 0.0f);
+            for (int k = 0; k < kTaps * 2; ++k) {
+                float const v = in[k];
+                float4 const w0 = w4[k][2 * q], w1 = w4[k][2 * q + 1];
+                a[0] = __fmaf_rn(w0.x, v, a[0]);
+                a[1] = __fmaf_rn(w0.y, v, a[1]);
+                a[2] = __fmaf_rn(w0.z, v, a[2]);
+                a[3] = __fmaf_rn(w0.w, v, a[3]);
+                a[4] = __fmaf_rn(w1.x, v, a[4]);
+                a[5] = __fmaf_rn(w1.y, v, a[5]);
+                a[6] = __fmaf_rn(w1.z, v, a[6]);
+                a[7] = __fmaf_rn(w1.w, v, a[7]);
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = fmaxf(a[i], 0.0f);
+            dst[q] = pack8(a);
         }
-    }
-    uint4* dst = reinterpret_cast<uint4*>(out + (o.offset + g) * kCh);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) dst[q] = pack8(acc + 8 * q);
+    });
 }
 
 // Output convolution 32 -> 1 (+ bias), FP32 out, zero border.
@@ -692,35 +784,33 @@ __global__ void __launch_bounds__(256) out_forward_kernel(const __grid_constant_
                                                           float const* params, float* out)
 {
     __shared__ float w[kOutW + 1];
+    __shared__ int64_t pre[kMaxImages + 1];
     for (int i = threadIdx.x; i < kOutW + 1; i += blockDim.x) w[i] = params[kOffOut + i];
-    __syncthreads();
-    int const im = blockIdx.y;
-    if (im >= t.nimg || !image_active(t, im)) return;
-    Img const o = t.img[im];
-    int const P = o.w + 2, npx = P * (o.h + 2);
-    int const g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= npx) return;
-    int const y = g / P, x = g - y * P;
-    float a = 0.0f;
-    if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
-        a = w[kOutW];
-        uint4 const* src = reinterpret_cast<uint4 const*>(in) + o.offset * kChunks;
+    walk_active(t, pre, 1, [&](int im, int g) {
+        Img const o = t.img[im];
+        int const P = o.w + 2;
+        int const y = g / P, x = g - y * P;
+        float a = 0.0f;
+        if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
+            a = w[kOutW];
+            uint4 const* src = reinterpret_cast<uint4 const*>(in) + o.offset * kChunks;
 #pragma unroll 3
-        for (int tap = 0; tap < kTaps; ++tap) {
-            int const q = g + (tap / 3 - 1) * P + (tap % 3 - 1);
-            uint4 v[kChunks];
+            for (int tap = 0; tap < kTaps; ++tap) {
+                int const q = g + (tap / 3 - 1) * P + (tap % 3 - 1);
+                uint4 v[kChunks];
 #pragma unroll
-            for (int c = 0; c < kChunks; ++c) v[c] = __ldg(src + static_cast<int64_t>(q) * kChunks + c);
+                for (int c = 0; c < kChunks; ++c) v[c] = __ldg(src + static_cast<int64_t>(q) * kChunks + c);
 #pragma unroll
-            for (int c = 0; c < kChunks; ++c) {
-                float f[8];
-                unpack8(v[c], f);
+                for (int c = 0; c < kChunks; ++c) {
+                    float f[8];
+                    unpack8(v[c], f);
 #pragma unroll
-                for (int e = 0; e < 8; ++e) a = __fmaf_rn(w[tap * kCh + c * 8 + e], f[e], a);
+                    for (int e = 0; e < 8; ++e) a = __fmaf_rn(w[tap * kCh + c * 8 + e], f[e], a);
+                }
             }
         }
-    }
-    out[o.offset + g] = a;
+        out[o.offset + g] = a;
+    });
 }
 
 // Data gradient of the output convolution: dg[p][ci] = sum_tap du[p - tap] w[tap][ci].
@@ -924,13 +1014,11 @@ __global__ void upadd_adjoint_coarse_kernel(const __grid_constant__ Table t, flo
 // dst = src over every pixel of the table's images (16 bytes per thread).
 __global__ void copy_act_kernel(const __grid_constant__ Table t, bf16 const* src, bf16* dst)
 {
-    int const im = blockIdx.y;
-    if (im >= t.nimg || !image_active(t, im)) return;
-    Img const f = t.img[im];
-    int64_t const idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (idx >= static_cast<int64_t>(f.h + 2) * (f.w + 2) * kChunks) return;
-    int64_t const q = f.offset * kChunks + idx;
-    reinterpret_cast<uint4*>(dst)[q] = reinterpret_cast<uint4 const*>(src)[q];
+    __shared__ int64_t pre[kMaxImages + 1];
+    walk_active(t, pre, kChunks, [&](int im, int idx) {
+        int64_t const q = t.img[im].offset * kChunks + idx;
+        reinterpret_cast<uint4*>(dst)[q] = reinterpret_cast<uint4 const*>(src)[q];
+    });
 }
 
 // ------------------------------------------------------------------ node-level wrapper (FP32)
@@ -1056,55 +1144,39 @@ __global__ void dots_finish_kernel(double const* part, int nsamples, int nblocks
 // Feature image of the network's top level: 2x2 average of
 // [D^-1/2 r1 / s, log(nu)/log(1000)] over the nodes of each half-resolution
 // pixel (nodes outside the grid count as zero), s = rms(D^-1/2 r1).
-__global__ void features_kernel(const __grid_constant__ Samples ss, float const* r1, float const* nu,
-                                float const* dinv, double const* dots, float* feat)
+__global__ void features_kernel(const __grid_constant__ Samples ss, const __grid_constant__ Table t, float const* r1,
+                                float const* nu, float const* dinv, double const* dots, float* feat)
 {
-    int const sidx = blockIdx.y;
-    if (!sample_active(ss, sidx)) return;
-    Sample const sm = ss.s[sidx];
-    Img const o = ss.top[sidx];
-    int64_t const P = o.w + 2, npx = P * (o.h + 2);
-    int64_t const g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (g >= npx) return;
-    int64_t const y = g / P, x = g - y * P;
-    float f0 = 0.0f, f1 = 0.0f;
-    if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
-        double const n = static_cast<double>(sm.nx) * sm.ny;
-        double const ms = dots[sidx * 3] / n;
-        float const inv_s = ms > 0.0 ? static_cast<float>(1.0 / sqrt(ms)) : 0.0f;
-        float const inv_l = static_cast<float>(1.0 / log(1000.0));
-        for (int a = 0; a < 2; ++a)
-            for (int b = 0; b < 2; ++b) {
-                int64_t const j = 2 * (y - 1) + a, i = 2 * (x - 1) + b;
-                if (j >= sm.ny || i >= sm.nx) continue;
-                int64_t const q = sm.offset + j * sm.nx + i;
-                f0 = f0 + r1[q] * sqrtf(dinv[q]) * inv_s;
-                f1 = f1 + logf(nu[q]) * inv_l;
-            }
-        f0 = f0 * 0.25f;
-        f1 = f1 * 0.25f;
+    __shared__ int64_t pre[kMaxImages + 1];
+    __shared__ float inv_rms[kMaxImages];   // 1 / rms(D^-1/2 r1) per sample
+    for (int k = threadIdx.x; k < ss.n; k += blockDim.x) {
+        double const ms = dots[k * 3] / (static_cast<double>(ss.s[k].nx) * ss.s[k].ny);
+        inv_rms[k] = ms > 0.0 ? static_cast<float>(1.0 / sqrt(ms)) : 0.0f;
     }
-    feat[2 * (o.offset + g)] = f0;
-    feat[2 * (o.offset + g) + 1] = f1;
-}
-
-// e2 = e1 + s * up(u_net), zero on the Dirichlet boundary.
-__global__ void correction_kernel(const __grid_constant__ Samples ss, float const* e1, float const* unet,
-                                  double const* dots, float* e2)
-{
-    int64_t row;
-    Sample sm;
-    if (!node_of(ss, row, sm)) return;
-    Img const o = ss.top[blockIdx.y];
-    int64_t const nx = sm.nx, ny = sm.ny;
-    int64_t const i = row % nx, j = row / nx;
-    float v = 0.0f;
-    if (!(i == 0 || j == 0 || i + 1 == nx || j + 1 == ny)) {
-        double const ms = dots[blockIdx.y * 3] / (static_cast<double>(nx) * ny);
-        float const s = static_cast<float>(sqrt(ms));
-        v = s * unet[o.offset + (j / 2 + 1) * (o.w + 2) + (i / 2 + 1)];
-    }
-    e2[sm.offset + row] = e1[sm.offset + row] + v;
+    float const inv_l = static_cast<float>(1.0 / log(1000.0));
+    walk_active(t, pre, 1, [&](int im, int g) {
+        int const sidx = t.sample[im];
+        Sample const sm = ss.s[sidx];
+        Img const o = t.img[im];
+        int const P = o.w + 2;
+        int const y = g / P, x = g - y * P;
+        float f0 = 0.0f, f1 = 0.0f;
+        if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
+            float const inv_s = inv_rms[sidx];
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b) {
+                    int64_t const j = 2 * (y - 1) + a, i = 2 * (x - 1) + b;
+                    if (j >= sm.ny || i >= sm.nx) continue;
+                    int64_t const q = sm.offset + j * sm.nx + i;
+                    f0 = f0 + r1[q] * sqrtf(dinv[q]) * inv_s;
+                    f1 = f1 + logf(nu[q]) * inv_l;
+                }
+            f0 = f0 * 0.25f;
+            f1 = f1 * 0.25f;
+        }
+        feat[2 * (o.offset + g)] = f0;
+        feat[2 * (o.offset + g) + 1] = f1;
+    });
 }
 
 // Gradient of the loss with respect to u:
@@ -1201,76 +1273,127 @@ __device__ __forceinline__ double block_sum_d(double v, double* red)
     return t;
 }
 
+// Prefix of the active samples' wrapper items (the items of a sample are
+// contiguous from item_base) and the item of active unit a.
+__device__ __forceinline__ int scan_items(Samples const& ss, int64_t* pre)
+{
+    scan_active(
+        ss.n, [&](int k) { return sample_active(ss, k) ? int64_t(ss.item_base[k + 1] - ss.item_base[k]) : int64_t(0); },
+        pre);
+    return static_cast<int>(pre[ss.n]);
+}
+
+__device__ __forceinline__ int item_of(Samples const& ss, int64_t const* pre, int a)
+{
+    int const k = find_unit(pre, ss.n, a);
+    return ss.item_base[k] + (a - static_cast<int>(pre[k]));
+}
+
 // e1 = w D^-1 r, r1 = r - K e1 (boundary rows: r1 = r - e1), and the partial
 // sums of |D^-1/2 r1|^2 per item.
 __global__ void __launch_bounds__(256) wrap_pre_kernel(const __grid_constant__ Samples ss, WrapItem const* items,
-                                                       float const* nu, float const* dinv, float const* r, float* e1,
-                                                       float* r1, double* part)
+                                                       float const* nu, float const* dinv, float const* r,
+                                                       float* e1, float* r1, double* part)
 {
     __shared__ double red[8];
-    WrapItem const it = items[blockIdx.x];
-    if (!sample_active(ss, it.sample)) return;
-    Sample const sm = ss.s[it.sample];
-    int const nx = sm.nx, ny = sm.ny;
-    float const* nu_s = nu + sm.offset;
-    float const* d_s = dinv + sm.offset;
-    float const* r_s = r + sm.offset;
-    auto e = [&](int q, int, int) { return kOmega * (d_s[q] * r_s[q]); };
-    double acc = 0.0;
-    for (int row = it.begin + threadIdx.x; row < it.end; row += blockDim.x) {
-        int const j = row / nx, i = row - j * nx;
-        float const ev = e(row, i, j);
-        float v;
-        if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) v = r_s[row] - ev;
-        else v = r_s[row] - k_row(e, nu_s, nx, row, i, j);
-        e1[sm.offset + row] = ev;
-        r1[sm.offset + row] = v;
-        acc += static_cast<double>(d_s[row]) * static_cast<double>(v) * static_cast<double>(v);
+    __shared__ int64_t pre[kMaxImages + 1];
+    int const nact = scan_items(ss, pre);
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
+        int const item = item_of(ss, pre, a);
+        WrapItem const it = items[item];
+        Sample const sm = ss.s[it.sample];
+        int const nx = sm.nx, ny = sm.ny;
+        float const* nu_s = nu + sm.offset;
+        float const* d_s = dinv + sm.offset;
+        float const* r_s = r + sm.offset;
+        auto e = [&](int q, int, int) { return kOmega * (d_s[q] * r_s[q]); };
+        double acc = 0.0;
+        for (int row = it.begin + threadIdx.x; row < it.end; row += blockDim.x) {
+            int const j = row / nx, i = row - j * nx;
+            float const ev = e(row, i, j);
+            float v;
+            if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) v = r_s[row] - ev;
+            else v = r_s[row] - k_row(e, nu_s, nx, row, i, j);
+            e1[sm.offset + row] = ev;
+            r1[sm.offset + row] = v;
+            acc += static_cast<double>(d_s[row]) * static_cast<double>(v) * static_cast<double>(v);
+        }
+        double const t = block_sum_d(acc, red);
+        if (threadIdx.x == 0) part[item] = t;
     }
-    double const t = block_sum_d(acc, red);
-    if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-// dots[s*3] = sum of the sample's item partials (fixed order).
+// dots[s*3] = sum of the sample's item partials: one warp per sample, each
+// lane summing a fixed strided subset in order, then a fixed butterfly
+// (deterministic for a given batch geometry).
 __global__ void wrap_finish_kernel(const __grid_constant__ Samples ss, double const* part, double* dots)
 {
-    int const sidx = blockIdx.x * blockDim.x + threadIdx.x;
+    int const sidx = blockIdx.x;
     if (sidx >= ss.n || !sample_active(ss, sidx)) return;
     double t = 0.0;
-    for (int k = ss.item_base[sidx]; k < ss.item_base[sidx + 1]; ++k) t += part[k];
-    dots[sidx * 3] = t;
+    for (int k = ss.item_base[sidx] + static_cast<int>(threadIdx.x); k < ss.item_base[sidx + 1]; k += 32) t += part[k];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) dots[sidx * 3] = t;
 }
 
-// M(r) = e2 + w D^-1 (r - K e2), e2 = e1 + s D^-1/2 up(unet) (zero correction on the boundary).
-__global__ void __launch_bounds__(256) wrap_post_kernel(const __grid_constant__ Samples ss, WrapItem const* items,
-                                                        float const* nu, float const* dinv, float const* r,
-                                                        float const* e1, float const* unet, double const* dots,
+// The active samples' nodes as one compacted range: f(k, row) for node row
+// of sample k (walk_range).  No barrier may sit inside f.
+template <class F>
+__device__ __forceinline__ void walk_nodes(Samples const& ss, int64_t* pre, F const& f)
+{
+    scan_active(
+        ss.n, [&](int k) { return sample_active(ss, k) ? static_cast<int64_t>(ss.s[k].nx) * ss.s[k].ny : int64_t(0); },
+        pre);
+    walk_range(pre, ss.n, 1, f);
+}
+
+// s = rms(D^-1/2 r1) per sample (dots[k*3] = |D^-1/2 r1|^2), staged in shared
+// memory before a walk (whose scan barrier publishes it).
+__device__ __forceinline__ void stage_rms(Samples const& ss, double const* dots, float* sc)
+{
+    for (int k = threadIdx.x; k < ss.n; k += blockDim.x)
+        sc[k] = static_cast<float>(sqrt(dots[k * 3] / (static_cast<double>(ss.s[k].nx) * ss.s[k].ny)));
+}
+
+// e2 = e1 + s D^-1/2 up(unet) at interior nodes, e1 on the boundary.
+__global__ void __launch_bounds__(256) wrap_e2_kernel(const __grid_constant__ Samples ss, float const* dinv,
+                                                      float const* e1, float const* unet, double const* dots,
+                                                      float* e2)
+{
+    __shared__ int64_t pre[kMaxImages + 1];
+    __shared__ float sc[kMaxImages];
+    stage_rms(ss, dots, sc);
+    walk_nodes(ss, pre, [&](int k, int row) {
+        Sample const sm = ss.s[k];
+        int const nx = sm.nx, ny = sm.ny;
+        int const j = row / nx, i = row - j * nx;
+        int64_t const q = sm.offset + row;
+        float v = e1[q];
+        if (!(i == 0 || j == 0 || i + 1 == nx || j + 1 == ny)) {
+            Img const o = ss.top[k];
+            v = v + sc[k] * sqrtf(dinv[q]) * unet[o.offset + (j / 2 + 1) * (o.w + 2) + (i / 2 + 1)];
+        }
+        e2[q] = v;
+    });
+}
+
+// M(r) = e2 + w D^-1 (r - K e2) (boundary rows: K e2 -> e2).
+__global__ void __launch_bounds__(256) wrap_post_kernel(const __grid_constant__ Samples ss, float const* nu,
+                                                        float const* dinv, float const* r, float const* e2,
                                                         float* out)
 {
-    WrapItem const it = items[blockIdx.x];
-    if (!sample_active(ss, it.sample)) return;
-    Sample const sm = ss.s[it.sample];
-    Img const o = ss.top[it.sample];
-    int const nx = sm.nx, ny = sm.ny;
-    int const P = o.w + 2;
-    float const s = static_cast<float>(sqrt(dots[it.sample * 3] / (static_cast<double>(nx) * ny)));
-    float const* nu_s = nu + sm.offset;
-    float const* e1_s = e1 + sm.offset;
-    float const* d_s = dinv + sm.offset;
-    float const* un = unet + o.offset;
-    auto e = [&](int q, int ii, int jj) {
-        float v = e1_s[q];
-        if (!(ii == 0 || jj == 0 || ii + 1 == nx || jj + 1 == ny))
-            v = v + s * sqrtf(d_s[q]) * un[(jj / 2 + 1) * P + (ii / 2 + 1)];
-        return v;
-    };
-    for (int row = it.begin + threadIdx.x; row < it.end; row += blockDim.x) {
+    __shared__ int64_t pre[kMaxImages + 1];
+    walk_nodes(ss, pre, [&](int k, int row) {
+        Sample const sm = ss.s[k];
+        int const nx = sm.nx, ny = sm.ny;
         int const j = row / nx, i = row - j * nx;
-        float const e0 = e(row, i, j);
-        float const ke = (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) ? e0 : k_row(e, nu_s, nx, row, i, j);
+        float const* e_s = e2 + sm.offset;
+        auto e = [&](int q, int, int) { return e_s[q]; };
+        float const e0 = e_s[row];
+        float const ke = (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) ? e0 : k_row(e, nu + sm.offset, nx, row, i, j);
         int64_t const q = sm.offset + row;
         out[q] = e0 + kOmega * (dinv[q] * (r[q] - ke));
-    }
+    });
 }
 
 __global__ void adam_kernel(float* p, float const* g, float* m, float* v, int n, float lr, float b1t, float b2t)
@@ -1461,9 +1584,11 @@ Table Workspace::table(int level, int aux_level, bool) const
     t.nimg = static_cast<int>(L.images.size());
     t.tile_base[0] = 0;
     t.active = active;
+    t.px_base[0] = 0;
     for (int k = 0; k < t.nimg; ++k) {
         t.img[k] = L.img[k];
         t.sample[k] = L.images[k];
+        t.px_base[k + 1] = t.px_base[k] + static_cast<int64_t>(L.img[k].h + 2) * (L.img[k].w + 2);
         int64_t const tiles = (static_cast<int64_t>(L.img[k].w + 2) * L.img[k].h + kTilePx - 1) / kTilePx;
         t.tile_base[k + 1] = t.tile_base[k] + static_cast<int32_t>(tiles);
         if (aux_level >= 0) {
@@ -1488,6 +1613,10 @@ size_t wgrad_smem() { return sizeof(WgradSmem) + 1024; }
 bool g_attr_done = false;
 int g_sms = 0;  // multiprocessor count, read once (outside any stream capture)
 int g_conv_per_sm[5] = {0, 0, 0, 0, 0};  // resident conv CTAs per SM, by input mode
+// Grid-stride kernels of the forward pass and their resident blocks per SM.
+enum WalkKind { kWalkInc = 0, kWalkOut, kWalkGather, kWalkPool, kWalkCopy, kWalkFeat, kWalkPre, kWalkPost, kWalkE2,
+                kWalkKinds };
+int g_walk_per_sm[kWalkKinds] = {1, 1, 1, 1, 1, 1, 1, 1, 1};
 
 sil_status ensure_attributes()
 {
@@ -1517,6 +1646,20 @@ sil_status ensure_attributes()
     }
     SIL_CUDA_CHECK(cudaFuncSetAttribute(wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(wgrad_smem())));
+    void const* const walk_fns[kWalkKinds] = {
+        reinterpret_cast<void const*>(inc_forward_kernel), reinterpret_cast<void const*>(out_forward_kernel),
+        reinterpret_cast<void const*>(out_gather_kernel),  reinterpret_cast<void const*>(pool_kernel),
+        reinterpret_cast<void const*>(copy_act_kernel),    reinterpret_cast<void const*>(features_kernel),
+        reinterpret_cast<void const*>(wrap_pre_kernel),    reinterpret_cast<void const*>(wrap_post_kernel),
+        reinterpret_cast<void const*>(wrap_e2_kernel)};
+    for (int k = 0; k < kWalkKinds; ++k) {
+        cudaFuncAttributes a {};
+        SIL_CUDA_CHECK(cudaFuncGetAttributes(&a, walk_fns[k]));
+        int const regs = (a.numRegs + 7) / 8 * 8;   // per-thread allocation granularity
+        int const by_regs = regs_sm / std::max(1, regs * 256);
+        int const by_smem = smem_sm / static_cast<int>(a.sharedSizeBytes + 1024);
+        g_walk_per_sm[k] = std::max(1, std::min(std::min(by_regs, by_smem), 8));
+    }
     g_attr_done = true;
     return SIL_OK;
 }
@@ -1527,6 +1670,29 @@ int conv_grid(int ntiles, int mode)
 {
     int const per_sm = g_conv_per_sm[mode] > 0 ? g_conv_per_sm[mode] : 1;
     return std::max(1, std::min(ntiles, per_sm * (g_sms > 0 ? g_sms : 148)));
+}
+
+// Blocks of 256 threads for a grid-stride kernel: four resident waves (its
+// blocks per multiprocessor from registers and shared memory), so blocks
+// that finish early pick up the remaining work; fewer when the work is
+// smaller.
+unsigned walk_grid(Table const& t, int per, int kind)
+{
+    int64_t const chunks = (t.px_base[t.nimg] * per + 255) / 256;
+    int64_t const wave = 4 * static_cast<int64_t>(g_walk_per_sm[kind]) * (g_sms > 0 ? g_sms : 148);
+    return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(chunks, wave)));
+}
+
+unsigned item_grid(int nitems, int kind)
+{
+    return static_cast<unsigned>(std::max(1, std::min(nitems, 4 * g_walk_per_sm[kind] * (g_sms > 0 ? g_sms : 148))));
+}
+
+unsigned node_walk_grid(Workspace const& w, int kind)
+{
+    int64_t const chunks = (w.nodes + 255) / 256;
+    int64_t const wave = 4 * static_cast<int64_t>(g_walk_per_sm[kind]) * (g_sms > 0 ? g_sms : 148);
+    return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(chunks, wave)));
 }
 
 // 1024-byte aligned dynamic shared memory: the kernels index from the start
@@ -1687,13 +1853,13 @@ sil_status net_forward(Net& net, Workspace& w, cudaStream_t st, bool keep)
     int* err = net.error_flag;
     {
         Table const t = w.table(0, -1, false);
-        inc_forward_kernel<<<image_grid(t, 1, 0), 256, 0, st>>>(t, w.feat.as<float>(), net.params, w.h[0].as<bf16>());
+        inc_forward_kernel<<<walk_grid(t, 1, kWalkInc), 256, 0, st>>>(t, w.feat.as<float>(), net.params, w.h[0].as<bf16>());
         SIL_CUDA_CHECK(cudaGetLastError());
     }
     for (int l = 1; l < D; ++l) {
         int const wl = weight_level_enc(l);
         Table const t = w.table(l, l - 1, true);
-        pool_kernel<<<image_grid(t, 1, 0), 256, 0, st>>>(t, w.h[l - 1].as<bf16>(), w.pin[l].as<bf16>());
+        pool_kernel<<<walk_grid(t, 1, kWalkPool), 256, 0, st>>>(t, w.h[l - 1].as<bf16>(), w.pin[l].as<bf16>());
         SIL_CUDA_CHECK(cudaGetLastError());
         Table const t2 = w.table(l, -1, false);
         sil_status s = launch_conv(st, t2, kPlain, w.pin[l].as<bf16>(), nullptr, nullptr, big_w(net, kDown, wl),
@@ -1707,7 +1873,7 @@ sil_status net_forward(Net& net, Workspace& w, cudaStream_t st, bool keep)
     for (int l = 0; l < D; ++l) {
         Table const t = deepest_table(w, l);
         if (t.nimg == 0) continue;
-        copy_act_kernel<<<image_grid(t, 4, 0), 256, 0, st>>>(t, w.h[l].as<bf16>(), w.g[l].as<bf16>());
+        copy_act_kernel<<<walk_grid(t, kChunks, kWalkCopy), 256, 0, st>>>(t, w.h[l].as<bf16>(), w.g[l].as<bf16>());
         SIL_CUDA_CHECK(cudaGetLastError());
     }
     int64_t const top = w.levels[0].npx;
@@ -1722,15 +1888,15 @@ sil_status net_forward(Net& net, Workspace& w, cudaStream_t st, bool keep)
     }
     if (keep) {
         Table const t = w.table(0, -1, false);
-        out_forward_kernel<<<image_grid(t, 1, 0), 256, 0, st>>>(t, w.g[0].as<bf16>(), net.params, w.unet.as<float>());
+        out_forward_kernel<<<walk_grid(t, 1, kWalkOut), 256, 0, st>>>(t, w.g[0].as<bf16>(), net.params, w.unet.as<float>());
     } else {
         Table const td = dec_table(w, 0);
         if (td.nimg > 0)
-            out_gather_kernel<<<image_grid(td, 1, 0), 256, 0, st>>>(td, w.taps.as<float>(), top, net.params,
+            out_gather_kernel<<<walk_grid(td, 1, kWalkGather), 256, 0, st>>>(td, w.taps.as<float>(), top, net.params,
                                                                    w.unet.as<float>());
         Table const t1 = deepest_table(w, 0);  // single-level images: no decoder
         if (t1.nimg > 0)
-            out_forward_kernel<<<image_grid(t1, 1, 0), 256, 0, st>>>(t1, w.g[0].as<bf16>(), net.params, w.unet.as<float>());
+            out_forward_kernel<<<walk_grid(t1, 1, kWalkOut), 256, 0, st>>>(t1, w.g[0].as<bf16>(), net.params, w.unet.as<float>());
     }
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
@@ -1749,6 +1915,7 @@ Table dec_table(Workspace const& w, int l)
         tt.img[q] = t.img[k];
         tt.aux[q] = t.aux[k];
         tt.sample[q] = t.sample[k];
+        tt.px_base[q + 1] = tt.px_base[q] + static_cast<int64_t>(t.img[k].h + 2) * (t.img[k].w + 2);
         tt.tile_base[q + 1] = tt.tile_base[q] + (t.tile_base[k + 1] - t.tile_base[k]);
     }
     return tt;
@@ -1766,6 +1933,7 @@ Table deepest_table(Workspace const& w, int l)
         t.img[q] = L.img[k];
         t.aux[q] = L.img[k];
         t.sample[q] = L.images[k];
+        t.px_base[q + 1] = t.px_base[q] + static_cast<int64_t>(L.img[k].h + 2) * (L.img[k].w + 2);
         t.tile_base[q + 1] = t.tile_base[q];
     }
     return t;
@@ -1878,17 +2046,22 @@ sil_status precond_forward(Net& net, Workspace& w, float const* nu, float const*
         dinv = w.dinv.as<float>();
     }
     WrapItem const* items = w.witems.as<WrapItem>();
-    wrap_pre_kernel<<<w.nwitems, 256, 0, st>>>(w.ss, items, nu, dinv, b, w.e1.as<float>(), w.r1.as<float>(),
+    Table const t0 = w.table(0, -1, false);
+    wrap_pre_kernel<<<item_grid(w.nwitems, kWalkPre), 256, 0, st>>>(w.ss, items, nu, dinv, b, w.e1.as<float>(),
+                                                          w.r1.as<float>(),
                                                w.wpart.as<double>());
-    wrap_finish_kernel<<<1, 64, 0, st>>>(w.ss, w.wpart.as<double>(), w.dots.as<double>());
+    wrap_finish_kernel<<<static_cast<unsigned>(w.samples.size()), 32, 0, st>>>(w.ss, w.wpart.as<double>(),
+                                                                                w.dots.as<double>());
     SIL_CUDA_CHECK(cudaGetLastError());
-    features_kernel<<<top_grid(w), 256, 0, st>>>(w.ss, w.r1.as<float>(), nu, dinv, w.dots.as<double>(),
+    features_kernel<<<walk_grid(t0, 1, kWalkFeat), 256, 0, st>>>(w.ss, t0, w.r1.as<float>(), nu, dinv, w.dots.as<double>(),
                                                  w.feat.as<float>());
     SIL_CUDA_CHECK(cudaGetLastError());
     sil_status s = net_forward(net, w, st, keep);
     if (s != SIL_OK) return s;
-    wrap_post_kernel<<<w.nwitems, 256, 0, st>>>(w.ss, items, nu, dinv, b, w.e1.as<float>(), w.unet.as<float>(),
-                                                w.dots.as<double>(), out);
+    unsigned const ng = node_walk_grid(w, kWalkE2);
+    wrap_e2_kernel<<<ng, 256, 0, st>>>(w.ss, dinv, w.e1.as<float>(), w.unet.as<float>(), w.dots.as<double>(),
+                                       w.e2.as<float>());
+    wrap_post_kernel<<<node_walk_grid(w, kWalkPost), 256, 0, st>>>(w.ss, nu, dinv, b, w.e2.as<float>(), out);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
