@@ -368,15 +368,17 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     ConvSmem& s = *reinterpret_cast<ConvSmem*>(smem_raw);
     int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    scan_active(
+        t.nimg, [&](int k) { return image_active(t, k) ? int64_t(t.tile_base[k + 1] - t.tile_base[k]) : int64_t(0); },
+        s.pre);
+    // a CTA without an active tile leaves before staging weights or taking TMEM
+    if (static_cast<int64_t>(blockIdx.x) >= s.pre[t.nimg]) return;
     for (int i = tid; i < kKChunks * kCh; i += 128) {
         int const co = i & 31, k = i >> 5;
         s.w[k * kCh + co] = __ldg(reinterpret_cast<uint4 const*>(wt + co * (kTaps * kCh)) + k);
     }
     if (out_taps != nullptr)
         for (int i = tid; i < kOutW; i += 128) s.wout[i] = wout[i];
-    scan_active(
-        t.nimg, [&](int k) { return image_active(t, k) ? int64_t(t.tile_base[k + 1] - t.tile_base[k]) : int64_t(0); },
-        s.pre);
     if (warp == 0) tmem_alloc(&s.tmem, 32);
     if (tid == 0) {
         mbar_init(&s.bar, 1);
