@@ -320,6 +320,19 @@ __device__ __forceinline__ void stage_halo(uint4* halo, Table const& t, int im, 
     int const npx = P * (o.h + 2);
     Img const ci = t.aux[im];
     uint4 const* base = reinterpret_cast<uint4 const*>(src);
+    // Image coordinates of each halo row's first pixel (floor division, so
+    // the pixel before the image is row -1); within a row they advance by
+    // adding, wrapping at the row pitch P.
+    int y0[3], x0[3];
+    if (up) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            int const g0 = start + (r - 1) * P - 1;
+            int const y = g0 >= 0 ? g0 / P : -1;
+            y0[r] = y;
+            x0[r] = g0 - y * P;
+        }
+    }
     for (int i = threadIdx.x; i < 3 * kHalo; i += blockDim.x) {
         int const r = i / kHalo, j = i - r * kHalo;
         int const g = start + (r - 1) * P - 1 + j;
@@ -327,7 +340,12 @@ __device__ __forceinline__ void stage_halo(uint4* halo, Table const& t, int im, 
         int64_t px = 0;
         if (valid) {
             if (up) {
-                int const y = g / P, x = g - y * P;
+                int y = r == 0 ? y0[0] : (r == 1 ? y0[1] : y0[2]);
+                int x = (r == 0 ? x0[0] : (r == 1 ? x0[1] : x0[2])) + j;
+                while (x >= P) {
+                    x -= P;
+                    ++y;
+                }
                 valid = !(y == 0 || x == 0 || y > o.h || x > o.w);
                 px = ci.offset + static_cast<int64_t>((y - 1) / 2 + 1) * (ci.w + 2) + ((x - 1) / 2 + 1);
             } else {
@@ -346,7 +364,7 @@ __device__ __forceinline__ void stage_halo(uint4* halo, Table const& t, int im, 
 struct ConvSmem
 {
     uint4 w[kKChunks * kCh];              // B operand: [K chunk][output channel], 18432 B
-    float wout[kOutW];                    // output-convolution weights (tap partials)
+    float4 wout[kCh][3];                  // output-convolution weights [input channel][tap, 12 with padding]
     uint64_t bar;
     uint32_t tmem;
     int abort;
@@ -378,7 +396,10 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
         s.w[k * kCh + co] = __ldg(reinterpret_cast<uint4 const*>(wt + co * (kTaps * kCh)) + k);
     }
     if (out_taps != nullptr)
-        for (int i = tid; i < kOutW; i += 128) s.wout[i] = wout[i];
+        for (int i = tid; i < kCh * 12; i += 128) {
+            int const ci = i / 12, tap = i - ci * 12;
+            reinterpret_cast<float*>(s.wout[ci])[tap] = tap < kTaps ? wout[tap * kCh + ci] : 0.0f;
+        }
     if (warp == 0) tmem_alloc(&s.tmem, 32);
     if (tid == 0) {
         mbar_init(&s.bar, 1);
@@ -516,13 +537,26 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ Ta
                     float f[32];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) unpack8(packed[q], f + 8 * q);
-#pragma unroll 1
-                    for (int tap = 0; tap < kTaps; ++tap) {
-                        float a = 0.0f;
+                    // nine accumulators side by side; each tap still sums its 32
+                    // channels in order from zero
+                    float a[kTaps];
 #pragma unroll
-                        for (int ci = 0; ci < 32; ++ci) a = __fmaf_rn(s.wout[tap * kCh + ci], f[ci], a);
-                        out_taps[tap * taps_stride + px] = a;
+                    for (int tap = 0; tap < kTaps; ++tap) a[tap] = 0.0f;
+#pragma unroll
+                    for (int ci = 0; ci < 32; ++ci) {
+                        float4 const w0 = s.wout[ci][0], w1 = s.wout[ci][1], w2 = s.wout[ci][2];
+                        a[0] = __fmaf_rn(w0.x, f[ci], a[0]);
+                        a[1] = __fmaf_rn(w0.y, f[ci], a[1]);
+                        a[2] = __fmaf_rn(w0.z, f[ci], a[2]);
+                        a[3] = __fmaf_rn(w0.w, f[ci], a[3]);
+                        a[4] = __fmaf_rn(w1.x, f[ci], a[4]);
+                        a[5] = __fmaf_rn(w1.y, f[ci], a[5]);
+                        a[6] = __fmaf_rn(w1.z, f[ci], a[6]);
+                        a[7] = __fmaf_rn(w1.w, f[ci], a[7]);
+                        a[8] = __fmaf_rn(w2.x, f[ci], a[8]);
                     }
+#pragma unroll
+                    for (int tap = 0; tap < kTaps; ++tap) out_taps[tap * taps_stride + px] = a[tap];
                 }
             }
         }
