@@ -24,14 +24,18 @@ from .precond import LearnedPreconditioner
 SNAPSHOT_TOLS = (1e-1, 1e-2, 1e-3, 1e-5)
 
 
-def generate_pairs(seed, count, sizes=(256, 384, 512, 768, 1024), snapshot_tols=SNAPSHOT_TOLS, batch=64):
+def generate_pairs(seed, count, sizes=(256, 384, 512, 768, 1024), snapshot_tols=SNAPSHOT_TOLS, batch=64,
+                   min_cores=0):
     """Pairs grouped by grid size: {n: [(nu, b, x), ...]} as flat FP32 CUDA tensors
-    (nu shared by the pairs of one problem)."""
+    (nu shared by the pairs of one problem).  min_cores > 0 draws the number
+    of permeability-1000 rectangles from min_cores..3 instead of 0..3."""
     import torch
     rng = np.random.default_rng(seed)
     pairs = {}
     for start in range(0, count, batch):
-        probs = [mag.synthetic_problem(rng, int(rng.choice(sizes))) for _ in range(min(batch, count - start))]
+        probs = [mag.synthetic_problem(rng, int(rng.choice(sizes)),
+                                       cores=int(rng.integers(min_cores, 4)) if min_cores > 0 else None)
+                 for _ in range(min(batch, count - start))]
         shapes = [(p.nx, p.ny) for p in probs]
         mus = [torch.from_numpy(p.node_mu()).cuda() for p in probs]
         rhss = [torch.from_numpy(p.rhs()).cuda() for p in probs]
@@ -85,12 +89,16 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--init", default=None, help="start from these parameters (.npy)")
+    ap.add_argument("--sizes", default="256,384,512,768,1024", help="grid sizes of the generated problems")
+    ap.add_argument("--min-cores", type=int, default=0,
+                    help="draw min..3 permeability-1000 rectangles per problem instead of 0..3")
     ap.add_argument("--out", default="precond_2d.npy")
     args = ap.parse_args()
     import torch
     torch.cuda.init()
     t0 = time.perf_counter()
-    pairs = generate_pairs(args.seed, args.problems)
+    pairs = generate_pairs(args.seed, args.problems, sizes=tuple(int(v) for v in args.sizes.split(",")),
+                           min_cores=args.min_cores)
     npairs = sum(len(v) for v in pairs.values())
     print(json.dumps({"pairs": npairs, "by_size": {int(k): len(v) for k, v in pairs.items()},
                       "generate_seconds": round(time.perf_counter() - t0, 2)}), flush=True)
