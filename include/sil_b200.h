@@ -260,6 +260,63 @@ sil_status sil_mag2d_solve_batch(const sil_mag2d_problem* problems, int nproblem
                                  sil_stream stream);
 
 /* ---------------------------------------------------------------------- */
+/* 2D magnetostatics with a nonlinear (saturating) ferromagnetic material.  */
+/* A node whose ferromagnetic fraction (share of adjacent cells made of the */
+/* material) is above 1/2 follows the B-H curve: at a sampled node with     */
+/* moments B = (B0, B1) and q = |B|^2 the field is H_c = B_c (F + q F'),     */
+/* F(q) = h(b)/b at b = sqrt(q), and the Jacobian is                        */
+/* d_rc (F + q F') + 4 B_r B_c F' + 2 q B_r B_c F''; other nodes keep B/mu.  */
+/* Replaces: MaterialMagnetostaticsHamiltonian + InterpolatedNonlinearBHCurve */
+/*   onelab_interface/magnetostatics_onelab.hpp:957-1011, 4471-4565;        */
+/*   src/similie/physics/magnetostatics/nonlinear_magnetostatics.py:14-369. */
+
+/* B-H curve: n samples (2..64) of b (increasing, b[0] >= 0) and h, HOST
+ * arrays; h is interpolated linearly in b and extended linearly beyond the
+ * last sample. */
+typedef struct sil_bh_curve {
+    int32_t n;
+    const double* b;
+    const double* h;
+} sil_bh_curve;
+
+/* One nonlinear problem; device FP64 node arrays of nx*ny (x fastest).
+ * node_ferro: ferromagnetic fraction per node.  solution holds the initial
+ * guess on entry (zero it for x0 = 0, as the linear solve starts) and the
+ * result on exit. */
+typedef struct sil_mag2d_nl_problem {
+    int64_t nx, ny;
+    const double* node_mu;
+    const double* node_ferro;
+    sil_bh_curve curve;
+    const double* rhs;
+    double* solution;
+} sil_mag2d_nl_problem;
+
+/* y = the nonlinear residual operator applied to a (identity rows on the
+ * boundary).  Replaces: MagnetostaticsOperator2D::apply with the material
+ * Hamiltonian, magnetostatics_onelab.hpp:1271-1426. */
+sil_status sil_mag2d_nl_apply(sil_stream stream, const sil_mag2d_nl_problem* problem, const double* a, double* y);
+
+/* y = J(state) x, the operator's Jacobian at `state` applied to x.
+ * Replaces: apply_jacobian (2D), magnetostatics_onelab.hpp:2799-2915. */
+sil_status sil_mag2d_nl_apply_jacobian(sil_stream stream, const sil_mag2d_nl_problem* problem, const double* state,
+                                       const double* x, double* y);
+
+/* Newton solve of every problem of the batch: at most 30 steps, each
+ * solving J(x) d = r by Jacobi-preconditioned CG (FP64) to
+ * settings->relative_tolerance (at most settings->max_iterations
+ * iterations), then a line search of at most 8 candidates x + alpha d,
+ * alpha halving from 1, that stops at the first residual below the current
+ * one, else takes the best seen.  Converged when ||b - F(x)|| <= tol *
+ * ||b - F(x0)||.  diag: iterations = all CG iterations, refinements =
+ * Newton steps.  Synchronous.  settings->solver is ignored.
+ * Replaces: solvers::minimize_strong_formulation_residual (nonlinear
+ *   branch), src/similie/solvers/minimize_strong_formulation_residual.hpp:1383-1569. */
+sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int nproblems,
+                                    const sil_solve_settings* settings, sil_solve_diagnostics* diag,
+                                    sil_stream stream);
+
+/* ---------------------------------------------------------------------- */
 /* Learned multilevel convolutional preconditioner of the 2D solve.        */
 /* M(r) = Jacobi step, then a U-Net correction computed at half resolution  */
 /* from [r1 / rms(r1), log(nu) / log(1000)], then a Jacobi step; 32          */

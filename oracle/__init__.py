@@ -57,6 +57,13 @@ def lib():
         _lib.silo_mag2d_diagonal.argtypes = [i64, i64, dp, dp]
         _lib.silo_mag2d_cg.argtypes = [i64, i64, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp]
         _lib.silo_num_threads.argtypes = []
+        ci = ctypes.c_int
+        _lib.silo_bh_eval.argtypes = [ci, dp, dp, ci, dp, dp, dp, dp]
+        _lib.silo_mag2d_nl_apply.argtypes = [i64, i64, dp, dp, ci, dp, dp, dp, dp]
+        _lib.silo_mag2d_nl_jacobian_apply.argtypes = [i64, i64, dp, dp, ci, dp, dp, dp, dp, dp]
+        _lib.silo_mag2d_nl_jacobian_diagonal.argtypes = [i64, i64, dp, dp, ci, dp, dp, dp, dp]
+        _lib.silo_mag2d_nl_solve.argtypes = [i64, i64, dp, dp, ci, dp, dp, dp, dp, ctypes.c_double, ci,
+                                             ctypes.POINTER(ci), dp]
         _lib.silo_mag3d_node_mu.argtypes = [i64, i64, i64, dp, ctypes.c_double, dp]
         _lib.silo_mag3d_rhs.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp]
         _lib.silo_mag3d_apply.argtypes = [i64, i64, i64, dp, dp, dp, dp, ctypes.c_double, dp, dp]
@@ -254,6 +261,50 @@ def mag2d_cg(nx, ny, node_mu, rhs, tol=1e-10, max_iter=100000):
 
 def num_threads():
     return lib().silo_num_threads()
+
+
+# ----------------------------------------------------------------- magnetostatics 2D, nonlinear material
+
+def bh_eval(curve_b, curve_h, q):
+    """F(q) = h/b at b = sqrt(q) of the interpolated B-H curve and its first two q-derivatives."""
+    b, h, q = _f64(curve_b), _f64(curve_h), _f64(q)
+    f, df, d2f = np.zeros(len(q)), np.zeros(len(q)), np.zeros(len(q))
+    lib().silo_bh_eval(len(b), _ptr(b), _ptr(h), len(q), _ptr(q), _ptr(f), _ptr(df), _ptr(d2f))
+    return f, df, d2f
+
+
+def mag2d_nl_apply(nx, ny, node_mu, node_ferro, curve_b, curve_h, a):
+    mu, fe, b, h, a = _f64(node_mu), _f64(node_ferro), _f64(curve_b), _f64(curve_h), _f64(a)
+    out = np.zeros(nx * ny)
+    lib().silo_mag2d_nl_apply(nx, ny, _ptr(mu), _ptr(fe), len(b), _ptr(b), _ptr(h), _ptr(a), _ptr(out))
+    return out
+
+
+def mag2d_nl_jacobian_apply(nx, ny, node_mu, node_ferro, curve_b, curve_h, state, x):
+    mu, fe, b, h = _f64(node_mu), _f64(node_ferro), _f64(curve_b), _f64(curve_h)
+    st, x = _f64(state), _f64(x)
+    out = np.zeros(nx * ny)
+    lib().silo_mag2d_nl_jacobian_apply(nx, ny, _ptr(mu), _ptr(fe), len(b), _ptr(b), _ptr(h), _ptr(st), _ptr(x),
+                                       _ptr(out))
+    return out
+
+
+def mag2d_nl_jacobian_diagonal(nx, ny, node_mu, node_ferro, curve_b, curve_h, state):
+    mu, fe, b, h, st = _f64(node_mu), _f64(node_ferro), _f64(curve_b), _f64(curve_h), _f64(state)
+    out = np.zeros(nx * ny)
+    lib().silo_mag2d_nl_jacobian_diagonal(nx, ny, _ptr(mu), _ptr(fe), len(b), _ptr(b), _ptr(h), _ptr(st), _ptr(out))
+    return out
+
+
+def mag2d_nl_solve(nx, ny, node_mu, node_ferro, curve_b, curve_h, rhs, x0=None, tol=1e-10, max_iter=100000):
+    """Newton + line search; returns (x, cg_iterations, newton_steps, final relative residual)."""
+    mu, fe, b, h, rhs = _f64(node_mu), _f64(node_ferro), _f64(curve_b), _f64(curve_h), _f64(rhs)
+    x = np.zeros(nx * ny) if x0 is None else np.array(x0, dtype=np.float64)
+    steps = ctypes.c_int(0)
+    rel = ctypes.c_double(0.0)
+    it = lib().silo_mag2d_nl_solve(nx, ny, _ptr(mu), _ptr(fe), len(b), _ptr(b), _ptr(h), _ptr(rhs), _ptr(x), tol,
+                                   max_iter, ctypes.byref(steps), ctypes.byref(rel))
+    return x, it, steps.value, rel.value
 
 
 # ----------------------------------------------------------------- magnetostatics 3D

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <tuple>
 #include <vector>
 
@@ -1529,3 +1530,337 @@ int silo_num_threads(void)
 }
 
 } // extern "C"
+
+// ------------------------------------------------------------------ magnetostatics 2D, nonlinear material
+
+namespace {
+
+// Interpolated B-H curve: h piecewise linear in b, intervals bracketed by q = b^2.
+// Ref: src/similie/physics/magnetostatics/nonlinear_magnetostatics.py:14-181
+// (InterpolatedNonlinearBHCurve: constructor, bracket_q, h_from_b,
+// dh_db_from_b, h_over_b_from_b and its b- and q-derivatives).
+struct BHCurve
+{
+    int n = 0;
+    std::vector<double> b, h, q, dh_db;
+
+    BHCurve(int n_, const double* b_, const double* h_) : n(n_), b(b_, b_ + n_), h(h_, h_ + n_), q(n_), dh_db(n_ - 1)
+    {
+        for (int i = 0; i < n; ++i) q[i] = b[i] * b[i];
+        for (int i = 0; i + 1 < n; ++i) dh_db[i] = (h[i + 1] - h[i]) / (b[i + 1] - b[i]);
+    }
+    int bracket_q(double qv) const
+    {
+        if (qv <= q[0]) return 0;
+        for (int i = 0; i + 1 < n; ++i)
+            if (qv <= q[i + 1]) return i;
+        return n - 2;
+    }
+    double h_from_b(double bv) const
+    {
+        if (bv <= b[0]) return h[0];
+        if (bv >= b[n - 1]) {
+            int const k = n - 2;
+            return h[k] + dh_db[k] * (bv - b[k]);
+        }
+        int const k = bracket_q(bv * bv);
+        return h[k] + dh_db[k] * (bv - b[k]);
+    }
+    double dh_db_from_b(double bv) const
+    {
+        if (bv <= b[0]) return dh_db[0];
+        if (bv >= b[n - 1]) return dh_db[n - 2];
+        return dh_db[bracket_q(bv * bv)];
+    }
+    double h_over_b_from_b(double bv) const { return bv == 0.0 ? dh_db_from_b(0.0) : h_from_b(bv) / bv; }
+    double d1_b(double bv) const
+    {
+        if (bv == 0.0) return 0.0;
+        return (dh_db_from_b(bv) * bv - h_from_b(bv)) / (bv * bv);
+    }
+    double d2_b(double bv) const
+    {
+        if (bv == 0.0) return 0.0;
+        double const intercept = h_from_b(bv) - dh_db_from_b(bv) * bv;
+        return 2.0 * intercept / (bv * bv * bv);
+    }
+    double f(double qv) const { return h_over_b_from_b(std::sqrt(qv)); }
+    double df(double qv) const
+    {
+        if (qv == 0.0) return 0.0;
+        double const bv = std::sqrt(qv);
+        return d1_b(bv) / (2.0 * bv);
+    }
+    double d2f(double qv) const
+    {
+        if (qv == 0.0) return 0.0;
+        double const bv = std::sqrt(qv);
+        return d2_b(bv) / (4.0 * qv) - d1_b(bv) / (4.0 * qv * bv);
+    }
+};
+
+// dH/dB_c and d2H/dB_r dB_c at a sampled node.  Ferromagnetic nodes use the
+// Hamiltonian q F(q) / 2 (F = h/b, q = |B|^2): dH/dB_c = B_c F + q B_c F',
+// d2H/dB_r dB_c = delta_rc (F + q F') + 4 B_r B_c F' + 2 q B_r B_c F''; the
+// others B_c / mu.
+// Ref: onelab_interface/magnetostatics_onelab.hpp:957-1011
+// (MaterialMagnetostaticsHamiltonian); the Hamiltonian and its derivatives:
+// src/similie/physics/magnetostatics/nonlinear_magnetostatics.py:331-369,
+// src/similie/physics/generate_cpp_hamiltonian.py:280-400.
+struct NodeLaw
+{
+    const double* mu;
+    const double* ferro;
+    BHCurve const* curve;
+    void field(int64_t s, double b0, double b1, double* h0, double* h1) const
+    {
+        if (ferro[s] > 0.5) {
+            double const q = b0 * b0 + b1 * b1;
+            double const F = curve->f(q), dF = curve->df(q);
+            *h0 = b0 * F + q * b0 * dF;
+            *h1 = b1 * F + q * b1 * dF;
+        } else {
+            *h0 = b0 / mu[s];
+            *h1 = b1 / mu[s];
+        }
+    }
+    void jacobian(int64_t s, double b0, double b1, double* j00, double* j01, double* j11) const
+    {
+        if (ferro[s] > 0.5) {
+            double const q = b0 * b0 + b1 * b1;
+            double const F = curve->f(q), dF = curve->df(q), d2F = curve->d2f(q);
+            double const base = F + q * dF;
+            *j00 = base + 4.0 * b0 * b0 * dF + 2.0 * q * b0 * b0 * d2F;
+            *j11 = base + 4.0 * b1 * b1 * dF + 2.0 * q * b1 * b1 * d2F;
+            *j01 = 4.0 * b0 * b1 * dF + 2.0 * q * b0 * b1 * d2F;
+        } else {
+            *j00 = 1.0 / mu[s];
+            *j11 = 1.0 / mu[s];
+            *j01 = 0.0;
+        }
+    }
+};
+
+double nrm2(int64_t n, const double* v)
+{
+    double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (int64_t i = 0; i < n; ++i) s += v[i] * v[i];
+    return std::sqrt(s);
+}
+
+double dotp(int64_t n, const double* a, const double* b)
+{
+    double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+
+// Nonlinear operator, same sampled nodes and order as silo_mag2d_apply.
+// Ref: onelab_interface/magnetostatics_onelab.hpp:1271-1426 (moments criterion)
+void nl_apply(int64_t nx, int64_t ny, NodeLaw const& law, const double* a, double* y)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ny; ++j) {
+        for (int64_t i = 0; i < nx; ++i) {
+            int64_t const row = i + nx * j;
+            if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) {
+                y[row] = a[row];
+                continue;
+            }
+            double residual = 0.0, h0, h1;
+            if (j - 1 >= 1) {
+                law.field(row - nx, m0(nx, a, i, j - 1), m1(nx, a, i, j - 1), &h0, &h1);
+                residual -= -1. * h0;
+            }
+            law.field(row, m0(nx, a, i, j), m1(nx, a, i, j), &h0, &h1);
+            residual -= 1. * h0;
+            if (i - 1 >= 1) {
+                law.field(row - 1, m0(nx, a, i - 1, j), m1(nx, a, i - 1, j), &h0, &h1);
+                residual -= 1. * h1;
+            }
+            law.field(row, m0(nx, a, i, j), m1(nx, a, i, j), &h0, &h1);
+            residual -= -1. * h1;
+            y[row] = residual;
+        }
+    }
+}
+
+// Jacobian apply: every sampled node contributes (-outer coefficient) x the
+// row (X) or second row (Y) of its 2x2 Jacobian times the moments of x.
+// Ref: onelab_interface/magnetostatics_onelab.hpp:2799-2915 (apply_jacobian, 2D)
+void nl_jacobian_apply(int64_t nx, int64_t ny, NodeLaw const& law, const double* st, const double* x, double* y)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ny; ++j) {
+        for (int64_t i = 0; i < nx; ++i) {
+            int64_t const row = i + nx * j;
+            if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) {
+                y[row] = x[row];
+                continue;
+            }
+            double residual = 0.0, j00, j01, j11;
+            auto add = [&](double c, int64_t si, int64_t sj, bool first) {
+                law.jacobian(si + nx * sj, m0(nx, st, si, sj), m1(nx, st, si, sj), &j00, &j01, &j11);
+                double const d0 = m0(nx, x, si, sj), d1 = m1(nx, x, si, sj);
+                residual += c * (first ? (j00 * d0 + j01 * d1) : (j01 * d0 + j11 * d1));
+            };
+            if (j - 1 >= 1) add(1.0, i, j - 1, true);
+            add(-1.0, i, j, true);
+            if (i - 1 >= 1) add(-1.0, i - 1, j, false);
+            add(1.0, i, j, false);
+            y[row] = residual;
+        }
+    }
+}
+
+void nl_jacobian_diagonal(int64_t nx, int64_t ny, NodeLaw const& law, const double* st, double* diag)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ny; ++j) {
+        for (int64_t i = 0; i < nx; ++i) {
+            int64_t const row = i + nx * j;
+            if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) {
+                diag[row] = 1.0;
+                continue;
+            }
+            double d = 0.0, j00, j01, j11;
+            if (j - 1 >= 1) {
+                law.jacobian(row - nx, m0(nx, st, i, j - 1), m1(nx, st, i, j - 1), &j00, &j01, &j11);
+                d += j00;
+            }
+            law.jacobian(row, m0(nx, st, i, j), m1(nx, st, i, j), &j00, &j01, &j11);
+            d += j00 - j01;
+            if (i - 1 >= 1) {
+                law.jacobian(row - 1, m0(nx, st, i - 1, j), m1(nx, st, i - 1, j), &j00, &j01, &j11);
+                d += j11;
+            }
+            law.jacobian(row, m0(nx, st, i, j), m1(nx, st, i, j), &j00, &j01, &j11);
+            d += j11 - j01;
+            diag[row] = d;
+        }
+    }
+}
+
+} // namespace
+
+void silo_bh_eval(int n, const double* b, const double* h, int count, const double* q, double* f, double* df,
+                  double* d2f)
+{
+    BHCurve const c(n, b, h);
+    for (int i = 0; i < count; ++i) {
+        f[i] = c.f(q[i]);
+        df[i] = c.df(q[i]);
+        d2f[i] = c.d2f(q[i]);
+    }
+}
+
+void silo_mag2d_nl_apply(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
+                         const double* b, const double* h, const double* a, double* y)
+{
+    BHCurve const c(n, b, h);
+    NodeLaw const law {node_mu, node_ferro, &c};
+    nl_apply(nx, ny, law, a, y);
+}
+
+void silo_mag2d_nl_jacobian_apply(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
+                                  const double* b, const double* h, const double* state, const double* x,
+                                  double* y)
+{
+    BHCurve const c(n, b, h);
+    NodeLaw const law {node_mu, node_ferro, &c};
+    nl_jacobian_apply(nx, ny, law, state, x, y);
+}
+
+void silo_mag2d_nl_jacobian_diagonal(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro,
+                                     int n, const double* b, const double* h, const double* state, double* diag)
+{
+    BHCurve const c(n, b, h);
+    NodeLaw const law {node_mu, node_ferro, &c};
+    nl_jacobian_diagonal(nx, ny, law, state, diag);
+}
+
+// Ref: src/similie/solvers/minimize_strong_formulation_residual.hpp:1383-1569
+// (nonlinear branch: at most 30 Newton steps; each solves the linearised
+// system to the relative tolerance, then a line search of at most 8 steps
+// halving alpha from 1 that stops at the first candidate below the current
+// residual, else takes the best candidate seen).
+int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
+                        const double* b, const double* h, const double* rhs, double* x, double tol, int max_iter,
+                        int* newton_steps, double* final_rel)
+{
+    BHCurve const c(n, b, h);
+    NodeLaw const law {node_mu, node_ferro, &c};
+    int64_t const N = nx * ny;
+    std::vector<double> fa(N), r(N), d(N), cand(N), cand_f(N), cand_r(N), dinv(N), cr(N), z(N), p(N), q(N);
+    nl_apply(nx, ny, law, x, fa.data());
+    for (int64_t i = 0; i < N; ++i) r[i] = rhs[i] - fa[i];
+    double const r0 = nrm2(N, r.data());
+    int total = 0, steps = 0;
+    if (r0 == 0.0) {
+        *newton_steps = 0;
+        *final_rel = 0.0;
+        return 0;
+    }
+    for (int it = 0; it < 30; ++it) {
+        double const res = nrm2(N, r.data());
+        if (res / r0 <= tol) break;
+        ++steps;
+        // Jacobi-CG on J(x) d = r from d = 0
+        nl_jacobian_diagonal(nx, ny, law, x, dinv.data());
+        for (int64_t i = 0; i < N; ++i) dinv[i] = 1.0 / dinv[i];
+        std::fill(d.begin(), d.end(), 0.0);
+        cr = r;
+        for (int64_t i = 0; i < N; ++i) z[i] = dinv[i] * cr[i];
+        p = z;
+        double rz = dotp(N, cr.data(), z.data());
+        double const bn = nrm2(N, r.data());
+        double rn = bn;
+        int k = 0;
+        while (k < max_iter && rn > tol * bn) {
+            nl_jacobian_apply(nx, ny, law, x, p.data(), q.data());
+            double const alpha = rz / dotp(N, p.data(), q.data());
+            for (int64_t i = 0; i < N; ++i) {
+                d[i] += alpha * p[i];
+                cr[i] -= alpha * q[i];
+            }
+            ++k;
+            rn = nrm2(N, cr.data());
+            if (rn <= tol * bn) break;
+            for (int64_t i = 0; i < N; ++i) z[i] = dinv[i] * cr[i];
+            double const rz2 = dotp(N, cr.data(), z.data());
+            double const beta = rz2 / rz;
+            rz = rz2;
+            for (int64_t i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
+        }
+        total += k;
+        // line search
+        double const cur = nrm2(N, r.data());
+        double alpha = 1.0, best_alpha = 0.0, best = std::numeric_limits<double>::infinity();
+        auto candidate = [&](double al) {
+            for (int64_t i = 0; i < N; ++i) cand[i] = x[i] + al * d[i];
+            nl_apply(nx, ny, law, cand.data(), cand_f.data());
+            for (int64_t i = 0; i < N; ++i) cand_r[i] = rhs[i] - cand_f[i];
+            return nrm2(N, cand_r.data());
+        };
+        for (int ls = 0; ls < 8; ++ls) {
+            double const nr = candidate(alpha);
+            if (nr < best) {
+                best = nr;
+                best_alpha = alpha;
+            }
+            if (nr < cur) break;
+            alpha *= 0.5;
+        }
+        if (best_alpha != alpha) {
+            alpha = best_alpha;
+            candidate(alpha);
+        }
+        std::copy(cand.begin(), cand.end(), x);
+        r = cand_r;
+    }
+    *newton_steps = steps;
+    *final_rel = nrm2(N, r.data()) / r0;
+    return total;
+}

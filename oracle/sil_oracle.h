@@ -121,6 +121,30 @@ int silo_mag3d_cg(int64_t nx, int64_t ny, int64_t nz, const double* x, const dou
                   const double* node_mu, double gamma, const double* rhs, double* sol, double tol, int max_iter,
                   double* final_rel);
 
+/* ------------------------------------------------------------------ */
+/* 2D nonlinear magnetostatics: ferromagnetic nodes (node_ferro > 0.5)   */
+/* follow an interpolated B-H curve given by n samples (b, h), 2..64.    */
+
+/* F(q) = h(b)/b at b = sqrt(q) and its first two q-derivatives. */
+void silo_bh_eval(int n, const double* b, const double* h, int count, const double* q, double* f, double* df,
+                  double* d2f);
+/* y = nonlinear residual operator (moments criterion), identity rows on the boundary. */
+void silo_mag2d_nl_apply(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
+                         const double* b, const double* h, const double* a, double* y);
+/* y = J(state) x, the operator's Jacobian at `state` applied to x. */
+void silo_mag2d_nl_jacobian_apply(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
+                                  const double* b, const double* h, const double* state, const double* x,
+                                  double* y);
+/* Diagonal of the Jacobian at `state` (1 on boundary rows). */
+void silo_mag2d_nl_jacobian_diagonal(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro,
+                                     int n, const double* b, const double* h, const double* state, double* diag);
+/* Newton with a halving line search from the initial guess in x; every step
+ * solves J d = r by Jacobi-CG to the relative tolerance tol.  Returns the
+ * CG iterations; newton_steps and final_rel (||r|| / ||r0||) are written. */
+int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
+                        const double* b, const double* h, const double* rhs, double* x, double tol, int max_iter,
+                        int* newton_steps, double* final_rel);
+
 /* Threads OpenMP uses (for reporting). */
 int silo_num_threads(void);
 

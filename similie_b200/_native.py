@@ -43,6 +43,26 @@ class SilMag2dProblem(ctypes.Structure):
     ]
 
 
+class SilBHCurve(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("b", ctypes.c_void_p),
+        ("h", ctypes.c_void_p),
+    ]
+
+
+class SilMag2dNlProblem(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int64),
+        ("ny", ctypes.c_int64),
+        ("node_mu", ctypes.c_void_p),
+        ("node_ferro", ctypes.c_void_p),
+        ("curve", SilBHCurve),
+        ("rhs", ctypes.c_void_p),
+        ("solution", ctypes.c_void_p),
+    ]
+
+
 class SilMag3dProblem(ctypes.Structure):
     _fields_ = [
         ("nx", ctypes.c_int64),
@@ -126,6 +146,11 @@ SIGNATURES = [
     ("sil_laplacian", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_int, _F, _F]),
     ("sil_mag2d_apply", ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, _P, _P]),
     ("sil_mag2d_apply_noalloc", ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, _P, _P]),
+    ("sil_mag2d_nl_apply", ctypes.c_int, [_P, ctypes.POINTER(SilMag2dNlProblem), _P, _P]),
+    ("sil_mag2d_nl_apply_jacobian", ctypes.c_int, [_P, ctypes.POINTER(SilMag2dNlProblem), _P, _P, _P]),
+    ("sil_mag2d_nl_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag2dNlProblem), ctypes.c_int,
+                                                ctypes.POINTER(SilSolveSettings),
+                                                ctypes.POINTER(SilSolveDiagnostics), _P]),
     ("sil_mag2d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag2dProblem), ctypes.c_int,
                                              ctypes.POINTER(SilSolveSettings),
                                              ctypes.POINTER(SilSolveDiagnostics), _P]),

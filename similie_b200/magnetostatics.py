@@ -171,3 +171,109 @@ def solve_batch(mus, rhss, sols, shapes, solver="cg", tol=1e-10, max_iterations=
            for d in diag]
     check(rc, "mag2d_solve_batch")
     return out
+
+
+# ----------------------------------------------------------------- nonlinear (saturating) material
+
+def node_ferro(nx, ny, cell_nonlinear):
+    """Share of the adjacent cells made of the nonlinear material, per node; a
+    node follows the B-H curve when it is above 1/2
+    (onelab_interface/magnetostatics_onelab.hpp:4491-4517)."""
+    return node_mu(nx, ny, np.asarray(cell_nonlinear, dtype=np.float64), mu0=0.0)
+
+
+def synthetic_bh_curve(b_knee, mu_r=1000.0, samples=64, b_max=4.0):
+    """Samples (b, h) of a saturating curve h = (b / mu_r) (1 + (b / b_knee)^4)
+    on b in [0, b_max * b_knee]: permeability mu_r below the knee, falling
+    beyond it.  A synthetic stand-in for a measured B-H table.
+
+    The field of the reference's material law is the derivative of
+    b h(b) / 2, which involves dh/db: with h interpolated linearly between
+    samples it jumps at every sample, so Newton converges when the solution's
+    moments stay off those kinks (mild saturation) and can stall otherwise."""
+    b = np.linspace(0.0, b_max * b_knee, samples)
+    h = (b / mu_r) * (1.0 + (b / b_knee) ** 4)
+    return b, h
+
+
+def nonlinear_knee(n):
+    """Knee of the synthetic curve for an n x n unit-square problem of the
+    batched distribution: the moments are potential differences, so they
+    scale with the spacing 1/(n-1); at this knee the strongest moments in the
+    cores saturate."""
+    return 80.0 / (n - 1)
+
+
+def nonlinear_problem(n, seed):
+    """(Problem, node_mu, node_ferro, curve b, curve h) of a seeded nonlinear
+    problem: the batched distribution's permeability-1000 rectangles made of
+    the saturating material."""
+    rng = np.random.default_rng(seed)
+    p = synthetic_problem(rng, n, cores=int(rng.integers(1, 4)))
+    b, h = synthetic_bh_curve(nonlinear_knee(n))
+    return p, p.node_mu(), node_ferro(n, n, p.cell_mu > 1.0), b, h
+
+
+class _Curve:
+    def __init__(self, b, h):
+        self.b = np.ascontiguousarray(b, dtype=np.float64)
+        self.h = np.ascontiguousarray(h, dtype=np.float64)
+
+    def struct(self):
+        return _native.SilBHCurve(len(self.b), self.b.ctypes.data, self.h.ctypes.data)
+
+
+def _nl_problem(nx, ny, mu, ferro, curve, rhs=None, sol=None):
+    p = _native.SilMag2dNlProblem()
+    p.nx, p.ny = nx, ny
+    p.node_mu = mu.data_ptr()
+    p.node_ferro = ferro.data_ptr()
+    p.curve = curve.struct()
+    p.rhs = rhs.data_ptr() if rhs is not None else None
+    p.solution = sol.data_ptr() if sol is not None else None
+    return p
+
+
+def nl_apply(node_mu_dev, node_ferro_dev, curve_b, curve_h, a_dev, y_dev, nx, ny, stream=None):
+    """y = F(a), the nonlinear residual operator (torch CUDA float64 tensors)."""
+    import torch
+    c = _Curve(curve_b, curve_h)
+    p = _nl_problem(nx, ny, node_mu_dev, node_ferro_dev, c)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+    check(lib().sil_mag2d_nl_apply(s, ctypes.byref(p), ctypes.c_void_p(a_dev.data_ptr()),
+                                   ctypes.c_void_p(y_dev.data_ptr())), "mag2d_nl_apply")
+    return y_dev
+
+
+def nl_apply_jacobian(node_mu_dev, node_ferro_dev, curve_b, curve_h, state_dev, x_dev, y_dev, nx, ny, stream=None):
+    """y = J(state) x."""
+    import torch
+    c = _Curve(curve_b, curve_h)
+    p = _nl_problem(nx, ny, node_mu_dev, node_ferro_dev, c)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+    check(lib().sil_mag2d_nl_apply_jacobian(s, ctypes.byref(p), ctypes.c_void_p(state_dev.data_ptr()),
+                                            ctypes.c_void_p(x_dev.data_ptr()), ctypes.c_void_p(y_dev.data_ptr())),
+          "mag2d_nl_apply_jacobian")
+    return y_dev
+
+
+def nl_solve_batch(mus, ferros, curves, rhss, sols, shapes, tol=1e-10, max_iterations=100000, stream=None):
+    """Newton + line search for a batch of nonlinear problems (minimize_strong_formulation_residual,
+    nonlinear branch).  curves: list of (b, h) sample arrays; sols hold the initial guesses and
+    receive the solutions.  Returns one Diagnostics per problem (refinements = Newton steps)."""
+    import torch
+    n = len(shapes)
+    keep = [_Curve(b, h) for b, h in curves]
+    probs = (_native.SilMag2dNlProblem * n)()
+    for k, (nx, ny) in enumerate(shapes):
+        probs[k] = _nl_problem(nx, ny, mus[k], ferros[k], keep[k], rhss[k], sols[k])
+    st = _native.SilSolveSettings()
+    st.max_iterations = max_iterations
+    st.relative_tolerance = tol
+    diag = (_native.SilSolveDiagnostics * n)()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+    rc = lib().sil_mag2d_nl_solve_batch(probs, n, ctypes.byref(st), diag, s)
+    out = [Diagnostics(d.iterations, bool(d.converged), d.refinements, d.status, d.initial_residual_l2,
+                       d.final_residual_l2, d.final_relative_residual) for d in diag]
+    check(rc, "mag2d_nl_solve_batch")
+    return out
