@@ -195,7 +195,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--extras", action="store_true", help="also time the unfused chain, FP32 and the 512^2 0-form")
-    ap.add_argument("--workload", default="laplacian", choices=["laplacian", "solve", "mag3d", "precond", "hodge3d"])
+    ap.add_argument("--workload", default="laplacian",
+                    choices=["laplacian", "solve", "mag3d", "precond", "hodge3d", "nonlinear"])
+    ap.add_argument("--n2d", type=int, default=257, help="nonlinear: nodes per axis")
     ap.add_argument("--solvers", default="cg,mixed,learned", help="solve / mag3d: solver kinds to time")
     ap.add_argument("--max-iterations", type=int, default=200000, help="solve / mag3d: iteration budget")
     ap.add_argument("--shapes", default=None, help="precond: NxC (C grids of N^2 nodes); default the 64-problem batch")
@@ -216,6 +218,9 @@ def main():
         return
     if args.workload == "mag3d":
         run_mag3d_workload(args)
+        return
+    if args.workload == "nonlinear":
+        run_nonlinear_workload(args)
         return
     if args.workload == "precond":
         run_precond_workload(args)
@@ -577,6 +582,55 @@ def run_mag3d_workload(args):
             "config": {"workload": f"{len(probs)} x {n}^3 nodes x 3 components, gamma 20", "host_setup_s": setup,
                        "best": best},
             "solvers": results, "hodge_star_1_to_2_form": hodge, "clocks": clocks.summary()}
+    print(json.dumps(line))
+
+
+def run_nonlinear_workload(args):
+    """Batch of seeded 2D problems whose permeability-1000 rectangles are a
+    saturating material: Newton (at most 30 steps) + line search, each step a
+    Jacobi-CG solve of the Jacobian to 1e-10.  Beside it, the oracle's solve
+    of the batch's first problem on all host cores (same algorithm)."""
+    import torch
+    import similie_b200.magnetostatics as mag
+    torch.cuda.set_device(0)
+    n = args.n2d
+    count = args.count or 8
+    cases = [mag.nonlinear_problem(n, s) for s in range(count)]
+    mus = [torch.from_numpy(c[1]).cuda() for c in cases]
+    fes = [torch.from_numpy(c[2]).cuda() for c in cases]
+    rhss = [torch.from_numpy(c[0].rhs()).cuda() for c in cases]
+    curves = [(c[3], c[4]) for c in cases]
+    with ClockSampler(0) as clocks:
+        sols = [torch.zeros_like(r) for r in rhss]
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d = mag.nl_solve_batch(mus, fes, curves, rhss, sols, [(n, n)] * count, tol=1e-10,
+                               max_iterations=args.max_iterations)
+        e1.record()
+        torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    steps = sum(x.refinements for x in d)
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle as O
+        p, mu, fe, b, h = cases[0]
+        t0 = time.perf_counter()
+        xo, it, st, rel = O.mag2d_nl_solve(n, n, mu, fe, b, h, p.rhs(), tol=1e-10, max_iter=args.max_iterations)
+        tc = time.perf_counter() - t0
+        cpu = {"value": 1.0 / tc, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"the batch's first problem ({n}^2, {st} Newton steps, {it} CG iterations) in {tc:.2f} s",
+               "gpu_solution_rel_diff": float(np.linalg.norm(sols[0].cpu().numpy() - xo) / np.linalg.norm(xo))}
+    line = {"metric": f"nonlinear 2D magnetostatics (Newton + line search), batch of {count} problems {n}^2",
+            "value": count / sec, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded coils; saturating permeability-1000 rectangles, 64-sample B-H curve)",
+            "config": {"workload": f"{count} x {n}^2 nodes, tol 1e-10, at most 30 Newton steps"},
+            "newton_steps": steps, "ms_per_newton_step": sec * 1e3 / max(steps, 1),
+            "cg_iterations": sum(x.iterations for x in d), "converged": sum(x.converged for x in d),
+            "final_relative_residuals": [x.final_relative_residual for x in d],
+            "cpu_baseline": cpu, "clocks": clocks.summary()}
     print(json.dumps(line))
 
 

@@ -612,6 +612,40 @@ sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int np
             D.converged = 1;
             continue;
         }
+        // 16 CG iterations captured once per problem (the kernels stop doing
+        // work once the state is marked done) and replayed until convergence.
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        {
+            cudaStream_t cs;
+            SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+            for (int c = 0; c < 16 && err == cudaSuccess; ++c) {
+                cg_jac_kernel<<<G, kBlock, 0, cs>>>(g, c00, c01, c11, pv, qv, part, d_cg);
+                cg_alpha_kernel<<<1, kBlock, 0, cs>>>(part, static_cast<int>(G), d_cg);
+                cg_update_kernel<<<G, kBlock, 0, cs>>>(n, dvec, cr, pv, qv, dinv, z, part, d_cg);
+                cg_beta_kernel<<<1, kBlock, 0, cs>>>(part, static_cast<int>(G), d_cg, tol, max_iter);
+                cg_direction_kernel<<<G, kBlock, 0, cs>>>(n, pv, z, d_cg);
+            }
+            cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
+            if (err == cudaSuccess) err = err2;
+            if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+            cudaStreamDestroy(cs);
+            if (err != cudaSuccess) {
+                if (graph != nullptr) cudaGraphDestroy(graph);
+                return cuda_fail(err, "nonlinear CG graph capture");
+            }
+        }
+        struct GraphGuard
+        {
+            cudaGraph_t g;
+            cudaGraphExec_t e;
+            ~GraphGuard()
+            {
+                cudaGraphExecDestroy(e);
+                cudaGraphDestroy(g);
+            }
+        } guard {graph, exec};
         int cg_total = 0, steps = 0;
         for (int it = 0; it < 30; ++it) {
             if (res / r0 <= tol) break;
@@ -623,14 +657,7 @@ sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int np
             SIL_CUDA_CHECK(cudaGetLastError());
             CgState hs {};
             for (;;) {
-                for (int c = 0; c < 16; ++c) {
-                    cg_jac_kernel<<<G, kBlock, 0, st>>>(g, c00, c01, c11, pv, qv, part, d_cg);
-                    cg_alpha_kernel<<<1, kBlock, 0, st>>>(part, static_cast<int>(G), d_cg);
-                    cg_update_kernel<<<G, kBlock, 0, st>>>(n, dvec, cr, pv, qv, dinv, z, part, d_cg);
-                    cg_beta_kernel<<<1, kBlock, 0, st>>>(part, static_cast<int>(G), d_cg, tol, max_iter);
-                    cg_direction_kernel<<<G, kBlock, 0, st>>>(n, pv, z, d_cg);
-                }
-                SIL_CUDA_CHECK(cudaGetLastError());
+                SIL_CUDA_CHECK(cudaGraphLaunch(exec, st));
                 SIL_CUDA_CHECK(cudaMemcpyAsync(&hs, d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, st));
                 SIL_CUDA_CHECK(cudaStreamSynchronize(st));
                 if (hs.done) break;
