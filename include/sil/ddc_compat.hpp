@@ -1,0 +1,378 @@
+// ddc_compat.hpp -- the call shapes of SimiLie's exterior-calculus and
+// solver entry points, over the sil_b200 C ABI, so that call sites written
+// against the reference port line by line:
+//
+//   reference (src/similie/...)                           here
+//   deriv<TagToAdd, CochainTag>(exec, out, in)            deriv<K>(exec, out, in)
+//     exterior/coboundary.hpp:698-709
+//   transposed_coboundary(exec, out, in)                  transposed_coboundary<K>(exec, out, in)
+//     exterior/coboundary.hpp:661-696
+//   fill_discrete_hodge_star<Idx1, Idx2>(exec, hodge,     fill_discrete_hodge_star<KIn>(exec, hodge,
+//     metric, position)  exterior/hodge_star.hpp:453-494    metric, position)
+//   tensor_prod(out, in, hodge) on the stored star        hodge_star_stored<KIn>(exec, out, in, hodge)
+//   make_staged_codifferential(...).run(out, in),         codifferential<K>(exec, geometry, out, in)
+//   codifferential(...)  exterior/codifferential.hpp:439-656
+//   make_staged_laplacian(exec, out, in, metric,          make_staged_laplacian<K>(exec, geometry, out, in)
+//     position).run(out, in)  exterior/laplacian.hpp:327-358   .run(out, in)
+//   laplacian(...)  exterior/laplacian.hpp:814-951        laplacian<K>(exec, geometry, out, in)
+//   solvers::minimize_strong_formulation_residual(        minimize_strong_formulation_residual(
+//     exec, operator_model, rhs, solution, settings)        exec, operator_model, rhs, solution, settings)
+//     solvers/minimize_strong_formulation_residual.hpp:1308-1570
+//
+// The reference's tags become the form degree K (a template argument) and
+// the dimension (the field's); its DDC tensor spans become Tensor, a
+// non-owning view of device memory (sil_field); the Kokkos execution space
+// becomes ExecSpace, a CUDA stream.  The metric / position pair of the
+// staged operators on a rectilinear grid with the identity metric becomes a
+// Geometry built from the node coordinates.  As in the reference the calls
+// are asynchronous on the stream (the caller fences), the solver calls are
+// synchronous, and errors are thrown (Error, carrying the sil_status).
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../sil_b200.h"
+
+namespace sil {
+namespace compat {
+
+class Error : public std::runtime_error
+{
+public:
+    Error(sil_status s, std::string const& what) : std::runtime_error(what), status(s) {}
+    sil_status status;
+};
+
+inline void check(sil_status s, char const* what)
+{
+    if (s != SIL_OK) throw Error(s, std::string(what) + ": " + sil_status_string(s) + ": " + sil_last_error());
+}
+
+// A Kokkos execution-space instance: here a CUDA stream (nullptr: the legacy default stream).
+struct ExecSpace
+{
+    sil_stream stream = nullptr;
+};
+
+// Non-owning view of a device field in the reference's DDC layout_right
+// ordering: lattice dimensions slowest to fastest, then the form component.
+struct Tensor
+{
+    sil_field field {};
+
+    // extents: lattice points per dimension (the last ones may be spectator
+    // dimensions); ncomp: stored form components; front: absolute discrete
+    // coordinate of element 0 per dimension (nullptr: all zero).
+    static Tensor make(void* data, sil_dtype dtype, std::vector<int64_t> const& extents, int ncomp,
+                       int64_t const* front = nullptr)
+    {
+        if (extents.empty() || extents.size() > SIL_MAX_DIMS) throw Error(SIL_ERR_INVALID, "Tensor: 1 to SIL_MAX_DIMS dimensions");
+        Tensor t;
+        t.field.data = data;
+        t.field.dtype = dtype;
+        t.field.ndims = static_cast<int32_t>(extents.size());
+        t.field.ncomp = ncomp;
+        int64_t stride = ncomp;
+        for (int d = static_cast<int>(extents.size()) - 1; d >= 0; --d) {
+            t.field.extent[d] = extents[d];
+            t.field.stride[d] = stride;
+            t.field.front[d] = front != nullptr ? front[d] : 0;
+            stride *= extents[d];
+        }
+        t.field.comp_stride = 1;
+        return t;
+    }
+};
+
+// Rectilinear grid with the identity metric (the metric + position tensors
+// of the staged operators): node coordinates per form dimension.
+class Geometry
+{
+public:
+    Geometry(std::vector<std::vector<double>> const& coords, std::vector<int64_t> const& front = {})
+    {
+        std::vector<double const*> c;
+        std::vector<int64_t> n;
+        for (auto const& v : coords) {
+            c.push_back(v.data());
+            n.push_back(static_cast<int64_t>(v.size()));
+        }
+        check(sil_geometry_create(&g_, static_cast<int>(coords.size()), c.data(), n.data(),
+                                  front.empty() ? nullptr : front.data()),
+              "Geometry");
+    }
+    Geometry(Geometry const&) = delete;
+    Geometry& operator=(Geometry const&) = delete;
+    ~Geometry() { sil_geometry_destroy(g_); }
+    sil_geometry get() const { return g_; }
+
+private:
+    sil_geometry g_ = nullptr;
+};
+
+// Every dimension of the field is a form dimension.
+inline uint32_t all_form_dims(Tensor const& t) { return (1u << t.field.ndims) - 1u; }
+
+// ------------------------------------------------------------------ exterior calculus
+
+template <int K>
+Tensor deriv(ExecSpace exec, Tensor out, Tensor in, uint32_t form_mask = 0)
+{
+    check(sil_deriv(exec.stream, form_mask ? form_mask : all_form_dims(in), K, &in.field, &out.field), "deriv");
+    return out;
+}
+
+template <int K>
+Tensor transposed_coboundary(ExecSpace exec, Tensor out, Tensor in, uint32_t form_mask = 0)
+{
+    check(sil_transposed_coboundary(exec.stream, form_mask ? form_mask : all_form_dims(in), K, &in.field,
+                                    &out.field),
+          "transposed_coboundary");
+    return out;
+}
+
+template <int K>
+Tensor hodge_star(ExecSpace exec, Geometry const& geometry, Tensor out, Tensor in, uint32_t form_mask = 0)
+{
+    check(sil_hodge_star(geometry.get(), exec.stream, form_mask ? form_mask : all_form_dims(in), K, &in.field,
+                         &out.field),
+          "hodge_star");
+    return out;
+}
+
+// General per-node metric (metric == nullptr: identity), n form dimensions.
+template <int KIn>
+Tensor fill_discrete_hodge_star(ExecSpace exec, Tensor hodge, Tensor const* metric, Tensor position, int n)
+{
+    check(sil_fill_discrete_hodge_star_metric(exec.stream, n, KIn, &position.field,
+                                              metric != nullptr ? &metric->field : nullptr, &hodge.field),
+          "fill_discrete_hodge_star");
+    return hodge;
+}
+
+template <int KIn>
+Tensor hodge_star_stored(ExecSpace exec, Tensor out, Tensor in, Tensor hodge, int n)
+{
+    check(sil_hodge_star_stored(exec.stream, n, KIn, &hodge.field, &in.field, &out.field), "hodge_star_stored");
+    return out;
+}
+
+template <int K>
+Tensor codifferential(ExecSpace exec, Geometry const& geometry, Tensor out, Tensor in, uint32_t form_mask = 0)
+{
+    check(sil_codifferential(geometry.get(), exec.stream, form_mask ? form_mask : all_form_dims(in), K, &in.field,
+                             &out.field),
+          "codifferential");
+    return out;
+}
+
+template <int K>
+Tensor laplacian(ExecSpace exec, Geometry const& geometry, Tensor out, Tensor in, uint32_t form_mask = 0)
+{
+    check(sil_laplacian(geometry.get(), exec.stream, form_mask ? form_mask : all_form_dims(in), K, &in.field,
+                        &out.field),
+          "laplacian");
+    return out;
+}
+
+// StagedLaplacian: built once for fields shaped like (out, in), run many times.
+template <int K>
+class StagedLaplacian
+{
+public:
+    StagedLaplacian(Geometry const& geometry, Tensor out_like, Tensor in_like, bool fused, uint32_t form_mask)
+    {
+        check(sil_laplacian_plan_create(&plan_, geometry.get(), form_mask ? form_mask : all_form_dims(in_like), K,
+                                        &in_like.field, &out_like.field,
+                                        fused ? SIL_LAPLACIAN_FUSED : SIL_LAPLACIAN_UNFUSED),
+              "make_staged_laplacian");
+    }
+    StagedLaplacian(StagedLaplacian&& o) noexcept : plan_(std::exchange(o.plan_, nullptr)) {}
+    StagedLaplacian(StagedLaplacian const&) = delete;
+    ~StagedLaplacian()
+    {
+        if (plan_ != nullptr) sil_laplacian_plan_destroy(plan_);
+    }
+    Tensor run(ExecSpace exec, Tensor out, Tensor in) const
+    {
+        check(sil_laplacian_run(plan_, exec.stream, &in.field, &out.field), "StagedLaplacian::run");
+        return out;
+    }
+
+private:
+    sil_laplacian_plan plan_ = nullptr;
+};
+
+template <int K>
+StagedLaplacian<K> make_staged_laplacian(ExecSpace, Geometry const& geometry, Tensor out, Tensor in,
+                                         bool fused = true, uint32_t form_mask = 0)
+{
+    return StagedLaplacian<K>(geometry, out, in, fused, form_mask);
+}
+
+// ------------------------------------------------------------------ solvers
+
+// solvers/minimize_strong_formulation_residual.hpp: the settings this path reads.
+struct StrongFormulationSolverSettings
+{
+    double relative_tolerance = 1e-10;
+    unsigned int max_iterations = 100000;
+    // Jacobi-CG in FP64 (the reference's), or FP32 inner CG with FP64
+    // refinement; linear operators only.
+    bool mixed_precision = false;
+};
+
+struct StrongFormulationSolverDiagnostics
+{
+    unsigned int iterations = 0;
+    bool converged = false;
+    double initial_residual_l2 = 0.0;
+    double final_residual_l2 = 0.0;
+    double final_relative_residual = 0.0;
+    unsigned int nonlinear_iterations = 0;  // Newton steps (nonlinear operators)
+};
+
+// The OperatorModel concept of the reference (IS_LINEAR, size(), apply,
+// apply_jacobian) for the magnetostatics operators; device FP64 arrays.
+// magnetostatics_onelab.hpp:1013-1426 (2D), 1625-2700 (3D), 957-1011 and 2799-2915 (nonlinear material).
+struct MagnetostaticsOperator2D
+{
+    static constexpr bool IS_LINEAR = true;
+    int64_t nx, ny;
+    double const* node_mu;
+    int64_t size() const { return nx * ny; }
+    void apply(ExecSpace exec, double const* in, double* out) const
+    {
+        check(sil_mag2d_apply(exec.stream, nx, ny, node_mu, in, out), "MagnetostaticsOperator2D::apply");
+    }
+};
+
+struct MagnetostaticsOperator3D
+{
+    static constexpr bool IS_LINEAR = true;
+    std::vector<double> x, y, z;  // node coordinates (host)
+    double const* node_mu;
+    double gauge_penalty = 20.0;
+    int64_t size() const { return 3 * static_cast<int64_t>(x.size() * y.size() * z.size()); }
+    sil_mag3d_problem problem(double const* rhs = nullptr, double* solution = nullptr) const
+    {
+        sil_mag3d_problem p {};
+        p.nx = static_cast<int64_t>(x.size());
+        p.ny = static_cast<int64_t>(y.size());
+        p.nz = static_cast<int64_t>(z.size());
+        p.x = x.data();
+        p.y = y.data();
+        p.z = z.data();
+        p.node_mu = node_mu;
+        p.rhs = rhs;
+        p.solution = solution;
+        p.gauge_penalty = gauge_penalty;
+        return p;
+    }
+    void apply(ExecSpace exec, double const* in, double* out) const
+    {
+        sil_mag3d_problem const p = problem();
+        check(sil_mag3d_apply(exec.stream, &p, in, out), "MagnetostaticsOperator3D::apply");
+    }
+};
+
+struct NonlinearMagnetostaticsOperator2D
+{
+    static constexpr bool IS_LINEAR = false;
+    int64_t nx, ny;
+    double const* node_mu;
+    double const* node_ferro;
+    std::vector<double> curve_b, curve_h;  // B-H samples (host)
+    int64_t size() const { return nx * ny; }
+    sil_mag2d_nl_problem problem(double const* rhs = nullptr, double* solution = nullptr) const
+    {
+        sil_mag2d_nl_problem p {};
+        p.nx = nx;
+        p.ny = ny;
+        p.node_mu = node_mu;
+        p.node_ferro = node_ferro;
+        p.curve.n = static_cast<int32_t>(curve_b.size());
+        p.curve.b = curve_b.data();
+        p.curve.h = curve_h.data();
+        p.rhs = rhs;
+        p.solution = solution;
+        return p;
+    }
+    void apply(ExecSpace exec, double const* in, double* out) const
+    {
+        sil_mag2d_nl_problem const p = problem();
+        check(sil_mag2d_nl_apply(exec.stream, &p, in, out), "NonlinearMagnetostaticsOperator2D::apply");
+    }
+    void apply_jacobian(ExecSpace exec, double const* state, double const* in, double* out) const
+    {
+        sil_mag2d_nl_problem const p = problem();
+        check(sil_mag2d_nl_apply_jacobian(exec.stream, &p, state, in, out), "apply_jacobian");
+    }
+};
+
+namespace detail {
+
+inline sil_solve_settings to_settings(StrongFormulationSolverSettings const& s)
+{
+    sil_solve_settings r {};
+    r.solver = s.mixed_precision ? SIL_SOLVER_MIXED_IR : SIL_SOLVER_CG_F64;
+    r.max_iterations = static_cast<int32_t>(s.max_iterations);
+    r.relative_tolerance = s.relative_tolerance;
+    return r;
+}
+
+inline StrongFormulationSolverDiagnostics to_diagnostics(sil_solve_diagnostics const& d, bool nonlinear)
+{
+    StrongFormulationSolverDiagnostics r;
+    r.iterations = static_cast<unsigned int>(d.iterations);
+    r.converged = d.converged != 0;
+    r.initial_residual_l2 = d.initial_residual_l2;
+    r.final_residual_l2 = d.final_residual_l2;
+    r.final_relative_residual = d.final_relative_residual;
+    r.nonlinear_iterations = nonlinear ? static_cast<unsigned int>(d.refinements) : 0u;
+    return r;
+}
+
+}  // namespace detail
+
+// The linear solves start from x = 0 (as the reference's); the nonlinear
+// one from the content of `solution`.  Synchronous.
+inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
+        ExecSpace exec, MagnetostaticsOperator2D const& op, double const* rhs, double* solution,
+        StrongFormulationSolverSettings const& settings)
+{
+    sil_mag2d_problem p {op.nx, op.ny, op.node_mu, rhs, solution};
+    sil_solve_settings const s = detail::to_settings(settings);
+    sil_solve_diagnostics d {};
+    check(sil_mag2d_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
+    return detail::to_diagnostics(d, false);
+}
+
+inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
+        ExecSpace exec, MagnetostaticsOperator3D const& op, double const* rhs, double* solution,
+        StrongFormulationSolverSettings const& settings)
+{
+    sil_mag3d_problem const p = op.problem(rhs, solution);
+    sil_solve_settings const s = detail::to_settings(settings);
+    sil_solve_diagnostics d {};
+    check(sil_mag3d_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
+    return detail::to_diagnostics(d, false);
+}
+
+inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
+        ExecSpace exec, NonlinearMagnetostaticsOperator2D const& op, double const* rhs, double* solution,
+        StrongFormulationSolverSettings const& settings)
+{
+    sil_mag2d_nl_problem const p = op.problem(rhs, solution);
+    sil_solve_settings const s = detail::to_settings(settings);
+    sil_solve_diagnostics d {};
+    check(sil_mag2d_nl_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
+    return detail::to_diagnostics(d, true);
+}
+
+}  // namespace compat
+}  // namespace sil

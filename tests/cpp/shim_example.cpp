@@ -1,0 +1,105 @@
+// A reference-style call site compiled against include/sil/ddc_compat.hpp:
+// d of a 0-form, the staged Laplacian of that 0-form, and a 2D
+// magnetostatics solve through minimize_strong_formulation_residual.
+// Writes its outputs as raw little-endian doubles into the directory given
+// as the first argument; tests/test_gpu_cpp_shim.py checks them against the
+// oracle.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "sil/ddc_compat.hpp"
+
+using namespace sil::compat;
+
+namespace {
+
+double* to_device(std::vector<double> const& h)
+{
+    double* d = nullptr;
+    cudaMalloc(&d, h.size() * sizeof(double));
+    cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+    return d;
+}
+
+std::vector<double> to_host(double const* d, size_t n)
+{
+    std::vector<double> h(n);
+    cudaMemcpy(h.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost);
+    return h;
+}
+
+void write(std::string const& path, std::vector<double> const& v)
+{
+    FILE* f = std::fopen(path.c_str(), "wb");
+    std::fwrite(v.data(), sizeof(double), v.size(), f);
+    std::fclose(f);
+}
+
+}  // namespace
+
+int main(int argc, char** argv)
+{
+    if (argc < 2) return 2;
+    std::string const dir = argv[1];
+    ExecSpace const exec {};
+    try {
+        // d and the Laplacian of a 0-form on a 12 x 9 lattice (x slowest)
+        int const nx = 12, ny = 9;
+        std::vector<double> phi(nx * ny), xs(nx), ys(ny);
+        for (int i = 0; i < nx; ++i) xs[i] = 0.1 * i + 0.002 * i * i;
+        for (int j = 0; j < ny; ++j) ys[j] = 0.15 * j;
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) phi[i * ny + j] = std::sin(0.3 * i) * std::cos(0.2 * j) + 0.01 * i * j;
+        double* d_phi = to_device(phi);
+        double* d_dphi = to_device(std::vector<double>(nx * ny * 2, 0.0));
+        double* d_lap = to_device(std::vector<double>((nx - 1) * (ny - 1), 0.0));
+        Tensor const in = Tensor::make(d_phi, SIL_F64, {nx, ny}, 1);
+        Tensor const dout = Tensor::make(d_dphi, SIL_F64, {nx, ny}, 2);
+        Tensor const lout = Tensor::make(d_lap, SIL_F64, {nx - 1, ny - 1}, 1);
+        deriv<0>(exec, dout, in);
+        Geometry const geometry({xs, ys});
+        auto const staged = make_staged_laplacian<0>(exec, geometry, lout, in);
+        staged.run(exec, lout, in);
+
+        // 2D magnetostatics, 33 x 33 nodes: a permeability-1000 block and a source block
+        int const n = 33;
+        std::vector<double> mu(n * n, 1.0), rhs(n * n, 0.0);
+        for (int j = 10; j < 20; ++j)
+            for (int i = 12; i < 24; ++i) mu[i + n * j] = 1000.0;
+        for (int j = 5; j < 9; ++j)
+            for (int i = 4; i < 9; ++i) rhs[i + n * j] = 1e-3;
+        double* d_mu = to_device(mu);
+        double* d_rhs = to_device(rhs);
+        double* d_sol = to_device(std::vector<double>(n * n, 0.0));
+        MagnetostaticsOperator2D const op {n, n, d_mu};
+        StrongFormulationSolverSettings settings;
+        settings.relative_tolerance = 1e-10;
+        StrongFormulationSolverDiagnostics const diag =
+                minimize_strong_formulation_residual(exec, op, d_rhs, d_sol, settings);
+        cudaDeviceSynchronize();
+
+        write(dir + "/phi.bin", phi);
+        write(dir + "/dphi.bin", to_host(d_dphi, nx * ny * 2));
+        write(dir + "/lap.bin", to_host(d_lap, (nx - 1) * (ny - 1)));
+        write(dir + "/mu.bin", mu);
+        write(dir + "/rhs.bin", rhs);
+        write(dir + "/sol.bin", to_host(d_sol, n * n));
+        std::printf("%u %d %.6e\n", diag.iterations, diag.converged ? 1 : 0, diag.final_relative_residual);
+
+        // errors surface as exceptions carrying the status, as in the reference
+        try {
+            deriv<3>(exec, dout, in);
+            std::printf("no-error\n");
+        } catch (Error const& e) {
+            std::printf("error %d\n", static_cast<int>(e.status));
+        }
+    } catch (Error const& e) {
+        std::fprintf(stderr, "%s\n", e.what());
+        return 1;
+    }
+    return 0;
+}
