@@ -19,6 +19,8 @@
 #include <algorithm>
 #include <cmath>
 #include <limits>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "sil_internal.cuh"
@@ -544,32 +546,45 @@ sil_status sil_mag2d_nl_apply_jacobian(sil_stream stream, const sil_mag2d_nl_pro
     return SIL_OK;
 }
 
-sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int nproblems,
-                                    const sil_solve_settings* settings, sil_solve_diagnostics* diag,
-                                    sil_stream stream)
-{
-    if (problems == nullptr || settings == nullptr || diag == nullptr || nproblems <= 0)
-        return fail(SIL_ERR_INVALID, "sil_mag2d_nl_solve_batch: NULL argument or empty batch");
-    std::vector<DevCurve> curves(nproblems);
-    int64_t maxn = 0;
-    for (int p = 0; p < nproblems; ++p) {
-        sil_mag2d_nl_problem const& q = problems[p];
-        if (sil_status s = check_problem(q, "sil_mag2d_nl_solve_batch"); s != SIL_OK) return s;
-        if (q.rhs == nullptr || q.solution == nullptr) return fail(SIL_ERR_INVALID, "sil_mag2d_nl_solve_batch: NULL field pointer");
-        if (sil_status s = make_curve(q.curve, &curves[p]); s != SIL_OK) return s;
-        maxn = std::max<int64_t>(maxn, q.nx * q.ny);
-    }
-    double const tol = settings->relative_tolerance > 0 ? settings->relative_tolerance : 1e-10;
-    int const max_iter = settings->max_iterations > 0 ? settings->max_iterations : 100000;
-    cudaStream_t const st = static_cast<cudaStream_t>(stream);
+namespace sil {
+namespace {
 
+// One problem's Newton solve on its own stream and buffers (the problems of
+// a batch run on concurrent host threads).
+sil_status solve_one(sil_mag2d_nl_problem const& P, DevCurve const& C, double tol, int max_iter,
+                     sil_solve_diagnostics& D)
+{
+    int64_t const maxn = P.nx * P.ny;
     // r, cand_r, cand, d, cr, z, p, q, dinv, c00, c01, c11 + partials + scalars
     int const nvec = 12;
     size_t const vbytes = ((static_cast<size_t>(maxn) * sizeof(double) + 255) / 256) * 256;
     unsigned const gmax = grid_for(maxn);
     size_t const pbytes = ((2 * static_cast<size_t>(gmax) * sizeof(double) + 255) / 256) * 256;
-    DeviceBuffer buf;
-    SIL_CUDA_CHECK(cudaMalloc(&buf.ptr, nvec * vbytes + pbytes + 2 * 256));
+    struct StreamGuard
+    {
+        cudaStream_t s = nullptr;
+        ~StreamGuard()
+        {
+            if (s != nullptr) cudaStreamDestroy(s);
+        }
+    } sg;
+    SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&sg.s, cudaStreamNonBlocking));
+    cudaStream_t const st = sg.s;
+    // stream-ordered allocation: freeing does not synchronise the other
+    // problems' streams
+    struct AsyncBuffer
+    {
+        void* ptr = nullptr;
+        cudaStream_t s;
+        ~AsyncBuffer()
+        {
+            if (ptr != nullptr) {
+                cudaFreeAsync(ptr, s);
+                cudaStreamSynchronize(s);
+            }
+        }
+    } buf {nullptr, st};
+    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, nvec * vbytes + pbytes + 2 * 256, st));
     char* base = static_cast<char*>(buf.ptr);
     double* v[nvec];
     for (int k = 0; k < nvec; ++k) v[k] = reinterpret_cast<double*>(base + k * vbytes);
@@ -578,15 +593,11 @@ sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int np
     CgState* d_cg = reinterpret_cast<CgState*>(base + nvec * vbytes + pbytes + 256);
     double *r = v[0], *cand_r = v[1], *cand = v[2], *dvec = v[3], *cr = v[4], *z = v[5], *pv = v[6], *qv = v[7],
            *dinv = v[8], *c00 = v[9], *c01 = v[10], *c11 = v[11];
-
-    for (int pi = 0; pi < nproblems; ++pi) {
-        sil_mag2d_nl_problem const& P = problems[pi];
-        sil_solve_diagnostics& D = diag[pi];
+    do {
         D = sil_solve_diagnostics {};
         Geo const g {static_cast<int>(P.nx), static_cast<int>(P.ny)};
         int const n = g.nx * g.ny;
         unsigned const G = grid_for(n);
-        DevCurve const& C = curves[pi];
         double* x = P.solution;
         // residual norm of rhs - F(v) into out (returned on the host)
         auto residual = [&](double const* val, double* out, double* norm) -> sil_status {
@@ -606,11 +617,11 @@ sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int np
             D.status = SIL_ERR_NONFINITE;
             D.final_residual_l2 = r0;
             D.final_relative_residual = r0;
-            continue;
+            break;
         }
         if (r0 == 0.0) {
             D.converged = 1;
-            continue;
+            break;
         }
         // 16 CG iterations captured once per problem (the kernels stop doing
         // work once the state is marked done) and replayed until convergence.
@@ -692,7 +703,55 @@ sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int np
         D.final_relative_residual = res / r0;
         D.converged = (res / r0 <= tol) ? 1 : 0;
         if (!std::isfinite(res)) D.status = SIL_ERR_NONFINITE;
-    }
+    } while (false);
     SIL_CUDA_CHECK(cudaStreamSynchronize(st));
+    return SIL_OK;
+}
+
+}  // namespace
+}  // namespace sil
+
+using namespace sil;
+
+sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int nproblems,
+                                    const sil_solve_settings* settings, sil_solve_diagnostics* diag,
+                                    sil_stream stream)
+{
+    if (problems == nullptr || settings == nullptr || diag == nullptr || nproblems <= 0)
+        return fail(SIL_ERR_INVALID, "sil_mag2d_nl_solve_batch: NULL argument or empty batch");
+    std::vector<DevCurve> curves(nproblems);
+    for (int p = 0; p < nproblems; ++p) {
+        sil_mag2d_nl_problem const& q = problems[p];
+        if (sil_status s = check_problem(q, "sil_mag2d_nl_solve_batch"); s != SIL_OK) return s;
+        if (q.rhs == nullptr || q.solution == nullptr) return fail(SIL_ERR_INVALID, "sil_mag2d_nl_solve_batch: NULL field pointer");
+        if (sil_status s = make_curve(q.curve, &curves[p]); s != SIL_OK) return s;
+    }
+    double const tol = settings->relative_tolerance > 0 ? settings->relative_tolerance : 1e-10;
+    int const max_iter = settings->max_iterations > 0 ? settings->max_iterations : 100000;
+    // the inputs come from the caller's stream
+    SIL_CUDA_CHECK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    (void)grid_for(1);  // device attributes read once, before the threads start
+    int dev = 0;
+    SIL_CUDA_CHECK(cudaGetDevice(&dev));
+    // Up to kConcurrent problems at a time, each on a host thread with its
+    // own stream: one problem's CG kernels are small and launch bound, so
+    // several problems together fill the GPU.
+    constexpr int kConcurrent = 8;
+    std::vector<sil_status> status(nproblems, SIL_OK);
+    std::vector<std::string> message(nproblems);
+    for (int first = 0; first < nproblems; first += kConcurrent) {
+        int const last = std::min(nproblems, first + kConcurrent);
+        std::vector<std::thread> workers;
+        for (int p = first; p < last; ++p) {
+            workers.emplace_back([&, p] {
+                cudaSetDevice(dev);
+                status[p] = solve_one(problems[p], curves[p], tol, max_iter, diag[p]);
+                if (status[p] != SIL_OK) message[p] = sil_last_error();
+            });
+        }
+        for (auto& w : workers) w.join();
+    }
+    for (int p = 0; p < nproblems; ++p)
+        if (status[p] != SIL_OK) return fail(status[p], message[p]);
     return SIL_OK;
 }
