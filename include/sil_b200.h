@@ -382,6 +382,12 @@ typedef struct sil_mag3d_problem {
     const double* rhs;       /* device, 3*nx*ny*nz: right-hand side, 0 on the boundary */
     double* solution;        /* device, 3*nx*ny*nz: written (initial guess is 0) */
     double gauge_penalty;    /* gamma > 0 (the reference's default is 20) */
+    int32_t gauge;           /* 0: penalty gamma * (star A), the default.  1: divergence gauge
+                              * gamma * sum_c w(c) D(c, row) (D A)(c), D the codifferential of the
+                              * 1-form A (boundary columns dropped), w(c) the product of the local
+                              * spacings at node c (the reference's SIMILIE_DIVERGENCE_GAUGE_3D,
+                              * magnetostatics_onelab.hpp:1890-1945, 2355-2392); gamma may then be
+                              * negative (SIMILIE_VECTOR_POTENTIAL_GAUGE_SIGN_3D folded in). */
 } sil_mag3d_problem;
 
 /* y = K a for one problem (a, y: device, 3*nx*ny*nz doubles; rhs and

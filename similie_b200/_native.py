@@ -75,6 +75,7 @@ class SilMag3dProblem(ctypes.Structure):
         ("rhs", ctypes.c_void_p),
         ("solution", ctypes.c_void_p),
         ("gauge_penalty", ctypes.c_double),
+        ("gauge", ctypes.c_int32),
     ]
 
 

@@ -90,6 +90,9 @@ struct ProbInfo
     double const* ils64[3];
     float const* ls32[3];
     float const* ils32[3];
+    int gauge;                // 3D: 0 penalty, 1 divergence gauge
+    double const* gd64;       // divergence gauge, 8 per node: E0[3], E1[3], w, 0
+    float const* gd32;
 };
 
 template <class T>
@@ -115,6 +118,47 @@ __device__ __forceinline__ T const* inv_spacing(ProbInfo const& pi, int axis)
 // (boundary DOFs dropped from the stencils), weighted by the Hodge factor of
 // B (d_m / (d_a d_b), central local spacings) and 1/mu(s); the gauge term is
 // gamma * (d_a d_b / d_c) * A.  Boundary rows are the identity.
+template <class T>
+__device__ __forceinline__ T const* gauge_table(ProbInfo const& pi)
+{
+    if constexpr (sizeof(T) == 8) return pi.gd64;
+    else return pi.gd32;
+}
+
+// Divergence gauge.  The codifferential of the 1-form A at node m is
+// (D A)(m) = sum_a E0(m, a) A_a(m) + E1(m, a) A_a(m - e_a), with the
+// coefficients of boundary columns zero (they are dropped from the
+// reference's stencils, magnetostatics_onelab.hpp:1894-1945).  The gauge
+// term of row (n, c) is sum over the codifferential rows holding the column,
+// m = n and m = n + e_c, of w(m) D(m, (n, c)) (D A)(m).
+template <class T>
+__device__ __forceinline__ T gauge_div(T const* a, T const* gd, int m, int i, int j, int k, int nx, int ny)
+{
+    T const* e = gd + 8 * m;
+    T s = T(0);
+    s = s + e[0] * a[3 * m];
+    if (i > 0) s = s + e[3] * a[3 * (m - 1)];
+    s = s + e[1] * a[3 * m + 1];
+    if (j > 0) s = s + e[4] * a[3 * (m - nx) + 1];
+    s = s + e[2] * a[3 * m + 2];
+    if (k > 0) s = s + e[5] * a[3 * (m - nx * ny) + 2];
+    return s;
+}
+
+// Gauge term of component c at interior node n = (i, j, k), given (D A)(n).
+template <class T>
+__device__ __forceinline__ T gauge_term(T const* a, T const* gd, int n, int i, int j, int k, int nx, int ny, int c,
+                                        T div_n)
+{
+    int const step = c == 0 ? 1 : (c == 1 ? nx : nx * ny);
+    int const m = n + step;
+    T const div_m = gauge_div(a, gd, m, i + (c == 0), j + (c == 1), k + (c == 2), nx, ny);
+    T t = T(0);
+    t = t + gd[8 * n + 6] * gd[8 * n + c] * div_n;
+    t = t + gd[8 * m + 6] * gd[8 * m + 3 + c] * div_m;
+    return t;
+}
+
 template <class T>
 __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_t row64)
 {
@@ -192,6 +236,11 @@ __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_
         if (interior(i - 1, j, k)) res = res - w(-1, 0, 0, 1) * by(-1, 0, 0);
         ha = lx[i] * ly[j] * ilz[k];
     }
+    if (pi.gauge) {
+        T const* gd = gauge_table<T>(pi);
+        T const dn = gauge_div(a, gd, node, i, j, k, nx, ny);
+        return res + static_cast<T>(pi.gamma) * gauge_term(a, gd, node, i, j, k, nx, ny, c, dn);
+    }
     return res + static_cast<T>(pi.gamma) * ha * a[row];
 }
 
@@ -257,13 +306,24 @@ __device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, in
     T const Bx = bx(0, 0, 0), By = by(0, 0, 0), Bz = bz(0, 0, 0);
     T const Wx = w(0, 0, 0, 0), Wy = w(0, 0, 0, 1), Wz = w(0, 0, 0, 2);
     T const g = static_cast<T>(pi.gamma);
+    // gauge term per component: penalty g (d_a d_b / d_c) A_c, or the divergence gauge
+    T gt[3];
+    if (pi.gauge) {
+        T const* gd = gauge_table<T>(pi);
+        T const dn = gauge_div(a, gd, node, i, j, k, nx, ny);
+        for (int c = 0; c < 3; ++c) gt[c] = g * gauge_term(a, gd, node, i, j, k, nx, ny, c, dn);
+    } else {
+        gt[0] = g * (ly[j] * lz[k] * ilx[i]) * a[row0];
+        gt[1] = g * (lx[i] * lz[k] * ily[j]) * a[row0 + 1];
+        gt[2] = g * (lx[i] * ly[j] * ilz[k]) * a[row0 + 2];
+    }
     {
         T res = T(0);
         res = res - Wy * By;
         if (in_k) res = res + w(0, 0, -1, 1) * by(0, 0, -1);
         res = res + Wz * Bz;
         if (in_j) res = res - w(0, -1, 0, 2) * bz(0, -1, 0);
-        out[0] = res + g * (ly[j] * lz[k] * ilx[i]) * a[row0];
+        out[0] = res + gt[0];
     }
     {
         T res = T(0);
@@ -271,7 +331,7 @@ __device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, in
         if (in_k) res = res - w(0, 0, -1, 0) * bx(0, 0, -1);
         res = res - Wz * Bz;
         if (in_i) res = res + w(-1, 0, 0, 2) * bz(-1, 0, 0);
-        out[1] = res + g * (lx[i] * lz[k] * ily[j]) * a[row0 + 1];
+        out[1] = res + gt[1];
     }
     {
         T res = T(0);
@@ -279,7 +339,7 @@ __device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, in
         if (in_j) res = res + w(0, -1, 0, 0) * bx(0, -1, 0);
         res = res + Wy * By;
         if (in_i) res = res - w(-1, 0, 0, 1) * by(-1, 0, 0);
-        out[2] = res + g * (lx[i] * ly[j] * ilz[k]) * a[row0 + 2];
+        out[2] = res + gt[2];
     }
 }
 
@@ -324,6 +384,27 @@ __device__ double mag_diag_row(double const* mu, ProbInfo const& pi, int64_t row
         return lz[kk] * ilx[ii] * ily[jj] * nuv;
     };
     double d = 0.0;
+    if (pi.gauge) {
+        // divergence gauge: sum over the codifferential rows m of w(m) D(m, row)^2
+        int64_t const step = c == 0 ? 1 : (c == 1 ? nx : nx * ny);
+        double const* gd = pi.gd64;
+        double const e0 = gd[8 * node + c], e1 = gd[8 * (node + step) + 3 + c];
+        double const gdiv = gd[8 * node + 6] * e0 * e0 + gd[8 * (node + step) + 6] * e1 * e1;
+        if (c == 0) {
+            d += w(i, j, k, 1) + w(i, j, k, 2);
+            if (interior(i, j, k - 1)) d += w(i, j, k - 1, 1);
+            if (interior(i, j - 1, k)) d += w(i, j - 1, k, 2);
+        } else if (c == 1) {
+            d += w(i, j, k, 0) + w(i, j, k, 2);
+            if (interior(i, j, k - 1)) d += w(i, j, k - 1, 0);
+            if (interior(i - 1, j, k)) d += w(i - 1, j, k, 2);
+        } else {
+            d += w(i, j, k, 0) + w(i, j, k, 1);
+            if (interior(i, j - 1, k)) d += w(i, j - 1, k, 0);
+            if (interior(i - 1, j, k)) d += w(i - 1, j, k, 1);
+        }
+        return d + pi.gamma * gdiv;
+    }
     if (c == 0) {
         d += w(i, j, k, 1) + w(i, j, k, 2);
         if (interior(i, j, k - 1)) d += w(i, j, k - 1, 1);
@@ -878,6 +959,7 @@ struct ProblemDesc
     double const* rhs;
     double* solution;
     double const* coords[3];  // 3D: host node coordinates per axis
+    int gauge = 0;            // 3D: 0 penalty, 1 divergence gauge
 };
 
 // Central local spacing of a node along one axis (one-sided at the ends),
@@ -889,6 +971,97 @@ double local_spacing(double const* c, int64_t n, int64_t i)
     if (i == 0) return c[1] - c[0];
     if (i + 1 == n) return c[n - 1] - c[n - 2];
     return 0.5 * (c[i + 1] - c[i - 1]);
+}
+
+// ---- divergence gauge: the codifferential's coefficients, read off the
+// library's own codifferential (the reference's SimiLie Codifferential::value
+// at every node, identity metric, node positions) applied to six probes.
+// Probe (a, parity) is 1 on component a at the interior nodes whose index
+// along a has that parity; at a node of the same parity the output is the
+// coefficient of A_a(m), at the others that of A_a(m - e_a), each already
+// zero where the column is a boundary DOF.
+
+__global__ void gauge_probe_kernel(double* p, int nx, int ny, int nz, int a, int parity)
+{
+    int64_t const node = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (node >= static_cast<int64_t>(nx) * ny * nz) return;
+    int const i = static_cast<int>(node % nx);
+    int64_t const t = node / nx;
+    int const j = static_cast<int>(t % ny), k = static_cast<int>(t / ny);
+    int const idx = a == 0 ? i : (a == 1 ? j : k);
+    bool const in = i > 0 && j > 0 && k > 0 && i + 1 < nx && j + 1 < ny && k + 1 < nz;
+    for (int c = 0; c < 3; ++c) p[3 * node + c] = (c == a && in && idx % 2 == parity) ? 1.0 : 0.0;
+}
+
+__global__ void gauge_extract_kernel(double const* q, double* gd, int nx, int ny, int nz, int a, int parity)
+{
+    int64_t const node = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (node >= static_cast<int64_t>(nx) * ny * nz) return;
+    int const i = static_cast<int>(node % nx);
+    int64_t const t = node / nx;
+    int const j = static_cast<int>(t % ny), k = static_cast<int>(t / ny);
+    int const idx = a == 0 ? i : (a == 1 ? j : k);
+    if (idx % 2 == parity) gd[8 * node + a] = q[node];
+    else gd[8 * node + 3 + a] = q[node];
+}
+
+// w(m) = product of the local spacings (the reference's codifferential
+// weights, magnetostatics_onelab.hpp:1896-1898); FP32 copy of the table.
+__global__ void gauge_weight_kernel(ProbInfo pi, double* gd, float* gd32)
+{
+    int64_t const node = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (node >= pi.nodes) return;
+    int64_t const i = node % pi.nx, t = node / pi.nx, j = t % pi.ny, k = t / pi.ny;
+    gd[8 * node + 6] = pi.ls64[0][i] * pi.ls64[1][j] * pi.ls64[2][k];
+    gd[8 * node + 7] = 0.0;
+    if (gd32 != nullptr)
+        for (int q = 0; q < 8; ++q) gd32[8 * node + q] = static_cast<float>(gd[8 * node + q]);
+}
+
+// gd (8 doubles per node), gd32 (8 floats per node, may be NULL); probe (3
+// doubles per node) and out (1 per node) are scratch.  pi carries the
+// device spacing tables.
+sil_status build_divergence_gauge(ProblemDesc const& q, ProbInfo const& pi, double* gd, float* gd32, double* probe,
+                                  double* out, cudaStream_t st)
+{
+    int64_t const len[3] = {q.nx, q.ny, q.nz};
+    sil_geometry geo = nullptr;
+    if (sil_status s = sil_geometry_create(&geo, 3, q.coords, len, nullptr); s != SIL_OK) return s;
+    struct GeoGuard
+    {
+        sil_geometry g;
+        ~GeoGuard() { sil_geometry_destroy(g); }
+    } guard {geo};
+    sil_field in {}, o {};
+    in.data = probe;
+    in.dtype = SIL_F64;
+    in.ndims = 3;
+    in.ncomp = 3;
+    o.data = out;
+    o.dtype = SIL_F64;
+    o.ndims = 3;
+    o.ncomp = 1;
+    int64_t stride = 1;
+    for (int a = 0; a < 3; ++a) {
+        in.extent[a] = o.extent[a] = len[a];
+        in.stride[a] = 3 * stride;  // solver layout: 3 * (i + nx (j + ny k)) + c
+        o.stride[a] = stride;
+        stride *= len[a];
+    }
+    in.comp_stride = 1;
+    o.comp_stride = 1;
+    int const nodes_blocks = static_cast<int>((pi.nodes + 255) / 256);
+    int const nx = static_cast<int>(q.nx), ny = static_cast<int>(q.ny), nz = static_cast<int>(q.nz);
+    SIL_CUDA_CHECK(cudaMemsetAsync(gd, 0, sizeof(double) * 8 * pi.nodes, st));
+    for (int a = 0; a < 3; ++a)
+        for (int parity = 0; parity < 2; ++parity) {
+            gauge_probe_kernel<<<nodes_blocks, 256, 0, st>>>(probe, nx, ny, nz, a, parity);
+            if (sil_status s = sil_codifferential(geo, st, 7u, 1, &in, &o); s != SIL_OK) return s;
+            gauge_extract_kernel<<<nodes_blocks, 256, 0, st>>>(out, gd, nx, ny, nz, a, parity);
+        }
+    gauge_weight_kernel<<<nodes_blocks, 256, 0, st>>>(pi, gd, gd32);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
 }
 
 template <class T>
@@ -941,6 +1114,15 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     if (fdirs > kMaxDirs) return fail(SIL_ERR_INVALID, "flexible_directions exceeds 16");
     int const nhist = fdirs > 1 ? 2 * fdirs : 0;
     size_t bytes = (nvec + nhist) * vec_bytes + ndouble_vecs * d_bytes;
+    // divergence-gauge coefficient tables (8 doubles + 8 floats per node)
+    std::vector<size_t> gauge_off(np, 0);
+    size_t gauge_bytes = 0;
+    for (int p = 0; p < np; ++p) {
+        if (probs[p].dim != 3 || probs[p].gauge == 0) continue;
+        gauge_off[p] = gauge_bytes;
+        gauge_bytes += ((static_cast<size_t>(info[p].nodes) * 8 * (sizeof(double) + sizeof(float)) + 255) / 256) * 256;
+    }
+    bytes += gauge_bytes + 256;
     bytes += sizeof(Item) * nitems + sizeof(ProbInfo) * np + sizeof(Vecs<T>) * np + sizeof(Scalars) * np
              + (3 + kMaxDirs) * sizeof(double) * nitems + 7 * sizeof(void*) * np
              + sp64.size() * (sizeof(double) + sizeof(float)) + sizeof(int) * np + 22 * 256;
@@ -968,6 +1150,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     double* part_c = reinterpret_cast<double*>(take(sizeof(double) * nitems));
     double* part_h = reinterpret_cast<double*>(take(sizeof(double) * kMaxDirs * nitems));
     int* d_active = reinterpret_cast<int*>(take(sizeof(int) * np));
+    char* gauge_base = gauge_bytes > 0 ? take(gauge_bytes) : nullptr;
     double const** d_mu = reinterpret_cast<double const**>(take(sizeof(void*) * np));
     double const** d_rhs = reinterpret_cast<double const**>(take(sizeof(void*) * np));
     double** d_nu64 = reinterpret_cast<double**>(take(sizeof(void*) * np));
@@ -995,6 +1178,24 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     if (!sp64.empty()) {
         SIL_CUDA_CHECK(cudaMemcpyAsync(d_sp64, sp64.data(), sizeof(double) * sp64.size(), cudaMemcpyHostToDevice, stream));
         SIL_CUDA_CHECK(cudaMemcpyAsync(d_sp32, sp32.data(), sizeof(float) * sp32.size(), cudaMemcpyHostToDevice, stream));
+    }
+    // Divergence gauge tables, with the problem's slices of r64 / x64 as
+    // probe scratch (both are rewritten before the solve reads them).
+    {
+        int64_t goff = 0;
+        for (int p = 0; p < np; ++p) {
+            if (probs[p].dim == 3 && probs[p].gauge != 0) {
+                double* gd = reinterpret_cast<double*>(gauge_base + gauge_off[p]);
+                float* g32 = reinterpret_cast<float*>(gd + 8 * info[p].nodes);
+                info[p].gauge = 1;
+                info[p].gd64 = gd;
+                info[p].gd32 = g32;
+                sil_status const gs = build_divergence_gauge(probs[p], info[p], gd, g32, r64_base + goff,
+                                                             x64_base + goff, stream);
+                if (gs != SIL_OK) return gs;
+            }
+            goff += info[p].n;
+        }
     }
 
     std::vector<Vecs<T>> vecs(np);
@@ -1397,8 +1598,10 @@ sil_status check_mag3d(sil_mag3d_problem const& q, char const* who, bool need_fi
     if (q.node_mu == nullptr) return fail(SIL_ERR_INVALID, std::string(who) + ": NULL node_mu");
     if (need_fields && (q.rhs == nullptr || q.solution == nullptr))
         return fail(SIL_ERR_INVALID, std::string(who) + ": NULL field pointer");
-    if (!(q.gauge_penalty > 0.0) || !std::isfinite(q.gauge_penalty))
-        return fail(SIL_ERR_INVALID, std::string(who) + ": gauge_penalty must be positive and finite");
+    if (q.gauge != 0 && q.gauge != 1) return fail(SIL_ERR_INVALID, std::string(who) + ": gauge must be 0 or 1");
+    if (!std::isfinite(q.gauge_penalty) || (q.gauge == 0 ? !(q.gauge_penalty > 0.0) : q.gauge_penalty == 0.0))
+        return fail(SIL_ERR_INVALID, std::string(who) + ": gauge_penalty must be finite and positive "
+                                                        "(nonzero for the divergence gauge)");
     double const* c[3] = {q.x, q.y, q.z};
     int64_t const len[3] = {q.nx, q.ny, q.nz};
     for (int a = 0; a < 3; ++a)
@@ -1438,10 +1641,13 @@ sil_status sil_mag3d_apply(sil_stream stream, const sil_mag3d_problem* problem, 
     for (int a2 = 0; a2 < 3; ++a2)
         for (int64_t i = 0; i < len[a2]; ++i) sp.push_back(1.0 / local_spacing(c[a2], len[a2], i));
     size_t const nu_bytes = (nodes * sizeof(double) + 255) / 256 * 256;
+    // divergence gauge: coefficient table (8 per node) and probe scratch (3 + 1 per node)
+    size_t const gauge_bytes = q.gauge ? static_cast<size_t>(nodes) * 12 * sizeof(double) : 0;
     DeviceBuffer buf;
-    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, nu_bytes + sp.size() * sizeof(double), s));
+    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, nu_bytes + gauge_bytes + sp.size() * sizeof(double), s));
     double* nu = static_cast<double*>(buf.ptr);
-    double* dsp = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + nu_bytes);
+    double* gd = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + nu_bytes);
+    double* dsp = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + nu_bytes + gauge_bytes);
     SIL_CUDA_CHECK(cudaMemcpyAsync(dsp, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     ProbInfo pi {};
     pi.dim = 3;
@@ -1459,6 +1665,13 @@ sil_status sil_mag3d_apply(sil_stream stream, const sil_mag3d_problem* problem, 
     for (int a2 = 0; a2 < 3; ++a2) {
         pi.ils64[a2] = dsp + o;
         o += len[a2];
+    }
+    if (q.gauge) {
+        ProblemDesc desc {3, q.nx, q.ny, q.nz, q.gauge_penalty, q.node_mu, nullptr, nullptr, {q.x, q.y, q.z}, 1};
+        sil_status const gs = build_divergence_gauge(desc, pi, gd, nullptr, gd + 8 * nodes, gd + 11 * nodes, s);
+        if (gs != SIL_OK) return gs;
+        pi.gauge = 1;
+        pi.gd64 = gd;
     }
     reciprocal_kernel<<<static_cast<int>((nodes + 255) / 256), 256, 0, s>>>(q.node_mu, nu, nodes);
     mag3d_apply_kernel<<<static_cast<int>((nodes + 255) / 256), 256, 0, s>>>(pi, nu, a, y);
@@ -1480,7 +1693,7 @@ sil_status sil_mag3d_solve_batch(const sil_mag3d_problem* problems, int nproblem
         sil_mag3d_problem const& q = problems[p];
         sil_status const st = check_mag3d(q, "sil_mag3d_solve_batch", true);
         if (st != SIL_OK) return st;
-        descs[p] = {3, q.nx, q.ny, q.nz, q.gauge_penalty, q.node_mu, q.rhs, q.solution, {q.x, q.y, q.z}};
+        descs[p] = {3, q.nx, q.ny, q.nz, q.gauge_penalty, q.node_mu, q.rhs, q.solution, {q.x, q.y, q.z}, q.gauge};
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     std::memset(diag, 0, sizeof(sil_solve_diagnostics) * nproblems);

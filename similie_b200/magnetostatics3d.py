@@ -141,7 +141,10 @@ def synthetic_batch(seed, count=8, n=256, **kw):
     return [synthetic_problem(rng, n, **kw) for _ in range(count)]
 
 
-def _problem_struct(x, y, z, mu, gamma, rhs_dev=None, sol_dev=None):
+GAUGES = {"penalty": 0, "divergence": 1}
+
+
+def _problem_struct(x, y, z, mu, gamma, rhs_dev=None, sol_dev=None, gauge="penalty"):
     p = _native.SilMag3dProblem()
     p.nx, p.ny, p.nz = len(x), len(y), len(z)
     p.x, p.y, p.z = (v.ctypes.data for v in (x, y, z))
@@ -149,6 +152,7 @@ def _problem_struct(x, y, z, mu, gamma, rhs_dev=None, sol_dev=None):
     p.rhs = 0 if rhs_dev is None else rhs_dev.data_ptr()
     p.solution = 0 if sol_dev is None else sol_dev.data_ptr()
     p.gauge_penalty = gamma
+    p.gauge = GAUGES[gauge]
     return p
 
 
@@ -156,11 +160,13 @@ def _f64(v):
     return np.ascontiguousarray(v, dtype=np.float64)
 
 
-def apply(x, y, z, node_mu_dev, a_dev, y_dev, gamma=DEFAULT_GAUGE_PENALTY, stream=None):
-    """y = K a on the GPU (torch CUDA float64 tensors; node_mu flat nodes, a/y flat 3*nodes)."""
+def apply(x, y, z, node_mu_dev, a_dev, y_dev, gamma=DEFAULT_GAUGE_PENALTY, stream=None, gauge="penalty"):
+    """y = K a on the GPU (torch CUDA float64 tensors; node_mu flat nodes, a/y flat 3*nodes).
+    gauge: "penalty" (gamma * star A) or "divergence" (gamma times the
+    codifferential gauge term, the reference's SIMILIE_DIVERGENCE_GAUGE_3D)."""
     import torch
     x, y, z = _f64(x), _f64(y), _f64(z)
-    p = _problem_struct(x, y, z, node_mu_dev, gamma)
+    p = _problem_struct(x, y, z, node_mu_dev, gamma, gauge=gauge)
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
     check(lib().sil_mag3d_apply(s, ctypes.byref(p), ctypes.c_void_p(a_dev.data_ptr()),
                                 ctypes.c_void_p(y_dev.data_ptr())), "mag3d_apply")
@@ -168,7 +174,7 @@ def apply(x, y, z, node_mu_dev, a_dev, y_dev, gamma=DEFAULT_GAUGE_PENALTY, strea
 
 
 def solve_batch(coords, mus, rhss, sols, gammas=None, solver="cg", tol=1e-10, max_iterations=200000,
-                inner_iterations=4000, inner_tolerance=1e-4, stream=None):
+                inner_iterations=4000, inner_tolerance=1e-4, stream=None, gauge="penalty"):
     """minimize_strong_formulation_residual for a batch of 3D linear problems.
 
     coords: list of (x, y, z) host coordinate arrays; mus: torch CUDA float64
@@ -180,7 +186,7 @@ def solve_batch(coords, mus, rhss, sols, gammas=None, solver="cg", tol=1e-10, ma
     keep = [tuple(_f64(v) for v in c) for c in coords]
     probs = (_native.SilMag3dProblem * n)()
     for p in range(n):
-        probs[p] = _problem_struct(*keep[p], mus[p], gammas[p], rhss[p], sols[p])
+        probs[p] = _problem_struct(*keep[p], mus[p], gammas[p], rhss[p], sols[p], gauge=gauge)
     st = _native.SilSolveSettings()
     st.solver = SOLVERS[solver]
     st.max_iterations = max_iterations
