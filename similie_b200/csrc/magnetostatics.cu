@@ -159,7 +159,10 @@ __device__ __forceinline__ T gauge_term(T const* a, T const* gd, int n, int i, i
     return t;
 }
 
-template <class T>
+// G: the divergence-gauge code is compiled in (kernels of batches that hold
+// a divergence-gauge problem); without it the kernels keep the register
+// budget of the penalty operator.
+template <class T, bool G = false>
 __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_t row64)
 {
     // fewer than 2^31 unknowns per problem (checked by the entry points)
@@ -236,10 +239,12 @@ __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_
         if (interior(i - 1, j, k)) res = res - w(-1, 0, 0, 1) * by(-1, 0, 0);
         ha = lx[i] * ly[j] * ilz[k];
     }
-    if (pi.gauge) {
-        T const* gd = gauge_table<T>(pi);
-        T const dn = gauge_div(a, gd, node, i, j, k, nx, ny);
-        return res + static_cast<T>(pi.gamma) * gauge_term(a, gd, node, i, j, k, nx, ny, c, dn);
+    if constexpr (G) {
+        if (pi.gauge) {
+            T const* gd = gauge_table<T>(pi);
+            T const dn = gauge_div(a, gd, node, i, j, k, nx, ny);
+            return res + static_cast<T>(pi.gamma) * gauge_term(a, gd, node, i, j, k, nx, ny, c, dn);
+        }
     }
     return res + static_cast<T>(pi.gamma) * ha * a[row];
 }
@@ -247,7 +252,7 @@ __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_
 // All three rows of a node at once (the curl moments shared between the
 // components are formed once); each component sums its terms in the order of
 // mag3d_apply_row, so the values are the same.
-template <class T>
+template <class T, bool G = false>
 __device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, int node, T* out)
 {
     int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
@@ -308,11 +313,16 @@ __device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, in
     T const g = static_cast<T>(pi.gamma);
     // gauge term per component: penalty g (d_a d_b / d_c) A_c, or the divergence gauge
     T gt[3];
-    if (pi.gauge) {
-        T const* gd = gauge_table<T>(pi);
-        T const dn = gauge_div(a, gd, node, i, j, k, nx, ny);
-        for (int c = 0; c < 3; ++c) gt[c] = g * gauge_term(a, gd, node, i, j, k, nx, ny, c, dn);
-    } else {
+    bool gauge_done = false;
+    if constexpr (G) {
+        if (pi.gauge) {
+            T const* gd = gauge_table<T>(pi);
+            T const dn = gauge_div(a, gd, node, i, j, k, nx, ny);
+            for (int c = 0; c < 3; ++c) gt[c] = g * gauge_term(a, gd, node, i, j, k, nx, ny, c, dn);
+            gauge_done = true;
+        }
+    }
+    if (!gauge_done) {
         gt[0] = g * (ly[j] * lz[k] * ilx[i]) * a[row0];
         gt[1] = g * (lx[i] * lz[k] * ily[j]) * a[row0 + 1];
         gt[2] = g * (lx[i] * ly[j] * ilz[k]) * a[row0 + 2];
@@ -343,11 +353,11 @@ __device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, in
     }
 }
 
-template <class T>
+template <class T, bool G = false>
 __device__ __forceinline__ T mag_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_t row)
 {
     if (pi.dim == 2) return mag_apply_node(a, nu, pi.nx, pi.ny, row);
-    return mag3d_apply_row(a, nu, pi, row);
+    return mag3d_apply_row<T, G>(a, nu, pi, row);
 }
 
 // Diagonal of the operator at a row (Jacobi preconditioner), from mu directly.
@@ -543,7 +553,7 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(Item const* items, Pr
 }
 
 // q = A p and the partial p.q; the problem's last CTA forms alpha = rz / (p.q).
-template <class T>
+template <class T, bool G = false>
 __global__ void __launch_bounds__(kThreads) cg_apply_kernel(Item const* items, ProbInfo const* info, Vecs<T> const* vecs,
                                                             Scalars* sc, double* part)
 {
@@ -557,7 +567,7 @@ __global__ void __launch_bounds__(kThreads) cg_apply_kernel(Item const* items, P
     if (pi.dim == 3) {
         for (int64_t node = it.begin / 3 + threadIdx.x; node < it.end / 3; node += kThreads) {
             T q[3];
-            mag3d_apply_node(v.p, v.nu, pi, static_cast<int>(node), q);
+            mag3d_apply_node<T, G>(v.p, v.nu, pi, static_cast<int>(node), q);
             for (int c = 0; c < 3; ++c) {
                 v.q[3 * node + c] = q[c];
                 pq += static_cast<double>(v.p[3 * node + c]) * static_cast<double>(q[c]);
@@ -565,7 +575,7 @@ __global__ void __launch_bounds__(kThreads) cg_apply_kernel(Item const* items, P
         }
     } else {
         for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-            T const q = mag_apply_row(v.p, v.nu, pi, row);
+            T const q = mag_apply_row<T, G>(v.p, v.nu, pi, row);
             v.q[row] = q;
             pq += static_cast<double>(v.p[row]) * static_cast<double>(q);
         }
@@ -847,6 +857,7 @@ __global__ void fcg_active_kernel(Scalars const* sc, int np, int* active)
 }
 
 // r64 = b - A x64 and its norm (outer residual, FP64); marks outer convergence.
+template <bool G = false>
 __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items, ProbInfo const* info,
                                                               double const* const* nu64, double const* const* rhs,
                                                               double* const* x64, double* const* r64, Scalars* sc,
@@ -861,7 +872,7 @@ __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items,
     if (pi.dim == 3) {
         for (int64_t node = it.begin / 3 + threadIdx.x; node < it.end / 3; node += kThreads) {
             double ax[3];
-            mag3d_apply_node(x64[it.prob], nu64[it.prob], pi, static_cast<int>(node), ax);
+            mag3d_apply_node<double, G>(x64[it.prob], nu64[it.prob], pi, static_cast<int>(node), ax);
             for (int c = 0; c < 3; ++c) {
                 double const r = rhs[it.prob][3 * node + c] - ax[c];
                 r64[it.prob][3 * node + c] = r;
@@ -870,7 +881,7 @@ __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items,
         }
     } else {
         for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-            double const ax = mag_apply_row(x64[it.prob], nu64[it.prob], pi, row);
+            double const ax = mag_apply_row<double, G>(x64[it.prob], nu64[it.prob], pi, row);
             double const r = rhs[it.prob][row] - ax;
             r64[it.prob][row] = r;
             rr += r * r;
@@ -1116,6 +1127,11 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     size_t bytes = (nvec + nhist) * vec_bytes + ndouble_vecs * d_bytes;
     // divergence-gauge coefficient tables (8 doubles + 8 floats per node)
     std::vector<size_t> gauge_off(np, 0);
+    bool const any_gauge = std::any_of(probs.begin(), probs.end(), [](ProblemDesc const& q) {
+        return q.dim == 3 && q.gauge != 0;
+    });
+    // the divergence-gauge variants only where a problem needs them
+    auto const residual64 = any_gauge ? residual64_kernel<true> : residual64_kernel<false>;
     size_t gauge_bytes = 0;
     for (int p = 0; p < np; ++p) {
         if (probs[p].dim != 3 || probs[p].gauge == 0) continue;
@@ -1255,7 +1271,8 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
         cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         for (int c = 0; c < chunk && err == cudaSuccess; ++c) {
-            cg_apply_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a);
+            if (any_gauge) cg_apply_kernel<T, true><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a);
+            else cg_apply_kernel<T, false><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a);
             cg_update_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_b, part_c);
             cg_direction_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc);
         }
@@ -1362,7 +1379,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
             }
             int tot = 0;
             while (lst == SIL_OK && tot < max_iter) {
-                residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc,
+                residual64<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc,
                                                                    part_a, tol * tol, ltol * ltol, 1);
                 SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
                 SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
@@ -1408,7 +1425,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         if (learned != nullptr && st == SIL_OK) st = learned_stage(learned, &total, &refinements);
     }
     while (st == SIL_OK && total < max_iter) {
-        residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc, part_a,
+        residual64<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc, part_a,
                                                            tol * tol, inner_tol * inner_tol, 1);
         SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
         SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
@@ -1437,7 +1454,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         hs2[p].counter_a = hs2[p].counter_b = hs2[p].counter_c = 0;
     }
     SIL_CUDA_CHECK(cudaMemcpyAsync(d_sc, hs2.data(), sizeof(Scalars) * np, cudaMemcpyHostToDevice, stream));
-    residual64_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_sol, d_scratch, d_sc, part_a,
+    residual64<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_sol, d_scratch, d_sc, part_a,
                                                        tol * tol, 0.0, 0);
     SIL_CUDA_CHECK(cudaGetLastError());
     SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
@@ -1616,7 +1633,7 @@ __global__ void mag3d_apply_kernel(ProbInfo pi, double const* nu, double const* 
     int64_t const node = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (node >= pi.nodes) return;
     double out[3];
-    mag3d_apply_node(a, nu, pi, static_cast<int>(node), out);
+    mag3d_apply_node<double, true>(a, nu, pi, static_cast<int>(node), out);
     for (int c = 0; c < 3; ++c) y[3 * node + c] = out[c];
 }
 
