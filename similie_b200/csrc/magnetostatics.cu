@@ -1100,8 +1100,9 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         pi.gamma = q.gamma;
         pi.first_item = static_cast<int>(items.size());
         int idx = 0;
-        // 3D items hold whole nodes (3 rows each) so the apply can work per node
-        int64_t const step = q.dim == 3 ? (kItemNodes / 3) * 3 : kItemNodes;
+        // 3D items: whole nodes (3 rows each), four times the 2D item, so
+        // the per-CTA prologue is amortised over more of the costlier 3D rows
+        int64_t const step = q.dim == 3 ? (4 * kItemNodes / 3) * 3 : kItemNodes;
         for (int64_t b = 0; b < pi.n; b += step, ++idx) items.push_back({p, idx, b, std::min(pi.n, b + step)});
         pi.nitems = idx;
         total_rows += pi.n;
