@@ -505,12 +505,6 @@ unsigned grid_for(int64_t n)
     return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(blocks, 4 * sms)));
 }
 
-struct DeviceBuffer
-{
-    void* ptr = nullptr;
-    ~DeviceBuffer() { cudaFree(ptr); }
-};
-
 }  // namespace
 }  // namespace sil
 
