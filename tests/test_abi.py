@@ -78,6 +78,59 @@ def test_mag3d_arguments_checked_on_host():
     assert L.sil_mag3d_solve_batch(None, 0, None, None, None) == 1
 
 
+def test_gauge_and_nonlinear_arguments_checked_on_host():
+    import numpy as np
+    L = sil.lib()
+    # 3D gauge kind and sign rules
+    x = np.linspace(0.0, 1.0, 4)
+    p = _native.SilMag3dProblem()
+    p.nx = p.ny = p.nz = 4
+    p.x = p.y = p.z = x.ctypes.data
+    p.node_mu = p.rhs = p.solution = 256
+    p.gauge_penalty = 20.0
+    p.gauge = 2
+    assert L.sil_mag3d_apply(None, ctypes.byref(p), 256, 256) == 1
+    assert b"gauge must be 0 or 1" in L.sil_last_error()
+    p.gauge = 0
+    p.gauge_penalty = -20.0                # a negative penalty: only the divergence gauge takes a sign
+    assert L.sil_mag3d_apply(None, ctypes.byref(p), 256, 256) == 1
+    p.gauge = 1
+    p.gauge_penalty = 0.0
+    assert L.sil_mag3d_apply(None, ctypes.byref(p), 256, 256) == 1
+    assert b"nonzero" in L.sil_last_error()
+    # nonlinear problem: geometry, material arrays and the B-H curve are checked before any launch
+    b = np.array([0.0, 1.0, 2.0])
+    h = np.array([0.0, 1.0, 3.0])
+    q = _native.SilMag2dNlProblem()
+    q.nx, q.ny = 2, 8
+    q.node_mu = q.node_ferro = 256
+    q.curve = _native.SilBHCurve(3, b.ctypes.data, h.ctypes.data)
+    assert L.sil_mag2d_nl_apply(None, ctypes.byref(q), 256, 256) == 1
+    assert b"3x3" in L.sil_last_error()
+    q.nx = 8
+    q.node_ferro = None
+    assert L.sil_mag2d_nl_apply(None, ctypes.byref(q), 256, 256) == 1
+    assert b"NULL" in L.sil_last_error()
+    q.node_ferro = 256
+    bad = np.array([0.0, 1.0, 1.0])
+    q.curve = _native.SilBHCurve(3, bad.ctypes.data, h.ctypes.data)
+    assert L.sil_mag2d_nl_apply_jacobian(None, ctypes.byref(q), 256, 256, 256) == 1
+    assert b"increase" in L.sil_last_error()
+    q.curve = _native.SilBHCurve(65, b.ctypes.data, h.ctypes.data)
+    assert L.sil_mag2d_nl_apply(None, ctypes.byref(q), 256, 256) == 1
+    assert b"64" in L.sil_last_error()
+    neg = np.array([-1.0, 1.0, 2.0])
+    q.curve = _native.SilBHCurve(3, neg.ctypes.data, h.ctypes.data)
+    assert L.sil_mag2d_nl_apply(None, ctypes.byref(q), 256, 256) == 1
+    q.curve = _native.SilBHCurve(3, b.ctypes.data, h.ctypes.data)
+    st = _native.SilSolveSettings()
+    diag = (_native.SilSolveDiagnostics * 1)()
+    q.rhs = None
+    assert L.sil_mag2d_nl_solve_batch(ctypes.byref(q), 1, ctypes.byref(st), diag, None) == 1
+    assert b"NULL" in L.sil_last_error()
+    assert L.sil_mag2d_nl_solve_batch(None, 0, None, None, None) == 1
+
+
 def test_rank_and_component_checks_on_host():
     L = sil.lib()
     fi = _native.SilField()
