@@ -196,7 +196,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--extras", action="store_true", help="also time the unfused chain, FP32 and the 512^2 0-form")
     ap.add_argument("--workload", default="laplacian",
-                    choices=["laplacian", "solve", "mag3d", "precond", "hodge3d", "nonlinear"])
+                    choices=["laplacian", "solve", "mag3d", "precond", "hodge3d", "nonlinear", "nonlinear3d"])
     ap.add_argument("--n2d", type=int, default=257, help="nonlinear: nodes per axis")
     ap.add_argument("--chunk", type=int, default=64, help="solve: problems per solver call (at most 64 for learned)")
     ap.add_argument("--concurrent", type=int, default=1,
@@ -210,6 +210,7 @@ def main():
                     help="solve / mag3d: also time the oracle's FP64 CPU CG on this many problems of the batch")
     ap.add_argument("--count", type=int, default=None, help="solve / mag3d: problems per batch (64 / 8)")
     ap.add_argument("--n3d", type=int, default=256, help="mag3d: nodes per axis")
+    ap.add_argument("--nl3d", type=int, default=25, help="nonlinear3d: nodes per axis")
     ap.add_argument("--kernel-only", action="store_true",
                     help="warm-up + timed launches of the fused kernel only (profiling runs): no e2e, extras or CPU leg")
     args = ap.parse_args()
@@ -224,6 +225,9 @@ def main():
         return
     if args.workload == "nonlinear":
         run_nonlinear_workload(args)
+        return
+    if args.workload == "nonlinear3d":
+        run_nonlinear3d_workload(args)
         return
     if args.workload == "precond":
         run_precond_workload(args)
@@ -660,6 +664,57 @@ def run_nonlinear_workload(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded coils; saturating permeability-1000 rectangles, 64-sample B-H curve)",
             "config": {"workload": f"{count} x {n}^2 nodes, tol 1e-10, at most 30 Newton steps"},
+            "newton_steps": steps, "ms_per_newton_step": sec * 1e3 / max(steps, 1),
+            "cg_iterations": sum(x.iterations for x in d), "converged": sum(x.converged for x in d),
+            "final_relative_residuals": [x.final_relative_residual for x in d],
+            "cpu_baseline": cpu, "clocks": clocks.summary()}
+    print(json.dumps(line))
+
+
+def run_nonlinear3d_workload(args):
+    """Batch of seeded 3D loop-current problems with a box core of the
+    saturating material: Newton (at most 30 steps) + line search, each step a
+    Jacobi-CG solve of the Jacobian to 1e-10.  Beside it, the oracle's solve
+    of the batch's first problem on all host cores (same algorithm)."""
+    import torch
+    import similie_b200.magnetostatics3d as m3
+    torch.cuda.set_device(0)
+    n = args.nl3d
+    count = args.count or 8
+    cases = [m3.nonlinear_problem(n, s) for s in range(count)]
+    coords = [(c[0].x, c[0].y, c[0].z) for c in cases]
+    mus = [torch.from_numpy(c[1]).cuda() for c in cases]
+    fes = [torch.from_numpy(c[2]).cuda() for c in cases]
+    rhss = [torch.from_numpy(c[0].rhs()).cuda() for c in cases]
+    curves = [(c[3], c[4]) for c in cases]
+    with ClockSampler(0) as clocks:
+        sols = [torch.zeros_like(r) for r in rhss]
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d = m3.nl_solve_batch(coords, mus, fes, curves, rhss, sols, tol=1e-10, max_iterations=args.max_iterations)
+        e1.record()
+        torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    steps = sum(x.refinements for x in d)
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle as O
+        p, mu, fe, b, h = cases[0]
+        t0 = time.perf_counter()
+        xo, it, st, rel = O.mag3d_nl_solve(p.x, p.y, p.z, mu, fe, p.gamma, b, h, p.rhs(), tol=1e-10,
+                                           max_iter=args.max_iterations)
+        tc = time.perf_counter() - t0
+        cpu = {"value": 1.0 / tc, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"the batch's first problem ({n}^3, {st} Newton steps, {it} CG iterations) in {tc:.2f} s",
+               "gpu_solution_rel_diff": float(np.linalg.norm(sols[0].cpu().numpy() - xo) / np.linalg.norm(xo))}
+    line = {"metric": f"nonlinear 3D magnetostatics (Newton + line search), batch of {count} problems {n}^3",
+            "value": count / sec, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded current loops; saturating permeability-1000 box core, 64-sample B-H curve)",
+            "config": {"workload": f"{count} x {n}^3 nodes x 3 components, gamma 20, tol 1e-10, "
+                                   "at most 30 Newton steps"},
             "newton_steps": steps, "ms_per_newton_step": sec * 1e3 / max(steps, 1),
             "cg_iterations": sum(x.iterations for x in d), "converged": sum(x.converged for x in d),
             "final_relative_residuals": [x.final_relative_residual for x in d],

@@ -316,6 +316,40 @@ sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int np
                                     const sil_solve_settings* settings, sil_solve_diagnostics* diag,
                                     sil_stream stream);
 
+/* 3D magnetostatics with the nonlinear material: the 3D curl-curl operator
+ * with the penalty gauge (sil_mag3d_problem, gauge 0) whose sampled nodes
+ * follow the material law above with q = |B|^2 over the three curl moments;
+ * the Jacobian applies each sampled node's 3x3 Hessian of the Hamiltonian.
+ * Replaces: MagnetostaticsOperator3D with MaterialMagnetostaticsHamiltonian,
+ *   magnetostatics_onelab.hpp:5110-5126 (nonlinear dispatch), 2241-2396
+ *   (operator, dpotential_dt of the equations), 2924-3110 (apply_jacobian). */
+typedef struct sil_mag3d_nl_problem {
+    int64_t nx, ny, nz;       /* nodes per axis (>= 3) */
+    const double* x;          /* HOST, nx strictly increasing node coordinates */
+    const double* y;          /* HOST, ny */
+    const double* z;          /* HOST, nz */
+    const double* node_mu;    /* device, nx*ny*nz */
+    const double* node_ferro; /* device, nx*ny*nz: ferromagnetic fraction per node */
+    sil_bh_curve curve;
+    const double* rhs;        /* device, 3*nx*ny*nz */
+    double* solution;         /* device, 3*nx*ny*nz: initial guess on entry, result on exit */
+    double gauge_penalty;     /* gamma > 0 */
+} sil_mag3d_nl_problem;
+
+/* y = the 3D nonlinear operator applied to a (3*nx*ny*nz doubles, device). */
+sil_status sil_mag3d_nl_apply(sil_stream stream, const sil_mag3d_nl_problem* problem, const double* a, double* y);
+
+/* y = J(state) x for the 3D nonlinear operator. */
+sil_status sil_mag3d_nl_apply_jacobian(sil_stream stream, const sil_mag3d_nl_problem* problem, const double* state,
+                                       const double* x, double* y);
+
+/* Newton solve of every 3D problem of the batch, the scheme of
+ * sil_mag2d_nl_solve_batch (Jacobi-CG on the Jacobian, halving line
+ * search).  Synchronous. */
+sil_status sil_mag3d_nl_solve_batch(const sil_mag3d_nl_problem* problems, int nproblems,
+                                    const sil_solve_settings* settings, sil_solve_diagnostics* diag,
+                                    sil_stream stream);
+
 /* ---------------------------------------------------------------------- */
 /* Learned multilevel convolutional preconditioner of the 2D solve.        */
 /* M(r) = Jacobi step, then a U-Net correction computed at half resolution  */

@@ -70,6 +70,12 @@ def lib():
         _lib.silo_mag3d_diagonal.argtypes = [i64, i64, i64, dp, dp, dp, dp, ctypes.c_double, dp]
         _lib.silo_mag3d_cg.argtypes = [i64, i64, i64, dp, dp, dp, dp, ctypes.c_double, dp, dp, ctypes.c_double,
                                        ctypes.c_int, dp]
+        d = ctypes.c_double
+        _lib.silo_mag3d_nl_apply.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp]
+        _lib.silo_mag3d_nl_jacobian_apply.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp, dp]
+        _lib.silo_mag3d_nl_jacobian_diagonal.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp]
+        _lib.silo_mag3d_nl_solve.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp, d, ci,
+                                             ctypes.POINTER(ci), dp]
     return _lib
 
 
@@ -348,3 +354,50 @@ def mag3d_cg(x, y, z, node_mu, gamma, rhs, tol=1e-10, max_iter=100000):
     it = lib().silo_mag3d_cg(len(x), len(y), len(z), _ptr(x), _ptr(y), _ptr(z), _ptr(mu), gamma, _ptr(b), _ptr(sol),
                              tol, max_iter, ctypes.byref(rel))
     return sol, it, rel.value
+
+
+# ----------------------------------------------------------------- magnetostatics 3D, nonlinear material
+
+def _nl3_args(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h):
+    x, y, z, mu, fe, b, h = (_f64(v) for v in (x, y, z, node_mu, node_ferro, curve_b, curve_h))
+    keep = (x, y, z, mu, fe, b, h)
+    args = [len(x), len(y), len(z), _ptr(x), _ptr(y), _ptr(z), _ptr(mu), _ptr(fe), float(gamma), len(b), _ptr(b),
+            _ptr(h)]
+    return keep, args
+
+
+def mag3d_nl_apply(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h, a):
+    keep, args = _nl3_args(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h)
+    a = _f64(a)
+    out = np.zeros_like(a)
+    lib().silo_mag3d_nl_apply(*args, _ptr(a), _ptr(out))
+    return out
+
+
+def mag3d_nl_jacobian_apply(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h, state, v):
+    keep, args = _nl3_args(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h)
+    st, v = _f64(state), _f64(v)
+    out = np.zeros_like(v)
+    lib().silo_mag3d_nl_jacobian_apply(*args, _ptr(st), _ptr(v), _ptr(out))
+    return out
+
+
+def mag3d_nl_jacobian_diagonal(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h, state):
+    keep, args = _nl3_args(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h)
+    st = _f64(state)
+    out = np.zeros_like(st)
+    lib().silo_mag3d_nl_jacobian_diagonal(*args, _ptr(st), _ptr(out))
+    return out
+
+
+def mag3d_nl_solve(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h, rhs, x0=None, tol=1e-10,
+                   max_iter=100000):
+    """Newton + line search on the 3D operator; returns (x, cg_iterations, newton_steps, final relative residual)."""
+    keep, args = _nl3_args(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h)
+    rhs = _f64(rhs)
+    sol = np.zeros_like(rhs) if x0 is None else np.array(x0, dtype=np.float64)
+    steps = ctypes.c_int(0)
+    rel = ctypes.c_double(0.0)
+    it = lib().silo_mag3d_nl_solve(*args, _ptr(rhs), _ptr(sol), tol, max_iter, ctypes.byref(steps),
+                                   ctypes.byref(rel))
+    return sol, it, steps.value, rel.value

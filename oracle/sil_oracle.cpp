@@ -1781,20 +1781,21 @@ void silo_mag2d_nl_jacobian_diagonal(int64_t nx, int64_t ny, const double* node_
     nl_jacobian_diagonal(nx, ny, law, state, diag);
 }
 
+namespace {
+
+// Newton with a halving line search on F(x) = rhs; every step solves
+// J(x) d = r by Jacobi-CG from d = 0 to the relative tolerance.
 // Ref: src/similie/solvers/minimize_strong_formulation_residual.hpp:1383-1569
 // (nonlinear branch: at most 30 Newton steps; each solves the linearised
 // system to the relative tolerance, then a line search of at most 8 steps
 // halving alpha from 1 that stops at the first candidate below the current
 // residual, else takes the best candidate seen).
-int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
-                        const double* b, const double* h, const double* rhs, double* x, double tol, int max_iter,
-                        int* newton_steps, double* final_rel)
+template <class Apply, class Jacobian, class Diagonal>
+int newton_solve(int64_t N, Apply const& apply, Jacobian const& jacobian, Diagonal const& diagonal,
+                 const double* rhs, double* x, double tol, int max_iter, int* newton_steps, double* final_rel)
 {
-    BHCurve const c(n, b, h);
-    NodeLaw const law {node_mu, node_ferro, &c};
-    int64_t const N = nx * ny;
     std::vector<double> fa(N), r(N), d(N), cand(N), cand_f(N), cand_r(N), dinv(N), cr(N), z(N), p(N), q(N);
-    nl_apply(nx, ny, law, x, fa.data());
+    apply(x, fa.data());
     for (int64_t i = 0; i < N; ++i) r[i] = rhs[i] - fa[i];
     double const r0 = nrm2(N, r.data());
     int total = 0, steps = 0;
@@ -1808,7 +1809,7 @@ int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const dou
         if (res / r0 <= tol) break;
         ++steps;
         // Jacobi-CG on J(x) d = r from d = 0
-        nl_jacobian_diagonal(nx, ny, law, x, dinv.data());
+        diagonal(x, dinv.data());
         for (int64_t i = 0; i < N; ++i) dinv[i] = 1.0 / dinv[i];
         std::fill(d.begin(), d.end(), 0.0);
         cr = r;
@@ -1819,7 +1820,7 @@ int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const dou
         double rn = bn;
         int k = 0;
         while (k < max_iter && rn > tol * bn) {
-            nl_jacobian_apply(nx, ny, law, x, p.data(), q.data());
+            jacobian(x, p.data(), q.data());
             double const alpha = rz / dotp(N, p.data(), q.data());
             for (int64_t i = 0; i < N; ++i) {
                 d[i] += alpha * p[i];
@@ -1840,7 +1841,7 @@ int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const dou
         double alpha = 1.0, best_alpha = 0.0, best = std::numeric_limits<double>::infinity();
         auto candidate = [&](double al) {
             for (int64_t i = 0; i < N; ++i) cand[i] = x[i] + al * d[i];
-            nl_apply(nx, ny, law, cand.data(), cand_f.data());
+            apply(cand.data(), cand_f.data());
             for (int64_t i = 0; i < N; ++i) cand_r[i] = rhs[i] - cand_f[i];
             return nrm2(N, cand_r.data());
         };
@@ -1863,4 +1864,206 @@ int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const dou
     *newton_steps = steps;
     *final_rel = nrm2(N, r.data()) / r0;
     return total;
+}
+
+// 3D material law at a sampled node with moments B = (B_x, B_y, B_z):
+// the same Hamiltonian as NodeLaw with q = |B|^2 over three components.
+struct NodeLaw3
+{
+    const double* mu;
+    const double* ferro;
+    BHCurve const* curve;
+    void field(int64_t s, const double* B, double* H) const
+    {
+        if (ferro[s] > 0.5) {
+            double const q = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+            double const F = curve->f(q), dF = curve->df(q);
+            for (int c = 0; c < 3; ++c) H[c] = B[c] * F + q * B[c] * dF;
+        } else {
+            for (int c = 0; c < 3; ++c) H[c] = B[c] / mu[s];
+        }
+    }
+    // J[3 * r + c] = d2H / dB_r dB_c
+    void jacobian(int64_t s, const double* B, double* J) const
+    {
+        if (ferro[s] > 0.5) {
+            double const q = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+            double const F = curve->f(q), dF = curve->df(q), d2F = curve->d2f(q);
+            double const base = F + q * dF;
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c)
+                    J[3 * r + c] = (r == c ? base : 0.0) + 4.0 * B[r] * B[c] * dF + 2.0 * q * B[r] * B[c] * d2F;
+        } else {
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) J[3 * r + c] = r == c ? 1.0 / mu[s] : 0.0;
+        }
+    }
+};
+
+struct Mag3Nl
+{
+    Grid3 g;
+    Transposed t;
+    NodeLaw3 law;
+    double gamma;
+
+    void moments(int64_t s, const double* a, double* B) const
+    {
+        for (int m = 0; m < 3; ++m) B[m] = moment_value(g, s, m, a);
+    }
+    bool interior_node(int64_t s) const
+    {
+        return g.interior(s % g.nx, (s / g.nx) % g.ny, s / (g.nx * g.ny));
+    }
+    // out[row] = sum over the row's transposed moment entries (s, m, coeff)
+    // of coeff * hodge_b(s, m) * v[3 s + m] + gamma * hodge_a * a[row];
+    // identity rows on the boundary.
+    void gather(const double* v, const double* a, double* out) const
+    {
+        int64_t const nn = g.nx * g.ny * g.nz;
+#pragma omp parallel for schedule(static)
+        for (int64_t node = 0; node < nn; ++node) {
+            int64_t const i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
+            for (int c = 0; c < 3; ++c) {
+                int64_t const row = 3 * node + c;
+                if (!g.interior(i, j, k)) {
+                    out[row] = a[row];
+                    continue;
+                }
+                double residual = 0.0;
+                for (auto const& [s, m, coeff] : t.rows[row]) {
+                    int64_t const si = s % g.nx, sj = (s / g.nx) % g.ny, sk = s / (g.nx * g.ny);
+                    residual += coeff * hodge_b(g, si, sj, sk, m) * v[3 * s + m];
+                }
+                out[row] = residual + gamma * hodge_a(g, i, j, k, c) * a[row];
+            }
+        }
+    }
+    // Nonlinear operator: the linear 3D operator with B_m / mu replaced by
+    // the material field H_m(B) at the sampled nodes.
+    // Ref: onelab_interface/magnetostatics_onelab.hpp:2241-2396 (3D apply with
+    // dpotential_dt of the equations), 957-1011 (material Hamiltonian)
+    void apply(const double* a, double* y) const
+    {
+        int64_t const nn = g.nx * g.ny * g.nz;
+        std::vector<double> H(3 * nn, 0.0);
+#pragma omp parallel for schedule(static)
+        for (int64_t s = 0; s < nn; ++s) {
+            if (!interior_node(s)) continue;
+            double B[3];
+            moments(s, a, B);
+            law.field(s, B, &H[3 * s]);
+        }
+        gather(H.data(), a, y);
+    }
+    // Jacobian at st applied to x: each sampled node contributes its 3x3
+    // Hessian times the moments of x.
+    // Ref: onelab_interface/magnetostatics_onelab.hpp:2924-3110 (apply_jacobian, 3D)
+    void jacobian(const double* st, const double* x, double* y) const
+    {
+        int64_t const nn = g.nx * g.ny * g.nz;
+        std::vector<double> G(3 * nn, 0.0);
+#pragma omp parallel for schedule(static)
+        for (int64_t s = 0; s < nn; ++s) {
+            if (!interior_node(s)) continue;
+            double B[3], D[3], J[9];
+            moments(s, st, B);
+            moments(s, x, D);
+            law.jacobian(s, B, J);
+            for (int m = 0; m < 3; ++m) G[3 * s + m] = J[3 * m] * D[0] + J[3 * m + 1] * D[1] + J[3 * m + 2] * D[2];
+        }
+        gather(G.data(), x, y);
+    }
+    // Diagonal of the Jacobian at st: for each entry (s, m, coeff) of the
+    // row, coeff * hodge_b(s, m) * sum_c J_mc(s) * (coefficient of the row in
+    // B_c(s)); plus the gauge term; 1 on boundary rows.
+    void diagonal(const double* st, double* diag) const
+    {
+        int64_t const nn = g.nx * g.ny * g.nz;
+#pragma omp parallel for schedule(static)
+        for (int64_t node = 0; node < nn; ++node) {
+            int64_t const i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
+            for (int c = 0; c < 3; ++c) {
+                int64_t const row = 3 * node + c;
+                if (!g.interior(i, j, k)) {
+                    diag[row] = 1.0;
+                    continue;
+                }
+                double d = 0.0;
+                for (auto const& [s, m, coeff] : t.rows[row]) {
+                    int64_t const si = s % g.nx, sj = (s / g.nx) % g.ny, sk = s / (g.nx * g.ny);
+                    double B[3], J[9];
+                    moments(s, st, B);
+                    law.jacobian(s, B, J);
+                    double acc = 0.0;
+                    for (int cc = 0; cc < 3; ++cc)
+                        for (auto const& term : moment_stencil(g, si, sj, sk, cc))
+                            if (term.node == node && term.comp == c) acc += J[3 * m + cc] * term.coeff;
+                    d += coeff * hodge_b(g, si, sj, sk, m) * acc;
+                }
+                diag[row] = d + gamma * hodge_a(g, i, j, k, c);
+            }
+        }
+    }
+};
+
+} // namespace
+
+int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
+                        const double* b, const double* h, const double* rhs, double* x, double tol, int max_iter,
+                        int* newton_steps, double* final_rel)
+{
+    BHCurve const c(n, b, h);
+    NodeLaw const law {node_mu, node_ferro, &c};
+    return newton_solve(
+            nx * ny, [&](const double* v, double* out) { nl_apply(nx, ny, law, v, out); },
+            [&](const double* st, const double* v, double* out) { nl_jacobian_apply(nx, ny, law, st, v, out); },
+            [&](const double* st, double* out) { nl_jacobian_diagonal(nx, ny, law, st, out); }, rhs, x, tol, max_iter,
+            newton_steps, final_rel);
+}
+
+void silo_mag3d_nl_apply(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                         const double* node_mu, const double* node_ferro, double gamma, int n, const double* b,
+                         const double* h, const double* a, double* out)
+{
+    BHCurve const c(n, b, h);
+    Grid3 const g {nx, ny, nz, x, y, z};
+    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    op.apply(a, out);
+}
+
+void silo_mag3d_nl_jacobian_apply(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y,
+                                  const double* z, const double* node_mu, const double* node_ferro, double gamma,
+                                  int n, const double* b, const double* h, const double* state, const double* v,
+                                  double* out)
+{
+    BHCurve const c(n, b, h);
+    Grid3 const g {nx, ny, nz, x, y, z};
+    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    op.jacobian(state, v, out);
+}
+
+void silo_mag3d_nl_jacobian_diagonal(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y,
+                                     const double* z, const double* node_mu, const double* node_ferro, double gamma,
+                                     int n, const double* b, const double* h, const double* state, double* diag)
+{
+    BHCurve const c(n, b, h);
+    Grid3 const g {nx, ny, nz, x, y, z};
+    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    op.diagonal(state, diag);
+}
+
+int silo_mag3d_nl_solve(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                        const double* node_mu, const double* node_ferro, double gamma, int n, const double* b,
+                        const double* h, const double* rhs, double* sol, double tol, int max_iter, int* newton_steps,
+                        double* final_rel)
+{
+    BHCurve const c(n, b, h);
+    Grid3 const g {nx, ny, nz, x, y, z};
+    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    return newton_solve(
+            3 * nx * ny * nz, [&](const double* v, double* out) { op.apply(v, out); },
+            [&](const double* st, const double* v, double* out) { op.jacobian(st, v, out); },
+            [&](const double* st, double* out) { op.diagonal(st, out); }, rhs, sol, tol, max_iter, newton_steps,
+            final_rel);
 }

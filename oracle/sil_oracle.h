@@ -145,6 +145,26 @@ int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const dou
                         const double* b, const double* h, const double* rhs, double* x, double tol, int max_iter,
                         int* newton_steps, double* final_rel);
 
+/* ------------------------------------------------------------------ */
+/* 3D nonlinear magnetostatics: the 3D curl-curl + penalty-gauge operator */
+/* with the material law of the 2D problem at the sampled nodes.         */
+
+void silo_mag3d_nl_apply(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                         const double* node_mu, const double* node_ferro, double gamma, int n, const double* b,
+                         const double* h, const double* a, double* out);
+void silo_mag3d_nl_jacobian_apply(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y,
+                                  const double* z, const double* node_mu, const double* node_ferro, double gamma,
+                                  int n, const double* b, const double* h, const double* state, const double* v,
+                                  double* out);
+void silo_mag3d_nl_jacobian_diagonal(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y,
+                                     const double* z, const double* node_mu, const double* node_ferro, double gamma,
+                                     int n, const double* b, const double* h, const double* state, double* diag);
+/* Newton as silo_mag2d_nl_solve, on the 3D operator (3 * nx*ny*nz unknowns). */
+int silo_mag3d_nl_solve(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                        const double* node_mu, const double* node_ferro, double gamma, int n, const double* b,
+                        const double* h, const double* rhs, double* sol, double tol, int max_iter, int* newton_steps,
+                        double* final_rel);
+
 /* Threads OpenMP uses (for reporting). */
 int silo_num_threads(void);
 

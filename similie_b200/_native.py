@@ -79,6 +79,23 @@ class SilMag3dProblem(ctypes.Structure):
     ]
 
 
+class SilMag3dNlProblem(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int64),
+        ("ny", ctypes.c_int64),
+        ("nz", ctypes.c_int64),
+        ("x", ctypes.c_void_p),
+        ("y", ctypes.c_void_p),
+        ("z", ctypes.c_void_p),
+        ("node_mu", ctypes.c_void_p),
+        ("node_ferro", ctypes.c_void_p),
+        ("curve", SilBHCurve),
+        ("rhs", ctypes.c_void_p),
+        ("solution", ctypes.c_void_p),
+        ("gauge_penalty", ctypes.c_double),
+    ]
+
+
 class SilPrecondSample(ctypes.Structure):
     _fields_ = [
         ("nx", ctypes.c_int32),
@@ -174,6 +191,11 @@ SIGNATURES = [
     ("sil_mag3d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag3dProblem), ctypes.c_int,
                                              ctypes.POINTER(SilSolveSettings),
                                              ctypes.POINTER(SilSolveDiagnostics), _P]),
+    ("sil_mag3d_nl_apply", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dNlProblem), _P, _P]),
+    ("sil_mag3d_nl_apply_jacobian", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dNlProblem), _P, _P, _P]),
+    ("sil_mag3d_nl_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag3dNlProblem), ctypes.c_int,
+                                                ctypes.POINTER(SilSolveSettings),
+                                                ctypes.POINTER(SilSolveDiagnostics), _P]),
 ]
 
 

@@ -1,7 +1,8 @@
-// nonlinear.cu -- 2D magnetostatics with a saturating ferromagnetic
-// material: the nonlinear residual operator, its Jacobian, and the Newton
-// solve with a line search whose linear systems are solved by Jacobi-CG on
-// the Jacobian (FP64).
+// nonlinear.cu -- 2D and 3D magnetostatics with a saturating ferromagnetic
+// material: the nonlinear residual operators, their Jacobians, and the
+// Newton solve with a line search whose linear systems are solved by
+// Jacobi-CG on the Jacobian (FP64).  The 2D operator is described here; the
+// 3D one above its kernels.
 //
 // Operator (moments criterion, onelab_interface/magnetostatics_onelab.hpp:
 // 1271-1426): at an interior row, over the sampled nodes s whose moment
@@ -464,6 +465,285 @@ __global__ void __launch_bounds__(kBlock) axpy_kernel(int n, double const* x, do
     for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) out[i] = x[i] + alpha * d[i];
 }
 
+// ---------------------------------------------------------------- 3D operator
+//
+// Rows 3 * node + c of the vector potential A (x fastest); interior rows sum,
+// over the sampled nodes s whose curl moments hold the row (s = node and its
+// neighbours at -e_a for the two other axes), +-hodge_m(s) H_m(B(s)), with
+// hodge_m = d_m / (d_a d_b) from the reference's local spacings, then add
+// the penalty gauge gamma (d_a d_b / d_c) A_c; boundary rows are the
+// identity.  Two passes: the hodge-weighted field per sampled node, then the
+// per-row gather in the order of the reference's transposed stencils (by
+// sampled node, then moment component).
+// Ref: onelab_interface/magnetostatics_onelab.hpp:2241-2396 (operator),
+//      2924-3110 (apply_jacobian), 856-910 (Hodge factors).
+
+struct Geo3
+{
+    int nx, ny, nz;
+    double gamma;
+    double const* ls[3];  // local spacing per axis
+};
+
+__device__ __forceinline__ bool interior3(Geo3 const& g, int i, int j, int k)
+{
+    return i > 0 && j > 0 && k > 0 && i + 1 < g.nx && j + 1 < g.ny && k + 1 < g.nz;
+}
+
+__device__ __forceinline__ void node_coords(Geo3 const& g, int s, int* i, int* j, int* k)
+{
+    int const t = s / g.nx;
+    *i = s - t * g.nx;
+    *k = t / g.ny;
+    *j = t - *k * g.ny;
+}
+
+// Curl moments of v at the interior sampled node s = (i, j, k), columns on
+// the boundary dropped, in the stencils' order:
+//   B_x = A_y(s) - A_z(s) - A_y(s+z) + A_z(s+y)
+//   B_y = -A_x(s) + A_z(s) + A_x(s+z) - A_z(s+x)
+//   B_z = A_x(s) - A_y(s) - A_x(s+y) + A_y(s+x)
+__device__ __forceinline__ void moments3(Geo3 const& g, double const* v, int s, int i, int j, int k, double* B)
+{
+    int const b = 3 * s, oy = 3 * g.nx, oz = 3 * g.nx * g.ny;
+    bool const ix = interior3(g, i + 1, j, k), iy = interior3(g, i, j + 1, k), iz = interior3(g, i, j, k + 1);
+    double const ax = v[b], ay = v[b + 1], az = v[b + 2];
+    double m = 0.0;
+    m += ay;
+    m -= az;
+    if (iz) m -= v[b + oz + 1];
+    if (iy) m += v[b + oy + 2];
+    B[0] = m;
+    m = 0.0;
+    m -= ax;
+    m += az;
+    if (iz) m += v[b + oz];
+    if (ix) m -= v[b + 3 + 2];
+    B[1] = m;
+    m = 0.0;
+    m += ax;
+    m -= ay;
+    if (iy) m -= v[b + oy];
+    if (ix) m += v[b + 3 + 1];
+    B[2] = m;
+}
+
+__device__ __forceinline__ void hodge_b3(Geo3 const& g, int i, int j, int k, double* h)
+{
+    double const dx = g.ls[0][i], dy = g.ls[1][j], dz = g.ls[2][k];
+    h[0] = dx / (dy * dz);
+    h[1] = dy / (dx * dz);
+    h[2] = dz / (dx * dy);
+}
+
+__device__ __forceinline__ void node_field3(DevCurve const& c, double mu, double ferro, double const* B, double* H)
+{
+    if (ferro > 0.5) {
+        double const q = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+        double F, dF, d2F;
+        curve_f(c, q, &F, &dF, &d2F);
+        for (int m = 0; m < 3; ++m) H[m] = B[m] * F + q * B[m] * dF;
+    } else {
+        for (int m = 0; m < 3; ++m) H[m] = B[m] / mu;
+    }
+}
+
+// J[3 r + c] = d2H / dB_r dB_c at a sampled node.
+__device__ __forceinline__ void node_jacobian3(DevCurve const& c, double mu, double ferro, double const* B, double* J)
+{
+    if (ferro > 0.5) {
+        double const q = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+        double F, dF, d2F;
+        curve_f(c, q, &F, &dF, &d2F);
+        double const base = F + q * dF;
+        for (int r = 0; r < 3; ++r)
+            for (int cc = 0; cc < 3; ++cc)
+                J[3 * r + cc] = (r == cc ? base : 0.0) + 4.0 * B[r] * B[cc] * dF + 2.0 * q * B[r] * B[cc] * d2F;
+    } else {
+        for (int r = 0; r < 3; ++r)
+            for (int cc = 0; cc < 3; ++cc) J[3 * r + cc] = r == cc ? 1.0 / mu : 0.0;
+    }
+}
+
+// hh[3 s + m] = hodge_m(s) H_m(B(s)) at interior sampled nodes, 0 elsewhere.
+__global__ void __launch_bounds__(kBlock) nl3_field_kernel(const __grid_constant__ DevCurve curve, Geo3 g,
+                                                           double const* a, double const* mu, double const* ferro,
+                                                           double* hh)
+{
+    __shared__ DevCurve c;
+    stage_curve(curve, c);
+    int const nodes = g.nx * g.ny * g.nz;
+    for (int s = blockIdx.x * kBlock + threadIdx.x; s < nodes; s += gridDim.x * kBlock) {
+        int i, j, k;
+        node_coords(g, s, &i, &j, &k);
+        double* out = hh + 3 * s;
+        if (!interior3(g, i, j, k)) {
+            out[0] = 0.0;
+            out[1] = 0.0;
+            out[2] = 0.0;
+            continue;
+        }
+        double B[3], H[3], h[3];
+        moments3(g, a, s, i, j, k, B);
+        node_field3(c, mu[s], ferro[s], B, H);
+        hodge_b3(g, i, j, k, h);
+        out[0] = h[0] * H[0];
+        out[1] = h[1] * H[1];
+        out[2] = h[2] * H[2];
+    }
+}
+
+// kh[9 s + 3 m + c] = hodge_m(s) J_mc(B(s)) of the state at interior sampled
+// nodes, 0 elsewhere.
+__global__ void __launch_bounds__(kBlock) nl3_coef_kernel(const __grid_constant__ DevCurve curve, Geo3 g,
+                                                          double const* st, double const* mu, double const* ferro,
+                                                          double* kh)
+{
+    __shared__ DevCurve c;
+    stage_curve(curve, c);
+    int const nodes = g.nx * g.ny * g.nz;
+    for (int s = blockIdx.x * kBlock + threadIdx.x; s < nodes; s += gridDim.x * kBlock) {
+        int i, j, k;
+        node_coords(g, s, &i, &j, &k);
+        double* out = kh + 9 * s;
+        if (!interior3(g, i, j, k)) {
+            for (int e = 0; e < 9; ++e) out[e] = 0.0;
+            continue;
+        }
+        double B[3], J[9], h[3];
+        moments3(g, st, s, i, j, k, B);
+        node_jacobian3(c, mu[s], ferro[s], B, J);
+        hodge_b3(g, i, j, k, h);
+        for (int m = 0; m < 3; ++m)
+            for (int cc = 0; cc < 3; ++cc) out[3 * m + cc] = h[m] * J[3 * m + cc];
+    }
+}
+
+// gv[3 s + m] = sum_c kh[9 s + 3 m + c] B_c(x)(s) at interior sampled nodes.
+__global__ void __launch_bounds__(kBlock) nl3_jfield_kernel(Geo3 g, double const* kh, double const* x, double* gv,
+                                                            CgState const* st)
+{
+    if (st != nullptr && st->done) return;
+    int const nodes = g.nx * g.ny * g.nz;
+    for (int s = blockIdx.x * kBlock + threadIdx.x; s < nodes; s += gridDim.x * kBlock) {
+        int i, j, k;
+        node_coords(g, s, &i, &j, &k);
+        double* out = gv + 3 * s;
+        if (!interior3(g, i, j, k)) {
+            out[0] = 0.0;
+            out[1] = 0.0;
+            out[2] = 0.0;
+            continue;
+        }
+        double D[3];
+        moments3(g, x, s, i, j, k, D);
+        double const* K = kh + 9 * s;
+        for (int m = 0; m < 3; ++m) out[m] = K[3 * m] * D[0] + K[3 * m + 1] * D[1] + K[3 * m + 2] * D[2];
+    }
+}
+
+// Per row: the gather of the per-node values hv (+- by the moment
+// stencils' coefficients) plus the penalty gauge on v; v[row] on the
+// boundary.  MODE 0: out = f.  MODE 1: out = rhs - f, partial sums of
+// out^2.  MODE 2 (CG step): out = f, partial sums of v . out; skipped once
+// the CG state is done.
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) nl3_gather_kernel(Geo3 g, double const* hv, double const* v,
+                                                            double const* rhs, double* out, double* part,
+                                                            CgState const* st)
+{
+    __shared__ double red[kBlock / 32];
+    if (MODE == 2 && st->done) return;
+    int const nodes = g.nx * g.ny * g.nz;
+    int const nrows = 3 * nodes;
+    int const oy = 3 * g.nx, oz = 3 * g.nx * g.ny;
+    double acc = 0.0;
+    for (int row = blockIdx.x * kBlock + threadIdx.x; row < nrows; row += gridDim.x * kBlock) {
+        int const s = row / 3, c = row - 3 * s;
+        int i, j, k;
+        node_coords(g, s, &i, &j, &k);
+        double f;
+        if (!interior3(g, i, j, k)) {
+            f = v[row];
+        } else {
+            int const b = 3 * s;
+            double const dx = g.ls[0][i], dy = g.ls[1][j], dz = g.ls[2][k];
+            double r = 0.0, ha;
+            if (c == 0) {
+                if (k > 1) r += hv[b - oz + 1];
+                if (j > 1) r -= hv[b - oy + 2];
+                r -= hv[b + 1];
+                r += hv[b + 2];
+                ha = dy * dz / dx;
+            } else if (c == 1) {
+                if (k > 1) r -= hv[b - oz];
+                if (i > 1) r += hv[b - 3 + 2];
+                r += hv[b];
+                r -= hv[b + 2];
+                ha = dx * dz / dy;
+            } else {
+                if (j > 1) r += hv[b - oy];
+                if (i > 1) r -= hv[b - 3 + 1];
+                r -= hv[b];
+                r += hv[b + 1];
+                ha = dx * dy / dz;
+            }
+            f = __dadd_rn(r, __dmul_rn(__dmul_rn(g.gamma, ha), v[row]));
+        }
+        if (MODE == 1) {
+            double const rv = rhs[row] - f;
+            out[row] = rv;
+            acc += rv * rv;
+        } else {
+            out[row] = f;
+            if (MODE == 2) acc += v[row] * f;
+        }
+    }
+    if (MODE != 0) {
+        double const t = block_sum(acc, red);
+        if (threadIdx.x == 0) part[blockIdx.x] = t;
+    }
+}
+
+// Inverse Jacobian diagonal from the weighted coefficients: for each entry
+// of the row, the row's own coefficient in the sampled node's moments times
+// that node's weighted Jacobian row; plus the gauge; 1 on the boundary.
+__global__ void __launch_bounds__(kBlock) nl3_dinv_kernel(Geo3 g, double const* kh, double* dinv)
+{
+    int const nodes = g.nx * g.ny * g.nz;
+    int const nrows = 3 * nodes;
+    int const oy = 9 * g.nx, oz = 9 * g.nx * g.ny;
+    for (int row = blockIdx.x * kBlock + threadIdx.x; row < nrows; row += gridDim.x * kBlock) {
+        int const s = row / 3, c = row - 3 * s;
+        int i, j, k;
+        node_coords(g, s, &i, &j, &k);
+        if (!interior3(g, i, j, k)) {
+            dinv[row] = 1.0;
+            continue;
+        }
+        double const* K = kh + 9 * s;
+        double const dx = g.ls[0][i], dy = g.ls[1][j], dz = g.ls[2][k];
+        double d = 0.0, ha;
+        if (c == 0) {
+            if (k > 1) d += K[-oz + 4];
+            if (j > 1) d += K[-oy + 8];
+            d += K[4] - K[5] - K[7] + K[8];
+            ha = dy * dz / dx;
+        } else if (c == 1) {
+            if (k > 1) d += K[-oz + 0];
+            if (i > 1) d += K[-9 + 8];
+            d += K[0] - K[2] - K[6] + K[8];
+            ha = dx * dz / dy;
+        } else {
+            if (j > 1) d += K[-oy + 0];
+            if (i > 1) d += K[-9 + 4];
+            d += K[0] - K[1] - K[3] + K[4];
+            ha = dx * dy / dz;
+        }
+        dinv[row] = 1.0 / (d + g.gamma * ha);
+    }
+}
+
 // ---------------------------------------------------------------- host side
 
 sil_status make_curve(sil_bh_curve const& in, DevCurve* out)
@@ -505,6 +785,101 @@ unsigned grid_for(int64_t n)
     return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(blocks, 4 * sms)));
 }
 
+sil_status check_problem3(sil_mag3d_nl_problem const& p, char const* who, bool need_fields)
+{
+    std::string const w(who);
+    if (p.nx < 3 || p.ny < 3 || p.nz < 3) return fail(SIL_ERR_INVALID, w + ": need at least 3x3x3 nodes");
+    if (3 * p.nx * p.ny * p.nz >= (int64_t(1) << 31))
+        return fail(SIL_ERR_INVALID, w + ": fewer than 2^31 unknowns per problem supported");
+    if (p.x == nullptr || p.y == nullptr || p.z == nullptr) return fail(SIL_ERR_INVALID, w + ": NULL coordinate array");
+    if (p.node_mu == nullptr || p.node_ferro == nullptr) return fail(SIL_ERR_INVALID, w + ": NULL material array");
+    if (need_fields && (p.rhs == nullptr || p.solution == nullptr)) return fail(SIL_ERR_INVALID, w + ": NULL field pointer");
+    if (!std::isfinite(p.gauge_penalty) || !(p.gauge_penalty > 0.0))
+        return fail(SIL_ERR_INVALID, w + ": gauge_penalty must be finite and positive");
+    double const* c[3] = {p.x, p.y, p.z};
+    int64_t const len[3] = {p.nx, p.ny, p.nz};
+    for (int a = 0; a < 3; ++a)
+        for (int64_t i = 0; i + 1 < len[a]; ++i)
+            if (!(c[a][i + 1] > c[a][i])) return fail(SIL_ERR_INVALID, w + ": node coordinates must increase strictly");
+    return SIL_OK;
+}
+
+// The reference's local spacing per axis (one-sided at the ends, central
+// average inside; magnetostatics_onelab.hpp:856-870), axes concatenated.
+std::vector<double> local_spacings(sil_mag3d_nl_problem const& p)
+{
+    double const* c[3] = {p.x, p.y, p.z};
+    int64_t const len[3] = {p.nx, p.ny, p.nz};
+    std::vector<double> out;
+    for (int a = 0; a < 3; ++a)
+        for (int64_t i = 0; i < len[a]; ++i) {
+            int64_t const n = len[a];
+            double v;
+            if (i == 0) v = c[a][1] - c[a][0];
+            else if (i + 1 == n) v = c[a][n - 1] - c[a][n - 2];
+            else v = 0.5 * (c[a][i + 1] - c[a][i - 1]);
+            out.push_back(v);
+        }
+    return out;
+}
+
+Geo3 make_geo3(sil_mag3d_nl_problem const& p, double const* dls)
+{
+    Geo3 g {};
+    g.nx = static_cast<int>(p.nx);
+    g.ny = static_cast<int>(p.ny);
+    g.nz = static_cast<int>(p.nz);
+    g.gamma = p.gauge_penalty;
+    g.ls[0] = dls;
+    g.ls[1] = dls + p.nx;
+    g.ls[2] = dls + p.nx + p.ny;
+    return g;
+}
+
+// Stream-ordered device allocation, freed in stream order.
+struct AsyncBuffer
+{
+    void* ptr = nullptr;
+    cudaStream_t s = nullptr;
+    bool sync = false;  // wait for the free (a stream the buffer's owner destroys next)
+    ~AsyncBuffer()
+    {
+        if (ptr != nullptr) {
+            cudaFreeAsync(ptr, s);
+            if (sync) cudaStreamSynchronize(s);
+        }
+    }
+};
+
+// Up to kConcurrent problems at a time, each on a host thread with its own
+// stream (one problem's CG kernels are small and launch bound, so several
+// problems together fill the GPU).
+template <class Solve>
+sil_status run_concurrent(int nproblems, Solve const& solve)
+{
+    (void)grid_for(1);  // device attributes read once, before the threads start
+    int dev = 0;
+    SIL_CUDA_CHECK(cudaGetDevice(&dev));
+    constexpr int kConcurrent = 8;
+    std::vector<sil_status> status(nproblems, SIL_OK);
+    std::vector<std::string> message(nproblems);
+    for (int first = 0; first < nproblems; first += kConcurrent) {
+        int const last = std::min(nproblems, first + kConcurrent);
+        std::vector<std::thread> workers;
+        for (int p = first; p < last; ++p) {
+            workers.emplace_back([&, p] {
+                cudaSetDevice(dev);
+                status[p] = solve(p);
+                if (status[p] != SIL_OK) message[p] = sil_last_error();
+            });
+        }
+        for (auto& w : workers) w.join();
+    }
+    for (int p = 0; p < nproblems; ++p)
+        if (status[p] != SIL_OK) return fail(status[p], message[p]);
+    return SIL_OK;
+}
+
 }  // namespace
 }  // namespace sil
 
@@ -543,17 +918,185 @@ sil_status sil_mag2d_nl_apply_jacobian(sil_stream stream, const sil_mag2d_nl_pro
 namespace sil {
 namespace {
 
-// One problem's Newton solve on its own stream and buffers (the problems of
-// a batch run on concurrent host threads).
-sil_status solve_one(sil_mag2d_nl_problem const& P, DevCurve const& C, double tol, int max_iter,
-                     sil_solve_diagnostics& D)
+// Newton with the line search for one problem on stream st.  v: nine
+// vectors of ops.n doubles (r, cand_r, cand, d, cr, z, p, q, dinv); part:
+// 2 * ops.G doubles.  Ops supplies
+//   residual(s, val, out, part):   out = rhs - F(val), ops.G partials of out^2
+//   jacobian_setup(s, x, dinv):    Jacobian coefficients at x, inverse diagonal
+//   cg_product(s, p, q, part, cg): q = J p, ops.G partials of p.q, no work once
+//                                  the CG state is done
+template <class Ops>
+sil_status newton(Ops const& ops, double* x, double* const* v, double* part, double* d_norm, CgState* d_cg,
+                  cudaStream_t st, double tol, int max_iter, sil_solve_diagnostics& D)
 {
-    int64_t const maxn = P.nx * P.ny;
-    // r, cand_r, cand, d, cr, z, p, q, dinv, c00, c01, c11 + partials + scalars
-    int const nvec = 12;
-    size_t const vbytes = ((static_cast<size_t>(maxn) * sizeof(double) + 255) / 256) * 256;
-    unsigned const gmax = grid_for(maxn);
-    size_t const pbytes = ((2 * static_cast<size_t>(gmax) * sizeof(double) + 255) / 256) * 256;
+    double *r = v[0], *cand_r = v[1], *cand = v[2], *dvec = v[3], *cr = v[4], *z = v[5], *pv = v[6], *qv = v[7],
+           *dinv = v[8];
+    D = sil_solve_diagnostics {};
+    int const n = static_cast<int>(ops.n);
+    unsigned const G = ops.G;
+    // residual norm of rhs - F(val) into out (returned on the host)
+    auto residual = [&](double const* val, double* out, double* norm) -> sil_status {
+        ops.residual(st, val, out, part);
+        norm_finish_kernel<<<1, kBlock, 0, st>>>(part, static_cast<int>(G), d_norm);
+        SIL_CUDA_CHECK(cudaGetLastError());
+        SIL_CUDA_CHECK(cudaMemcpyAsync(norm, d_norm, sizeof(double), cudaMemcpyDeviceToHost, st));
+        SIL_CUDA_CHECK(cudaStreamSynchronize(st));
+        return SIL_OK;
+    };
+    double res = 0.0;
+    if (sil_status s = residual(x, r, &res); s != SIL_OK) return s;
+    double const r0 = res;
+    D.initial_residual_l2 = r0;
+    D.status = SIL_OK;
+    if (!std::isfinite(r0)) {
+        D.status = SIL_ERR_NONFINITE;
+        D.final_residual_l2 = r0;
+        D.final_relative_residual = r0;
+        return SIL_OK;
+    }
+    if (r0 == 0.0) {
+        D.converged = 1;
+        return SIL_OK;
+    }
+    // 16 CG iterations captured once per problem (the kernels stop doing
+    // work once the state is marked done) and replayed until convergence.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    {
+        cudaStream_t cs;
+        SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        for (int c = 0; c < 16 && err == cudaSuccess; ++c) {
+            ops.cg_product(cs, pv, qv, part, d_cg);
+            cg_alpha_kernel<<<1, kBlock, 0, cs>>>(part, static_cast<int>(G), d_cg);
+            cg_update_kernel<<<G, kBlock, 0, cs>>>(n, dvec, cr, pv, qv, dinv, z, part, d_cg);
+            cg_beta_kernel<<<1, kBlock, 0, cs>>>(part, static_cast<int>(G), d_cg, tol, max_iter);
+            cg_direction_kernel<<<G, kBlock, 0, cs>>>(n, pv, z, d_cg);
+        }
+        cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
+        if (err == cudaSuccess) err = err2;
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+        cudaStreamDestroy(cs);
+        if (err != cudaSuccess) {
+            if (graph != nullptr) cudaGraphDestroy(graph);
+            return cuda_fail(err, "nonlinear CG graph capture");
+        }
+    }
+    struct GraphGuard
+    {
+        cudaGraph_t g;
+        cudaGraphExec_t e;
+        ~GraphGuard()
+        {
+            cudaGraphExecDestroy(e);
+            cudaGraphDestroy(g);
+        }
+    } guard {graph, exec};
+    int cg_total = 0, steps = 0;
+    for (int it = 0; it < 30; ++it) {
+        if (res / r0 <= tol) break;
+        ++steps;
+        ops.jacobian_setup(st, x, dinv);
+        cg_start_kernel<<<G, kBlock, 0, st>>>(n, r, dinv, dvec, cr, z, pv, part);
+        cg_init_kernel<<<1, kBlock, 0, st>>>(part, static_cast<int>(G), d_cg, tol, max_iter);
+        SIL_CUDA_CHECK(cudaGetLastError());
+        CgState hs {};
+        for (;;) {
+            SIL_CUDA_CHECK(cudaGraphLaunch(exec, st));
+            SIL_CUDA_CHECK(cudaMemcpyAsync(&hs, d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, st));
+            SIL_CUDA_CHECK(cudaStreamSynchronize(st));
+            if (hs.done) break;
+        }
+        cg_total += hs.iters;
+        // line search
+        double const cur = res;
+        double alpha = 1.0, best_alpha = 0.0, best = std::numeric_limits<double>::infinity(), nr = 0.0;
+        for (int ls = 0; ls < 8; ++ls) {
+            axpy_kernel<<<G, kBlock, 0, st>>>(n, x, alpha, dvec, cand);
+            if (sil_status s = residual(cand, cand_r, &nr); s != SIL_OK) return s;
+            if (nr < best) {
+                best = nr;
+                best_alpha = alpha;
+            }
+            if (nr < cur) break;
+            alpha *= 0.5;
+        }
+        if (best_alpha != alpha) {
+            alpha = best_alpha;
+            axpy_kernel<<<G, kBlock, 0, st>>>(n, x, alpha, dvec, cand);
+            if (sil_status s = residual(cand, cand_r, &nr); s != SIL_OK) return s;
+        }
+        SIL_CUDA_CHECK(cudaMemcpyAsync(x, cand, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        std::swap(r, cand_r);
+        res = nr;
+        if (!std::isfinite(res)) break;
+    }
+    D.iterations = cg_total;
+    D.refinements = steps;
+    D.final_residual_l2 = res;
+    D.final_relative_residual = res / r0;
+    D.converged = (res / r0 <= tol) ? 1 : 0;
+    if (!std::isfinite(res)) D.status = SIL_ERR_NONFINITE;
+    return SIL_OK;
+}
+
+struct Ops2
+{
+    DevCurve const& C;
+    Geo g;
+    sil_mag2d_nl_problem const& P;
+    double *c00, *c01, *c11;
+    int64_t n;
+    unsigned G;
+    void residual(cudaStream_t s, double const* val, double* out, double* part) const
+    {
+        nl_apply_kernel<<<G, kBlock, 0, s>>>(C, g, val, P.node_mu, P.node_ferro, P.rhs, out, part);
+    }
+    void jacobian_setup(cudaStream_t s, double const* x, double* dinv) const
+    {
+        nl_coef_kernel<<<G, kBlock, 0, s>>>(C, g, x, P.node_mu, P.node_ferro, c00, c01, c11);
+        nl_dinv_kernel<<<G, kBlock, 0, s>>>(g, c00, c01, c11, dinv);
+    }
+    void cg_product(cudaStream_t s, double const* p, double* q, double* part, CgState const* cg) const
+    {
+        cg_jac_kernel<<<G, kBlock, 0, s>>>(g, c00, c01, c11, p, q, part, cg);
+    }
+};
+
+struct Ops3
+{
+    DevCurve const& C;
+    Geo3 g;
+    sil_mag3d_nl_problem const& P;
+    double* hv;  // 3 per node: the weighted field, or the Jacobian's image in CG
+    double* kh;  // 9 per node: weighted Jacobian coefficients
+    int64_t n;   // rows: 3 per node
+    unsigned G;  // grid of the row and vector kernels
+    unsigned Gn; // grid of the node kernels
+    void residual(cudaStream_t s, double const* val, double* out, double* part) const
+    {
+        nl3_field_kernel<<<Gn, kBlock, 0, s>>>(C, g, val, P.node_mu, P.node_ferro, hv);
+        nl3_gather_kernel<1><<<G, kBlock, 0, s>>>(g, hv, val, P.rhs, out, part, nullptr);
+    }
+    void jacobian_setup(cudaStream_t s, double const* x, double* dinv) const
+    {
+        nl3_coef_kernel<<<Gn, kBlock, 0, s>>>(C, g, x, P.node_mu, P.node_ferro, kh);
+        nl3_dinv_kernel<<<G, kBlock, 0, s>>>(g, kh, dinv);
+    }
+    void cg_product(cudaStream_t s, double const* p, double* q, double* part, CgState const* cg) const
+    {
+        nl3_jfield_kernel<<<Gn, kBlock, 0, s>>>(g, kh, p, hv, cg);
+        nl3_gather_kernel<2><<<G, kBlock, 0, s>>>(g, hv, p, nullptr, q, part, cg);
+    }
+};
+
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+// One problem's Newton solve on its own stream and buffers (the problems of
+// a batch run on concurrent host threads).  extra: doubles of the problem's
+// own work arrays after the nine Newton vectors.
+struct Workspace
+{
     struct StreamGuard
     {
         cudaStream_t s = nullptr;
@@ -562,143 +1105,65 @@ sil_status solve_one(sil_mag2d_nl_problem const& P, DevCurve const& C, double to
             if (s != nullptr) cudaStreamDestroy(s);
         }
     } sg;
-    SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&sg.s, cudaStreamNonBlocking));
-    cudaStream_t const st = sg.s;
-    // stream-ordered allocation: freeing does not synchronise the other
-    // problems' streams
-    struct AsyncBuffer
+    AsyncBuffer buf;
+    double* v[9];
+    double* part;
+    double* d_norm;
+    CgState* d_cg;
+    double* extra;
+
+    sil_status init(int64_t n, unsigned G, size_t extra_doubles)
     {
-        void* ptr = nullptr;
-        cudaStream_t s;
-        ~AsyncBuffer()
-        {
-            if (ptr != nullptr) {
-                cudaFreeAsync(ptr, s);
-                cudaStreamSynchronize(s);
-            }
-        }
-    } buf {nullptr, st};
-    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, nvec * vbytes + pbytes + 2 * 256, st));
-    char* base = static_cast<char*>(buf.ptr);
-    double* v[nvec];
-    for (int k = 0; k < nvec; ++k) v[k] = reinterpret_cast<double*>(base + k * vbytes);
-    double* part = reinterpret_cast<double*>(base + nvec * vbytes);
-    double* d_norm = reinterpret_cast<double*>(base + nvec * vbytes + pbytes);
-    CgState* d_cg = reinterpret_cast<CgState*>(base + nvec * vbytes + pbytes + 256);
-    double *r = v[0], *cand_r = v[1], *cand = v[2], *dvec = v[3], *cr = v[4], *z = v[5], *pv = v[6], *qv = v[7],
-           *dinv = v[8], *c00 = v[9], *c01 = v[10], *c11 = v[11];
-    do {
-        D = sil_solve_diagnostics {};
-        Geo const g {static_cast<int>(P.nx), static_cast<int>(P.ny)};
-        int const n = g.nx * g.ny;
-        unsigned const G = grid_for(n);
-        double* x = P.solution;
-        // residual norm of rhs - F(v) into out (returned on the host)
-        auto residual = [&](double const* val, double* out, double* norm) -> sil_status {
-            nl_apply_kernel<<<G, kBlock, 0, st>>>(C, g, val, P.node_mu, P.node_ferro, P.rhs, out, part);
-            norm_finish_kernel<<<1, kBlock, 0, st>>>(part, static_cast<int>(G), d_norm);
-            SIL_CUDA_CHECK(cudaGetLastError());
-            SIL_CUDA_CHECK(cudaMemcpyAsync(norm, d_norm, sizeof(double), cudaMemcpyDeviceToHost, st));
-            SIL_CUDA_CHECK(cudaStreamSynchronize(st));
-            return SIL_OK;
-        };
-        double res = 0.0;
-        if (sil_status s = residual(x, r, &res); s != SIL_OK) return s;
-        double const r0 = res;
-        D.initial_residual_l2 = r0;
-        D.status = SIL_OK;
-        if (!std::isfinite(r0)) {
-            D.status = SIL_ERR_NONFINITE;
-            D.final_residual_l2 = r0;
-            D.final_relative_residual = r0;
-            break;
-        }
-        if (r0 == 0.0) {
-            D.converged = 1;
-            break;
-        }
-        // 16 CG iterations captured once per problem (the kernels stop doing
-        // work once the state is marked done) and replayed until convergence.
-        cudaGraph_t graph = nullptr;
-        cudaGraphExec_t exec = nullptr;
-        {
-            cudaStream_t cs;
-            SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-            cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-            for (int c = 0; c < 16 && err == cudaSuccess; ++c) {
-                cg_jac_kernel<<<G, kBlock, 0, cs>>>(g, c00, c01, c11, pv, qv, part, d_cg);
-                cg_alpha_kernel<<<1, kBlock, 0, cs>>>(part, static_cast<int>(G), d_cg);
-                cg_update_kernel<<<G, kBlock, 0, cs>>>(n, dvec, cr, pv, qv, dinv, z, part, d_cg);
-                cg_beta_kernel<<<1, kBlock, 0, cs>>>(part, static_cast<int>(G), d_cg, tol, max_iter);
-                cg_direction_kernel<<<G, kBlock, 0, cs>>>(n, pv, z, d_cg);
-            }
-            cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
-            if (err == cudaSuccess) err = err2;
-            if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
-            cudaStreamDestroy(cs);
-            if (err != cudaSuccess) {
-                if (graph != nullptr) cudaGraphDestroy(graph);
-                return cuda_fail(err, "nonlinear CG graph capture");
-            }
-        }
-        struct GraphGuard
-        {
-            cudaGraph_t g;
-            cudaGraphExec_t e;
-            ~GraphGuard()
-            {
-                cudaGraphExecDestroy(e);
-                cudaGraphDestroy(g);
-            }
-        } guard {graph, exec};
-        int cg_total = 0, steps = 0;
-        for (int it = 0; it < 30; ++it) {
-            if (res / r0 <= tol) break;
-            ++steps;
-            nl_coef_kernel<<<G, kBlock, 0, st>>>(C, g, x, P.node_mu, P.node_ferro, c00, c01, c11);
-            nl_dinv_kernel<<<G, kBlock, 0, st>>>(g, c00, c01, c11, dinv);
-            cg_start_kernel<<<G, kBlock, 0, st>>>(n, r, dinv, dvec, cr, z, pv, part);
-            cg_init_kernel<<<1, kBlock, 0, st>>>(part, static_cast<int>(G), d_cg, tol, max_iter);
-            SIL_CUDA_CHECK(cudaGetLastError());
-            CgState hs {};
-            for (;;) {
-                SIL_CUDA_CHECK(cudaGraphLaunch(exec, st));
-                SIL_CUDA_CHECK(cudaMemcpyAsync(&hs, d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, st));
-                SIL_CUDA_CHECK(cudaStreamSynchronize(st));
-                if (hs.done) break;
-            }
-            cg_total += hs.iters;
-            // line search
-            double const cur = res;
-            double alpha = 1.0, best_alpha = 0.0, best = std::numeric_limits<double>::infinity(), nr = 0.0;
-            for (int ls = 0; ls < 8; ++ls) {
-                axpy_kernel<<<G, kBlock, 0, st>>>(n, x, alpha, dvec, cand);
-                if (sil_status s = residual(cand, cand_r, &nr); s != SIL_OK) return s;
-                if (nr < best) {
-                    best = nr;
-                    best_alpha = alpha;
-                }
-                if (nr < cur) break;
-                alpha *= 0.5;
-            }
-            if (best_alpha != alpha) {
-                alpha = best_alpha;
-                axpy_kernel<<<G, kBlock, 0, st>>>(n, x, alpha, dvec, cand);
-                if (sil_status s = residual(cand, cand_r, &nr); s != SIL_OK) return s;
-            }
-            SIL_CUDA_CHECK(cudaMemcpyAsync(x, cand, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-            std::swap(r, cand_r);
-            res = nr;
-            if (!std::isfinite(res)) break;
-        }
-        D.iterations = cg_total;
-        D.refinements = steps;
-        D.final_residual_l2 = res;
-        D.final_relative_residual = res / r0;
-        D.converged = (res / r0 <= tol) ? 1 : 0;
-        if (!std::isfinite(res)) D.status = SIL_ERR_NONFINITE;
-    } while (false);
-    SIL_CUDA_CHECK(cudaStreamSynchronize(st));
+        SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&sg.s, cudaStreamNonBlocking));
+        buf.s = sg.s;
+        buf.sync = true;
+        size_t const vbytes = round256(static_cast<size_t>(n) * sizeof(double));
+        size_t const pbytes = round256(2 * static_cast<size_t>(G) * sizeof(double));
+        size_t const ebytes = round256(extra_doubles * sizeof(double));
+        SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, 9 * vbytes + pbytes + 2 * 256 + ebytes, sg.s));
+        char* base = static_cast<char*>(buf.ptr);
+        for (int k = 0; k < 9; ++k) v[k] = reinterpret_cast<double*>(base + k * vbytes);
+        part = reinterpret_cast<double*>(base + 9 * vbytes);
+        d_norm = reinterpret_cast<double*>(base + 9 * vbytes + pbytes);
+        d_cg = reinterpret_cast<CgState*>(base + 9 * vbytes + pbytes + 256);
+        extra = reinterpret_cast<double*>(base + 9 * vbytes + pbytes + 2 * 256);
+        return SIL_OK;
+    }
+};
+
+sil_status solve_one(sil_mag2d_nl_problem const& P, DevCurve const& C, double tol, int max_iter,
+                     sil_solve_diagnostics& D)
+{
+    int64_t const n = P.nx * P.ny;
+    unsigned const G = grid_for(n);
+    size_t const vb = round256(static_cast<size_t>(n) * sizeof(double)) / sizeof(double);
+    Workspace w;
+    if (sil_status s = w.init(n, G, 3 * vb); s != SIL_OK) return s;
+    Ops2 const ops {C, Geo {static_cast<int>(P.nx), static_cast<int>(P.ny)}, P, w.extra, w.extra + vb,
+                    w.extra + 2 * vb, n, G};
+    if (sil_status s = newton(ops, P.solution, w.v, w.part, w.d_norm, w.d_cg, w.sg.s, tol, max_iter, D); s != SIL_OK)
+        return s;
+    SIL_CUDA_CHECK(cudaStreamSynchronize(w.sg.s));
+    return SIL_OK;
+}
+
+sil_status solve_one3(sil_mag3d_nl_problem const& P, DevCurve const& C, double tol, int max_iter,
+                      sil_solve_diagnostics& D)
+{
+    int64_t const nodes = P.nx * P.ny * P.nz;
+    int64_t const n = 3 * nodes;
+    unsigned const G = grid_for(n);
+    std::vector<double> const sp = local_spacings(P);
+    size_t const hb = round256(static_cast<size_t>(3 * nodes) * sizeof(double)) / sizeof(double);
+    size_t const kb = round256(static_cast<size_t>(9 * nodes) * sizeof(double)) / sizeof(double);
+    Workspace w;
+    if (sil_status s = w.init(n, G, hb + kb + sp.size()); s != SIL_OK) return s;
+    double* dls = w.extra + hb + kb;
+    SIL_CUDA_CHECK(cudaMemcpyAsync(dls, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, w.sg.s));
+    Ops3 const ops {C, make_geo3(P, dls), P, w.extra, w.extra + hb, n, G, grid_for(nodes)};
+    if (sil_status s = newton(ops, P.solution, w.v, w.part, w.d_norm, w.d_cg, w.sg.s, tol, max_iter, D); s != SIL_OK)
+        return s;
+    SIL_CUDA_CHECK(cudaStreamSynchronize(w.sg.s));
     return SIL_OK;
 }
 
@@ -724,28 +1189,84 @@ sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int np
     int const max_iter = settings->max_iterations > 0 ? settings->max_iterations : 100000;
     // the inputs come from the caller's stream
     SIL_CUDA_CHECK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
-    (void)grid_for(1);  // device attributes read once, before the threads start
-    int dev = 0;
-    SIL_CUDA_CHECK(cudaGetDevice(&dev));
-    // Up to kConcurrent problems at a time, each on a host thread with its
-    // own stream: one problem's CG kernels are small and launch bound, so
-    // several problems together fill the GPU.
-    constexpr int kConcurrent = 8;
-    std::vector<sil_status> status(nproblems, SIL_OK);
-    std::vector<std::string> message(nproblems);
-    for (int first = 0; first < nproblems; first += kConcurrent) {
-        int const last = std::min(nproblems, first + kConcurrent);
-        std::vector<std::thread> workers;
-        for (int p = first; p < last; ++p) {
-            workers.emplace_back([&, p] {
-                cudaSetDevice(dev);
-                status[p] = solve_one(problems[p], curves[p], tol, max_iter, diag[p]);
-                if (status[p] != SIL_OK) message[p] = sil_last_error();
-            });
-        }
-        for (auto& w : workers) w.join();
-    }
-    for (int p = 0; p < nproblems; ++p)
-        if (status[p] != SIL_OK) return fail(status[p], message[p]);
+    return run_concurrent(nproblems, [&](int p) { return solve_one(problems[p], curves[p], tol, max_iter, diag[p]); });
+}
+
+namespace {
+
+sil_status nl3_prepare(sil_mag3d_nl_problem const* problem, char const* who, DevCurve* c)
+{
+    if (sil_status s = check_problem3(*problem, who, false); s != SIL_OK) return s;
+    return make_curve(problem->curve, c);
+}
+
+}  // namespace
+
+sil_status sil_mag3d_nl_apply(sil_stream stream, const sil_mag3d_nl_problem* problem, const double* a, double* y)
+{
+    if (problem == nullptr || a == nullptr || y == nullptr) return fail(SIL_ERR_INVALID, "sil_mag3d_nl_apply: NULL argument");
+    DevCurve c;
+    if (sil_status s = nl3_prepare(problem, "sil_mag3d_nl_apply", &c); s != SIL_OK) return s;
+    sil_mag3d_nl_problem const& P = *problem;
+    cudaStream_t const st = static_cast<cudaStream_t>(stream);
+    int64_t const nodes = P.nx * P.ny * P.nz;
+    std::vector<double> const sp = local_spacings(P);
+    size_t const hb = round256(static_cast<size_t>(3 * nodes) * sizeof(double));
+    AsyncBuffer buf {nullptr, st, false};
+    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, hb + sp.size() * sizeof(double), st));
+    double* hv = static_cast<double*>(buf.ptr);
+    double* dls = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb);
+    // a copy from pageable memory has left the host table once it returns
+    SIL_CUDA_CHECK(cudaMemcpyAsync(dls, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    Geo3 const g = make_geo3(P, dls);
+    nl3_field_kernel<<<grid_for(nodes), kBlock, 0, st>>>(c, g, a, P.node_mu, P.node_ferro, hv);
+    nl3_gather_kernel<0><<<grid_for(3 * nodes), kBlock, 0, st>>>(g, hv, a, nullptr, y, nullptr, nullptr);
+    SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
+}
+
+sil_status sil_mag3d_nl_apply_jacobian(sil_stream stream, const sil_mag3d_nl_problem* problem, const double* state,
+                                       const double* x, double* y)
+{
+    if (problem == nullptr || state == nullptr || x == nullptr || y == nullptr)
+        return fail(SIL_ERR_INVALID, "sil_mag3d_nl_apply_jacobian: NULL argument");
+    DevCurve c;
+    if (sil_status s = nl3_prepare(problem, "sil_mag3d_nl_apply_jacobian", &c); s != SIL_OK) return s;
+    sil_mag3d_nl_problem const& P = *problem;
+    cudaStream_t const st = static_cast<cudaStream_t>(stream);
+    int64_t const nodes = P.nx * P.ny * P.nz;
+    std::vector<double> const sp = local_spacings(P);
+    size_t const hb = round256(static_cast<size_t>(3 * nodes) * sizeof(double));
+    size_t const kb = round256(static_cast<size_t>(9 * nodes) * sizeof(double));
+    AsyncBuffer buf {nullptr, st, false};
+    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, hb + kb + sp.size() * sizeof(double), st));
+    double* hv = static_cast<double*>(buf.ptr);
+    double* kh = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb);
+    double* dls = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb + kb);
+    SIL_CUDA_CHECK(cudaMemcpyAsync(dls, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    Geo3 const g = make_geo3(P, dls);
+    unsigned const gn = grid_for(nodes);
+    nl3_coef_kernel<<<gn, kBlock, 0, st>>>(c, g, state, P.node_mu, P.node_ferro, kh);
+    nl3_jfield_kernel<<<gn, kBlock, 0, st>>>(g, kh, x, hv, nullptr);
+    nl3_gather_kernel<0><<<grid_for(3 * nodes), kBlock, 0, st>>>(g, hv, x, nullptr, y, nullptr, nullptr);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+sil_status sil_mag3d_nl_solve_batch(const sil_mag3d_nl_problem* problems, int nproblems,
+                                    const sil_solve_settings* settings, sil_solve_diagnostics* diag,
+                                    sil_stream stream)
+{
+    if (problems == nullptr || settings == nullptr || diag == nullptr || nproblems <= 0)
+        return fail(SIL_ERR_INVALID, "sil_mag3d_nl_solve_batch: NULL argument or empty batch");
+    std::vector<DevCurve> curves(nproblems);
+    for (int p = 0; p < nproblems; ++p) {
+        if (sil_status s = check_problem3(problems[p], "sil_mag3d_nl_solve_batch", true); s != SIL_OK) return s;
+        if (sil_status s = make_curve(problems[p].curve, &curves[p]); s != SIL_OK) return s;
+    }
+    double const tol = settings->relative_tolerance > 0 ? settings->relative_tolerance : 1e-10;
+    int const max_iter = settings->max_iterations > 0 ? settings->max_iterations : 100000;
+    // the inputs come from the caller's stream
+    SIL_CUDA_CHECK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    return run_concurrent(nproblems, [&](int p) { return solve_one3(problems[p], curves[p], tol, max_iter, diag[p]); });
 }

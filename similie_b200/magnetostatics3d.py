@@ -201,3 +201,106 @@ def solve_batch(coords, mus, rhss, sols, gammas=None, solver="cg", tol=1e-10, ma
            for d in diag]
     check(rc, "mag3d_solve_batch")
     return out
+
+
+# ----------------------------------------------------------------- nonlinear material
+
+def node_ferro(nx, ny, nz, cell_nonlinear):
+    """Share of the adjacent cells made of the nonlinear material, per node (0 where a
+    node has no cell); a node follows the B-H curve when it is above 1/2
+    (onelab_interface/magnetostatics_onelab.hpp:5030-5066)."""
+    return node_mu(nx, ny, nz, np.asarray(cell_nonlinear, dtype=np.float64), mu0=0.0)
+
+
+def nonlinear_knee(n):
+    """Knee of the synthetic B-H curve for an n^3 unit-cube problem of the
+    loop-current distribution: the 3D curl moments are circulations of A
+    around a cell face and scale with the spacing 1/(n-1); at this knee the
+    strongest moments in the core saturate mildly."""
+    return 0.08 / (n - 1)
+
+
+def nonlinear_problem(n, seed, tube=0.12):
+    """(Problem, node_mu, node_ferro, curve b, curve h) of a seeded 3D
+    nonlinear problem: the loop-current distribution with a random box core
+    of permeability 1000 made of the saturating material."""
+    from .magnetostatics import synthetic_bh_curve
+    rng = np.random.default_rng(seed)
+    p = synthetic_problem(rng, n, tube=tube)
+    nc = n - 1
+    lo = rng.integers(nc // 4, nc // 2, 3)
+    hi = lo + rng.integers(nc // 6 + 1, nc // 3 + 1, 3)
+    core = np.zeros((nc, nc, nc), dtype=bool)
+    core[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] = True
+    p.cell_mu = np.where(core, 1000.0, 1.0).ravel()
+    p.meta["core"] = (lo.tolist(), hi.tolist())
+    b, h = synthetic_bh_curve(nonlinear_knee(n))
+    return p, p.node_mu(), node_ferro(n, n, n, core.ravel()), b, h
+
+
+def _nl_problem_struct(x, y, z, mu, ferro, curve, gamma, rhs_dev=None, sol_dev=None):
+    p = _native.SilMag3dNlProblem()
+    p.nx, p.ny, p.nz = len(x), len(y), len(z)
+    p.x, p.y, p.z = (v.ctypes.data for v in (x, y, z))
+    p.node_mu = mu.data_ptr()
+    p.node_ferro = ferro.data_ptr()
+    p.curve = curve.struct()
+    p.rhs = 0 if rhs_dev is None else rhs_dev.data_ptr()
+    p.solution = 0 if sol_dev is None else sol_dev.data_ptr()
+    p.gauge_penalty = gamma
+    return p
+
+
+def nl_apply(x, y, z, node_mu_dev, node_ferro_dev, curve_b, curve_h, a_dev, y_dev, gamma=DEFAULT_GAUGE_PENALTY,
+             stream=None):
+    """y = F(a), the 3D nonlinear operator (torch CUDA float64 tensors, a/y flat 3*nodes)."""
+    import torch
+    from .magnetostatics import _Curve
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    c = _Curve(curve_b, curve_h)
+    p = _nl_problem_struct(x, y, z, node_mu_dev, node_ferro_dev, c, gamma)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+    check(lib().sil_mag3d_nl_apply(s, ctypes.byref(p), ctypes.c_void_p(a_dev.data_ptr()),
+                                   ctypes.c_void_p(y_dev.data_ptr())), "mag3d_nl_apply")
+    return y_dev
+
+
+def nl_apply_jacobian(x, y, z, node_mu_dev, node_ferro_dev, curve_b, curve_h, state_dev, v_dev, y_dev,
+                      gamma=DEFAULT_GAUGE_PENALTY, stream=None):
+    """y = J(state) v for the 3D nonlinear operator."""
+    import torch
+    from .magnetostatics import _Curve
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    c = _Curve(curve_b, curve_h)
+    p = _nl_problem_struct(x, y, z, node_mu_dev, node_ferro_dev, c, gamma)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+    check(lib().sil_mag3d_nl_apply_jacobian(s, ctypes.byref(p), ctypes.c_void_p(state_dev.data_ptr()),
+                                            ctypes.c_void_p(v_dev.data_ptr()), ctypes.c_void_p(y_dev.data_ptr())),
+          "mag3d_nl_apply_jacobian")
+    return y_dev
+
+
+def nl_solve_batch(coords, mus, ferros, curves, rhss, sols, gammas=None, tol=1e-10, max_iterations=100000,
+                   stream=None):
+    """Newton + line search for a batch of 3D nonlinear problems.  coords: (x, y, z) host arrays;
+    curves: (b, h) sample arrays; sols hold the initial guesses and receive the solutions.
+    Returns one Diagnostics per problem (refinements = Newton steps)."""
+    import torch
+    from .magnetostatics import _Curve
+    n = len(coords)
+    gammas = [DEFAULT_GAUGE_PENALTY] * n if gammas is None else list(gammas)
+    keep = [tuple(_f64(v) for v in c) for c in coords]
+    kc = [_Curve(b, h) for b, h in curves]
+    probs = (_native.SilMag3dNlProblem * n)()
+    for k in range(n):
+        probs[k] = _nl_problem_struct(*keep[k], mus[k], ferros[k], kc[k], gammas[k], rhss[k], sols[k])
+    st = _native.SilSolveSettings()
+    st.max_iterations = max_iterations
+    st.relative_tolerance = tol
+    diag = (_native.SilSolveDiagnostics * n)()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+    rc = lib().sil_mag3d_nl_solve_batch(probs, n, ctypes.byref(st), diag, s)
+    out = [Diagnostics(d.iterations, bool(d.converged), d.refinements, d.status, d.initial_residual_l2,
+                       d.final_residual_l2, d.final_relative_residual) for d in diag]
+    check(rc, "mag3d_nl_solve_batch")
+    return out

@@ -129,6 +129,37 @@ def test_gauge_and_nonlinear_arguments_checked_on_host():
     assert L.sil_mag2d_nl_solve_batch(ctypes.byref(q), 1, ctypes.byref(st), diag, None) == 1
     assert b"NULL" in L.sil_last_error()
     assert L.sil_mag2d_nl_solve_batch(None, 0, None, None, None) == 1
+    # 3D nonlinear problem: grid, coordinates, gauge penalty, material arrays, curve, fields
+    r = _native.SilMag3dNlProblem()
+    r.nx, r.ny, r.nz = 4, 4, 2
+    r.x = r.y = r.z = x.ctypes.data
+    r.node_mu = r.node_ferro = 256
+    r.curve = _native.SilBHCurve(3, b.ctypes.data, h.ctypes.data)
+    r.gauge_penalty = 20.0
+    assert L.sil_mag3d_nl_apply(None, ctypes.byref(r), 256, 256) == 1
+    assert b"3x3x3" in L.sil_last_error()
+    r.nz = 4
+    r.gauge_penalty = 0.0
+    assert L.sil_mag3d_nl_apply(None, ctypes.byref(r), 256, 256) == 1
+    assert b"gauge_penalty" in L.sil_last_error()
+    r.gauge_penalty = 20.0
+    down = np.array([0.0, 0.5, 0.4, 1.0])
+    r.z = down.ctypes.data
+    assert L.sil_mag3d_nl_apply_jacobian(None, ctypes.byref(r), 256, 256, 256) == 1
+    assert b"increase strictly" in L.sil_last_error()
+    r.z = x.ctypes.data
+    r.node_ferro = None
+    assert L.sil_mag3d_nl_apply(None, ctypes.byref(r), 256, 256) == 1
+    assert b"NULL material" in L.sil_last_error()
+    r.node_ferro = 256
+    r.curve = _native.SilBHCurve(3, bad.ctypes.data, h.ctypes.data)
+    assert L.sil_mag3d_nl_apply(None, ctypes.byref(r), 256, 256) == 1
+    assert b"increase" in L.sil_last_error()
+    r.curve = _native.SilBHCurve(3, b.ctypes.data, h.ctypes.data)
+    r.rhs = None
+    assert L.sil_mag3d_nl_solve_batch(ctypes.byref(r), 1, ctypes.byref(st), diag, None) == 1
+    assert b"NULL field" in L.sil_last_error()
+    assert L.sil_mag3d_nl_solve_batch(None, 0, None, None, None) == 1
 
 
 def test_rank_and_component_checks_on_host():
