@@ -438,6 +438,87 @@ sil_status sil_mag3d_solve_batch(const sil_mag3d_problem* problems, int nproblem
                                  const sil_solve_settings* settings, sil_solve_diagnostics* diag,
                                  sil_stream stream);
 
+/* ---------------------------------------------------------------------- */
+/* Assembled operators: the magnetostatics operators as CSR matrices, the   */
+/* reference's preconditioner menu on them, and a preconditioned CG.       */
+
+/* CSR matrix in device memory (int32 row pointers and columns, FP64
+ * values, columns ascending, exact zeros dropped); opaque, owned by the
+ * library.
+ * Replaces: assemble_matrix_data, magnetostatics_onelab.hpp:3554-3737 (2D),
+ *   3120-3534 (3D), read into a gko::matrix::Csr<double, int32>. */
+typedef struct sil_csr_s* sil_csr;
+
+/* The 2D operator of sil_mag2d_apply as a CSR matrix.  Synchronous. */
+sil_status sil_mag2d_assemble(sil_stream stream, int64_t nx, int64_t ny, const double* node_mu, sil_csr* out);
+/* The 3D operator of sil_mag3d_apply (either gauge) as a CSR matrix.  Synchronous. */
+sil_status sil_mag3d_assemble(sil_stream stream, const sil_mag3d_problem* problem, sil_csr* out);
+/* Size and device arrays of a matrix (any output may be NULL). */
+sil_status sil_csr_get(sil_csr m, int64_t* n, int64_t* nnz, const int32_t** row_ptr, const int32_t** col,
+                       const double** val);
+/* Copies the arrays (n + 1 row pointers, nnz columns and values) to host or
+ * device buffers.  Synchronous. */
+sil_status sil_csr_copy(sil_stream stream, sil_csr m, int32_t* row_ptr, int32_t* col, double* val);
+/* y = A x (device vectors of n doubles). */
+sil_status sil_csr_spmv(sil_stream stream, sil_csr m, const double* x, double* y);
+void sil_csr_destroy(sil_csr m);
+
+/* The reference's PreconditionerType, in its order
+ * (minimize_strong_formulation_residual.hpp:53-63). */
+typedef enum sil_pc_kind {
+    SIL_PC_IDENTITY = 0,
+    SIL_PC_JACOBI = 1,
+    SIL_PC_SPD_ISAI = 2,
+    SIL_PC_SYMMETRIC_GAUSS_SEIDEL = 3,
+    SIL_PC_SSOR = 4,
+    SIL_PC_CHEBYSHEV_JACOBI = 5,
+    SIL_PC_IR_JACOBI = 6,
+    SIL_PC_GENERAL_ISAI = 7
+} sil_pc_kind;
+
+/* The menu's parameters; 0 selects the reference's default
+ * (StrongFormulationSolverSettings, minimize_strong_formulation_residual.hpp:
+ * 61-75): SOR relaxation 1.2, 8 Chebyshev steps on [0.05, 1.5], 8 IR steps
+ * with relaxation 1. */
+typedef struct sil_menu_settings {
+    int32_t kind;                  /* sil_pc_kind */
+    double sor_relaxation_factor;  /* Ssor */
+    int32_t chebyshev_iterations;
+    double chebyshev_lower_bound;  /* eigenvalue bounds of the Jacobi-preconditioned operator */
+    double chebyshev_upper_bound;
+    int32_t ir_iterations;
+    double ir_relaxation_factor;
+} sil_menu_settings;
+
+/* A preconditioner built on a matrix (which must outlive it): Jacobi
+ * z = D^-1 r; SpdIsai z = Z^T Z r with Z the factorized sparse approximate
+ * inverse on the pattern of tril(A); GeneralIsai z = M r with M the
+ * incomplete sparse approximate inverse on the pattern of A (ISAI rows of
+ * at most 32 entries); SymmetricGaussSeidel / Ssor the symmetric
+ * successive over-relaxation M = (D - wE) D^-1 (D - wF) / (w (2 - w)),
+ * w = 1 for Gauss-Seidel, its triangular solves run level by level;
+ * ChebyshevJacobi / IrJacobi a fixed number of Chebyshev / Richardson steps
+ * on the Jacobi-preconditioned system from a zero guess.  Synchronous.
+ * Replaces: build_preconditioner, minimize_strong_formulation_residual.hpp:
+ *   921-1026 (Ginkgo's Jacobi, SpdIsai, GeneralIsai, GaussSeidel, Sor,
+ *   Chebyshev and Ir). */
+typedef struct sil_csr_precond_s* sil_csr_precond;
+sil_status sil_csr_precond_create(sil_stream stream, sil_csr m, const sil_menu_settings* settings,
+                                  sil_csr_precond* out);
+/* z = M^-1 r (device vectors). */
+sil_status sil_csr_precond_apply(sil_stream stream, sil_csr_precond p, const double* r, double* z);
+void sil_csr_precond_destroy(sil_csr_precond p);
+
+/* Preconditioned CG from x = 0 until ||r|| <= tol ||b|| (recursive
+ * residual, as Ginkgo's ResidualNorm with a reduction factor) or
+ * settings->max_iterations; diag->iterations, converged, residuals.
+ * settings->solver is ignored.  Synchronous.
+ * Replaces: solve_linearized_system with the assembled matrix
+ *   (use_matrix_free = false), minimize_strong_formulation_residual.hpp:
+ *   1028-1304. */
+sil_status sil_csr_solve(sil_stream stream, sil_csr m, sil_csr_precond p, const double* rhs, double* x,
+                         const sil_solve_settings* settings, sil_solve_diagnostics* diag);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,11 @@ def lib():
         _lib.silo_mag3d_cg.argtypes = [i64, i64, i64, dp, dp, dp, dp, ctypes.c_double, dp, dp, ctypes.c_double,
                                        ctypes.c_int, dp]
         d = ctypes.c_double
+        ip = ctypes.POINTER(ctypes.c_int64)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        _lib.silo_csr_precond_apply.argtypes = [i64, ip, i32p, dp, ci, dp, dp, dp]
+        _lib.silo_csr_isai_values.argtypes = [i64, ip, i32p, dp, ci, dp]
+        _lib.silo_csr_pcg.argtypes = [i64, ip, i32p, dp, ci, dp, dp, dp, d, ci, dp]
         _lib.silo_mag3d_nl_apply.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp]
         _lib.silo_mag3d_nl_jacobian_apply.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp, dp]
         _lib.silo_mag3d_nl_jacobian_diagonal.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp]
@@ -401,3 +406,125 @@ def mag3d_nl_solve(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h, rhs, x
     it = lib().silo_mag3d_nl_solve(*args, _ptr(rhs), _ptr(sol), tol, max_iter, ctypes.byref(steps),
                                    ctypes.byref(rel))
     return sol, it, steps.value, rel.value
+
+
+# ----------------------------------------------------------------- assembled operators, preconditioner menu
+
+PRECONDITIONERS = {"identity": 0, "jacobi": 1, "spd-isai": 2, "symmetric-gauss-seidel": 3, "ssor": 4,
+                   "chebyshev-jacobi": 5, "ir-jacobi": 6, "general-isai": 7}
+MENU_DEFAULTS = {"sor_relaxation_factor": 1.2, "chebyshev_iterations": 8, "chebyshev_lower_bound": 0.05,
+                 "chebyshev_upper_bound": 1.5, "ir_iterations": 8, "ir_relaxation_factor": 1.0}
+
+
+def _probe_assemble(n, offsets_of_row, color_of, ncolors, apply):
+    """CSR of a linear operator whose row r only touches the columns
+    offsets_of_row(r) (sorted), by one apply per column colour (columns of one
+    colour never share a row).  Exact zeros are dropped, columns ascending."""
+    import scipy.sparse as sp
+    rows, cols, vals = [], [], []
+    colors = color_of(np.arange(n))
+    for k in range(ncolors):
+        probe = (colors == k).astype(np.float64)
+        y = apply(probe)
+        for r in range(n):
+            for c in offsets_of_row(r):
+                if colors[c] == k and y[r] != 0.0:
+                    rows.append(r)
+                    cols.append(c)
+                    vals.append(y[r])
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    A.sort_indices()
+    return A
+
+
+def assemble2d(nx, ny, node_mu):
+    """The 2D operator as a CSR matrix (the reference's assemble_matrix_data,
+    onelab_interface/magnetostatics_onelab.hpp:3554-3737), probed through
+    mag2d_apply: every row lies in the 3x3 node neighbourhood, so nine
+    colours (i mod 3, j mod 3) separate the columns of a row."""
+    def nbrs(r):
+        i, j = r % nx, r // nx
+        return [(i + di) + nx * (j + dj) for dj in (-1, 0, 1) for di in (-1, 0, 1)
+                if 0 <= i + di < nx and 0 <= j + dj < ny]
+    def color(c):
+        return (c % nx) % 3 + 3 * ((c // nx) % 3)
+    return _probe_assemble(nx * ny, nbrs, color, 9, lambda v: mag2d_apply(nx, ny, node_mu, v))
+
+
+def assemble3d(x, y, z, node_mu, gamma):
+    """The 3D operator as a CSR matrix (magnetostatics_onelab.hpp:3120-3534),
+    probed through mag3d_apply: rows lie in the 3x3x3 node neighbourhood, so
+    27 node colours times 3 components separate the columns of a row."""
+    nx, ny, nz = len(x), len(y), len(z)
+    def nbrs(r):
+        node, comp = divmod(r, 3)
+        i, j, k = node % nx, (node // nx) % ny, node // (nx * ny)
+        out = []
+        for dk in (-1, 0, 1):
+            for dj in (-1, 0, 1):
+                for di in (-1, 0, 1):
+                    if 0 <= i + di < nx and 0 <= j + dj < ny and 0 <= k + dk < nz:
+                        m = (i + di) + nx * ((j + dj) + ny * (k + dk))
+                        out.extend(3 * m + c for c in range(3))
+        return out
+    def color(c):
+        node, comp = c // 3, c % 3
+        i, j, k = node % nx, (node // nx) % ny, node // (nx * ny)
+        return comp + 3 * (i % 3 + 3 * (j % 3) + 9 * (k % 3))
+    return _probe_assemble(3 * nx * ny * nz, nbrs, color, 81, lambda v: mag3d_apply(x, y, z, node_mu, gamma, v))
+
+
+def _csr_args(A):
+    ptr = np.ascontiguousarray(A.indptr, dtype=np.int64)
+    col = np.ascontiguousarray(A.indices, dtype=np.int32)
+    val = np.ascontiguousarray(A.data, dtype=np.float64)
+    keep = (ptr, col, val)
+    args = [A.shape[0], ptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            col.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _ptr(val)]
+    return keep, args
+
+
+def _menu_params(**kw):
+    p = dict(MENU_DEFAULTS)
+    p.update(kw)
+    return np.array([p["sor_relaxation_factor"], p["chebyshev_iterations"], p["chebyshev_lower_bound"],
+                     p["chebyshev_upper_bound"], p["ir_iterations"], p["ir_relaxation_factor"]], dtype=np.float64)
+
+
+def csr_precond_apply(A, kind, r, **params):
+    keep, args = _csr_args(A)
+    pv = _menu_params(**params)
+    r = _f64(r)
+    z = np.zeros_like(r)
+    rc = lib().silo_csr_precond_apply(*args, PRECONDITIONERS[kind], _ptr(pv), _ptr(r), _ptr(z))
+    if rc != 0:
+        raise ValueError("singular ISAI system")
+    return z
+
+
+def csr_isai_values(A, kind):
+    """Values of the ISAI factor: Z on the pattern of tril(A) (spd-isai) or M on that of A (general-isai)."""
+    import scipy.sparse as sp
+    keep, args = _csr_args(A)
+    pat = sp.tril(A, format="csr") if kind == "spd-isai" else A.copy()
+    pat.sort_indices()
+    out = np.zeros(pat.nnz)
+    rc = lib().silo_csr_isai_values(*args, PRECONDITIONERS[kind], _ptr(out))
+    if rc != 0:
+        raise ValueError("singular ISAI system")
+    pat.data = out
+    return pat
+
+
+def csr_pcg(A, b, kind="jacobi", tol=1e-10, max_iter=100000, **params):
+    """Preconditioned CG from x = 0; returns (x, iterations, final relative residual)."""
+    keep, args = _csr_args(A)
+    pv = _menu_params(**params)
+    b = _f64(b)
+    x = np.zeros_like(b)
+    rel = ctypes.c_double(0.0)
+    it = lib().silo_csr_pcg(*args, PRECONDITIONERS[kind], _ptr(pv), _ptr(b), _ptr(x), tol, max_iter,
+                            ctypes.byref(rel))
+    if it < 0:
+        raise ValueError("singular ISAI system")
+    return x, it, rel.value

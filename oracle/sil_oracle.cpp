@@ -2067,3 +2067,309 @@ int silo_mag3d_nl_solve(int64_t nx, int64_t ny, int64_t nz, const double* x, con
             [&](const double* st, double* out) { op.diagonal(st, out); }, rhs, sol, tol, max_iter, newton_steps,
             final_rel);
 }
+
+// ------------------------------------------------------------------ assembled operators
+//
+// The reference's preconditioner menu on an assembled CSR matrix
+// (src/similie/solvers/minimize_strong_formulation_residual.hpp:53-63 names,
+// 61-75 defaults, 921-1026 construction through Ginkgo v1.11.0).  Ginkgo's
+// source is not available here; each preconditioner restates the published
+// algorithm it names:
+//   Jacobi            z = D^-1 r (block size 1)
+//   SpdIsai           factorized sparse approximate inverse (Kolotilina &
+//                     Yeremin): Z with the pattern of tril(A), row i solving
+//                     A(P_i, P_i) y = e_i and scaled by 1/sqrt(y_i); M = Z^T Z
+//   GeneralIsai       incomplete sparse approximate inverse (Anzt et al. 2018):
+//                     M with the pattern of A, (M A)(i, P_i) = e_i per row
+//   SymmetricGaussSeidel / Ssor
+//                     M = (D - w E) D^-1 (D - w F) / (w (2 - w)), A = D - E - F
+//                     (Saad, Iterative Methods for Sparse Linear Systems,
+//                     sec. 10.2), w = 1 for Gauss-Seidel; triangular solves
+//                     in row order
+//   ChebyshevJacobi   k steps of the Chebyshev iteration on the Jacobi-
+//                     preconditioned system with eigenvalue bounds [l, u] from
+//                     a zero guess (Saad, Algorithm 12.1)
+//   IrJacobi          k steps of x += w D^-1 (b - A x) from a zero guess
+// The CG is the one of silo_mag3d_cg with the preconditioner in place of
+// Jacobi.
+namespace {
+
+struct CsrView
+{
+    int64_t n;
+    const int64_t* ptr;
+    const int32_t* col;
+    const double* val;
+    double at(int64_t r, int64_t c) const
+    {
+        for (int64_t k = ptr[r]; k < ptr[r + 1]; ++k)
+            if (col[k] == c) return val[k];
+        return 0.0;
+    }
+};
+
+void spmv(CsrView const& A, const double* x, double* y)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < A.n; ++i) {
+        double s = 0.0;
+        for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) s += A.val[k] * x[A.col[k]];
+        y[i] = s;
+    }
+}
+
+// Solves G y = e_t (m x m, row-major) by Gaussian elimination with partial
+// pivoting; false if singular.
+bool dense_unit_solve(std::vector<double>& G, int m, int t, std::vector<double>& y)
+{
+    y.assign(m, 0.0);
+    y[t] = 1.0;
+    for (int c = 0; c < m; ++c) {
+        int p = c;
+        for (int r = c + 1; r < m; ++r)
+            if (std::fabs(G[r * m + c]) > std::fabs(G[p * m + c])) p = r;
+        if (G[p * m + c] == 0.0) return false;
+        if (p != c) {
+            for (int k = 0; k < m; ++k) std::swap(G[c * m + k], G[p * m + k]);
+            std::swap(y[c], y[p]);
+        }
+        for (int r = c + 1; r < m; ++r) {
+            double const f = G[r * m + c] / G[c * m + c];
+            for (int k = c; k < m; ++k) G[r * m + k] -= f * G[c * m + k];
+            y[r] -= f * y[c];
+        }
+    }
+    for (int r = m - 1; r >= 0; --r) {
+        double s = y[r];
+        for (int k = r + 1; k < m; ++k) s -= G[r * m + k] * y[k];
+        y[r] = s / G[r * m + r];
+    }
+    return true;
+}
+
+enum MenuKind
+{
+    kIdentity = 0,
+    kJacobi = 1,
+    kSpdIsai = 2,
+    kSymGaussSeidel = 3,
+    kSsor = 4,
+    kChebyshevJacobi = 5,
+    kIrJacobi = 6,
+    kGeneralIsai = 7
+};
+
+struct MenuPrecond
+{
+    CsrView A;
+    int kind;
+    double omega;
+    int cheb_iters;
+    double cheb_lo, cheb_hi;
+    int ir_iters;
+    double ir_omega;
+    std::vector<double> diag, dinv;
+    std::vector<int64_t> mptr;  // ISAI factor: Z (SpdIsai, lower) or M (GeneralIsai)
+    std::vector<int32_t> mcol;
+    std::vector<double> mval;
+    bool ok = true;
+
+    void setup()
+    {
+        int64_t const n = A.n;
+        diag.resize(n);
+        dinv.resize(n);
+        for (int64_t i = 0; i < n; ++i) {
+            diag[i] = A.at(i, i);
+            dinv[i] = 1.0 / diag[i];
+        }
+        if (kind != kSpdIsai && kind != kGeneralIsai) return;
+        mptr.assign(n + 1, 0);
+        for (int64_t i = 0; i < n; ++i) {
+            int64_t cnt = 0;
+            for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+                if (kind == kGeneralIsai || A.col[k] <= i) ++cnt;
+            mptr[i + 1] = mptr[i] + cnt;
+        }
+        mcol.resize(mptr[n]);
+        mval.resize(mptr[n]);
+        std::vector<double> G, y;
+        for (int64_t i = 0; i < n; ++i) {
+            std::vector<int32_t> P;
+            for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+                if (kind == kGeneralIsai || A.col[k] <= i) P.push_back(A.col[k]);
+            int const m = static_cast<int>(P.size());
+            G.assign(static_cast<size_t>(m) * m, 0.0);
+            int t = 0;
+            for (int a = 0; a < m; ++a) {
+                if (P[a] == i) t = a;
+                for (int b = 0; b < m; ++b)
+                    G[a * m + b] = kind == kSpdIsai ? A.at(P[a], P[b]) : A.at(P[b], P[a]);
+            }
+            if (!dense_unit_solve(G, m, t, y)) {
+                ok = false;
+                return;
+            }
+            double const scale = kind == kSpdIsai ? 1.0 / std::sqrt(y[t]) : 1.0;
+            for (int a = 0; a < m; ++a) {
+                mcol[mptr[i] + a] = P[a];
+                mval[mptr[i] + a] = kind == kSpdIsai ? y[a] * scale : y[a];
+            }
+        }
+    }
+
+    void apply(const double* r, double* z) const
+    {
+        int64_t const n = A.n;
+        switch (kind) {
+        case kIdentity:
+            std::copy(r, r + n, z);
+            return;
+        case kJacobi:
+            for (int64_t i = 0; i < n; ++i) z[i] = dinv[i] * r[i];
+            return;
+        case kSpdIsai: {
+            std::vector<double> t(n, 0.0);
+            for (int64_t i = 0; i < n; ++i) {
+                double s = 0.0;
+                for (int64_t k = mptr[i]; k < mptr[i + 1]; ++k) s += mval[k] * r[mcol[k]];
+                t[i] = s;
+            }
+            std::fill(z, z + n, 0.0);
+            for (int64_t i = 0; i < n; ++i)
+                for (int64_t k = mptr[i]; k < mptr[i + 1]; ++k) z[mcol[k]] += mval[k] * t[i];
+            return;
+        }
+        case kGeneralIsai:
+            for (int64_t i = 0; i < n; ++i) {
+                double s = 0.0;
+                for (int64_t k = mptr[i]; k < mptr[i + 1]; ++k) s += mval[k] * r[mcol[k]];
+                z[i] = s;
+            }
+            return;
+        case kSymGaussSeidel:
+        case kSsor: {
+            double const w = kind == kSsor ? omega : 1.0;
+            double const c = w * (2.0 - w);
+            std::vector<double> y(n);
+            for (int64_t i = 0; i < n; ++i) {
+                double s = c * r[i];
+                for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+                    if (A.col[k] < i) s -= w * A.val[k] * y[A.col[k]];
+                y[i] = s / diag[i];
+            }
+            for (int64_t i = n - 1; i >= 0; --i) {
+                double s = diag[i] * y[i];
+                for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+                    if (A.col[k] > i) s -= w * A.val[k] * z[A.col[k]];
+                z[i] = s / diag[i];
+            }
+            return;
+        }
+        case kChebyshevJacobi: {
+            double const theta = 0.5 * (cheb_hi + cheb_lo), delta = 0.5 * (cheb_hi - cheb_lo);
+            double const sigma = theta / delta;
+            double rho = 1.0 / sigma;
+            std::vector<double> d(n), res(n), ax(n);
+            for (int64_t i = 0; i < n; ++i) {
+                d[i] = dinv[i] * r[i] / theta;
+                z[i] = d[i];
+            }
+            for (int it = 1; it < cheb_iters; ++it) {
+                spmv(A, z, ax.data());
+                double const rho1 = 1.0 / (2.0 * sigma - rho);
+                for (int64_t i = 0; i < n; ++i) {
+                    res[i] = r[i] - ax[i];
+                    d[i] = rho1 * rho * d[i] + (2.0 * rho1 / delta) * (dinv[i] * res[i]);
+                    z[i] += d[i];
+                }
+                rho = rho1;
+            }
+            return;
+        }
+        case kIrJacobi: {
+            std::vector<double> ax(n);
+            for (int64_t i = 0; i < n; ++i) z[i] = ir_omega * (dinv[i] * r[i]);
+            for (int it = 1; it < ir_iters; ++it) {
+                spmv(A, z, ax.data());
+                for (int64_t i = 0; i < n; ++i) z[i] += ir_omega * (dinv[i] * (r[i] - ax[i]));
+            }
+            return;
+        }
+        }
+    }
+};
+
+MenuPrecond make_menu(CsrView A, int kind, const double* params)
+{
+    MenuPrecond m {A, kind, params[0], static_cast<int>(params[1]), params[2], params[3],
+                   static_cast<int>(params[4]), params[5]};
+    m.setup();
+    return m;
+}
+
+} // namespace
+
+// params: sor relaxation factor, Chebyshev iterations, lower bound, upper
+// bound, IR iterations, IR relaxation factor.  Returns 0, or -1 when an ISAI
+// system is singular.
+int silo_csr_precond_apply(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int kind,
+                           const double* params, const double* r, double* z)
+{
+    MenuPrecond const m = make_menu(CsrView {n, ptr, col, val}, kind, params);
+    if (!m.ok) return -1;
+    m.apply(r, z);
+    return 0;
+}
+
+// The ISAI factor's values in its pattern (tril(A) for SpdIsai, A for
+// GeneralIsai): out_val holds one value per pattern entry in row order.
+int silo_csr_isai_values(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int kind,
+                         double* out_val)
+{
+    double const params[6] = {1.2, 8, 0.05, 1.5, 8, 1.0};
+    MenuPrecond const m = make_menu(CsrView {n, ptr, col, val}, kind, params);
+    if (!m.ok) return -1;
+    std::copy(m.mval.begin(), m.mval.end(), out_val);
+    return 0;
+}
+
+// Preconditioned CG from x = 0 until ||r|| <= tol ||b||; returns the
+// iterations (-1 when the preconditioner cannot be built).
+int silo_csr_pcg(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int kind, const double* params,
+                 const double* b, double* x, double tol, int max_iter, double* final_rel)
+{
+    CsrView const A {n, ptr, col, val};
+    MenuPrecond const m = make_menu(A, kind, params);
+    if (!m.ok) return -1;
+    std::vector<double> r(b, b + n), z(n), p(n), q(n);
+    std::fill(x, x + n, 0.0);
+    double const bnorm = nrm2(n, b);
+    if (bnorm == 0.0) {
+        *final_rel = 0.0;
+        return 0;
+    }
+    m.apply(r.data(), z.data());
+    p = z;
+    double rz = dotp(n, r.data(), z.data());
+    double rnorm = bnorm;
+    int it = 0;
+    while (it < max_iter) {
+        spmv(A, p.data(), q.data());
+        double const alpha = rz / dotp(n, p.data(), q.data());
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * q[i];
+        }
+        ++it;
+        rnorm = nrm2(n, r.data());
+        if (rnorm <= tol * bnorm) break;
+        m.apply(r.data(), z.data());
+        double const rz2 = dotp(n, r.data(), z.data());
+        double const beta = rz2 / rz;
+        rz = rz2;
+        for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+    }
+    *final_rel = rnorm / bnorm;
+    return it;
+}

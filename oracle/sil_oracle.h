@@ -165,6 +165,19 @@ int silo_mag3d_nl_solve(int64_t nx, int64_t ny, int64_t nz, const double* x, con
                         const double* h, const double* rhs, double* sol, double tol, int max_iter, int* newton_steps,
                         double* final_rel);
 
+/* ------------------------------------------------------------------ */
+/* Assembled CSR operators (int64 row pointers, int32 columns) and the   */
+/* reference's preconditioner menu: kind 0 Identity, 1 Jacobi, 2 SpdIsai, */
+/* 3 SymmetricGaussSeidel, 4 Ssor, 5 ChebyshevJacobi, 6 IrJacobi,         */
+/* 7 GeneralIsai.  params: sor relaxation factor, Chebyshev iterations,   */
+/* lower and upper bound, IR iterations, IR relaxation factor.            */
+int silo_csr_precond_apply(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int kind,
+                           const double* params, const double* r, double* z);
+int silo_csr_isai_values(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int kind,
+                         double* out_val);
+int silo_csr_pcg(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int kind, const double* params,
+                 const double* b, double* x, double tol, int max_iter, double* final_rel);
+
 /* Threads OpenMP uses (for reporting). */
 int silo_num_threads(void);
 

@@ -96,6 +96,18 @@ class SilMag3dNlProblem(ctypes.Structure):
     ]
 
 
+class SilMenuSettings(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("sor_relaxation_factor", ctypes.c_double),
+        ("chebyshev_iterations", ctypes.c_int32),
+        ("chebyshev_lower_bound", ctypes.c_double),
+        ("chebyshev_upper_bound", ctypes.c_double),
+        ("ir_iterations", ctypes.c_int32),
+        ("ir_relaxation_factor", ctypes.c_double),
+    ]
+
+
 class SilPrecondSample(ctypes.Structure):
     _fields_ = [
         ("nx", ctypes.c_int32),
@@ -191,6 +203,18 @@ SIGNATURES = [
     ("sil_mag3d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag3dProblem), ctypes.c_int,
                                              ctypes.POINTER(SilSolveSettings),
                                              ctypes.POINTER(SilSolveDiagnostics), _P]),
+    ("sil_mag2d_assemble", ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, ctypes.POINTER(_P)]),
+    ("sil_mag3d_assemble", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dProblem), ctypes.POINTER(_P)]),
+    ("sil_csr_get", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                   ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P)]),
+    ("sil_csr_copy", ctypes.c_int, [_P, _P, _P, _P, _P]),
+    ("sil_csr_spmv", ctypes.c_int, [_P, _P, _P, _P]),
+    ("sil_csr_destroy", None, [_P]),
+    ("sil_csr_precond_create", ctypes.c_int, [_P, _P, ctypes.POINTER(SilMenuSettings), ctypes.POINTER(_P)]),
+    ("sil_csr_precond_apply", ctypes.c_int, [_P, _P, _P, _P]),
+    ("sil_csr_precond_destroy", None, [_P]),
+    ("sil_csr_solve", ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.POINTER(SilSolveSettings),
+                                     ctypes.POINTER(SilSolveDiagnostics)]),
     ("sil_mag3d_nl_apply", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dNlProblem), _P, _P]),
     ("sil_mag3d_nl_apply_jacobian", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dNlProblem), _P, _P, _P]),
     ("sil_mag3d_nl_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag3dNlProblem), ctypes.c_int,

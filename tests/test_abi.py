@@ -162,6 +162,31 @@ def test_gauge_and_nonlinear_arguments_checked_on_host():
     assert L.sil_mag3d_nl_solve_batch(None, 0, None, None, None) == 1
 
 
+def test_assembled_path_arguments_checked_on_host():
+    L = sil.lib()
+    h = ctypes.c_void_p()
+    assert L.sil_mag2d_assemble(None, 8, 8, None, ctypes.byref(h)) == 1
+    assert L.sil_mag2d_assemble(None, 2, 8, 256, ctypes.byref(h)) == 1
+    assert b"3x3" in L.sil_last_error()
+    p = _native.SilMag3dProblem()
+    p.nx, p.ny, p.nz = 4, 4, 2
+    assert L.sil_mag3d_assemble(None, ctypes.byref(p), ctypes.byref(h)) == 1
+    assert b"3x3x3" in L.sil_last_error()
+    assert L.sil_csr_get(None, None, None, None, None, None) == 1
+    assert L.sil_csr_spmv(None, None, 256, 256) == 1
+    assert L.sil_csr_copy(None, None, 256, 256, 256) == 1
+    cfg = _native.SilMenuSettings()
+    assert L.sil_csr_precond_create(None, None, ctypes.byref(cfg), ctypes.byref(h)) == 1
+    assert L.sil_csr_precond_apply(None, None, 256, 256) == 1
+    st = _native.SilSolveSettings()
+    d = _native.SilSolveDiagnostics()
+    assert L.sil_csr_solve(None, None, None, 256, 256, ctypes.byref(st), ctypes.byref(d)) == 1
+    L.sil_csr_destroy(None)
+    L.sil_csr_precond_destroy(None)
+    import similie_b200.assembled as asm
+    assert asm.kind_of("SSOR") == 4 and asm.kind_of("isai") == 7 and asm.kind_of("spd_isai") == 2
+
+
 def test_rank_and_component_checks_on_host():
     L = sil.lib()
     fi = _native.SilField()
