@@ -18,6 +18,8 @@
 //   solvers::minimize_strong_formulation_residual(        minimize_strong_formulation_residual(
 //     exec, operator_model, rhs, solution, settings)        exec, operator_model, rhs, solution, settings)
 //     solvers/minimize_strong_formulation_residual.hpp:1308-1570
+//   assemble_matrix_data(operator_model)                  assemble_matrix_data(exec, operator_model)
+//     onelab_interface/magnetostatics_onelab.hpp:3120-3748
 //
 // The reference's tags become the form degree K (a template argument) and
 // the dimension (the field's); its DDC tensor spans become Tensor, a
@@ -216,14 +218,77 @@ StagedLaplacian<K> make_staged_laplacian(ExecSpace, Geometry const& geometry, Te
 
 // ------------------------------------------------------------------ solvers
 
-// solvers/minimize_strong_formulation_residual.hpp: the settings this path reads.
+// solvers/minimize_strong_formulation_residual.hpp:53-63: the preconditioner
+// menu, in the reference's order and with its spellings.
+enum class PreconditionerType
+{
+    Identity,
+    Jacobi,
+    SpdIsai,
+    SymmetricGaussSeidel,
+    Ssor,
+    ChebyshevJacobi,
+    IrJacobi,
+    GeneralIsai,
+};
+
+inline PreconditionerType parse_preconditioner(std::string const& name)
+{
+    struct Entry
+    {
+        char const* name;
+        PreconditionerType type;
+    };
+    static Entry const table[] = {
+            {"Identity", PreconditionerType::Identity},
+            {"identity", PreconditionerType::Identity},
+            {"Jacobi", PreconditionerType::Jacobi},
+            {"jacobi", PreconditionerType::Jacobi},
+            {"SpdIsai", PreconditionerType::SpdIsai},
+            {"spd-isai", PreconditionerType::SpdIsai},
+            {"spd_isai", PreconditionerType::SpdIsai},
+            {"SymmetricGaussSeidel", PreconditionerType::SymmetricGaussSeidel},
+            {"symmetric-gauss-seidel", PreconditionerType::SymmetricGaussSeidel},
+            {"symmetric_gauss_seidel", PreconditionerType::SymmetricGaussSeidel},
+            {"Ssor", PreconditionerType::Ssor},
+            {"SSOR", PreconditionerType::Ssor},
+            {"ssor", PreconditionerType::Ssor},
+            {"ChebyshevJacobi", PreconditionerType::ChebyshevJacobi},
+            {"chebyshev-jacobi", PreconditionerType::ChebyshevJacobi},
+            {"chebyshev_jacobi", PreconditionerType::ChebyshevJacobi},
+            {"IrJacobi", PreconditionerType::IrJacobi},
+            {"ir-jacobi", PreconditionerType::IrJacobi},
+            {"ir_jacobi", PreconditionerType::IrJacobi},
+            {"GeneralIsai", PreconditionerType::GeneralIsai},
+            {"general-isai", PreconditionerType::GeneralIsai},
+            {"general_isai", PreconditionerType::GeneralIsai},
+            {"isai", PreconditionerType::GeneralIsai},
+    };
+    for (Entry const& e : table)
+        if (name == e.name) return e.type;
+    throw std::runtime_error("unknown strong-formulation preconditioner: " + name);
+}
+
+// solvers/minimize_strong_formulation_residual.hpp:61-75: the settings this
+// path reads, with the reference's defaults for the menu.
 struct StrongFormulationSolverSettings
 {
     double relative_tolerance = 1e-10;
     unsigned int max_iterations = 100000;
-    // Jacobi-CG in FP64 (the reference's), or FP32 inner CG with FP64
-    // refinement; linear operators only.
+    // matrix-free Jacobi-CG in FP64 (the reference's default), or FP32 inner
+    // CG with FP64 refinement; linear matrix-free solves only.
     bool mixed_precision = false;
+    // false, or any preconditioner but Jacobi: the linear solve assembles
+    // the operator (sil_mag2d/3d_assemble) and runs CG with the chosen
+    // preconditioner on it.  Nonlinear solves use Jacobi-CG.
+    bool use_matrix_free = true;
+    PreconditionerType preconditioner = PreconditionerType::Jacobi;
+    double sor_relaxation_factor = 1.2;
+    unsigned int chebyshev_iterations = 8;
+    double chebyshev_lower_bound = 0.05;
+    double chebyshev_upper_bound = 1.5;
+    unsigned int ir_iterations = 8;
+    double ir_relaxation_factor = 1.0;
 };
 
 struct StrongFormulationSolverDiagnostics
@@ -257,6 +322,7 @@ struct MagnetostaticsOperator3D
     std::vector<double> x, y, z;  // node coordinates (host)
     double const* node_mu;
     double gauge_penalty = 20.0;
+    bool divergence_gauge = false;  // SIMILIE_DIVERGENCE_GAUGE_3D
     int64_t size() const { return 3 * static_cast<int64_t>(x.size() * y.size() * z.size()); }
     sil_mag3d_problem problem(double const* rhs = nullptr, double* solution = nullptr) const
     {
@@ -271,6 +337,7 @@ struct MagnetostaticsOperator3D
         p.rhs = rhs;
         p.solution = solution;
         p.gauge_penalty = gauge_penalty;
+        p.gauge = divergence_gauge ? 1 : 0;
         return p;
     }
     void apply(ExecSpace exec, double const* in, double* out) const
@@ -314,6 +381,98 @@ struct NonlinearMagnetostaticsOperator2D
     }
 };
 
+struct NonlinearMagnetostaticsOperator3D
+{
+    static constexpr bool IS_LINEAR = false;
+    std::vector<double> x, y, z;  // node coordinates (host)
+    double const* node_mu;
+    double const* node_ferro;
+    std::vector<double> curve_b, curve_h;  // B-H samples (host)
+    double gauge_penalty = 20.0;
+    int64_t size() const { return 3 * static_cast<int64_t>(x.size() * y.size() * z.size()); }
+    sil_mag3d_nl_problem problem(double const* rhs = nullptr, double* solution = nullptr) const
+    {
+        sil_mag3d_nl_problem p {};
+        p.nx = static_cast<int64_t>(x.size());
+        p.ny = static_cast<int64_t>(y.size());
+        p.nz = static_cast<int64_t>(z.size());
+        p.x = x.data();
+        p.y = y.data();
+        p.z = z.data();
+        p.node_mu = node_mu;
+        p.node_ferro = node_ferro;
+        p.curve.n = static_cast<int32_t>(curve_b.size());
+        p.curve.b = curve_b.data();
+        p.curve.h = curve_h.data();
+        p.rhs = rhs;
+        p.solution = solution;
+        p.gauge_penalty = gauge_penalty;
+        return p;
+    }
+    void apply(ExecSpace exec, double const* in, double* out) const
+    {
+        sil_mag3d_nl_problem const p = problem();
+        check(sil_mag3d_nl_apply(exec.stream, &p, in, out), "NonlinearMagnetostaticsOperator3D::apply");
+    }
+    void apply_jacobian(ExecSpace exec, double const* state, double const* in, double* out) const
+    {
+        sil_mag3d_nl_problem const p = problem();
+        check(sil_mag3d_nl_apply_jacobian(exec.stream, &p, state, in, out), "apply_jacobian");
+    }
+};
+
+// An assembled operator (the reference's assemble_matrix_data read into a
+// Csr<double, int32>); owns the library's matrix.
+class CsrMatrix
+{
+public:
+    explicit CsrMatrix(sil_csr m) : m_(m) {}
+    CsrMatrix(CsrMatrix&& o) noexcept : m_(o.m_) { o.m_ = nullptr; }
+    CsrMatrix& operator=(CsrMatrix&& o) noexcept
+    {
+        std::swap(m_, o.m_);
+        return *this;
+    }
+    CsrMatrix(CsrMatrix const&) = delete;
+    CsrMatrix& operator=(CsrMatrix const&) = delete;
+    ~CsrMatrix() { sil_csr_destroy(m_); }
+    sil_csr get() const { return m_; }
+    int64_t rows() const
+    {
+        int64_t n = 0;
+        check(sil_csr_get(m_, &n, nullptr, nullptr, nullptr, nullptr), "CsrMatrix::rows");
+        return n;
+    }
+    int64_t nonzeros() const
+    {
+        int64_t nnz = 0;
+        check(sil_csr_get(m_, nullptr, &nnz, nullptr, nullptr, nullptr), "CsrMatrix::nonzeros");
+        return nnz;
+    }
+    void apply(ExecSpace exec, double const* in, double* out) const
+    {
+        check(sil_csr_spmv(exec.stream, m_, in, out), "CsrMatrix::apply");
+    }
+
+private:
+    sil_csr m_ = nullptr;
+};
+
+inline CsrMatrix assemble_matrix_data(ExecSpace exec, MagnetostaticsOperator2D const& op)
+{
+    sil_csr m = nullptr;
+    check(sil_mag2d_assemble(exec.stream, op.nx, op.ny, op.node_mu, &m), "assemble_matrix_data");
+    return CsrMatrix(m);
+}
+
+inline CsrMatrix assemble_matrix_data(ExecSpace exec, MagnetostaticsOperator3D const& op)
+{
+    sil_mag3d_problem const p = op.problem();
+    sil_csr m = nullptr;
+    check(sil_mag3d_assemble(exec.stream, &p, &m), "assemble_matrix_data");
+    return CsrMatrix(m);
+}
+
 namespace detail {
 
 inline sil_solve_settings to_settings(StrongFormulationSolverSettings const& s)
@@ -337,6 +496,35 @@ inline StrongFormulationSolverDiagnostics to_diagnostics(sil_solve_diagnostics c
     return r;
 }
 
+inline bool assembled(StrongFormulationSolverSettings const& s)
+{
+    return !s.use_matrix_free || s.preconditioner != PreconditionerType::Jacobi;
+}
+
+// CG with the chosen preconditioner on the assembled matrix
+// (solve_linearized_system with an assembled system matrix).
+inline StrongFormulationSolverDiagnostics solve_assembled(ExecSpace exec, CsrMatrix const& m, double const* rhs,
+                                                          double* solution,
+                                                          StrongFormulationSolverSettings const& settings)
+{
+    sil_menu_settings cfg {};
+    cfg.kind = static_cast<int32_t>(settings.preconditioner);
+    cfg.sor_relaxation_factor = settings.sor_relaxation_factor;
+    cfg.chebyshev_iterations = static_cast<int32_t>(settings.chebyshev_iterations);
+    cfg.chebyshev_lower_bound = settings.chebyshev_lower_bound;
+    cfg.chebyshev_upper_bound = settings.chebyshev_upper_bound;
+    cfg.ir_iterations = static_cast<int32_t>(settings.ir_iterations);
+    cfg.ir_relaxation_factor = settings.ir_relaxation_factor;
+    sil_csr_precond pc = nullptr;
+    check(sil_csr_precond_create(exec.stream, m.get(), &cfg, &pc), "build_preconditioner");
+    sil_solve_settings const s = to_settings(settings);
+    sil_solve_diagnostics d {};
+    sil_status const st = sil_csr_solve(exec.stream, m.get(), pc, rhs, solution, &s, &d);
+    sil_csr_precond_destroy(pc);
+    check(st, "minimize_strong_formulation_residual");
+    return to_diagnostics(d, false);
+}
+
 }  // namespace detail
 
 // The linear solves start from x = 0 (as the reference's); the nonlinear
@@ -345,6 +533,8 @@ inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
         ExecSpace exec, MagnetostaticsOperator2D const& op, double const* rhs, double* solution,
         StrongFormulationSolverSettings const& settings)
 {
+    if (detail::assembled(settings))
+        return detail::solve_assembled(exec, assemble_matrix_data(exec, op), rhs, solution, settings);
     sil_mag2d_problem p {op.nx, op.ny, op.node_mu, rhs, solution};
     sil_solve_settings const s = detail::to_settings(settings);
     sil_solve_diagnostics d {};
@@ -356,6 +546,8 @@ inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
         ExecSpace exec, MagnetostaticsOperator3D const& op, double const* rhs, double* solution,
         StrongFormulationSolverSettings const& settings)
 {
+    if (detail::assembled(settings))
+        return detail::solve_assembled(exec, assemble_matrix_data(exec, op), rhs, solution, settings);
     sil_mag3d_problem const p = op.problem(rhs, solution);
     sil_solve_settings const s = detail::to_settings(settings);
     sil_solve_diagnostics d {};
@@ -371,6 +563,17 @@ inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
     sil_solve_settings const s = detail::to_settings(settings);
     sil_solve_diagnostics d {};
     check(sil_mag2d_nl_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
+    return detail::to_diagnostics(d, true);
+}
+
+inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
+        ExecSpace exec, NonlinearMagnetostaticsOperator3D const& op, double const* rhs, double* solution,
+        StrongFormulationSolverSettings const& settings)
+{
+    sil_mag3d_nl_problem const p = op.problem(rhs, solution);
+    sil_solve_settings const s = detail::to_settings(settings);
+    sil_solve_diagnostics d {};
+    check(sil_mag3d_nl_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
     return detail::to_diagnostics(d, true);
 }
 

@@ -97,6 +97,21 @@ int main(int argc, char** argv)
         } catch (Error const& e) {
             std::printf("error %d\n", static_cast<int>(e.status));
         }
+
+        // the same solve on the assembled matrix with the reference's SSOR
+        // (SIMILIE_PRECONDITIONER=ssor, use_matrix_free = false)
+        StrongFormulationSolverSettings assembled;
+        assembled.relative_tolerance = 1e-10;
+        assembled.use_matrix_free = false;
+        assembled.preconditioner = parse_preconditioner("ssor");
+        double* d_sol2 = to_device(std::vector<double>(n * n, 0.0));
+        StrongFormulationSolverDiagnostics const diag2 =
+                minimize_strong_formulation_residual(exec, op, d_rhs, d_sol2, assembled);
+        CsrMatrix const matrix = assemble_matrix_data(exec, op);
+        cudaDeviceSynchronize();
+        write(dir + "/sol_ssor.bin", to_host(d_sol2, n * n));
+        std::printf("assembled %u %d %.6e %lld\n", diag2.iterations, diag2.converged ? 1 : 0,
+                    diag2.final_relative_residual, static_cast<long long>(matrix.nonzeros()));
     } catch (Error const& e) {
         std::fprintf(stderr, "%s\n", e.what());
         return 1;

@@ -38,6 +38,11 @@ def test_example_matches_the_oracle(tmp_path):
     it, conv, rel = out[0].split()
     assert int(conv) == 1 and float(rel) <= 1e-10
     assert out[1].startswith("error 1")       # k = 3 on a 2D field: SIL_ERR_INVALID
+    tag, it2, conv2, rel2, nnz = out[2].split()
+    assert tag == "assembled" and int(conv2) == 1 and float(rel2) <= 1e-10
+    assert int(it2) < int(it)                  # SSOR needs fewer iterations than Jacobi
+    ref_nnz = O.assemble2d(33, 33, rd_mu(tmp_path)).nnz  # up to entries cancelling to exactly zero in one arithmetic
+    assert abs(int(nnz) - ref_nnz) <= ref_nnz // 100
     rd = lambda name: np.fromfile(str(tmp_path / name), dtype=np.float64)
     nx, ny = 12, 9
     phi = rd("phi.bin").reshape(nx, ny, 1)
@@ -51,3 +56,9 @@ def test_example_matches_the_oracle(tmp_path):
     n = 33
     r = rd("rhs.bin") - O.mag2d_apply(n, n, rd("mu.bin"), rd("sol.bin"))
     assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(rd("rhs.bin"))
+    r2 = rd("rhs.bin") - O.mag2d_apply(n, n, rd("mu.bin"), rd("sol_ssor.bin"))
+    assert np.linalg.norm(r2) <= 2e-10 * np.linalg.norm(rd("rhs.bin"))
+
+
+def rd_mu(tmp_path):
+    return np.fromfile(str(tmp_path / "mu.bin"), dtype=np.float64)
