@@ -279,8 +279,8 @@ struct StrongFormulationSolverSettings
     // CG with FP64 refinement; linear matrix-free solves only.
     bool mixed_precision = false;
     // false, or any preconditioner but Jacobi: the linear solve assembles
-    // the operator (sil_mag2d/3d_assemble) and runs CG with the chosen
-    // preconditioner on it.  Nonlinear solves use Jacobi-CG.
+    // the operator (sil_mag2d/3d_assemble), a nonlinear solve its Jacobian
+    // at every Newton step, and CG runs with the chosen preconditioner.
     bool use_matrix_free = true;
     PreconditionerType preconditioner = PreconditionerType::Jacobi;
     double sor_relaxation_factor = 1.2;
@@ -501,11 +501,7 @@ inline bool assembled(StrongFormulationSolverSettings const& s)
     return !s.use_matrix_free || s.preconditioner != PreconditionerType::Jacobi;
 }
 
-// CG with the chosen preconditioner on the assembled matrix
-// (solve_linearized_system with an assembled system matrix).
-inline StrongFormulationSolverDiagnostics solve_assembled(ExecSpace exec, CsrMatrix const& m, double const* rhs,
-                                                          double* solution,
-                                                          StrongFormulationSolverSettings const& settings)
+inline sil_menu_settings to_menu(StrongFormulationSolverSettings const& settings)
 {
     sil_menu_settings cfg {};
     cfg.kind = static_cast<int32_t>(settings.preconditioner);
@@ -515,6 +511,16 @@ inline StrongFormulationSolverDiagnostics solve_assembled(ExecSpace exec, CsrMat
     cfg.chebyshev_upper_bound = settings.chebyshev_upper_bound;
     cfg.ir_iterations = static_cast<int32_t>(settings.ir_iterations);
     cfg.ir_relaxation_factor = settings.ir_relaxation_factor;
+    return cfg;
+}
+
+// CG with the chosen preconditioner on the assembled matrix
+// (solve_linearized_system with an assembled system matrix).
+inline StrongFormulationSolverDiagnostics solve_assembled(ExecSpace exec, CsrMatrix const& m, double const* rhs,
+                                                          double* solution,
+                                                          StrongFormulationSolverSettings const& settings)
+{
+    sil_menu_settings const cfg = to_menu(settings);
     sil_csr_precond pc = nullptr;
     check(sil_csr_precond_create(exec.stream, m.get(), &cfg, &pc), "build_preconditioner");
     sil_solve_settings const s = to_settings(settings);
@@ -560,7 +566,9 @@ inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
         StrongFormulationSolverSettings const& settings)
 {
     sil_mag2d_nl_problem const p = op.problem(rhs, solution);
-    sil_solve_settings const s = detail::to_settings(settings);
+    sil_solve_settings s = detail::to_settings(settings);
+    sil_menu_settings const menu = detail::to_menu(settings);
+    if (detail::assembled(settings)) s.jacobian_preconditioner = &menu;
     sil_solve_diagnostics d {};
     check(sil_mag2d_nl_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
     return detail::to_diagnostics(d, true);
@@ -571,7 +579,9 @@ inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
         StrongFormulationSolverSettings const& settings)
 {
     sil_mag3d_nl_problem const p = op.problem(rhs, solution);
-    sil_solve_settings const s = detail::to_settings(settings);
+    sil_solve_settings s = detail::to_settings(settings);
+    sil_menu_settings const menu = detail::to_menu(settings);
+    if (detail::assembled(settings)) s.jacobian_preconditioner = &menu;
     sil_solve_diagnostics d {};
     check(sil_mag3d_nl_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
     return detail::to_diagnostics(d, true);

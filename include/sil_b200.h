@@ -236,6 +236,12 @@ typedef struct sil_solve_settings {
     sil_precond preconditioner;  /* LEARNED: the trained network */
     int32_t stall_window;        /* LEARNED: iterations per stall check (0: 200) */
     int32_t flexible_directions; /* LEARNED: directions the flexible CG keeps, 1..16 (0: 8) */
+    /* Nonlinear solves: NULL runs every Newton step's linear solve as the
+     * matrix-free Jacobi-CG; otherwise the Jacobian is assembled at the state
+     * every step and CG runs with this preconditioner of the menu (the
+     * reference's nonlinear branch with build_matrix + build_preconditioner,
+     * minimize_strong_formulation_residual.hpp:1432-1436). */
+    const struct sil_menu_settings* jacobian_preconditioner;
 } sil_solve_settings;
 
 typedef struct sil_solve_diagnostics {
@@ -453,6 +459,12 @@ typedef struct sil_csr_s* sil_csr;
 sil_status sil_mag2d_assemble(sil_stream stream, int64_t nx, int64_t ny, const double* node_mu, sil_csr* out);
 /* The 3D operator of sil_mag3d_apply (either gauge) as a CSR matrix.  Synchronous. */
 sil_status sil_mag3d_assemble(sil_stream stream, const sil_mag3d_problem* problem, sil_csr* out);
+/* The Jacobians of the nonlinear operators at `state` (device) as CSR
+ * matrices (assemble_matrix_data(operator_model, state)).  Synchronous. */
+sil_status sil_mag2d_nl_assemble_jacobian(sil_stream stream, const sil_mag2d_nl_problem* problem,
+                                          const double* state, sil_csr* out);
+sil_status sil_mag3d_nl_assemble_jacobian(sil_stream stream, const sil_mag3d_nl_problem* problem,
+                                          const double* state, sil_csr* out);
 /* Size and device arrays of a matrix (any output may be NULL). */
 sil_status sil_csr_get(sil_csr m, int64_t* n, int64_t* nnz, const int32_t** row_ptr, const int32_t** col,
                        const double** val);

@@ -76,6 +76,10 @@ def lib():
         _lib.silo_csr_precond_apply.argtypes = [i64, ip, i32p, dp, ci, dp, dp, dp]
         _lib.silo_csr_isai_values.argtypes = [i64, ip, i32p, dp, ci, dp]
         _lib.silo_csr_pcg.argtypes = [i64, ip, i32p, dp, ci, dp, dp, dp, d, ci, dp]
+        _lib.silo_mag2d_nl_solve_menu.argtypes = [i64, i64, dp, dp, ci, dp, dp, ci, dp, dp, dp, d, ci,
+                                                  ctypes.POINTER(ci), dp]
+        _lib.silo_mag3d_nl_solve_menu.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, ci, dp, dp, dp,
+                                                  d, ci, ctypes.POINTER(ci), dp]
         _lib.silo_mag3d_nl_apply.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp]
         _lib.silo_mag3d_nl_jacobian_apply.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp, dp]
         _lib.silo_mag3d_nl_jacobian_diagonal.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, dp, dp]
@@ -528,3 +532,47 @@ def csr_pcg(A, b, kind="jacobi", tol=1e-10, max_iter=100000, **params):
     if it < 0:
         raise ValueError("singular ISAI system")
     return x, it, rel.value
+
+
+def jacobian2d_csr(nx, ny, node_mu, node_ferro, curve_b, curve_h, state):
+    """The 2D nonlinear operator's Jacobian at `state` as a CSR matrix (probed)."""
+    def nbrs(r):
+        i, j = r % nx, r // nx
+        return [(i + di) + nx * (j + dj) for dj in (-1, 0, 1) for di in (-1, 0, 1)
+                if 0 <= i + di < nx and 0 <= j + dj < ny]
+    def color(c):
+        return (c % nx) % 3 + 3 * ((c // nx) % 3)
+    return _probe_assemble(nx * ny, nbrs, color, 9,
+                           lambda v: mag2d_nl_jacobian_apply(nx, ny, node_mu, node_ferro, curve_b, curve_h, state, v))
+
+
+def mag2d_nl_solve_menu(nx, ny, node_mu, node_ferro, curve_b, curve_h, rhs, kind, x0=None, tol=1e-10,
+                        max_iter=100000, **params):
+    """Newton + line search, each linear solve a CG with the menu preconditioner on the assembled
+    Jacobian; returns (x, cg_iterations, newton_steps, final relative residual)."""
+    mu, fe, b, h, rhs = _f64(node_mu), _f64(node_ferro), _f64(curve_b), _f64(curve_h), _f64(rhs)
+    pv = _menu_params(**params)
+    x = np.zeros(nx * ny) if x0 is None else np.array(x0, dtype=np.float64)
+    steps = ctypes.c_int(0)
+    rel = ctypes.c_double(0.0)
+    it = lib().silo_mag2d_nl_solve_menu(nx, ny, _ptr(mu), _ptr(fe), len(b), _ptr(b), _ptr(h), PRECONDITIONERS[kind],
+                                        _ptr(pv), _ptr(rhs), _ptr(x), tol, max_iter, ctypes.byref(steps),
+                                        ctypes.byref(rel))
+    if it < 0:
+        raise ValueError("singular ISAI system")
+    return x, it, steps.value, rel.value
+
+
+def mag3d_nl_solve_menu(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h, rhs, kind, x0=None, tol=1e-10,
+                        max_iter=100000, **params):
+    keep, args = _nl3_args(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h)
+    pv = _menu_params(**params)
+    rhs = _f64(rhs)
+    sol = np.zeros_like(rhs) if x0 is None else np.array(x0, dtype=np.float64)
+    steps = ctypes.c_int(0)
+    rel = ctypes.c_double(0.0)
+    it = lib().silo_mag3d_nl_solve_menu(*args, PRECONDITIONERS[kind], _ptr(pv), _ptr(rhs), _ptr(sol), tol, max_iter,
+                                        ctypes.byref(steps), ctypes.byref(rel))
+    if it < 0:
+        raise ValueError("singular ISAI system")
+    return sol, it, steps.value, rel.value

@@ -1790,11 +1790,13 @@ namespace {
 // system to the relative tolerance, then a line search of at most 8 steps
 // halving alpha from 1 that stops at the first candidate below the current
 // residual, else takes the best candidate seen).
-template <class Apply, class Jacobian, class Diagonal>
-int newton_solve(int64_t N, Apply const& apply, Jacobian const& jacobian, Diagonal const& diagonal,
-                 const double* rhs, double* x, double tol, int max_iter, int* newton_steps, double* final_rel)
+// The outer loop: step(x, r, d) solves J(x) d = r from d = 0 and returns its
+// CG iterations.
+template <class Apply, class Step>
+int newton_core(int64_t N, Apply const& apply, Step const& step, const double* rhs, double* x, double tol,
+                int* newton_steps, double* final_rel)
 {
-    std::vector<double> fa(N), r(N), d(N), cand(N), cand_f(N), cand_r(N), dinv(N), cr(N), z(N), p(N), q(N);
+    std::vector<double> fa(N), r(N), d(N), cand(N), cand_f(N), cand_r(N);
     apply(x, fa.data());
     for (int64_t i = 0; i < N; ++i) r[i] = rhs[i] - fa[i];
     double const r0 = nrm2(N, r.data());
@@ -1808,34 +1810,7 @@ int newton_solve(int64_t N, Apply const& apply, Jacobian const& jacobian, Diagon
         double const res = nrm2(N, r.data());
         if (res / r0 <= tol) break;
         ++steps;
-        // Jacobi-CG on J(x) d = r from d = 0
-        diagonal(x, dinv.data());
-        for (int64_t i = 0; i < N; ++i) dinv[i] = 1.0 / dinv[i];
-        std::fill(d.begin(), d.end(), 0.0);
-        cr = r;
-        for (int64_t i = 0; i < N; ++i) z[i] = dinv[i] * cr[i];
-        p = z;
-        double rz = dotp(N, cr.data(), z.data());
-        double const bn = nrm2(N, r.data());
-        double rn = bn;
-        int k = 0;
-        while (k < max_iter && rn > tol * bn) {
-            jacobian(x, p.data(), q.data());
-            double const alpha = rz / dotp(N, p.data(), q.data());
-            for (int64_t i = 0; i < N; ++i) {
-                d[i] += alpha * p[i];
-                cr[i] -= alpha * q[i];
-            }
-            ++k;
-            rn = nrm2(N, cr.data());
-            if (rn <= tol * bn) break;
-            for (int64_t i = 0; i < N; ++i) z[i] = dinv[i] * cr[i];
-            double const rz2 = dotp(N, cr.data(), z.data());
-            double const beta = rz2 / rz;
-            rz = rz2;
-            for (int64_t i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
-        }
-        total += k;
+        total += step(x, r.data(), d.data());
         // line search
         double const cur = nrm2(N, r.data());
         double alpha = 1.0, best_alpha = 0.0, best = std::numeric_limits<double>::infinity();
@@ -1864,6 +1839,60 @@ int newton_solve(int64_t N, Apply const& apply, Jacobian const& jacobian, Diagon
     *newton_steps = steps;
     *final_rel = nrm2(N, r.data()) / r0;
     return total;
+}
+
+// Jacobi-CG on J(x) d = r from d = 0 to the relative tolerance (the
+// matrix-free linear solve of the nonlinear branch).
+template <class Jacobian, class Diagonal>
+int jacobi_cg_step(int64_t N, Jacobian const& jacobian, Diagonal const& diagonal, const double* x, const double* r,
+                   double* d, double tol, int max_iter)
+{
+    std::vector<double> dinv(N), cr(r, r + N), z(N), p(N), q(N);
+    diagonal(x, dinv.data());
+    for (int64_t i = 0; i < N; ++i) dinv[i] = 1.0 / dinv[i];
+    std::fill(d, d + N, 0.0);
+    for (int64_t i = 0; i < N; ++i) z[i] = dinv[i] * cr[i];
+    p = z;
+    double rz = dotp(N, cr.data(), z.data());
+    double const bn = nrm2(N, r);
+    double rn = bn;
+    int k = 0;
+    while (k < max_iter && rn > tol * bn) {
+        jacobian(x, p.data(), q.data());
+        double const alpha = rz / dotp(N, p.data(), q.data());
+        for (int64_t i = 0; i < N; ++i) {
+            d[i] += alpha * p[i];
+            cr[i] -= alpha * q[i];
+        }
+        ++k;
+        rn = nrm2(N, cr.data());
+        if (rn <= tol * bn) break;
+        for (int64_t i = 0; i < N; ++i) z[i] = dinv[i] * cr[i];
+        double const rz2 = dotp(N, cr.data(), z.data());
+        double const beta = rz2 / rz;
+        rz = rz2;
+        for (int64_t i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
+    }
+    return k;
+}
+
+// Newton with a halving line search on F(x) = rhs; every step solves
+// J(x) d = r by Jacobi-CG from d = 0 to the relative tolerance.
+// Ref: src/similie/solvers/minimize_strong_formulation_residual.hpp:1383-1569
+// (nonlinear branch: at most 30 Newton steps; each solves the linearised
+// system to the relative tolerance, then a line search of at most 8 steps
+// halving alpha from 1 that stops at the first candidate below the current
+// residual, else takes the best candidate seen).
+template <class Apply, class Jacobian, class Diagonal>
+int newton_solve(int64_t N, Apply const& apply, Jacobian const& jacobian, Diagonal const& diagonal,
+                 const double* rhs, double* x, double tol, int max_iter, int* newton_steps, double* final_rel)
+{
+    return newton_core(
+            N, apply,
+            [&](const double* xs, const double* r, double* d) {
+                return jacobi_cg_step(N, jacobian, diagonal, xs, r, d, tol, max_iter);
+            },
+            rhs, x, tol, newton_steps, final_rel);
 }
 
 // 3D material law at a sampled node with moments B = (B_x, B_y, B_z):
@@ -2334,14 +2363,12 @@ int silo_csr_isai_values(int64_t n, const int64_t* ptr, const int32_t* col, cons
     return 0;
 }
 
-// Preconditioned CG from x = 0 until ||r|| <= tol ||b||; returns the
-// iterations (-1 when the preconditioner cannot be built).
-int silo_csr_pcg(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int kind, const double* params,
-                 const double* b, double* x, double tol, int max_iter, double* final_rel)
+namespace {
+
+int pcg_run(CsrView const& A, MenuPrecond const& m, const double* b, double* x, double tol, int max_iter,
+            double* final_rel)
 {
-    CsrView const A {n, ptr, col, val};
-    MenuPrecond const m = make_menu(A, kind, params);
-    if (!m.ok) return -1;
+    int64_t const n = A.n;
     std::vector<double> r(b, b + n), z(n), p(n), q(n);
     std::fill(x, x + n, 0.0);
     double const bnorm = nrm2(n, b);
@@ -2372,4 +2399,130 @@ int silo_csr_pcg(int64_t n, const int64_t* ptr, const int32_t* col, const double
     }
     *final_rel = rnorm / bnorm;
     return it;
+}
+
+// CSR of a linear map whose rows touch only the 3x3 (2D nodes) or 3x3x3
+// (3D nodes x 3 components) neighbourhood, by one apply per column colour
+// (node coordinates mod 3, and component); exact zeros dropped, columns
+// ascending.  The same construction as oracle.assemble2d / assemble3d.
+struct OwnedCsr
+{
+    std::vector<int64_t> ptr;
+    std::vector<int32_t> col;
+    std::vector<double> val;
+    CsrView view(int64_t n) const { return CsrView {n, ptr.data(), col.data(), val.data()}; }
+};
+
+template <class Apply>
+OwnedCsr probe_csr(int dim, int64_t nx, int64_t ny, int64_t nz, Apply const& apply)
+{
+    int64_t const n = dim == 2 ? nx * ny : 3 * nx * ny * nz;
+    int const ncolors = dim == 2 ? 9 : 81;
+    auto color_of = [&](int64_t c) -> int {
+        if (dim == 2) return static_cast<int>((c % nx) % 3 + 3 * ((c / nx) % 3));
+        int64_t const node = c / 3, comp = c % 3;
+        int64_t const i = node % nx, j = (node / nx) % ny, k = node / (nx * ny);
+        return static_cast<int>(comp + 3 * (i % 3 + 3 * (j % 3) + 9 * (k % 3)));
+    };
+    std::vector<std::vector<std::pair<int32_t, double>>> rows(n);
+    std::vector<double> probe(n), y(n);
+    for (int color = 0; color < ncolors; ++color) {
+        for (int64_t c = 0; c < n; ++c) probe[c] = color_of(c) == color ? 1.0 : 0.0;
+        apply(probe.data(), y.data());
+        for (int64_t r = 0; r < n; ++r) {
+            if (y[r] == 0.0) continue;
+            int64_t const node = dim == 2 ? r : r / 3;
+            int64_t const i = node % nx, j = (node / nx) % ny, k = dim == 2 ? 0 : node / (nx * ny);
+            for (int dk = (dim == 2 ? 0 : -1); dk <= (dim == 2 ? 0 : 1); ++dk)
+                for (int dj = -1; dj <= 1; ++dj)
+                    for (int di = -1; di <= 1; ++di) {
+                        int64_t const ii = i + di, jj = j + dj, kk = k + dk;
+                        if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= (dim == 2 ? 1 : nz)) continue;
+                        int64_t const m = ii + nx * (jj + ny * kk);
+                        for (int comp = 0; comp < (dim == 2 ? 1 : 3); ++comp) {
+                            int64_t const c = dim == 2 ? m : 3 * m + comp;
+                            if (color_of(c) == color) rows[r].push_back({static_cast<int32_t>(c), y[r]});
+                        }
+                    }
+        }
+    }
+    OwnedCsr out;
+    out.ptr.assign(n + 1, 0);
+    for (int64_t r = 0; r < n; ++r) {
+        std::sort(rows[r].begin(), rows[r].end());
+        out.ptr[r + 1] = out.ptr[r] + static_cast<int64_t>(rows[r].size());
+        for (auto const& [c, v] : rows[r]) {
+            out.col.push_back(c);
+            out.val.push_back(v);
+        }
+    }
+    return out;
+}
+
+// Newton whose linear solves run CG with a menu preconditioner on the
+// Jacobian assembled at the state (the reference's nonlinear branch with
+// build_matrix(operator_model, solution) + build_preconditioner,
+// minimize_strong_formulation_residual.hpp:1432-1436, assembled system).
+template <class Apply, class Jacobian>
+int newton_menu(int dim, int64_t nx, int64_t ny, int64_t nz, Apply const& apply, Jacobian const& jacobian, int kind,
+                const double* params, const double* rhs, double* x, double tol, int max_iter, int* newton_steps,
+                double* final_rel)
+{
+    int64_t const N = dim == 2 ? nx * ny : 3 * nx * ny * nz;
+    bool ok = true;
+    int const total = newton_core(
+            N, apply,
+            [&](const double* xs, const double* r, double* d) {
+                OwnedCsr const J = probe_csr(dim, nx, ny, nz,
+                                             [&](const double* v, double* out) { jacobian(xs, v, out); });
+                MenuPrecond const m = make_menu(J.view(N), kind, params);
+                if (!m.ok) {
+                    ok = false;
+                    std::fill(d, d + N, 0.0);
+                    return 0;
+                }
+                double rel = 0.0;
+                return pcg_run(J.view(N), m, r, d, tol, max_iter, &rel);
+            },
+            rhs, x, tol, newton_steps, final_rel);
+    return ok ? total : -1;
+}
+
+} // namespace
+
+// Preconditioned CG from x = 0 until ||r|| <= tol ||b||; returns the
+// iterations (-1 when the preconditioner cannot be built).
+int silo_csr_pcg(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int kind, const double* params,
+                 const double* b, double* x, double tol, int max_iter, double* final_rel)
+{
+    CsrView const A {n, ptr, col, val};
+    MenuPrecond const m = make_menu(A, kind, params);
+    if (!m.ok) return -1;
+    return pcg_run(A, m, b, x, tol, max_iter, final_rel);
+}
+
+int silo_mag2d_nl_solve_menu(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
+                             const double* b, const double* h, int kind, const double* params, const double* rhs,
+                             double* x, double tol, int max_iter, int* newton_steps, double* final_rel)
+{
+    BHCurve const c(n, b, h);
+    NodeLaw const law {node_mu, node_ferro, &c};
+    return newton_menu(
+            2, nx, ny, 1, [&](const double* v, double* out) { nl_apply(nx, ny, law, v, out); },
+            [&](const double* st, const double* v, double* out) { nl_jacobian_apply(nx, ny, law, st, v, out); },
+            kind, params, rhs, x, tol, max_iter, newton_steps, final_rel);
+}
+
+int silo_mag3d_nl_solve_menu(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                             const double* node_mu, const double* node_ferro, double gamma, int n, const double* b,
+                             const double* h, int kind, const double* params, const double* rhs, double* sol,
+                             double tol, int max_iter, int* newton_steps, double* final_rel)
+{
+    BHCurve const c(n, b, h);
+    Grid3 const g {nx, ny, nz, x, y, z};
+    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    return newton_menu(
+            3, nx, ny, nz, [&](const double* v, double* out) { op.apply(v, out); },
+            [&](const double* st, const double* v, double* out) { op.jacobian(st, v, out); }, kind, params, rhs, sol,
+            tol, max_iter, newton_steps, final_rel);
 }

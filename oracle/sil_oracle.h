@@ -178,6 +178,17 @@ int silo_csr_isai_values(int64_t n, const int64_t* ptr, const int32_t* col, cons
 int silo_csr_pcg(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int kind, const double* params,
                  const double* b, double* x, double tol, int max_iter, double* final_rel);
 
+/* Newton as silo_mag2d_nl_solve / silo_mag3d_nl_solve, each linear solve a
+ * CG with the menu preconditioner `kind` on the Jacobian assembled at the
+ * state.  Returns the CG iterations (-1 if a preconditioner cannot be built). */
+int silo_mag2d_nl_solve_menu(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
+                             const double* b, const double* h, int kind, const double* params, const double* rhs,
+                             double* x, double tol, int max_iter, int* newton_steps, double* final_rel);
+int silo_mag3d_nl_solve_menu(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                             const double* node_mu, const double* node_ferro, double gamma, int n, const double* b,
+                             const double* h, int kind, const double* params, const double* rhs, double* sol,
+                             double tol, int max_iter, int* newton_steps, double* final_rel);
+
 /* Threads OpenMP uses (for reporting). */
 int silo_num_threads(void);
 

@@ -126,6 +126,7 @@ class SilSolveSettings(ctypes.Structure):
         ("preconditioner", ctypes.c_void_p),
         ("stall_window", ctypes.c_int32),
         ("flexible_directions", ctypes.c_int32),
+        ("jacobian_preconditioner", ctypes.c_void_p),
     ]
 
 
@@ -205,6 +206,8 @@ SIGNATURES = [
                                              ctypes.POINTER(SilSolveDiagnostics), _P]),
     ("sil_mag2d_assemble", ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, ctypes.POINTER(_P)]),
     ("sil_mag3d_assemble", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dProblem), ctypes.POINTER(_P)]),
+    ("sil_mag2d_nl_assemble_jacobian", ctypes.c_int, [_P, ctypes.POINTER(SilMag2dNlProblem), _P, ctypes.POINTER(_P)]),
+    ("sil_mag3d_nl_assemble_jacobian", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dNlProblem), _P, ctypes.POINTER(_P)]),
     ("sil_csr_get", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                    ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P)]),
     ("sil_csr_copy", ctypes.c_int, [_P, _P, _P, _P, _P]),

@@ -112,6 +112,38 @@ class CsrMatrix:
             pass
 
 
+def menu_settings(kind="jacobi", sor_relaxation_factor=0.0, chebyshev_iterations=0, chebyshev_lower_bound=0.0,
+                  chebyshev_upper_bound=0.0, ir_iterations=0, ir_relaxation_factor=0.0):
+    """A sil_menu_settings for one menu entry (0 keeps the reference's default of a field)."""
+    cfg = _native.SilMenuSettings()
+    cfg.kind = kind_of(kind)
+    cfg.sor_relaxation_factor = sor_relaxation_factor
+    cfg.chebyshev_iterations = chebyshev_iterations
+    cfg.chebyshev_lower_bound = chebyshev_lower_bound
+    cfg.chebyshev_upper_bound = chebyshev_upper_bound
+    cfg.ir_iterations = ir_iterations
+    cfg.ir_relaxation_factor = ir_relaxation_factor
+    return cfg
+
+
+def jacobian2d(problem_struct, state_dev, stream=None):
+    """The Jacobian of a 2D nonlinear problem (a SilMag2dNlProblem) at `state` as a CsrMatrix."""
+    h = ctypes.c_void_p()
+    check(lib().sil_mag2d_nl_assemble_jacobian(_stream(stream), ctypes.byref(problem_struct),
+                                               ctypes.c_void_p(state_dev.data_ptr()), ctypes.byref(h)),
+          "mag2d_nl_assemble_jacobian")
+    return CsrMatrix(h.value)
+
+
+def jacobian3d(problem_struct, state_dev, stream=None):
+    """The Jacobian of a 3D nonlinear problem (a SilMag3dNlProblem) at `state` as a CsrMatrix."""
+    h = ctypes.c_void_p()
+    check(lib().sil_mag3d_nl_assemble_jacobian(_stream(stream), ctypes.byref(problem_struct),
+                                               ctypes.c_void_p(state_dev.data_ptr()), ctypes.byref(h)),
+          "mag3d_nl_assemble_jacobian")
+    return CsrMatrix(h.value)
+
+
 class Preconditioner:
     """One entry of the reference's preconditioner menu, built on a CsrMatrix (which it keeps alive)."""
 
@@ -119,14 +151,8 @@ class Preconditioner:
                  chebyshev_lower_bound=0.0, chebyshev_upper_bound=0.0, ir_iterations=0, ir_relaxation_factor=0.0,
                  stream=None):
         self.matrix = matrix
-        cfg = _native.SilMenuSettings()
-        cfg.kind = kind_of(kind)
-        cfg.sor_relaxation_factor = sor_relaxation_factor
-        cfg.chebyshev_iterations = chebyshev_iterations
-        cfg.chebyshev_lower_bound = chebyshev_lower_bound
-        cfg.chebyshev_upper_bound = chebyshev_upper_bound
-        cfg.ir_iterations = ir_iterations
-        cfg.ir_relaxation_factor = ir_relaxation_factor
+        cfg = menu_settings(kind, sor_relaxation_factor, chebyshev_iterations, chebyshev_lower_bound,
+                            chebyshev_upper_bound, ir_iterations, ir_relaxation_factor)
         h = ctypes.c_void_p()
         check(lib().sil_csr_precond_create(_stream(stream), matrix._h, ctypes.byref(cfg), ctypes.byref(h)),
               "csr_precond_create")

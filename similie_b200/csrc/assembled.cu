@@ -764,6 +764,37 @@ sil_status sil_mag3d_assemble(sil_stream stream, const sil_mag3d_problem* proble
                     [&](double const* v, double* y) { return sil_mag3d_apply(stream, problem, v, y); }, out);
 }
 
+sil_status sil_mag2d_nl_assemble_jacobian(sil_stream stream, const sil_mag2d_nl_problem* problem,
+                                          const double* state, sil_csr* out)
+{
+    if (out == nullptr || problem == nullptr || state == nullptr)
+        return fail(SIL_ERR_INVALID, "sil_mag2d_nl_assemble_jacobian: NULL argument");
+    *out = nullptr;
+    sil_mag2d_nl_problem const& q = *problem;
+    if (q.nx < 3 || q.ny < 3) return fail(SIL_ERR_INVALID, "sil_mag2d_nl_assemble_jacobian: need at least 3x3 nodes");
+    cudaStream_t const s = static_cast<cudaStream_t>(stream);
+    Probe const g {2, static_cast<int>(q.nx), static_cast<int>(q.ny), 1};
+    return assemble(s, g, q.nx * q.ny, 9,
+                    [&](double const* v, double* y) { return sil_mag2d_nl_apply_jacobian(stream, problem, state, v, y); },
+                    out);
+}
+
+sil_status sil_mag3d_nl_assemble_jacobian(sil_stream stream, const sil_mag3d_nl_problem* problem,
+                                          const double* state, sil_csr* out)
+{
+    if (out == nullptr || problem == nullptr || state == nullptr)
+        return fail(SIL_ERR_INVALID, "sil_mag3d_nl_assemble_jacobian: NULL argument");
+    *out = nullptr;
+    sil_mag3d_nl_problem const& q = *problem;
+    if (q.nx < 3 || q.ny < 3 || q.nz < 3)
+        return fail(SIL_ERR_INVALID, "sil_mag3d_nl_assemble_jacobian: need at least 3x3x3 nodes");
+    cudaStream_t const s = static_cast<cudaStream_t>(stream);
+    Probe const g {3, static_cast<int>(q.nx), static_cast<int>(q.ny), static_cast<int>(q.nz)};
+    return assemble(s, g, 3 * q.nx * q.ny * q.nz, 81,
+                    [&](double const* v, double* y) { return sil_mag3d_nl_apply_jacobian(stream, problem, state, v, y); },
+                    out);
+}
+
 sil_status sil_csr_get(sil_csr m, int64_t* n, int64_t* nnz, const int32_t** row_ptr, const int32_t** col,
                        const double** val)
 {

@@ -925,9 +925,33 @@ namespace {
 //   jacobian_setup(s, x, dinv):    Jacobian coefficients at x, inverse diagonal
 //   cg_product(s, p, q, part, cg): q = J p, ops.G partials of p.q, no work once
 //                                  the CG state is done
+// One linear solve of a Newton step with a menu preconditioner: the Jacobian
+// assembled at x, the preconditioner built on it, CG for d from 0.
+template <class Ops>
+sil_status menu_step(Ops const& ops, sil_menu_settings const& menu, cudaStream_t st, double const* x,
+                     double const* r, double* d, double tol, int max_iter, int* iterations)
+{
+    sil_csr J = nullptr;
+    if (sil_status s = ops.assemble_jacobian(st, x, &J); s != SIL_OK) return s;
+    sil_csr_precond pc = nullptr;
+    sil_status s = sil_csr_precond_create(st, J, &menu, &pc);
+    if (s == SIL_OK) {
+        sil_solve_settings ls {};
+        ls.max_iterations = max_iter;
+        ls.relative_tolerance = tol;
+        sil_solve_diagnostics ld {};
+        s = sil_csr_solve(st, J, pc, r, d, &ls, &ld);
+        *iterations = ld.iterations;
+        sil_csr_precond_destroy(pc);
+    }
+    sil_csr_destroy(J);
+    return s;
+}
+
 template <class Ops>
 sil_status newton(Ops const& ops, double* x, double* const* v, double* part, double* d_norm, CgState* d_cg,
-                  cudaStream_t st, double tol, int max_iter, sil_solve_diagnostics& D)
+                  cudaStream_t st, double tol, int max_iter, sil_solve_diagnostics& D,
+                  sil_menu_settings const* menu = nullptr)
 {
     double *r = v[0], *cand_r = v[1], *cand = v[2], *dvec = v[3], *cr = v[4], *z = v[5], *pv = v[6], *qv = v[7],
            *dinv = v[8];
@@ -959,10 +983,11 @@ sil_status newton(Ops const& ops, double* x, double* const* v, double* part, dou
         return SIL_OK;
     }
     // 16 CG iterations captured once per problem (the kernels stop doing
-    // work once the state is marked done) and replayed until convergence.
+    // work once the state is marked done) and replayed until convergence;
+    // not needed when a menu preconditioner runs the linear solves.
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    {
+    if (menu == nullptr) {
         cudaStream_t cs;
         SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
         cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
@@ -988,26 +1013,32 @@ sil_status newton(Ops const& ops, double* x, double* const* v, double* part, dou
         cudaGraphExec_t e;
         ~GraphGuard()
         {
-            cudaGraphExecDestroy(e);
-            cudaGraphDestroy(g);
+            if (e != nullptr) cudaGraphExecDestroy(e);
+            if (g != nullptr) cudaGraphDestroy(g);
         }
     } guard {graph, exec};
     int cg_total = 0, steps = 0;
     for (int it = 0; it < 30; ++it) {
         if (res / r0 <= tol) break;
         ++steps;
-        ops.jacobian_setup(st, x, dinv);
-        cg_start_kernel<<<G, kBlock, 0, st>>>(n, r, dinv, dvec, cr, z, pv, part);
-        cg_init_kernel<<<1, kBlock, 0, st>>>(part, static_cast<int>(G), d_cg, tol, max_iter);
-        SIL_CUDA_CHECK(cudaGetLastError());
-        CgState hs {};
-        for (;;) {
-            SIL_CUDA_CHECK(cudaGraphLaunch(exec, st));
-            SIL_CUDA_CHECK(cudaMemcpyAsync(&hs, d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, st));
-            SIL_CUDA_CHECK(cudaStreamSynchronize(st));
-            if (hs.done) break;
+        if (menu != nullptr) {
+            int its = 0;
+            if (sil_status s = menu_step(ops, *menu, st, x, r, dvec, tol, max_iter, &its); s != SIL_OK) return s;
+            cg_total += its;
+        } else {
+            ops.jacobian_setup(st, x, dinv);
+            cg_start_kernel<<<G, kBlock, 0, st>>>(n, r, dinv, dvec, cr, z, pv, part);
+            cg_init_kernel<<<1, kBlock, 0, st>>>(part, static_cast<int>(G), d_cg, tol, max_iter);
+            SIL_CUDA_CHECK(cudaGetLastError());
+            CgState hs {};
+            for (;;) {
+                SIL_CUDA_CHECK(cudaGraphLaunch(exec, st));
+                SIL_CUDA_CHECK(cudaMemcpyAsync(&hs, d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, st));
+                SIL_CUDA_CHECK(cudaStreamSynchronize(st));
+                if (hs.done) break;
+            }
+            cg_total += hs.iters;
         }
-        cg_total += hs.iters;
         // line search
         double const cur = res;
         double alpha = 1.0, best_alpha = 0.0, best = std::numeric_limits<double>::infinity(), nr = 0.0;
@@ -1061,6 +1092,10 @@ struct Ops2
     {
         cg_jac_kernel<<<G, kBlock, 0, s>>>(g, c00, c01, c11, p, q, part, cg);
     }
+    sil_status assemble_jacobian(cudaStream_t s, double const* x, sil_csr* out) const
+    {
+        return sil_mag2d_nl_assemble_jacobian(s, &P, x, out);
+    }
 };
 
 struct Ops3
@@ -1087,6 +1122,10 @@ struct Ops3
     {
         nl3_jfield_kernel<<<Gn, kBlock, 0, s>>>(g, kh, p, hv, cg);
         nl3_gather_kernel<2><<<G, kBlock, 0, s>>>(g, hv, p, nullptr, q, part, cg);
+    }
+    sil_status assemble_jacobian(cudaStream_t s, double const* x, sil_csr* out) const
+    {
+        return sil_mag3d_nl_assemble_jacobian(s, &P, x, out);
     }
 };
 
@@ -1132,7 +1171,7 @@ struct Workspace
 };
 
 sil_status solve_one(sil_mag2d_nl_problem const& P, DevCurve const& C, double tol, int max_iter,
-                     sil_solve_diagnostics& D)
+                     sil_solve_diagnostics& D, sil_menu_settings const* menu)
 {
     int64_t const n = P.nx * P.ny;
     unsigned const G = grid_for(n);
@@ -1141,14 +1180,15 @@ sil_status solve_one(sil_mag2d_nl_problem const& P, DevCurve const& C, double to
     if (sil_status s = w.init(n, G, 3 * vb); s != SIL_OK) return s;
     Ops2 const ops {C, Geo {static_cast<int>(P.nx), static_cast<int>(P.ny)}, P, w.extra, w.extra + vb,
                     w.extra + 2 * vb, n, G};
-    if (sil_status s = newton(ops, P.solution, w.v, w.part, w.d_norm, w.d_cg, w.sg.s, tol, max_iter, D); s != SIL_OK)
+    if (sil_status s = newton(ops, P.solution, w.v, w.part, w.d_norm, w.d_cg, w.sg.s, tol, max_iter, D, menu);
+        s != SIL_OK)
         return s;
     SIL_CUDA_CHECK(cudaStreamSynchronize(w.sg.s));
     return SIL_OK;
 }
 
 sil_status solve_one3(sil_mag3d_nl_problem const& P, DevCurve const& C, double tol, int max_iter,
-                      sil_solve_diagnostics& D)
+                      sil_solve_diagnostics& D, sil_menu_settings const* menu)
 {
     int64_t const nodes = P.nx * P.ny * P.nz;
     int64_t const n = 3 * nodes;
@@ -1161,7 +1201,8 @@ sil_status solve_one3(sil_mag3d_nl_problem const& P, DevCurve const& C, double t
     double* dls = w.extra + hb + kb;
     SIL_CUDA_CHECK(cudaMemcpyAsync(dls, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, w.sg.s));
     Ops3 const ops {C, make_geo3(P, dls), P, w.extra, w.extra + hb, n, G, grid_for(nodes)};
-    if (sil_status s = newton(ops, P.solution, w.v, w.part, w.d_norm, w.d_cg, w.sg.s, tol, max_iter, D); s != SIL_OK)
+    if (sil_status s = newton(ops, P.solution, w.v, w.part, w.d_norm, w.d_cg, w.sg.s, tol, max_iter, D, menu);
+        s != SIL_OK)
         return s;
     SIL_CUDA_CHECK(cudaStreamSynchronize(w.sg.s));
     return SIL_OK;
@@ -1189,7 +1230,9 @@ sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int np
     int const max_iter = settings->max_iterations > 0 ? settings->max_iterations : 100000;
     // the inputs come from the caller's stream
     SIL_CUDA_CHECK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
-    return run_concurrent(nproblems, [&](int p) { return solve_one(problems[p], curves[p], tol, max_iter, diag[p]); });
+    sil_menu_settings const* menu = settings->jacobian_preconditioner;
+    return run_concurrent(nproblems,
+                          [&](int p) { return solve_one(problems[p], curves[p], tol, max_iter, diag[p], menu); });
 }
 
 namespace {
@@ -1268,5 +1311,7 @@ sil_status sil_mag3d_nl_solve_batch(const sil_mag3d_nl_problem* problems, int np
     int const max_iter = settings->max_iterations > 0 ? settings->max_iterations : 100000;
     // the inputs come from the caller's stream
     SIL_CUDA_CHECK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
-    return run_concurrent(nproblems, [&](int p) { return solve_one3(problems[p], curves[p], tol, max_iter, diag[p]); });
+    sil_menu_settings const* menu = settings->jacobian_preconditioner;
+    return run_concurrent(nproblems,
+                          [&](int p) { return solve_one3(problems[p], curves[p], tol, max_iter, diag[p], menu); });
 }

@@ -257,10 +257,25 @@ def nl_apply_jacobian(node_mu_dev, node_ferro_dev, curve_b, curve_h, state_dev, 
     return y_dev
 
 
-def nl_solve_batch(mus, ferros, curves, rhss, sols, shapes, tol=1e-10, max_iterations=100000, stream=None):
+def _menu_pointer(st, jacobian_preconditioner):
+    """Points st.jacobian_preconditioner at a menu entry (a name or a dict of
+    sil_menu_settings fields); returns the structure to keep alive."""
+    if jacobian_preconditioner is None:
+        return None
+    from .assembled import menu_settings
+    cfg = (menu_settings(jacobian_preconditioner) if isinstance(jacobian_preconditioner, str)
+           else menu_settings(**jacobian_preconditioner))
+    st.jacobian_preconditioner = ctypes.addressof(cfg)
+    return cfg
+
+
+def nl_solve_batch(mus, ferros, curves, rhss, sols, shapes, tol=1e-10, max_iterations=100000, stream=None,
+                   jacobian_preconditioner=None):
     """Newton + line search for a batch of nonlinear problems (minimize_strong_formulation_residual,
     nonlinear branch).  curves: list of (b, h) sample arrays; sols hold the initial guesses and
-    receive the solutions.  Returns one Diagnostics per problem (refinements = Newton steps)."""
+    receive the solutions.  jacobian_preconditioner: None for the matrix-free Jacobi-CG, or a menu
+    entry ("ssor", or a dict of sil_menu_settings fields) for CG on the assembled Jacobian.
+    Returns one Diagnostics per problem (refinements = Newton steps)."""
     import torch
     n = len(shapes)
     keep = [_Curve(b, h) for b, h in curves]
@@ -270,6 +285,7 @@ def nl_solve_batch(mus, ferros, curves, rhss, sols, shapes, tol=1e-10, max_itera
     st = _native.SilSolveSettings()
     st.max_iterations = max_iterations
     st.relative_tolerance = tol
+    menu = _menu_pointer(st, jacobian_preconditioner)
     diag = (_native.SilSolveDiagnostics * n)()
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
     rc = lib().sil_mag2d_nl_solve_batch(probs, n, ctypes.byref(st), diag, s)

@@ -281,12 +281,13 @@ def nl_apply_jacobian(x, y, z, node_mu_dev, node_ferro_dev, curve_b, curve_h, st
 
 
 def nl_solve_batch(coords, mus, ferros, curves, rhss, sols, gammas=None, tol=1e-10, max_iterations=100000,
-                   stream=None):
+                   stream=None, jacobian_preconditioner=None):
     """Newton + line search for a batch of 3D nonlinear problems.  coords: (x, y, z) host arrays;
     curves: (b, h) sample arrays; sols hold the initial guesses and receive the solutions.
+    jacobian_preconditioner as in magnetostatics.nl_solve_batch.
     Returns one Diagnostics per problem (refinements = Newton steps)."""
     import torch
-    from .magnetostatics import _Curve
+    from .magnetostatics import _Curve, _menu_pointer
     n = len(coords)
     gammas = [DEFAULT_GAUGE_PENALTY] * n if gammas is None else list(gammas)
     keep = [tuple(_f64(v) for v in c) for c in coords]
@@ -297,9 +298,11 @@ def nl_solve_batch(coords, mus, ferros, curves, rhss, sols, gammas=None, tol=1e-
     st = _native.SilSolveSettings()
     st.max_iterations = max_iterations
     st.relative_tolerance = tol
+    menu = _menu_pointer(st, jacobian_preconditioner)
     diag = (_native.SilSolveDiagnostics * n)()
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
     rc = lib().sil_mag3d_nl_solve_batch(probs, n, ctypes.byref(st), diag, s)
+    del menu
     out = [Diagnostics(d.iterations, bool(d.converged), d.refinements, d.status, d.initial_residual_l2,
                        d.final_residual_l2, d.final_relative_residual) for d in diag]
     check(rc, "mag3d_nl_solve_batch")

@@ -181,6 +181,15 @@ def test_assembled_path_arguments_checked_on_host():
     st = _native.SilSolveSettings()
     d = _native.SilSolveDiagnostics()
     assert L.sil_csr_solve(None, None, None, 256, 256, ctypes.byref(st), ctypes.byref(d)) == 1
+    q = _native.SilMag2dNlProblem()
+    q.nx, q.ny = 2, 8
+    assert L.sil_mag2d_nl_assemble_jacobian(None, ctypes.byref(q), 256, ctypes.byref(h)) == 1
+    assert b"3x3" in L.sil_last_error()
+    assert L.sil_mag2d_nl_assemble_jacobian(None, ctypes.byref(q), None, ctypes.byref(h)) == 1
+    r = _native.SilMag3dNlProblem()
+    r.nx, r.ny, r.nz = 4, 2, 4
+    assert L.sil_mag3d_nl_assemble_jacobian(None, ctypes.byref(r), 256, ctypes.byref(h)) == 1
+    assert b"3x3x3" in L.sil_last_error()
     L.sil_csr_destroy(None)
     L.sil_csr_precond_destroy(None)
     import similie_b200.assembled as asm

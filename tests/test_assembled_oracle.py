@@ -143,3 +143,34 @@ def test_stronger_preconditioners_take_fewer_iterations_in_3d():
     its = {k: O.csr_pcg(A, b, k, tol=1e-10)[1] for k in ("jacobi", "spd-isai", "symmetric-gauss-seidel", "ssor")}
     assert its["symmetric-gauss-seidel"] < its["jacobi"] and its["spd-isai"] < its["jacobi"]
     assert its["ssor"] < its["jacobi"]
+
+
+def test_menu_newton_matches_the_matrix_free_newton():
+    """The nonlinear branch with an assembled Jacobian: Jacobi on the assembled
+    matrix is the matrix-free Jacobi-CG; SSOR and SpdIsai take the same Newton
+    steps with fewer CG iterations."""
+    p, mu, fe, b, h = mag.nonlinear_problem(49, 3)
+    rhs = p.rhs()
+    x0, it0, s0, r0 = O.mag2d_nl_solve(49, 49, mu, fe, b, h, rhs)
+    xj, itj, sj, rj = O.mag2d_nl_solve_menu(49, 49, mu, fe, b, h, rhs, "jacobi")
+    assert (itj, sj) == (it0, s0) and np.linalg.norm(xj - x0) <= 1e-14 * np.linalg.norm(x0)
+    for kind in ("ssor", "spd-isai"):
+        x, it, st, rel = O.mag2d_nl_solve_menu(49, 49, mu, fe, b, h, rhs, kind)
+        assert st == s0 and rel <= 1e-10 and it < it0
+        assert np.linalg.norm(x - x0) <= 1e-12 * np.linalg.norm(x0)
+    p3, mu3, fe3, b3, h3 = m3.nonlinear_problem(13, 6)
+    rhs3 = p3.rhs()
+    y0, jt0, t0, _ = O.mag3d_nl_solve(p3.x, p3.y, p3.z, mu3, fe3, p3.gamma, b3, h3, rhs3)
+    y1, jt1, t1, rel = O.mag3d_nl_solve_menu(p3.x, p3.y, p3.z, mu3, fe3, p3.gamma, b3, h3, rhs3, "ssor")
+    assert t1 == t0 and rel <= 1e-10 and jt1 < jt0
+    assert np.linalg.norm(y1 - y0) <= 1e-9 * np.linalg.norm(y0)
+
+
+def test_assembled_jacobian_matches_the_jacobian_apply():
+    p, mu, fe, b, h = mag.nonlinear_problem(33, 4)
+    rng = np.random.default_rng(7)
+    st = rng.standard_normal(33 * 33) * 3 * b[-1]
+    J = O.jacobian2d_csr(33, 33, mu, fe, b, h, st)
+    v = rng.standard_normal(33 * 33)
+    ref = O.mag2d_nl_jacobian_apply(33, 33, mu, fe, b, h, st, v)
+    np.testing.assert_allclose(J @ v, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
