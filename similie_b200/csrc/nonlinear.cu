@@ -918,13 +918,6 @@ sil_status sil_mag2d_nl_apply_jacobian(sil_stream stream, const sil_mag2d_nl_pro
 namespace sil {
 namespace {
 
-// Newton with the line search for one problem on stream st.  v: nine
-// vectors of ops.n doubles (r, cand_r, cand, d, cr, z, p, q, dinv); part:
-// 2 * ops.G doubles.  Ops supplies
-//   residual(s, val, out, part):   out = rhs - F(val), ops.G partials of out^2
-//   jacobian_setup(s, x, dinv):    Jacobian coefficients at x, inverse diagonal
-//   cg_product(s, p, q, part, cg): q = J p, ops.G partials of p.q, no work once
-//                                  the CG state is done
 // One linear solve of a Newton step with a menu preconditioner: the Jacobian
 // assembled at x, the preconditioner built on it, CG for d from 0.
 template <class Ops>
@@ -948,6 +941,13 @@ sil_status menu_step(Ops const& ops, sil_menu_settings const& menu, cudaStream_t
     return s;
 }
 
+// Newton with the line search for one problem on stream st.  v: nine
+// vectors of ops.n doubles (r, cand_r, cand, d, cr, z, p, q, dinv); part:
+// 2 * ops.G doubles.  Ops supplies
+//   residual(s, val, out, part):   out = rhs - F(val), ops.G partials of out^2
+//   jacobian_setup(s, x, dinv):    Jacobian coefficients at x, inverse diagonal
+//   cg_product(s, p, q, part, cg): q = J p, ops.G partials of p.q, no work once
+//                                  the CG state is done
 template <class Ops>
 sil_status newton(Ops const& ops, double* x, double* const* v, double* part, double* d_norm, CgState* d_cg,
                   cudaStream_t st, double tol, int max_iter, sil_solve_diagnostics& D,
