@@ -517,7 +517,8 @@ typedef struct sil_menu_settings {
 typedef struct sil_csr_precond_s* sil_csr_precond;
 sil_status sil_csr_precond_create(sil_stream stream, sil_csr m, const sil_menu_settings* settings,
                                   sil_csr_precond* out);
-/* z = M^-1 r (device vectors). */
+/* z = M^-1 r (device vectors).  The preconditioner's scratch is shared by
+ * its applies and solves: use one preconditioner on one stream at a time. */
 sil_status sil_csr_precond_apply(sil_stream stream, sil_csr_precond p, const double* r, double* z);
 void sil_csr_precond_destroy(sil_csr_precond p);
 

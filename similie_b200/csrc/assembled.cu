@@ -65,13 +65,14 @@ constexpr int kMaxIsai = 32;  // ISAI rows: at most this many pattern entries
 
 unsigned grid_of(int64_t n)
 {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
+    // initialised once, thread-safely (the nonlinear batches call this from
+    // several host threads)
+    static int const sms = [] {
+        int dev = 0, count = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        return count > 0 ? count : 148;
+    }();
     int64_t const blocks = (n + kBlock - 1) / kBlock;
     return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(blocks, 8 * sms)));
 }

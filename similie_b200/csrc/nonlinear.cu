@@ -774,13 +774,14 @@ sil_status check_problem(sil_mag2d_nl_problem const& p, char const* who)
 
 unsigned grid_for(int64_t n)
 {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
+    // initialised once, thread-safely (the nonlinear batches call this from
+    // several host threads)
+    static int const sms = [] {
+        int dev = 0, count = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        return count > 0 ? count : 148;
+    }();
     int64_t const blocks = (n + kBlock - 1) / kBlock;
     return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(blocks, 4 * sms)));
 }
@@ -857,7 +858,7 @@ struct AsyncBuffer
 template <class Solve>
 sil_status run_concurrent(int nproblems, Solve const& solve)
 {
-    (void)grid_for(1);  // device attributes read once, before the threads start
+    (void)grid_for(1);  // device attributes read on the calling thread's device
     int dev = 0;
     SIL_CUDA_CHECK(cudaGetDevice(&dev));
     constexpr int kConcurrent = 8;
