@@ -76,6 +76,7 @@ def lib():
         _lib.silo_csr_precond_apply.argtypes = [i64, ip, i32p, dp, ci, dp, dp, dp]
         _lib.silo_csr_isai_values.argtypes = [i64, ip, i32p, dp, ci, dp]
         _lib.silo_csr_pcg.argtypes = [i64, ip, i32p, dp, ci, dp, dp, dp, d, ci, dp]
+        _lib.silo_csr_krylov.argtypes = [i64, ip, i32p, dp, ci, ci, ci, dp, dp, dp, d, ci, dp]
         _lib.silo_mag2d_nl_solve_menu.argtypes = [i64, i64, dp, dp, ci, dp, dp, ci, dp, dp, dp, d, ci,
                                                   ctypes.POINTER(ci), dp]
         _lib.silo_mag3d_nl_solve_menu.argtypes = [i64, i64, i64, dp, dp, dp, dp, dp, d, ci, dp, dp, ci, dp, dp, dp,
@@ -576,3 +577,23 @@ def mag3d_nl_solve_menu(x, y, z, node_mu, node_ferro, gamma, curve_b, curve_h, r
     if it < 0:
         raise ValueError("singular ISAI system")
     return sol, it, steps.value, rel.value
+
+
+KRYLOV = {"cg": 0, "minres": 1, "fcg": 2, "gmres": 3, "bicgstab": 4, "gcr": 5, "idr": 6}
+KRYLOV_DIMS = {"gmres": 100, "gcr": 100, "idr": 8}
+
+
+def csr_krylov(A, b, solver="cg", kind="jacobi", tol=1e-10, max_iter=100000, dim=None, **params):
+    """The reference's SIMILIE_SOLVER menu with a menu preconditioner, x from 0;
+    returns (x, iterations, final relative residual)."""
+    keep, args = _csr_args(A)
+    pv = _menu_params(**params)
+    b = _f64(b)
+    x = np.zeros_like(b)
+    rel = ctypes.c_double(0.0)
+    d = KRYLOV_DIMS.get(solver, 0) if dim is None else dim
+    it = lib().silo_csr_krylov(*args, KRYLOV[solver], d, PRECONDITIONERS[kind], _ptr(pv), _ptr(b), _ptr(x), tol,
+                               max_iter, ctypes.byref(rel))
+    if it < 0:
+        raise ValueError("unknown solver or singular ISAI system")
+    return x, it, rel.value

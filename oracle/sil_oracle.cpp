@@ -2526,3 +2526,355 @@ int silo_mag3d_nl_solve_menu(int64_t nx, int64_t ny, int64_t nz, const double* x
             [&](const double* st, const double* v, double* out) { op.jacobian(st, v, out); }, kind, params, rhs, sol,
             tol, max_iter, newton_steps, final_rel);
 }
+
+// ------------------------------------------------------------------ Krylov menu
+//
+// The reference's SIMILIE_SOLVER alternatives to CG
+// (src/similie/solvers/minimize_strong_formulation_residual.hpp:1069-1130:
+// Ginkgo's Minres, Fcg, Gmres with Krylov dimension SIMILIE_GMRES_KRYLOV_DIM
+// (100), Bicgstab, Gcr with SIMILIE_GCR_KRYLOV_DIM (100), Idr with subspace
+// SIMILIE_IDR_SUBSPACE_DIM (8) and a deterministic shadow space), each with
+// the menu preconditioner, x0 = 0 and the stop ||r|| <= tol ||b||.  Ginkgo's
+// source is not available here; each restates the published method it
+// names, preconditioned on the right (x = M^-1 u) except MINRES and FCG,
+// which take M^-1 as the symmetric preconditioner of the Lanczos / CG
+// recurrences:
+//   MINRES    Paige & Saunders (1975), preconditioned Lanczos with Givens
+//             rotations; stops on the true residual of its iterate
+//   FCG       flexible CG, beta = z_k . (r_k - r_{k-1}) / (z_{k-1} . r_{k-1})
+//             (Notay 2000, one stored direction)
+//   GMRES(m)  Saad & Schultz (1986), modified Gram-Schmidt Arnoldi, Givens
+//             rotations, restart after m; stops on the least-squares residual
+//   BiCGSTAB  van der Vorst (1992)
+//   GCR(m)    Eisenstat, Elman & Schultz (1983), A-images orthogonalised by
+//             modified Gram-Schmidt, restart after m
+//   IDR(s)    van Gijzen & Sonneveld (2011), Algorithm 2 (biorthogonal
+//             IDR(s)); shadow space: s Gaussian vectors from a fixed seed,
+//             orthonormalised
+namespace {
+
+enum KrylovKind
+{
+    kCg = 0,
+    kMinres = 1,
+    kFcg = 2,
+    kGmres = 3,
+    kBicgstab = 4,
+    kGcr = 5,
+    kIdr = 6
+};
+
+void axpy(int64_t n, double a, const double* x, double* y)
+{
+    for (int64_t i = 0; i < n; ++i) y[i] += a * x[i];
+}
+
+// returns iterations; x from 0
+int krylov_run(CsrView const& A, MenuPrecond const& M, int solver, int dim, const double* b, double* x, double tol,
+               int max_iter, double* final_rel)
+{
+    int64_t const n = A.n;
+    std::fill(x, x + n, 0.0);
+    double const bn = nrm2(n, b);
+    *final_rel = 0.0;
+    if (bn == 0.0) return 0;
+    double const target = tol * bn;
+    std::vector<double> r(b, b + n), z(n), p(n), q(n), t(n);
+    auto true_residual = [&]() {
+        spmv(A, x, t.data());
+        for (int64_t i = 0; i < n; ++i) t[i] = b[i] - t[i];
+        return nrm2(n, t.data());
+    };
+    int it = 0;
+    if (solver == kCg) {
+        double rel = 0.0;
+        it = pcg_run(A, M, b, x, tol, max_iter, &rel);
+        *final_rel = rel;
+        return it;
+    }
+    if (solver == kFcg) {
+        std::vector<double> r_old(n);
+        M.apply(r.data(), z.data());
+        p = z;
+        double rz = dotp(n, r.data(), z.data());
+        double rn = bn;
+        while (it < max_iter) {
+            spmv(A, p.data(), q.data());
+            double const alpha = rz / dotp(n, p.data(), q.data());
+            r_old = r;
+            for (int64_t i = 0; i < n; ++i) {
+                x[i] += alpha * p[i];
+                r[i] -= alpha * q[i];
+            }
+            ++it;
+            rn = nrm2(n, r.data());
+            if (rn <= target) break;
+            M.apply(r.data(), z.data());
+            double num = 0.0;
+            for (int64_t i = 0; i < n; ++i) num += z[i] * (r[i] - r_old[i]);
+            double const beta = num / rz;
+            rz = dotp(n, r.data(), z.data());
+            for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+        }
+        *final_rel = rn / bn;
+        return it;
+    }
+    if (solver == kMinres) {
+        // preconditioned Lanczos: v = residual vectors, w = M^-1 v
+        std::vector<double> v_old(n, 0.0), v(b, b + n), w(n), v_new(n), d_old(n, 0.0), d_older(n, 0.0), d(n);
+        M.apply(v.data(), w.data());
+        double beta = std::sqrt(dotp(n, v.data(), w.data()));
+        double beta_prev = 1.0;  // multiplies v_old = 0 in the first step
+        double eta = beta;
+        double c_old = 1.0, s_old = 0.0, c = 1.0, s = 0.0;
+        double rn = bn;
+        while (it < max_iter && beta > 0.0) {
+            for (int64_t i = 0; i < n; ++i) w[i] /= beta;   // w_k = M^-1 v_k / beta_k
+            spmv(A, w.data(), q.data());
+            double const alpha = dotp(n, w.data(), q.data());
+            for (int64_t i = 0; i < n; ++i) v_new[i] = q[i] - (alpha / beta) * v[i] - (beta / beta_prev) * v_old[i];
+            std::vector<double> w_new(n);
+            M.apply(v_new.data(), w_new.data());
+            double const beta_new = std::sqrt(std::max(0.0, dotp(n, v_new.data(), w_new.data())));
+            // QR of the tridiagonal by Givens rotations
+            double const delta = c * alpha - c_old * s * beta;
+            double const rho2 = s * alpha + c_old * c * beta;
+            double const rho3 = s_old * beta;
+            double const rho1 = std::sqrt(delta * delta + beta_new * beta_new);
+            double const c_new = delta / rho1, s_new = beta_new / rho1;
+            for (int64_t i = 0; i < n; ++i) d[i] = (w[i] - rho3 * d_older[i] - rho2 * d_old[i]) / rho1;
+            axpy(n, c_new * eta, d.data(), x);
+            eta = -s_new * eta;
+            d_older = d_old;
+            d_old = d;
+            v_old = v;
+            v = v_new;
+            w = w_new;
+            beta_prev = beta;
+            beta = beta_new;
+            c_old = c;
+            s_old = s;
+            c = c_new;
+            s = s_new;
+            ++it;
+            rn = true_residual();
+            if (rn <= target) break;
+        }
+        *final_rel = rn / bn;
+        return it;
+    }
+    if (solver == kGmres) {
+        int const m = std::max(1, dim);
+        std::vector<std::vector<double>> V(m + 1, std::vector<double>(n));
+        std::vector<double> H(static_cast<size_t>(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), u(n);
+        double rn = bn;
+        while (it < max_iter) {
+            double const beta = nrm2(n, r.data());
+            if (beta <= target) break;
+            for (int64_t i = 0; i < n; ++i) V[0][i] = r[i] / beta;
+            std::fill(g.begin(), g.end(), 0.0);
+            g[0] = beta;
+            int k = 0;
+            for (; k < m && it < max_iter; ++k) {
+                M.apply(V[k].data(), z.data());
+                spmv(A, z.data(), u.data());
+                for (int j = 0; j <= k; ++j) {
+                    double const h = dotp(n, u.data(), V[j].data());
+                    H[j * m + k] = h;
+                    axpy(n, -h, V[j].data(), u.data());
+                }
+                double const hn = nrm2(n, u.data());
+                H[(k + 1) * m + k] = hn;
+                if (hn != 0.0)
+                    for (int64_t i = 0; i < n; ++i) V[k + 1][i] = u[i] / hn;
+                for (int j = 0; j < k; ++j) {
+                    double const a = H[j * m + k], bb = H[(j + 1) * m + k];
+                    H[j * m + k] = cs[j] * a + sn[j] * bb;
+                    H[(j + 1) * m + k] = -sn[j] * a + cs[j] * bb;
+                }
+                double const a = H[k * m + k], bb = H[(k + 1) * m + k];
+                double const den = std::sqrt(a * a + bb * bb);
+                cs[k] = a / den;
+                sn[k] = bb / den;
+                H[k * m + k] = den;
+                H[(k + 1) * m + k] = 0.0;
+                g[k + 1] = -sn[k] * g[k];
+                g[k] = cs[k] * g[k];
+                ++it;
+                rn = std::fabs(g[k + 1]);
+                if (rn <= target) {
+                    ++k;
+                    break;
+                }
+            }
+            // x += M^-1 (V y), H y = g
+            for (int j = k - 1; j >= 0; --j) {
+                double sacc = g[j];
+                for (int l = j + 1; l < k; ++l) sacc -= H[j * m + l] * y[l];
+                y[j] = sacc / H[j * m + j];
+            }
+            std::fill(u.begin(), u.end(), 0.0);
+            for (int j = 0; j < k; ++j) axpy(n, y[j], V[j].data(), u.data());
+            M.apply(u.data(), z.data());
+            axpy(n, 1.0, z.data(), x);
+            spmv(A, x, t.data());
+            for (int64_t i = 0; i < n; ++i) r[i] = b[i] - t[i];
+            if (rn <= target) break;
+        }
+        *final_rel = rn / bn;
+        return it;
+    }
+    if (solver == kBicgstab) {
+        std::vector<double> r0(r), v(n, 0.0), ph(n), sv(n), sh(n), tv(n);
+        double rho = 1.0, alpha = 1.0, omega = 1.0, rn = bn;
+        std::fill(p.begin(), p.end(), 0.0);
+        while (it < max_iter) {
+            double const rho_new = dotp(n, r0.data(), r.data());
+            double const beta = (rho_new / rho) * (alpha / omega);
+            for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+            M.apply(p.data(), ph.data());
+            spmv(A, ph.data(), v.data());
+            alpha = rho_new / dotp(n, r0.data(), v.data());
+            for (int64_t i = 0; i < n; ++i) sv[i] = r[i] - alpha * v[i];
+            ++it;
+            double const sn_ = nrm2(n, sv.data());
+            if (sn_ <= target) {
+                axpy(n, alpha, ph.data(), x);
+                rn = sn_;
+                break;
+            }
+            M.apply(sv.data(), sh.data());
+            spmv(A, sh.data(), tv.data());
+            omega = dotp(n, tv.data(), sv.data()) / dotp(n, tv.data(), tv.data());
+            for (int64_t i = 0; i < n; ++i) {
+                x[i] += alpha * ph[i] + omega * sh[i];
+                r[i] = sv[i] - omega * tv[i];
+            }
+            rho = rho_new;
+            rn = nrm2(n, r.data());
+            if (rn <= target) break;
+        }
+        *final_rel = rn / bn;
+        return it;
+    }
+    if (solver == kGcr) {
+        int const m = std::max(1, dim);
+        std::vector<std::vector<double>> P(m, std::vector<double>(n)), Q(m, std::vector<double>(n));
+        double rn = bn;
+        int k = 0;
+        while (it < max_iter) {
+            if (k == m) k = 0;
+            M.apply(r.data(), P[k].data());
+            spmv(A, P[k].data(), Q[k].data());
+            for (int j = 0; j < k; ++j) {
+                double const h = dotp(n, Q[k].data(), Q[j].data());
+                axpy(n, -h, Q[j].data(), Q[k].data());
+                axpy(n, -h, P[j].data(), P[k].data());
+            }
+            double const qn = nrm2(n, Q[k].data());
+            for (int64_t i = 0; i < n; ++i) {
+                Q[k][i] /= qn;
+                P[k][i] /= qn;
+            }
+            double const alpha = dotp(n, r.data(), Q[k].data());
+            axpy(n, alpha, P[k].data(), x);
+            axpy(n, -alpha, Q[k].data(), r.data());
+            ++k;
+            ++it;
+            rn = nrm2(n, r.data());
+            if (rn <= target) break;
+        }
+        *final_rel = rn / bn;
+        return it;
+    }
+    if (solver == kIdr) {
+        int const s = std::max(1, dim);
+        // shadow space: s orthonormalised Gaussian vectors, fixed seed
+        std::vector<std::vector<double>> P(s, std::vector<double>(n));
+        uint64_t state = 0x9E3779B97F4A7C15ull;
+        auto uniform = [&]() {
+            state ^= state << 13;
+            state ^= state >> 7;
+            state ^= state << 17;
+            return (static_cast<double>(state >> 11) + 0.5) / 9007199254740992.0;
+        };
+        for (int j = 0; j < s; ++j) {
+            for (int64_t i = 0; i < n; ++i) {
+                double const u1 = uniform(), u2 = uniform();
+                P[j][i] = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+            }
+            for (int l = 0; l < j; ++l) axpy(n, -dotp(n, P[j].data(), P[l].data()), P[l].data(), P[j].data());
+            double const pn = nrm2(n, P[j].data());
+            for (int64_t i = 0; i < n; ++i) P[j][i] /= pn;
+        }
+        std::vector<std::vector<double>> G(s, std::vector<double>(n, 0.0)), U(s, std::vector<double>(n, 0.0));
+        std::vector<double> Mm(static_cast<size_t>(s) * s, 0.0), f(s), c(s), vv(n), vh(n), tt(n);
+        for (int j = 0; j < s; ++j) Mm[j * s + j] = 1.0;
+        double om = 1.0, rn = bn;
+        while (it < max_iter) {
+            for (int j = 0; j < s; ++j) f[j] = dotp(n, P[j].data(), r.data());
+            for (int k = 0; k < s && it < max_iter; ++k) {
+                // solve the lower triangular M(k:s, k:s) c = f(k:s)
+                for (int i = k; i < s; ++i) {
+                    double acc = f[i];
+                    for (int j = k; j < i; ++j) acc -= Mm[i * s + j] * c[j];
+                    c[i] = acc / Mm[i * s + i];
+                }
+                vv = r;
+                for (int i = k; i < s; ++i) axpy(n, -c[i], G[i].data(), vv.data());
+                M.apply(vv.data(), vh.data());
+                for (int64_t i = 0; i < n; ++i) {
+                    double acc = om * vh[i];
+                    for (int j = k; j < s; ++j) acc += c[j] * U[j][i];
+                    U[k][i] = acc;
+                }
+                spmv(A, U[k].data(), G[k].data());
+                for (int i = 0; i < k; ++i) {
+                    double const a = dotp(n, P[i].data(), G[k].data()) / Mm[i * s + i];
+                    axpy(n, -a, G[i].data(), G[k].data());
+                    axpy(n, -a, U[i].data(), U[k].data());
+                }
+                for (int i = k; i < s; ++i) Mm[i * s + k] = dotp(n, P[i].data(), G[k].data());
+                double const beta = f[k] / Mm[k * s + k];
+                axpy(n, -beta, G[k].data(), r.data());
+                axpy(n, beta, U[k].data(), x);
+                ++it;
+                rn = nrm2(n, r.data());
+                if (rn <= target) break;
+                for (int i = k + 1; i < s; ++i) f[i] -= beta * Mm[i * s + k];
+            }
+            if (rn <= target || it >= max_iter) break;
+            // the step into the next subspace
+            M.apply(r.data(), vh.data());
+            spmv(A, vh.data(), tt.data());
+            double const tn = dotp(n, tt.data(), tt.data());
+            double const tr = dotp(n, tt.data(), r.data());
+            om = tr / tn;
+            double const rho = std::fabs(tr) / (std::sqrt(tn) * nrm2(n, r.data()));
+            if (rho < 0.7) om *= 0.7 / rho;   // the "maintaining the convergence" safeguard
+            axpy(n, -om, tt.data(), r.data());
+            axpy(n, om, vh.data(), x);
+            ++it;
+            rn = nrm2(n, r.data());
+            if (rn <= target) break;
+        }
+        *final_rel = rn / bn;
+        return it;
+    }
+    return -1;
+}
+
+} // namespace
+
+// solver: 0 cg, 1 minres, 2 fcg, 3 gmres, 4 bicgstab, 5 gcr, 6 idr; dim the
+// GMRES / GCR Krylov dimension or the IDR subspace dimension.  Returns the
+// iterations (-1: unknown solver or a singular ISAI system).
+int silo_csr_krylov(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int solver, int dim,
+                    int kind, const double* params, const double* b, double* x, double tol, int max_iter,
+                    double* final_rel)
+{
+    CsrView const A {n, ptr, col, val};
+    MenuPrecond const m = make_menu(A, kind, params);
+    if (!m.ok) return -1;
+    return krylov_run(A, m, solver, dim, b, x, tol, max_iter, final_rel);
+}

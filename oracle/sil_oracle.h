@@ -189,6 +189,14 @@ int silo_mag3d_nl_solve_menu(int64_t nx, int64_t ny, int64_t nz, const double* x
                              const double* h, int kind, const double* params, const double* rhs, double* sol,
                              double tol, int max_iter, int* newton_steps, double* final_rel);
 
+/* The reference's SIMILIE_SOLVER menu on a CSR matrix with a menu
+ * preconditioner: solver 0 cg, 1 minres, 2 fcg, 3 gmres, 4 bicgstab, 5 gcr,
+ * 6 idr; dim = GMRES / GCR Krylov dimension or IDR subspace dimension.
+ * x from 0 until ||r|| <= tol ||b||; returns the iterations (-1 on error). */
+int silo_csr_krylov(int64_t n, const int64_t* ptr, const int32_t* col, const double* val, int solver, int dim,
+                    int kind, const double* params, const double* b, double* x, double tol, int max_iter,
+                    double* final_rel);
+
 /* Threads OpenMP uses (for reporting). */
 int silo_num_threads(void);
 
