@@ -9,7 +9,6 @@ form-component axis last unless `comp_axis` says otherwise; any strides are
 accepted (component-first and component-last layouts both work).
 """
 import ctypes
-import os
 
 import numpy as np
 

@@ -4,7 +4,6 @@ import ctypes
 import os
 import re
 
-import pytest
 
 import similie_b200 as sil
 from similie_b200 import _native

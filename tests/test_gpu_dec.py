@@ -4,14 +4,13 @@ Bar: the coboundary and its transpose are bit-exact in FP64; the Hodge star,
 codifferential and Laplacian agree with the oracle to 1e-12 relative
 (max-norm over the field); FP32 variants state their error against the FP64
 oracle (bound 1e-5 relative here)."""
-import itertools
 from math import comb
 
 import numpy as np
 import pytest
 
 import oracle as O
-from helpers import (combos, comp_index, gaussian_random_field, kat_field, load_golden, rel_err, sinusoid_field,
+from helpers import (comp_index, gaussian_random_field, kat_field, load_golden, rel_err, sinusoid_field,
                      stretched_coords)
 
 pytestmark = pytest.mark.gpu
