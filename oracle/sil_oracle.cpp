@@ -1477,46 +1477,6 @@ void silo_mag3d_diagonal(int64_t nx, int64_t ny, int64_t nz, const double* x, co
     }
 }
 
-int silo_mag3d_cg(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
-                  const double* node_mu, double gamma, const double* b, double* sol, double tol, int max_iter,
-                  double* final_rel)
-{
-    int64_t const n = 3 * nx * ny * nz;
-    std::vector<double> r(b, b + n), zv(n), p(n), q(n), dinv(n);
-    silo_mag3d_diagonal(nx, ny, nz, x, y, z, node_mu, gamma, dinv.data());
-    for (int64_t i = 0; i < n; ++i) {
-        dinv[i] = 1. / dinv[i];
-        sol[i] = 0.;
-        zv[i] = dinv[i] * r[i];
-        p[i] = zv[i];
-    }
-    double const bnorm = std::sqrt(dot(n, b, b));
-    if (bnorm == 0.) {
-        if (final_rel) *final_rel = 0.;
-        return 0;
-    }
-    double rz = dot(n, r.data(), zv.data());
-    double rnorm = bnorm;
-    int it = 0;
-    while (it < max_iter) {
-        silo_mag3d_apply(nx, ny, nz, x, y, z, node_mu, gamma, p.data(), q.data());
-        double const alpha = rz / dot(n, p.data(), q.data());
-        for (int64_t i = 0; i < n; ++i) {
-            sol[i] += alpha * p[i];
-            r[i] -= alpha * q[i];
-        }
-        ++it;
-        rnorm = std::sqrt(dot(n, r.data(), r.data()));
-        if (rnorm <= tol * bnorm) break;
-        for (int64_t i = 0; i < n; ++i) zv[i] = dinv[i] * r[i];
-        double const rz_new = dot(n, r.data(), zv.data());
-        double const beta = rz_new / rz;
-        rz = rz_new;
-        for (int64_t i = 0; i < n; ++i) p[i] = zv[i] + beta * p[i];
-    }
-    if (final_rel) *final_rel = rnorm / bnorm;
-    return it;
-}
 
 } // extern "C"
 
@@ -1798,6 +1758,7 @@ int newton_core(int64_t N, Apply const& apply, Step const& step, const double* r
 {
     std::vector<double> fa(N), r(N), d(N), cand(N), cand_f(N), cand_r(N);
     apply(x, fa.data());
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < N; ++i) r[i] = rhs[i] - fa[i];
     double const r0 = nrm2(N, r.data());
     int total = 0, steps = 0;
@@ -1815,8 +1776,10 @@ int newton_core(int64_t N, Apply const& apply, Step const& step, const double* r
         double const cur = nrm2(N, r.data());
         double alpha = 1.0, best_alpha = 0.0, best = std::numeric_limits<double>::infinity();
         auto candidate = [&](double al) {
+#pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < N; ++i) cand[i] = x[i] + al * d[i];
             apply(cand.data(), cand_f.data());
+#pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < N; ++i) cand_r[i] = rhs[i] - cand_f[i];
             return nrm2(N, cand_r.data());
         };
@@ -1849,8 +1812,10 @@ int jacobi_cg_step(int64_t N, Jacobian const& jacobian, Diagonal const& diagonal
 {
     std::vector<double> dinv(N), cr(r, r + N), z(N), p(N), q(N);
     diagonal(x, dinv.data());
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < N; ++i) dinv[i] = 1.0 / dinv[i];
     std::fill(d, d + N, 0.0);
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < N; ++i) z[i] = dinv[i] * cr[i];
     p = z;
     double rz = dotp(N, cr.data(), z.data());
@@ -1860,6 +1825,7 @@ int jacobi_cg_step(int64_t N, Jacobian const& jacobian, Diagonal const& diagonal
     while (k < max_iter && rn > tol * bn) {
         jacobian(x, p.data(), q.data());
         double const alpha = rz / dotp(N, p.data(), q.data());
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < N; ++i) {
             d[i] += alpha * p[i];
             cr[i] -= alpha * q[i];
@@ -1867,10 +1833,12 @@ int jacobi_cg_step(int64_t N, Jacobian const& jacobian, Diagonal const& diagonal
         ++k;
         rn = nrm2(N, cr.data());
         if (rn <= tol * bn) break;
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < N; ++i) z[i] = dinv[i] * cr[i];
         double const rz2 = dotp(N, cr.data(), z.data());
         double const beta = rz2 / rz;
         rz = rz2;
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
     }
     return k;
@@ -1883,17 +1851,84 @@ int jacobi_cg_step(int64_t N, Jacobian const& jacobian, Diagonal const& diagonal
 // system to the relative tolerance, then a line search of at most 8 steps
 // halving alpha from 1 that stops at the first candidate below the current
 // residual, else takes the best candidate seen).
-template <class Apply, class Jacobian, class Diagonal>
-int newton_solve(int64_t N, Apply const& apply, Jacobian const& jacobian, Diagonal const& diagonal,
-                 const double* rhs, double* x, double tol, int max_iter, int* newton_steps, double* final_rel)
+// prepare(x) returns the Jacobian at x with apply(v, out) and diagonal(out);
+// its coefficients are evaluated once per Newton step, as on the GPU.
+template <class Apply, class Prepare>
+int newton_solve(int64_t N, Apply const& apply, Prepare const& prepare, const double* rhs, double* x, double tol,
+                 int max_iter, int* newton_steps, double* final_rel)
 {
     return newton_core(
             N, apply,
             [&](const double* xs, const double* r, double* d) {
-                return jacobi_cg_step(N, jacobian, diagonal, xs, r, d, tol, max_iter);
+                auto const J = prepare(xs);
+                return jacobi_cg_step(
+                        N, [&](const double*, const double* v, double* out) { J.apply(v, out); },
+                        [&](const double*, double* out) { J.diagonal(out); }, xs, r, d, tol, max_iter);
             },
             rhs, x, tol, newton_steps, final_rel);
 }
+
+// The 2D Jacobian with the nodes' 2x2 blocks evaluated once at the state;
+// apply and diagonal repeat nl_jacobian_apply / nl_jacobian_diagonal term
+// by term.
+struct Jac2
+{
+    int64_t nx, ny;
+    std::vector<double> c00, c01, c11;
+    Jac2(int64_t nx_, int64_t ny_, NodeLaw const& law, const double* st)
+        : nx(nx_), ny(ny_), c00(nx_ * ny_, 0.0), c01(nx_ * ny_, 0.0), c11(nx_ * ny_, 0.0)
+    {
+#pragma omp parallel for schedule(static)
+        for (int64_t j = 1; j < ny - 1; ++j)
+            for (int64_t i = 1; i < nx - 1; ++i) {
+                int64_t const s = i + nx * j;
+                law.jacobian(s, m0(nx, st, i, j), m1(nx, st, i, j), &c00[s], &c01[s], &c11[s]);
+            }
+    }
+    void apply(const double* x, double* y) const
+    {
+#pragma omp parallel for schedule(static)
+        for (int64_t j = 0; j < ny; ++j) {
+            for (int64_t i = 0; i < nx; ++i) {
+                int64_t const row = i + nx * j;
+                if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) {
+                    y[row] = x[row];
+                    continue;
+                }
+                double residual = 0.0;
+                auto add = [&](double c, int64_t si, int64_t sj, bool first) {
+                    int64_t const s = si + nx * sj;
+                    double const d0 = m0(nx, x, si, sj), d1 = m1(nx, x, si, sj);
+                    residual += c * (first ? (c00[s] * d0 + c01[s] * d1) : (c01[s] * d0 + c11[s] * d1));
+                };
+                if (j - 1 >= 1) add(1.0, i, j - 1, true);
+                add(-1.0, i, j, true);
+                if (i - 1 >= 1) add(-1.0, i - 1, j, false);
+                add(1.0, i, j, false);
+                y[row] = residual;
+            }
+        }
+    }
+    void diagonal(double* diag) const
+    {
+#pragma omp parallel for schedule(static)
+        for (int64_t j = 0; j < ny; ++j) {
+            for (int64_t i = 0; i < nx; ++i) {
+                int64_t const row = i + nx * j;
+                if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) {
+                    diag[row] = 1.0;
+                    continue;
+                }
+                double d = 0.0;
+                if (j - 1 >= 1) d += c00[row - nx];
+                d += c00[row] - c01[row];
+                if (i - 1 >= 1) d += c11[row - 1];
+                d += c11[row] - c01[row];
+                diag[row] = d;
+            }
+        }
+    }
+};
 
 // 3D material law at a sampled node with moments B = (B_x, B_y, B_z):
 // the same Hamiltonian as NodeLaw with q = |B|^2 over three components.
@@ -1935,10 +1970,40 @@ struct Mag3Nl
     Transposed t;
     NodeLaw3 law;
     double gamma;
+    // per interior sampled node s and moment m: its stencil terms
+    // [sptr[3 s + m], sptr[3 s + m + 1]) in moment_stencil's order, and the
+    // Hodge factors hodge_b(s, m), hodge_a(s, c) (3 per node each)
+    std::vector<int64_t> sptr;
+    std::vector<MomentTerm> sterm;
+    std::vector<double> hb, ha;
 
+    void prepare()
+    {
+        int64_t const nn = g.nx * g.ny * g.nz;
+        sptr.assign(3 * nn + 1, 0);
+        hb.assign(3 * nn, 0.0);
+        ha.assign(3 * nn, 0.0);
+        for (int64_t s = 0; s < nn; ++s) {
+            int64_t const i = s % g.nx, j = (s / g.nx) % g.ny, k = s / (g.nx * g.ny);
+            for (int m = 0; m < 3; ++m) {
+                if (g.interior(i, j, k))
+                    for (auto const& term : moment_stencil(g, i, j, k, m)) sterm.push_back(term);
+                sptr[3 * s + m + 1] = static_cast<int64_t>(sterm.size());
+                hb[3 * s + m] = hodge_b(g, i, j, k, m);
+                ha[3 * s + m] = hodge_a(g, i, j, k, m);
+            }
+        }
+    }
+    double moment(int64_t s, int m, const double* a) const
+    {
+        double v = 0.0;
+        for (int64_t e = sptr[3 * s + m]; e < sptr[3 * s + m + 1]; ++e)
+            v += sterm[e].coeff * a[3 * sterm[e].node + sterm[e].comp];
+        return v;
+    }
     void moments(int64_t s, const double* a, double* B) const
     {
-        for (int m = 0; m < 3; ++m) B[m] = moment_value(g, s, m, a);
+        for (int m = 0; m < 3; ++m) B[m] = moment(s, m, a);
     }
     bool interior_node(int64_t s) const
     {
@@ -1960,11 +2025,8 @@ struct Mag3Nl
                     continue;
                 }
                 double residual = 0.0;
-                for (auto const& [s, m, coeff] : t.rows[row]) {
-                    int64_t const si = s % g.nx, sj = (s / g.nx) % g.ny, sk = s / (g.nx * g.ny);
-                    residual += coeff * hodge_b(g, si, sj, sk, m) * v[3 * s + m];
-                }
-                out[row] = residual + gamma * hodge_a(g, i, j, k, c) * a[row];
+                for (auto const& [s, m, coeff] : t.rows[row]) residual += coeff * hb[3 * s + m] * v[3 * s + m];
+                out[row] = residual + gamma * ha[3 * node + c] * a[row];
             }
         }
     }
@@ -2003,6 +2065,72 @@ struct Mag3Nl
         }
         gather(G.data(), x, y);
     }
+    // The Jacobian at st with every sampled node's 3x3 block evaluated once
+    // (the same values jacobian / diagonal compute per call).
+    struct Prepared
+    {
+        Mag3Nl const* op;
+        std::vector<double> J;  // 9 per node
+        void apply(const double* x, double* y) const
+        {
+            Mag3Nl const& o = *op;
+            int64_t const nn = o.g.nx * o.g.ny * o.g.nz;
+            std::vector<double> G(3 * nn, 0.0);
+#pragma omp parallel for schedule(static)
+            for (int64_t s = 0; s < nn; ++s) {
+                if (!o.interior_node(s)) continue;
+                double D[3];
+                o.moments(s, x, D);
+                double const* Js = &J[9 * s];
+                for (int m = 0; m < 3; ++m)
+                    G[3 * s + m] = Js[3 * m] * D[0] + Js[3 * m + 1] * D[1] + Js[3 * m + 2] * D[2];
+            }
+            o.gather(G.data(), x, y);
+        }
+        void diagonal(double* diag) const { op->diagonal_with(J.data(), diag); }
+    };
+    Prepared prepare_jacobian(const double* st) const
+    {
+        int64_t const nn = g.nx * g.ny * g.nz;
+        Prepared p {this, std::vector<double>(9 * nn, 0.0)};
+#pragma omp parallel for schedule(static)
+        for (int64_t s = 0; s < nn; ++s) {
+            if (!interior_node(s)) continue;
+            double B[3];
+            moments(s, st, B);
+            law.jacobian(s, B, &p.J[9 * s]);
+        }
+        return p;
+    }
+    // Diagonal from precomputed node blocks Jn (9 per node): for each entry
+    // (s, m, coeff) of the row, coeff * hodge_b(s, m) * sum_c J_mc(s) *
+    // (coefficient of the row in B_c(s)); plus the gauge term; 1 on boundary
+    // rows.
+    void diagonal_with(const double* Jn, double* diag) const
+    {
+        int64_t const nn = g.nx * g.ny * g.nz;
+#pragma omp parallel for schedule(static)
+        for (int64_t node = 0; node < nn; ++node) {
+            int64_t const i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
+            for (int c = 0; c < 3; ++c) {
+                int64_t const row = 3 * node + c;
+                if (!g.interior(i, j, k)) {
+                    diag[row] = 1.0;
+                    continue;
+                }
+                double d = 0.0;
+                for (auto const& [s, m, coeff] : t.rows[row]) {
+                    double const* J = Jn + 9 * s;
+                    double acc = 0.0;
+                    for (int cc = 0; cc < 3; ++cc)
+                        for (int64_t e = sptr[3 * s + cc]; e < sptr[3 * s + cc + 1]; ++e)
+                            if (sterm[e].node == node && sterm[e].comp == c) acc += J[3 * m + cc] * sterm[e].coeff;
+                    d += coeff * hb[3 * s + m] * acc;
+                }
+                diag[row] = d + gamma * ha[3 * node + c];
+            }
+        }
+    }
     // Diagonal of the Jacobian at st: for each entry (s, m, coeff) of the
     // row, coeff * hodge_b(s, m) * sum_c J_mc(s) * (coefficient of the row in
     // B_c(s)); plus the gauge term; 1 on boundary rows.
@@ -2020,23 +2148,80 @@ struct Mag3Nl
                 }
                 double d = 0.0;
                 for (auto const& [s, m, coeff] : t.rows[row]) {
-                    int64_t const si = s % g.nx, sj = (s / g.nx) % g.ny, sk = s / (g.nx * g.ny);
                     double B[3], J[9];
                     moments(s, st, B);
                     law.jacobian(s, B, J);
                     double acc = 0.0;
                     for (int cc = 0; cc < 3; ++cc)
-                        for (auto const& term : moment_stencil(g, si, sj, sk, cc))
-                            if (term.node == node && term.comp == c) acc += J[3 * m + cc] * term.coeff;
-                    d += coeff * hodge_b(g, si, sj, sk, m) * acc;
+                        for (int64_t e = sptr[3 * s + cc]; e < sptr[3 * s + cc + 1]; ++e)
+                            if (sterm[e].node == node && sterm[e].comp == c) acc += J[3 * m + cc] * sterm[e].coeff;
+                    d += coeff * hb[3 * s + m] * acc;
                 }
-                diag[row] = d + gamma * hodge_a(g, i, j, k, c);
+                diag[row] = d + gamma * ha[3 * node + c];
             }
         }
     }
 };
 
+Mag3Nl make_mag3nl(Grid3 const& g, NodeLaw3 const& law, double gamma)
+{
+    Mag3Nl op {g, transposed_lists(g), law, gamma, {}, {}, {}, {}};
+    op.prepare();
+    return op;
+}
+
 } // namespace
+
+// Ref: the linear 3D CG of silo_mag3d_apply (Jacobi, x0 = 0), the
+// operator's stencil tables built once per solve.
+int silo_mag3d_cg(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
+                  const double* node_mu, double gamma, const double* b, double* sol, double tol, int max_iter,
+                  double* final_rel)
+{
+    int64_t const n = 3 * nx * ny * nz;
+    // the operator of silo_mag3d_apply, its stencil tables built once
+    Grid3 const g {nx, ny, nz, x, y, z};
+    std::vector<double> const no_ferro(nx * ny * nz, 0.0);
+    Mag3Nl const op = make_mag3nl(g, NodeLaw3 {node_mu, no_ferro.data(), nullptr}, gamma);
+    std::vector<double> r(b, b + n), zv(n), p(n), q(n), dinv(n);
+    silo_mag3d_diagonal(nx, ny, nz, x, y, z, node_mu, gamma, dinv.data());
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        dinv[i] = 1. / dinv[i];
+        sol[i] = 0.;
+        zv[i] = dinv[i] * r[i];
+        p[i] = zv[i];
+    }
+    double const bnorm = std::sqrt(dot(n, b, b));
+    if (bnorm == 0.) {
+        if (final_rel) *final_rel = 0.;
+        return 0;
+    }
+    double rz = dot(n, r.data(), zv.data());
+    double rnorm = bnorm;
+    int it = 0;
+    while (it < max_iter) {
+        op.apply(p.data(), q.data());
+        double const alpha = rz / dot(n, p.data(), q.data());
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) {
+            sol[i] += alpha * p[i];
+            r[i] -= alpha * q[i];
+        }
+        ++it;
+        rnorm = std::sqrt(dot(n, r.data(), r.data()));
+        if (rnorm <= tol * bnorm) break;
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) zv[i] = dinv[i] * r[i];
+        double const rz_new = dot(n, r.data(), zv.data());
+        double const beta = rz_new / rz;
+        rz = rz_new;
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) p[i] = zv[i] + beta * p[i];
+    }
+    if (final_rel) *final_rel = rnorm / bnorm;
+    return it;
+}
 
 int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const double* node_ferro, int n,
                         const double* b, const double* h, const double* rhs, double* x, double tol, int max_iter,
@@ -2046,9 +2231,7 @@ int silo_mag2d_nl_solve(int64_t nx, int64_t ny, const double* node_mu, const dou
     NodeLaw const law {node_mu, node_ferro, &c};
     return newton_solve(
             nx * ny, [&](const double* v, double* out) { nl_apply(nx, ny, law, v, out); },
-            [&](const double* st, const double* v, double* out) { nl_jacobian_apply(nx, ny, law, st, v, out); },
-            [&](const double* st, double* out) { nl_jacobian_diagonal(nx, ny, law, st, out); }, rhs, x, tol, max_iter,
-            newton_steps, final_rel);
+            [&](const double* st) { return Jac2(nx, ny, law, st); }, rhs, x, tol, max_iter, newton_steps, final_rel);
 }
 
 void silo_mag3d_nl_apply(int64_t nx, int64_t ny, int64_t nz, const double* x, const double* y, const double* z,
@@ -2057,7 +2240,7 @@ void silo_mag3d_nl_apply(int64_t nx, int64_t ny, int64_t nz, const double* x, co
 {
     BHCurve const c(n, b, h);
     Grid3 const g {nx, ny, nz, x, y, z};
-    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    Mag3Nl const op = make_mag3nl(g, NodeLaw3 {node_mu, node_ferro, &c}, gamma);
     op.apply(a, out);
 }
 
@@ -2068,7 +2251,7 @@ void silo_mag3d_nl_jacobian_apply(int64_t nx, int64_t ny, int64_t nz, const doub
 {
     BHCurve const c(n, b, h);
     Grid3 const g {nx, ny, nz, x, y, z};
-    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    Mag3Nl const op = make_mag3nl(g, NodeLaw3 {node_mu, node_ferro, &c}, gamma);
     op.jacobian(state, v, out);
 }
 
@@ -2078,7 +2261,7 @@ void silo_mag3d_nl_jacobian_diagonal(int64_t nx, int64_t ny, int64_t nz, const d
 {
     BHCurve const c(n, b, h);
     Grid3 const g {nx, ny, nz, x, y, z};
-    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    Mag3Nl const op = make_mag3nl(g, NodeLaw3 {node_mu, node_ferro, &c}, gamma);
     op.diagonal(state, diag);
 }
 
@@ -2089,11 +2272,10 @@ int silo_mag3d_nl_solve(int64_t nx, int64_t ny, int64_t nz, const double* x, con
 {
     BHCurve const c(n, b, h);
     Grid3 const g {nx, ny, nz, x, y, z};
-    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    Mag3Nl const op = make_mag3nl(g, NodeLaw3 {node_mu, node_ferro, &c}, gamma);
     return newton_solve(
             3 * nx * ny * nz, [&](const double* v, double* out) { op.apply(v, out); },
-            [&](const double* st, const double* v, double* out) { op.jacobian(st, v, out); },
-            [&](const double* st, double* out) { op.diagonal(st, out); }, rhs, sol, tol, max_iter, newton_steps,
+            [&](const double* st) { return op.prepare_jacobian(st); }, rhs, sol, tol, max_iter, newton_steps,
             final_rel);
 }
 
@@ -2384,6 +2566,7 @@ int pcg_run(CsrView const& A, MenuPrecond const& m, const double* b, double* x, 
     while (it < max_iter) {
         spmv(A, p.data(), q.data());
         double const alpha = rz / dotp(n, p.data(), q.data());
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < n; ++i) {
             x[i] += alpha * p[i];
             r[i] -= alpha * q[i];
@@ -2395,6 +2578,7 @@ int pcg_run(CsrView const& A, MenuPrecond const& m, const double* b, double* x, 
         double const rz2 = dotp(n, r.data(), z.data());
         double const beta = rz2 / rz;
         rz = rz2;
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
     }
     *final_rel = rnorm / bnorm;
@@ -2520,7 +2704,7 @@ int silo_mag3d_nl_solve_menu(int64_t nx, int64_t ny, int64_t nz, const double* x
 {
     BHCurve const c(n, b, h);
     Grid3 const g {nx, ny, nz, x, y, z};
-    Mag3Nl const op {g, transposed_lists(g), NodeLaw3 {node_mu, node_ferro, &c}, gamma};
+    Mag3Nl const op = make_mag3nl(g, NodeLaw3 {node_mu, node_ferro, &c}, gamma);
     return newton_menu(
             3, nx, ny, nz, [&](const double* v, double* out) { op.apply(v, out); },
             [&](const double* st, const double* v, double* out) { op.jacobian(st, v, out); }, kind, params, rhs, sol,
