@@ -420,23 +420,50 @@ MENU_DEFAULTS = {"sor_relaxation_factor": 1.2, "chebyshev_iterations": 8, "cheby
                  "chebyshev_upper_bound": 1.5, "ir_iterations": 8, "ir_relaxation_factor": 1.0}
 
 
-def _probe_assemble(n, offsets_of_row, color_of, ncolors, apply):
-    """CSR of a linear operator whose row r only touches the columns
-    offsets_of_row(r) (sorted), by one apply per column colour (columns of one
-    colour never share a row).  Exact zeros are dropped, columns ascending."""
+def _offset3(target, at):
+    """The offset d in {-1, 0, 1} with (at + d) mod 3 == target."""
+    d = (target - at % 3) % 3
+    return np.where(d == 2, -1, d)
+
+
+def _probe_assemble(dims, apply):
+    """CSR of a linear operator whose row touches only columns in the 3x3
+    (2D nodes) or 3x3x3 (3D nodes x 3 components) neighbourhood, by one apply
+    per column colour (node coordinates mod 3, and component): columns of one
+    colour never share a row.  Exact zeros are dropped, columns ascending."""
     import scipy.sparse as sp
+    if len(dims) == 2:
+        nx, ny = dims
+        n = nx * ny
+        r = np.arange(n)
+        i, j, k = r % nx, r // nx, np.zeros(n, dtype=np.int64)
+        colors = [(cx, cy, 0, None) for cy in range(3) for cx in range(3)]
+        col_color = (r % nx) % 3 + 3 * ((r // nx) % 3)
+    else:
+        nx, ny, nz = dims
+        n = 3 * nx * ny * nz
+        r = np.arange(n)
+        node = r // 3
+        i, j, k = node % nx, (node // nx) % ny, node // (nx * ny)
+        colors = [(cx, cy, cz, c) for cz in range(3) for cy in range(3) for cx in range(3) for c in range(3)]
+        col_color = (r % 3) + 3 * (i % 3 + 3 * (j % 3) + 9 * (k % 3))
     rows, cols, vals = [], [], []
-    colors = color_of(np.arange(n))
-    for k in range(ncolors):
-        probe = (colors == k).astype(np.float64)
-        y = apply(probe)
-        for r in range(n):
-            for c in offsets_of_row(r):
-                if colors[c] == k and y[r] != 0.0:
-                    rows.append(r)
-                    cols.append(c)
-                    vals.append(y[r])
-    A = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    for cx, cy, cz, c in colors:
+        color = cx + 3 * cy if len(dims) == 2 else c + 3 * (cx + 3 * cy + 9 * cz)
+        y = apply((col_color == color).astype(np.float64))
+        di, dj = _offset3(cx, i), _offset3(cy, j)
+        ok = (i + di >= 0) & (i + di < nx) & (j + dj >= 0) & (j + dj < ny)
+        if len(dims) == 2:
+            col = (i + di) + nx * (j + dj)
+        else:
+            dk = _offset3(cz, k)
+            ok &= (k + dk >= 0) & (k + dk < nz)
+            col = 3 * ((i + di) + nx * ((j + dj) + ny * (k + dk))) + c
+        ok &= y != 0.0
+        rows.append(r[ok])
+        cols.append(col[ok])
+        vals.append(y[ok])
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
     A.sort_indices()
     return A
 
@@ -444,38 +471,14 @@ def _probe_assemble(n, offsets_of_row, color_of, ncolors, apply):
 def assemble2d(nx, ny, node_mu):
     """The 2D operator as a CSR matrix (the reference's assemble_matrix_data,
     onelab_interface/magnetostatics_onelab.hpp:3554-3737), probed through
-    mag2d_apply: every row lies in the 3x3 node neighbourhood, so nine
-    colours (i mod 3, j mod 3) separate the columns of a row."""
-    def nbrs(r):
-        i, j = r % nx, r // nx
-        return [(i + di) + nx * (j + dj) for dj in (-1, 0, 1) for di in (-1, 0, 1)
-                if 0 <= i + di < nx and 0 <= j + dj < ny]
-    def color(c):
-        return (c % nx) % 3 + 3 * ((c // nx) % 3)
-    return _probe_assemble(nx * ny, nbrs, color, 9, lambda v: mag2d_apply(nx, ny, node_mu, v))
+    mag2d_apply with nine colours (i mod 3, j mod 3)."""
+    return _probe_assemble((nx, ny), lambda v: mag2d_apply(nx, ny, node_mu, v))
 
 
 def assemble3d(x, y, z, node_mu, gamma):
     """The 3D operator as a CSR matrix (magnetostatics_onelab.hpp:3120-3534),
-    probed through mag3d_apply: rows lie in the 3x3x3 node neighbourhood, so
-    27 node colours times 3 components separate the columns of a row."""
-    nx, ny, nz = len(x), len(y), len(z)
-    def nbrs(r):
-        node, comp = divmod(r, 3)
-        i, j, k = node % nx, (node // nx) % ny, node // (nx * ny)
-        out = []
-        for dk in (-1, 0, 1):
-            for dj in (-1, 0, 1):
-                for di in (-1, 0, 1):
-                    if 0 <= i + di < nx and 0 <= j + dj < ny and 0 <= k + dk < nz:
-                        m = (i + di) + nx * ((j + dj) + ny * (k + dk))
-                        out.extend(3 * m + c for c in range(3))
-        return out
-    def color(c):
-        node, comp = c // 3, c % 3
-        i, j, k = node % nx, (node // nx) % ny, node // (nx * ny)
-        return comp + 3 * (i % 3 + 3 * (j % 3) + 9 * (k % 3))
-    return _probe_assemble(3 * nx * ny * nz, nbrs, color, 81, lambda v: mag3d_apply(x, y, z, node_mu, gamma, v))
+    probed through mag3d_apply with 27 node colours times 3 components."""
+    return _probe_assemble((len(x), len(y), len(z)), lambda v: mag3d_apply(x, y, z, node_mu, gamma, v))
 
 
 def _csr_args(A):
@@ -536,14 +539,8 @@ def csr_pcg(A, b, kind="jacobi", tol=1e-10, max_iter=100000, **params):
 
 def jacobian2d_csr(nx, ny, node_mu, node_ferro, curve_b, curve_h, state):
     """The 2D nonlinear operator's Jacobian at `state` as a CSR matrix (probed)."""
-    def nbrs(r):
-        i, j = r % nx, r // nx
-        return [(i + di) + nx * (j + dj) for dj in (-1, 0, 1) for di in (-1, 0, 1)
-                if 0 <= i + di < nx and 0 <= j + dj < ny]
-    def color(c):
-        return (c % nx) % 3 + 3 * ((c // nx) % 3)
-    return _probe_assemble(nx * ny, nbrs, color, 9,
-                           lambda v: mag2d_nl_jacobian_apply(nx, ny, node_mu, node_ferro, curve_b, curve_h, state, v))
+    return _probe_assemble((nx, ny), lambda v: mag2d_nl_jacobian_apply(nx, ny, node_mu, node_ferro, curve_b, curve_h,
+                                                                       state, v))
 
 
 def mag2d_nl_solve_menu(nx, ny, node_mu, node_ferro, curve_b, curve_h, rhs, kind, x0=None, tol=1e-10,
