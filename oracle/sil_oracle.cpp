@@ -2437,10 +2437,12 @@ struct MenuPrecond
             std::copy(r, r + n, z);
             return;
         case kJacobi:
+#pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < n; ++i) z[i] = dinv[i] * r[i];
             return;
         case kSpdIsai: {
             std::vector<double> t(n, 0.0);
+#pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < n; ++i) {
                 double s = 0.0;
                 for (int64_t k = mptr[i]; k < mptr[i + 1]; ++k) s += mval[k] * r[mcol[k]];
@@ -2452,6 +2454,7 @@ struct MenuPrecond
             return;
         }
         case kGeneralIsai:
+#pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < n; ++i) {
                 double s = 0.0;
                 for (int64_t k = mptr[i]; k < mptr[i + 1]; ++k) s += mval[k] * r[mcol[k]];
@@ -2482,6 +2485,7 @@ struct MenuPrecond
             double const sigma = theta / delta;
             double rho = 1.0 / sigma;
             std::vector<double> d(n), res(n), ax(n);
+#pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < n; ++i) {
                 d[i] = dinv[i] * r[i] / theta;
                 z[i] = d[i];
@@ -2489,6 +2493,7 @@ struct MenuPrecond
             for (int it = 1; it < cheb_iters; ++it) {
                 spmv(A, z, ax.data());
                 double const rho1 = 1.0 / (2.0 * sigma - rho);
+#pragma omp parallel for schedule(static)
                 for (int64_t i = 0; i < n; ++i) {
                     res[i] = r[i] - ax[i];
                     d[i] = rho1 * rho * d[i] + (2.0 * rho1 / delta) * (dinv[i] * res[i]);
@@ -2500,9 +2505,11 @@ struct MenuPrecond
         }
         case kIrJacobi: {
             std::vector<double> ax(n);
+#pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < n; ++i) z[i] = ir_omega * (dinv[i] * r[i]);
             for (int it = 1; it < ir_iters; ++it) {
                 spmv(A, z, ax.data());
+#pragma omp parallel for schedule(static)
                 for (int64_t i = 0; i < n; ++i) z[i] += ir_omega * (dinv[i] * (r[i] - ax[i]));
             }
             return;
