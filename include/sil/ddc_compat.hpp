@@ -31,7 +31,10 @@
 // synchronous, and errors are thrown (Error, carrying the sil_status).
 #pragma once
 
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -291,6 +294,91 @@ struct StrongFormulationSolverSettings
     double ir_relaxation_factor = 1.0;
 };
 
+// The reference's SIMILIE_* environment overrides
+// (solvers/minimize_strong_formulation_residual.hpp:148-218, 932-942,
+// 1069-1130, 1510-1515; onelab_interface/magnetostatics_onelab.hpp:796-828).
+// Those whose meaning this library implements are applied; those it does not
+// (another Krylov solver, a flipped y response, another line search) raise
+// SIL_ERR_UNSUPPORTED instead of being ignored.
+namespace env {
+
+// set, non-empty and not starting with '0'
+inline bool flag(char const* name)
+{
+    char const* const v = std::getenv(name);
+    return v != nullptr && v[0] != '\0' && v[0] != '0';
+}
+
+// the value as a number, or `fallback` when unset, empty or not a number
+inline double number_or(char const* name, double fallback)
+{
+    char const* const v = std::getenv(name);
+    if (v == nullptr || v[0] == '\0') return fallback;
+    char* end = nullptr;
+    double const x = std::strtod(v, &end);
+    return end == v ? fallback : x;
+}
+
+// -1 for a negative number, else 1 (unset, empty, zero or not a number)
+inline double sign_or_one(char const* name)
+{
+    double const x = number_or(name, 0.0);
+    return x < 0.0 ? -1.0 : 1.0;
+}
+
+}  // namespace env
+
+// SIMILIE_PRECONDITIONER first, then SIMILIE_DISABLE_JACOBI_PRECONDITIONER
+// (Identity), else the settings' choice (selected_preconditioner, 932-942).
+inline PreconditionerType selected_preconditioner(StrongFormulationSolverSettings const& settings)
+{
+    char const* const v = std::getenv("SIMILIE_PRECONDITIONER");
+    if (v != nullptr && v[0] != '\0') return parse_preconditioner(v);
+    if (env::flag("SIMILIE_DISABLE_JACOBI_PRECONDITIONER")) return PreconditionerType::Identity;
+    return settings.preconditioner;
+}
+
+inline void check_supported_environment()
+{
+    char const* const solver = std::getenv("SIMILIE_SOLVER");
+    if (solver != nullptr && solver[0] != '\0' && std::string(solver) != "cg")
+        throw Error(SIL_ERR_UNSUPPORTED, std::string("SIMILIE_SOLVER=") + solver + ": only cg is available");
+    if (env::sign_or_one("SIMILIE_MAGNETIC_Y_RESPONSE_SIGN_3D") < 0.0)
+        throw Error(SIL_ERR_UNSUPPORTED, "SIMILIE_MAGNETIC_Y_RESPONSE_SIGN_3D < 0 is not available");
+    if (env::number_or("SIMILIE_NONLINEAR_LINE_SEARCH_STEPS", 8.0) != 8.0
+        || env::number_or("SIMILIE_NONLINEAR_LINE_SEARCH_REDUCTION", 0.5) != 0.5)
+        throw Error(SIL_ERR_UNSUPPORTED, "the line search is fixed at 8 halving steps");
+}
+
+// The settings a solve uses: the environment's preconditioner and SOR
+// relaxation factor over the caller's.
+inline StrongFormulationSolverSettings with_environment(StrongFormulationSolverSettings settings)
+{
+    check_supported_environment();
+    settings.preconditioner = selected_preconditioner(settings);
+    settings.sor_relaxation_factor = env::number_or("SIMILIE_SOR_RELAXATION_FACTOR", settings.sor_relaxation_factor);
+    return settings;
+}
+
+// SIMILIE_SOLVER_TIMING: one line per solver stage on stdout.
+class StageTimer
+{
+public:
+    StageTimer() : on_(env::flag("SIMILIE_SOLVER_TIMING")), t0_(std::chrono::steady_clock::now()) {}
+    void done(char const* stage)
+    {
+        auto const t1 = std::chrono::steady_clock::now();
+        if (on_)
+            std::printf("SimiLie solver stage: %s duration=%.6f\n", stage,
+                        std::chrono::duration<double>(t1 - t0_).count());
+        t0_ = t1;
+    }
+
+private:
+    bool on_;
+    std::chrono::steady_clock::time_point t0_;
+};
+
 struct StrongFormulationSolverDiagnostics
 {
     unsigned int iterations = 0;
@@ -336,8 +424,12 @@ struct MagnetostaticsOperator3D
         p.node_mu = node_mu;
         p.rhs = rhs;
         p.solution = solution;
-        p.gauge_penalty = gauge_penalty;
-        p.gauge = divergence_gauge ? 1 : 0;
+        // SIMILIE_DIVERGENCE_GAUGE_3D selects the divergence gauge, whose
+        // factor takes the sign SIMILIE_VECTOR_POTENTIAL_GAUGE_SIGN_3D
+        bool const divergence = divergence_gauge || env::flag("SIMILIE_DIVERGENCE_GAUGE_3D");
+        p.gauge = divergence ? 1 : 0;
+        p.gauge_penalty = divergence ? gauge_penalty * env::sign_or_one("SIMILIE_VECTOR_POTENTIAL_GAUGE_SIGN_3D")
+                                     : gauge_penalty;
         return p;
     }
     void apply(ExecSpace exec, double const* in, double* out) const
@@ -518,17 +610,31 @@ inline sil_menu_settings to_menu(StrongFormulationSolverSettings const& settings
 // (solve_linearized_system with an assembled system matrix).
 inline StrongFormulationSolverDiagnostics solve_assembled(ExecSpace exec, CsrMatrix const& m, double const* rhs,
                                                           double* solution,
-                                                          StrongFormulationSolverSettings const& settings)
+                                                          StrongFormulationSolverSettings const& settings,
+                                                          StageTimer& timer)
 {
     sil_menu_settings const cfg = to_menu(settings);
     sil_csr_precond pc = nullptr;
     check(sil_csr_precond_create(exec.stream, m.get(), &cfg, &pc), "build_preconditioner");
+    timer.done("preconditioner build");
     sil_solve_settings const s = to_settings(settings);
     sil_solve_diagnostics d {};
     sil_status const st = sil_csr_solve(exec.stream, m.get(), pc, rhs, solution, &s, &d);
     sil_csr_precond_destroy(pc);
     check(st, "minimize_strong_formulation_residual");
+    timer.done("solve");
     return to_diagnostics(d, false);
+}
+
+template <class Operator>
+StrongFormulationSolverDiagnostics assemble_and_solve(ExecSpace exec, Operator const& op, double const* rhs,
+                                                      double* solution,
+                                                      StrongFormulationSolverSettings const& settings)
+{
+    StageTimer timer;
+    CsrMatrix const m = assemble_matrix_data(exec, op);
+    timer.done("matrix build");
+    return solve_assembled(exec, m, rhs, solution, settings, timer);
 }
 
 }  // namespace detail
@@ -537,53 +643,63 @@ inline StrongFormulationSolverDiagnostics solve_assembled(ExecSpace exec, CsrMat
 // one from the content of `solution`.  Synchronous.
 inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
         ExecSpace exec, MagnetostaticsOperator2D const& op, double const* rhs, double* solution,
-        StrongFormulationSolverSettings const& settings)
+        StrongFormulationSolverSettings const& requested)
 {
-    if (detail::assembled(settings))
-        return detail::solve_assembled(exec, assemble_matrix_data(exec, op), rhs, solution, settings);
+    StrongFormulationSolverSettings const settings = with_environment(requested);
+    if (detail::assembled(settings)) return detail::assemble_and_solve(exec, op, rhs, solution, settings);
+    StageTimer timer;
     sil_mag2d_problem p {op.nx, op.ny, op.node_mu, rhs, solution};
     sil_solve_settings const s = detail::to_settings(settings);
     sil_solve_diagnostics d {};
     check(sil_mag2d_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
+    timer.done("solve");
     return detail::to_diagnostics(d, false);
 }
 
 inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
         ExecSpace exec, MagnetostaticsOperator3D const& op, double const* rhs, double* solution,
-        StrongFormulationSolverSettings const& settings)
+        StrongFormulationSolverSettings const& requested)
 {
-    if (detail::assembled(settings))
-        return detail::solve_assembled(exec, assemble_matrix_data(exec, op), rhs, solution, settings);
+    StrongFormulationSolverSettings const settings = with_environment(requested);
+    if (detail::assembled(settings)) return detail::assemble_and_solve(exec, op, rhs, solution, settings);
+    StageTimer timer;
     sil_mag3d_problem const p = op.problem(rhs, solution);
     sil_solve_settings const s = detail::to_settings(settings);
     sil_solve_diagnostics d {};
     check(sil_mag3d_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
+    timer.done("solve");
     return detail::to_diagnostics(d, false);
 }
 
 inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
         ExecSpace exec, NonlinearMagnetostaticsOperator2D const& op, double const* rhs, double* solution,
-        StrongFormulationSolverSettings const& settings)
+        StrongFormulationSolverSettings const& requested)
 {
+    StrongFormulationSolverSettings const settings = with_environment(requested);
+    StageTimer timer;
     sil_mag2d_nl_problem const p = op.problem(rhs, solution);
     sil_solve_settings s = detail::to_settings(settings);
     sil_menu_settings const menu = detail::to_menu(settings);
     if (detail::assembled(settings)) s.jacobian_preconditioner = &menu;
     sil_solve_diagnostics d {};
     check(sil_mag2d_nl_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
+    timer.done("nonlinear solve");
     return detail::to_diagnostics(d, true);
 }
 
 inline StrongFormulationSolverDiagnostics minimize_strong_formulation_residual(
         ExecSpace exec, NonlinearMagnetostaticsOperator3D const& op, double const* rhs, double* solution,
-        StrongFormulationSolverSettings const& settings)
+        StrongFormulationSolverSettings const& requested)
 {
+    StrongFormulationSolverSettings const settings = with_environment(requested);
+    StageTimer timer;
     sil_mag3d_nl_problem const p = op.problem(rhs, solution);
     sil_solve_settings s = detail::to_settings(settings);
     sil_menu_settings const menu = detail::to_menu(settings);
     if (detail::assembled(settings)) s.jacobian_preconditioner = &menu;
     sil_solve_diagnostics d {};
     check(sil_mag3d_nl_solve_batch(&p, 1, &s, &d, exec.stream), "minimize_strong_formulation_residual");
+    timer.done("nonlinear solve");
     return detail::to_diagnostics(d, true);
 }
 

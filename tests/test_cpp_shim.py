@@ -25,6 +25,19 @@ def test_shim_and_example_compile():
                            "-I", os.path.join(ROOT, "include"), "-I", os.path.join(CUDA, "include"), EXAMPLE])
 
 
+@pytest.mark.skipif(_gxx() is None, reason="no g++")
+def test_environment_overrides(tmp_path):
+    """The reference's SIMILIE_* overrides: applied where the library has the
+    feature, refused with SIL_ERR_UNSUPPORTED where it has not (no GPU call)."""
+    exe = str(tmp_path / "shim_env")
+    subprocess.check_call([_gxx(), "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                           "-I", os.path.join(CUDA, "include"), os.path.join(ROOT, "tests", "cpp", "shim_env.cpp"),
+                           "-o", exe])
+    env = {k: v for k, v in os.environ.items() if not k.startswith("SIMILIE_")}
+    out = subprocess.run([exe], check=True, capture_output=True, text=True, env=env).stdout
+    assert out.strip().endswith("env ok"), out
+
+
 @pytest.mark.gpu
 def test_example_matches_the_oracle(tmp_path):
     lib = os.path.join(ROOT, "similie_b200", "libsil_b200.so")
