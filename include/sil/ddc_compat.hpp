@@ -40,6 +40,8 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../sil_b200.h"
 
 namespace sil {
@@ -360,17 +362,26 @@ inline StrongFormulationSolverSettings with_environment(StrongFormulationSolverS
     return settings;
 }
 
-// SIMILIE_SOLVER_TIMING: one line per solver stage on stdout.
+// The solver's stages: an NVTX range around the whole solve (seen by
+// profilers, free otherwise) and, with SIMILIE_SOLVER_TIMING, one line per
+// stage on stdout.
 class StageTimer
 {
 public:
-    StageTimer() : on_(env::flag("SIMILIE_SOLVER_TIMING")), t0_(std::chrono::steady_clock::now()) {}
+    StageTimer() : on_(env::flag("SIMILIE_SOLVER_TIMING")), t0_(std::chrono::steady_clock::now())
+    {
+        nvtxRangePushA("minimize_strong_formulation_residual");
+    }
+    ~StageTimer() { nvtxRangePop(); }
+    StageTimer(StageTimer const&) = delete;
+    StageTimer& operator=(StageTimer const&) = delete;
     void done(char const* stage)
     {
         auto const t1 = std::chrono::steady_clock::now();
         if (on_)
             std::printf("SimiLie solver stage: %s duration=%.6f\n", stage,
                         std::chrono::duration<double>(t1 - t0_).count());
+        nvtxMarkA(stage);
         t0_ = t1;
     }
 
