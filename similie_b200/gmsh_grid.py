@@ -166,3 +166,55 @@ def problem_from_grid(coords, cell_tags, mu_by_tag, j_by_tag, mu_default=1.0):
     cell_mu = np.array([mu_by_tag.get(int(t), mu_default) for t in tags], dtype=np.float64)
     cell_j = np.array([j_by_tag.get(int(t), 0.0) for t in tags], dtype=np.float64)
     return mag.Problem(x, y, cell_mu, cell_j, {"source": "gmsh"})
+
+
+def cell_inputs_from_tags(cell_tags, dim, magnetic_material_tags=(), positive_conductor_tags=(),
+                          negative_conductor_tags=(), positive_conductor_x_tags=(), negative_conductor_x_tags=(),
+                          mu0=1.0, core_mu=1000.0, current_density_z=0.0, current_density_x=0.0, nonlinear=False):
+    """The reference's tag-to-cell-input rule (onelab_interface/
+    magnetostatics_onelab.hpp:4376-4397 in 2D, 4870-4897 in 3D): the first
+    group a cell's physical tag belongs to decides, in the order magnetic
+    material (permeability core_mu, and the nonlinear flag when the run uses
+    the nonlinear material), conductors along +x / -x (3D only), conductors
+    along +z / -z; any other cell is air (permeability mu0, no current).
+
+    Returns (cell_mu, cell_j, cell_nonlinear, counts): cell_j has one
+    component in 2D (J_z) and three in 3D, counts the core, coil and air
+    cells."""
+    tags = np.asarray(cell_tags).ravel().astype(np.int64)
+    n = tags.size
+    cell_mu = np.full(n, float(mu0))
+    cell_j = np.zeros((n, 3))
+    cell_nl = np.zeros(n, dtype=bool)
+    counts = {"core": 0, "coil": 0, "air": 0}
+    groups = [("core", magnetic_material_tags, None, 0.0)]
+    if dim == 3:
+        groups += [("coil", positive_conductor_x_tags, 0, current_density_x),
+                   ("coil", negative_conductor_x_tags, 0, -current_density_x)]
+    groups += [("coil", positive_conductor_tags, 2, current_density_z),
+               ("coil", negative_conductor_tags, 2, -current_density_z)]
+    decided = np.zeros(n, dtype=bool)
+    for kind, group, comp, value in groups:
+        hit = np.isin(tags, np.asarray(list(group), dtype=np.int64)) & ~decided
+        if kind == "core":
+            cell_mu[hit] = core_mu
+            cell_nl[hit] = bool(nonlinear)
+        else:
+            cell_j[hit, comp] = value
+        counts[kind] += int(hit.sum())
+        decided |= hit
+    counts["air"] = int((~decided).sum())
+    return cell_mu, (cell_j[:, 2].copy() if dim == 2 else cell_j.ravel()), cell_nl, counts
+
+
+def problem3d_from_grid(coords, cell_tags, gamma=None, **rules):
+    """A 3D magnetostatics Problem from a structured hexahedral grid by the
+    reference's tag rule (cell_inputs_from_tags); returns (problem,
+    cell_nonlinear, counts).  With the nonlinear material, the node
+    ferromagnetic share is magnetostatics3d.node_ferro(nx, ny, nz,
+    cell_nonlinear)."""
+    from . import magnetostatics3d as m3
+    x, y, z = (np.asarray(c, dtype=np.float64) for c in coords)
+    cell_mu, cell_j, cell_nl, counts = cell_inputs_from_tags(cell_tags, 3, **rules)
+    g = m3.DEFAULT_GAUGE_PENALTY if gamma is None else gamma
+    return m3.Problem(x, y, z, cell_mu, cell_j, g, {"source": "gmsh"}), cell_nl, counts

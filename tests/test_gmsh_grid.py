@@ -140,3 +140,46 @@ def test_xdmf_export_round_trip(tmp_path):
         np.testing.assert_array_equal(c, r)
     np.testing.assert_array_equal(fields["A"], a)
     np.testing.assert_array_equal(fields["B"], b)
+
+
+def test_tag_rule_precedence_and_counts():
+    import similie_b200.gmsh_grid as gg
+    tags = np.array([1, 2, 3, 4, 5, 6, 7, 1])
+    rules = dict(magnetic_material_tags=(1, 4), positive_conductor_tags=(2, 4), negative_conductor_tags=(3,),
+                 positive_conductor_x_tags=(5,), negative_conductor_x_tags=(6, 2), mu0=1.0, core_mu=500.0,
+                 current_density_z=2.0, current_density_x=3.0, nonlinear=True)
+    mu, j, nl, counts = gg.cell_inputs_from_tags(tags, 3, **rules)
+    j = j.reshape(-1, 3)
+    # 4 is both material and conductor: the material comes first
+    np.testing.assert_array_equal(mu, [500, 1, 1, 500, 1, 1, 1, 500])
+    np.testing.assert_array_equal(nl, [1, 0, 0, 1, 0, 0, 0, 1])
+    # 2 is a -x conductor and a +z conductor: x groups come first in 3D
+    np.testing.assert_array_equal(j[:, 0], [0, -3, 0, 0, 3, -3, 0, 0])
+    np.testing.assert_array_equal(j[:, 2], [0, 0, -2, 0, 0, 0, 0, 0])
+    assert counts == {"core": 3, "coil": 4, "air": 1}
+    # 2D: no x groups, J_z only
+    mu2, j2, nl2, c2 = gg.cell_inputs_from_tags(tags, 2, **rules)
+    np.testing.assert_array_equal(j2, [0, 2, -2, 0, 0, 0, 0, 0])
+    assert c2 == {"core": 3, "coil": 2, "air": 3}
+
+
+def test_hexahedral_mesh_to_3d_problem(tmp_path):
+    import similie_b200.gmsh_grid as gg
+    import similie_b200.magnetostatics3d as m3
+    rng = np.random.default_rng(5)
+    coords = [np.cumsum(rng.uniform(0.5, 1.5, n)) for n in (5, 4, 6)]
+    tags = rng.choice([10, 20, 30], size=(5, 3, 4))   # (ncz, ncy, ncx), x fastest
+    path = str(tmp_path / "box.msh")
+    gg.write_msh2(path, coords, tags.ravel(), seed=3)
+    dim, got_coords, got_tags, _ = gg.read_structured_grid(path)
+    assert dim == 3
+    prob, nl, counts = gg.problem3d_from_grid(got_coords, got_tags, magnetic_material_tags=(10,),
+                                              positive_conductor_tags=(20,), core_mu=1000.0,
+                                              current_density_z=1.5, nonlinear=True)
+    flat = tags.ravel()
+    np.testing.assert_array_equal(prob.cell_mu, np.where(flat == 10, 1000.0, 1.0))
+    np.testing.assert_array_equal(prob.cell_j.reshape(-1, 3)[:, 2], np.where(flat == 20, 1.5, 0.0))
+    assert counts["air"] == int((flat == 30).sum())
+    ferro = m3.node_ferro(5, 4, 6, nl)
+    assert ferro.shape == (5 * 4 * 6,) and ferro.max() <= 1.0
+    assert prob.rhs().shape == (3 * 5 * 4 * 6,)
