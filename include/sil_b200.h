@@ -311,7 +311,8 @@ sil_status sil_mag2d_nl_apply_jacobian(sil_stream stream, const sil_mag2d_nl_pro
 /* Newton solve of every problem of the batch: at most 30 steps, each
  * solving J(x) d = r by Jacobi-preconditioned CG (FP64) to
  * settings->relative_tolerance (at most settings->max_iterations
- * iterations), then a line search of at most 8 candidates x + alpha d,
+ * iterations; with settings->jacobian_preconditioner, CG with that menu
+ * preconditioner on the Jacobian assembled at x), then a line search of at most 8 candidates x + alpha d,
  * alpha halving from 1, that stops at the first residual below the current
  * one, else takes the best seen.  Converged when ||b - F(x)|| <= tol *
  * ||b - F(x0)||.  diag: iterations = all CG iterations, refinements =
@@ -350,8 +351,9 @@ sil_status sil_mag3d_nl_apply_jacobian(sil_stream stream, const sil_mag3d_nl_pro
                                        const double* x, double* y);
 
 /* Newton solve of every 3D problem of the batch, the scheme of
- * sil_mag2d_nl_solve_batch (Jacobi-CG on the Jacobian, halving line
- * search).  Synchronous. */
+ * sil_mag2d_nl_solve_batch (Jacobi-CG on the Jacobian, or the settings'
+ * jacobian_preconditioner on the assembled Jacobian; halving line search).
+ * Synchronous. */
 sil_status sil_mag3d_nl_solve_batch(const sil_mag3d_nl_problem* problems, int nproblems,
                                     const sil_solve_settings* settings, sil_solve_diagnostics* diag,
                                     sil_stream stream);
