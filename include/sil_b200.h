@@ -331,7 +331,7 @@ sil_status sil_mag2d_nl_solve_batch(const sil_mag2d_nl_problem* problems, int np
  *   magnetostatics_onelab.hpp:5110-5126 (nonlinear dispatch), 2241-2396
  *   (operator, dpotential_dt of the equations), 2924-3110 (apply_jacobian). */
 typedef struct sil_mag3d_nl_problem {
-    int64_t nx, ny, nz;       /* nodes per axis (>= 3) */
+    int64_t nx, ny, nz;       /* nodes per axis (>= 3), nx*ny*nz < 2^31 / 9 */
     const double* x;          /* HOST, nx strictly increasing node coordinates */
     const double* y;          /* HOST, ny */
     const double* z;          /* HOST, nz */

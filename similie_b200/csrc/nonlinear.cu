@@ -790,8 +790,9 @@ sil_status check_problem3(sil_mag3d_nl_problem const& p, char const* who, bool n
 {
     std::string const w(who);
     if (p.nx < 3 || p.ny < 3 || p.nz < 3) return fail(SIL_ERR_INVALID, w + ": need at least 3x3x3 nodes");
-    if (3 * p.nx * p.ny * p.nz >= (int64_t(1) << 31))
-        return fail(SIL_ERR_INVALID, w + ": fewer than 2^31 unknowns per problem supported");
+    // the kernels index the 9 Jacobian coefficients of a node with int
+    if (9 * p.nx * p.ny * p.nz >= (int64_t(1) << 31))
+        return fail(SIL_ERR_INVALID, w + ": fewer than 2^31 / 9 nodes per problem supported");
     if (p.x == nullptr || p.y == nullptr || p.z == nullptr) return fail(SIL_ERR_INVALID, w + ": NULL coordinate array");
     if (p.node_mu == nullptr || p.node_ferro == nullptr) return fail(SIL_ERR_INVALID, w + ": NULL material array");
     if (need_fields && (p.rhs == nullptr || p.solution == nullptr)) return fail(SIL_ERR_INVALID, w + ": NULL field pointer");
