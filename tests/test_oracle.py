@@ -262,3 +262,55 @@ def test_mag3d_oracle_operator_properties():
     rhs[inner] = rng.standard_normal(inner.size)
     sol, it, rel = O.mag3d_cg(x, y, z, mu, 20.0, rhs, tol=1e-11)
     assert rel <= 1e-11 and np.linalg.norm(A @ sol - rhs) <= 1e-10 * np.linalg.norm(rhs)
+
+
+def _greville_cubic(lo, hi, ncells):
+    """Greville points of uniform cubic B-splines with clamped knots on
+    [lo, hi] (the reference examples' Mesher<3>, ncells + 3 points): the knot
+    averages, uniform inside and lo + h/3, hi - h/3 next to the ends."""
+    h = (hi - lo) / ncells
+    inner = lo + h * np.arange(1, ncells)
+    return np.concatenate([[lo, lo + h / 3.0], inner, [hi - h / 3.0, hi]])
+
+
+def _example_index(frac, extent):
+    return int(np.floor(frac * (extent - 1) + 0.5))      # std::llround on a positive value
+
+
+def test_examples_2d_laplacian_correctness_checks():
+    """examples/2d_laplacian.cpp:97-113, 240-251: potential -alpha r^2 inside
+    R = 2 and alpha R^2 (2 log(R/r) - 1) outside on the 1003^2 Greville grid
+    of [-5, 5]^2; the Laplacian (a positive operator) is 1 near (5/8 Lx, 0)
+    and 0 near (7/8 Lx, 0), within 5e-2."""
+    x = _greville_cubic(-5.0, 5.0, 1000)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    r = np.sqrt(X * X + Y * Y)
+    R, alpha = 2.0, 0.25
+    rs = np.where(r <= R, 1.0, r)          # the outside branch is only taken away from the origin
+    phi = np.where(r <= R, -alpha * r * r, alpha * R * R * (2.0 * np.log(R / rs) - 1.0))
+    lap = O.laplacian(2, 0, O.position_from_coords([x, x]), phi[..., None])
+    ext = lap.shape[0]
+    iy = _example_index(0.5, ext)
+    assert abs(lap[_example_index(5 / 8, ext), iy, 0] - 1.0) <= 5e-2
+    assert abs(lap[_example_index(7 / 8, ext), iy, 0] - 0.0) <= 5e-2
+
+
+def test_examples_2d_vector_laplacian_correctness_checks():
+    """examples/2d_vector_laplacian.cpp:189-215, 241-267: the rotational
+    1-form field of the example; the Laplacian's magnitude is 1 near
+    (5/8 Lx, 0) and 0 near (7/8 Lx, 0), within 5e-2."""
+    x = _greville_cubic(-5.0, 5.0, 1000)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    r = np.sqrt(X * X + Y * Y)
+    R = 2.0
+    inside = r <= R
+    rs = np.where(inside, 1.0, r)          # the outside branch is only taken away from the origin
+    w = np.zeros(X.shape + (2,))
+    w[..., 0] = np.where(inside, Y * (r / 3.0 - R / 2.0), -Y * R ** 3 / (6.0 * rs * rs))
+    w[..., 1] = np.where(inside, -X * (r / 3.0 - R / 2.0), X * R ** 3 / (6.0 * rs * rs))
+    lap = O.laplacian(2, 1, O.position_from_coords([x, x]), w)
+    ext = lap.shape[0]
+    iy = _example_index(0.5, ext)
+    for frac, expected in ((5 / 8, 1.0), (7 / 8, 0.0)):
+        v = lap[_example_index(frac, ext), iy]
+        assert abs(np.hypot(v[0], v[1]) - expected) <= 5e-2
