@@ -75,6 +75,8 @@ def lib():
         _lib.silo_csr_precond_apply.argtypes = [i64, ip, i32p, dp, ci, dp, dp, dp]
         _lib.silo_csr_isai_values.argtypes = [i64, ip, i32p, dp, ci, dp]
         _lib.silo_csr_pcg.argtypes = [i64, ip, i32p, dp, ci, dp, dp, dp, d, ci, dp]
+        _lib.silo_reduce_primal.argtypes = [ci, ci, ctypes.POINTER(_Field), ip, dp, dp]
+        _lib.silo_reconstruct_primal.argtypes = [ci, ci, ctypes.POINTER(_Field), ip, dp, dp]
         _lib.silo_csr_krylov.argtypes = [i64, ip, i32p, dp, ci, ci, ci, dp, dp, dp, d, ci, dp]
         _lib.silo_mag2d_nl_solve_menu.argtypes = [i64, i64, dp, dp, ci, dp, dp, ci, dp, dp, dp, d, ci,
                                                   ctypes.POINTER(ci), dp]
@@ -593,3 +595,27 @@ def csr_krylov(A, b, solver="cg", kind="jacobi", tol=1e-10, max_iter=100000, dim
     if it < 0:
         raise ValueError("unknown solver or singular ISAI system")
     return x, it, rel.value
+
+
+# ----------------------------------------------------------------- primal reduction / reconstruction
+
+def reduce_primal(n, k, position, node, form):
+    """Reduction<Primal>::run at one node of a position field ([...][n])."""
+    fp = field(np.ascontiguousarray(position, dtype=np.float64))
+    nd = np.ascontiguousarray(node, dtype=np.int64)
+    f = _f64(form)
+    out = np.zeros(binom(n, k))
+    _check(lib().silo_reduce_primal(n, k, ctypes.byref(fp), nd.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                    _ptr(f), _ptr(out)), "reduce_primal")
+    return out
+
+
+def reconstruct_primal(n, k, position, node, cochain):
+    """Reconstruction<Primal>::run at one node."""
+    fp = field(np.ascontiguousarray(position, dtype=np.float64))
+    nd = np.ascontiguousarray(node, dtype=np.int64)
+    c = _f64(cochain)
+    out = np.zeros(binom(n, k))
+    _check(lib().silo_reconstruct_primal(n, k, ctypes.byref(fp), nd.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                         _ptr(c), _ptr(out)), "reconstruct_primal")
+    return out

@@ -1008,6 +1008,66 @@ int silo_transposed_coboundary(uint32_t form_mask, int k, const silo_field* in, 
     return coboundary_impl(form_mask, k, in, out, true);
 }
 
+// Reduction<Primal>::run at one node: reduced[t] = sum over the ordered
+// source tuples of value(source, t) * form.get(source), value = det(J) / K!
+// with J[row][col] = edge_{t[col]}[source[row]] (0 for repeated ids), and
+// form.get the antisymmetric tensor's signed component.
+// Ref: src/similie/exterior/reduction_and_reconstruction.hpp:472-534, 649-677;
+//      volume.hpp:46-53 (complex volume factor 1 on the primal complex)
+int silo_reduce_primal(int n, int K, const silo_field* position, const int64_t* node, const double* form, double* out)
+{
+    if (n < 1 || n > MAXN || K < 0 || K > n) return 1;
+    Geometry const G {n, position, nullptr};
+    if (K == 0) {
+        out[0] = form[0];
+        return 0;
+    }
+    int64_t const nb = binom(n, K);
+    int64_t const ntuples = ipow(n, K);
+    for (int64_t t = 0; t < nb; ++t) {
+        auto const tids = combination_from_rank(n, K, t);
+        double reduced = 0.;
+        for (int64_t tu = 0; tu < ntuples; ++tu) {
+            std::vector<int> tuple(K);
+            int64_t rr = tu;
+            for (int a = K - 1; a >= 0; --a) {
+                tuple[a] = static_cast<int>(rr % n);
+                rr /= n;
+            }
+            double value = 0.;
+            double fv = 0.;
+            if (unique_ids(n, tuple)) {
+                std::vector<double> j(K * K);
+                for (int row = 0; row < K; ++row)
+                    for (int col = 0; col < K; ++col) {
+                        double e[MAXN];
+                        G.edge_vector(node, tids[col], e);
+                        j[row * K + col] = e[tuple[row]];
+                    }
+                value = reduction_determinant(j, K) / factorial(K);
+                std::vector<int> sorted(tuple);
+                std::sort(sorted.begin(), sorted.end());
+                std::vector<int> none;
+                fv = permutation_sign(tuple, none) * form[combination_rank(n, sorted)];
+            }
+            reduced += value * fv;
+        }
+        out[t] = reduced;
+    }
+    return 0;
+}
+
+// Reconstruction<Primal>::run at one node.
+// Ref: src/similie/exterior/reduction_and_reconstruction.hpp:814-892
+int silo_reconstruct_primal(int n, int K, const silo_field* position, const int64_t* node, const double* cochain,
+                            double* out)
+{
+    if (n < 1 || n > MAXN || K < 0 || K > n) return 1;
+    Geometry const G {n, position, nullptr};
+    G.reconstruct(node, K, cochain, out);
+    return 0;
+}
+
 int silo_fill_hodge_star(int n, int k_in, const silo_field* position, const silo_field* metric,
                          silo_field* hodge)
 {

@@ -197,6 +197,13 @@ int silo_csr_krylov(int64_t n, const int64_t* ptr, const int32_t* col, const dou
                     int kind, const double* params, const double* b, double* x, double tol, int max_iter,
                     double* final_rel);
 
+/* Primal reduction and reconstruction of one node's form / cochain
+ * (Reduction<Primal>::run, Reconstruction<Primal>::run); binom(n, K) values
+ * in and out.  Return 0, or 1 for a bad rank. */
+int silo_reduce_primal(int n, int K, const silo_field* position, const int64_t* node, const double* form, double* out);
+int silo_reconstruct_primal(int n, int K, const silo_field* position, const int64_t* node, const double* cochain,
+                            double* out);
+
 /* Threads OpenMP uses (for reporting). */
 int silo_num_threads(void);
 

@@ -314,3 +314,29 @@ def test_examples_2d_vector_laplacian_correctness_checks():
     for frac, expected in ((5 / 8, 1.0), (7 / 8, 0.0)):
         v = lap[_example_index(frac, ext), iy]
         assert abs(np.hypot(v[0], v[1]) - expected) <= 5e-2
+
+
+def _kat_position(fn):
+    """Positions of the reference's 2 x 2 test lattice: UniformPointSampling
+    on [0, 2] with 2 points, so xi, eta in {0, 2}."""
+    c = np.array([0.0, 2.0])
+    xi, eta = np.meshgrid(c, c, indexing="ij")
+    px, py = fn(xi, eta)
+    return np.ascontiguousarray(np.stack([px, py], axis=-1))
+
+
+@pytest.mark.parametrize("k,form,reduced", [(0, [3.5], [3.5]), (1, [3.0, -1.0], [6.0, 2.0]), (2, [4.0], [32.0])])
+def test_reduction_kat(k, form, reduced):
+    """tests/exterior/reduction_and_reconstruction.cpp:231-283: primal
+    reduction of constant forms on the sheared lattice (xi + eta, 2 eta)."""
+    pos = _kat_position(lambda xi, eta: (xi + eta, 2.0 * eta))
+    assert list(O.reduce_primal(2, k, pos, [0, 0], form)) == reduced
+
+
+@pytest.mark.parametrize("k,form", [(0, [3.5]), (1, [3.0, -1.0]), (2, [4.0])])
+def test_reconstruction_kat(k, form):
+    """tests/exterior/reduction_and_reconstruction.cpp:285-329: reduce, then
+    reconstruct, on the lattice (2 xi, 3 eta): the form comes back."""
+    pos = _kat_position(lambda xi, eta: (2.0 * xi, 3.0 * eta))
+    red = O.reduce_primal(2, k, pos, [0, 0], form)
+    assert list(O.reconstruct_primal(2, k, pos, [0, 0], red)) == form
