@@ -63,6 +63,16 @@ class LearnedPreconditioner:
     def load(self, path):
         self.set_params(np.load(path))
 
+    def save_checkpoint(self, path, step, seed, extra=None):
+        """A training checkpoint: header (format, dtype, count, step, seed) + parameters."""
+        write_checkpoint(path, self.get_params(), step, seed, extra)
+
+    def load_checkpoint(self, path):
+        """Restores the parameters of a checkpoint; returns its (step, seed, extra)."""
+        params, step, seed, extra = read_checkpoint(path)
+        self.set_params(params)
+        return step, seed, extra
+
     def apply(self, shapes, nu, r, out, stream=None, active=None):
         """out = M(r); nu, r, out: flat torch CUDA float32 tensors laid out as pack_samples(shapes).
         active: optional torch CUDA int32 tensor, one entry per sample; samples
@@ -98,3 +108,45 @@ class LearnedPreconditioner:
         out = np.zeros(count, dtype=np.float32)
         check(lib().sil_precond_debug_fetch(self._h, which, level, out.ctypes.data, count), "precond_debug_fetch")
         return out
+
+
+# ----------------------------------------------------------------- checkpoints
+#
+# Flat binary: 8-byte magic, then little-endian uint32 version, uint32 dtype
+# code (1 = float32), uint64 parameter count, uint64 step, uint64 seed,
+# uint64 length of a UTF-8 JSON block of extra fields, the JSON, then the
+# parameters.  The Adam moments stay inside the library's handle, so a
+# resumed run restarts them (the learning-rate schedule resumes at `step`).
+
+_MAGIC = b"SILPCKPT"
+
+
+def write_checkpoint(path, params, step, seed, extra=None):
+    import json
+    import struct
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    blob = json.dumps(extra or {}, sort_keys=True).encode()
+    with open(path, "wb") as f:
+        f.write(_MAGIC)
+        f.write(struct.pack("<IIQQQQ", 1, 1, p.size, int(step), int(seed), len(blob)))
+        f.write(blob)
+        f.write(p.tobytes())
+
+
+def read_checkpoint(path):
+    """(params, step, seed, extra) of a checkpoint; ValueError on a malformed file."""
+    import json
+    import struct
+    with open(path, "rb") as f:
+        data = f.read()
+    head = 8 + struct.calcsize("<IIQQQQ")
+    if len(data) < head or data[:8] != _MAGIC:
+        raise ValueError("not a preconditioner checkpoint")
+    version, dtype, count, step, seed, nblob = struct.unpack("<IIQQQQ", data[8:head])
+    if version != 1 or dtype != 1:
+        raise ValueError(f"unsupported checkpoint version {version} / dtype {dtype}")
+    if len(data) != head + nblob + 4 * count:
+        raise ValueError("truncated or padded checkpoint")
+    extra = json.loads(data[head:head + nblob].decode())
+    params = np.frombuffer(data, dtype="<f4", count=count, offset=head + nblob).copy()
+    return params, step, seed, extra

@@ -55,9 +55,12 @@ def generate_pairs(seed, count, sizes=(256, 384, 512, 768, 1024), snapshot_tols=
     return pairs
 
 
-def train(net, pairs, steps, batch=8, lr=1e-3, seed=0, log_every=100, log=None):
+def train(net, pairs, steps, batch=8, lr=1e-3, seed=0, log_every=100, log=None, start=0, checkpoint=None,
+          checkpoint_every=500):
     """Adam with a cosine learning-rate schedule; each step draws `batch` pairs
-    of one grid size (sizes drawn in proportion to their pair counts)."""
+    of one grid size (sizes drawn in proportion to their pair counts).
+    start: the step to resume from (the schedule and the draws continue
+    there); checkpoint: a path written every `checkpoint_every` steps."""
     import torch
     rng = np.random.default_rng(seed)
     sizes = sorted(pairs)
@@ -65,7 +68,10 @@ def train(net, pairs, steps, batch=8, lr=1e-3, seed=0, log_every=100, log=None):
     weights /= weights.sum()
     history = []
     t0 = time.perf_counter()
-    for step in range(steps):
+    for _ in range(start):                      # replay the draws of the steps already taken
+        n = sizes[int(rng.choice(len(sizes), p=weights))]
+        rng.integers(0, len(pairs[n]), batch)
+    for step in range(start, steps):
         n = sizes[int(rng.choice(len(sizes), p=weights))]
         idx = rng.integers(0, len(pairs[n]), batch)
         nu = torch.cat([pairs[n][i][0] for i in idx])
@@ -77,6 +83,8 @@ def train(net, pairs, steps, batch=8, lr=1e-3, seed=0, log_every=100, log=None):
         if log is not None and (step % log_every == 0 or step == steps - 1):
             log(json.dumps({"step": step, "size": n, "loss": round(float(np.mean(history[-log_every:])), 5),
                             "seconds": round(time.perf_counter() - t0, 2)}))
+        if checkpoint is not None and ((step + 1) % checkpoint_every == 0 or step == steps - 1):
+            net.save_checkpoint(checkpoint, step + 1, seed, {"steps": steps, "batch": batch, "lr": lr})
     torch.cuda.synchronize()
     return history, time.perf_counter() - t0
 
@@ -93,6 +101,8 @@ def main():
     ap.add_argument("--min-cores", type=int, default=0,
                     help="draw min..3 permeability-1000 rectangles per problem instead of 0..3")
     ap.add_argument("--out", default="precond_2d.npy")
+    ap.add_argument("--checkpoint", default=None, help="write a resumable checkpoint here while training")
+    ap.add_argument("--resume", default=None, help="continue from this checkpoint (parameters, step)")
     args = ap.parse_args()
     import torch
     torch.cuda.init()
@@ -105,7 +115,11 @@ def main():
     net = LearnedPreconditioner(seed=args.seed)
     if args.init:
         net.load(args.init)
-    hist, t_train = train(net, pairs, args.steps, args.batch, args.lr, args.seed, log=lambda s: print(s, flush=True))
+    start = 0
+    if args.resume:
+        start, _, _ = net.load_checkpoint(args.resume)
+    hist, t_train = train(net, pairs, args.steps, args.batch, args.lr, args.seed, log=lambda s: print(s, flush=True),
+                          start=start, checkpoint=args.checkpoint)
     net.save(args.out)
     print(json.dumps({"train_seconds": round(t_train, 2), "final_loss": float(np.mean(hist[-100:]))}), flush=True)
 

@@ -1,7 +1,9 @@
 """CPU checks of the preconditioner oracle: its operator equals the C oracle's,
 its BF16 rounding equals torch's, and its parameter gradient equals central
-finite differences of its own float64 loss."""
+finite differences of its own float64 loss; the training checkpoint format
+round-trips and rejects malformed files."""
 import numpy as np
+import pytest
 
 import oracle as O
 from oracle import precond_oracle as P
@@ -59,3 +61,19 @@ def test_depth_and_pooling_shapes():
     c = P.pool(P.pad(x))
     assert c.shape == (3, 4, 1)
     assert c[0, 0, 0] == (0 + 1 + 7 + 8) / 4 and c[2, 3, 0] == x[4, 6, 0] / 4
+
+
+def test_checkpoint_round_trip_and_rejections(tmp_path):
+    from similie_b200.precond import read_checkpoint, write_checkpoint
+    rng = np.random.default_rng(3)
+    params = rng.standard_normal(1234).astype(np.float32)
+    path = str(tmp_path / "ck.bin")
+    write_checkpoint(path, params, step=700, seed=9, extra={"lr": 1e-3, "steps": 2000})
+    p2, step, seed, extra = read_checkpoint(path)
+    np.testing.assert_array_equal(p2, params)
+    assert (step, seed, extra) == (700, 9, {"lr": 1e-3, "steps": 2000})
+    data = open(path, "rb").read()
+    for bad in (b"XXXXXXXX" + data[8:], data[:-4], data + b"\0"):
+        open(path, "wb").write(bad)
+        with pytest.raises(ValueError):
+            read_checkpoint(path)
