@@ -534,6 +534,32 @@ void sil_csr_precond_destroy(sil_csr_precond p);
 sil_status sil_csr_solve(sil_stream stream, sil_csr m, sil_csr_precond p, const double* rhs, double* x,
                          const sil_solve_settings* settings, sil_solve_diagnostics* diag);
 
+/* The reference's SIMILIE_SOLVER menu on an assembled matrix, in its order:
+ * 0 cg, 1 minres, 2 fcg, 3 gmres, 4 bicgstab, 5 gcr, 6 idr. */
+typedef enum sil_krylov_kind {
+    SIL_KRYLOV_CG = 0,
+    SIL_KRYLOV_MINRES = 1,
+    SIL_KRYLOV_FCG = 2,
+    SIL_KRYLOV_GMRES = 3,
+    SIL_KRYLOV_BICGSTAB = 4,
+    SIL_KRYLOV_GCR = 5,
+    SIL_KRYLOV_IDR = 6
+} sil_krylov_kind;
+
+/* x = A^-1 rhs by the chosen Krylov method with the preconditioner p, from
+ * x = 0 until ||r|| <= tol ||b|| or settings->max_iterations: MINRES (Paige
+ * & Saunders, stopping on its iterate's true residual), flexible CG, GMRES
+ * and GCR restarted after `dim` directions (0: 100), BiCGSTAB, IDR(s) with
+ * s = `dim` (0: 8) and a fixed-seed shadow space; all but MINRES and FCG
+ * preconditioned on the right.  CG is sil_csr_solve.  Scalars are reduced on
+ * the host in a fixed order.  Synchronous.
+ * Replaces: the SIMILIE_SOLVER choices of solve_linearized_system,
+ *   minimize_strong_formulation_residual.hpp:1069-1130 (Ginkgo's Minres, Fcg,
+ *   Gmres, Bicgstab, Gcr, Idr; Krylov dimensions 1079-1120). */
+sil_status sil_csr_krylov_solve(sil_stream stream, sil_csr m, sil_csr_precond p, int32_t solver, int32_t dim,
+                                const double* rhs, double* x, const sil_solve_settings* settings,
+                                sil_solve_diagnostics* diag);
+
 #ifdef __cplusplus
 }
 #endif

@@ -218,6 +218,8 @@ SIGNATURES = [
     ("sil_csr_precond_destroy", None, [_P]),
     ("sil_csr_solve", ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.POINTER(SilSolveSettings),
                                      ctypes.POINTER(SilSolveDiagnostics)]),
+    ("sil_csr_krylov_solve", ctypes.c_int, [_P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P,
+                                            ctypes.POINTER(SilSolveSettings), ctypes.POINTER(SilSolveDiagnostics)]),
     ("sil_mag3d_nl_apply", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dNlProblem), _P, _P]),
     ("sil_mag3d_nl_apply_jacobian", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dNlProblem), _P, _P, _P]),
     ("sil_mag3d_nl_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag3dNlProblem), ctypes.c_int,
