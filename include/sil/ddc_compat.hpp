@@ -522,6 +522,7 @@ struct NonlinearMagnetostaticsOperator3D
     double const* node_ferro;
     std::vector<double> curve_b, curve_h;  // B-H samples (host)
     double gauge_penalty = 20.0;
+    bool divergence_gauge = false;  // SIMILIE_DIVERGENCE_GAUGE_3D
     int64_t size() const { return 3 * static_cast<int64_t>(x.size() * y.size() * z.size()); }
     sil_mag3d_nl_problem problem(double const* rhs = nullptr, double* solution = nullptr) const
     {
@@ -539,7 +540,10 @@ struct NonlinearMagnetostaticsOperator3D
         p.curve.h = curve_h.data();
         p.rhs = rhs;
         p.solution = solution;
-        p.gauge_penalty = gauge_penalty;
+        bool const divergence = divergence_gauge || env::flag("SIMILIE_DIVERGENCE_GAUGE_3D");
+        p.gauge = divergence ? 1 : 0;
+        p.gauge_penalty = divergence ? gauge_penalty * env::sign_or_one("SIMILIE_VECTOR_POTENTIAL_GAUGE_SIGN_3D")
+                                     : gauge_penalty;
         return p;
     }
     void apply(ExecSpace exec, double const* in, double* out) const

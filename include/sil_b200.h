@@ -340,7 +340,8 @@ typedef struct sil_mag3d_nl_problem {
     sil_bh_curve curve;
     const double* rhs;        /* device, 3*nx*ny*nz */
     double* solution;         /* device, 3*nx*ny*nz: initial guess on entry, result on exit */
-    double gauge_penalty;     /* gamma > 0 */
+    double gauge_penalty;     /* gamma: > 0 for the penalty gauge, nonzero for the divergence gauge */
+    int32_t gauge;            /* 0: penalty (the default); 1: divergence gauge, as in sil_mag3d_problem */
 } sil_mag3d_nl_problem;
 
 /* y = the 3D nonlinear operator applied to a (3*nx*ny*nz doubles, device). */

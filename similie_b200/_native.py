@@ -93,6 +93,7 @@ class SilMag3dNlProblem(ctypes.Structure):
         ("rhs", ctypes.c_void_p),
         ("solution", ctypes.c_void_p),
         ("gauge_penalty", ctypes.c_double),
+        ("gauge", ctypes.c_int32),
     ]
 
 

@@ -1639,6 +1639,30 @@ __global__ void mag3d_apply_kernel(ProbInfo pi, double const* nu, double const* 
 }
 
 } // namespace
+
+sil_status divergence_gauge_table(int64_t nx, int64_t ny, int64_t nz, double const* const coords[3], double const* ls,
+                                  double* gd, double* probe, double* out, cudaStream_t st)
+{
+    ProblemDesc q {};
+    q.dim = 3;
+    q.nx = nx;
+    q.ny = ny;
+    q.nz = nz;
+    for (int a = 0; a < 3; ++a) q.coords[a] = coords[a];
+    q.gauge = 1;
+    ProbInfo pi {};
+    pi.dim = 3;
+    pi.nx = nx;
+    pi.ny = ny;
+    pi.nz = nz;
+    pi.nodes = nx * ny * nz;
+    pi.n = 3 * pi.nodes;
+    pi.ls64[0] = ls;
+    pi.ls64[1] = ls + nx;
+    pi.ls64[2] = ls + nx + ny;
+    return build_divergence_gauge(q, pi, gd, nullptr, probe, out, st);
+}
+
 } // namespace sil
 
 extern "C" {
