@@ -1429,20 +1429,54 @@ sil_status sil_csr_solve(sil_stream stream, sil_csr m, sil_csr_precond pc, const
     cg_rz_kernel<<<1, kBlock, 0, s>>>(part, np, st);
     cg_direction_kernel<<<G, kBlock, 0, s>>>(n, part, np, z, p, st, 1);
     SIL_CUDA_CHECK(cudaGetLastError());
-    // iterations issued in chunks, the state read back after each chunk
+    // A chunk of iterations captured once as a CUDA graph (every kernel does
+    // nothing once the state is done) and replayed until convergence, the
+    // state read back after each replay.  The level-scheduled
+    // preconditioners launch two kernels per level, so their chunks are
+    // shorter (at most about 4,096 launches per graph).
+    int const per_apply = static_cast<int>(pc->fwd_lev.size() + pc->bwd_lev.size()) + 8;
+    int const chunk = std::max(1, std::min(16, 4096 / per_apply));
+    auto issue = [&](cudaStream_t cs) {
+        for (int c = 0; c < chunk; ++c) {
+            cg_spmv_kernel<<<G, kBlock, 0, cs>>>(n, m->ptr, m->col, m->val, p, q, part, st);
+            cg_alpha_kernel<<<1, kBlock, 0, cs>>>(part, np, st);
+            cg_update_kernel<<<G, kBlock, 0, cs>>>(n, x, r, p, q, part, st);
+            cg_check_kernel<<<1, kBlock, 0, cs>>>(part, np, st, tol, max_iter);
+            precond_launch(*pc, cs, r, z, st);
+            dot_kernel<<<G, kBlock, 0, cs>>>(n, r, z, part, st);
+            cg_direction_kernel<<<G, kBlock, 0, cs>>>(n, part, np, z, p, st, 0);
+            cg_rz_kernel<<<1, kBlock, 0, cs>>>(part, np, st);
+        }
+    };
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    {
+        cudaStream_t cs;
+        SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) issue(cs);
+        cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
+        if (err == cudaSuccess) err = err2;
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+        cudaStreamDestroy(cs);
+        if (err != cudaSuccess) {
+            if (graph != nullptr) cudaGraphDestroy(graph);
+            return cuda_fail(err, "sil_csr_solve: CG graph capture");
+        }
+    }
+    struct GraphGuard
+    {
+        cudaGraph_t g;
+        cudaGraphExec_t e;
+        ~GraphGuard()
+        {
+            cudaGraphExecDestroy(e);
+            cudaGraphDestroy(g);
+        }
+    } guard {graph, exec};
     CgState hs {};
     for (;;) {
-        for (int c = 0; c < 16; ++c) {
-            cg_spmv_kernel<<<G, kBlock, 0, s>>>(n, m->ptr, m->col, m->val, p, q, part, st);
-            cg_alpha_kernel<<<1, kBlock, 0, s>>>(part, np, st);
-            cg_update_kernel<<<G, kBlock, 0, s>>>(n, x, r, p, q, part, st);
-            cg_check_kernel<<<1, kBlock, 0, s>>>(part, np, st, tol, max_iter);
-            precond_launch(*pc, s, r, z, st);
-            dot_kernel<<<G, kBlock, 0, s>>>(n, r, z, part, st);
-            cg_direction_kernel<<<G, kBlock, 0, s>>>(n, part, np, z, p, st, 0);
-            cg_rz_kernel<<<1, kBlock, 0, s>>>(part, np, st);
-        }
-        SIL_CUDA_CHECK(cudaGetLastError());
+        SIL_CUDA_CHECK(cudaGraphLaunch(exec, s));
         SIL_CUDA_CHECK(cudaMemcpyAsync(&hs, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
         SIL_CUDA_CHECK(cudaStreamSynchronize(s));
         if (hs.done) break;
