@@ -387,6 +387,13 @@ void sil_precond_destroy(sil_precond p);
  * (save / load); set_params resets the optimiser state. */
 sil_status sil_precond_get_params(sil_precond p, float* host);
 sil_status sil_precond_set_params(sil_precond p, const float* host, sil_stream stream);
+/* The Adam state of training: first and second moments (host FP32
+ * [sil_precond_num_params()] each, either may be NULL) and the steps taken.
+ * set_params resets it; set_optimizer_state after it restores a checkpoint
+ * exactly.  Synchronous.  No counterpart in the reference. */
+sil_status sil_precond_get_optimizer_state(sil_precond p, float* m, float* v, int64_t* step);
+sil_status sil_precond_set_optimizer_state(sil_precond p, const float* m, const float* v, int64_t step,
+                                           sil_stream stream);
 /* out = M(r) for 1..64 samples (device arrays). */
 sil_status sil_precond_apply(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
                              const float* nu, const float* r, float* out);

@@ -193,6 +193,8 @@ SIGNATURES = [
     ("sil_precond_destroy", None, [_P]),
     ("sil_precond_get_params", ctypes.c_int, [_P, _P]),
     ("sil_precond_set_params", ctypes.c_int, [_P, _P, _P]),
+    ("sil_precond_get_optimizer_state", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_int64)]),
+    ("sil_precond_set_optimizer_state", ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
     ("sil_precond_apply", ctypes.c_int, [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P]),
     ("sil_precond_apply_active", ctypes.c_int,
      [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P, _P]),
