@@ -31,6 +31,7 @@
 // synchronous, and errors are thrown (Error, carrying the sil_status).
 #pragma once
 
+#include <algorithm>
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -340,11 +341,40 @@ inline PreconditionerType selected_preconditioner(StrongFormulationSolverSetting
     return settings.preconditioner;
 }
 
+// SIMILIE_SOLVER: minres, fcg, gmres, bicgstab, gcr or idr; anything else is
+// CG (solve_linearized_system, 1069-1130), with the Krylov dimensions of
+// SIMILIE_GMRES_KRYLOV_DIM (100), SIMILIE_GCR_KRYLOV_DIM (100) and
+// SIMILIE_IDR_SUBSPACE_DIM (8).
+struct KrylovChoice
+{
+    sil_krylov_kind kind = SIL_KRYLOV_CG;
+    int dim = 0;
+};
+
+inline KrylovChoice selected_solver()
+{
+    KrylovChoice c;
+    char const* const v = std::getenv("SIMILIE_SOLVER");
+    std::string const name = v == nullptr ? "" : v;
+    if (name == "minres") c.kind = SIL_KRYLOV_MINRES;
+    else if (name == "fcg") c.kind = SIL_KRYLOV_FCG;
+    else if (name == "gmres") {
+        c.kind = SIL_KRYLOV_GMRES;
+        c.dim = static_cast<int>(env::number_or("SIMILIE_GMRES_KRYLOV_DIM", 100.0));
+    } else if (name == "bicgstab") c.kind = SIL_KRYLOV_BICGSTAB;
+    else if (name == "gcr") {
+        c.kind = SIL_KRYLOV_GCR;
+        c.dim = std::max(1, static_cast<int>(env::number_or("SIMILIE_GCR_KRYLOV_DIM", 100.0)));
+    } else if (name == "idr") {
+        c.kind = SIL_KRYLOV_IDR;
+        c.dim = std::max(1, static_cast<int>(env::number_or("SIMILIE_IDR_SUBSPACE_DIM", 8.0)));
+    }
+    if (c.dim < 1 && (c.kind == SIL_KRYLOV_GMRES)) c.dim = 1;
+    return c;
+}
+
 inline void check_supported_environment()
 {
-    char const* const solver = std::getenv("SIMILIE_SOLVER");
-    if (solver != nullptr && solver[0] != '\0' && std::string(solver) != "cg")
-        throw Error(SIL_ERR_UNSUPPORTED, std::string("SIMILIE_SOLVER=") + solver + ": only cg is available");
     if (env::sign_or_one("SIMILIE_MAGNETIC_Y_RESPONSE_SIGN_3D") < 0.0)
         throw Error(SIL_ERR_UNSUPPORTED, "SIMILIE_MAGNETIC_Y_RESPONSE_SIGN_3D < 0 is not available");
     if (env::number_or("SIMILIE_NONLINEAR_LINE_SEARCH_STEPS", 8.0) != 8.0
@@ -492,6 +522,7 @@ struct NonlinearMagnetostaticsOperator3D
     double const* node_ferro;
     std::vector<double> curve_b, curve_h;  // B-H samples (host)
     double gauge_penalty = 20.0;
+    bool divergence_gauge = false;  // SIMILIE_DIVERGENCE_GAUGE_3D
     int64_t size() const { return 3 * static_cast<int64_t>(x.size() * y.size() * z.size()); }
     sil_mag3d_nl_problem problem(double const* rhs = nullptr, double* solution = nullptr) const
     {
@@ -509,7 +540,10 @@ struct NonlinearMagnetostaticsOperator3D
         p.curve.h = curve_h.data();
         p.rhs = rhs;
         p.solution = solution;
-        p.gauge_penalty = gauge_penalty;
+        bool const divergence = divergence_gauge || env::flag("SIMILIE_DIVERGENCE_GAUGE_3D");
+        p.gauge = divergence ? 1 : 0;
+        p.gauge_penalty = divergence ? gauge_penalty * env::sign_or_one("SIMILIE_VECTOR_POTENTIAL_GAUGE_SIGN_3D")
+                                     : gauge_penalty;
         return p;
     }
     void apply(ExecSpace exec, double const* in, double* out) const
@@ -601,7 +635,8 @@ inline StrongFormulationSolverDiagnostics to_diagnostics(sil_solve_diagnostics c
 
 inline bool assembled(StrongFormulationSolverSettings const& s)
 {
-    return !s.use_matrix_free || s.preconditioner != PreconditionerType::Jacobi;
+    return !s.use_matrix_free || s.preconditioner != PreconditionerType::Jacobi
+           || selected_solver().kind != SIL_KRYLOV_CG;
 }
 
 inline sil_menu_settings to_menu(StrongFormulationSolverSettings const& settings)
@@ -630,7 +665,8 @@ inline StrongFormulationSolverDiagnostics solve_assembled(ExecSpace exec, CsrMat
     timer.done("preconditioner build");
     sil_solve_settings const s = to_settings(settings);
     sil_solve_diagnostics d {};
-    sil_status const st = sil_csr_solve(exec.stream, m.get(), pc, rhs, solution, &s, &d);
+    KrylovChoice const k = selected_solver();
+    sil_status const st = sil_csr_krylov_solve(exec.stream, m.get(), pc, k.kind, k.dim, rhs, solution, &s, &d);
     sil_csr_precond_destroy(pc);
     check(st, "minimize_strong_formulation_residual");
     timer.done("solve");

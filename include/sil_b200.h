@@ -340,7 +340,8 @@ typedef struct sil_mag3d_nl_problem {
     sil_bh_curve curve;
     const double* rhs;        /* device, 3*nx*ny*nz */
     double* solution;         /* device, 3*nx*ny*nz: initial guess on entry, result on exit */
-    double gauge_penalty;     /* gamma > 0 */
+    double gauge_penalty;     /* gamma: > 0 for the penalty gauge, nonzero for the divergence gauge */
+    int32_t gauge;            /* 0: penalty (the default); 1: divergence gauge, as in sil_mag3d_problem */
 } sil_mag3d_nl_problem;
 
 /* y = the 3D nonlinear operator applied to a (3*nx*ny*nz doubles, device). */
@@ -386,6 +387,13 @@ void sil_precond_destroy(sil_precond p);
  * (save / load); set_params resets the optimiser state. */
 sil_status sil_precond_get_params(sil_precond p, float* host);
 sil_status sil_precond_set_params(sil_precond p, const float* host, sil_stream stream);
+/* The Adam state of training: first and second moments (host FP32
+ * [sil_precond_num_params()] each, either may be NULL) and the steps taken.
+ * set_params resets it; set_optimizer_state after it restores a checkpoint
+ * exactly.  Synchronous.  No counterpart in the reference. */
+sil_status sil_precond_get_optimizer_state(sil_precond p, float* m, float* v, int64_t* step);
+sil_status sil_precond_set_optimizer_state(sil_precond p, const float* m, const float* v, int64_t step,
+                                           sil_stream stream);
 /* out = M(r) for 1..64 samples (device arrays). */
 sil_status sil_precond_apply(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
                              const float* nu, const float* r, float* out);
@@ -533,6 +541,32 @@ void sil_csr_precond_destroy(sil_csr_precond p);
  *   1028-1304. */
 sil_status sil_csr_solve(sil_stream stream, sil_csr m, sil_csr_precond p, const double* rhs, double* x,
                          const sil_solve_settings* settings, sil_solve_diagnostics* diag);
+
+/* The reference's SIMILIE_SOLVER menu on an assembled matrix, in its order:
+ * 0 cg, 1 minres, 2 fcg, 3 gmres, 4 bicgstab, 5 gcr, 6 idr. */
+typedef enum sil_krylov_kind {
+    SIL_KRYLOV_CG = 0,
+    SIL_KRYLOV_MINRES = 1,
+    SIL_KRYLOV_FCG = 2,
+    SIL_KRYLOV_GMRES = 3,
+    SIL_KRYLOV_BICGSTAB = 4,
+    SIL_KRYLOV_GCR = 5,
+    SIL_KRYLOV_IDR = 6
+} sil_krylov_kind;
+
+/* x = A^-1 rhs by the chosen Krylov method with the preconditioner p, from
+ * x = 0 until ||r|| <= tol ||b|| or settings->max_iterations: MINRES (Paige
+ * & Saunders, stopping on its iterate's true residual), flexible CG, GMRES
+ * and GCR restarted after `dim` directions (0: 100), BiCGSTAB, IDR(s) with
+ * s = `dim` (0: 8) and a fixed-seed shadow space; all but MINRES and FCG
+ * preconditioned on the right.  CG is sil_csr_solve.  Scalars are reduced on
+ * the host in a fixed order.  Synchronous.
+ * Replaces: the SIMILIE_SOLVER choices of solve_linearized_system,
+ *   minimize_strong_formulation_residual.hpp:1069-1130 (Ginkgo's Minres, Fcg,
+ *   Gmres, Bicgstab, Gcr, Idr; Krylov dimensions 1079-1120). */
+sil_status sil_csr_krylov_solve(sil_stream stream, sil_csr m, sil_csr_precond p, int32_t solver, int32_t dim,
+                                const double* rhs, double* x, const sil_solve_settings* settings,
+                                sil_solve_diagnostics* diag);
 
 #ifdef __cplusplus
 }

@@ -93,6 +93,7 @@ class SilMag3dNlProblem(ctypes.Structure):
         ("rhs", ctypes.c_void_p),
         ("solution", ctypes.c_void_p),
         ("gauge_penalty", ctypes.c_double),
+        ("gauge", ctypes.c_int32),
     ]
 
 
@@ -192,6 +193,8 @@ SIGNATURES = [
     ("sil_precond_destroy", None, [_P]),
     ("sil_precond_get_params", ctypes.c_int, [_P, _P]),
     ("sil_precond_set_params", ctypes.c_int, [_P, _P, _P]),
+    ("sil_precond_get_optimizer_state", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_int64)]),
+    ("sil_precond_set_optimizer_state", ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
     ("sil_precond_apply", ctypes.c_int, [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P]),
     ("sil_precond_apply_active", ctypes.c_int,
      [_P, _P, ctypes.POINTER(SilPrecondSample), ctypes.c_int, _P, _P, _P, _P]),
@@ -218,6 +221,8 @@ SIGNATURES = [
     ("sil_csr_precond_destroy", None, [_P]),
     ("sil_csr_solve", ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.POINTER(SilSolveSettings),
                                      ctypes.POINTER(SilSolveDiagnostics)]),
+    ("sil_csr_krylov_solve", ctypes.c_int, [_P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P,
+                                            ctypes.POINTER(SilSolveSettings), ctypes.POINTER(SilSolveDiagnostics)]),
     ("sil_mag3d_nl_apply", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dNlProblem), _P, _P]),
     ("sil_mag3d_nl_apply_jacobian", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dNlProblem), _P, _P, _P]),
     ("sil_mag3d_nl_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag3dNlProblem), ctypes.c_int,

@@ -175,13 +175,23 @@ class Preconditioner:
             pass
 
 
-def solve(matrix, preconditioner, rhs_dev, x_dev, tol=1e-10, max_iterations=100000, stream=None):
-    """Preconditioned CG from x = 0 (the reference's assembled-matrix solve); returns Diagnostics."""
+# the reference's SIMILIE_SOLVER values (minimize_strong_formulation_residual.hpp:1069-1130)
+SOLVERS = {"cg": 0, "minres": 1, "fcg": 2, "gmres": 3, "bicgstab": 4, "gcr": 5, "idr": 6}
+
+
+def solve(matrix, preconditioner, rhs_dev, x_dev, tol=1e-10, max_iterations=100000, stream=None, solver="cg",
+          dim=0):
+    """The assembled-matrix solve from x = 0 with a Krylov method of the reference's menu (CG by
+    default; dim: GMRES / GCR Krylov dimension or IDR subspace, 0 for the reference's 100 / 8);
+    returns Diagnostics."""
     st = _native.SilSolveSettings()
     st.max_iterations = max_iterations
     st.relative_tolerance = tol
     d = _native.SilSolveDiagnostics()
-    check(lib().sil_csr_solve(_stream(stream), matrix._h, preconditioner._h, ctypes.c_void_p(rhs_dev.data_ptr()),
-                              ctypes.c_void_p(x_dev.data_ptr()), ctypes.byref(st), ctypes.byref(d)), "csr_solve")
+    if solver not in SOLVERS:
+        raise ValueError(f"unknown solver: {solver}")
+    check(lib().sil_csr_krylov_solve(_stream(stream), matrix._h, preconditioner._h, SOLVERS[solver], dim,
+                                     ctypes.c_void_p(rhs_dev.data_ptr()), ctypes.c_void_p(x_dev.data_ptr()),
+                                     ctypes.byref(st), ctypes.byref(d)), "csr_krylov_solve")
     return Diagnostics(d.iterations, bool(d.converged), d.refinements, d.status, d.initial_residual_l2,
                        d.final_residual_l2, d.final_relative_residual)

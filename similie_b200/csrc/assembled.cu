@@ -738,6 +738,471 @@ __global__ void cg_check_kernel(double const* part, int nparts, CgState* st, dou
 }  // namespace
 }  // namespace sil
 
+namespace sil {
+namespace {
+
+// ------------------------------------------------------------------ Krylov menu
+//
+// Host-driven restatements of the published methods (the same steps as the
+// CPU restatement): vectors on the device, scalars on the host, every dot
+// product reduced from fixed per-block partials in a fixed order.
+
+__global__ void axpy_k(int64_t n, double a, double const* x, double* y)
+{
+    for (int64_t i = blockIdx.x * int64_t(kBlock) + threadIdx.x; i < n; i += int64_t(gridDim.x) * kBlock)
+        y[i] += a * x[i];
+}
+
+// out = a x + b y
+__global__ void lin2_k(int64_t n, double a, double const* x, double b, double const* y, double* out)
+{
+    for (int64_t i = blockIdx.x * int64_t(kBlock) + threadIdx.x; i < n; i += int64_t(gridDim.x) * kBlock)
+        out[i] = a * x[i] + b * y[i];
+}
+
+__global__ void scale_k(int64_t n, double a, double const* x, double* out)
+{
+    for (int64_t i = blockIdx.x * int64_t(kBlock) + threadIdx.x; i < n; i += int64_t(gridDim.x) * kBlock)
+        out[i] = x[i] / a;
+}
+
+// BiCGSTAB direction: p = r + beta (p - omega v)
+__global__ void bicg_p_k(int64_t n, double beta, double omega, double const* r, double const* v, double* p)
+{
+    for (int64_t i = blockIdx.x * int64_t(kBlock) + threadIdx.x; i < n; i += int64_t(gridDim.x) * kBlock)
+        p[i] = r[i] + beta * (p[i] - omega * v[i]);
+}
+
+// MINRES direction: d = (w - r3 d_older - r2 d_old) / r1
+__global__ void minres_d_k(int64_t n, double r1, double r2, double r3, double const* w, double const* d_older,
+                           double const* d_old, double* d)
+{
+    for (int64_t i = blockIdx.x * int64_t(kBlock) + threadIdx.x; i < n; i += int64_t(gridDim.x) * kBlock)
+        d[i] = (w[i] - r3 * d_older[i] - r2 * d_old[i]) / r1;
+}
+
+// MINRES Lanczos vector: v_new = q - a v - b v_old
+__global__ void lanczos_k(int64_t n, double a, double b, double const* q, double const* v, double const* v_old,
+                          double* v_new)
+{
+    for (int64_t i = blockIdx.x * int64_t(kBlock) + threadIdx.x; i < n; i += int64_t(gridDim.x) * kBlock)
+        v_new[i] = q[i] - a * v[i] - b * v_old[i];
+}
+
+class Krylov
+{
+public:
+    Krylov(cudaStream_t s, sil_csr_s const& A, sil_csr_precond_s const& P)
+        : s_(s), A_(A), P_(P), n_(A.n), G_(grid_of(A.n)), hpart_(G_)
+    {
+    }
+    ~Krylov() { cudaFree(buf_); }
+
+    // device vectors, zeroed
+    sil_status alloc(int count)
+    {
+        size_t const vb = (static_cast<size_t>(n_) * sizeof(double) + 255) / 256 * 256;
+        size_t const pb = (static_cast<size_t>(G_) * sizeof(double) + 255) / 256 * 256;
+        SIL_CUDA_CHECK(cudaMalloc(&buf_, count * vb + pb));
+        SIL_CUDA_CHECK(cudaMemsetAsync(buf_, 0, count * vb + pb, s_));
+        for (int k = 0; k < count; ++k) v_.push_back(reinterpret_cast<double*>(static_cast<char*>(buf_) + k * vb));
+        part_ = reinterpret_cast<double*>(static_cast<char*>(buf_) + count * vb);
+        return SIL_OK;
+    }
+    double* vec(int k) const { return v_[k]; }
+    int64_t n() const { return n_; }
+
+    sil_status dot(double const* a, double const* b, double* out)
+    {
+        dot_kernel<<<G_, kBlock, 0, s_>>>(n_, a, b, part_, nullptr);
+        SIL_CUDA_CHECK(cudaGetLastError());
+        SIL_CUDA_CHECK(cudaMemcpyAsync(hpart_.data(), part_, G_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        SIL_CUDA_CHECK(cudaStreamSynchronize(s_));
+        double t = 0.0;
+        for (double v : hpart_) t += v;
+        *out = t;
+        return SIL_OK;
+    }
+    sil_status norm(double const* a, double* out)
+    {
+        double t = 0.0;
+        if (sil_status st = dot(a, a, &t); st != SIL_OK) return st;
+        *out = std::sqrt(t);
+        return SIL_OK;
+    }
+    void spmv(double const* x, double* y) { spmv_kernel<<<G_, kBlock, 0, s_>>>(n_, A_.ptr, A_.col, A_.val, x, y); }
+    void precond(double const* r, double* z) { precond_launch(P_, s_, r, z, nullptr); }
+    void axpy(double a, double const* x, double* y) { axpy_k<<<G_, kBlock, 0, s_>>>(n_, a, x, y); }
+    void lin2(double a, double const* x, double b, double const* y, double* out)
+    {
+        lin2_k<<<G_, kBlock, 0, s_>>>(n_, a, x, b, y, out);
+    }
+    void copy(double const* x, double* y)
+    {
+        cudaMemcpyAsync(y, x, static_cast<size_t>(n_) * sizeof(double), cudaMemcpyDeviceToDevice, s_);
+    }
+    void divide(double const* x, double a, double* out) { scale_k<<<G_, kBlock, 0, s_>>>(n_, a, x, out); }
+    unsigned grid() const { return G_; }
+    cudaStream_t stream() const { return s_; }
+
+private:
+    cudaStream_t s_;
+    sil_csr_s const& A_;
+    sil_csr_precond_s const& P_;
+    int64_t n_;
+    unsigned G_;
+    void* buf_ = nullptr;
+    std::vector<double*> v_;
+    double* part_ = nullptr;
+    std::vector<double> hpart_;
+};
+
+#define KRY_CHECK(call)                                    \
+    do {                                                   \
+        if (sil_status const kst_ = (call); kst_ != SIL_OK) \
+            return kst_;                                   \
+    } while (0)
+
+// Each returns the iterations in *its and the last residual norm in *rn.
+sil_status run_fcg(Krylov& K, double const* b, double* x, double target, int max_iter, int* its, double* rn)
+{
+    KRY_CHECK(K.alloc(6));
+    double *r = K.vec(0), *z = K.vec(1), *p = K.vec(2), *q = K.vec(3), *r_old = K.vec(4), *t = K.vec(5);
+    K.copy(b, r);
+    K.precond(r, z);
+    K.copy(z, p);
+    double rz = 0.0;
+    KRY_CHECK(K.dot(r, z, &rz));
+    KRY_CHECK(K.norm(b, rn));
+    int it = 0;
+    while (it < max_iter) {
+        K.spmv(p, q);
+        double pq = 0.0;
+        KRY_CHECK(K.dot(p, q, &pq));
+        double const alpha = rz / pq;
+        K.axpy(alpha, p, x);
+        K.copy(r, r_old);
+        K.axpy(-alpha, q, r);
+        ++it;
+        KRY_CHECK(K.norm(r, rn));
+        if (!(*rn > target)) break;
+        K.precond(r, z);
+        K.lin2(1.0, r, -1.0, r_old, t);
+        double num = 0.0;
+        KRY_CHECK(K.dot(z, t, &num));
+        double const beta = num / rz;
+        KRY_CHECK(K.dot(r, z, &rz));
+        K.lin2(1.0, z, beta, p, p);
+    }
+    *its = it;
+    return SIL_OK;
+}
+
+sil_status run_minres(Krylov& K, double const* b, double* x, double target, int max_iter, int* its, double* rn)
+{
+    KRY_CHECK(K.alloc(12));
+    double *v_old = K.vec(0), *v = K.vec(1), *w = K.vec(2), *v_new = K.vec(3), *w_new = K.vec(4), *q = K.vec(5);
+    double *d_older = K.vec(6), *d_old = K.vec(7), *d = K.vec(8), *t = K.vec(9);
+    K.copy(b, v);
+    K.precond(v, w);
+    double vw = 0.0;
+    KRY_CHECK(K.dot(v, w, &vw));
+    double beta = std::sqrt(vw), beta_prev = 1.0, eta = beta;
+    double c_old = 1.0, s_old = 0.0, c = 1.0, s = 0.0;
+    KRY_CHECK(K.norm(b, rn));
+    int it = 0;
+    while (it < max_iter && beta > 0.0) {
+        K.divide(w, beta, w);
+        K.spmv(w, q);
+        double alpha = 0.0;
+        KRY_CHECK(K.dot(w, q, &alpha));
+        lanczos_k<<<K.grid(), kBlock, 0, K.stream()>>>(K.n(), alpha / beta, beta / beta_prev, q, v, v_old, v_new);
+        K.precond(v_new, w_new);
+        double vv = 0.0;
+        KRY_CHECK(K.dot(v_new, w_new, &vv));
+        double const beta_new = std::sqrt(std::max(0.0, vv));
+        double const delta = c * alpha - c_old * s * beta;
+        double const rho2 = s * alpha + c_old * c * beta;
+        double const rho3 = s_old * beta;
+        double const rho1 = std::sqrt(delta * delta + beta_new * beta_new);
+        double const c_new = delta / rho1, s_new = beta_new / rho1;
+        minres_d_k<<<K.grid(), kBlock, 0, K.stream()>>>(K.n(), rho1, rho2, rho3, w, d_older, d_old, d);
+        K.axpy(c_new * eta, d, x);
+        eta = -s_new * eta;
+        K.copy(d_old, d_older);
+        K.copy(d, d_old);
+        K.copy(v, v_old);
+        K.copy(v_new, v);
+        K.copy(w_new, w);
+        beta_prev = beta;
+        beta = beta_new;
+        c_old = c;
+        s_old = s;
+        c = c_new;
+        s = s_new;
+        ++it;
+        K.spmv(x, t);
+        K.lin2(1.0, b, -1.0, t, t);
+        KRY_CHECK(K.norm(t, rn));
+        if (!(*rn > target)) break;
+    }
+    *its = it;
+    return SIL_OK;
+}
+
+sil_status run_gmres(Krylov& K, int m, double const* b, double* x, double target, int max_iter, int* its, double* rn)
+{
+    KRY_CHECK(K.alloc(m + 5));
+    double *r = K.vec(m + 1), *z = K.vec(m + 2), *u = K.vec(m + 3), *t = K.vec(m + 4);
+    std::vector<double> H(static_cast<size_t>(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    K.copy(b, r);
+    KRY_CHECK(K.norm(b, rn));
+    int it = 0;
+    while (it < max_iter) {
+        double beta = 0.0;
+        KRY_CHECK(K.norm(r, &beta));
+        if (!(beta > target)) {
+            *rn = beta;
+            break;
+        }
+        K.divide(r, beta, K.vec(0));
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int k = 0;
+        bool done = false;
+        for (; k < m && it < max_iter; ++k) {
+            K.precond(K.vec(k), z);
+            K.spmv(z, u);
+            for (int j = 0; j <= k; ++j) {
+                double h = 0.0;
+                KRY_CHECK(K.dot(u, K.vec(j), &h));
+                H[j * m + k] = h;
+                K.axpy(-h, K.vec(j), u);
+            }
+            double hn = 0.0;
+            KRY_CHECK(K.norm(u, &hn));
+            H[(k + 1) * m + k] = hn;
+            if (hn != 0.0) K.divide(u, hn, K.vec(k + 1));
+            for (int j = 0; j < k; ++j) {
+                double const a = H[j * m + k], bb = H[(j + 1) * m + k];
+                H[j * m + k] = cs[j] * a + sn[j] * bb;
+                H[(j + 1) * m + k] = -sn[j] * a + cs[j] * bb;
+            }
+            double const a = H[k * m + k], bb = H[(k + 1) * m + k];
+            double const den = std::sqrt(a * a + bb * bb);
+            cs[k] = a / den;
+            sn[k] = bb / den;
+            H[k * m + k] = den;
+            H[(k + 1) * m + k] = 0.0;
+            g[k + 1] = -sn[k] * g[k];
+            g[k] = cs[k] * g[k];
+            ++it;
+            *rn = std::fabs(g[k + 1]);
+            if (!(*rn > target)) {
+                ++k;
+                done = true;
+                break;
+            }
+        }
+        for (int j = k - 1; j >= 0; --j) {
+            double acc = g[j];
+            for (int l = j + 1; l < k; ++l) acc -= H[j * m + l] * y[l];
+            y[j] = acc / H[j * m + j];
+        }
+        cudaMemsetAsync(u, 0, static_cast<size_t>(K.n()) * sizeof(double), K.stream());
+        for (int j = 0; j < k; ++j) K.axpy(y[j], K.vec(j), u);
+        K.precond(u, z);
+        K.axpy(1.0, z, x);
+        K.spmv(x, t);
+        K.lin2(1.0, b, -1.0, t, r);
+        if (done) break;
+    }
+    *its = it;
+    return SIL_OK;
+}
+
+sil_status run_bicgstab(Krylov& K, double const* b, double* x, double target, int max_iter, int* its, double* rn)
+{
+    KRY_CHECK(K.alloc(8));
+    double *r = K.vec(0), *r0 = K.vec(1), *v = K.vec(2), *p = K.vec(3), *ph = K.vec(4), *sv = K.vec(5),
+           *sh = K.vec(6), *tv = K.vec(7);
+    K.copy(b, r);
+    K.copy(b, r0);
+    double rho = 1.0, alpha = 1.0, omega = 1.0;
+    KRY_CHECK(K.norm(b, rn));
+    int it = 0;
+    while (it < max_iter) {
+        double rho_new = 0.0;
+        KRY_CHECK(K.dot(r0, r, &rho_new));
+        double const beta = (rho_new / rho) * (alpha / omega);
+        bicg_p_k<<<K.grid(), kBlock, 0, K.stream()>>>(K.n(), beta, omega, r, v, p);
+        K.precond(p, ph);
+        K.spmv(ph, v);
+        double r0v = 0.0;
+        KRY_CHECK(K.dot(r0, v, &r0v));
+        alpha = rho_new / r0v;
+        K.lin2(1.0, r, -alpha, v, sv);
+        ++it;
+        double sn = 0.0;
+        KRY_CHECK(K.norm(sv, &sn));
+        if (!(sn > target)) {
+            K.axpy(alpha, ph, x);
+            *rn = sn;
+            break;
+        }
+        K.precond(sv, sh);
+        K.spmv(sh, tv);
+        double ts = 0.0, tt = 0.0;
+        KRY_CHECK(K.dot(tv, sv, &ts));
+        KRY_CHECK(K.dot(tv, tv, &tt));
+        omega = ts / tt;
+        K.axpy(alpha, ph, x);
+        K.axpy(omega, sh, x);
+        K.lin2(1.0, sv, -omega, tv, r);
+        rho = rho_new;
+        KRY_CHECK(K.norm(r, rn));
+        if (!(*rn > target)) break;
+    }
+    *its = it;
+    return SIL_OK;
+}
+
+sil_status run_gcr(Krylov& K, int m, double const* b, double* x, double target, int max_iter, int* its, double* rn)
+{
+    KRY_CHECK(K.alloc(2 * m + 1));
+    double* r = K.vec(2 * m);
+    K.copy(b, r);
+    KRY_CHECK(K.norm(b, rn));
+    int it = 0, k = 0;
+    while (it < max_iter) {
+        if (k == m) k = 0;
+        double *P = K.vec(k), *Q = K.vec(m + k);
+        K.precond(r, P);
+        K.spmv(P, Q);
+        for (int j = 0; j < k; ++j) {
+            double h = 0.0;
+            KRY_CHECK(K.dot(Q, K.vec(m + j), &h));
+            K.axpy(-h, K.vec(m + j), Q);
+            K.axpy(-h, K.vec(j), P);
+        }
+        double qn = 0.0;
+        KRY_CHECK(K.norm(Q, &qn));
+        K.divide(Q, qn, Q);
+        K.divide(P, qn, P);
+        double alpha = 0.0;
+        KRY_CHECK(K.dot(r, Q, &alpha));
+        K.axpy(alpha, P, x);
+        K.axpy(-alpha, Q, r);
+        ++k;
+        ++it;
+        KRY_CHECK(K.norm(r, rn));
+        if (!(*rn > target)) break;
+    }
+    *its = it;
+    return SIL_OK;
+}
+
+sil_status run_idr(Krylov& K, int s, double const* b, double* x, double target, int max_iter, int* its, double* rn)
+{
+    int64_t const n = K.n();
+    KRY_CHECK(K.alloc(3 * s + 4));
+    double *r = K.vec(3 * s), *vv = K.vec(3 * s + 1), *vh = K.vec(3 * s + 2), *tt = K.vec(3 * s + 3);
+    auto Pv = [&](int j) { return K.vec(j); };
+    auto Gv = [&](int j) { return K.vec(s + j); };
+    auto Uv = [&](int j) { return K.vec(2 * s + j); };
+    // the shadow space of the CPU restatement: xorshift64 + Box-Muller, the
+    // vectors orthonormalised in order (on the host)
+    {
+        std::vector<std::vector<double>> P(s, std::vector<double>(n));
+        uint64_t state = 0x9E3779B97F4A7C15ull;
+        auto uniform = [&]() {
+            state ^= state << 13;
+            state ^= state >> 7;
+            state ^= state << 17;
+            return (static_cast<double>(state >> 11) + 0.5) / 9007199254740992.0;
+        };
+        auto hdot = [&](std::vector<double> const& a, std::vector<double> const& c) {
+            double t = 0.0;
+            for (int64_t i = 0; i < n; ++i) t += a[i] * c[i];
+            return t;
+        };
+        for (int j = 0; j < s; ++j) {
+            for (int64_t i = 0; i < n; ++i) {
+                double const u1 = uniform(), u2 = uniform();
+                P[j][i] = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+            }
+            for (int l = 0; l < j; ++l) {
+                double const h = hdot(P[j], P[l]);
+                for (int64_t i = 0; i < n; ++i) P[j][i] += -h * P[l][i];
+            }
+            double const pn = std::sqrt(hdot(P[j], P[j]));
+            for (int64_t i = 0; i < n; ++i) P[j][i] /= pn;
+            SIL_CUDA_CHECK(cudaMemcpyAsync(Pv(j), P[j].data(), n * sizeof(double), cudaMemcpyHostToDevice, K.stream()));
+        }
+        SIL_CUDA_CHECK(cudaStreamSynchronize(K.stream()));
+    }
+    std::vector<double> Mm(static_cast<size_t>(s) * s, 0.0), f(s), c(s);
+    for (int j = 0; j < s; ++j) Mm[j * s + j] = 1.0;
+    K.copy(b, r);
+    double om = 1.0;
+    KRY_CHECK(K.norm(b, rn));
+    int it = 0;
+    while (it < max_iter) {
+        for (int j = 0; j < s; ++j) KRY_CHECK(K.dot(Pv(j), r, &f[j]));
+        for (int k = 0; k < s && it < max_iter; ++k) {
+            for (int i = k; i < s; ++i) {
+                double acc = f[i];
+                for (int j = k; j < i; ++j) acc -= Mm[i * s + j] * c[j];
+                c[i] = acc / Mm[i * s + i];
+            }
+            K.copy(r, vv);
+            for (int i = k; i < s; ++i) K.axpy(-c[i], Gv(i), vv);
+            K.precond(vv, vh);
+            // U_k = om vh + sum_{j >= k} c_j U_j (U_k's old value included)
+            K.lin2(om, vh, c[k], Uv(k), Uv(k));
+            for (int j = k + 1; j < s; ++j) K.axpy(c[j], Uv(j), Uv(k));
+            K.spmv(Uv(k), Gv(k));
+            for (int i = 0; i < k; ++i) {
+                double pg = 0.0;
+                KRY_CHECK(K.dot(Pv(i), Gv(k), &pg));
+                double const a = pg / Mm[i * s + i];
+                K.axpy(-a, Gv(i), Gv(k));
+                K.axpy(-a, Uv(i), Uv(k));
+            }
+            for (int i = k; i < s; ++i) KRY_CHECK(K.dot(Pv(i), Gv(k), &Mm[i * s + k]));
+            double const beta = f[k] / Mm[k * s + k];
+            K.axpy(-beta, Gv(k), r);
+            K.axpy(beta, Uv(k), x);
+            ++it;
+            KRY_CHECK(K.norm(r, rn));
+            if (!(*rn > target)) break;
+            for (int i = k + 1; i < s; ++i) f[i] -= beta * Mm[i * s + k];
+        }
+        if (!(*rn > target) || it >= max_iter) break;
+        K.precond(r, vh);
+        K.spmv(vh, tt);
+        double tn = 0.0, tr = 0.0, rr = 0.0;
+        KRY_CHECK(K.dot(tt, tt, &tn));
+        KRY_CHECK(K.dot(tt, r, &tr));
+        KRY_CHECK(K.norm(r, &rr));
+        om = tr / tn;
+        double const rho = std::fabs(tr) / (std::sqrt(tn) * rr);
+        if (rho < 0.7) om *= 0.7 / rho;
+        K.axpy(-om, tt, r);
+        K.axpy(om, vh, x);
+        ++it;
+        KRY_CHECK(K.norm(r, rn));
+        if (!(*rn > target)) break;
+    }
+    *its = it;
+    return SIL_OK;
+}
+
+#undef KRY_CHECK
+
+}  // namespace
+}  // namespace sil
+
 using namespace sil;
 
 extern "C" {
@@ -964,20 +1429,54 @@ sil_status sil_csr_solve(sil_stream stream, sil_csr m, sil_csr_precond pc, const
     cg_rz_kernel<<<1, kBlock, 0, s>>>(part, np, st);
     cg_direction_kernel<<<G, kBlock, 0, s>>>(n, part, np, z, p, st, 1);
     SIL_CUDA_CHECK(cudaGetLastError());
-    // iterations issued in chunks, the state read back after each chunk
+    // A chunk of iterations captured once as a CUDA graph (every kernel does
+    // nothing once the state is done) and replayed until convergence, the
+    // state read back after each replay.  The level-scheduled
+    // preconditioners launch two kernels per level, so their chunks are
+    // shorter (at most about 4,096 launches per graph).
+    int const per_apply = static_cast<int>(pc->fwd_lev.size() + pc->bwd_lev.size()) + 8;
+    int const chunk = std::max(1, std::min(16, 4096 / per_apply));
+    auto issue = [&](cudaStream_t cs) {
+        for (int c = 0; c < chunk; ++c) {
+            cg_spmv_kernel<<<G, kBlock, 0, cs>>>(n, m->ptr, m->col, m->val, p, q, part, st);
+            cg_alpha_kernel<<<1, kBlock, 0, cs>>>(part, np, st);
+            cg_update_kernel<<<G, kBlock, 0, cs>>>(n, x, r, p, q, part, st);
+            cg_check_kernel<<<1, kBlock, 0, cs>>>(part, np, st, tol, max_iter);
+            precond_launch(*pc, cs, r, z, st);
+            dot_kernel<<<G, kBlock, 0, cs>>>(n, r, z, part, st);
+            cg_direction_kernel<<<G, kBlock, 0, cs>>>(n, part, np, z, p, st, 0);
+            cg_rz_kernel<<<1, kBlock, 0, cs>>>(part, np, st);
+        }
+    };
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    {
+        cudaStream_t cs;
+        SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) issue(cs);
+        cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
+        if (err == cudaSuccess) err = err2;
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+        cudaStreamDestroy(cs);
+        if (err != cudaSuccess) {
+            if (graph != nullptr) cudaGraphDestroy(graph);
+            return cuda_fail(err, "sil_csr_solve: CG graph capture");
+        }
+    }
+    struct GraphGuard
+    {
+        cudaGraph_t g;
+        cudaGraphExec_t e;
+        ~GraphGuard()
+        {
+            cudaGraphExecDestroy(e);
+            cudaGraphDestroy(g);
+        }
+    } guard {graph, exec};
     CgState hs {};
     for (;;) {
-        for (int c = 0; c < 16; ++c) {
-            cg_spmv_kernel<<<G, kBlock, 0, s>>>(n, m->ptr, m->col, m->val, p, q, part, st);
-            cg_alpha_kernel<<<1, kBlock, 0, s>>>(part, np, st);
-            cg_update_kernel<<<G, kBlock, 0, s>>>(n, x, r, p, q, part, st);
-            cg_check_kernel<<<1, kBlock, 0, s>>>(part, np, st, tol, max_iter);
-            precond_launch(*pc, s, r, z, st);
-            dot_kernel<<<G, kBlock, 0, s>>>(n, r, z, part, st);
-            cg_direction_kernel<<<G, kBlock, 0, s>>>(n, part, np, z, p, st, 0);
-            cg_rz_kernel<<<1, kBlock, 0, s>>>(part, np, st);
-        }
-        SIL_CUDA_CHECK(cudaGetLastError());
+        SIL_CUDA_CHECK(cudaGraphLaunch(exec, s));
         SIL_CUDA_CHECK(cudaMemcpyAsync(&hs, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
         SIL_CUDA_CHECK(cudaStreamSynchronize(s));
         if (hs.done) break;
@@ -990,6 +1489,56 @@ sil_status sil_csr_solve(sil_stream stream, sil_csr m, sil_csr_precond pc, const
     diag->converged = (hs.bn == 0.0 || hs.rn <= tol * hs.bn) ? 1 : 0;
     diag->status = std::isfinite(hs.rn) ? SIL_OK : SIL_ERR_NONFINITE;
     diag->refinements = 0;
+    return SIL_OK;
+}
+
+sil_status sil_csr_krylov_solve(sil_stream stream, sil_csr m, sil_csr_precond pc, int32_t solver, int32_t dim,
+                                const double* rhs, double* x, const sil_solve_settings* settings,
+                                sil_solve_diagnostics* diag)
+{
+    if (m == nullptr || pc == nullptr || rhs == nullptr || x == nullptr || settings == nullptr || diag == nullptr)
+        return fail(SIL_ERR_INVALID, "sil_csr_krylov_solve: NULL argument");
+    if (pc->A != m) return fail(SIL_ERR_INVALID, "sil_csr_krylov_solve: preconditioner built for another matrix");
+    if (solver < SIL_KRYLOV_CG || solver > SIL_KRYLOV_IDR)
+        return fail(SIL_ERR_INVALID, "sil_csr_krylov_solve: unknown solver");
+    if (dim < 0) return fail(SIL_ERR_INVALID, "sil_csr_krylov_solve: negative Krylov dimension");
+    if (solver == SIL_KRYLOV_CG) return sil_csr_solve(stream, m, pc, rhs, x, settings, diag);
+    cudaStream_t const s = static_cast<cudaStream_t>(stream);
+    double const tol = settings->relative_tolerance > 0 ? settings->relative_tolerance : 1e-10;
+    int const max_iter = settings->max_iterations > 0 ? settings->max_iterations : 100000;
+    SIL_CUDA_CHECK(cudaMemsetAsync(x, 0, static_cast<size_t>(m->n) * sizeof(double), s));
+    Krylov K(s, *m, *pc);
+    double bn = 0.0;
+    {
+        Krylov N(s, *m, *pc);
+        if (sil_status st = N.alloc(0); st != SIL_OK) return st;
+        if (sil_status st = N.norm(rhs, &bn); st != SIL_OK) return st;
+    }
+    *diag = sil_solve_diagnostics {};
+    diag->initial_residual_l2 = bn;
+    int its = 0;
+    double rn = bn;
+    if (bn > 0.0) {
+        double const target = tol * bn;
+        int const d = dim > 0 ? dim : (solver == SIL_KRYLOV_IDR ? 8 : 100);
+        sil_status st = SIL_OK;
+        switch (solver) {
+        case SIL_KRYLOV_MINRES: st = run_minres(K, rhs, x, target, max_iter, &its, &rn); break;
+        case SIL_KRYLOV_FCG: st = run_fcg(K, rhs, x, target, max_iter, &its, &rn); break;
+        case SIL_KRYLOV_GMRES: st = run_gmres(K, d, rhs, x, target, max_iter, &its, &rn); break;
+        case SIL_KRYLOV_BICGSTAB: st = run_bicgstab(K, rhs, x, target, max_iter, &its, &rn); break;
+        case SIL_KRYLOV_GCR: st = run_gcr(K, d, rhs, x, target, max_iter, &its, &rn); break;
+        default: st = run_idr(K, d, rhs, x, target, max_iter, &its, &rn); break;
+        }
+        if (st != SIL_OK) return st;
+        SIL_CUDA_CHECK(cudaGetLastError());
+    }
+    SIL_CUDA_CHECK(cudaStreamSynchronize(s));
+    diag->iterations = its;
+    diag->final_residual_l2 = rn;
+    diag->final_relative_residual = bn == 0.0 ? 0.0 : rn / bn;
+    diag->converged = (bn == 0.0 || rn <= tol * bn) ? 1 : 0;
+    diag->status = std::isfinite(rn) ? SIL_OK : SIL_ERR_NONFINITE;
     return SIL_OK;
 }
 

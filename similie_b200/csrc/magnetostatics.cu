@@ -93,6 +93,7 @@ struct ProbInfo
     int gauge;                // 3D: 0 penalty, 1 divergence gauge
     double const* gd64;       // divergence gauge, 8 per node: E0[3], E1[3], w, 0
     float const* gd32;
+    int max_iters;            // iteration budget: the problem stops once it has done this many
 };
 
 template <class T>
@@ -547,7 +548,7 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(Item const* items, Pr
         s->rr0 = tot_bb;
         if (!from_r64) s->bb = tot_bb;
         s->iters = 0;
-        s->done = (tot_bb == 0.0) ? 1 : 0;
+        s->done = (tot_bb == 0.0 || s->total_iters >= pi.max_iters) ? 1 : 0;
         s->nonfinite = 0;
     }
 }
@@ -626,7 +627,7 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(Item const* items, 
         s->iters += 1;
         s->total_iters += 1;
         if (!isfinite(tot_rr) || !isfinite(trz)) s->nonfinite = 1;
-        if (tot_rr <= s->inner_tol2 * s->rr0 || s->nonfinite) s->done = 1;
+        if (tot_rr <= s->inner_tol2 * s->rr0 || s->nonfinite || s->total_iters >= pi.max_iters) s->done = 1;
     }
 }
 
@@ -691,7 +692,7 @@ __global__ void __launch_bounds__(kThreads) fcg_init_kernel(Item const* items, P
         s->win_rr = tot;
         s->win_iters = 0;
         s->iters = 0;
-        s->done = (tot == 0.0) ? 1 : 0;
+        s->done = (tot == 0.0 || s->total_iters >= pi.max_iters) ? 1 : 0;
         s->nonfinite = 0;
     }
 }
@@ -834,7 +835,7 @@ __global__ void __launch_bounds__(kThreads) fcg_update_kernel(Item const* items,
         s->total_iters += 1;
         s->learned_iters += 1;
         if (!isfinite(tot)) s->nonfinite = 1;
-        if (tot <= s->inner_tol2 * s->rr0 || s->nonfinite) s->done = 1;
+        if (tot <= s->inner_tol2 * s->rr0 || s->nonfinite || s->total_iters >= pi.max_iters) s->done = 1;
         if (++s->win_iters >= window) {
             if (!(tot <= 0.01 * s->win_rr)) {
                 s->fallback = 1;
@@ -1098,6 +1099,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         pi.nodes = pi.nx * pi.ny * pi.nz;
         pi.n = q.dim == 3 ? 3 * pi.nodes : pi.nodes;
         pi.gamma = q.gamma;
+        pi.max_iters = set.max_iterations > 0 ? set.max_iterations : 100000;
         pi.first_item = static_cast<int>(items.size());
         int idx = 0;
         // 3D items: whole nodes (3 rows each), four times the 2D item, so
@@ -1639,6 +1641,30 @@ __global__ void mag3d_apply_kernel(ProbInfo pi, double const* nu, double const* 
 }
 
 } // namespace
+
+sil_status divergence_gauge_table(int64_t nx, int64_t ny, int64_t nz, double const* const coords[3], double const* ls,
+                                  double* gd, double* probe, double* out, cudaStream_t st)
+{
+    ProblemDesc q {};
+    q.dim = 3;
+    q.nx = nx;
+    q.ny = ny;
+    q.nz = nz;
+    for (int a = 0; a < 3; ++a) q.coords[a] = coords[a];
+    q.gauge = 1;
+    ProbInfo pi {};
+    pi.dim = 3;
+    pi.nx = nx;
+    pi.ny = ny;
+    pi.nz = nz;
+    pi.nodes = nx * ny * nz;
+    pi.n = 3 * pi.nodes;
+    pi.ls64[0] = ls;
+    pi.ls64[1] = ls + nx;
+    pi.ls64[2] = ls + nx + ny;
+    return build_divergence_gauge(q, pi, gd, nullptr, probe, out, st);
+}
+
 } // namespace sil
 
 extern "C" {

@@ -483,6 +483,8 @@ struct Geo3
     int nx, ny, nz;
     double gamma;
     double const* ls[3];  // local spacing per axis
+    int gauge;            // 0 penalty, 1 divergence gauge
+    double const* gd;     // divergence gauge: 8 per node, E0[3], E1[3], w, 0
 };
 
 __device__ __forceinline__ bool interior3(Geo3 const& g, int i, int j, int k)
@@ -496,6 +498,38 @@ __device__ __forceinline__ void node_coords(Geo3 const& g, int s, int* i, int* j
     *i = s - t * g.nx;
     *k = t / g.ny;
     *j = t - *k * g.ny;
+}
+
+// Divergence gauge, the terms of the linear 3D operator: (D A)(m) =
+// sum_a E0(m, a) A_a(m) + E1(m, a) A_a(m - e_a) (boundary columns carry zero
+// coefficients), and the term of row (n, c), w(n) E0(n, c) (D A)(n) +
+// w(n + e_c) E1(n + e_c, c) (D A)(n + e_c)
+// (magnetostatics_onelab.hpp:1890-1945, 2355-2392).
+__device__ __forceinline__ double gauge_div3(double const* a, double const* gd, int m, int i, int j, int k, int nx,
+                                             int ny)
+{
+    double const* e = gd + 8 * m;
+    double s = 0.0;
+    s = s + e[0] * a[3 * m];
+    if (i > 0) s = s + e[3] * a[3 * (m - 1)];
+    s = s + e[1] * a[3 * m + 1];
+    if (j > 0) s = s + e[4] * a[3 * (m - nx) + 1];
+    s = s + e[2] * a[3 * m + 2];
+    if (k > 0) s = s + e[5] * a[3 * (m - nx * ny) + 2];
+    return s;
+}
+
+__device__ __forceinline__ double gauge_term3(double const* a, double const* gd, int n, int i, int j, int k, int nx,
+                                              int ny, int c)
+{
+    int const step = c == 0 ? 1 : (c == 1 ? nx : nx * ny);
+    int const m = n + step;
+    double const div_n = gauge_div3(a, gd, n, i, j, k, nx, ny);
+    double const div_m = gauge_div3(a, gd, m, i + (c == 0), j + (c == 1), k + (c == 2), nx, ny);
+    double t = 0.0;
+    t = t + gd[8 * n + 6] * gd[8 * n + c] * div_n;
+    t = t + gd[8 * m + 6] * gd[8 * m + 3 + c] * div_m;
+    return t;
 }
 
 // Curl moments of v at the interior sampled node s = (i, j, k), columns on
@@ -688,7 +722,8 @@ __global__ void __launch_bounds__(kBlock) nl3_gather_kernel(Geo3 g, double const
                 r += hv[b + 1];
                 ha = dx * dy / dz;
             }
-            f = __dadd_rn(r, __dmul_rn(__dmul_rn(g.gamma, ha), v[row]));
+            if (g.gauge) f = r + g.gamma * gauge_term3(v, g.gd, s, i, j, k, g.nx, g.ny, c);
+            else f = __dadd_rn(r, __dmul_rn(__dmul_rn(g.gamma, ha), v[row]));
         }
         if (MODE == 1) {
             double const rv = rhs[row] - f;
@@ -740,7 +775,14 @@ __global__ void __launch_bounds__(kBlock) nl3_dinv_kernel(Geo3 g, double const* 
             d += K[0] - K[1] - K[3] + K[4];
             ha = dx * dy / dz;
         }
-        dinv[row] = 1.0 / (d + g.gamma * ha);
+        if (g.gauge) {
+            int const step = c == 0 ? 1 : (c == 1 ? g.nx : g.nx * g.ny);
+            double const e0 = g.gd[8 * s + c], e1 = g.gd[8 * (s + step) + 3 + c];
+            double const gdiv = g.gd[8 * s + 6] * e0 * e0 + g.gd[8 * (s + step) + 6] * e1 * e1;
+            dinv[row] = 1.0 / (d + g.gamma * gdiv);
+        } else {
+            dinv[row] = 1.0 / (d + g.gamma * ha);
+        }
     }
 }
 
@@ -796,8 +838,9 @@ sil_status check_problem3(sil_mag3d_nl_problem const& p, char const* who, bool n
     if (p.x == nullptr || p.y == nullptr || p.z == nullptr) return fail(SIL_ERR_INVALID, w + ": NULL coordinate array");
     if (p.node_mu == nullptr || p.node_ferro == nullptr) return fail(SIL_ERR_INVALID, w + ": NULL material array");
     if (need_fields && (p.rhs == nullptr || p.solution == nullptr)) return fail(SIL_ERR_INVALID, w + ": NULL field pointer");
-    if (!std::isfinite(p.gauge_penalty) || !(p.gauge_penalty > 0.0))
-        return fail(SIL_ERR_INVALID, w + ": gauge_penalty must be finite and positive");
+    if (p.gauge != 0 && p.gauge != 1) return fail(SIL_ERR_INVALID, w + ": gauge must be 0 or 1");
+    if (!std::isfinite(p.gauge_penalty) || (p.gauge == 0 ? !(p.gauge_penalty > 0.0) : p.gauge_penalty == 0.0))
+        return fail(SIL_ERR_INVALID, w + ": gauge_penalty must be finite and positive (nonzero for the divergence gauge)");
     double const* c[3] = {p.x, p.y, p.z};
     int64_t const len[3] = {p.nx, p.ny, p.nz};
     for (int a = 0; a < 3; ++a)
@@ -825,9 +868,11 @@ std::vector<double> local_spacings(sil_mag3d_nl_problem const& p)
     return out;
 }
 
-Geo3 make_geo3(sil_mag3d_nl_problem const& p, double const* dls)
+Geo3 make_geo3(sil_mag3d_nl_problem const& p, double const* dls, double const* gd = nullptr)
 {
     Geo3 g {};
+    g.gauge = p.gauge;
+    g.gd = gd;
     g.nx = static_cast<int>(p.nx);
     g.ny = static_cast<int>(p.ny);
     g.nz = static_cast<int>(p.nz);
@@ -836,6 +881,16 @@ Geo3 make_geo3(sil_mag3d_nl_problem const& p, double const* dls)
     g.ls[1] = dls + p.nx;
     g.ls[2] = dls + p.nx + p.ny;
     return g;
+}
+
+// The divergence-gauge table of a problem into gd (8 per node); scratch: 4
+// doubles per node.
+sil_status gauge_table3(sil_mag3d_nl_problem const& p, double const* dls, double* gd, double* scratch,
+                        cudaStream_t st)
+{
+    int64_t const nodes = p.nx * p.ny * p.nz;
+    double const* coords[3] = {p.x, p.y, p.z};
+    return divergence_gauge_table(p.nx, p.ny, p.nz, coords, dls, gd, scratch, scratch + 3 * nodes, st);
 }
 
 // Stream-ordered device allocation, freed in stream order.
@@ -1198,11 +1253,16 @@ sil_status solve_one3(sil_mag3d_nl_problem const& P, DevCurve const& C, double t
     std::vector<double> const sp = local_spacings(P);
     size_t const hb = round256(static_cast<size_t>(3 * nodes) * sizeof(double)) / sizeof(double);
     size_t const kb = round256(static_cast<size_t>(9 * nodes) * sizeof(double)) / sizeof(double);
+    // divergence gauge: its table (8 per node) and the builder's scratch (4 per node)
+    size_t const gb = P.gauge ? round256(static_cast<size_t>(12 * nodes) * sizeof(double)) / sizeof(double) : 0;
     Workspace w;
-    if (sil_status s = w.init(n, G, hb + kb + sp.size()); s != SIL_OK) return s;
-    double* dls = w.extra + hb + kb;
+    if (sil_status s = w.init(n, G, hb + kb + gb + sp.size()); s != SIL_OK) return s;
+    double* gd = P.gauge ? w.extra + hb + kb : nullptr;
+    double* dls = w.extra + hb + kb + gb;
     SIL_CUDA_CHECK(cudaMemcpyAsync(dls, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, w.sg.s));
-    Ops3 const ops {C, make_geo3(P, dls), P, w.extra, w.extra + hb, n, G, grid_for(nodes)};
+    if (P.gauge)
+        if (sil_status s = gauge_table3(P, dls, gd, gd + 8 * nodes, w.sg.s); s != SIL_OK) return s;
+    Ops3 const ops {C, make_geo3(P, dls, gd), P, w.extra, w.extra + hb, n, G, grid_for(nodes)};
     if (sil_status s = newton(ops, P.solution, w.v, w.part, w.d_norm, w.d_cg, w.sg.s, tol, max_iter, D, menu);
         s != SIL_OK)
         return s;
@@ -1257,13 +1317,17 @@ sil_status sil_mag3d_nl_apply(sil_stream stream, const sil_mag3d_nl_problem* pro
     int64_t const nodes = P.nx * P.ny * P.nz;
     std::vector<double> const sp = local_spacings(P);
     size_t const hb = round256(static_cast<size_t>(3 * nodes) * sizeof(double));
+    size_t const gb = P.gauge ? round256(static_cast<size_t>(12 * nodes) * sizeof(double)) : 0;
     AsyncBuffer buf {nullptr, st, false};
-    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, hb + sp.size() * sizeof(double), st));
+    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, hb + gb + sp.size() * sizeof(double), st));
     double* hv = static_cast<double*>(buf.ptr);
-    double* dls = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb);
+    double* gd = P.gauge ? reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb) : nullptr;
+    double* dls = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb + gb);
     // a copy from pageable memory has left the host table once it returns
     SIL_CUDA_CHECK(cudaMemcpyAsync(dls, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    Geo3 const g = make_geo3(P, dls);
+    if (P.gauge)
+        if (sil_status s = gauge_table3(P, dls, gd, gd + 8 * nodes, st); s != SIL_OK) return s;
+    Geo3 const g = make_geo3(P, dls, gd);
     nl3_field_kernel<<<grid_for(nodes), kBlock, 0, st>>>(c, g, a, P.node_mu, P.node_ferro, hv);
     nl3_gather_kernel<0><<<grid_for(3 * nodes), kBlock, 0, st>>>(g, hv, a, nullptr, y, nullptr, nullptr);
     SIL_CUDA_CHECK(cudaGetLastError());
@@ -1283,13 +1347,17 @@ sil_status sil_mag3d_nl_apply_jacobian(sil_stream stream, const sil_mag3d_nl_pro
     std::vector<double> const sp = local_spacings(P);
     size_t const hb = round256(static_cast<size_t>(3 * nodes) * sizeof(double));
     size_t const kb = round256(static_cast<size_t>(9 * nodes) * sizeof(double));
+    size_t const gb = P.gauge ? round256(static_cast<size_t>(12 * nodes) * sizeof(double)) : 0;
     AsyncBuffer buf {nullptr, st, false};
-    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, hb + kb + sp.size() * sizeof(double), st));
+    SIL_CUDA_CHECK(cudaMallocAsync(&buf.ptr, hb + kb + gb + sp.size() * sizeof(double), st));
     double* hv = static_cast<double*>(buf.ptr);
     double* kh = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb);
-    double* dls = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb + kb);
+    double* gd = P.gauge ? reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb + kb) : nullptr;
+    double* dls = reinterpret_cast<double*>(static_cast<char*>(buf.ptr) + hb + kb + gb);
     SIL_CUDA_CHECK(cudaMemcpyAsync(dls, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    Geo3 const g = make_geo3(P, dls);
+    if (P.gauge)
+        if (sil_status s = gauge_table3(P, dls, gd, gd + 8 * nodes, st); s != SIL_OK) return s;
+    Geo3 const g = make_geo3(P, dls, gd);
     unsigned const gn = grid_for(nodes);
     nl3_coef_kernel<<<gn, kBlock, 0, st>>>(c, g, state, P.node_mu, P.node_ferro, kh);
     nl3_jfield_kernel<<<gn, kBlock, 0, st>>>(g, kh, x, hv, nullptr);

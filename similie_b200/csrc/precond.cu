@@ -2288,6 +2288,40 @@ sil_status sil_precond_set_params(sil_precond p, const float* host, sil_stream s
     return p->net.set_params(host, static_cast<cudaStream_t>(stream));
 }
 
+sil_status sil_precond_get_optimizer_state(sil_precond p, float* m, float* v, int64_t* step)
+{
+    if (p == nullptr) return sil::fail(SIL_ERR_INVALID, "sil_precond_get_optimizer_state: NULL");
+    sil::nn::Net& net = p->net;
+    size_t const bytes = sizeof(float) * sil::nn::kNumParams;
+    if (net.adam_m == nullptr) {
+        if (m != nullptr) std::memset(m, 0, bytes);
+        if (v != nullptr) std::memset(v, 0, bytes);
+        if (step != nullptr) *step = 0;
+        return SIL_OK;
+    }
+    SIL_CUDA_CHECK(cudaDeviceSynchronize());
+    if (m != nullptr) SIL_CUDA_CHECK(cudaMemcpy(m, net.adam_m, bytes, cudaMemcpyDeviceToHost));
+    if (v != nullptr) SIL_CUDA_CHECK(cudaMemcpy(v, net.adam_v, bytes, cudaMemcpyDeviceToHost));
+    if (step != nullptr) *step = net.adam_t;
+    return SIL_OK;
+}
+
+sil_status sil_precond_set_optimizer_state(sil_precond p, const float* m, const float* v, int64_t step,
+                                           sil_stream stream)
+{
+    if (p == nullptr || m == nullptr || v == nullptr || step < 0 || step > (int64_t(1) << 30))
+        return sil::fail(SIL_ERR_INVALID, "sil_precond_set_optimizer_state: NULL state or bad step");
+    sil::nn::Net& net = p->net;
+    if (net.adam_m == nullptr) return sil::fail(SIL_ERR_INVALID, "sil_precond_set_optimizer_state: set the parameters first");
+    cudaStream_t const s = static_cast<cudaStream_t>(stream);
+    size_t const bytes = sizeof(float) * sil::nn::kNumParams;
+    SIL_CUDA_CHECK(cudaMemcpyAsync(net.adam_m, m, bytes, cudaMemcpyHostToDevice, s));
+    SIL_CUDA_CHECK(cudaMemcpyAsync(net.adam_v, v, bytes, cudaMemcpyHostToDevice, s));
+    SIL_CUDA_CHECK(cudaStreamSynchronize(s));
+    net.adam_t = static_cast<int>(step);
+    return SIL_OK;
+}
+
 sil_status sil_precond_apply(sil_precond p, sil_stream stream, const sil_precond_sample* samples, int n,
                              const float* nu, const float* r, float* out)
 {

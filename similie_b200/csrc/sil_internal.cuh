@@ -141,6 +141,15 @@ struct GeoView
 template <class T>
 GeoView<T> geo_view(Geometry const& g);
 
+// The divergence-gauge table of a 3D grid (8 doubles per node: the
+// codifferential's coefficients E0[3], E1[3] read off parity probes, the
+// node weight w, 0), as the linear 3D operator builds it; coords: host node
+// coordinates per axis; ls: the device local-spacing table (x, y, z
+// concatenated); probe (3 doubles per node) and out (1 per node) are
+// scratch.  Defined in magnetostatics.cu.
+sil_status divergence_gauge_table(int64_t nx, int64_t ny, int64_t nz, double const* const coords[3],
+                                  double const* ls, double* gd, double* probe, double* out, cudaStream_t st);
+
 } // namespace sil
 
 struct sil_geometry_s

@@ -238,7 +238,7 @@ def nonlinear_problem(n, seed, tube=0.12):
     return p, p.node_mu(), node_ferro(n, n, n, core.ravel()), b, h
 
 
-def _nl_problem_struct(x, y, z, mu, ferro, curve, gamma, rhs_dev=None, sol_dev=None):
+def _nl_problem_struct(x, y, z, mu, ferro, curve, gamma, rhs_dev=None, sol_dev=None, gauge="penalty"):
     p = _native.SilMag3dNlProblem()
     p.nx, p.ny, p.nz = len(x), len(y), len(z)
     p.x, p.y, p.z = (v.ctypes.data for v in (x, y, z))
@@ -248,17 +248,18 @@ def _nl_problem_struct(x, y, z, mu, ferro, curve, gamma, rhs_dev=None, sol_dev=N
     p.rhs = 0 if rhs_dev is None else rhs_dev.data_ptr()
     p.solution = 0 if sol_dev is None else sol_dev.data_ptr()
     p.gauge_penalty = gamma
+    p.gauge = GAUGES[gauge]
     return p
 
 
 def nl_apply(x, y, z, node_mu_dev, node_ferro_dev, curve_b, curve_h, a_dev, y_dev, gamma=DEFAULT_GAUGE_PENALTY,
-             stream=None):
+             stream=None, gauge="penalty"):
     """y = F(a), the 3D nonlinear operator (torch CUDA float64 tensors, a/y flat 3*nodes)."""
     import torch
     from .magnetostatics import _Curve
     x, y, z = _f64(x), _f64(y), _f64(z)
     c = _Curve(curve_b, curve_h)
-    p = _nl_problem_struct(x, y, z, node_mu_dev, node_ferro_dev, c, gamma)
+    p = _nl_problem_struct(x, y, z, node_mu_dev, node_ferro_dev, c, gamma, gauge=gauge)
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
     check(lib().sil_mag3d_nl_apply(s, ctypes.byref(p), ctypes.c_void_p(a_dev.data_ptr()),
                                    ctypes.c_void_p(y_dev.data_ptr())), "mag3d_nl_apply")
@@ -266,13 +267,13 @@ def nl_apply(x, y, z, node_mu_dev, node_ferro_dev, curve_b, curve_h, a_dev, y_de
 
 
 def nl_apply_jacobian(x, y, z, node_mu_dev, node_ferro_dev, curve_b, curve_h, state_dev, v_dev, y_dev,
-                      gamma=DEFAULT_GAUGE_PENALTY, stream=None):
+                      gamma=DEFAULT_GAUGE_PENALTY, stream=None, gauge="penalty"):
     """y = J(state) v for the 3D nonlinear operator."""
     import torch
     from .magnetostatics import _Curve
     x, y, z = _f64(x), _f64(y), _f64(z)
     c = _Curve(curve_b, curve_h)
-    p = _nl_problem_struct(x, y, z, node_mu_dev, node_ferro_dev, c, gamma)
+    p = _nl_problem_struct(x, y, z, node_mu_dev, node_ferro_dev, c, gamma, gauge=gauge)
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
     check(lib().sil_mag3d_nl_apply_jacobian(s, ctypes.byref(p), ctypes.c_void_p(state_dev.data_ptr()),
                                             ctypes.c_void_p(v_dev.data_ptr()), ctypes.c_void_p(y_dev.data_ptr())),
@@ -281,7 +282,7 @@ def nl_apply_jacobian(x, y, z, node_mu_dev, node_ferro_dev, curve_b, curve_h, st
 
 
 def nl_solve_batch(coords, mus, ferros, curves, rhss, sols, gammas=None, tol=1e-10, max_iterations=100000,
-                   stream=None, jacobian_preconditioner=None):
+                   stream=None, jacobian_preconditioner=None, gauge="penalty"):
     """Newton + line search for a batch of 3D nonlinear problems.  coords: (x, y, z) host arrays;
     curves: (b, h) sample arrays; sols hold the initial guesses and receive the solutions.
     jacobian_preconditioner as in magnetostatics.nl_solve_batch.
@@ -294,7 +295,7 @@ def nl_solve_batch(coords, mus, ferros, curves, rhss, sols, gammas=None, tol=1e-
     kc = [_Curve(b, h) for b, h in curves]
     probs = (_native.SilMag3dNlProblem * n)()
     for k in range(n):
-        probs[k] = _nl_problem_struct(*keep[k], mus[k], ferros[k], kc[k], gammas[k], rhss[k], sols[k])
+        probs[k] = _nl_problem_struct(*keep[k], mus[k], ferros[k], kc[k], gammas[k], rhss[k], sols[k], gauge=gauge)
     st = _native.SilSolveSettings()
     st.max_iterations = max_iterations
     st.relative_tolerance = tol

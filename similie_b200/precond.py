@@ -63,14 +63,33 @@ class LearnedPreconditioner:
     def load(self, path):
         self.set_params(np.load(path))
 
+    def get_optimizer_state(self):
+        """(m, v, steps) of the library's Adam."""
+        m = np.zeros(self.num_params(), dtype=np.float32)
+        v = np.zeros(self.num_params(), dtype=np.float32)
+        t = ctypes.c_int64(0)
+        check(lib().sil_precond_get_optimizer_state(self._h, m.ctypes.data, v.ctypes.data, ctypes.byref(t)),
+              "precond_get_optimizer_state")
+        return m, v, t.value
+
+    def set_optimizer_state(self, m, v, steps, stream=None):
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        v = np.ascontiguousarray(v, dtype=np.float32)
+        check(lib().sil_precond_set_optimizer_state(self._h, m.ctypes.data, v.ctypes.data, int(steps), _stream(stream)),
+              "precond_set_optimizer_state")
+
     def save_checkpoint(self, path, step, seed, extra=None):
-        """A training checkpoint: header (format, dtype, count, step, seed) + parameters."""
-        write_checkpoint(path, self.get_params(), step, seed, extra)
+        """A training checkpoint: header, parameters and the Adam state."""
+        m, v, t = self.get_optimizer_state()
+        write_checkpoint(path, self.get_params(), step, seed, dict(extra or {}, adam_steps=t), m=m, v=v)
 
     def load_checkpoint(self, path):
-        """Restores the parameters of a checkpoint; returns its (step, seed, extra)."""
-        params, step, seed, extra = read_checkpoint(path)
+        """Restores the parameters (and the Adam state when the checkpoint has
+        it) of a checkpoint; returns its (step, seed, extra)."""
+        params, step, seed, extra, m, v = read_checkpoint(path, with_optimizer=True)
         self.set_params(params)
+        if m is not None:
+            self.set_optimizer_state(m, v, extra.get("adam_steps", step))
         return step, seed, extra
 
     def apply(self, shapes, nu, r, out, stream=None, active=None):
@@ -115,26 +134,31 @@ class LearnedPreconditioner:
 # Flat binary: 8-byte magic, then little-endian uint32 version, uint32 dtype
 # code (1 = float32), uint64 parameter count, uint64 step, uint64 seed,
 # uint64 length of a UTF-8 JSON block of extra fields, the JSON, then the
-# parameters.  The Adam moments stay inside the library's handle, so a
-# resumed run restarts them (the learning-rate schedule resumes at `step`).
+# parameters; version 2 adds the Adam moments m and v after them, so a
+# resumed run continues exactly.
 
 _MAGIC = b"SILPCKPT"
 
 
-def write_checkpoint(path, params, step, seed, extra=None):
+def write_checkpoint(path, params, step, seed, extra=None, m=None, v=None):
     import json
     import struct
     p = np.ascontiguousarray(params, dtype=np.float32)
     blob = json.dumps(extra or {}, sort_keys=True).encode()
+    version = 1 if m is None else 2
     with open(path, "wb") as f:
         f.write(_MAGIC)
-        f.write(struct.pack("<IIQQQQ", 1, 1, p.size, int(step), int(seed), len(blob)))
+        f.write(struct.pack("<IIQQQQ", version, 1, p.size, int(step), int(seed), len(blob)))
         f.write(blob)
         f.write(p.tobytes())
+        if m is not None:
+            f.write(np.ascontiguousarray(m, dtype=np.float32).tobytes())
+            f.write(np.ascontiguousarray(v, dtype=np.float32).tobytes())
 
 
-def read_checkpoint(path):
-    """(params, step, seed, extra) of a checkpoint; ValueError on a malformed file."""
+def read_checkpoint(path, with_optimizer=False):
+    """(params, step, seed, extra[, m, v]) of a checkpoint (m, v None for a
+    version-1 file); ValueError on a malformed file."""
     import json
     import struct
     with open(path, "rb") as f:
@@ -143,10 +167,16 @@ def read_checkpoint(path):
     if len(data) < head or data[:8] != _MAGIC:
         raise ValueError("not a preconditioner checkpoint")
     version, dtype, count, step, seed, nblob = struct.unpack("<IIQQQQ", data[8:head])
-    if version != 1 or dtype != 1:
+    if version not in (1, 2) or dtype != 1:
         raise ValueError(f"unsupported checkpoint version {version} / dtype {dtype}")
-    if len(data) != head + nblob + 4 * count:
+    arrays = 1 if version == 1 else 3
+    if len(data) != head + nblob + 4 * count * arrays:
         raise ValueError("truncated or padded checkpoint")
     extra = json.loads(data[head:head + nblob].decode())
-    params = np.frombuffer(data, dtype="<f4", count=count, offset=head + nblob).copy()
-    return params, step, seed, extra
+    off = head + nblob
+    params = np.frombuffer(data, dtype="<f4", count=count, offset=off).copy()
+    m = v = None
+    if version == 2:
+        m = np.frombuffer(data, dtype="<f4", count=count, offset=off + 4 * count).copy()
+        v = np.frombuffer(data, dtype="<f4", count=count, offset=off + 8 * count).copy()
+    return (params, step, seed, extra, m, v) if with_optimizer else (params, step, seed, extra)

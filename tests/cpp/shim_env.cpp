@@ -59,8 +59,16 @@ int main()
     }
     unsetenv("SIMILIE_PRECONDITIONER");
 
-    expect(refused("SIMILIE_SOLVER", "gmres"), "gmres refused");
-    expect(!refused("SIMILIE_SOLVER", "cg"), "cg accepted");
+    expect(!refused("SIMILIE_SOLVER", "gmres"), "gmres accepted");
+    setenv("SIMILIE_SOLVER", "gmres", 1);
+    setenv("SIMILIE_GMRES_KRYLOV_DIM", "30", 1);
+    expect(selected_solver().kind == SIL_KRYLOV_GMRES && selected_solver().dim == 30, "gmres and its dimension");
+    setenv("SIMILIE_SOLVER", "idr", 1);
+    expect(selected_solver().kind == SIL_KRYLOV_IDR && selected_solver().dim == 8, "idr with the default subspace");
+    setenv("SIMILIE_SOLVER", "something", 1);
+    expect(selected_solver().kind == SIL_KRYLOV_CG, "an unknown name is CG, as in the reference");
+    unsetenv("SIMILIE_SOLVER");
+    unsetenv("SIMILIE_GMRES_KRYLOV_DIM");
     expect(refused("SIMILIE_MAGNETIC_Y_RESPONSE_SIGN_3D", "-1"), "flipped y response refused");
     expect(!refused("SIMILIE_MAGNETIC_Y_RESPONSE_SIGN_3D", "1"), "y response +1 accepted");
     expect(refused("SIMILIE_NONLINEAR_LINE_SEARCH_STEPS", "4"), "other line search refused");

@@ -180,6 +180,7 @@ def test_assembled_path_arguments_checked_on_host():
     st = _native.SilSolveSettings()
     d = _native.SilSolveDiagnostics()
     assert L.sil_csr_solve(None, None, None, 256, 256, ctypes.byref(st), ctypes.byref(d)) == 1
+    assert L.sil_csr_krylov_solve(None, None, None, 3, 0, 256, 256, ctypes.byref(st), ctypes.byref(d)) == 1
     q = _native.SilMag2dNlProblem()
     q.nx, q.ny = 2, 8
     assert L.sil_mag2d_nl_assemble_jacobian(None, ctypes.byref(q), 256, ctypes.byref(h)) == 1

@@ -77,3 +77,16 @@ def test_checkpoint_round_trip_and_rejections(tmp_path):
         open(path, "wb").write(bad)
         with pytest.raises(ValueError):
             read_checkpoint(path)
+
+
+def test_checkpoint_with_optimizer_state(tmp_path):
+    from similie_b200.precond import read_checkpoint, write_checkpoint
+    rng = np.random.default_rng(4)
+    p, m, v = (rng.standard_normal(50).astype(np.float32) for _ in range(3))
+    path = str(tmp_path / "ck2.bin")
+    write_checkpoint(path, p, 12, 1, {"adam_steps": 12}, m=m, v=v)
+    p2, step, seed, extra, m2, v2 = read_checkpoint(path, with_optimizer=True)
+    np.testing.assert_array_equal(p2, p)
+    np.testing.assert_array_equal(m2, m)
+    np.testing.assert_array_equal(v2, v)
+    assert step == 12 and extra["adam_steps"] == 12
