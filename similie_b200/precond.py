@@ -141,12 +141,17 @@ _MAGIC = b"SILPCKPT"
 
 
 def write_checkpoint(path, params, step, seed, extra=None, m=None, v=None):
+    """Writes the checkpoint to `path` + '.tmp', flushes it to disk and then
+    renames it over `path`, so a crash or kill during the write leaves the
+    previous checkpoint intact."""
     import json
+    import os
     import struct
     p = np.ascontiguousarray(params, dtype=np.float32)
     blob = json.dumps(extra or {}, sort_keys=True).encode()
     version = 1 if m is None else 2
-    with open(path, "wb") as f:
+    tmp = str(path) + ".tmp"
+    with open(tmp, "wb") as f:
         f.write(_MAGIC)
         f.write(struct.pack("<IIQQQQ", version, 1, p.size, int(step), int(seed), len(blob)))
         f.write(blob)
@@ -154,6 +159,9 @@ def write_checkpoint(path, params, step, seed, extra=None, m=None, v=None):
         if m is not None:
             f.write(np.ascontiguousarray(m, dtype=np.float32).tobytes())
             f.write(np.ascontiguousarray(v, dtype=np.float32).tobytes())
+        f.flush()
+        os.fsync(f.fileno())
+    os.replace(tmp, path)
 
 
 def read_checkpoint(path, with_optimizer=False):

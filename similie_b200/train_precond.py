@@ -85,8 +85,26 @@ def train(net, pairs, steps, batch=8, lr=1e-3, seed=0, log_every=100, log=None, 
                             "seconds": round(time.perf_counter() - t0, 2)}))
         if checkpoint is not None and ((step + 1) % checkpoint_every == 0 or step == steps - 1):
             net.save_checkpoint(checkpoint, step + 1, seed, {"steps": steps, "batch": batch, "lr": lr})
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     return history, time.perf_counter() - t0
+
+
+def check_resume(path, seed, steps, batch, lr):
+    """Raises ValueError when the run's seed, step count, batch or learning
+    rate differ from those the checkpoint was written with: the pair set and
+    the batch draws follow the seed and the cosine schedule follows the step
+    count, so a resumed run continues the original one only with the same
+    settings."""
+    from .precond import read_checkpoint
+    _, step, ck_seed, extra = read_checkpoint(path)
+    want = {"seed": ck_seed, "steps": extra.get("steps"), "batch": extra.get("batch"), "lr": extra.get("lr")}
+    have = {"seed": seed, "steps": steps, "batch": batch, "lr": lr}
+    bad = {k: (want[k], have[k]) for k in want if want[k] is not None and want[k] != have[k]}
+    if bad:
+        raise ValueError("--resume: settings differ from the checkpoint's (checkpoint, run): "
+                         + ", ".join(f"{k} {a!r} vs {b!r}" for k, (a, b) in sorted(bad.items())))
+    return step
 
 
 def main():
@@ -102,8 +120,16 @@ def main():
                     help="draw min..3 permeability-1000 rectangles per problem instead of 0..3")
     ap.add_argument("--out", default="precond_2d.npy")
     ap.add_argument("--checkpoint", default=None, help="write a resumable checkpoint here while training")
-    ap.add_argument("--resume", default=None, help="continue from this checkpoint (parameters, step)")
+    ap.add_argument("--resume", default=None,
+                    help="continue from this checkpoint: parameters, step and (version-2 checkpoints) the Adam "
+                         "moments; a version-1 checkpoint restarts the Adam moments.  The seed, --steps, --batch "
+                         "and --lr must be the checkpoint's (the pair set, the batch draws and the schedule depend "
+                         "on them); a mismatch is an error.  Not combinable with --init")
     args = ap.parse_args()
+    if args.init and args.resume:
+        ap.error("--init and --resume are exclusive: a resumed run takes its parameters from the checkpoint")
+    if args.resume:
+        check_resume(args.resume, args.seed, args.steps, args.batch, args.lr)
     import torch
     torch.cuda.init()
     t0 = time.perf_counter()

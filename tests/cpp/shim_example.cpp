@@ -2,7 +2,7 @@
 // d of a 0-form, the staged Laplacian of that 0-form, and a 2D
 // magnetostatics solve through minimize_strong_formulation_residual.
 // Writes its outputs as raw little-endian doubles into the directory given
-// as the first argument; tests/test_gpu_cpp_shim.py checks them against the
+// as the first argument; tests/test_cpp_shim.py checks them against the
 // oracle.
 #include <cuda_runtime.h>
 

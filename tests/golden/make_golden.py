@@ -16,7 +16,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SIMILIE_REF", "/root/reference")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SIMILIE_REF")
+if not REF:
+    sys.exit("usage: make_golden.py <path of a SimiLie checkout>  (or set SIMILIE_REF)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 DIM_TAGS = {"DDimT": "T", "DDimX": "X", "DDimY": "Y", "DDimZ": "Z"}
