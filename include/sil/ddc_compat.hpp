@@ -12,8 +12,12 @@
 //   tensor_prod(out, in, hodge) on the stored star        hodge_star_stored<KIn>(exec, out, in, hodge)
 //   make_staged_codifferential(...).run(out, in),         codifferential<K>(exec, geometry, out, in)
 //   codifferential(...)  exterior/codifferential.hpp:439-656
+//   make_staged_codifferential(exec, tensor, metric,      make_staged_codifferential<K>(exec, in, &metric,
+//     position).run(out, in)  codifferential.hpp:510-540     position).run(exec, out, in)
 //   make_staged_laplacian(exec, out, in, metric,          make_staged_laplacian<K>(exec, geometry, out, in)
-//     position).run(out, in)  exterior/laplacian.hpp:327-358   .run(out, in)
+//     position).run(out, in)  exterior/laplacian.hpp:327-358   .run(out, in)  (rectilinear, identity metric)
+//                                                         make_staged_laplacian<K>(exec, out, in, &metric,
+//                                                           position).run(exec, out, in)  (general metric)
 //   laplacian(...)  exterior/laplacian.hpp:814-951        laplacian<K>(exec, geometry, out, in)
 //   solvers::minimize_strong_formulation_residual(        minimize_strong_formulation_residual(
 //     exec, operator_model, rhs, solution, settings)        exec, operator_model, rhs, solution, settings)
@@ -220,6 +224,79 @@ StagedLaplacian<K> make_staged_laplacian(ExecSpace, Geometry const& geometry, Te
                                          bool fused = true, uint32_t form_mask = 0)
 {
     return StagedLaplacian<K>(geometry, out, in, fused, form_mask);
+}
+
+// The general-metric staged operators: built from the (metric, position)
+// tensor pair as in the reference (metric == nullptr: identity), they store
+// the per-node Hodge tensors fill_discrete_hodge_star computes and run one
+// fused kernel per call.  FP64, fields over exactly the position's n dims.
+template <int K>
+class MetricStagedLaplacian
+{
+public:
+    MetricStagedLaplacian(ExecSpace exec, Tensor out_like, Tensor in_like, Tensor const* metric, Tensor position)
+    {
+        check(sil_laplacian_plan_create_metric(&plan_, exec.stream, position.field.ndims, K, &position.field,
+                                               metric != nullptr ? &metric->field : nullptr, &in_like.field,
+                                               &out_like.field),
+              "make_staged_laplacian");
+    }
+    MetricStagedLaplacian(MetricStagedLaplacian&& o) noexcept : plan_(std::exchange(o.plan_, nullptr)) {}
+    MetricStagedLaplacian(MetricStagedLaplacian const&) = delete;
+    ~MetricStagedLaplacian()
+    {
+        if (plan_ != nullptr) sil_laplacian_plan_destroy(plan_);
+    }
+    Tensor run(ExecSpace exec, Tensor out, Tensor in) const
+    {
+        check(sil_laplacian_run(plan_, exec.stream, &in.field, &out.field), "StagedLaplacian::run");
+        return out;
+    }
+
+private:
+    sil_laplacian_plan plan_ = nullptr;
+};
+
+template <int K>
+MetricStagedLaplacian<K> make_staged_laplacian(ExecSpace exec, Tensor out, Tensor in, Tensor const* metric,
+                                               Tensor position)
+{
+    return MetricStagedLaplacian<K>(exec, out, in, metric, position);
+}
+
+template <int K>
+class MetricStagedCodifferential
+{
+public:
+    MetricStagedCodifferential(ExecSpace exec, Tensor const* metric, Tensor position)
+    {
+        check(sil_codifferential_plan_create(&plan_, exec.stream, position.field.ndims, K, &position.field,
+                                             metric != nullptr ? &metric->field : nullptr),
+              "make_staged_codifferential");
+    }
+    MetricStagedCodifferential(MetricStagedCodifferential&& o) noexcept : plan_(std::exchange(o.plan_, nullptr)) {}
+    MetricStagedCodifferential(MetricStagedCodifferential const&) = delete;
+    ~MetricStagedCodifferential()
+    {
+        if (plan_ != nullptr) sil_codifferential_plan_destroy(plan_);
+    }
+    Tensor run(ExecSpace exec, Tensor out, Tensor in) const
+    {
+        check(sil_codifferential_run(plan_, exec.stream, &in.field, &out.field), "StagedCodifferential::run");
+        return out;
+    }
+
+private:
+    sil_codifferential_plan plan_ = nullptr;
+};
+
+// `tensor` is the input the reference sizes its dual buffer from; the fused
+// kernel needs no buffer, so only its rank (K) matters here.
+template <int K>
+MetricStagedCodifferential<K> make_staged_codifferential(ExecSpace exec, Tensor /*tensor*/, Tensor const* metric,
+                                                         Tensor position)
+{
+    return MetricStagedCodifferential<K>(exec, metric, position);
 }
 
 // ------------------------------------------------------------------ solvers

@@ -134,6 +134,25 @@ sil_status sil_hodge_star_stored(sil_stream stream, int n, int k_in, const sil_f
 sil_status sil_codifferential(sil_geometry geometry, sil_stream stream, uint32_t form_mask, int k,
                               const sil_field* in, sil_field* out);
 
+/* Staged codifferential of a k-form (1 <= k <= n <= 3) built from a
+ * (metric, position) pair: position (n components per node) and metric (n*n
+ * per node, row-major; NULL for the identity) FP64 fields spanning exactly
+ * the n form dims, the metric lattice covering the position lattice.
+ * create fills the two Hodge tensors the reference stores (k-form star and
+ * (n-k+1)-form star, sil_fill_discrete_hodge_star_metric) over the position
+ * lattice and owns them (enqueued on `stream`); run is one fused kernel per
+ * call over every node of `out`, FP64, in and out lattices inside the
+ * position lattice, no spectator dims.
+ * Replaces: make_staged_codifferential(exec, tensor, metric, position) /
+ *   StagedCodifferential ctor and run,
+ *   src/similie/exterior/codifferential.hpp:398-437, 439-507, 510-540. */
+typedef struct sil_codifferential_plan_s* sil_codifferential_plan;
+sil_status sil_codifferential_plan_create(sil_codifferential_plan* plan, sil_stream stream, int n, int k,
+                                          const sil_field* position, const sil_field* metric);
+sil_status sil_codifferential_run(sil_codifferential_plan plan, sil_stream stream, const sil_field* in,
+                                  sil_field* out);
+sil_status sil_codifferential_plan_destroy(sil_codifferential_plan plan);
+
 /* ---------------------------------------------------------------------- */
 /* Hodge Laplacian (delta d for k = 0, delta d + d delta for 0 < k < n,     */
 /* d delta for k = n).                                                      */
@@ -152,6 +171,19 @@ typedef struct sil_laplacian_plan_s* sil_laplacian_plan;
 sil_status sil_laplacian_plan_create(sil_laplacian_plan* plan, sil_geometry geometry,
                                      uint32_t form_mask, int k, const sil_field* in_like,
                                      const sil_field* out_like, int mode);
+/* Staged Laplacian of a k-form (0 <= k <= n <= 3) built from a (metric,
+ * position) pair (same fields as sil_codifferential_plan_create): create
+ * fills the up to four Hodge tensors the reference stores ((k+1)-, (n-k)-,
+ * k- and (n-k+1)-form stars) over the position lattice, enqueued on
+ * `stream`; sil_laplacian_run then evaluates delta d + d delta in one fused
+ * kernel reading the stored tensors (plan kernel 4).  FP64, in_like and
+ * out_like over exactly the n form dims, inside the position lattice.
+ * Replaces: make_staged_laplacian(exec, laplacian_tensor, tensor, metric, position),
+ *   src/similie/exterior/laplacian.hpp:261-310 (rank 0), 508-597 (intermediate
+ *   ranks), 740-789 (top rank), 327-358. */
+sil_status sil_laplacian_plan_create_metric(sil_laplacian_plan* plan, sil_stream stream, int n, int k,
+                                            const sil_field* position, const sil_field* metric,
+                                            const sil_field* in_like, const sil_field* out_like);
 /* Replaces: StagedLaplacian::run, laplacian.hpp:312-324, 599-647, 791-811. */
 sil_status sil_laplacian_run(sil_laplacian_plan plan, sil_stream stream, const sil_field* in,
                              sil_field* out);
@@ -159,7 +191,8 @@ sil_status sil_laplacian_plan_destroy(sil_laplacian_plan plan);
 /* Device bytes of scratch the plan owns (0 for the fused mode). */
 size_t sil_laplacian_plan_scratch_bytes(sil_laplacian_plan plan);
 /* Kernel the plan runs: 0 table-driven fused (any rank / layout), 1 fused 2D
- * 0-form, 2 fused 2D 1-form with TMA-staged tiles, 3 unfused reference chain. */
+ * 0-form, 2 fused 2D 1-form with TMA-staged tiles, 3 unfused reference chain,
+ * 4 fused over stored general-metric Hodge tensors. */
 int sil_laplacian_plan_kernel(sil_laplacian_plan plan);
 /* Pipeline shape of kernel 2 chosen by the autotuner on the plan's first
  * run (-1 before it).  The first run times each shape on the caller's fields

@@ -27,7 +27,7 @@ from . import _native
 from ._native import SilError, check, lib
 
 __all__ = [
-    "Geometry", "deriv", "coboundary", "transposed_coboundary", "hodge_star", "fill_discrete_hodge_star",
+    "Geometry", "MetricGeometry", "deriv", "coboundary", "transposed_coboundary", "hodge_star", "fill_discrete_hodge_star",
     "codifferential", "make_staged_codifferential", "laplacian", "make_staged_laplacian", "StagedLaplacian",
     "SilError", "field_struct",
 ]
@@ -221,7 +221,58 @@ class StagedCodifferential:
 
 
 def make_staged_codifferential(geometry, k, form_dims=None, comp_axis=-1):
+    """Staged codifferential of a k-form: over a Geometry (rectilinear grid,
+    identity metric; the Hodge factors come from the coordinates inside the
+    kernel) or a MetricGeometry (the stored general-metric stars are filled
+    once here)."""
+    if isinstance(geometry, MetricGeometry):
+        return MetricStagedCodifferential(geometry, k)
     return StagedCodifferential(geometry, k, form_dims, comp_axis)
+
+
+class MetricGeometry:
+    """The (position, metric) tensor-field pair of SimiLie's staged operators
+    in the general case: position (*lattice, n) and metric (*lattice, n*n,
+    row-major; None for the identity) as FP64 CUDA tensors over the n <= 3
+    form dims, with optional lattice fronts.  Operators built on it store the
+    per-node Hodge tensors fill_discrete_hodge_star computes from them."""
+
+    def __init__(self, position, metric=None, position_front=None, metric_front=None):
+        self.position = position.contiguous()
+        self.metric = metric.contiguous() if metric is not None else None
+        self.n = self.position.shape[-1]
+        self._fp = field_struct(self.position, -1, position_front)
+        self._fm = field_struct(self.metric, -1, metric_front) if self.metric is not None else None
+
+    def fields(self):
+        return ctypes.byref(self._fp), (ctypes.byref(self._fm) if self._fm is not None else None)
+
+
+class MetricStagedCodifferential:
+    """make_staged_codifferential(exec, tensor, metric, position): the k-form
+    and (n-k+1)-form Hodge tensors are filled at construction over the
+    position lattice; run(out, inp) is one fused kernel (FP64, fields over
+    exactly the n form dims, inside the position lattice)."""
+
+    def __init__(self, geometry, k, stream=None):
+        self.geometry, self.k = geometry, k
+        self._p = ctypes.c_void_p()
+        fp, fm = geometry.fields()
+        check(lib().sil_codifferential_plan_create(ctypes.byref(self._p), _stream(stream), geometry.n, k, fp, fm),
+              "make_staged_codifferential")
+
+    def run(self, out, inp, in_front=None, out_front=None, stream=None):
+        fi = field_struct(inp, -1, in_front)
+        fo = field_struct(out, -1, out_front)
+        check(lib().sil_codifferential_run(self._p, _stream(stream), ctypes.byref(fi), ctypes.byref(fo)),
+              "codifferential")
+        return out
+
+    def __del__(self):
+        p = getattr(self, "_p", None)
+        if p is not None and p.value is not None and _native._lib is not None:
+            _native._lib.sil_codifferential_plan_destroy(p)
+            self._p = None
 
 
 class StagedLaplacian:
@@ -239,6 +290,14 @@ class StagedLaplacian:
         self.mask = _mask(form_dims, fi.ndims)
         self._p = ctypes.c_void_p()
         m = {"fused": 0, "unfused": 1}[mode]
+        if isinstance(geometry, MetricGeometry):
+            # stored general-metric Hodge tensors, filled here (fused only)
+            if mode != "fused" or comp_axis % inp_like.dim() != inp_like.dim() - 1:
+                raise ValueError("a MetricGeometry Laplacian is fused, component-last")
+            fp, fm = geometry.fields()
+            check(lib().sil_laplacian_plan_create_metric(ctypes.byref(self._p), _stream(None), geometry.n, k, fp, fm,
+                                                         ctypes.byref(fi), ctypes.byref(fo)), "make_staged_laplacian")
+            return
         check(lib().sil_laplacian_plan_create(ctypes.byref(self._p), geometry.handle, self.mask, k, ctypes.byref(fi),
                                               ctypes.byref(fo), m), "make_staged_laplacian")
 

@@ -169,6 +169,11 @@ SIGNATURES = [
     ("sil_codifferential", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_int, _F, _F]),
     ("sil_laplacian_plan_create", ctypes.c_int, [ctypes.POINTER(_P), _P, ctypes.c_uint32, ctypes.c_int, _F, _F,
                                                  ctypes.c_int]),
+    ("sil_laplacian_plan_create_metric", ctypes.c_int, [ctypes.POINTER(_P), _P, ctypes.c_int, ctypes.c_int, _F, _F,
+                                                        _F, _F]),
+    ("sil_codifferential_plan_create", ctypes.c_int, [ctypes.POINTER(_P), _P, ctypes.c_int, ctypes.c_int, _F, _F]),
+    ("sil_codifferential_run", ctypes.c_int, [_P, _P, _F, _F]),
+    ("sil_codifferential_plan_destroy", ctypes.c_int, [_P]),
     ("sil_laplacian_run", ctypes.c_int, [_P, _P, _F, _F]),
     ("sil_laplacian_plan_destroy", ctypes.c_int, [_P]),
     ("sil_laplacian_plan_scratch_bytes", ctypes.c_size_t, [_P]),

@@ -110,6 +110,8 @@ struct sil_laplacian_plan_s
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
     sil_field dual_a {}, dual_b {}, codiff {}, cob {};
+    StoredHodges hodges {};       // kernel 4: stored general-metric stars
+    void* hodge_mem = nullptr;
 };
 
 namespace {
@@ -292,6 +294,44 @@ sil_status sil_laplacian_plan_create(sil_laplacian_plan* plan, sil_geometry geom
     return SIL_OK;
 }
 
+sil_status sil_laplacian_plan_create_metric(sil_laplacian_plan* plan, sil_stream stream, int n, int k,
+                                            const sil_field* position, const sil_field* metric,
+                                            const sil_field* in_like, const sil_field* out_like)
+{
+    if (plan == nullptr) return fail(SIL_ERR_INVALID, "sil_laplacian_plan_create_metric: NULL plan");
+    *plan = nullptr;
+    sil_status st = check_stored_laplacian(n, k, position, metric);
+    if (st == SIL_OK) st = check_field(in_like, "in_like", static_cast<int>(binom(n, k)));
+    if (st == SIL_OK) st = check_field(out_like, "out_like", static_cast<int>(binom(n, k)));
+    if (st != SIL_OK) return st;
+    if (in_like->dtype != SIL_F64 || out_like->dtype != SIL_F64)
+        return fail(SIL_ERR_UNSUPPORTED, "sil_laplacian_plan_create_metric: FP64 fields only");
+    if (in_like->ndims != n || out_like->ndims != n)
+        return fail(SIL_ERR_INVALID, "sil_laplacian_plan_create_metric: fields must span exactly the n form dims");
+    auto* p = new (std::nothrow) sil_laplacian_plan_s();
+    if (p == nullptr) return fail(SIL_ERR_ALLOC, "sil_laplacian_plan_create_metric: host allocation");
+    p->mask = (1u << n) - 1;
+    p->n = n;
+    p->k = k;
+    p->mode = SIL_LAPLACIAN_FUSED;
+    p->kernel = 4;
+    p->in_like = *in_like;
+    p->out_like = *out_like;
+    cudaError_t err = cudaMalloc(&p->error_flag, sizeof(int));
+    if (err == cudaSuccess) err = cudaMemset(p->error_flag, 0, sizeof(int));
+    if (err != cudaSuccess) {
+        sil_laplacian_plan_destroy(p);
+        return cuda_fail(err, "sil_laplacian_plan_create_metric");
+    }
+    st = fill_stored_hodges(as_stream(stream), n, k, *position, metric, true, &p->hodge_mem, &p->hodges);
+    if (st != SIL_OK) {
+        sil_laplacian_plan_destroy(p);
+        return st;
+    }
+    *plan = p;
+    return SIL_OK;
+}
+
 sil_status sil_laplacian_run(sil_laplacian_plan plan, sil_stream stream, const sil_field* in, sil_field* out)
 {
     if (plan == nullptr) return fail(SIL_ERR_INVALID, "sil_laplacian_run: NULL plan");
@@ -323,6 +363,7 @@ sil_status sil_laplacian_run(sil_laplacian_plan plan, sil_stream stream, const s
         return launch_lap2d_1form_tma(s, *plan->geo, *in, *out, plan->error_flag, plan->variant);
     }
     case 3: return run_unfused(*plan, s, *in, *out);
+    case 4: return launch_stored_laplacian(s, plan->hodges, in, out);
     default: return launch_fused_laplacian(s, *plan->geo, plan->mask, plan->k, *in, *out);
     }
 }
@@ -332,6 +373,7 @@ sil_status sil_laplacian_plan_destroy(sil_laplacian_plan plan)
     if (plan == nullptr) return SIL_OK;
     cudaFree(plan->error_flag);
     cudaFree(plan->scratch);
+    cudaFree(plan->hodge_mem);
     delete plan;
     return SIL_OK;
 }

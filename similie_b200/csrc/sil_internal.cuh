@@ -150,6 +150,27 @@ GeoView<T> geo_view(Geometry const& g);
 sil_status divergence_gauge_table(int64_t nx, int64_t ny, int64_t nz, double const* const coords[3],
                                   double const* ls, double* gd, double* probe, double* out, cudaStream_t st);
 
+// Stored Hodge tensors of a staged operator built from a (metric, position)
+// pair, over the position lattice: h[0] the (k+1)-form star, h[1] the
+// (n-k)-form star, h[2] the k-form star, h[3] the (n-k+1)-form star, with
+// kin[w] their source ranks; data == nullptr where the operator needs none.
+// Defined in staged_metric.cu.
+struct StoredHodges
+{
+    int n = 0;
+    int k = 0;
+    int kin[4] = {0, 0, 0, 0};
+    sil_field lattice {};
+    sil_field h[4] {};
+};
+
+// Fills the tensors a Laplacian (laplacian = true: all four that its rank
+// needs) or a codifferential (h[2], h[3]) stores; *mem owns them (cudaFree).
+sil_status fill_stored_hodges(cudaStream_t stream, int n, int k, sil_field const& position, sil_field const* metric,
+                              bool laplacian, void** mem, StoredHodges* out);
+sil_status check_stored_laplacian(int n, int k, sil_field const* position, sil_field const* metric);
+sil_status launch_stored_laplacian(cudaStream_t s, StoredHodges const& H, sil_field const* in, sil_field const* out);
+
 } // namespace sil
 
 struct sil_geometry_s

@@ -112,6 +112,44 @@ int main(int argc, char** argv)
         write(dir + "/sol_ssor.bin", to_host(d_sol2, n * n));
         std::printf("assembled %u %d %.6e %lld\n", diag2.iterations, diag2.converged ? 1 : 0,
                     diag2.final_relative_residual, static_cast<long long>(matrix.nonzeros()));
+
+        // the general-metric staged Laplacian of a 1-form on a sheared 10 x 8
+        // lattice with a dense metric per node (make_staged_laplacian(exec,
+        // out, in, metric, position)), and its codifferential
+        int const mx = 10, my = 8;
+        std::vector<double> pos(mx * my * 2), met(mx * my * 4), w1(mx * my * 2);
+        for (int i = 0; i < mx; ++i)
+            for (int j = 0; j < my; ++j) {
+                int const node = i * my + j;
+                pos[2 * node] = 0.2 * i + 0.05 * j;
+                pos[2 * node + 1] = 0.25 * j + 0.01 * i * i;
+                double const a = 0.3 * std::sin(0.7 * i + 0.3 * j), b = 0.2 * std::cos(0.4 * i - 0.5 * j);
+                met[4 * node] = 1.0 + a * a;
+                met[4 * node + 1] = met[4 * node + 2] = a * b;
+                met[4 * node + 3] = 1.2 + b * b;
+                w1[2 * node] = std::sin(0.5 * i) * std::cos(0.3 * j);
+                w1[2 * node + 1] = std::cos(0.2 * i + 0.4 * j);
+            }
+        double* d_pos = to_device(pos);
+        double* d_met = to_device(met);
+        double* d_w1 = to_device(w1);
+        double* d_lap1 = to_device(std::vector<double>((mx - 1) * (my - 1) * 2, 0.0));
+        double* d_cod = to_device(std::vector<double>(mx * my, 0.0));
+        Tensor const position = Tensor::make(d_pos, SIL_F64, {mx, my}, 2);
+        Tensor const metric = Tensor::make(d_met, SIL_F64, {mx, my}, 4);
+        Tensor const w1in = Tensor::make(d_w1, SIL_F64, {mx, my}, 2);
+        Tensor const lap1 = Tensor::make(d_lap1, SIL_F64, {mx - 1, my - 1}, 2);
+        Tensor const cod = Tensor::make(d_cod, SIL_F64, {mx, my}, 1);
+        auto const staged1 = make_staged_laplacian<1>(exec, lap1, w1in, &metric, position);
+        staged1.run(exec, lap1, w1in);
+        make_staged_codifferential<1>(exec, w1in, &metric, position).run(exec, cod, w1in);
+        cudaDeviceSynchronize();
+        write(dir + "/pos.bin", pos);
+        write(dir + "/met.bin", met);
+        write(dir + "/w1.bin", w1);
+        write(dir + "/lap1.bin", to_host(d_lap1, (mx - 1) * (my - 1) * 2));
+        write(dir + "/cod.bin", to_host(d_cod, mx * my));
+        std::printf("metric ok\n");
     } catch (Error const& e) {
         std::fprintf(stderr, "%s\n", e.what());
         return 1;

@@ -1,6 +1,7 @@
 """The C++ shim include/sil/ddc_compat.hpp: it and a reference-style call
 site (tests/cpp/shim_example.cpp) compile; on a GPU the call site's outputs
-match the oracle (d bit-exact, Laplacian 1e-12, solve to 1e-10)."""
+match the oracle (d bit-exact, Laplacian 1e-12, solve to 1e-10, the
+general-metric staged Laplacian and codifferential 1e-12)."""
 import os
 import shutil
 import subprocess
@@ -71,6 +72,16 @@ def test_example_matches_the_oracle(tmp_path):
     assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(rd("rhs.bin"))
     r2 = rd("rhs.bin") - O.mag2d_apply(n, n, rd("mu.bin"), rd("sol_ssor.bin"))
     assert np.linalg.norm(r2) <= 2e-10 * np.linalg.norm(rd("rhs.bin"))
+    # general-metric staged Laplacian and codifferential through the shim
+    assert out[3] == "metric ok"
+    mx, my = 10, 8
+    pos, met, w1 = rd("pos.bin").reshape(mx, my, 2), rd("met.bin").reshape(mx, my, 4), rd("w1.bin").reshape(mx, my, 2)
+    lap1 = O.laplacian(2, 1, pos, w1, metric=met)
+    got = rd("lap1.bin").reshape(mx - 1, my - 1, 2)
+    assert np.max(np.abs(got - lap1)) <= 1e-12 * np.max(np.abs(lap1))
+    cod = O.codifferential(2, 1, pos, w1, metric=met)
+    got = rd("cod.bin").reshape(mx, my, 1)
+    assert np.max(np.abs(got - cod)) <= 1e-12 * np.max(np.abs(cod))
 
 
 def rd_mu(tmp_path):
