@@ -13,7 +13,14 @@ reported time is the maximum over ranks.
                   [--workload laplacian|solve|mag3d]
 
 --impl reference times the reference algorithm's CPU path (the oracle's
-C++/OpenMP restatement, reference-structured staged chain) on the host cores.
+C++/OpenMP restatement, reference-structured staged chain) on the host cores,
+on the same 4096^2 field.
+
+On one GPU the default line also carries two records beside the headline
+(--no-solve leaves them out): "config1", the 512^2 scalar Laplacian timed warm
+and L2-flushed cold with its oracle parity, and "solve", the 64-problem
+batched 2D magnetostatics time-to-1e-10 of the plain FP64, FP32-inner and
+learned solvers with every solution checked by the oracle's FP64 operator.
 
 Secondary workloads (one JSON line each, not the headline):
   --workload solve   batched 2D magnetostatics: 64 problems of {128..1024}^2
@@ -140,41 +147,48 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_baseline(steps=1, sample_n=1024, seed=2):
-    """Oracle staged chain (stored Hodge tensors, separate passes, FP64) on a
-    sample_n^2 sample of the workload; setup (Hodge fill) excluded."""
+def cpu_baseline(steps=1, warmup=1, sample_n=N_NODES, seed=2):
+    """Oracle staged chain (stored Hodge tensors, separate passes, FP64) on the
+    workload's own sample_n^2 field (the full 4096^2 field by default, the same
+    input the GPU arm reads); the staged set-up (Hodge fill) is excluded, as
+    the reference's staged constructor is, and `warmup` untimed runs come
+    first."""
     import oracle as O
     from tests.helpers import gaussian_random_field
     w = gaussian_random_field(sample_n, seed=seed)
     coords = [np.arange(sample_n) / N_NODES, np.arange(sample_n) / N_NODES]
     pos = O.position_from_coords(coords)
+    t0 = time.perf_counter()
     st = O.StagedLaplacian(2, 1, pos)
+    setup_s = time.perf_counter() - t0
     out = np.zeros((sample_n - 1, sample_n - 1, 2))
-    st.run(w, out)  # warm-up
+    for _ in range(max(warmup, 0)):
+        st.run(w, out)
     times = []
-    for _ in range(steps):
+    for _ in range(max(steps, 1)):
         t0 = time.perf_counter()
         st.run(w, out)
         times.append(time.perf_counter() - t0)
     t = statistics.median(times)
     gbs = algorithmic_bytes(sample_n) / t / 1e9
+    what = "the full 4096^2 1-form" if sample_n == N_NODES else f"a {sample_n}x{sample_n} sample of the 4096^2 1-form"
     return {"value": gbs, "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
-            "sample": f"{sample_n}x{sample_n} sample of the 4096^2 1-form, reference-structured staged chain "
-                      f"(d+star, transposed d+star, star, transposed d+star, d, add), Hodge fill excluded",
-            "cell_updates_per_s": cell_updates(sample_n) / t, "seconds_per_sample": t}
+            "sample": f"{what}, reference-structured staged chain (d+star, transposed d+star, star, "
+                      f"transposed d+star, d, add), Hodge fill excluded ({setup_s:.1f} s), "
+                      f"median of {len(times)} runs after {max(warmup, 0)} warm-up",
+            "cell_updates_per_s": cell_updates(sample_n) / t, "seconds_per_sample": t,
+            "seconds_per_step": times, "same_config": sample_n == N_NODES}
 
 
 def run_reference(args):
+    """The reference algorithm's CPU path (the oracle's staged chain on all
+    host threads) on the same 4096^2 FP64 field as the GPU arm: W untimed
+    warm-up applies, then K timed applies; rank 0 only."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import oracle as O
     os.environ.setdefault("OMP_PROC_BIND", "close")
-    sample_n = 1024
-    cb = None
-    for _ in range(max(args.warmup, 0)):
-        pass
-    cb = cpu_baseline(steps=max(args.steps, 1), sample_n=sample_n)
+    cb = cpu_baseline(steps=max(args.steps, 1), warmup=args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["seconds_per_sample"] * 1e3,
@@ -194,6 +208,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-solve", action="store_true",
+                    help="leave the configuration-1 and configuration-3 records out of the default line")
     ap.add_argument("--extras", action="store_true", help="also time the unfused chain, FP32 and the 512^2 0-form")
     ap.add_argument("--workload", default="laplacian",
                     choices=["laplacian", "solve", "mag3d", "precond", "hodge3d", "nonlinear", "nonlinear3d",
@@ -287,23 +303,32 @@ def main():
     torch.cuda.synchronize()
     plan.status()
 
-    # Device-timed region: CUDA events on the launching stream around every launch.
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # Device-timed region: the K launches run back to back from one CUDA
+    # graph (captured after the warm-up, replayed once untimed), bracketed by
+    # CUDA events on the launching stream, so neither the host's launch rate
+    # nor per-launch events pace the kernels.
+    side = torch.cuda.Stream()
+    side.wait_stream(stream)
+    with torch.cuda.stream(side):
+        plan.run(out, inp)
+    stream.wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for _ in range(args.steps):
+            plan.run(out, inp)
+    graph.replay()
+    torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     with clocks:
         t_start.record(stream)
-        for s in range(args.steps):
-            evs[s][0].record(stream)
-            plan.run(out, inp)
-            evs[s][1].record(stream)
+        graph.replay()
         t_end.record(stream)
         torch.cuda.synchronize()
     barrier()
     total_ms = t_start.elapsed_time(t_end)
-    per_launch_ms = [a.elapsed_time(b) for a, b in evs]
     plan.status()
     if pg is not None:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
@@ -312,7 +337,7 @@ def main():
     ms_per_step = total_ms / args.steps
     bytes_per_step = algorithmic_bytes(n)
     value = world * bytes_per_step * args.steps / (total_ms * 1e-3) / 1e9
-    avg_launch_ms = statistics.mean(per_launch_ms)
+    avg_launch_ms = total_ms / args.steps  # launches back to back: the kernel's steady-state duration
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_step / (avg_launch_ms * 1e-3) / 1e9
     traffic = ncu_traffic("lap2d_1form_tma_4096_fp64.md")
@@ -384,11 +409,17 @@ def main():
     extras = {}
     if args.extras and rank == 0:
         extras = run_extras(torch, sil, geo, inp, out, args)
+    # configurations 1 and 3 beside the headline (one GPU: the batch would
+    # otherwise shard across ranks, as --workload solve does)
+    secondary = {}
+    if rank == 0 and world == 1 and not args.no_solve:
+        secondary["config1"] = config1_record(torch, sil)
+        secondary["solve"] = solve_record(torch)
 
     if rank == 0:
         cb = None
         if not args.no_cpu_baseline and world == 1:
-            cb = cpu_baseline(steps=1)
+            cb = cpu_baseline(steps=2, warmup=1)
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -400,7 +431,10 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
                          "traffic": traffic, "algorithmic_bytes_per_launch": bytes_per_step,
-                         "avg_launch_ms": avg_launch_ms},
+                         "avg_launch_ms": avg_launch_ms,
+                         "timing": f"{args.steps} launches back to back from one CUDA graph, CUDA events around the replay",
+                         "traffic_source": "profiles/lap2d_1form_tma_4096_fp64.md (steady state: mean over 4 "
+                                           "back-to-back launches without cache flushes)"},
             "cpu_baseline": cb,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": int(n * n * 2 * 8),
                     "d2h_bytes_per_step": int((n - 1) * (n - 1) * 2 * 8), "steps": e2e_steps,
@@ -409,6 +443,7 @@ def main():
             "gpu_launches": args.steps,
             "clocks": dict(clocks.summary() or {}, window="1 s preheat on the same kernel + warm-up + timed region"),
         }
+        line.update(secondary)
         if extras:
             line["extras"] = extras
         print(json.dumps(line))
@@ -458,13 +493,196 @@ def run_extras(torch, sil, geo, inp, out, args):
     return res
 
 
+def load_network():
+    """The shipped trained network (similie_b200/data/precond_2d.npy), or None."""
+    from similie_b200.precond import LearnedPreconditioner
+    weights = os.path.join(ROOT, "similie_b200", "data", "precond_2d.npy")
+    if not os.path.exists(weights):
+        return None, weights
+    net = LearnedPreconditioner(seed=0)
+    net.load(weights)
+    return net, weights
+
+
+def oracle_residuals(probs, sols):
+    """FP64 true relative residual ||b - A x|| / ||b|| of every solution, by the oracle's operator."""
+    import oracle as O
+    out = []
+    for p, x in zip(probs, sols):
+        b = p.rhs()
+        r = b - O.mag2d_apply(p.nx, p.ny, p.node_mu(), x.cpu().numpy())
+        out.append(float(np.linalg.norm(r) / np.linalg.norm(b)))
+    return out
+
+
+def time_solver_kinds(torch, probs, kinds, net, weights=None, chunk=64, concurrent=1, max_iterations=200000):
+    """Time each solver kind on the batch (device-resident inputs, a fresh
+    zero initial guess per kind) and check every problem's solution with the
+    oracle's FP64 operator."""
+    import similie_b200.magnetostatics as mag
+    from similie_b200 import dist as sd
+    from similie_b200.precond import LearnedPreconditioner
+    shapes = [(p.nx, p.ny) for p in probs]
+    mus = [torch.from_numpy(p.node_mu()).cuda() for p in probs]
+    rhss = [torch.from_numpy(p.rhs()).cuda() for p in probs]
+    results = {}
+    for kind in kinds:
+        sols = [torch.zeros_like(r) for r in rhss]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        chunk = min(chunk, 64)  # the learned solver takes 64 problems per call
+        slices = [slice(c0, c0 + chunk) for c0 in range(0, len(probs), chunk)]
+        per_chunk = [None] * len(slices)
+
+        def run(mine, stream, pnet):
+            for ci in mine:
+                sl = slices[ci]
+                per_chunk[ci] = mag.solve_batch(
+                    mus[sl], rhss[sl], sols[sl], shapes[sl], solver=kind, tol=1e-10,
+                    max_iterations=max_iterations, inner_iterations=min(4000, max_iterations),
+                    preconditioner=pnet if kind == "learned" else None,
+                    stream=None if stream is None else stream.cuda_stream)
+
+        workers = max(1, min(concurrent, len(slices)))
+        if workers == 1:
+            run(range(len(slices)), None, net)
+        else:
+            # solver calls in flight together on their own streams, so one
+            # call's straggling problems overlap the others' work
+            nets = [net] + [LearnedPreconditioner(seed=0) for _ in range(workers - 1)]
+            if kind == "learned":
+                for extra in nets[1:]:
+                    extra.load(weights)
+            streams = [torch.cuda.Stream() for _ in range(workers)]
+            torch.cuda.synchronize()
+            threads = [threading.Thread(target=run, args=(range(w, len(slices), workers), streams[w], nets[w]))
+                       for w in range(workers)]
+            for th in threads:
+                th.start()
+            for th in threads:
+                th.join()
+        d = [x for part in per_chunk for x in part]
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        rels = oracle_residuals(probs, sols)
+        # concurrent calls run on their own streams: time them by the host
+        # clock between device-wide synchronisations
+        sec = sd.max_over_ranks(e0.elapsed_time(e1) / 1e3 if workers == 1 else wall, device="cuda")
+        results[kind] = {"seconds": sec, "wall_seconds": wall, "solves_per_s": len(probs) / sec,
+                         "converged": sum(x.converged for x in d),
+                         "converged_by_oracle": sum(r <= 1e-10 for r in rels),
+                         "max_iterations": max(x.iterations for x in d),
+                         "median_iterations": float(np.median([x.iterations for x in d])),
+                         "total_iterations": int(sum(x.iterations for x in d)),
+                         "fallbacks": sum(x.fallback for x in d),
+                         "median_learned_iterations": float(np.median([x.learned_iterations for x in d])),
+                         "max_rel_residual_gpu": max(x.final_relative_residual for x in d),
+                         "max_rel_residual_oracle": max(rels), "problems_checked_by_oracle": len(rels)}
+    return results
+
+
+def solve_record(torch, kinds=("cg", "mixed", "learned"), seed=7, count=64):
+    """Configuration 3 inside the default line: the 64-problem batch of
+    {128..1024}^2 grids (seed 7) solved to a 1e-10 relative residual by the
+    plain FP64 solver, FP32-inner / FP64-refinement and the learned
+    preconditioner, every solution checked by the oracle's FP64 operator."""
+    import similie_b200.magnetostatics as mag
+    t0 = time.perf_counter()
+    probs = mag.synthetic_batch(seed=seed, count=count)
+    net, weights = load_network()
+    kinds = [k for k in kinds if k != "learned" or net is not None]
+    setup = time.perf_counter() - t0
+    res = time_solver_kinds(torch, probs, kinds, net, weights)
+    base = res["cg"]["seconds"] if "cg" in res else None
+    return {"metric": "time-to-1e-10 relative residual (FP64, checked by the oracle's operator), batch of "
+                      f"{count} 2D magnetostatics problems",
+            "workload": f"{count} problems, sizes uniform over {{128,256,384,512,768,1024}}^2 (seed {seed}), "
+                        "1-8 coils, 0-3 permeability-1000 rectangles, tol 1e-10, one solver call for the batch",
+            "nodes": int(sum(p.nx * p.ny for p in probs)), "host_setup_s": setup, "solvers": res,
+            "speedup_vs_plain_fp64": {k: base / v["seconds"] for k, v in res.items()} if base else None}
+
+
+def config1_record(torch, sil):
+    """Configuration 1: the 2D scalar Hodge Laplacian (delta d of a 0-form) on
+    a uniform 512^2 grid, FP64, 16 algorithmic bytes per cell update; timed
+    warm (back-to-back launches, the 4 MB of fields stay in L2) and cold (a
+    256 MB buffer written between launches flushes the 126 MB L2, each launch
+    timed alone), with its parity against the oracle."""
+    import oracle as O
+    from tests.helpers import sinusoid_field
+    m = 512
+    host = sinusoid_field(m, seed=1)[..., None].copy()
+    phi = torch.from_numpy(host).cuda()
+    coords = [np.arange(m) / m, np.arange(m) / m]
+    g2 = sil.Geometry(coords)
+    o2 = torch.empty((m - 1, m - 1, 1), device="cuda", dtype=torch.float64)
+    p2 = sil.make_staged_laplacian(g2, o2, phi, 0)
+    nbytes = (m * m + (m - 1) ** 2) * 8
+    for _ in range(5):
+        p2.run(o2, phi)
+    torch.cuda.synchronize()
+    # warm: 200 launches replayed from one CUDA graph, so the host's launch
+    # rate does not pace the 5-us kernels
+    reps = 200
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        p2.run(o2, phi)
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for _ in range(reps):
+            p2.run(o2, phi)
+    graph.replay()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    graph.replay()
+    b.record()
+    torch.cuda.synchronize()
+    warm_ms = a.elapsed_time(b) / reps
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    cold = []
+    for _ in range(30):
+        flush.fill_(1)
+        a.record()
+        p2.run(o2, phi)
+        b.record()
+        torch.cuda.synchronize()
+        cold.append(a.elapsed_time(b))
+    cold_ms = statistics.median(cold)
+    ref = O.laplacian(2, 0, O.position_from_coords(coords), host)
+    got = o2.cpu().numpy()
+    rel = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+    d = torch.zeros((m - 1, m - 1, 2), device="cuda", dtype=torch.float64)
+    sil.deriv(d, phi, 0)
+    dref = np.zeros((m - 1, m - 1, 2))
+    O.coboundary(host, dref, 0)
+    cu = (m - 1) ** 2
+    return {"workload": "2D scalar Hodge Laplacian delta d of a 0-form, 512x512 uniform grid, spacing 1/512, FP64 "
+                        "(8 sinusoidal modes + 1e-3 noise, seed 1)",
+            "bytes_per_cell_update": 16, "algorithmic_bytes_per_launch": nbytes,
+            "warm": {"us": warm_ms * 1e3, "GB/s": nbytes / (warm_ms * 1e-3) / 1e9,
+                     "cell_updates_per_s": cu / (warm_ms * 1e-3),
+                     "how": f"{reps} back-to-back launches from one CUDA graph, L2 resident"},
+            "cold": {"us": cold_ms * 1e3, "GB/s": nbytes / (cold_ms * 1e-3) / 1e9,
+                     "cell_updates_per_s": cu / (cold_ms * 1e-3),
+                     "how": "median of 30 launches, each after a 256 MB write that flushes L2"},
+            "laplacian_rel_err_vs_oracle": rel, "coboundary_bit_exact": bool(np.array_equal(d.cpu().numpy(), dref)),
+            "kernel": p2.kernel}
+
+
 def run_solve_workload(args):
     """Batched 2D magnetostatics time-to-1e-10 (device-resident inputs, whole batch per solve call)."""
     import torch
     import oracle as O
     import similie_b200.magnetostatics as mag
     from similie_b200 import dist as sd
-    from similie_b200.precond import LearnedPreconditioner
     rank, world, local = sd.env()
     torch.cuda.set_device(local)
     if world > 1:
@@ -479,76 +697,11 @@ def run_solve_workload(args):
     # problems shard across ranks by work (nodes), no collective on the data path
     mine = sd.shard_by_work([p.nx * p.ny for p in allp], world)[rank]
     probs = [allp[i] for i in mine]
-    shapes = [(p.nx, p.ny) for p in probs]
-    mus = [torch.from_numpy(p.node_mu()).cuda() for p in probs]
-    rhss = [torch.from_numpy(p.rhs()).cuda() for p in probs]
-    weights = os.path.join(ROOT, "similie_b200", "data", "precond_2d.npy")
-    net = None
-    if os.path.exists(weights):
-        net = LearnedPreconditioner(seed=0)
-        net.load(weights)
-    results = {}
+    net, weights = load_network()
     kinds = [k for k in args.solvers.split(",") if k in ("cg", "mixed") or (k == "learned" and net is not None)]
     with ClockSampler(local) as clocks:
-        for kind in kinds:
-            sols = [torch.zeros_like(r) for r in rhss]
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            chunk = min(args.chunk, 64)  # the learned solver takes 64 problems per call
-            slices = [slice(c0, c0 + chunk) for c0 in range(0, len(probs), chunk)]
-            per_chunk = [None] * len(slices)
-
-            def run(mine, stream, pnet):
-                for ci in mine:
-                    sl = slices[ci]
-                    per_chunk[ci] = mag.solve_batch(
-                        mus[sl], rhss[sl], sols[sl], shapes[sl], solver=kind, tol=1e-10,
-                        max_iterations=args.max_iterations, inner_iterations=min(4000, args.max_iterations),
-                        preconditioner=pnet if kind == "learned" else None,
-                        stream=None if stream is None else stream.cuda_stream)
-
-            workers = max(1, min(args.concurrent, len(slices)))
-            if workers == 1:
-                run(range(len(slices)), None, net)
-            else:
-                # solver calls in flight together on their own streams, so one
-                # call's straggling problems overlap the others' work
-                import threading
-                nets = [net] + [LearnedPreconditioner(seed=0) for _ in range(workers - 1)]
-                if kind == "learned":
-                    for extra in nets[1:]:
-                        extra.load(weights)
-                streams = [torch.cuda.Stream() for _ in range(workers)]
-                torch.cuda.synchronize()
-                threads = [threading.Thread(target=run, args=(range(w, len(slices), workers), streams[w], nets[w]))
-                           for w in range(workers)]
-                for th in threads:
-                    th.start()
-                for th in threads:
-                    th.join()
-            d = [x for part in per_chunk for x in part]
-            e1.record()
-            torch.cuda.synchronize()
-            wall = time.perf_counter() - t0
-            worst = 0.0
-            for i in range(0, len(probs), max(1, len(probs) // 8)):
-                p = probs[i]
-                xb = sols[i].cpu().numpy()
-                b = p.rhs()
-                worst = max(worst, float(np.linalg.norm(b - O.mag2d_apply(p.nx, p.ny, p.node_mu(), xb)) / np.linalg.norm(b)))
-            # concurrent calls run on their own streams: time them by the host
-            # clock between device-wide synchronisations
-            sec = sd.max_over_ranks(e0.elapsed_time(e1) / 1e3 if workers == 1 else wall, device="cuda")
-            results[kind] = {"seconds": sec, "wall_seconds": wall, "solves_per_s": len(allp) / sec,
-                             "converged": sum(x.converged for x in d), "max_iterations": max(x.iterations for x in d),
-                             "fallbacks": sum(x.fallback for x in d),
-                             "median_iterations": float(np.median([x.iterations for x in d])),
-                             "median_learned_iterations": float(np.median([x.learned_iterations for x in d])),
-                             "max_rel_residual_gpu": max(x.final_relative_residual for x in d),
-                             "max_rel_residual_oracle_sampled": worst}
+        results = time_solver_kinds(torch, probs, kinds, net, weights, chunk=args.chunk, concurrent=args.concurrent,
+                                    max_iterations=args.max_iterations)
     gathered = sd.gather_to_rank0(results)
     if world > 1:
         import torch.distributed as tdist
@@ -557,10 +710,10 @@ def run_solve_workload(args):
     if rank != 0:
         return
     for kind in results:  # per-problem figures over all ranks
-        results[kind]["converged"] = sum(g[kind]["converged"] for g in gathered)
-        results[kind]["fallbacks"] = sum(g[kind]["fallbacks"] for g in gathered)
-        results[kind]["max_iterations"] = max(g[kind]["max_iterations"] for g in gathered)
-        results[kind]["max_rel_residual_gpu"] = max(g[kind]["max_rel_residual_gpu"] for g in gathered)
+        for key in ("converged", "converged_by_oracle", "fallbacks", "total_iterations", "problems_checked_by_oracle"):
+            results[kind][key] = sum(g[kind][key] for g in gathered)
+        for key in ("max_iterations", "max_rel_residual_gpu", "max_rel_residual_oracle"):
+            results[kind][key] = max(g[kind][key] for g in gathered)
     cpu = None
     if args.cpu_sample > 0:
         sample = allp[:args.cpu_sample]

@@ -18,6 +18,7 @@
 // ||r|| <= tol ||b||; the final residual is re-evaluated in FP64.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 #include <mutex>
@@ -32,7 +33,7 @@ namespace sil {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kNodesPerThread = 8;
+constexpr int kNodesPerThread = 16;
 constexpr int kItemNodes = kThreads * kNodesPerThread;  // nodes per work item (one CTA)
 
 // ------------------------------------------------------------------ operator
@@ -75,6 +76,7 @@ struct Vecs
     T* nu;
     T* ph;  // flexible CG: m stored directions p_j at ph + j * hstride
     T* qh;  // and their images q_j = A p_j
+    T* p2;  // persistent CG: the direction's second buffer (p and p2 alternate)
 };
 
 struct ProbInfo
@@ -132,21 +134,40 @@ __device__ __forceinline__ T const* gauge_table(ProbInfo const& pi)
 // reference's stencils, magnetostatics_onelab.hpp:1894-1945).  The gauge
 // term of row (n, c) is sum over the codifferential rows holding the column,
 // m = n and m = n + e_c, of w(m) D(m, (n, c)) (D A)(m).
-template <class T>
-__device__ __forceinline__ T gauge_div(T const* a, T const* gd, int m, int i, int j, int k, int nx, int ny)
+template <class T, class A>
+__device__ __forceinline__ T gauge_div_ld(A const& a, T const* gd, int m, int i, int j, int k, int nx, int ny)
 {
     T const* e = gd + 8 * m;
     T s = T(0);
-    s = s + e[0] * a[3 * m];
-    if (i > 0) s = s + e[3] * a[3 * (m - 1)];
-    s = s + e[1] * a[3 * m + 1];
-    if (j > 0) s = s + e[4] * a[3 * (m - nx) + 1];
-    s = s + e[2] * a[3 * m + 2];
-    if (k > 0) s = s + e[5] * a[3 * (m - nx * ny) + 2];
+    s = s + e[0] * a(3 * m);
+    if (i > 0) s = s + e[3] * a(3 * (m - 1));
+    s = s + e[1] * a(3 * m + 1);
+    if (j > 0) s = s + e[4] * a(3 * (m - nx) + 1);
+    s = s + e[2] * a(3 * m + 2);
+    if (k > 0) s = s + e[5] * a(3 * (m - nx * ny) + 2);
     return s;
 }
 
+template <class T>
+__device__ __forceinline__ T gauge_div(T const* a, T const* gd, int m, int i, int j, int k, int nx, int ny)
+{
+    return gauge_div_ld<T>([a](int idx) { return a[idx]; }, gd, m, i, j, k, nx, ny);
+}
+
 // Gauge term of component c at interior node n = (i, j, k), given (D A)(n).
+template <class T, class A>
+__device__ __forceinline__ T gauge_term_ld(A const& a, T const* gd, int n, int i, int j, int k, int nx, int ny, int c,
+                                           T div_n)
+{
+    int const step = c == 0 ? 1 : (c == 1 ? nx : nx * ny);
+    int const m = n + step;
+    T const div_m = gauge_div_ld<T>(a, gd, m, i + (c == 0), j + (c == 1), k + (c == 2), nx, ny);
+    T t = T(0);
+    t = t + gd[8 * n + 6] * gd[8 * n + c] * div_n;
+    t = t + gd[8 * m + 6] * gd[8 * m + 3 + c] * div_m;
+    return t;
+}
+
 template <class T>
 __device__ __forceinline__ T gauge_term(T const* a, T const* gd, int n, int i, int j, int k, int nx, int ny, int c,
                                         T div_n)
@@ -253,8 +274,8 @@ __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_
 // All three rows of a node at once (the curl moments shared between the
 // components are formed once); each component sums its terms in the order of
 // mag3d_apply_row, so the values are the same.
-template <class T, bool G = false>
-__device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, int node, T* out)
+template <class T, bool G, class LD>
+__device__ void mag3d_apply_node_ld(LD const& a, T const* nu, ProbInfo const& pi, int node, T* out)
 {
     int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
     int const t = node / nx, i = node - t * nx, k = t / ny, j = t - k * ny;
@@ -263,14 +284,14 @@ __device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, in
         return ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz;
     };
     if (!interior(i, j, k)) {
-        out[0] = a[row0];
-        out[1] = a[row0 + 1];
-        out[2] = a[row0 + 2];
+        out[0] = a(row0);
+        out[1] = a(row0 + 1);
+        out[2] = a(row0 + 2);
         return;
     }
     int const sy = 3 * nx, sz = 3 * nx * ny;
     auto A = [&](int di, int dj, int dk, int cc) -> T {
-        return interior(i + di, j + dj, k + dk) ? a[row0 + 3 * di + sy * dj + sz * dk + cc] : T(0);
+        return interior(i + di, j + dj, k + dk) ? a(row0 + 3 * di + sy * dj + sz * dk + cc) : T(0);
     };
     auto bx = [&](int oi, int oj, int ok) {
         T m = T(0);
@@ -318,15 +339,15 @@ __device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, in
     if constexpr (G) {
         if (pi.gauge) {
             T const* gd = gauge_table<T>(pi);
-            T const dn = gauge_div(a, gd, node, i, j, k, nx, ny);
-            for (int c = 0; c < 3; ++c) gt[c] = g * gauge_term(a, gd, node, i, j, k, nx, ny, c, dn);
+            T const dn = gauge_div_ld<T>(a, gd, node, i, j, k, nx, ny);
+            for (int c = 0; c < 3; ++c) gt[c] = g * gauge_term_ld<T>(a, gd, node, i, j, k, nx, ny, c, dn);
             gauge_done = true;
         }
     }
     if (!gauge_done) {
-        gt[0] = g * (ly[j] * lz[k] * ilx[i]) * a[row0];
-        gt[1] = g * (lx[i] * lz[k] * ily[j]) * a[row0 + 1];
-        gt[2] = g * (lx[i] * ly[j] * ilz[k]) * a[row0 + 2];
+        gt[0] = g * (ly[j] * lz[k] * ilx[i]) * a(row0);
+        gt[1] = g * (lx[i] * lz[k] * ily[j]) * a(row0 + 1);
+        gt[2] = g * (lx[i] * ly[j] * ilz[k]) * a(row0 + 2);
     }
     {
         T res = T(0);
@@ -352,6 +373,12 @@ __device__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, in
         if (in_i) res = res - w(-1, 0, 0, 1) * by(-1, 0, 0);
         out[2] = res + gt[2];
     }
+}
+
+template <class T, bool G = false>
+__device__ __forceinline__ void mag3d_apply_node(T const* a, T const* nu, ProbInfo const& pi, int node, T* out)
+{
+    mag3d_apply_node_ld<T, G>([a](int idx) { return a[idx]; }, nu, pi, node, out);
 }
 
 template <class T, bool G = false>
@@ -457,6 +484,9 @@ struct Scalars
     int learned_iters;
     double pq_hist[kMaxDirs];  // p_j . q_j of the stored directions
     double coef[kMaxDirs];     // (z . q_j) / (p_j . q_j) of the current z
+    // persistent CG
+    int pbuf;                  // buffer (0: p, 1: p2) holding the latest direction
+    double scale_prev;         // outer residual norm of the previous refinement pass
 };
 
 // Deterministic block sum of one double per thread.
@@ -553,32 +583,65 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(Item const* items, Pr
     }
 }
 
-// q = A p and the partial p.q; the problem's last CTA forms alpha = rz / (p.q).
+// ------------------------------------------------------------------ CG iteration
+//
+// One Jacobi-CG iteration is two kernels over the items of the problems that
+// still iterate (`act`, one CTA per item, so converged problems launch
+// nothing):
+//   cg_dir_apply  p = z + beta p_old (formed on the fly at the row and at its
+//                 stencil neighbours; p double-buffered), q = A p, partial
+//                 p.q; the problem's last CTA forms alpha
+//   cg_update     x += alpha p, r -= alpha q, z = D^-1 r, partials r.z and
+//                 r.r; the last CTA forms beta, counts the iteration, flips
+//                 the direction buffer and decides convergence
+// Chunks of iterations are captured as a CUDA graph, captured again when the
+// set of iterating problems changes.
+
 template <class T, bool G = false>
-__global__ void __launch_bounds__(kThreads) cg_apply_kernel(Item const* items, ProbInfo const* info, Vecs<T> const* vecs,
-                                                            Scalars* sc, double* part)
+__global__ void __launch_bounds__(kThreads) cg_dir_apply_kernel(Item const* items, int const* act, ProbInfo const* info,
+                                                                Vecs<T> const* vecs, Scalars* sc, double* part)
 {
     __shared__ double red[kThreads / 32];
-    Item const it = items[blockIdx.x];
+    Item const it = items[act[blockIdx.x]];
     Scalars* s = sc + it.prob;
     if (s->done || s->outer_done) return;
     ProbInfo const pi = info[it.prob];
     Vecs<T> const v = vecs[it.prob];
+    int const pb = s->pbuf;
+    T const* pold = pb == 0 ? v.p : v.p2;
+    T* pnew = pb == 0 ? v.p2 : v.p;
+    T const beta = static_cast<T>(s->beta);
+    T const* z = v.z;
+    auto dir = [&](int idx) -> T { return z[idx] + beta * pold[idx]; };
     double pq = 0.0;
     if (pi.dim == 3) {
         for (int64_t node = it.begin / 3 + threadIdx.x; node < it.end / 3; node += kThreads) {
             T q[3];
-            mag3d_apply_node<T, G>(v.p, v.nu, pi, static_cast<int>(node), q);
-            for (int c = 0; c < 3; ++c) {
-                v.q[3 * node + c] = q[c];
-                pq += static_cast<double>(v.p[3 * node + c]) * static_cast<double>(q[c]);
+            mag3d_apply_node_ld<T, G>(dir, v.nu, pi, static_cast<int>(node), q);
+            for (int cc = 0; cc < 3; ++cc) {
+                int const row = static_cast<int>(3 * node + cc);
+                T const pr = dir(row);
+                pnew[row] = pr;
+                v.q[row] = q[cc];
+                pq += static_cast<double>(pr) * static_cast<double>(q[cc]);
             }
         }
     } else {
-        for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-            T const q = mag_apply_row<T, G>(v.p, v.nu, pi, row);
+        // (i, j) of the thread's rows advance by adding: no division per row
+        int const nx = static_cast<int>(pi.nx);
+        int row = static_cast<int>(it.begin) + threadIdx.x;
+        int j = row / nx, i = row - j * nx;
+        for (; row < it.end; row += kThreads) {
+            T const q = mag_apply_node_ij<T>(dir, v.nu, nx, static_cast<int>(pi.ny), row, i, j);
+            T const pr = dir(row);
+            pnew[row] = pr;
             v.q[row] = q;
-            pq += static_cast<double>(v.p[row]) * static_cast<double>(q);
+            pq += static_cast<double>(pr) * static_cast<double>(q);
+            i += kThreads;
+            while (i >= nx) {
+                i -= nx;
+                ++j;
+            }
         }
     }
     double const pq_b = block_sum(pq, red);
@@ -589,23 +652,22 @@ __global__ void __launch_bounds__(kThreads) cg_apply_kernel(Item const* items, P
     }
 }
 
-// x += alpha p, r -= alpha q, z = dinv r; partials r.z and r.r; the last CTA
-// forms beta and decides convergence.
 template <class T>
-__global__ void __launch_bounds__(kThreads) cg_update_kernel(Item const* items, ProbInfo const* info,
+__global__ void __launch_bounds__(kThreads) cg_update_kernel(Item const* items, int const* act, ProbInfo const* info,
                                                              Vecs<T> const* vecs, Scalars* sc, double* part_a,
                                                              double* part_b)
 {
     __shared__ double red[kThreads / 32];
-    Item const it = items[blockIdx.x];
+    Item const it = items[act[blockIdx.x]];
     Scalars* s = sc + it.prob;
     if (s->done || s->outer_done) return;
     ProbInfo const pi = info[it.prob];
     Vecs<T> const v = vecs[it.prob];
+    T const* pcur = s->pbuf == 0 ? v.p2 : v.p;
     T const alpha = static_cast<T>(s->alpha);
     double rz = 0.0, rr = 0.0;
     for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
-        T const x = v.x[row] + alpha * v.p[row];
+        T const x = v.x[row] + alpha * pcur[row];
         T const r = v.r[row] - alpha * v.q[row];
         T const z = v.dinv[row] * r;
         v.x[row] = x;
@@ -626,21 +688,66 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(Item const* items, 
         s->rr = tot_rr;
         s->iters += 1;
         s->total_iters += 1;
+        s->pbuf ^= 1;
         if (!isfinite(tot_rr) || !isfinite(trz)) s->nonfinite = 1;
         if (tot_rr <= s->inner_tol2 * s->rr0 || s->nonfinite || s->total_iters >= pi.max_iters) s->done = 1;
     }
 }
 
-// p = z + beta p (skipped once converged).
+// Start or continue the CG of a refinement pass on the new outer residual:
+// r = r64 / scale, z = D^-1 r, x = 0 (the correction restarts; x64 holds the
+// previous ones), r.z and r.r.  fresh: p_old = z and beta = 0, so the first
+// direction is z.  Otherwise the direction of the previous pass is kept (the
+// Krylov space survives the residual replacement).  The pass ended at
+// iterate k with (r.z)_k and beta_old = (r.z)_k / (r.z)_{k-1}; the replaced
+// residual continues iterate k, so its direction is z + beta' p_{k-1} with
+// beta' = (r.z)~ / (r.z)_{k-1}, all in the units of the new scale: p_{k-1}
+// is rho p_old there and (r.z)_{k-1} is rho^2 (r.z)_k / beta_old, rho =
+// scale_prev / scale, so beta = beta_old (r.z)~ / (rho (r.z)_k) applied to
+// the stored p_old.
 template <class T>
-__global__ void __launch_bounds__(kThreads) cg_direction_kernel(Item const* items, Vecs<T> const* vecs, Scalars* sc)
+__global__ void __launch_bounds__(kThreads) cg_replace_kernel(Item const* items, int const* act, ProbInfo const* info,
+                                                              Vecs<T> const* vecs, double const* const* r64,
+                                                              Scalars* sc, double* part_a, double* part_b, int fresh)
 {
-    Item const it = items[blockIdx.x];
+    __shared__ double red[kThreads / 32];
+    Item const it = items[act[blockIdx.x]];
     Scalars* s = sc + it.prob;
-    if (s->done || s->outer_done) return;
+    if (s->outer_done) return;
+    ProbInfo const pi = info[it.prob];
     Vecs<T> const v = vecs[it.prob];
-    T const beta = static_cast<T>(s->beta);
-    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) v.p[row] = v.z[row] + beta * v.p[row];
+    double const scale = s->scale;
+    T* pold = s->pbuf == 0 ? v.p : v.p2;
+    double rz = 0.0, rr = 0.0;
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) {
+        T const r = static_cast<T>(r64[it.prob][row] / scale);
+        T const z = v.dinv[row] * r;
+        v.x[row] = T(0);
+        v.r[row] = r;
+        v.z[row] = z;
+        if (fresh) pold[row] = z;
+        rz += static_cast<double>(r) * static_cast<double>(z);
+        rr += static_cast<double>(r) * static_cast<double>(r);
+    }
+    double const rz_b = block_sum(rz, red);
+    double const rr_b = block_sum(rr, red);
+    double const vals[2] = {rz_b, rr_b};
+    double* parts[2] = {part_a, part_b};
+    double tot[2];
+    if (finish_reduction_k<2>(vals, parts, it.index, pi.first_item, pi.nitems, &s->counter_a, tot)) {
+        double const trz = tot[0], tot_rr = tot[1];
+        // beta = 0 (the direction restarts from z) on a fresh pass, and when
+        // no iterate has run since the last replacement
+        bool const keep = !fresh && s->iters > 0 && s->rz > 0.0 && s->scale_prev > 0.0;
+        s->beta = keep ? s->beta * trz / ((s->scale_prev / scale) * s->rz) : 0.0;
+        if (fresh) s->pbuf = 0;
+        s->rz = trz;
+        s->rr = tot_rr;
+        s->rr0 = tot_rr;
+        s->iters = 0;
+        s->done = (tot_rr == 0.0 || s->total_iters >= pi.max_iters) ? 1 : 0;
+        s->nonfinite = 0;
+    }
 }
 
 // ------------------------------------------------------------------ flexible CG (learned preconditioner)
@@ -660,14 +767,18 @@ __device__ __forceinline__ T* fcg_slot(T* base, int64_t hstride, int slot)
 }
 
 // x = 0, r = r64 / scale (precision T), rr0 = r.r; stall window reset.
-// Problems already handed to the plain solver get a zero correction.
+// Problems already handed to the plain solver get a zero correction.  After
+// the first pass (fresh = 0) the stored directions are kept: the projections
+// (z.q_j)/(p_j.q_j) p_j and alpha = (p.r)/(p.q) do not depend on the units
+// the directions were formed in, so the flexible CG continues on the
+// replaced residual instead of restarting.
 template <class T>
-__global__ void __launch_bounds__(kThreads) fcg_init_kernel(Item const* items, ProbInfo const* info,
+__global__ void __launch_bounds__(kThreads) fcg_init_kernel(Item const* items, int const* act, ProbInfo const* info,
                                                             Vecs<T> const* vecs, double const* const* r64,
-                                                            Scalars* sc, double* part)
+                                                            Scalars* sc, double* part, int fresh)
 {
     __shared__ double red[kThreads / 32];
-    Item const it = items[blockIdx.x];
+    Item const it = items[act != nullptr ? act[blockIdx.x] : blockIdx.x];
     Scalars* s = sc + it.prob;
     if (s->outer_done) return;
     Vecs<T> const v = vecs[it.prob];
@@ -691,7 +802,7 @@ __global__ void __launch_bounds__(kThreads) fcg_init_kernel(Item const* items, P
         s->rr0 = tot;
         s->win_rr = tot;
         s->win_iters = 0;
-        s->iters = 0;
+        if (fresh) s->iters = 0;
         s->done = (tot == 0.0 || s->total_iters >= pi.max_iters) ? 1 : 0;
         s->nonfinite = 0;
     }
@@ -700,13 +811,13 @@ __global__ void __launch_bounds__(kThreads) fcg_init_kernel(Item const* items, P
 // Partials z.q_j over the stored directions (the first min(iters, m)); the
 // last CTA forms coef_j = (z.q_j)/(p_j.q_j).  M >= m is the compile-time bound.
 template <class T, int M>
-__global__ void __launch_bounds__(kThreads) fcg_orth_kernel(Item const* items, ProbInfo const* info,
+__global__ void __launch_bounds__(kThreads) fcg_orth_kernel(Item const* items, int const* act, ProbInfo const* info,
                                                             Vecs<T> const* vecs, Scalars* sc, double* parts_base,
-                                                            int64_t hstride, int m)
+                                                            int64_t hstride, int m, int nitems_all)
 {
     __shared__ double red[kThreads / 32];
     __shared__ double vals[M];
-    Item const it = items[blockIdx.x];
+    Item const it = items[act != nullptr ? act[blockIdx.x] : blockIdx.x];
     Scalars* s = sc + it.prob;
     if (s->done || s->outer_done || s->fallback) return;
     ProbInfo const pi = info[it.prob];
@@ -730,7 +841,7 @@ __global__ void __launch_bounds__(kThreads) fcg_orth_kernel(Item const* items, P
     __syncthreads();
     double* parts[M];
 #pragma unroll
-    for (int j = 0; j < M; ++j) parts[j] = parts_base + static_cast<int64_t>(j) * gridDim.x;
+    for (int j = 0; j < M; ++j) parts[j] = parts_base + static_cast<int64_t>(j) * nitems_all;  // one slot per item of the batch
     double tot[M];
     if (finish_reduction_k<M>(vals, parts, it.index, pi.first_item, pi.nitems, &s->counter_a, tot)) {
         for (int j = 0; j < nvalid; ++j) {
@@ -744,10 +855,10 @@ __global__ void __launch_bounds__(kThreads) fcg_orth_kernel(Item const* items, P
 // the slot being written is also the oldest term of the sum; each thread
 // reads its element of every p_j before writing.
 template <class T, int M>
-__global__ void __launch_bounds__(kThreads) fcg_direction_kernel(Item const* items, Vecs<T> const* vecs,
+__global__ void __launch_bounds__(kThreads) fcg_direction_kernel(Item const* items, int const* act, Vecs<T> const* vecs,
                                                                  Scalars const* sc, int64_t hstride, int m)
 {
-    Item const it = items[blockIdx.x];
+    Item const it = items[act != nullptr ? act[blockIdx.x] : blockIdx.x];
     Scalars const* s = sc + it.prob;
     if (s->done || s->outer_done || s->fallback) return;
     Vecs<T> const v = vecs[it.prob];
@@ -769,12 +880,12 @@ __global__ void __launch_bounds__(kThreads) fcg_direction_kernel(Item const* ite
 // q_slot = A p_slot, partials p.q and p.r; the last CTA stores p.q for the
 // slot and forms alpha.
 template <class T>
-__global__ void __launch_bounds__(kThreads) fcg_apply_kernel(Item const* items, ProbInfo const* info,
+__global__ void __launch_bounds__(kThreads) fcg_apply_kernel(Item const* items, int const* act, ProbInfo const* info,
                                                              Vecs<T> const* vecs, Scalars* sc, double* part_a,
                                                              double* part_b, int64_t hstride, int m)
 {
     __shared__ double red[kThreads / 32];
-    Item const it = items[blockIdx.x];
+    Item const it = items[act != nullptr ? act[blockIdx.x] : blockIdx.x];
     Scalars* s = sc + it.prob;
     if (s->done || s->outer_done || s->fallback) return;
     ProbInfo const pi = info[it.prob];
@@ -806,12 +917,12 @@ __global__ void __launch_bounds__(kThreads) fcg_apply_kernel(Item const* items, 
 // x += alpha p_slot, r -= alpha q_slot, partial r.r; the last CTA advances
 // the iteration (and so the slot) and checks convergence and the stall window.
 template <class T>
-__global__ void __launch_bounds__(kThreads) fcg_update_kernel(Item const* items, ProbInfo const* info,
+__global__ void __launch_bounds__(kThreads) fcg_update_kernel(Item const* items, int const* act, ProbInfo const* info,
                                                               Vecs<T> const* vecs, Scalars* sc, double* part,
                                                               int window, int64_t hstride, int m)
 {
     __shared__ double red[kThreads / 32];
-    Item const it = items[blockIdx.x];
+    Item const it = items[act != nullptr ? act[blockIdx.x] : blockIdx.x];
     Scalars* s = sc + it.prob;
     if (s->done || s->outer_done || s->fallback) return;
     ProbInfo const pi = info[it.prob];
@@ -858,14 +969,15 @@ __global__ void fcg_active_kernel(Scalars const* sc, int np, int* active)
 }
 
 // r64 = b - A x64 and its norm (outer residual, FP64); marks outer convergence.
+// act: the items to visit (NULL: every item, one CTA each).
 template <bool G = false>
-__global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items, ProbInfo const* info,
+__global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items, int const* act, ProbInfo const* info,
                                                               double const* const* nu64, double const* const* rhs,
                                                               double* const* x64, double* const* r64, Scalars* sc,
                                                               double* part, double tol2, double floor2, int mark)
 {
     __shared__ double red[kThreads / 32];
-    Item const it = items[blockIdx.x];
+    Item const it = items[act != nullptr ? act[blockIdx.x] : blockIdx.x];
     Scalars* s = sc + it.prob;
     if (s->outer_done) return;
     ProbInfo const pi = info[it.prob];
@@ -892,6 +1004,7 @@ __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items,
     double tot = 0.0;
     if (finish_reduction(rr_b, part, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot)) {
         s->rr = tot;
+        s->scale_prev = s->scale;
         s->scale = sqrt(tot);
         if (mark && (tot <= tol2 * s->bb || !isfinite(tot))) s->outer_done = 1;
         // Next inner solve: reduce the (unit-scaled) residual until the outer
@@ -904,10 +1017,10 @@ __global__ void __launch_bounds__(kThreads) residual64_kernel(Item const* items,
 
 // x64 += scale * e (inner correction, promoted to FP64).
 template <class T>
-__global__ void __launch_bounds__(kThreads) refine_kernel(Item const* items, Vecs<T> const* vecs, double* const* x64,
-                                                          Scalars const* sc)
+__global__ void __launch_bounds__(kThreads) refine_kernel(Item const* items, int const* act, Vecs<T> const* vecs,
+                                                          double* const* x64, Scalars const* sc)
 {
-    Item const it = items[blockIdx.x];
+    Item const it = items[act != nullptr ? act[blockIdx.x] : blockIdx.x];
     Scalars const* s = sc + it.prob;
     if (s->outer_done) return;
     T const* e = vecs[it.prob].x;
@@ -1081,7 +1194,13 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
                        cudaStream_t stream, nn::Net* learned = nullptr)
 {
     int const np = static_cast<int>(probs.size());
-    // Work items: contiguous row ranges of kItemNodes per problem.
+    // Work items: contiguous row ranges of item_rows rows per problem (3D:
+    // whole nodes, four thirds of that), one CTA each.
+    int item_rows = kItemNodes;
+    if (char const* e = std::getenv("SIMILIE_B200_ITEM_ROWS")) {
+        int const v = std::atoi(e);
+        if (v >= kThreads && v % kThreads == 0 && v <= 64 * kThreads) item_rows = v;
+    }
     std::vector<Item> items;
     std::vector<ProbInfo> info(np);
     int64_t total_rows = 0;
@@ -1104,7 +1223,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         int idx = 0;
         // 3D items: whole nodes (3 rows each), four times the 2D item, so
         // the per-CTA prologue is amortised over more of the costlier 3D rows
-        int64_t const step = q.dim == 3 ? (4 * kItemNodes / 3) * 3 : kItemNodes;
+        int64_t const step = q.dim == 3 ? (4 * item_rows / 3) * 3 : item_rows;
         for (int64_t b = 0; b < pi.n; b += step, ++idx) items.push_back({p, idx, b, std::min(pi.n, b + step)});
         pi.nitems = idx;
         total_rows += pi.n;
@@ -1119,7 +1238,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     }
     std::vector<float> sp32(sp64.begin(), sp64.end());
     int const nitems = static_cast<int>(items.size());
-    int const nvec = 7;  // x r z p q dinv nu in precision T
+    int const nvec = 8;  // x r z p q dinv nu p2 in precision T
     size_t const vec_bytes = ((total_rows * sizeof(T) + 255) / 256) * 256;
     size_t const d_bytes = ((total_rows * sizeof(double) + 255) / 256) * 256;
     size_t const ndouble_vecs = 3;  // nu64, r64, x64
@@ -1144,7 +1263,8 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     bytes += gauge_bytes + 256;
     bytes += sizeof(Item) * nitems + sizeof(ProbInfo) * np + sizeof(Vecs<T>) * np + sizeof(Scalars) * np
              + (3 + kMaxDirs) * sizeof(double) * nitems + 7 * sizeof(void*) * np
-             + sp64.size() * (sizeof(double) + sizeof(float)) + sizeof(int) * np + 22 * 256;
+             + sp64.size() * (sizeof(double) + sizeof(float)) + sizeof(int) * np + sizeof(int) * nitems
+             + 23 * 256;
     DeviceBuffer buf;
     SIL_CUDA_CHECK(cudaMalloc(&buf.ptr, bytes));
     char* base = static_cast<char*>(buf.ptr);
@@ -1169,6 +1289,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     double* part_c = reinterpret_cast<double*>(take(sizeof(double) * nitems));
     double* part_h = reinterpret_cast<double*>(take(sizeof(double) * kMaxDirs * nitems));
     int* d_active = reinterpret_cast<int*>(take(sizeof(int) * np));
+    int* d_act = reinterpret_cast<int*>(take(sizeof(int) * nitems));
     char* gauge_base = gauge_bytes > 0 ? take(gauge_bytes) : nullptr;
     double const** d_mu = reinterpret_cast<double const**>(take(sizeof(void*) * np));
     double const** d_rhs = reinterpret_cast<double const**>(take(sizeof(void*) * np));
@@ -1225,7 +1346,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         vecs[p] = {vec_base[0] + off, vec_base[1] + off, vec_base[2] + off, vec_base[3] + off,
                    vec_base[4] + off, vec_base[5] + off, vec_base[6] + off,
                    nhist > 0 ? hist_base + off : vec_base[3] + off,
-                   nhist > 0 ? hist_base + fdirs * hstride + off : vec_base[4] + off};
+                   nhist > 0 ? hist_base + fdirs * hstride + off : vec_base[4] + off, vec_base[7] + off};
         mu[p] = probs[p].node_mu;
         rhs[p] = probs[p].rhs;
         nu64[p] = nu64_base + off;
@@ -1258,64 +1379,61 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     int const chunk = 32;
     std::vector<Scalars> hs(np);
 
-    // One chunk of CG iterations, captured once as a CUDA graph.
+    // Items of the problems not yet converged (the CG kernels skip problems
+    // whose inner solve has stopped); a chunk of iterations over them is
+    // captured as a CUDA graph, captured again once the list has shrunk by a
+    // tenth (a longer list is still correct: its finished problems return at
+    // once).
+    std::vector<int> open_host;
+    open_host.reserve(nitems);
+    int captured_n = -1;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    auto capture = [&](double) -> sil_status {
-        if (exec != nullptr) {
-            cudaGraphExecDestroy(exec);
-            exec = nullptr;
-        }
-        if (graph != nullptr) {
-            cudaGraphDestroy(graph);
-            graph = nullptr;
-        }
+    auto build_open = [&]() {
+        open_host.clear();
+        for (int i = 0; i < nitems; ++i)
+            if (!hs[items[i].prob].outer_done) open_host.push_back(i);
+    };
+    auto capture_chunk = [&]() -> sil_status {
+        if (exec != nullptr) cudaGraphExecDestroy(exec);
+        if (graph != nullptr) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        int const n = static_cast<int>(open_host.size());
+        SIL_CUDA_CHECK(cudaMemcpyAsync(d_act, open_host.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
         cudaStream_t cs;
         SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
         cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         for (int c = 0; c < chunk && err == cudaSuccess; ++c) {
-            if (any_gauge) cg_apply_kernel<T, true><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a);
-            else cg_apply_kernel<T, false><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a);
-            cg_update_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_b, part_c);
-            cg_direction_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc);
+            if (any_gauge) cg_dir_apply_kernel<T, true><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_a);
+            else cg_dir_apply_kernel<T, false><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_a);
+            cg_update_kernel<T><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_b, part_c);
         }
         cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
         if (err == cudaSuccess) err = err2;
         if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
         cudaStreamDestroy(cs);
         if (err != cudaSuccess) return cuda_fail(err, "solver graph capture");
+        captured_n = n;
         return SIL_OK;
     };
-    auto run_graph_until_done = [&](cudaGraphExec_t gexec, int gchunk, int budget, int* used) -> sil_status {
-        int spent = 0;
-        while (spent < budget) {
-            SIL_CUDA_CHECK(cudaGraphLaunch(gexec, stream));
-            spent += gchunk;
-            SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
-            SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
-            bool all = true;
-            for (int p = 0; p < np; ++p) all = all && (hs[p].done || hs[p].outer_done);
-            if (all) break;
-        }
-        *used = spent;
+    auto read_scalars = [&]() -> sil_status {
+        SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
+        SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
         return SIL_OK;
-    };
-    auto run_until_done = [&](int budget, int* used) -> sil_status {
-        return run_graph_until_done(exec, chunk, budget, used);
     };
 
-    // Iterative refinement on the FP64 residual: r = b - A x (FP64), an inner
-    // Jacobi-CG solve of A e = r / ||r|| in precision T, x += ||r|| e.  With
-    // T = double the inner target is adaptive (half the outer tolerance), so a
-    // single pass usually suffices and further passes only correct the drift
-    // between the CG recurrence residual and the true residual; with T =
-    // float each pass reduces the residual by about `inner_tolerance`.
+    // Iterative refinement on the FP64 residual with reliable updates: after
+    // every chunk of CG iterations in precision T, x64 += ||r|| x, the FP64
+    // true residual r = b - A x64 replaces the recurrence's residual, and CG
+    // continues with its previous search direction (residual replacement,
+    // not a restart), so the Krylov space survives and the recurrence never
+    // drifts far from the true residual.  A problem stops iterating once its
+    // recurrence reaches half the outer tolerance and converges once the
+    // FP64 residual does.  With T = float the chunks run at half the bytes
+    // of FP64 and converge at nearly the FP64 rate.
     sil_status st = SIL_OK;
     int refinements = 0;
-    bool const low = sizeof(T) < sizeof(double);
-    double const inner_tol = low ? (set.inner_tolerance > 0 ? set.inner_tolerance : 1e-4) : 0.0;
-    int const inner_max = low ? (set.inner_iterations > 0 ? set.inner_iterations : 4000) : max_iter;
-    st = capture(0.0);
     SIL_CUDA_CHECK(cudaMemsetAsync(x64_base, 0, d_bytes, stream));
 
     // Refinement passes whose inner solve is the flexible CG preconditioned by
@@ -1343,64 +1461,107 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
             double const ltol = set.inner_tolerance > 0 ? set.inner_tolerance : 1e-5;
             int const lmax = set.inner_iterations > 0 ? set.inner_iterations : 4000;
             int const lchunk = 8;
+            int ln = 0;  // items the flexible CG's kernels visit (listed in d_act)
             // z -> A-orthogonal direction in the next ring slot.
             auto new_direction = [&](cudaStream_t cs) {
                 if (fdirs <= 1) {
-                    fcg_orth_kernel<T, 1><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_h, hstride, fdirs);
-                    fcg_direction_kernel<T, 1><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc, hstride, fdirs);
+                    fcg_orth_kernel<T, 1><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_h, hstride, fdirs,
+                                                                    nitems);
+                    fcg_direction_kernel<T, 1><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_vecs, d_sc, hstride, fdirs);
                 } else if (fdirs <= 4) {
-                    fcg_orth_kernel<T, 4><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_h, hstride, fdirs);
-                    fcg_direction_kernel<T, 4><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc, hstride, fdirs);
+                    fcg_orth_kernel<T, 4><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_h, hstride, fdirs,
+                                                                    nitems);
+                    fcg_direction_kernel<T, 4><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_vecs, d_sc, hstride, fdirs);
                 } else if (fdirs <= 8) {
-                    fcg_orth_kernel<T, 8><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_h, hstride, fdirs);
-                    fcg_direction_kernel<T, 8><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc, hstride, fdirs);
+                    fcg_orth_kernel<T, 8><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_h, hstride, fdirs,
+                                                                    nitems);
+                    fcg_direction_kernel<T, 8><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_vecs, d_sc, hstride, fdirs);
                 } else {
-                    fcg_orth_kernel<T, 16><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_h, hstride, fdirs);
-                    fcg_direction_kernel<T, 16><<<nitems, kThreads, 0, cs>>>(d_items, d_vecs, d_sc, hstride, fdirs);
+                    fcg_orth_kernel<T, 16><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_h, hstride, fdirs,
+                                                                    nitems);
+                    fcg_direction_kernel<T, 16><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_vecs, d_sc, hstride, fdirs);
                 }
             };
+            // The flexible CG's kernels visit the items of the problems still
+            // iterating (`ln` of them, listed in d_act); the chunk graph is
+            // captured again once that list has shrunk by a tenth.
             cudaGraph_t lgraph = nullptr;
             cudaGraphExec_t lexec = nullptr;
-            {
+            std::vector<int> lopen;
+            lopen.reserve(nitems);
+            auto build_lopen = [&]() {
+                lopen.clear();
+                for (int i = 0; i < nitems; ++i) {
+                    Scalars const& q = hs[items[i].prob];
+                    if (!q.outer_done && !q.fallback && !q.done) lopen.push_back(i);
+                }
+            };
+            auto capture_learned = [&]() -> sil_status {
+                if (lexec != nullptr) cudaGraphExecDestroy(lexec);
+                if (lgraph != nullptr) cudaGraphDestroy(lgraph);
+                lexec = nullptr;
+                lgraph = nullptr;
+                ln = static_cast<int>(lopen.size());
+                SIL_CUDA_CHECK(cudaMemcpyAsync(d_act, lopen.data(), sizeof(int) * ln, cudaMemcpyHostToDevice, stream));
                 cudaStream_t cs;
                 SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+                sil_status cst = SIL_OK;
                 cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-                for (int c = 0; c < lchunk && err == cudaSuccess && lst == SIL_OK; ++c) {
-                    fcg_apply_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_a, part_b,
-                                                                     hstride, fdirs);
-                    fcg_update_kernel<T><<<nitems, kThreads, 0, cs>>>(d_items, d_info, d_vecs, d_sc, part_c, window,
-                                                                      hstride, fdirs);
+                for (int c = 0; c < lchunk && err == cudaSuccess && cst == SIL_OK; ++c) {
+                    fcg_apply_kernel<T><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_a, part_b,
+                                                                 hstride, fdirs);
+                    fcg_update_kernel<T><<<ln, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_c, window,
+                                                                  hstride, fdirs);
                     fcg_active_kernel<<<(np + 63) / 64, 64, 0, cs>>>(d_sc, np, d_active);
-                    lst = net->forward(ws, nuf, dv, rv, zv, cs, d_active);
+                    cst = net->forward(ws, nuf, dv, rv, zv, cs, d_active);
                     new_direction(cs);
                 }
                 cudaError_t const err2 = cudaStreamEndCapture(cs, &lgraph);
                 if (err == cudaSuccess) err = err2;
-                if (err == cudaSuccess && lst == SIL_OK) err = cudaGraphInstantiate(&lexec, lgraph, 0);
+                if (err == cudaSuccess && cst == SIL_OK) err = cudaGraphInstantiate(&lexec, lgraph, 0);
                 cudaStreamDestroy(cs);
-                if (lst == SIL_OK && err != cudaSuccess) lst = cuda_fail(err, "learned solver graph capture");
-            }
+                if (cst != SIL_OK) return cst;
+                if (err != cudaSuccess) return cuda_fail(err, "learned solver graph capture");
+                return SIL_OK;
+            };
             int tot = 0;
             while (lst == SIL_OK && tot < max_iter) {
-                residual64<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc,
-                                                                   part_a, tol * tol, ltol * ltol, 1);
+                residual64<<<nitems, kThreads, 0, stream>>>(d_items, nullptr, d_info, d_nu64, d_rhs, d_x64, d_r64,
+                                                                   d_sc, part_a, tol * tol, ltol * ltol, 1);
                 SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
                 SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
                 bool active = false;
                 for (int p = 0; p < np; ++p) active = active || (!hs[p].outer_done && !hs[p].fallback);
                 if (!active) break;
-                fcg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, d_r64, d_sc, part_a);
+                fcg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, nullptr, d_info, d_vecs, d_r64, d_sc, part_a,
+                                                                    *refinements_out == 0 ? 1 : 0);
+                // every problem not converged and not handed over iterates after the init
+                for (int p = 0; p < np; ++p) hs[p].done = 0;
+                build_lopen();
+                lst = capture_learned();
+                if (lst != SIL_OK) break;
                 fcg_active_kernel<<<(np + 63) / 64, 64, 0, stream>>>(d_sc, np, d_active);
                 lst = net->forward(ws, nuf, dv, rv, zv, stream, d_active);
                 if (lst != SIL_OK) break;
                 new_direction(stream);
                 SIL_CUDA_CHECK(cudaGetLastError());
-                int used = 0;
-                lst = run_graph_until_done(lexec, lchunk, std::min(lmax, max_iter - tot), &used);
-                tot += used;
+                int const budget = std::min(lmax, max_iter - tot);
+                int spent = 0;
+                while (spent < budget) {
+                    SIL_CUDA_CHECK(cudaGraphLaunch(lexec, stream));
+                    spent += lchunk;
+                    SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
+                    SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
+                    build_lopen();
+                    if (lopen.empty()) break;
+                    if (10 * static_cast<int>(lopen.size()) < 9 * ln) {
+                        lst = capture_learned();
+                        if (lst != SIL_OK) break;
+                    }
+                }
+                if (lst != SIL_OK) break;
+                tot += spent;
                 // A problem still unconverged after a full inner budget goes to the plain solver.
-                SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
-                SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
                 bool flagged = false;
                 for (int p = 0; p < np; ++p) {
                     if (!hs[p].outer_done && !hs[p].fallback && !hs[p].done) {
@@ -1408,7 +1569,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
                         flagged = true;
                     }
                 }
-                refine_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_x64, d_sc);
+                refine_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, nullptr, d_vecs, d_x64, d_sc);
                 if (flagged) {
                     SIL_CUDA_CHECK(cudaMemcpyAsync(d_sc, hs.data(), sizeof(Scalars) * np, cudaMemcpyHostToDevice, stream));
                 }
@@ -1427,25 +1588,37 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     if constexpr (std::is_same_v<T, float>) {
         if (learned != nullptr && st == SIL_OK) st = learned_stage(learned, &total, &refinements);
     }
-    while (st == SIL_OK && total < max_iter) {
-        residual64<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc, part_a,
-                                                           tol * tol, inner_tol * inner_tol, 1);
-        SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
-        SIL_CUDA_CHECK(cudaStreamSynchronize(stream));
-        bool all = true;
-        for (int p = 0; p < np; ++p) all = all && hs[p].outer_done;
-        if (all) break;
-        cg_init_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_vecs, nullptr, d_r64, d_sc, part_a,
-                                                           part_b, true);
-        int used = 0;
-        st = run_until_done(std::min(inner_max, max_iter - total), &used);
-        total += used;
-        refine_kernel<T><<<nitems, kThreads, 0, stream>>>(d_items, d_vecs, d_x64, d_sc);
+    // Cycle: FP64 residual (outer check) -> residual replacement -> a chunk
+    // of iterations -> x64 += ||r|| x; the host reads the problems' state
+    // once per cycle.
+    auto const residual_open = any_gauge ? residual64_kernel<true> : residual64_kernel<false>;
+    build_open();
+    if (!open_host.empty()) st = capture_chunk();
+    bool fresh = true;
+    while (st == SIL_OK && !open_host.empty()) {
+        int const n = captured_n;
+        residual_open<<<n, kThreads, 0, stream>>>(d_items, d_act, d_info, d_nu64, d_rhs, d_x64, d_r64, d_sc, part_a,
+                                                  tol * tol, 0.0, 1);
+        st = read_scalars();
+        if (st != SIL_OK) break;
+        build_open();
+        if (open_host.empty() || total >= max_iter) break;
+        if (10 * static_cast<int>(open_host.size()) < 9 * captured_n) {
+            st = capture_chunk();
+            if (st != SIL_OK) break;
+        }
+        cg_replace_kernel<T><<<captured_n, kThreads, 0, stream>>>(d_items, d_act, d_info, d_vecs, d_r64, d_sc,
+                                                                  part_a, part_b, fresh ? 1 : 0);
+        SIL_CUDA_CHECK(cudaGetLastError());
+        fresh = false;
+        SIL_CUDA_CHECK(cudaGraphLaunch(exec, stream));
+        total += chunk;
+        refine_kernel<T><<<captured_n, kThreads, 0, stream>>>(d_items, d_act, d_vecs, d_x64, d_sc);
         ++refinements;
     }
-    if (st == SIL_OK) copy_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_x64, d_sol, d_sc);
     if (exec != nullptr) cudaGraphExecDestroy(exec);
     if (graph != nullptr) cudaGraphDestroy(graph);
+    if (st == SIL_OK) copy_kernel<<<nitems, kThreads, 0, stream>>>(d_items, d_x64, d_sol, d_sc);
     if (st != SIL_OK) return st;
 
     // FP64 true residual ||b - A x|| of the returned solution for every problem.
@@ -1457,8 +1630,8 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
         hs2[p].counter_a = hs2[p].counter_b = hs2[p].counter_c = 0;
     }
     SIL_CUDA_CHECK(cudaMemcpyAsync(d_sc, hs2.data(), sizeof(Scalars) * np, cudaMemcpyHostToDevice, stream));
-    residual64<<<nitems, kThreads, 0, stream>>>(d_items, d_info, d_nu64, d_rhs, d_sol, d_scratch, d_sc, part_a,
-                                                       tol * tol, 0.0, 0);
+    residual64<<<nitems, kThreads, 0, stream>>>(d_items, nullptr, d_info, d_nu64, d_rhs, d_sol, d_scratch, d_sc,
+                                                       part_a, tol * tol, 0.0, 0);
     SIL_CUDA_CHECK(cudaGetLastError());
     SIL_CUDA_CHECK(cudaMemcpyAsync(hs.data(), d_sc, sizeof(Scalars) * np, cudaMemcpyDeviceToHost, stream));
     SIL_CUDA_CHECK(cudaStreamSynchronize(stream));

@@ -4,15 +4,18 @@ Callers that may not allocate device memory while applying the operator --
 a matrix-free operator called in every iteration of another library's Krylov
 loop, or code under a host framework's memory pool or cap -- use this entry
 point; its scratch is a fixed device array inside the library.  The test
-calls it through the C ABI and checks it against sil_mag2d_apply on two
-calls in a row (the shared array keeps the previous call's contents, which
-must not leak into the next result), and that oversized grids are refused.
+calls it through the C ABI and checks it against sil_mag2d_apply and against
+the oracle's operator on two calls in a row (the shared array keeps the
+previous call's contents, which must not leak into the next result), and
+that oversized grids are refused.
 This file sorts last so a run that stops at the first failure has already
 run every other test."""
 import ctypes
 
 import numpy as np
 import pytest
+
+import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -49,6 +52,8 @@ def test_noalloc_apply_matches_allocating_apply(torch):
         got = y_new.cpu().numpy()
         assert np.all(np.isfinite(got))
         assert np.max(np.abs(got - ref)) <= TOL * np.max(np.abs(ref))
+        oref = O.mag2d_apply(n, n, p.node_mu(), a.cpu().numpy())
+        assert np.max(np.abs(got - oref)) <= TOL * np.max(np.abs(oref))
 
 
 def test_noalloc_apply_rejects_oversized_grid(torch):
