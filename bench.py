@@ -596,6 +596,17 @@ def solve_record(torch, kinds=("cg", "mixed", "learned"), seed=7, count=64):
     net, weights = load_network()
     kinds = [k for k in kinds if k != "learned" or net is not None]
     setup = time.perf_counter() - t0
+    # untimed one-iteration solves first: the solver's one-time work-item
+    # tuning (first large batch per precision) and the network's workspace
+    # happen there, as in any long-running caller
+    import similie_b200.magnetostatics as mag_w
+    wmus = [torch.from_numpy(p.node_mu()).cuda() for p in probs]
+    wrhs = [torch.from_numpy(p.rhs()).cuda() for p in probs]
+    for kind in kinds:
+        mag_w.solve_batch(wmus, wrhs, [torch.zeros_like(r) for r in wrhs], [(p.nx, p.ny) for p in probs],
+                          solver=kind, max_iterations=1, preconditioner=net if kind == "learned" else None)
+    del wmus, wrhs
+    torch.cuda.synchronize()
     res = time_solver_kinds(torch, probs, kinds, net, weights)
     base = res["cg"]["seconds"] if "cg" in res else None
     return {"metric": "time-to-1e-10 relative residual (FP64, checked by the oracle's operator), batch of "

@@ -194,11 +194,19 @@ size_t sil_laplacian_plan_scratch_bytes(sil_laplacian_plan plan);
  * 0-form, 2 fused 2D 1-form with TMA-staged tiles, 3 unfused reference chain,
  * 4 fused over stored general-metric Hodge tensors. */
 int sil_laplacian_plan_kernel(sil_laplacian_plan plan);
-/* Pipeline shape of kernel 2 chosen by the autotuner on the plan's first
- * run (-1 before it).  The first run times each shape on the caller's fields
- * and synchronises the stream once; SIMILIE_B200_AUTOTUNE=0 skips the tuning
- * and uses shape 0, SIMILIE_B200_LAP1_VARIANT=<digit> forces a shape. */
+/* Launch shape chosen by the autotuner on the plan's first run (-1 before
+ * it): kernel 2's pipeline shape (6 candidates), kernel 1's block width (64,
+ * 128 or 256 threads: 0, 1, 2).  The first run times each candidate on the
+ * caller's fields and synchronises the stream once; SIMILIE_B200_AUTOTUNE=0
+ * skips the tuning (kernel 2: shape 0, kernel 1: 256 threads),
+ * SIMILIE_B200_LAP1_VARIANT=<digit> forces kernel 2's shape. */
 int sil_laplacian_plan_variant(sil_laplacian_plan plan);
+/* Bound of each pipeline wait of kernel 2, in mbarrier polls (-1: the default,
+ * 4,194,304; 0: every wait runs out at once).  A wait that runs out makes the
+ * kernel stop, let its loads in flight land and return; the plan's error flag
+ * then reports SIL_ERR_BUDGET.  The failure-path tests set a bound of 0; no
+ * counterpart in the reference. */
+sil_status sil_laplacian_plan_set_wait_bound(sil_laplacian_plan plan, int32_t tries);
 /* Synchronising check of the plan's device error flag: SIL_ERR_BUDGET when a
  * bounded wait inside a kernel ran out (the kernel returned early). */
 sil_status sil_laplacian_plan_status(sil_laplacian_plan plan);

@@ -322,6 +322,12 @@ class StagedLaplacian:
     def status(self):
         check(lib().sil_laplacian_plan_status(self._p), "laplacian status")
 
+    def set_wait_bound(self, tries):
+        """Bound of each pipeline wait of the TMA kernel in mbarrier polls (-1:
+        the default; 0: every wait runs out at once, which the failure-path
+        tests use)."""
+        check(lib().sil_laplacian_plan_set_wait_bound(self._p, int(tries)), "laplacian wait bound")
+
     def __del__(self):
         p = getattr(self, "_p", None)
         if p is not None and p.value is not None and _native._lib is not None:

@@ -180,6 +180,7 @@ SIGNATURES = [
     ("sil_laplacian_plan_kernel", ctypes.c_int, [_P]),
     ("sil_laplacian_plan_variant", ctypes.c_int, [_P]),
     ("sil_laplacian_plan_status", ctypes.c_int, [_P]),
+    ("sil_laplacian_plan_set_wait_bound", ctypes.c_int, [_P, ctypes.c_int32]),
     ("sil_laplacian", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_int, _F, _F]),
     ("sil_mag2d_apply", ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, _P, _P]),
     ("sil_mag2d_apply_noalloc", ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, _P, _P]),

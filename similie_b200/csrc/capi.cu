@@ -20,7 +20,10 @@ sil_status launch_add(cudaStream_t, sil_field const&, sil_field const&);
 bool lap2d_layout_ok(sil_field const&, sil_field const&, int);
 bool lap2d_1form_tma_ok(sil_field const&, sil_field const&);
 sil_status launch_lap2d_0form(cudaStream_t, Geometry const&, sil_field const&, sil_field const&);
+sil_status launch_lap2d_0form(cudaStream_t, Geometry const&, sil_field const&, sil_field const&, int);
+sil_status autotune_lap2d_0form(cudaStream_t, Geometry const&, sil_field const&, sil_field const&, int*);
 sil_status launch_lap2d_1form_tma(cudaStream_t, Geometry const&, sil_field const&, sil_field const&, int*, int);
+sil_status launch_lap2d_1form_tma(cudaStream_t, Geometry const&, sil_field const&, sil_field const&, int*, int, int);
 sil_status autotune_lap2d_1form(cudaStream_t, Geometry const&, sil_field const&, sil_field const&, int*, int*, float*);
 
 namespace {
@@ -107,6 +110,7 @@ struct sil_laplacian_plan_s
     sil_field in_like {};
     sil_field out_like {};
     int* error_flag = nullptr;
+    int wait_tries = -1;  // kernel 2's pipeline-wait bound (-1: the default)
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
     sil_field dual_a {}, dual_b {}, codiff {}, cob {};
@@ -342,7 +346,19 @@ sil_status sil_laplacian_run(sil_laplacian_plan plan, sil_stream stream, const s
         return fail(SIL_ERR_INVALID, "sil_laplacian_run: fields differ from the plan's shapes");
     cudaStream_t const s = as_stream(stream);
     switch (plan->kernel) {
-    case 1: return launch_lap2d_0form(s, *plan->geo, *in, *out);
+    case 1: {
+        if (plan->variant < 0) {
+            // First run: time the block widths on these fields (synchronises the stream once).
+            char const* env = std::getenv("SIMILIE_B200_AUTOTUNE");
+            if (env != nullptr && env[0] == '0') {
+                plan->variant = 2;
+            } else {
+                sil_status const st = autotune_lap2d_0form(s, *plan->geo, *in, *out, &plan->variant);
+                if (st != SIL_OK) return st;
+            }
+        }
+        return launch_lap2d_0form(s, *plan->geo, *in, *out, plan->variant);
+    }
     case 2: {
         if (!lap2d_1form_tma_ok(*in, *out)) return launch_fused_laplacian(s, *plan->geo, plan->mask, plan->k, *in, *out);
         if (plan->variant < 0) {
@@ -360,7 +376,7 @@ sil_status sil_laplacian_run(sil_laplacian_plan plan, sil_stream stream, const s
                 if (st != SIL_OK) return st;
             }
         }
-        return launch_lap2d_1form_tma(s, *plan->geo, *in, *out, plan->error_flag, plan->variant);
+        return launch_lap2d_1form_tma(s, *plan->geo, *in, *out, plan->error_flag, plan->variant, plan->wait_tries);
     }
     case 3: return run_unfused(*plan, s, *in, *out);
     case 4: return launch_stored_laplacian(s, plan->hodges, in, out);
@@ -391,6 +407,14 @@ int sil_laplacian_plan_kernel(sil_laplacian_plan plan)
 int sil_laplacian_plan_variant(sil_laplacian_plan plan)
 {
     return plan == nullptr ? -1 : plan->variant;
+}
+
+sil_status sil_laplacian_plan_set_wait_bound(sil_laplacian_plan plan, int32_t tries)
+{
+    if (plan == nullptr) return fail(SIL_ERR_INVALID, "sil_laplacian_plan_set_wait_bound: NULL plan");
+    if (tries < -1) return fail(SIL_ERR_INVALID, "sil_laplacian_plan_set_wait_bound: tries must be >= -1");
+    plan->wait_tries = tries;
+    return SIL_OK;
 }
 
 sil_status sil_laplacian_plan_status(sil_laplacian_plan plan)

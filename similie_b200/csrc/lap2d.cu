@@ -143,6 +143,7 @@ struct Lap1Params
     T const* hy;
     T const* ihy;
     int* error_flag;           // set when a bounded wait runs out
+    int wait_tries;            // bound of each pipeline wait, in mbarrier polls
 };
 
 __device__ __forceinline__ uint32_t smem_addr(void const* p)
@@ -166,11 +167,14 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-// Bounded wait on an mbarrier phase; returns false when the bound runs out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+constexpr int kWaitTries = 1 << 22;
+
+// Bounded wait on an mbarrier phase (at most max_tries polls; 0: the wait
+// runs out at once); returns false when the bound runs out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int max_tries = kWaitTries)
 {
     uint32_t const addr = smem_addr(bar);
-    for (int tries = 0; tries < (1 << 22); ++tries) {
+    for (int tries = 0; tries < max_tries; ++tries) {
         uint32_t done;
         asm volatile(
                 "{\n\t.reg .pred p;\n\t"
@@ -258,7 +262,7 @@ lap2d_1form_tma_kernel(const __grid_constant__ CUtensorMap map_main, const __gri
                 int const slot = static_cast<int>(g % S);
                 uint32_t const use = static_cast<uint32_t>(g / S);
                 if (use > 0) {
-                    bool const got = mbar_wait(&empty[slot], (use - 1) & 1u);
+                    bool const got = mbar_wait(&empty[slot], (use - 1) & 1u, P.wait_tries);
                     if (!__all_sync(0xffffffffu, got) || *reinterpret_cast<volatile int*>(&abort_flag)) {
                         ok = false;
                         break;
@@ -417,7 +421,7 @@ lap2d_1form_tma_kernel(const __grid_constant__ CUtensorMap map_main, const __gri
         for (int st = 0; st < nstages; ++st, ++g) {
             int const slot = static_cast<int>(g % S);
             uint32_t const use = static_cast<uint32_t>(g / S);
-            if (!mbar_wait(&full[slot], use & 1u)) {
+            if (!mbar_wait(&full[slot], use & 1u, P.wait_tries)) {
                 if (lane == 0) {
                     abort_flag = 1;
                     atomicExch(P.error_flag, 1);
@@ -495,12 +499,18 @@ bool lap2d_layout_ok(sil_field const& in, sil_field const& out, int ncomp)
     return in.extent[0] >= 2 && in.extent[1] >= 2;
 }
 
-sil_status launch_lap2d_0form(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out)
+// Block widths the 0-form kernel's tuner chooses from (threads along y).
+constexpr int kLap0Widths[3] = {64, 128, 256};
+constexpr int kLap0Variants = 3;
+
+sil_status launch_lap2d_0form(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
+                              int variant)
 {
     int64_t const mx = out.extent[0], my = out.extent[1];
     if (mx == 0 || my == 0) return SIL_OK;
-    dim3 const block(256);
-    dim3 const grid(static_cast<unsigned>((my + 255) / 256), static_cast<unsigned>(mx));
+    int const bx = kLap0Widths[(variant >= 0 && variant < kLap0Variants) ? variant : kLap0Variants - 1];
+    dim3 const block(bx);
+    dim3 const grid(static_cast<unsigned>((my + bx - 1) / bx), static_cast<unsigned>(mx));
     int64_t const gx = in.front[0] - geo.front[0], gy = in.front[1] - geo.front[1];
     if (in.dtype == SIL_F64) {
         Lap0Params<double> P {static_cast<double const*>(in.data), static_cast<double*>(out.data), in.extent[0],
@@ -517,6 +527,46 @@ sil_status launch_lap2d_0form(cudaStream_t stream, Geometry const& geo, sil_fiel
     }
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
+}
+
+sil_status launch_lap2d_0form(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out)
+{
+    return launch_lap2d_0form(stream, geo, in, out, kLap0Variants - 1);
+}
+
+// Time every block width on the caller's fields (two warm-up and twenty
+// timed launches each, the field stays in L2 as in use) and return the
+// fastest.  Runs on `stream` and synchronises it.
+sil_status autotune_lap2d_0form(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
+                                int* best_variant)
+{
+    cudaEvent_t e0, e1;
+    SIL_CUDA_CHECK(cudaEventCreate(&e0));
+    SIL_CUDA_CHECK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_v = kLap0Variants - 1;
+    sil_status st = SIL_OK;
+    for (int v = 0; v < kLap0Variants && st == SIL_OK; ++v) {
+        for (int i = 0; i < 2 && st == SIL_OK; ++i) st = launch_lap2d_0form(stream, geo, in, out, v);
+        cudaEventRecord(e0, stream);
+        for (int i = 0; i < 20 && st == SIL_OK; ++i) st = launch_lap2d_0form(stream, geo, in, out, v);
+        cudaEventRecord(e1, stream);
+        cudaError_t const err = cudaEventSynchronize(e1);
+        if (err != cudaSuccess) {
+            st = cuda_fail(err, "autotune");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+            best = ms;
+            best_v = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *best_variant = best_v;
+    return st;
 }
 
 // The TMA 1-form kernel additionally needs the output box to stay one node
@@ -553,7 +603,7 @@ int lap1_occupancy()
 
 template <class T, class C>
 sil_status launch_variant(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
-                          int* error_flag, int ctas_per_sm)
+                          int* error_flag, int ctas_per_sm, int wait_tries)
 {
     auto encode = encode_fn();
     if (encode == nullptr) return fail(SIL_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
@@ -589,7 +639,7 @@ sil_status launch_variant(cudaStream_t stream, Geometry const& geo, sil_field co
     Lap1Params<T> P {static_cast<T*>(out.data), out.stride[0], static_cast<int>(nx), static_cast<int>(ny),
                      static_cast<int>(mx), static_cast<int>(my), static_cast<int>(out.front[0] - in.front[0]),
                      static_cast<int>(out.front[1] - in.front[1]), strips, work, gh[0] + gx, gih[0] + gx, gh[1] + gy,
-                     gih[1] + gy, error_flag};
+                     gih[1] + gy, error_flag, wait_tries};
     lap2d_1form_tma_kernel<T, C><<<static_cast<unsigned>(ctas), kThreads1, C::kSmemBytes, stream>>>(map_main, map_halo, P);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
@@ -623,16 +673,16 @@ constexpr int kLap1Variants = 6;
 
 template <class T>
 sil_status launch_by_index(int v, cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
-                           int* error_flag, int ctas_per_sm)
+                           int* error_flag, int ctas_per_sm, int wait_tries)
 {
     using V = Lap1Variants<T>;
     switch (v) {
-    case 0: return launch_variant<T, typename V::V0>(stream, geo, in, out, error_flag, ctas_per_sm);
-    case 1: return launch_variant<T, typename V::V1>(stream, geo, in, out, error_flag, ctas_per_sm);
-    case 2: return launch_variant<T, typename V::V2>(stream, geo, in, out, error_flag, ctas_per_sm);
-    case 3: return launch_variant<T, typename V::V3>(stream, geo, in, out, error_flag, ctas_per_sm);
-    case 4: return launch_variant<T, typename V::V4>(stream, geo, in, out, error_flag, ctas_per_sm);
-    default: return launch_variant<T, typename V::V5>(stream, geo, in, out, error_flag, ctas_per_sm);
+    case 0: return launch_variant<T, typename V::V0>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
+    case 1: return launch_variant<T, typename V::V1>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
+    case 2: return launch_variant<T, typename V::V2>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
+    case 3: return launch_variant<T, typename V::V3>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
+    case 4: return launch_variant<T, typename V::V4>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
+    default: return launch_variant<T, typename V::V5>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
     }
 }
 
@@ -643,14 +693,22 @@ int lap2d_1form_variants()
     return kLap1Variants;
 }
 
-// Launch pipeline variant `variant` (0 = default) of the TMA 1-form kernel.
+// Launch pipeline variant `variant` (0 = default) of the TMA 1-form kernel;
+// wait_tries bounds each pipeline wait (< 0: the default bound).
 sil_status launch_lap2d_1form_tma(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
-                                  int* error_flag, int variant)
+                                  int* error_flag, int variant, int wait_tries)
 {
     if (out.extent[0] == 0 || out.extent[1] == 0) return SIL_OK;
     if (variant < 0 || variant >= kLap1Variants) variant = 0;
-    if (in.dtype == SIL_F64) return launch_by_index<double>(variant, stream, geo, in, out, error_flag, 0);
-    return launch_by_index<float>(variant, stream, geo, in, out, error_flag, 0);
+    int const tries = wait_tries < 0 ? kWaitTries : wait_tries;
+    if (in.dtype == SIL_F64) return launch_by_index<double>(variant, stream, geo, in, out, error_flag, 0, tries);
+    return launch_by_index<float>(variant, stream, geo, in, out, error_flag, 0, tries);
+}
+
+sil_status launch_lap2d_1form_tma(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
+                                  int* error_flag, int variant)
+{
+    return launch_lap2d_1form_tma(stream, geo, in, out, error_flag, variant, -1);
 }
 
 // Time every variant on the caller's fields (two warm-up and three timed

@@ -17,6 +17,7 @@
 // x = 0 with the inverse diagonal as preconditioner, stopped when
 // ||r|| <= tol ||b||; the final residual is re-evaluated in FP64.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -1190,17 +1191,12 @@ sil_status build_divergence_gauge(ProblemDesc const& q, ProbInfo const& pi, doub
 }
 
 template <class T>
-sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings const& set, sil_solve_diagnostics* diag,
-                       cudaStream_t stream, nn::Net* learned = nullptr)
+sil_status solve_batch_rows(std::vector<ProblemDesc> const& probs, sil_solve_settings const& set,
+                            sil_solve_diagnostics* diag, cudaStream_t stream, nn::Net* learned, int item_rows)
 {
     int const np = static_cast<int>(probs.size());
     // Work items: contiguous row ranges of item_rows rows per problem (3D:
     // whole nodes, four thirds of that), one CTA each.
-    int item_rows = kItemNodes;
-    if (char const* e = std::getenv("SIMILIE_B200_ITEM_ROWS")) {
-        int const v = std::atoi(e);
-        if (v >= kThreads && v % kThreads == 0 && v <= 64 * kThreads) item_rows = v;
-    }
     std::vector<Item> items;
     std::vector<ProbInfo> info(np);
     int64_t total_rows = 0;
@@ -1453,6 +1449,9 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
             nn::Workspace* ws = nullptr;
             sil_status lst = net->prepare(samples, stream, &ws);
             if (lst != SIL_OK) return lst;
+            // nu is fixed for the whole solve: the network's log(nu) input is formed once
+            lst = net->set_static_nu(ws, vec_base[6], stream);
+            if (lst != SIL_OK) return lst;
             float const* nuf = vec_base[6];
             float const* dv = vec_base[5];
             float* rv = vec_base[1];
@@ -1577,6 +1576,7 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
             }
             if (lexec != nullptr) cudaGraphExecDestroy(lexec);
             if (lgraph != nullptr) cudaGraphDestroy(lgraph);
+            net->set_static_nu(ws, nullptr, stream);
             *total_out = tot;
             return lst;
         }
@@ -1651,6 +1651,74 @@ sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings
     }
     if (overall != SIL_OK) set_error("a problem of the batch met a non-finite value");
     return overall;
+}
+
+// Work-item size of the batched CG kernels, picked by timing.  The first
+// batch of at least 4 M rows solved in a precision (2D and 3D batches apart)
+// runs a 96-iteration solve with items of 2,048, 4,096 and 8,192 rows and
+// keeps the fastest for the rest of the process (the tuning solves write the
+// caller's solution buffers, which the real solve overwrites).  Smaller
+// batches use 4,096 rows until a large one has been tuned.
+// SIMILIE_B200_ITEM_ROWS=<rows> forces a size; SIMILIE_B200_AUTOTUNE=0 keeps
+// the default.
+constexpr int kItemCandidates[3] = {2048, 4096, 8192};
+std::mutex g_item_mutex;
+int g_item_rows_tuned[4] = {0, 0, 0, 0};  // [precision FP64 / FP32][first problem 2D / 3D]
+
+template <class T>
+sil_status choose_item_rows(std::vector<ProblemDesc> const& probs, sil_solve_settings const& set, cudaStream_t stream,
+                            int* rows)
+{
+    *rows = kItemNodes;
+    if (char const* e = std::getenv("SIMILIE_B200_ITEM_ROWS")) {
+        int const v = std::atoi(e);
+        if (v >= kThreads && v % kThreads == 0 && v <= 64 * kThreads) {
+            *rows = v;
+            return SIL_OK;
+        }
+    }
+    int const key = (sizeof(T) == 8 ? 0 : 2) + (probs.front().dim == 3 ? 1 : 0);
+    {
+        std::lock_guard<std::mutex> lock(g_item_mutex);
+        if (g_item_rows_tuned[key] > 0) {
+            *rows = g_item_rows_tuned[key];
+            return SIL_OK;
+        }
+    }
+    char const* at = std::getenv("SIMILIE_B200_AUTOTUNE");
+    if (at != nullptr && at[0] == '0') return SIL_OK;
+    int64_t total = 0;
+    for (ProblemDesc const& q : probs) total += (q.dim == 3 ? 3 : 1) * q.nx * q.ny * (q.dim == 3 ? q.nz : 1);
+    if (total < (int64_t(1) << 22)) return SIL_OK;
+    sil_solve_settings probe = set;
+    probe.max_iterations = 96;
+    std::vector<sil_solve_diagnostics> scratch(probs.size());
+    double best = 1e300;
+    int best_rows = kItemNodes;
+    for (int c : kItemCandidates) {
+        auto const t0 = std::chrono::steady_clock::now();
+        sil_status const st = solve_batch_rows<T>(probs, probe, scratch.data(), stream, nullptr, c);
+        if (st != SIL_OK) return st;
+        double const sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (sec < best) {
+            best = sec;
+            best_rows = c;
+        }
+    }
+    std::lock_guard<std::mutex> lock(g_item_mutex);
+    g_item_rows_tuned[key] = best_rows;
+    *rows = best_rows;
+    return SIL_OK;
+}
+
+template <class T>
+sil_status solve_batch(std::vector<ProblemDesc> const& probs, sil_solve_settings const& set, sil_solve_diagnostics* diag,
+                       cudaStream_t stream, nn::Net* learned = nullptr)
+{
+    int rows = kItemNodes;
+    sil_status const st = choose_item_rows<T>(probs, set, stream, &rows);
+    if (st != SIL_OK) return st;
+    return solve_batch_rows<T>(probs, set, diag, stream, learned, rows);
 }
 
 } // namespace

@@ -1181,7 +1181,7 @@ __global__ void dots_finish_kernel(double const* part, int nsamples, int nblocks
 // [D^-1/2 r1 / s, log(nu)/log(1000)] over the nodes of each half-resolution
 // pixel (nodes outside the grid count as zero), s = rms(D^-1/2 r1).
 __global__ void features_kernel(const __grid_constant__ Samples ss, const __grid_constant__ Table t, float const* r1,
-                                float const* nu, float const* dinv, double const* dots, float* feat)
+                                float const* nu, float const* dinv, double const* dots, float const* lognu, float* feat)
 {
     __shared__ int64_t pre[kMaxImages + 1];
     __shared__ float inv_rms[kMaxImages];   // 1 / rms(D^-1/2 r1) per sample
@@ -1205,10 +1205,10 @@ __global__ void features_kernel(const __grid_constant__ Samples ss, const __grid
                     if (j >= sm.ny || i >= sm.nx) continue;
                     int64_t const q = sm.offset + j * sm.nx + i;
                     f0 = f0 + r1[q] * sqrtf(dinv[q]) * inv_s;
-                    f1 = f1 + logf(nu[q]) * inv_l;
+                    if (lognu == nullptr) f1 = f1 + logf(nu[q]) * inv_l;
                 }
             f0 = f0 * 0.25f;
-            f1 = f1 * 0.25f;
+            f1 = lognu != nullptr ? lognu[o.offset + g] : f1 * 0.25f;
         }
         feat[2 * (o.offset + g)] = f0;
         feat[2 * (o.offset + g) + 1] = f1;
@@ -1325,11 +1325,13 @@ __device__ __forceinline__ int item_of(Samples const& ss, int64_t const* pre, in
     return ss.item_base[k] + (a - static_cast<int>(pre[k]));
 }
 
-// e1 = w D^-1 r, r1 = r - K e1 (boundary rows: r1 = r - e1), and the partial
-// sums of |D^-1/2 r1|^2 per item.
+// r1 = r - K e1 with e1 = w D^-1 r formed on the fly at the row and its
+// neighbours (boundary rows: r1 = r - e1), and the partial sums of
+// |D^-1/2 r1|^2 per item.  A thread's (i, j) advance by adding, without a
+// division per node.
 __global__ void __launch_bounds__(256) wrap_pre_kernel(const __grid_constant__ Samples ss, WrapItem const* items,
                                                        float const* nu, float const* dinv, float const* r,
-                                                       float* e1, float* r1, double* part)
+                                                       float* r1, double* part)
 {
     __shared__ double red[8];
     __shared__ int64_t pre[kMaxImages + 1];
@@ -1344,15 +1346,20 @@ __global__ void __launch_bounds__(256) wrap_pre_kernel(const __grid_constant__ S
         float const* r_s = r + sm.offset;
         auto e = [&](int q, int, int) { return kOmega * (d_s[q] * r_s[q]); };
         double acc = 0.0;
-        for (int row = it.begin + threadIdx.x; row < it.end; row += blockDim.x) {
-            int const j = row / nx, i = row - j * nx;
+        int row = it.begin + static_cast<int>(threadIdx.x);
+        int j = row / nx, i = row - j * nx;
+        for (; row < it.end; row += blockDim.x) {
             float const ev = e(row, i, j);
             float v;
             if (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) v = r_s[row] - ev;
             else v = r_s[row] - k_row(e, nu_s, nx, row, i, j);
-            e1[sm.offset + row] = ev;
             r1[sm.offset + row] = v;
             acc += static_cast<double>(d_s[row]) * static_cast<double>(v) * static_cast<double>(v);
+            i += blockDim.x;
+            while (i >= nx) {
+                i -= nx;
+                ++j;
+            }
         }
         double const t = block_sum_d(acc, red);
         if (threadIdx.x == 0) part[item] = t;
@@ -1391,44 +1398,97 @@ __device__ __forceinline__ void stage_rms(Samples const& ss, double const* dots,
         sc[k] = static_cast<float>(sqrt(dots[k * 3] / (static_cast<double>(ss.s[k].nx) * ss.s[k].ny)));
 }
 
-// e2 = e1 + s D^-1/2 up(unet) at interior nodes, e1 on the boundary.
-__global__ void __launch_bounds__(256) wrap_e2_kernel(const __grid_constant__ Samples ss, float const* dinv,
-                                                      float const* e1, float const* unet, double const* dots,
-                                                      float* e2)
+// e2 = w D^-1 r + s D^-1/2 up(unet) at interior nodes (w D^-1 r on the
+// boundary), s = rms of the sample's D^-1/2 r1.  Items as wrap_pre.
+__global__ void __launch_bounds__(256) wrap_e2_kernel(const __grid_constant__ Samples ss, WrapItem const* items,
+                                                      float const* dinv, float const* r, float const* unet,
+                                                      double const* dots, float* e2)
 {
     __shared__ int64_t pre[kMaxImages + 1];
     __shared__ float sc[kMaxImages];
     stage_rms(ss, dots, sc);
-    walk_nodes(ss, pre, [&](int k, int row) {
+    int const nact = scan_items(ss, pre);
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
+        WrapItem const it = items[item_of(ss, pre, a)];
+        int const k = it.sample;
         Sample const sm = ss.s[k];
         int const nx = sm.nx, ny = sm.ny;
-        int const j = row / nx, i = row - j * nx;
-        int64_t const q = sm.offset + row;
-        float v = e1[q];
-        if (!(i == 0 || j == 0 || i + 1 == nx || j + 1 == ny)) {
-            Img const o = ss.top[k];
-            v = v + sc[k] * sqrtf(dinv[q]) * unet[o.offset + (j / 2 + 1) * (o.w + 2) + (i / 2 + 1)];
+        float const* d_s = dinv + sm.offset;
+        float const* r_s = r + sm.offset;
+        Img const o = ss.top[k];
+        float const* un = unet + o.offset;
+        int const P = o.w + 2;
+        float const s_k = sc[k];
+        int row = it.begin + static_cast<int>(threadIdx.x);
+        int j = row / nx, i = row - j * nx;
+        for (; row < it.end; row += blockDim.x) {
+            float v = kOmega * (d_s[row] * r_s[row]);
+            if (!(i == 0 || j == 0 || i + 1 == nx || j + 1 == ny))
+                v = v + s_k * sqrtf(d_s[row]) * un[(j / 2 + 1) * P + (i / 2 + 1)];
+            e2[sm.offset + row] = v;
+            i += blockDim.x;
+            while (i >= nx) {
+                i -= nx;
+                ++j;
+            }
         }
-        e2[q] = v;
-    });
+    }
 }
 
-// M(r) = e2 + w D^-1 (r - K e2) (boundary rows: K e2 -> e2).
-__global__ void __launch_bounds__(256) wrap_post_kernel(const __grid_constant__ Samples ss, float const* nu,
-                                                        float const* dinv, float const* r, float const* e2,
-                                                        float* out)
+// M(r) = e2 + w D^-1 (r - K e2) (boundary rows: K e2 -> e2).  Items as wrap_pre.
+__global__ void __launch_bounds__(256) wrap_post_kernel(const __grid_constant__ Samples ss, WrapItem const* items,
+                                                        float const* nu, float const* dinv, float const* r,
+                                                        float const* e2, float* out)
 {
     __shared__ int64_t pre[kMaxImages + 1];
-    walk_nodes(ss, pre, [&](int k, int row) {
-        Sample const sm = ss.s[k];
+    int const nact = scan_items(ss, pre);
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
+        WrapItem const it = items[item_of(ss, pre, a)];
+        Sample const sm = ss.s[it.sample];
         int const nx = sm.nx, ny = sm.ny;
-        int const j = row / nx, i = row - j * nx;
         float const* e_s = e2 + sm.offset;
+        float const* d_s = dinv + sm.offset;
+        float const* r_s = r + sm.offset;
         auto e = [&](int q, int, int) { return e_s[q]; };
-        float const e0 = e_s[row];
-        float const ke = (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) ? e0 : k_row(e, nu + sm.offset, nx, row, i, j);
-        int64_t const q = sm.offset + row;
-        out[q] = e0 + kOmega * (dinv[q] * (r[q] - ke));
+        int row = it.begin + static_cast<int>(threadIdx.x);
+        int j = row / nx, i = row - j * nx;
+        for (; row < it.end; row += blockDim.x) {
+            float const e0 = e_s[row];
+            float const ke = (i == 0 || j == 0 || i + 1 == nx || j + 1 == ny) ? e0
+                                                                                : k_row(e, nu + sm.offset, nx, row, i, j);
+            out[sm.offset + row] = e0 + kOmega * (d_s[row] * (r_s[row] - ke));
+            i += blockDim.x;
+            while (i >= nx) {
+                i -= nx;
+                ++j;
+            }
+        }
+    }
+}
+
+// log(nu) / log(1000), pooled 2 x 2 onto the top-level image of every sample
+// (the network's second input channel; zero on the image border).
+__global__ void lognu_feature_kernel(const __grid_constant__ Samples ss, const __grid_constant__ Table t, float const* nu,
+                                     float* lognu)
+{
+    __shared__ int64_t pre[kMaxImages + 1];
+    float const inv_l = static_cast<float>(1.0 / log(1000.0));
+    walk_active(t, pre, 1, [&](int im, int g) {
+        Sample const sm = ss.s[t.sample[im]];
+        Img const o = t.img[im];
+        int const P = o.w + 2;
+        int const y = g / P, x = g - y * P;
+        float f1 = 0.0f;
+        if (!(y == 0 || x == 0 || y > o.h || x > o.w)) {
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b) {
+                    int64_t const j = 2 * (y - 1) + a, i = 2 * (x - 1) + b;
+                    if (j >= sm.ny || i >= sm.nx) continue;
+                    f1 = f1 + logf(nu[sm.offset + j * sm.nx + i]) * inv_l;
+                }
+            f1 = f1 * 0.25f;
+        }
+        lognu[o.offset + g] = f1;
     });
 }
 
@@ -1485,7 +1545,9 @@ public:
     std::vector<int> depth;        // levels per sample
     Samples ss {};
     // node-level FP32 vectors
-    DevBuf dinv, e1, r1, e2, u, ku, tmp, gu, ge2;
+    DevBuf dinv, r1, e2, u, ku, tmp, gu, ge2;
+    DevBuf lognu;                  // top-level log(nu) feature channel of a fixed nu (set_static_nu)
+    float const* lognu_for = nullptr;  // the nu it was formed from (NULL: none)
     DevBuf dparts;                 // per-sample dot partials
     DevBuf dots;                   // [3 sets][nsamples][3]
     int dot_blocks = 0;
@@ -1554,7 +1616,7 @@ sil_status Workspace::build(std::vector<Sample> const& s)
     }
     for (int i = 0; i < n; ++i) ss.top[i] = levels[0].img[i];
     size_t const nb = static_cast<size_t>(nodes) * sizeof(float);
-    for (DevBuf* b : {&dinv, &e1, &r1, &e2, &u, &ku, &tmp, &gu, &ge2}) {
+    for (DevBuf* b : {&dinv, &r1, &e2, &u, &ku, &tmp, &gu, &ge2}) {
         sil_status const st = b->alloc(nb);
         if (st != SIL_OK) return st;
     }
@@ -1650,9 +1712,9 @@ bool g_attr_done = false;
 int g_sms = 0;  // multiprocessor count, read once (outside any stream capture)
 int g_conv_per_sm[5] = {0, 0, 0, 0, 0};  // resident conv CTAs per SM, by input mode
 // Grid-stride kernels of the forward pass and their resident blocks per SM.
-enum WalkKind { kWalkInc = 0, kWalkOut, kWalkGather, kWalkPool, kWalkCopy, kWalkFeat, kWalkPre, kWalkPost, kWalkE2,
-                kWalkKinds };
-int g_walk_per_sm[kWalkKinds] = {1, 1, 1, 1, 1, 1, 1, 1, 1};
+enum WalkKind { kWalkInc = 0, kWalkOut, kWalkGather, kWalkPool, kWalkCopy, kWalkFeat, kWalkPre, kWalkPost, kWalkLogNu,
+                kWalkE2, kWalkKinds };
+int g_walk_per_sm[kWalkKinds] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
 
 sil_status ensure_attributes()
 {
@@ -1687,7 +1749,7 @@ sil_status ensure_attributes()
         reinterpret_cast<void const*>(out_gather_kernel),  reinterpret_cast<void const*>(pool_kernel),
         reinterpret_cast<void const*>(copy_act_kernel),    reinterpret_cast<void const*>(features_kernel),
         reinterpret_cast<void const*>(wrap_pre_kernel),    reinterpret_cast<void const*>(wrap_post_kernel),
-        reinterpret_cast<void const*>(wrap_e2_kernel)};
+        reinterpret_cast<void const*>(lognu_feature_kernel), reinterpret_cast<void const*>(wrap_e2_kernel)};
     for (int k = 0; k < kWalkKinds; ++k) {
         cudaFuncAttributes a {};
         SIL_CUDA_CHECK(cudaFuncGetAttributes(&a, walk_fns[k]));
@@ -1724,12 +1786,6 @@ unsigned item_grid(int nitems, int kind)
     return static_cast<unsigned>(std::max(1, std::min(nitems, 4 * g_walk_per_sm[kind] * (g_sms > 0 ? g_sms : 148))));
 }
 
-unsigned node_walk_grid(Workspace const& w, int kind)
-{
-    int64_t const chunks = (w.nodes + 255) / 256;
-    int64_t const wave = 4 * static_cast<int64_t>(g_walk_per_sm[kind]) * (g_sms > 0 ? g_sms : 148);
-    return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(chunks, wave)));
-}
 
 // 1024-byte aligned dynamic shared memory: the kernels index from the start
 // of the dynamic block, which the runtime aligns to at least 1024 bytes when
@@ -2083,21 +2139,20 @@ sil_status precond_forward(Net& net, Workspace& w, float const* nu, float const*
     }
     WrapItem const* items = w.witems.as<WrapItem>();
     Table const t0 = w.table(0, -1, false);
-    wrap_pre_kernel<<<item_grid(w.nwitems, kWalkPre), 256, 0, st>>>(w.ss, items, nu, dinv, b, w.e1.as<float>(),
-                                                          w.r1.as<float>(),
-                                               w.wpart.as<double>());
+    wrap_pre_kernel<<<item_grid(w.nwitems, kWalkPre), 256, 0, st>>>(w.ss, items, nu, dinv, b, w.r1.as<float>(),
+                                                                    w.wpart.as<double>());
     wrap_finish_kernel<<<static_cast<unsigned>(w.samples.size()), 32, 0, st>>>(w.ss, w.wpart.as<double>(),
                                                                                 w.dots.as<double>());
     SIL_CUDA_CHECK(cudaGetLastError());
+    float const* lognu = (w.lognu_for != nullptr && w.lognu_for == nu) ? w.lognu.as<float>() : nullptr;
     features_kernel<<<walk_grid(t0, 1, kWalkFeat), 256, 0, st>>>(w.ss, t0, w.r1.as<float>(), nu, dinv, w.dots.as<double>(),
-                                                 w.feat.as<float>());
+                                                                 lognu, w.feat.as<float>());
     SIL_CUDA_CHECK(cudaGetLastError());
     sil_status s = net_forward(net, w, st, keep);
     if (s != SIL_OK) return s;
-    unsigned const ng = node_walk_grid(w, kWalkE2);
-    wrap_e2_kernel<<<ng, 256, 0, st>>>(w.ss, dinv, w.e1.as<float>(), w.unet.as<float>(), w.dots.as<double>(),
-                                       w.e2.as<float>());
-    wrap_post_kernel<<<node_walk_grid(w, kWalkPost), 256, 0, st>>>(w.ss, nu, dinv, b, w.e2.as<float>(), out);
+    wrap_e2_kernel<<<item_grid(w.nwitems, kWalkE2), 256, 0, st>>>(w.ss, items, dinv, b, w.unet.as<float>(),
+                                                                  w.dots.as<double>(), w.e2.as<float>());
+    wrap_post_kernel<<<item_grid(w.nwitems, kWalkPost), 256, 0, st>>>(w.ss, items, nu, dinv, b, w.e2.as<float>(), out);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
@@ -2130,6 +2185,22 @@ sil_status Net::prepare(std::vector<Sample> const& samples, cudaStream_t stream,
     sil_status st = SIL_OK;
     *out = workspace(samples, stream, &st);
     return *out == nullptr ? st : SIL_OK;
+}
+
+sil_status Net::set_static_nu(Workspace* w, float const* nu, cudaStream_t stream)
+{
+    w->lognu_for = nullptr;
+    if (nu == nullptr) return SIL_OK;
+    if (w->lognu.p == nullptr) {
+        if (sil_status st = w->lognu.alloc(sizeof(float) * w->levels[0].npx); st != SIL_OK) return st;
+    }
+    w->active = nullptr;
+    w->ss.active = nullptr;
+    Table const t0 = w->table(0, -1, false);
+    lognu_feature_kernel<<<walk_grid(t0, 1, kWalkLogNu), 256, 0, stream>>>(w->ss, t0, nu, w->lognu.as<float>());
+    SIL_CUDA_CHECK(cudaGetLastError());
+    w->lognu_for = nu;
+    return SIL_OK;
 }
 
 sil_status Net::forward(Workspace* w, float const* nu, float const* dinv, float const* r, float* out,

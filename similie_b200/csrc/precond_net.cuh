@@ -77,6 +77,11 @@ public:
 
     // Workspace of a batch geometry (allocated once, before any stream capture).
     sil_status prepare(std::vector<Sample> const& samples, cudaStream_t stream, Workspace** out);
+    // Declare nu (device, FP32 per node) fixed for the forward passes that
+    // follow on this workspace: the log(nu) input channel is formed once and
+    // reused while forward() is given the same nu pointer; NULL ends it.  A
+    // caller that changes nu in place must call this again.
+    sil_status set_static_nu(Workspace* w, float const* nu, cudaStream_t stream);
     // out = M(r) on a prepared workspace: kernel launches only (capturable).
     // dinv: inverse operator diagonal per node (FP32), or NULL.  active
     // (device, one int per sample, or NULL): samples whose entry is 0 at

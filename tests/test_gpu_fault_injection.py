@@ -2,7 +2,10 @@
 GPU: a non-finite value in a right-hand side, an iteration budget of one,
 and a zero right-hand side, for the batched, assembled and nonlinear solves.
 Every solve returns, and reports the failure in its status and diagnostics
-(per problem for a batch) while the other problems of the batch finish."""
+(per problem for a batch) while the other problems of the batch finish.
+The TMA Laplacian's pipeline waits are given a bound of zero polls, so they
+run out: the kernel stops, lets its loads in flight land and returns, the
+plan reports SIL_ERR_BUDGET and the context stays usable."""
 import ctypes
 
 import numpy as np
@@ -11,6 +14,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SIL_OK, SIL_ERR_NONFINITE = 0, 5
+SIL_ERR_BUDGET = 7
 
 
 @pytest.fixture(scope="module")
@@ -86,3 +90,30 @@ def test_nonlinear_solve_reports_nonfinite(torch):
     x = torch.zeros(33 * 33, dtype=torch.float64, device="cuda")
     d = mag.nl_solve_batch([_dev(torch, mu)], [_dev(torch, fe)], [(b, h)], [_dev(torch, rhs)], [x], [(33, 33)])
     assert d[0].status == SIL_ERR_NONFINITE and not d[0].converged and d[0].refinements == 0
+
+
+def test_laplacian_wait_that_runs_out_reports_budget(torch):
+    import oracle as O
+    import similie_b200 as sil
+    from helpers import gaussian_random_field, rel_err
+    n = 512
+    w = gaussian_random_field(n, seed=5)
+    coords = [np.arange(n) / n, np.arange(n) / n]
+    geo = sil.Geometry(coords)
+    inp = torch.from_numpy(w).cuda()
+    out = torch.zeros((n - 1, n - 1, 2), dtype=torch.float64, device="cuda")
+    bad = sil.make_staged_laplacian(geo, out, inp, 1)
+    assert bad.kernel == 2
+    bad.run(out, inp)           # first run: the pipeline shape is tuned with the default bound
+    bad.status()
+    bad.set_wait_bound(0)
+    bad.run(out, inp)
+    with pytest.raises(sil.SilError) as e:
+        bad.status()
+    assert e.value.status == SIL_ERR_BUDGET
+    # the context is still usable: a fresh plan computes the right Laplacian
+    good = sil.make_staged_laplacian(geo, out, inp, 1)
+    good.run(out, inp)
+    good.status()
+    ref = O.laplacian(2, 1, O.position_from_coords(coords), w)
+    assert rel_err(out.cpu().numpy(), ref) <= 1e-12
