@@ -616,15 +616,16 @@ __global__ void __launch_bounds__(kThreads) cg_dir_apply_kernel(Item const* item
     auto dir = [&](int idx) -> T { return z[idx] + beta * pold[idx]; };
     double pq = 0.0;
     if (pi.dim == 3) {
+        // 3D: the direction was formed by cg_direction3_kernel (the curl-curl
+        // stencil reads each operand many times, so forming it on the fly
+        // would double those loads)
         for (int64_t node = it.begin / 3 + threadIdx.x; node < it.end / 3; node += kThreads) {
             T q[3];
-            mag3d_apply_node_ld<T, G>(dir, v.nu, pi, static_cast<int>(node), q);
+            mag3d_apply_node<T, G>(pnew, v.nu, pi, static_cast<int>(node), q);
             for (int cc = 0; cc < 3; ++cc) {
                 int const row = static_cast<int>(3 * node + cc);
-                T const pr = dir(row);
-                pnew[row] = pr;
                 v.q[row] = q[cc];
-                pq += static_cast<double>(pr) * static_cast<double>(q[cc]);
+                pq += static_cast<double>(pnew[row]) * static_cast<double>(q[cc]);
             }
         }
     } else {
@@ -651,6 +652,22 @@ __global__ void __launch_bounds__(kThreads) cg_dir_apply_kernel(Item const* item
         s->alpha = s->rz / tot;
         if (!isfinite(s->alpha)) s->nonfinite = 1;
     }
+}
+
+// p = z + beta p_old into the other direction buffer, for the 3D problems of
+// the batch (2D problems form it inside cg_dir_apply_kernel).
+template <class T>
+__global__ void __launch_bounds__(kThreads) cg_direction3_kernel(Item const* items, int const* act, ProbInfo const* info,
+                                                                 Vecs<T> const* vecs, Scalars const* sc)
+{
+    Item const it = items[act[blockIdx.x]];
+    Scalars const* s = sc + it.prob;
+    if (s->done || s->outer_done || info[it.prob].dim != 3) return;
+    Vecs<T> const v = vecs[it.prob];
+    T const* pold = s->pbuf == 0 ? v.p : v.p2;
+    T* pnew = s->pbuf == 0 ? v.p2 : v.p;
+    T const beta = static_cast<T>(s->beta);
+    for (int64_t row = it.begin + threadIdx.x; row < it.end; row += kThreads) pnew[row] = v.z[row] + beta * pold[row];
 }
 
 template <class T>
@@ -1383,6 +1400,7 @@ sil_status solve_batch_rows(std::vector<ProblemDesc> const& probs, sil_solve_set
     std::vector<int> open_host;
     open_host.reserve(nitems);
     int captured_n = -1;
+    bool const any3d = std::any_of(probs.begin(), probs.end(), [](ProblemDesc const& q) { return q.dim == 3; });
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     auto build_open = [&]() {
@@ -1401,6 +1419,7 @@ sil_status solve_batch_rows(std::vector<ProblemDesc> const& probs, sil_solve_set
         SIL_CUDA_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
         cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         for (int c = 0; c < chunk && err == cudaSuccess; ++c) {
+            if (any3d) cg_direction3_kernel<T><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc);
             if (any_gauge) cg_dir_apply_kernel<T, true><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_a);
             else cg_dir_apply_kernel<T, false><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_a);
             cg_update_kernel<T><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_b, part_c);

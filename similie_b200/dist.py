@@ -52,3 +52,16 @@ def gather_to_rank0(obj):
     out = [None] * dist.get_world_size() if dist.get_rank() == 0 else None
     dist.gather_object(obj, out, dst=0)
     return out
+
+
+def merge_records(gathered, sum_keys, max_keys):
+    """Per-kind records of every rank (rank 0's gather_to_rank0 result, a list
+    of {kind: {key: value}}) merged into rank 0's: the keys of sum_keys added
+    over ranks, those of max_keys maximised; other keys keep rank 0's value."""
+    out = {kind: dict(rec) for kind, rec in gathered[0].items()}
+    for kind, rec in out.items():
+        for key in sum_keys:
+            rec[key] = sum(g[kind][key] for g in gathered)
+        for key in max_keys:
+            rec[key] = max(g[kind][key] for g in gathered)
+    return out
