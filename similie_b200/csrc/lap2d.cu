@@ -17,6 +17,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <mutex>
 
 #include "sil_internal.cuh"
@@ -448,6 +449,298 @@ lap2d_1form_tma_kernel(const __grid_constant__ CUtensorMap map_main, const __gri
     }
 }
 
+// ------------------------------------------------------------------ 1-form, TMA, column pairs (FP64)
+//
+// The same pipeline over 512-column strips: each consumer thread owns two
+// adjacent columns A = 2t, B = 2t + 1 and reads the four columns A-1..B+1 of
+// a row from shared memory.  Every value the two columns have in common is
+// formed once (the Hodge-factor products of columns A and B, the star of the
+// 1-form at A and B, eta at A, and delta(r-1, B), which is column A's
+// delta_up), so a row costs about two thirds of the single-column kernel's
+// instructions per output node, and the two columns' dependency chains
+// interleave.  Each shared value is the same expression, in the same order,
+// as the single-column kernel evaluates it, so the outputs are bit-identical.
+
+constexpr int kTJ2 = 512;               // output columns per strip
+constexpr int kQuarter = 128;           // nodes per TMA box row (one quarter strip)
+
+template <int ROWS, int STAGES>
+struct Lap1PairCfg
+{
+    static constexpr int kRows = ROWS;
+    static constexpr int kStages = STAGES;
+    static constexpr int kQuarterBytes = ROWS * kQuarter * 16;      // FP64: 16 B per node (2 components)
+    static constexpr int kHaloBytes = ROWS * 16;
+    static constexpr int kHaloPad = (kHaloBytes + 127) / 128 * 128;
+    static constexpr int kOffL = 4 * kQuarterBytes;
+    static constexpr int kOffR = kOffL + kHaloPad;
+    static constexpr int kOffF = kOffR + kHaloPad;
+    static constexpr int kStageStride = (kOffF + ROWS * 16 + 127) / 128 * 128;
+    static constexpr int kTxBytes = 4 * kQuarterBytes + 2 * kHaloBytes;
+    static constexpr int kSmemBytes = STAGES * kStageStride + 128;
+};
+
+template <class C>
+__global__ void __launch_bounds__(kThreads1, 1)
+lap2d_1form_pair_kernel(const __grid_constant__ CUtensorMap map_main, const __grid_constant__ CUtensorMap map_halo,
+                        Lap1Params<double> P)
+{
+    using Vec = double2;
+    constexpr int R = C::kRows;
+    constexpr int S = C::kStages;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* stages = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t empty[S];
+    __shared__ int abort_flag;
+
+    int const tid = threadIdx.x;
+    int const warp = tid / 32, lane = tid % 32;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kConsumerWarps);
+        }
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+
+    int64_t const begin = (P.work * blockIdx.x) / gridDim.x;
+    int64_t const end = (P.work * (blockIdx.x + 1)) / gridDim.x;
+
+    if (warp == kConsumerWarps) {
+        // ---------------- producer warp: TMA loads + row factors
+        int64_t g = 0;
+        bool ok = true;
+        int64_t item = begin;
+        while (item < end && ok) {
+            Segment const sg = next_segment(P, item, end);
+            int const col0 = P.oy + sg.strip * kTJ2;
+            int const load_row0 = P.ox + sg.r_begin - 1;
+            int const nload = sg.r_end - sg.r_begin + 2;
+            int const nstages = (nload + R - 1) / R;
+            for (int st = 0; st < nstages; ++st, ++g) {
+                int const slot = static_cast<int>(g % S);
+                uint32_t const use = static_cast<uint32_t>(g / S);
+                if (use > 0) {
+                    bool const got = mbar_wait(&empty[slot], (use - 1) & 1u, P.wait_tries);
+                    if (!__all_sync(0xffffffffu, got) || *reinterpret_cast<volatile int*>(&abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                }
+                unsigned char* stage = stages + slot * C::kStageStride;
+                int const row0 = load_row0 + st * R;
+                if (lane < R) {
+                    int const idx = min(row0 + lane + 1, P.nx + 1);
+                    double* fac = reinterpret_cast<double*>(stage + C::kOffF);
+                    fac[2 * lane] = __ldg(P.hx + idx);
+                    fac[2 * lane + 1] = __ldg(P.ihx + idx);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_expect_tx(&full[slot], C::kTxBytes);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        tma_load_2d(stage + q * C::kQuarterBytes, &map_main, &full[slot], 2 * (col0 + q * kQuarter), row0);
+                    tma_load_2d(stage + C::kOffL, &map_halo, &full[slot], 2 * (col0 - 1), row0);
+                    tma_load_2d(stage + C::kOffR, &map_halo, &full[slot], 2 * (col0 + kTJ2), row0);
+                }
+            }
+        }
+        if (!ok && lane == 0) {
+            abort_flag = 1;
+            atomicExch(P.error_flag, 1);
+            for (int64_t q = max(g - S, int64_t(0)); q < g; ++q)
+                mbar_wait(&full[q % S], static_cast<uint32_t>(q / S) & 1u);
+        }
+        return;
+    }
+
+    // ---------------- consumer warps: columns A = 2 tid, B = 2 tid + 1 of the strip
+    constexpr int kQV = C::kQuarterBytes / 16;  // Vecs per quarter block
+    int const q = tid / 64, c0 = 2 * (tid % 64);
+    int const oA = q * kQV + c0;
+    int m_off, m_stride, p_off, p_stride;
+    if (c0 > 0) {
+        m_off = oA - 1;
+        m_stride = kQuarter;
+    } else if (q > 0) {
+        m_off = (q - 1) * kQV + kQuarter - 1;
+        m_stride = kQuarter;
+    } else {
+        m_off = C::kOffL / 16;
+        m_stride = 1;
+    }
+    if (c0 + 1 < kQuarter - 1) {
+        p_off = oA + 2;
+        p_stride = kQuarter;
+    } else if (q < 3) {
+        p_off = (q + 1) * kQV;
+        p_stride = kQuarter;
+    } else {
+        p_off = C::kOffR / 16;
+        p_stride = 1;
+    }
+
+    int64_t g = 0;
+    int64_t item = begin;
+    while (item < end) {
+        Segment const sg = next_segment(P, item, end);
+        int const col0 = P.oy + sg.strip * kTJ2;
+        int const jA = col0 + 2 * tid;
+        int const i_first = P.ox + sg.r_begin;
+        int const nload = sg.r_end - sg.r_begin + 2;
+        int const nstages = (nload + R - 1) / R;
+
+        // Column constants from A's clamped index: columns past the output
+        // are never stored, and a stored column sees exactly the factors the
+        // single-column kernel gives it.
+        int const jq = min(jA, P.ny - 2);
+        double const ihy_M = __ldg(P.ihy + jq);
+        double const hy_A = __ldg(P.hy + jq + 1), ihy_A = __ldg(P.ihy + jq + 1);
+        double const hy_B = __ldg(P.hy + jq + 2), ihy_B = __ldg(P.ihy + jq + 2);
+        double const hy_P = __ldg(P.hy + jq + 3), ihy_P = __ldg(P.ihy + jq + 3);
+        bool const storeA = jA < P.oy + P.my;
+        bool const storeB = jA + 1 < P.oy + P.my;
+
+        double a_M = 0, b_M = 0, a_A = 0, b_A = 0, a_B = 0, b_B = 0, a_P = 0;   // components at row r-1
+        double xy_A = 0, xx_A = 0, xy_B = 0, xx_B = 0, xy_P = 0, xx_P = 0;     // star at row r-1
+        double xyB_prev = 0, xyP_prev = 0;                                    // xi_y at row r-2
+        double sA_prev = 0, sM_prev = 0, sB_prev = 0, sP_prev = 0;            // 1/(hx hy) at row r-1
+        double pxA_prev = 0, qyA_prev = 0, pxB_prev = 0, qyB_prev = 0;        // hx/hy, hy/hx at row r-1
+        double etaA_prev = 0, etaB_prev = 0;                                  // eta at row r-2
+        double dA_prev = 0, dB_prev = 0;                                      // delta at row r-1
+        int out_after = 2;
+        Vec* optr = reinterpret_cast<Vec*>(P.out + static_cast<int64_t>(i_first - P.ox) * P.out_row) + (jA - P.oy);
+        int64_t const ostep = P.out_row / 2;
+
+        auto row_step = [&](Vec const vM, Vec const vA, Vec const vB, Vec const vP, double const hx_r,
+                            double const ihx_r) {
+            double const px_M = hx_r * ihy_M;
+            double const qy_A = ihx_r * hy_A;
+            double const px_A = hx_r * ihy_A;
+            double const qy_B = ihx_r * hy_B;
+            double const px_B = hx_r * ihy_B;
+            double const s_A = ihx_r * ihy_A;
+            double const s_M = ihx_r * ihy_M;
+            double const s_B = ihx_r * ihy_B;
+            double const qy_P = ihx_r * hy_P;
+            double const px_P = hx_r * ihy_P;
+            double const s_P = ihx_r * ihy_P;
+            double const nxx_M = -(px_M * vM.y);
+            double const nxy_A = qy_A * vA.x;
+            double const nxx_A = -(px_A * vA.y);
+            double const nxy_B = qy_B * vB.x;
+            double const nxx_B = -(px_B * vB.y);
+            double const nxy_P = qy_P * vP.x;
+            double const nxx_P = -(px_P * vP.y);
+            // eta at row r-1: columns A, A-1 (A's eta_m) and B (B's eta_m is eta at A)
+            double const d0A = (((-b_A) + a_A) + vA.y) - a_B;
+            double const etaA = sA_prev * d0A;
+            double const dmA = (((-b_M) + a_M) + vM.y) - a_A;
+            double const etaM = sM_prev * dmA;
+            double const d0B = (((-b_B) + a_B) + vB.y) - a_P;
+            double const etaB = sB_prev * d0B;
+            // delta(r, A), delta(r, B), and delta(r-1, B+1) (B's delta_up); A's
+            // delta_up is delta(r-1, B) = dB_prev
+            double const accA = (((-nxy_A) + nxx_A) + xy_A) - nxx_M;
+            double const dA = s_A * accA;
+            double const accB = (((-nxy_B) + nxx_B) + xy_B) - nxx_A;
+            double const dB = s_B * accB;
+            double const acc2B = (((-xy_P) + xx_P) + xyP_prev) - xx_B;
+            double const dupB = sP_prev * acc2B;
+            if (out_after == 0) {
+                Vec o;
+                {
+                    double const sx = (-etaA) + etaA_prev;
+                    double const sy = (-etaA) + etaM;
+                    double const ddx = -(pxA_prev * sy);
+                    double const ddy = qyA_prev * sx;
+                    double const ex = (-dA_prev) + dA;
+                    double const ey = (-dA_prev) + dB_prev;
+                    o.x = ddx + ex;
+                    o.y = ddy + ey;
+                    if (storeA) __stcs(optr, o);
+                }
+                {
+                    double const sx = (-etaB) + etaB_prev;
+                    double const sy = (-etaB) + etaA;
+                    double const ddx = -(pxB_prev * sy);
+                    double const ddy = qyB_prev * sx;
+                    double const ex = (-dB_prev) + dB;
+                    double const ey = (-dB_prev) + dupB;
+                    o.x = ddx + ex;
+                    o.y = ddy + ey;
+                    if (storeB) __stcs(optr + 1, o);
+                }
+                optr += ostep;
+            } else {
+                --out_after;
+            }
+            etaA_prev = etaA;
+            etaB_prev = etaB;
+            dA_prev = dA;
+            dB_prev = dB;
+            xyB_prev = xy_B;
+            xyP_prev = xy_P;
+            xy_A = nxy_A;
+            xx_A = nxx_A;
+            xy_B = nxy_B;
+            xx_B = nxx_B;
+            xy_P = nxy_P;
+            xx_P = nxx_P;
+            sA_prev = s_A;
+            sM_prev = s_M;
+            sB_prev = s_B;
+            sP_prev = s_P;
+            pxA_prev = px_A;
+            qyA_prev = qy_A;
+            pxB_prev = px_B;
+            qyB_prev = qy_B;
+            a_M = vM.x;
+            b_M = vM.y;
+            a_A = vA.x;
+            b_A = vA.y;
+            a_B = vB.x;
+            b_B = vB.y;
+            a_P = vP.x;
+        };
+
+        for (int st = 0; st < nstages; ++st, ++g) {
+            int const slot = static_cast<int>(g % S);
+            uint32_t const use = static_cast<uint32_t>(g / S);
+            if (!mbar_wait(&full[slot], use & 1u, P.wait_tries)) {
+                if (lane == 0) {
+                    abort_flag = 1;
+                    atomicExch(P.error_flag, 1);
+                }
+                return;
+            }
+            Vec const* sv = reinterpret_cast<Vec const*>(stages + slot * C::kStageStride);
+            Vec const* pm = sv + m_off;
+            Vec const* pa = sv + oA;
+            Vec const* pp = sv + p_off;
+            double const* fac = reinterpret_cast<double const*>(stages + slot * C::kStageStride + C::kOffF);
+            int const rows_here = min(R, nload - st * R);
+            if (rows_here == R) {
+#pragma unroll
+                for (int rr = 0; rr < R; ++rr)
+                    row_step(pm[rr * m_stride], pa[rr * kQuarter], pa[rr * kQuarter + 1], pp[rr * p_stride],
+                             fac[2 * rr], fac[2 * rr + 1]);
+            } else {
+                for (int rr = 0; rr < rows_here; ++rr)
+                    row_step(pm[rr * m_stride], pa[rr * kQuarter], pa[rr * kQuarter + 1], pp[rr * p_stride],
+                             fac[2 * rr], fac[2 * rr + 1]);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[slot]);
+        }
+    }
+}
+
 } // namespace
 
 // ------------------------------------------------------------------ host side
@@ -645,6 +938,59 @@ sil_status launch_variant(cudaStream_t stream, Geometry const& geo, sil_field co
     return SIL_OK;
 }
 
+template <class C>
+int lap1_pair_occupancy()
+{
+    static int blocks = -1;
+    if (blocks < 0) {
+        cudaFuncSetAttribute(lap2d_1form_pair_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmemBytes);
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lap2d_1form_pair_kernel<C>, kThreads1, C::kSmemBytes);
+        blocks = b > 0 ? b : 0;
+    }
+    return blocks;
+}
+
+// The column-pair kernel (FP64): 512-column strips, the same tensor maps as
+// the single-column kernel with this shape's rows per box.
+template <class C>
+sil_status launch_pair_variant(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
+                               int* error_flag, int wait_tries)
+{
+    auto encode = encode_fn();
+    if (encode == nullptr) return fail(SIL_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
+    int64_t const mx = out.extent[0], my = out.extent[1];
+    uint64_t const nx = in.extent[0], ny = in.extent[1];
+    cuuint64_t dims[2] = {2 * ny, nx};
+    cuuint64_t strides[1] = {2 * ny * sizeof(double)};
+    cuuint32_t box_main[2] = {2 * kQuarter, static_cast<cuuint32_t>(C::kRows)};
+    cuuint32_t box_halo[2] = {2, static_cast<cuuint32_t>(C::kRows)};
+    cuuint32_t estr[2] = {1, 1};
+    CUtensorMap map_main, map_halo;
+    CUresult res = encode(&map_main, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, in.data, dims, strides, box_main, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (res == CUDA_SUCCESS)
+        res = encode(&map_halo, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, in.data, dims, strides, box_halo, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (res != CUDA_SUCCESS) return fail(SIL_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    int const occ = lap1_pair_occupancy<C>();
+    if (occ < 1) return fail(SIL_ERR_UNSUPPORTED, "1-form Laplacian pair variant does not fit on an SM");
+    int const strips = static_cast<int>((my + kTJ2 - 1) / kTJ2);
+    int64_t const work = static_cast<int64_t>(strips) * mx;
+    int64_t ctas = std::min<int64_t>(work, static_cast<int64_t>(sm_count()) * occ);
+    if (ctas < 1) ctas = 1;
+    int64_t const gx = in.front[0] - geo.front[0], gy = in.front[1] - geo.front[1];
+    Lap1Params<double> P {static_cast<double*>(out.data), out.stride[0], static_cast<int>(nx), static_cast<int>(ny),
+                          static_cast<int>(mx), static_cast<int>(my), static_cast<int>(out.front[0] - in.front[0]),
+                          static_cast<int>(out.front[1] - in.front[1]), strips, work, geo.h[0] + gx, geo.inv_h[0] + gx,
+                          geo.h[1] + gy, geo.inv_h[1] + gy, error_flag, wait_tries};
+    lap2d_1form_pair_kernel<C><<<static_cast<unsigned>(ctas), kThreads1, C::kSmemBytes, stream>>>(map_main, map_halo, P);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
 // Candidate pipeline shapes (rows per stage, stages, CTAs per SM sized for).
 template <class T>
 struct Lap1Variants;
@@ -669,7 +1015,13 @@ struct Lap1Variants<float>
     using V5 = Lap1Cfg<float, 16, 4, 1>;
 };
 
-constexpr int kLap1Variants = 6;
+constexpr int kLap1Variants = 6;      // single-column shapes (FP64 and FP32)
+constexpr int kLap1PairVariants = 3;  // column-pair shapes (FP64 only), indices 6..8
+
+int lap1_variant_count(bool f64)
+{
+    return kLap1Variants + (f64 ? kLap1PairVariants : 0);
+}
 
 template <class T>
 sil_status launch_by_index(int v, cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
@@ -682,6 +1034,21 @@ sil_status launch_by_index(int v, cudaStream_t stream, Geometry const& geo, sil_
     case 2: return launch_variant<T, typename V::V2>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
     case 3: return launch_variant<T, typename V::V3>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
     case 4: return launch_variant<T, typename V::V4>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
+    case 6:
+        if constexpr (std::is_same_v<T, double>)
+            return launch_pair_variant<Lap1PairCfg<8, 3>>(stream, geo, in, out, error_flag, wait_tries);
+        else
+            return launch_variant<T, typename V::V0>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
+    case 7:
+        if constexpr (std::is_same_v<T, double>)
+            return launch_pair_variant<Lap1PairCfg<4, 6>>(stream, geo, in, out, error_flag, wait_tries);
+        else
+            return launch_variant<T, typename V::V0>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
+    case 8:
+        if constexpr (std::is_same_v<T, double>)
+            return launch_pair_variant<Lap1PairCfg<2, 12>>(stream, geo, in, out, error_flag, wait_tries);
+        else
+            return launch_variant<T, typename V::V0>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
     default: return launch_variant<T, typename V::V5>(stream, geo, in, out, error_flag, ctas_per_sm, wait_tries);
     }
 }
@@ -690,7 +1057,7 @@ sil_status launch_by_index(int v, cudaStream_t stream, Geometry const& geo, sil_
 
 int lap2d_1form_variants()
 {
-    return kLap1Variants;
+    return kLap1Variants + kLap1PairVariants;
 }
 
 // Launch pipeline variant `variant` (0 = default) of the TMA 1-form kernel;
@@ -699,7 +1066,7 @@ sil_status launch_lap2d_1form_tma(cudaStream_t stream, Geometry const& geo, sil_
                                   int* error_flag, int variant, int wait_tries)
 {
     if (out.extent[0] == 0 || out.extent[1] == 0) return SIL_OK;
-    if (variant < 0 || variant >= kLap1Variants) variant = 0;
+    if (variant < 0 || variant >= lap1_variant_count(in.dtype == SIL_F64)) variant = 0;
     int const tries = wait_tries < 0 ? kWaitTries : wait_tries;
     if (in.dtype == SIL_F64) return launch_by_index<double>(variant, stream, geo, in, out, error_flag, 0, tries);
     return launch_by_index<float>(variant, stream, geo, in, out, error_flag, 0, tries);
@@ -722,7 +1089,7 @@ sil_status autotune_lap2d_1form(cudaStream_t stream, Geometry const& geo, sil_fi
     float best = 1e30f;
     int best_v = 0;
     sil_status st = SIL_OK;
-    for (int v = 0; v < kLap1Variants && st == SIL_OK; ++v) {
+    for (int v = 0; v < lap1_variant_count(in.dtype == SIL_F64) && st == SIL_OK; ++v) {
         sil_status const probe = launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
         if (probe == SIL_ERR_UNSUPPORTED) continue;  // does not fit: skip
         if (probe != SIL_OK) {

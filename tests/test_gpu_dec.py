@@ -330,6 +330,32 @@ def test_tma_1form_kernel_matches_generic_and_oracle(torch, sil, shape):
     assert rel_err(a, ref) <= TOL
 
 
+@pytest.mark.parametrize("shape", [(67, 300), (45, 1100), (130, 513)])
+def test_every_tma_pipeline_shape_is_bit_exact(torch, sil, shape, monkeypatch):
+    """Every pipeline shape the autotuner may pick -- the single-column
+    shapes 0-5 and the FP64 column-pair shapes 6-8 (512-column strips) --
+    agrees bit for bit with the table-driven kernel; the widths exercise
+    partial 512-column strips and the quarter-box and halo neighbours."""
+    nx, ny = shape
+    rng = np.random.default_rng(nx + 7 * ny)
+    coords = _two_d_case(rng, nx, ny)
+    geo = _geometry(sil, coords)
+    inp = rng.standard_normal((nx, ny, 2))
+    ti = dev(torch, inp)
+    gen = torch.full((nx - 1, ny - 1, 2), float("nan"), device="cuda", dtype=torch.float64)
+    sil.laplacian(geo, gen, ti, 1)
+    ref = host(gen)
+    for v in range(9):
+        monkeypatch.setenv("SIMILIE_B200_LAP1_VARIANT", str(v))
+        out = torch.full_like(gen, float("nan"))
+        st = sil.make_staged_laplacian(geo, out, ti, 1)
+        assert st.kernel == 2
+        st.run(out, ti)
+        st.status()
+        assert st.variant == v
+        assert np.array_equal(host(out), ref), v
+
+
 def test_tma_1form_kernel_output_offset(torch, sil):
     """Output box starting inside the input (nonzero front offset)."""
     rng = np.random.default_rng(5)
