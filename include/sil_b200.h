@@ -487,6 +487,19 @@ typedef struct sil_mag3d_problem {
  *   onelab_interface/magnetostatics_onelab.hpp:2241-2396 (Hodge factors 856-910). */
 sil_status sil_mag3d_apply(sil_stream stream, const sil_mag3d_problem* problem, const double* a, double* y);
 
+/* The same operator with its set-up done once (device spacing tables,
+ * 1/mu, the divergence gauge's coefficient table), as the reference builds
+ * its stencils once per operator; an apply is then one kernel on `stream`
+ * and may be captured in a CUDA graph.  The permeability is read at create
+ * time.  create is synchronous on `stream`.
+ * Replaces: the MagnetostaticsOperator3D constructor (precomputed stencils,
+ *   onelab_interface/magnetostatics_onelab.hpp:1815-1900) and
+ *   apply_with_precomputed_stencils (2241-2396). */
+typedef struct sil_mag3d_operator_s* sil_mag3d_operator;
+sil_status sil_mag3d_operator_create(sil_mag3d_operator* out, sil_stream stream, const sil_mag3d_problem* problem);
+sil_status sil_mag3d_operator_apply(sil_mag3d_operator op, sil_stream stream, const double* a, double* y);
+sil_status sil_mag3d_operator_destroy(sil_mag3d_operator op);
+
 /* Batched 3D solve; same settings, diagnostics and refinement scheme as
  * sil_mag2d_solve_batch.  Synchronous.
  * Replaces: solvers::minimize_strong_formulation_residual for

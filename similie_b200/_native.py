@@ -210,6 +210,9 @@ SIGNATURES = [
                                               ctypes.c_float, ctypes.POINTER(ctypes.c_double)]),
     ("sil_precond_debug_fetch", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int64]),
     ("sil_mag3d_apply", ctypes.c_int, [_P, ctypes.POINTER(SilMag3dProblem), _P, _P]),
+    ("sil_mag3d_operator_create", ctypes.c_int, [ctypes.POINTER(_P), _P, ctypes.POINTER(SilMag3dProblem)]),
+    ("sil_mag3d_operator_apply", ctypes.c_int, [_P, _P, _P, _P]),
+    ("sil_mag3d_operator_destroy", ctypes.c_int, [_P]),
     ("sil_mag3d_solve_batch", ctypes.c_int, [ctypes.POINTER(SilMag3dProblem), ctypes.c_int,
                                              ctypes.POINTER(SilSolveSettings),
                                              ctypes.POINTER(SilSolveDiagnostics), _P]),

@@ -199,40 +199,43 @@ __global__ void __launch_bounds__(256) hodge3d_dense_kernel(T const* in, T* out,
 }
 
 // Paired variant of the dense 3D row kernel for FP64 fields with three
-// components in and out: each thread owns two consecutive nodes along z, so
-// its 48 bytes in and out move as three 16-byte vector accesses.
+// components in and out and an even z extent: each thread owns two
+// consecutive nodes along z (never split across a row), so its 48 bytes in
+// and out move as three 16-byte vector accesses; the pairs of all rows form
+// one flat range, so every thread of every block has a pair.
 __global__ void __launch_bounds__(256) hodge3d_dense_pair_kernel(double const* in, double* out, StarRule star,
                                                                  GeoView<double> geo, int64_t fx, int64_t fy,
-                                                                 int64_t fz, int nx, int ny, int nz, int zchunks)
+                                                                 int64_t fz, int ny, int nz, uint32_t npairs)
 {
-    int const row = blockIdx.x / zchunks;
-    int const z0 = 2 * ((blockIdx.x - row * zchunks) * blockDim.x + threadIdx.x);
-    if (z0 >= nz) return;
-    int const y = row % ny, x = row / ny;
-    int64_t const node = static_cast<int64_t>(row) * nz + z0;
-    double2 const* src = reinterpret_cast<double2 const*>(in + node * 3);
-    double2 const a = src[0], b = src[1], c = src[2];
+    uint32_t const q = blockIdx.x * 256u + threadIdx.x;
+    if (q >= npairs) return;
+    uint32_t const node0 = 2u * q;
+    uint32_t const row = node0 / static_cast<uint32_t>(nz);
+    int const z0 = static_cast<int>(node0 - row * static_cast<uint32_t>(nz));
+    int const y = static_cast<int>(row % static_cast<uint32_t>(ny)), x = static_cast<int>(row / static_cast<uint32_t>(ny));
+    double2 const* src = reinterpret_cast<double2 const*>(in + static_cast<int64_t>(node0) * 3);
+    double2 const a = __ldg(src), b = __ldg(src + 1), c = __ldg(src + 2);
     double const v[2][3] = {{a.x, a.y, b.x}, {b.y, c.x, c.y}};
     int64_t const px = fx + x - geo.front[0] + 1, py = fy + y - geo.front[1] + 1;
     double r[2][3];
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        int64_t const p[3] = {px, py, fz + z0 + q - geo.front[2] + 1};
+    for (int k = 0; k < 2; ++k) {
+        int64_t const p[3] = {px, py, fz + z0 + k - geo.front[2] + 1};
 #pragma unroll
         for (int t = 0; t < 3; ++t) {
             double f = static_cast<double>(star.sgn[t]);
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) {
-                if (star.num_mask[t] & (1u << ax)) f *= geo.h[ax][p[ax]];
-                if (star.den_mask[t] & (1u << ax)) f *= geo.inv_h[ax][p[ax]];
+                if (star.num_mask[t] & (1u << ax)) f *= __ldg(geo.h[ax] + p[ax]);
+                if (star.den_mask[t] & (1u << ax)) f *= __ldg(geo.inv_h[ax] + p[ax]);
             }
-            r[q][t] = f * v[q][star.src[t]];
+            r[k][t] = f * v[k][star.src[t]];
         }
     }
-    double2* dst = reinterpret_cast<double2*>(out + node * 3);
-    dst[0] = make_double2(r[0][0], r[0][1]);
-    dst[1] = make_double2(r[0][2], r[1][0]);
-    dst[2] = make_double2(r[1][1], r[1][2]);
+    double2* dst = reinterpret_cast<double2*>(out + static_cast<int64_t>(node0) * 3);
+    __stcs(dst, make_double2(r[0][0], r[0][1]));
+    __stcs(dst + 1, make_double2(r[0][2], r[1][0]));
+    __stcs(dst + 2, make_double2(r[1][1], r[1][2]));
 }
 
 // Stored per-node Hodge tensor (Full<k> x Antisym<n-k>) of the diagonal metric.
@@ -589,12 +592,12 @@ sil_status launch_hodge(cudaStream_t stream, Geometry const& geo, uint32_t mask,
                               && reinterpret_cast<uintptr_t>(in.data) % 16 == 0
                               && reinterpret_cast<uintptr_t>(out.data) % 16 == 0;
         if (pairable) {
-            int const zc2 = (nz / 2 + 255) / 256;
-            int64_t const b2 = static_cast<int64_t>(nx) * ny * zc2;
-            if (b2 < (int64_t(1) << 31)) {
-                hodge3d_dense_pair_kernel<<<static_cast<unsigned>(b2), 256, 0, stream>>>(
+            int64_t const npairs = static_cast<int64_t>(nx) * ny * (nz / 2);
+            if (npairs < (int64_t(1) << 30)) {
+                unsigned const b2 = static_cast<unsigned>((npairs + 255) / 256);
+                hodge3d_dense_pair_kernel<<<b2, 256, 0, stream>>>(
                         static_cast<double const*>(in.data), static_cast<double*>(out.data), star, geo_view<double>(geo),
-                        out.front[0], out.front[1], out.front[2], nx, ny, nz, zc2);
+                        out.front[0], out.front[1], out.front[2], ny, nz, static_cast<uint32_t>(npairs));
                 SIL_CUDA_CHECK(cudaGetLastError());
                 return SIL_OK;
             }

@@ -189,6 +189,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int ma
     return false;
 }
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialization attribute may start (barrier set-up) while the
+// previous kernel on the stream drains; grid_dependency_wait() returns once
+// that kernel has completed and its writes are visible, so every global
+// access of the kernel comes after it.  Without the attribute both are no-ops.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ void tma_load_2d(void* dst, CUtensorMap const* map, uint64_t* bar, int c0, int c1)
 {
     asm volatile(
@@ -242,6 +250,8 @@ lap2d_1form_tma_kernel(const __grid_constant__ CUtensorMap map_main, const __gri
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
+    grid_dependency_wait();
+    grid_launch_dependents();
 
     int64_t const begin = (P.work * blockIdx.x) / gridDim.x;
     int64_t const end = (P.work * (blockIdx.x + 1)) / gridDim.x;
@@ -506,6 +516,8 @@ lap2d_1form_pair_kernel(const __grid_constant__ CUtensorMap map_main, const __gr
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
+    grid_dependency_wait();
+    grid_launch_dependents();
 
     int64_t const begin = (P.work * blockIdx.x) / gridDim.x;
     int64_t const end = (P.work * (blockIdx.x + 1)) / gridDim.x;
@@ -881,6 +893,25 @@ bool lap2d_1form_tma_ok(sil_field const& in, sil_field const& out)
 
 namespace {
 
+// Launch with the programmatic stream-serialization attribute, so that
+// back-to-back runs overlap one kernel's drain with the next one's set-up.
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t stream,
+                       Args... args)
+{
+    cudaLaunchConfig_t cfg {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <class T, class C>
 int lap1_occupancy()
 {
@@ -933,8 +964,8 @@ sil_status launch_variant(cudaStream_t stream, Geometry const& geo, sil_field co
                      static_cast<int>(mx), static_cast<int>(my), static_cast<int>(out.front[0] - in.front[0]),
                      static_cast<int>(out.front[1] - in.front[1]), strips, work, gh[0] + gx, gih[0] + gx, gh[1] + gy,
                      gih[1] + gy, error_flag, wait_tries};
-    lap2d_1form_tma_kernel<T, C><<<static_cast<unsigned>(ctas), kThreads1, C::kSmemBytes, stream>>>(map_main, map_halo, P);
-    SIL_CUDA_CHECK(cudaGetLastError());
+    SIL_CUDA_CHECK(launch_pdl(lap2d_1form_tma_kernel<T, C>, static_cast<unsigned>(ctas), kThreads1, C::kSmemBytes, stream,
+                              map_main, map_halo, P));
     return SIL_OK;
 }
 
@@ -986,8 +1017,8 @@ sil_status launch_pair_variant(cudaStream_t stream, Geometry const& geo, sil_fie
                           static_cast<int>(mx), static_cast<int>(my), static_cast<int>(out.front[0] - in.front[0]),
                           static_cast<int>(out.front[1] - in.front[1]), strips, work, geo.h[0] + gx, geo.inv_h[0] + gx,
                           geo.h[1] + gy, geo.inv_h[1] + gy, error_flag, wait_tries};
-    lap2d_1form_pair_kernel<C><<<static_cast<unsigned>(ctas), kThreads1, C::kSmemBytes, stream>>>(map_main, map_halo, P);
-    SIL_CUDA_CHECK(cudaGetLastError());
+    SIL_CUDA_CHECK(launch_pdl(lap2d_1form_pair_kernel<C>, static_cast<unsigned>(ctas), kThreads1, C::kSmemBytes, stream,
+                              map_main, map_halo, P));
     return SIL_OK;
 }
 

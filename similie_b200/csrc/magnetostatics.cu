@@ -1987,6 +1987,102 @@ sil_status sil_mag3d_apply(sil_stream stream, const sil_mag3d_problem* problem, 
     return SIL_OK;
 }
 
+// A 3D operator with its set-up done once: the device spacing tables, the
+// node reluctivity 1/mu and (divergence gauge) the codifferential
+// coefficient table, so that an apply is one kernel.
+} // extern "C"
+
+struct sil_mag3d_operator_s
+{
+    sil::ProbInfo pi {};
+    double const* nu = nullptr;
+    void* mem = nullptr;
+};
+
+extern "C" {
+
+sil_status sil_mag3d_operator_create(sil_mag3d_operator* out, sil_stream stream, const sil_mag3d_problem* problem)
+{
+    if (out == nullptr || problem == nullptr) return fail(SIL_ERR_INVALID, "sil_mag3d_operator_create: NULL pointer");
+    *out = nullptr;
+    sil_mag3d_problem const& q = *problem;
+    sil_status const st = check_mag3d(q, "sil_mag3d_operator_create", false);
+    if (st != SIL_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int64_t const nodes = q.nx * q.ny * q.nz;
+    int64_t const len[3] = {q.nx, q.ny, q.nz};
+    double const* c[3] = {q.x, q.y, q.z};
+    std::vector<double> sp;
+    for (int a2 = 0; a2 < 3; ++a2)
+        for (int64_t i = 0; i < len[a2]; ++i) sp.push_back(local_spacing(c[a2], len[a2], i));
+    for (int a2 = 0; a2 < 3; ++a2)
+        for (int64_t i = 0; i < len[a2]; ++i) sp.push_back(1.0 / local_spacing(c[a2], len[a2], i));
+    size_t const nu_bytes = (nodes * sizeof(double) + 255) / 256 * 256;
+    size_t const gauge_bytes = q.gauge ? static_cast<size_t>(nodes) * 12 * sizeof(double) : 0;
+    auto* op = new sil_mag3d_operator_s;
+    if (cudaMalloc(&op->mem, nu_bytes + gauge_bytes + sp.size() * sizeof(double)) != cudaSuccess) {
+        delete op;
+        return fail(SIL_ERR_CUDA, "sil_mag3d_operator_create: device allocation failed");
+    }
+    auto bail = [&](sil_status e) {
+        cudaFree(op->mem);
+        delete op;
+        return e;
+    };
+    double* nu = static_cast<double*>(op->mem);
+    double* gd = reinterpret_cast<double*>(static_cast<char*>(op->mem) + nu_bytes);
+    double* dsp = reinterpret_cast<double*>(static_cast<char*>(op->mem) + nu_bytes + gauge_bytes);
+    if (cudaMemcpyAsync(dsp, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return bail(fail(SIL_ERR_CUDA, "sil_mag3d_operator_create: table upload failed"));
+    ProbInfo& pi = op->pi;
+    pi.dim = 3;
+    pi.nx = q.nx;
+    pi.ny = q.ny;
+    pi.nz = q.nz;
+    pi.nodes = nodes;
+    pi.n = 3 * nodes;
+    pi.gamma = q.gauge_penalty;
+    int64_t o = 0;
+    for (int a2 = 0; a2 < 3; ++a2) {
+        pi.ls64[a2] = dsp + o;
+        o += len[a2];
+    }
+    for (int a2 = 0; a2 < 3; ++a2) {
+        pi.ils64[a2] = dsp + o;
+        o += len[a2];
+    }
+    if (q.gauge) {
+        ProblemDesc desc {3, q.nx, q.ny, q.nz, q.gauge_penalty, q.node_mu, nullptr, nullptr, {q.x, q.y, q.z}, 1};
+        sil_status const gs = build_divergence_gauge(desc, pi, gd, nullptr, gd + 8 * nodes, gd + 11 * nodes, s);
+        if (gs != SIL_OK) return bail(gs);
+        pi.gauge = 1;
+        pi.gd64 = gd;
+    }
+    reciprocal_kernel<<<static_cast<int>((nodes + 255) / 256), 256, 0, s>>>(q.node_mu, nu, nodes);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+        return bail(fail(SIL_ERR_CUDA, "sil_mag3d_operator_create: set-up kernels failed"));
+    op->nu = nu;
+    *out = op;
+    return SIL_OK;
+}
+
+sil_status sil_mag3d_operator_apply(sil_mag3d_operator op, sil_stream stream, const double* a, double* y)
+{
+    if (op == nullptr || a == nullptr || y == nullptr) return fail(SIL_ERR_INVALID, "sil_mag3d_operator_apply: NULL pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    mag3d_apply_kernel<<<static_cast<int>((op->pi.nodes + 255) / 256), 256, 0, s>>>(op->pi, op->nu, a, y);
+    SIL_CUDA_CHECK(cudaGetLastError());
+    return SIL_OK;
+}
+
+sil_status sil_mag3d_operator_destroy(sil_mag3d_operator op)
+{
+    if (op == nullptr) return SIL_OK;
+    cudaFree(op->mem);
+    delete op;
+    return SIL_OK;
+}
+
 sil_status sil_mag3d_solve_batch(const sil_mag3d_problem* problems, int nproblems, const sil_solve_settings* settings,
                                  sil_solve_diagnostics* diag, sil_stream stream)
 {

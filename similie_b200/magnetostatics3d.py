@@ -173,6 +173,36 @@ def apply(x, y, z, node_mu_dev, a_dev, y_dev, gamma=DEFAULT_GAUGE_PENALTY, strea
     return y_dev
 
 
+class Operator:
+    """y = K a with the set-up done once (spacing tables, 1/mu, the divergence
+    gauge's table), as the reference's MagnetostaticsOperator3D precomputes
+    its stencils; apply() is one kernel on the stream and can be captured in
+    a CUDA graph.  node_mu_dev is read at construction."""
+
+    def __init__(self, x, y, z, node_mu_dev, gamma=DEFAULT_GAUGE_PENALTY, stream=None, gauge="penalty"):
+        import torch
+        self._coords = tuple(_f64(v) for v in (x, y, z))
+        self.nodes = len(self._coords[0]) * len(self._coords[1]) * len(self._coords[2])
+        p = _problem_struct(*self._coords, node_mu_dev, gamma, gauge=gauge)
+        s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+        h = ctypes.c_void_p()
+        check(lib().sil_mag3d_operator_create(ctypes.byref(h), s, ctypes.byref(p)), "mag3d_operator_create")
+        self._h = h
+
+    def apply(self, a_dev, y_dev, stream=None):
+        import torch
+        s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+        check(lib().sil_mag3d_operator_apply(self._h, s, ctypes.c_void_p(a_dev.data_ptr()),
+                                             ctypes.c_void_p(y_dev.data_ptr())), "mag3d_operator_apply")
+        return y_dev
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().sil_mag3d_operator_destroy(h)
+            self._h = None
+
+
 def solve_batch(coords, mus, rhss, sols, gammas=None, solver="cg", tol=1e-10, max_iterations=200000,
                 inner_iterations=4000, inner_tolerance=1e-4, stream=None, gauge="penalty"):
     """minimize_strong_formulation_residual for a batch of 3D linear problems.

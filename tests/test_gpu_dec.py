@@ -154,12 +154,14 @@ def test_hodge_star_vs_oracle(torch, sil, n):
         assert rel_err(host(out), ref) <= TOL, (n, k)
 
 
+@pytest.mark.parametrize("shape", [(9, 7, 300), (5, 3, 6), (3, 4, 2), (4, 5, 7)])
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
-def test_hodge_star_dense_3d_path_matches_table_driven(torch, sil, dtype):
-    """Dense [x][y][z][c] fields take the row kernel; a strided view of the same
-    data takes the table-driven kernel; both must agree bit for bit."""
+def test_hodge_star_dense_3d_path_matches_table_driven(torch, sil, dtype, shape):
+    """Dense [x][y][z][c] fields take the row kernel (FP64 1- and 2-forms with
+    an even z extent: the node-pair kernel over one flat range of pairs); a
+    strided view of the same data takes the table-driven kernel; both must
+    agree bit for bit."""
     rng = np.random.default_rng(77)
-    shape = (9, 7, 300)
     coords = _coords(rng, shape)
     geo = _geometry(sil, coords)
     dt = getattr(torch, dtype)

@@ -47,6 +47,40 @@ def test_apply_matches_oracle(torch, m3, shape, ratio, gamma):
     assert rel_err(ty.cpu().numpy(), ref) <= 1e-12
 
 
+@pytest.mark.parametrize("gauge", ["penalty", "divergence"])
+def test_operator_object_matches_the_per_call_apply(torch, m3, gauge):
+    """The operator object (set-up once, one kernel per apply, replayable from
+    a CUDA graph) gives the per-call apply's result bit for bit, and the
+    oracle's to 1e-12 (penalty gauge)."""
+    rng = np.random.default_rng(31)
+    nx, ny, nz = 13, 10, 9
+    x, y, z, cell_mu = _grid(m3, rng, nx, ny, nz, 1.03)
+    mu_h = m3.node_mu(nx, ny, nz, cell_mu)
+    mu = torch.from_numpy(mu_h).cuda()
+    a = torch.from_numpy(rng.standard_normal(3 * nx * ny * nz)).cuda()
+    ref = torch.zeros_like(a)
+    m3.apply(x, y, z, mu, a, ref, 20.0, gauge=gauge)
+    op = m3.Operator(x, y, z, mu, 20.0, gauge=gauge)
+    got = torch.full_like(a, float("nan"))
+    op.apply(a, got)
+    torch.cuda.synchronize()
+    assert torch.equal(got, ref)
+    if gauge == "penalty":
+        assert rel_err(got.cpu().numpy(), O.mag3d_apply(x, y, z, mu_h, 20.0, a.cpu().numpy())) <= 1e-12
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        op.apply(a, got)
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    out2 = torch.full_like(a, float("nan"))
+    with torch.cuda.graph(g):
+        op.apply(a, out2)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(out2, ref)
+
+
 def test_apply_is_symmetric(torch, m3):
     rng = np.random.default_rng(5)
     x, y, z, cell_mu = _grid(m3, rng, 10, 9, 8, 1.02)
