@@ -1114,40 +1114,50 @@ sil_status launch_lap2d_1form_tma(cudaStream_t stream, Geometry const& geo, sil_
 sil_status autotune_lap2d_1form(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
                                 int* error_flag, int* best_variant, float* best_ms)
 {
+    // Every shape that fits is timed over 5 back-to-back launches in each of
+    // two rounds (the rounds interleave the shapes, so a slow spell of the
+    // GPU does not land on one shape alone); a shape's time is its faster
+    // round.
     cudaEvent_t e0, e1;
     SIL_CUDA_CHECK(cudaEventCreate(&e0));
     SIL_CUDA_CHECK(cudaEventCreate(&e1));
-    float best = 1e30f;
-    int best_v = 0;
+    int const nv = lap1_variant_count(in.dtype == SIL_F64);
+    std::vector<float> t(nv, 1e30f);
+    std::vector<char> fits(nv, 1);
     sil_status st = SIL_OK;
-    for (int v = 0; v < lap1_variant_count(in.dtype == SIL_F64) && st == SIL_OK; ++v) {
-        sil_status const probe = launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
-        if (probe == SIL_ERR_UNSUPPORTED) continue;  // does not fit: skip
-        if (probe != SIL_OK) {
-            st = probe;
-            break;
-        }
-        launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
-        cudaEventRecord(e0, stream);
-        for (int i = 0; i < 3; ++i) launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
-        cudaEventRecord(e1, stream);
-        cudaError_t const err = cudaEventSynchronize(e1);
-        if (err != cudaSuccess) {
-            st = cuda_fail(err, "autotune");
-            break;
-        }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        ms /= 3.f;
-        if (ms < best) {
-            best = ms;
-            best_v = v;
+    constexpr int kLaunches = 5;
+    for (int round = 0; round < 2 && st == SIL_OK; ++round) {
+        for (int v = 0; v < nv && st == SIL_OK; ++v) {
+            if (!fits[v]) continue;
+            sil_status const probe = launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
+            if (probe == SIL_ERR_UNSUPPORTED) {  // does not fit: skip
+                fits[v] = 0;
+                continue;
+            }
+            if (probe != SIL_OK) {
+                st = probe;
+                break;
+            }
+            cudaEventRecord(e0, stream);
+            for (int i = 0; i < kLaunches; ++i) launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
+            cudaEventRecord(e1, stream);
+            cudaError_t const err = cudaEventSynchronize(e1);
+            if (err != cudaSuccess) {
+                st = cuda_fail(err, "autotune");
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t[v] = std::min(t[v], ms / kLaunches);
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    int best_v = 0;
+    for (int v = 1; v < nv; ++v)
+        if (t[v] < t[best_v]) best_v = v;
     *best_variant = best_v;
-    *best_ms = best;
+    *best_ms = t[best_v];
     return st;
 }
 

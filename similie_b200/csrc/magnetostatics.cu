@@ -272,24 +272,20 @@ __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_
     return res + static_cast<T>(pi.gamma) * ha * a[row];
 }
 
-// All three rows of a node at once (the curl moments shared between the
-// components are formed once); each component sums its terms in the order of
-// mag3d_apply_row, so the values are the same.
-template <class T, bool G, class LD>
-__device__ void mag3d_apply_node_ld(LD const& a, T const* nu, ProbInfo const& pi, int node, T* out)
+// All three rows of an interior node at once (the curl moments shared
+// between the components are formed once); each component sums its terms in
+// the order of mag3d_apply_row, so the values are the same.  DEEP: every
+// node of the stencil (offsets -1..1 per axis) is interior, so no neighbour
+// needs the boundary test (the same values, fewer instructions).
+template <class T, bool G, bool DEEP, class LD>
+__device__ __forceinline__ void mag3d_interior_node(LD const& a, T const* nu, ProbInfo const& pi, int node, int i,
+                                                    int j, int k, T* out)
 {
     int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
-    int const t = node / nx, i = node - t * nx, k = t / ny, j = t - k * ny;
     int const row0 = 3 * node;
     auto interior = [&](int ii, int jj, int kk) {
-        return ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz;
+        return DEEP || (ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz);
     };
-    if (!interior(i, j, k)) {
-        out[0] = a(row0);
-        out[1] = a(row0 + 1);
-        out[2] = a(row0 + 2);
-        return;
-    }
     int const sy = 3 * nx, sz = 3 * nx * ny;
     auto A = [&](int di, int dj, int dk, int cc) -> T {
         return interior(i + di, j + dj, k + dk) ? a(row0 + 3 * di + sy * dj + sz * dk + cc) : T(0);
@@ -374,6 +370,27 @@ __device__ void mag3d_apply_node_ld(LD const& a, T const* nu, ProbInfo const& pi
         if (in_i) res = res - w(-1, 0, 0, 1) * by(-1, 0, 0);
         out[2] = res + gt[2];
     }
+}
+
+// All three rows of a node: identity on the Dirichlet boundary, else the
+// interior stencil (without boundary tests where the whole stencil is
+// interior).
+template <class T, bool G, class LD>
+__device__ void mag3d_apply_node_ld(LD const& a, T const* nu, ProbInfo const& pi, int node, T* out)
+{
+    int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
+    int const t = node / nx, i = node - t * nx, k = t / ny, j = t - k * ny;
+    if (!(i > 0 && j > 0 && k > 0 && i + 1 < nx && j + 1 < ny && k + 1 < nz)) {
+        int const row0 = 3 * node;
+        out[0] = a(row0);
+        out[1] = a(row0 + 1);
+        out[2] = a(row0 + 2);
+        return;
+    }
+    if (i > 1 && j > 1 && k > 1 && i + 2 < nx && j + 2 < ny && k + 2 < nz)
+        mag3d_interior_node<T, G, true>(a, nu, pi, node, i, j, k, out);
+    else
+        mag3d_interior_node<T, G, false>(a, nu, pi, node, i, j, k, out);
 }
 
 template <class T, bool G = false>
@@ -1891,12 +1908,14 @@ sil_status check_mag3d(sil_mag3d_problem const& q, char const* who, bool need_fi
     return SIL_OK;
 }
 
-__global__ void mag3d_apply_kernel(ProbInfo pi, double const* nu, double const* a, double* y)
+// G: the divergence-gauge variant (the penalty variant keeps fewer registers).
+template <bool G>
+__global__ void __launch_bounds__(256, 4) mag3d_apply_kernel(ProbInfo pi, double const* nu, double const* a, double* y)
 {
     int64_t const node = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (node >= pi.nodes) return;
     double out[3];
-    mag3d_apply_node<double, true>(a, nu, pi, static_cast<int>(node), out);
+    mag3d_apply_node<double, G>(a, nu, pi, static_cast<int>(node), out);
     for (int c = 0; c < 3; ++c) y[3 * node + c] = out[c];
 }
 
@@ -1978,7 +1997,8 @@ sil_status sil_mag3d_apply(sil_stream stream, const sil_mag3d_problem* problem, 
         pi.gd64 = gd;
     }
     reciprocal_kernel<<<static_cast<int>((nodes + 255) / 256), 256, 0, s>>>(q.node_mu, nu, nodes);
-    mag3d_apply_kernel<<<static_cast<int>((nodes + 255) / 256), 256, 0, s>>>(pi, nu, a, y);
+    auto const kern = pi.gauge ? mag3d_apply_kernel<true> : mag3d_apply_kernel<false>;
+    kern<<<static_cast<int>((nodes + 255) / 256), 256, 0, s>>>(pi, nu, a, y);
     SIL_CUDA_CHECK(cudaGetLastError());
     // A copy from pageable memory has left the host table once it returns;
     // the device buffer is freed in stream order after the apply.
@@ -2070,7 +2090,8 @@ sil_status sil_mag3d_operator_apply(sil_mag3d_operator op, sil_stream stream, co
 {
     if (op == nullptr || a == nullptr || y == nullptr) return fail(SIL_ERR_INVALID, "sil_mag3d_operator_apply: NULL pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    mag3d_apply_kernel<<<static_cast<int>((op->pi.nodes + 255) / 256), 256, 0, s>>>(op->pi, op->nu, a, y);
+    auto const kern = op->pi.gauge ? mag3d_apply_kernel<true> : mag3d_apply_kernel<false>;
+    kern<<<static_cast<int>((op->pi.nodes + 255) / 256), 256, 0, s>>>(op->pi, op->nu, a, y);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }
