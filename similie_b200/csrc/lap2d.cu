@@ -1114,45 +1114,63 @@ sil_status launch_lap2d_1form_tma(cudaStream_t stream, Geometry const& geo, sil_
 sil_status autotune_lap2d_1form(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
                                 int* error_flag, int* best_variant, float* best_ms)
 {
-    // Every shape that fits is timed over 5 back-to-back launches in each of
-    // two rounds (the rounds interleave the shapes, so a slow spell of the
-    // GPU does not land on one shape alone); a shape's time is its faster
-    // round.
-    cudaEvent_t e0, e1;
-    SIL_CUDA_CHECK(cudaEventCreate(&e0));
-    SIL_CUDA_CHECK(cudaEventCreate(&e1));
-    int const nv = lap1_variant_count(in.dtype == SIL_F64);
-    std::vector<float> t(nv, 1e30f);
-    std::vector<char> fits(nv, 1);
-    sil_status st = SIL_OK;
+    // Every shape that fits is timed as a CUDA graph of 5 back-to-back
+    // launches (the way repeated runs reach the GPU, the programmatic launch
+    // overlap included), replayed once in each of two rounds that interleave
+    // the shapes; a shape's time is its faster round.
     constexpr int kLaunches = 5;
-    for (int round = 0; round < 2 && st == SIL_OK; ++round) {
+    int const nv = lap1_variant_count(in.dtype == SIL_F64);
+    std::vector<cudaGraphExec_t> exec(nv, nullptr);
+    std::vector<float> t(nv, 1e30f);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t cs = nullptr;
+    sil_status st = SIL_OK;
+    auto cleanup = [&]() {
+        for (cudaGraphExec_t& g : exec)
+            if (g != nullptr) cudaGraphExecDestroy(g);
+        if (e0 != nullptr) cudaEventDestroy(e0);
+        if (e1 != nullptr) cudaEventDestroy(e1);
+        if (cs != nullptr) cudaStreamDestroy(cs);
+    };
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess
+        || cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+        cleanup();
+        return fail(SIL_ERR_CUDA, "autotune: event or stream creation failed");
+    }
+    for (int v = 0; v < nv && st == SIL_OK; ++v) {
+        sil_status const probe = launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
+        if (probe == SIL_ERR_UNSUPPORTED) continue;  // does not fit: skip
+        if (probe != SIL_OK) {
+            st = probe;
+            break;
+        }
+        cudaGraph_t graph = nullptr;
+        cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        for (int i = 0; i < kLaunches && err == cudaSuccess && st == SIL_OK; ++i)
+            st = launch_lap2d_1form_tma(cs, geo, in, out, error_flag, v);
+        cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
+        if (err == cudaSuccess) err = err2;
+        if (err == cudaSuccess && st == SIL_OK) err = cudaGraphInstantiate(&exec[v], graph, 0);
+        if (graph != nullptr) cudaGraphDestroy(graph);
+        if (st == SIL_OK && err != cudaSuccess) st = cuda_fail(err, "autotune graph");
+    }
+    for (int round = 0; round < 3 && st == SIL_OK; ++round) {
         for (int v = 0; v < nv && st == SIL_OK; ++v) {
-            if (!fits[v]) continue;
-            sil_status const probe = launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
-            if (probe == SIL_ERR_UNSUPPORTED) {  // does not fit: skip
-                fits[v] = 0;
-                continue;
-            }
-            if (probe != SIL_OK) {
-                st = probe;
-                break;
-            }
+            if (exec[v] == nullptr) continue;
             cudaEventRecord(e0, stream);
-            for (int i = 0; i < kLaunches; ++i) launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
+            cudaError_t err = cudaGraphLaunch(exec[v], stream);
             cudaEventRecord(e1, stream);
-            cudaError_t const err = cudaEventSynchronize(e1);
+            if (err == cudaSuccess) err = cudaEventSynchronize(e1);
             if (err != cudaSuccess) {
                 st = cuda_fail(err, "autotune");
                 break;
             }
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            t[v] = std::min(t[v], ms / kLaunches);
+            if (round > 0) t[v] = std::min(t[v], ms / kLaunches);  // round 0 warms up
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    cleanup();
     int best_v = 0;
     for (int v = 1; v < nv; ++v)
         if (t[v] < t[best_v]) best_v = v;
