@@ -212,8 +212,8 @@ def main():
                     help="leave the configuration-1 and configuration-3 records out of the default line")
     ap.add_argument("--extras", action="store_true", help="also time the unfused chain, FP32 and the 512^2 0-form")
     ap.add_argument("--workload", default="laplacian",
-                    choices=["laplacian", "solve", "mag3d", "precond", "hodge3d", "nonlinear", "nonlinear3d",
-                             "assembled"])
+                    choices=["laplacian", "solve", "mag3d", "precond", "hodge3d", "apply3d", "nonlinear",
+                             "nonlinear3d", "assembled"])
     ap.add_argument("--n2d", type=int, default=257, help="nonlinear: nodes per axis")
     ap.add_argument("--chunk", type=int, default=64, help="solve: problems per solver call (at most 64 for learned)")
     ap.add_argument("--concurrent", type=int, default=1,
@@ -262,6 +262,15 @@ def main():
         x = m3.stretched_coords(args.n3d, 1.01)
         print(json.dumps({"metric": f"3D Hodge star 1-form -> 2-form, {args.n3d}^3, FP64",
                           "hodge": hodge3d_gbs(torch, x, x.copy(), x.copy(), steps=args.steps)}))
+        return
+    if args.workload == "apply3d":
+        import torch
+        import similie_b200.magnetostatics3d as m3
+        torch.cuda.set_device(0)
+        prob = m3.synthetic_problem(np.random.default_rng(5), args.n3d)
+        mu = torch.from_numpy(prob.node_mu()).cuda()
+        print(json.dumps({"metric": f"3D curl-curl + gauge-penalty apply, {args.n3d}^3, FP64",
+                          "apply": apply3d_gbs(torch, prob, mu, steps=args.steps)}))
         return
 
     import torch
