@@ -448,6 +448,41 @@ __global__ void ssor_bwd_kernel(int count, int32_t const* rows, int32_t const* p
     z[i] = s / diag[i];
 }
 
+// One launch per triangular sweep of SSOR / symmetric Gauss-Seidel, in place
+// of one launch per level: a single CTA walks the levels in order, its
+// threads sharing each level's rows, with a barrier between levels (a
+// level's rows read only rows of earlier levels, which the barrier makes
+// visible within the CTA).  The sweeps are a chain of short levels (a 2D
+// grid of n^2 nodes has 2n - 1), so one CTA holds a level's rows and the
+// barrier costs far less than a launch.  Each row is the expression of the
+// level kernels, so the values are the same.
+constexpr int kSweepThreads = 1024;
+
+template <bool FWD>
+__global__ void __launch_bounds__(kSweepThreads) ssor_sweep_kernel(int nlev, int32_t const* lev, int32_t const* rows,
+                                                                    int32_t const* ptr, int32_t const* col,
+                                                                    double const* val, double const* diag, double w,
+                                                                    double c, double const* in, double* out,
+                                                                    CgState const* st)
+{
+    if (skip(st)) return;
+    for (int l = 0; l < nlev; ++l) {
+        int const end = lev[l + 1];
+        for (int pos = lev[l] + static_cast<int>(threadIdx.x); pos < end; pos += kSweepThreads) {
+            int const i = rows[pos];
+            // forward: y_i = (c r_i - sum_{j<i} w a_ij y_j) / a_ii
+            // backward: z_i = (a_ii y_i - sum_{j>i} w a_ij z_j) / a_ii
+            double s = FWD ? c * in[i] : diag[i] * in[i];
+            for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+                int const j = col[k];
+                if (FWD ? j < i : j > i) s -= w * val[k] * out[j];
+            }
+            out[i] = s / diag[i];
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 }  // namespace sil
 
@@ -465,12 +500,15 @@ struct sil_csr_precond_s
     // SSOR levels: rows in level order, level offsets on the host
     int32_t *fwd_rows = nullptr, *bwd_rows = nullptr;
     std::vector<int32_t> fwd_lev, bwd_lev;
+    // single-launch sweeps: the level offsets on the device
+    int32_t *fwd_lev_d = nullptr, *bwd_lev_d = nullptr;
     ~sil_csr_precond_s()
     {
         for (void* p : {static_cast<void*>(diag), static_cast<void*>(dinv), static_cast<void*>(scratch),
                         static_cast<void*>(mptr), static_cast<void*>(mcol), static_cast<void*>(tptr),
                         static_cast<void*>(tcol), static_cast<void*>(mval), static_cast<void*>(tval),
-                        static_cast<void*>(fwd_rows), static_cast<void*>(bwd_rows)})
+                        static_cast<void*>(fwd_rows), static_cast<void*>(bwd_rows), static_cast<void*>(fwd_lev_d),
+                        static_cast<void*>(bwd_lev_d)})
             cudaFree(p);
     }
 };
@@ -515,6 +553,14 @@ void precond_launch(sil_csr_precond_s const& P, cudaStream_t s, double const* r,
         double const w = c.kind == SIL_PC_SSOR ? c.sor_relaxation_factor : 1.0;
         double const cw = w * (2.0 - w);
         double* y = P.scratch;
+        if (P.fwd_lev_d != nullptr) {
+            ssor_sweep_kernel<true><<<1, kSweepThreads, 0, s>>>(static_cast<int>(P.fwd_lev.size()) - 1, P.fwd_lev_d,
+                                                                 P.fwd_rows, A.ptr, A.col, A.val, P.diag, w, cw, r, y, st);
+            ssor_sweep_kernel<false><<<1, kSweepThreads, 0, s>>>(static_cast<int>(P.bwd_lev.size()) - 1, P.bwd_lev_d,
+                                                                  P.bwd_rows, A.ptr, A.col, A.val, P.diag, w, 0.0, y, z,
+                                                                  st);
+            return;
+        }
         for (size_t l = 0; l + 1 < P.fwd_lev.size(); ++l) {
             int const cnt = P.fwd_lev[l + 1] - P.fwd_lev[l];
             ssor_fwd_kernel<<<(cnt + kBlock - 1) / kBlock, kBlock, 0, s>>>(cnt, P.fwd_rows + P.fwd_lev[l], A.ptr,
@@ -1335,6 +1381,11 @@ sil_status sil_csr_precond_create(sil_stream stream, sil_csr m, const sil_menu_s
             if (sil_status st = upload(&P->fwd_rows, rows, s); st != SIL_OK) return st;
             levels(hptr, hcol, false, rows, P->bwd_lev);
             if (sil_status st = upload(&P->bwd_rows, rows, s); st != SIL_OK) return st;
+            // single-launch sweeps (int row offsets)
+            if (n > 0 && n < (int64_t(1) << 31)) {
+                if (sil_status st = upload(&P->fwd_lev_d, P->fwd_lev, s); st != SIL_OK) return st;
+                if (sil_status st = upload(&P->bwd_lev_d, P->bwd_lev, s); st != SIL_OK) return st;
+            }
         } else {
             bool const spd = kind == SIL_PC_SPD_ISAI;
             std::vector<int32_t> mp(n + 1, 0), mc;
@@ -1431,10 +1482,11 @@ sil_status sil_csr_solve(sil_stream stream, sil_csr m, sil_csr_precond pc, const
     SIL_CUDA_CHECK(cudaGetLastError());
     // A chunk of iterations captured once as a CUDA graph (every kernel does
     // nothing once the state is done) and replayed until convergence, the
-    // state read back after each replay.  The level-scheduled
-    // preconditioners launch two kernels per level, so their chunks are
-    // shorter (at most about 4,096 launches per graph).
-    int const per_apply = static_cast<int>(pc->fwd_lev.size() + pc->bwd_lev.size()) + 8;
+    // state read back after each replay.  SSOR / symmetric Gauss-Seidel run
+    // each triangular sweep as one launch; where they fall back to one
+    // launch per level (2^31 rows or more), the chunks are shorter (at most
+    // about 4,096 launches per graph).
+    int const per_apply = pc->fwd_lev_d != nullptr ? 10 : static_cast<int>(pc->fwd_lev.size() + pc->bwd_lev.size()) + 8;
     int const chunk = std::max(1, std::min(16, 4096 / per_apply));
     auto issue = [&](cudaStream_t cs) {
         for (int c = 0; c < chunk; ++c) {

@@ -217,19 +217,29 @@ __global__ void __launch_bounds__(256) hodge3d_dense_pair_kernel(double const* i
     double2 const a = __ldg(src), b = __ldg(src + 1), c = __ldg(src + 2);
     double const v[2][3] = {{a.x, a.y, b.x}, {b.y, c.x, c.y}};
     int64_t const px = fx + x - geo.front[0] + 1, py = fy + y - geo.front[1] + 1;
+    int64_t const pz = fz + z0 - geo.front[2] + 1;
+    // The spacings this pair can use, loaded once; a factor the rule leaves
+    // out multiplies by 1.0, which is exact, so each product is the one the
+    // table-driven kernel forms.
+    double const hx = __ldg(geo.h[0] + px), ihx = __ldg(geo.inv_h[0] + px);
+    double const hy = __ldg(geo.h[1] + py), ihy = __ldg(geo.inv_h[1] + py);
+    double const hz[2] = {__ldg(geo.h[2] + pz), __ldg(geo.h[2] + pz + 1)};
+    double const ihz[2] = {__ldg(geo.inv_h[2] + pz), __ldg(geo.inv_h[2] + pz + 1)};
     double r[2][3];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-        int64_t const p[3] = {px, py, fz + z0 + k - geo.front[2] + 1};
+        double const hv[3] = {hx, hy, hz[k]}, ihv[3] = {ihx, ihy, ihz[k]};
 #pragma unroll
         for (int t = 0; t < 3; ++t) {
             double f = static_cast<double>(star.sgn[t]);
+            uint32_t const nm = star.num_mask[t], dm = star.den_mask[t];
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) {
-                if (star.num_mask[t] & (1u << ax)) f *= __ldg(geo.h[ax] + p[ax]);
-                if (star.den_mask[t] & (1u << ax)) f *= __ldg(geo.inv_h[ax] + p[ax]);
+                f *= (nm & (1u << ax)) ? hv[ax] : 1.0;
+                f *= (dm & (1u << ax)) ? ihv[ax] : 1.0;
             }
-            r[k][t] = f * v[k][star.src[t]];
+            double const vs = star.src[t] == 0 ? v[k][0] : (star.src[t] == 1 ? v[k][1] : v[k][2]);
+            r[k][t] = f * vs;
         }
     }
     double2* dst = reinterpret_cast<double2*>(out + static_cast<int64_t>(node0) * 3);
