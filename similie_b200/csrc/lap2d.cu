@@ -26,6 +26,32 @@ namespace sil {
 
 namespace {
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialization attribute may start (barrier set-up) while the
+// previous kernel on the stream drains; grid_dependency_wait() returns once
+// that kernel has completed and its writes are visible, so every global
+// access of the kernel comes after it.  Without the attribute both are no-ops.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Launch with the programmatic stream-serialization attribute, so that
+// back-to-back runs overlap one kernel's drain with the next one's set-up.
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args... args)
+{
+    cudaLaunchConfig_t cfg {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // ------------------------------------------------------------------ 0-form
 
 template <class T>
@@ -47,6 +73,8 @@ struct Lap0Params
 template <class T>
 __global__ void __launch_bounds__(256) lap2d_0form_kernel(Lap0Params<T> P)
 {
+    grid_dependency_wait();
+    grid_launch_dependents();
     int64_t const jj = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     int64_t const ii = blockIdx.y;
     if (jj >= P.my || ii >= P.mx) return;
@@ -188,14 +216,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int ma
     }
     return false;
 }
-
-// Programmatic dependent launch: a kernel launched with the programmatic
-// stream-serialization attribute may start (barrier set-up) while the
-// previous kernel on the stream drains; grid_dependency_wait() returns once
-// that kernel has completed and its writes are visible, so every global
-// access of the kernel comes after it.  Without the attribute both are no-ops.
-__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void grid_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, CUtensorMap const* map, uint64_t* bar, int c0, int c1)
 {
@@ -822,13 +842,13 @@ sil_status launch_lap2d_0form(cudaStream_t stream, Geometry const& geo, sil_fiel
                               in.extent[1], in.stride[0], mx, my, out.stride[0], out.front[0] - in.front[0],
                               out.front[1] - in.front[1], geo.h[0] + gx, geo.inv_h[0] + gx, geo.h[1] + gy,
                               geo.inv_h[1] + gy};
-        lap2d_0form_kernel<double><<<grid, block, 0, stream>>>(P);
+        SIL_CUDA_CHECK(launch_pdl(lap2d_0form_kernel<double>, grid, block, 0, stream, P));
     } else {
         Lap0Params<float> P {static_cast<float const*>(in.data), static_cast<float*>(out.data), in.extent[0],
                              in.extent[1], in.stride[0], mx, my, out.stride[0], out.front[0] - in.front[0],
                              out.front[1] - in.front[1], geo.h32[0] + gx, geo.inv_h32[0] + gx, geo.h32[1] + gy,
                              geo.inv_h32[1] + gy};
-        lap2d_0form_kernel<float><<<grid, block, 0, stream>>>(P);
+        SIL_CUDA_CHECK(launch_pdl(lap2d_0form_kernel<float>, grid, block, 0, stream, P));
     }
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
@@ -892,25 +912,6 @@ bool lap2d_1form_tma_ok(sil_field const& in, sil_field const& out)
 }
 
 namespace {
-
-// Launch with the programmatic stream-serialization attribute, so that
-// back-to-back runs overlap one kernel's drain with the next one's set-up.
-template <class... KArgs, class... Args>
-cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t stream,
-                       Args... args)
-{
-    cudaLaunchConfig_t cfg {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, args...);
-}
 
 template <class T, class C>
 int lap1_occupancy()
@@ -1114,11 +1115,12 @@ sil_status launch_lap2d_1form_tma(cudaStream_t stream, Geometry const& geo, sil_
 sil_status autotune_lap2d_1form(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
                                 int* error_flag, int* best_variant, float* best_ms)
 {
-    // Every shape that fits is timed as a CUDA graph of 5 back-to-back
+    // Every shape that fits is timed as a CUDA graph of 10 back-to-back
     // launches (the way repeated runs reach the GPU, the programmatic launch
-    // overlap included), replayed once in each of two rounds that interleave
-    // the shapes; a shape's time is its faster round.
-    constexpr int kLaunches = 5;
+    // overlap included), replayed once in each of three timed rounds that
+    // interleave the shapes, after a warm-up round; a shape's time is its
+    // fastest round.
+    constexpr int kLaunches = 10;
     int const nv = lap1_variant_count(in.dtype == SIL_F64);
     std::vector<cudaGraphExec_t> exec(nv, nullptr);
     std::vector<float> t(nv, 1e30f);
@@ -1154,7 +1156,7 @@ sil_status autotune_lap2d_1form(cudaStream_t stream, Geometry const& geo, sil_fi
         if (graph != nullptr) cudaGraphDestroy(graph);
         if (st == SIL_OK && err != cudaSuccess) st = cuda_fail(err, "autotune graph");
     }
-    for (int round = 0; round < 3 && st == SIL_OK; ++round) {
+    for (int round = 0; round < 4 && st == SIL_OK; ++round) {
         for (int v = 0; v < nv && st == SIL_OK; ++v) {
             if (exec[v] == nullptr) continue;
             cudaEventRecord(e0, stream);

@@ -272,23 +272,20 @@ __device__ T mag3d_apply_row(T const* a, T const* nu, ProbInfo const& pi, int64_
     return res + static_cast<T>(pi.gamma) * ha * a[row];
 }
 
-// All three rows of an interior node at once (the curl moments shared
-// between the components are formed once); each component sums its terms in
-// the order of mag3d_apply_row, so the values are the same.  DEEP: every
-// node of the stencil (offsets -1..1 per axis) is interior, so no neighbour
-// needs the boundary test (the same values, fewer instructions).
-template <class T, bool G, bool DEEP, class LD>
-__device__ __forceinline__ void mag3d_interior_node(LD const& a, T const* nu, ProbInfo const& pi, int node, int i,
-                                                    int j, int k, T* out)
+// The curl-curl part of the three rows of an interior node (i, j, k), from
+// accessors: A(di, dj, dk, c) the 1-form at node (i, j, k) + (di, dj, dk),
+// component c, zero at boundary nodes; NU(oi, oj, ok) the reluctivity at
+// the sampled node (i, j, k) + (oi, oj, ok).  The curl moments shared
+// between the components are formed once; each component sums its terms in
+// the order of mag3d_apply_row, so the values are the same whatever the
+// accessors read from.
+template <class T, class AF, class NF>
+__device__ __forceinline__ void mag3d_curl_rows(AF const& A, NF const& NU, ProbInfo const& pi, int i, int j, int k,
+                                                T* res)
 {
     int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
-    int const row0 = 3 * node;
     auto interior = [&](int ii, int jj, int kk) {
-        return DEEP || (ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz);
-    };
-    int const sy = 3 * nx, sz = 3 * nx * ny;
-    auto A = [&](int di, int dj, int dk, int cc) -> T {
-        return interior(i + di, j + dj, k + dk) ? a(row0 + 3 * di + sy * dj + sz * dk + cc) : T(0);
+        return ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz;
     };
     auto bx = [&](int oi, int oj, int ok) {
         T m = T(0);
@@ -321,7 +318,7 @@ __device__ __forceinline__ void mag3d_interior_node(LD const& a, T const* nu, Pr
     T const* ily = inv_spacing<T>(pi, 1);
     T const* ilz = inv_spacing<T>(pi, 2);
     auto w = [&](int oi, int oj, int ok, int m) -> T {
-        T const nuv = nu[node + oi + nx * oj + nx * ny * ok];
+        T const nuv = NU(oi, oj, ok);
         if (m == 0) return lx[i + oi] * ily[j + oj] * ilz[k + ok] * nuv;
         if (m == 1) return ly[j + oj] * ilx[i + oi] * ilz[k + ok] * nuv;
         return lz[k + ok] * ilx[i + oi] * ily[j + oj] * nuv;
@@ -329,6 +326,62 @@ __device__ __forceinline__ void mag3d_interior_node(LD const& a, T const* nu, Pr
     bool const in_k = interior(i, j, k - 1), in_j = interior(i, j - 1, k), in_i = interior(i - 1, j, k);
     T const Bx = bx(0, 0, 0), By = by(0, 0, 0), Bz = bz(0, 0, 0);
     T const Wx = w(0, 0, 0, 0), Wy = w(0, 0, 0, 1), Wz = w(0, 0, 0, 2);
+    {
+        T r = T(0);
+        r = r - Wy * By;
+        if (in_k) r = r + w(0, 0, -1, 1) * by(0, 0, -1);
+        r = r + Wz * Bz;
+        if (in_j) r = r - w(0, -1, 0, 2) * bz(0, -1, 0);
+        res[0] = r;
+    }
+    {
+        T r = T(0);
+        r = r + Wx * Bx;
+        if (in_k) r = r - w(0, 0, -1, 0) * bx(0, 0, -1);
+        r = r - Wz * Bz;
+        if (in_i) r = r + w(-1, 0, 0, 2) * bz(-1, 0, 0);
+        res[1] = r;
+    }
+    {
+        T r = T(0);
+        r = r - Wx * Bx;
+        if (in_j) r = r + w(0, -1, 0, 0) * bx(0, -1, 0);
+        r = r + Wy * By;
+        if (in_i) r = r - w(-1, 0, 0, 1) * by(-1, 0, 0);
+        res[2] = r;
+    }
+}
+
+// Penalty gauge term of component c at node (i, j, k): gamma (d_a d_b / d_c) A_c.
+template <class T>
+__device__ __forceinline__ T mag3d_penalty(ProbInfo const& pi, int i, int j, int k, int c, T ac)
+{
+    T const g = static_cast<T>(pi.gamma);
+    if (c == 0) return g * (spacing<T>(pi, 1)[j] * spacing<T>(pi, 2)[k] * inv_spacing<T>(pi, 0)[i]) * ac;
+    if (c == 1) return g * (spacing<T>(pi, 0)[i] * spacing<T>(pi, 2)[k] * inv_spacing<T>(pi, 1)[j]) * ac;
+    return g * (spacing<T>(pi, 0)[i] * spacing<T>(pi, 1)[j] * inv_spacing<T>(pi, 2)[k]) * ac;
+}
+
+// All three rows of an interior node at once, reading a through a loader by
+// row index.  DEEP: every node of the stencil (offsets -1..1 per axis) is
+// interior, so no neighbour needs the boundary test (the same values, fewer
+// instructions).
+template <class T, bool G, bool DEEP, class LD>
+__device__ __forceinline__ void mag3d_interior_node(LD const& a, T const* nu, ProbInfo const& pi, int node, int i,
+                                                    int j, int k, T* out)
+{
+    int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
+    int const row0 = 3 * node;
+    auto interior = [&](int ii, int jj, int kk) {
+        return DEEP || (ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz);
+    };
+    int const sy = 3 * nx, sz = 3 * nx * ny;
+    auto A = [&](int di, int dj, int dk, int cc) -> T {
+        return interior(i + di, j + dj, k + dk) ? a(row0 + 3 * di + sy * dj + sz * dk + cc) : T(0);
+    };
+    auto NU = [&](int oi, int oj, int ok) -> T { return nu[node + oi + nx * oj + nx * ny * ok]; };
+    T res[3];
+    mag3d_curl_rows<T>(A, NU, pi, i, j, k, res);
     T const g = static_cast<T>(pi.gamma);
     // gauge term per component: penalty g (d_a d_b / d_c) A_c, or the divergence gauge
     T gt[3];
@@ -341,35 +394,9 @@ __device__ __forceinline__ void mag3d_interior_node(LD const& a, T const* nu, Pr
             gauge_done = true;
         }
     }
-    if (!gauge_done) {
-        gt[0] = g * (ly[j] * lz[k] * ilx[i]) * a(row0);
-        gt[1] = g * (lx[i] * lz[k] * ily[j]) * a(row0 + 1);
-        gt[2] = g * (lx[i] * ly[j] * ilz[k]) * a(row0 + 2);
-    }
-    {
-        T res = T(0);
-        res = res - Wy * By;
-        if (in_k) res = res + w(0, 0, -1, 1) * by(0, 0, -1);
-        res = res + Wz * Bz;
-        if (in_j) res = res - w(0, -1, 0, 2) * bz(0, -1, 0);
-        out[0] = res + gt[0];
-    }
-    {
-        T res = T(0);
-        res = res + Wx * Bx;
-        if (in_k) res = res - w(0, 0, -1, 0) * bx(0, 0, -1);
-        res = res - Wz * Bz;
-        if (in_i) res = res + w(-1, 0, 0, 2) * bz(-1, 0, 0);
-        out[1] = res + gt[1];
-    }
-    {
-        T res = T(0);
-        res = res - Wx * Bx;
-        if (in_j) res = res + w(0, -1, 0, 0) * bx(0, -1, 0);
-        res = res + Wy * By;
-        if (in_i) res = res - w(-1, 0, 0, 1) * by(-1, 0, 0);
-        out[2] = res + gt[2];
-    }
+    if (!gauge_done)
+        for (int c = 0; c < 3; ++c) gt[c] = mag3d_penalty<T>(pi, i, j, k, c, a(row0 + c));
+    for (int c = 0; c < 3; ++c) out[c] = res[c] + gt[c];
 }
 
 // All three rows of a node: identity on the Dirichlet boundary, else the
@@ -1908,6 +1935,74 @@ sil_status check_mag3d(sil_mag3d_problem const& q, char const* who, bool need_fi
     return SIL_OK;
 }
 
+// y = K a for the penalty gauge by z-marching tiles: a CTA owns a 32 x 8
+// tile of (x, y) columns over a run of kZRun planes.  The 1-form of the
+// planes k-1, k, k+1 over the tile and a one-node halo sits in shared memory
+// (zero at boundary nodes, which is what the stencil reads there), with the
+// reluctivity of plane k; the reluctivity one plane down is the value a
+// thread read for its own column the step before.  Each node's neighbours
+// come from shared memory, and mag3d_curl_rows forms its rows with the
+// arithmetic of the per-node kernel, so the two agree bit for bit.
+constexpr int kZTX = 32, kZTY = 8, kZRun = 32;
+constexpr int kZPX = kZTX + 2, kZPY = kZTY + 2;
+
+__global__ void __launch_bounds__(kZTX * kZTY) mag3d_apply_zmarch_kernel(ProbInfo pi, double const* nu,
+                                                                       double const* a, double* y)
+{
+    __shared__ double sa[3][kZPY][kZPX][3];
+    __shared__ double snu[kZPY][kZPX];
+    int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
+    int const tx = static_cast<int>(threadIdx.x) % kZTX, ty = static_cast<int>(threadIdx.x) / kZTX;
+    int const i0 = static_cast<int>(blockIdx.x) * kZTX, j0 = static_cast<int>(blockIdx.y) * kZTY;
+    int const k0 = static_cast<int>(blockIdx.z) * kZRun, k1 = min(nz, k0 + kZRun);
+    int const i = i0 + tx, j = j0 + ty;
+    auto interior = [&](int ii, int jj, int kk) {
+        return ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz;
+    };
+    auto slot = [](int kk) { return (kk + 3) % 3; };
+    auto load_plane = [&](int kk) {
+        double(*dst)[kZPX][3] = sa[slot(kk)];
+        for (int e = static_cast<int>(threadIdx.x); e < kZPY * kZPX * 3; e += kZTX * kZTY) {
+            int const c = e % 3, q = e / 3, xx = q % kZPX, yy = q / kZPX;
+            int const gi = i0 - 1 + xx, gj = j0 - 1 + yy;
+            dst[yy][xx][c] = interior(gi, gj, kk) ? a[3 * (gi + static_cast<int64_t>(nx) * (gj + static_cast<int64_t>(ny) * kk)) + c]
+                                                   : 0.0;
+        }
+    };
+    bool const mine = i < nx && j < ny;
+    int64_t const plane = static_cast<int64_t>(nx) * ny;
+    double nu_down = (mine && k0 > 0) ? nu[i + static_cast<int64_t>(nx) * j + plane * (k0 - 1)] : 0.0;
+    load_plane(k0 - 1);
+    load_plane(k0);
+    for (int k = k0; k < k1; ++k) {
+        load_plane(k + 1);
+        for (int e = static_cast<int>(threadIdx.x); e < kZPY * kZPX; e += kZTX * kZTY) {
+            int const xx = e % kZPX, yy = e / kZPX;
+            int const gi = i0 - 1 + xx, gj = j0 - 1 + yy;
+            snu[yy][xx] = (gi >= 0 && gj >= 0 && gi < nx && gj < ny) ? nu[gi + static_cast<int64_t>(nx) * gj + plane * k] : 0.0;
+        }
+        __syncthreads();
+        if (mine) {
+            int64_t const node = i + static_cast<int64_t>(nx) * j + plane * k;
+            if (!interior(i, j, k)) {
+                for (int c = 0; c < 3; ++c) y[3 * node + c] = a[3 * node + c];
+            } else {
+                auto A = [&](int di, int dj, int dk, int c) -> double {
+                    return sa[slot(k + dk)][ty + 1 + dj][tx + 1 + di][c];
+                };
+                auto NU = [&](int oi, int oj, int ok) -> double {
+                    return ok == 0 ? snu[ty + 1 + oj][tx + 1 + oi] : nu_down;
+                };
+                double res[3];
+                mag3d_curl_rows<double>(A, NU, pi, i, j, k, res);
+                for (int c = 0; c < 3; ++c) y[3 * node + c] = res[c] + mag3d_penalty<double>(pi, i, j, k, c, A(0, 0, 0, c));
+            }
+            nu_down = snu[ty + 1][tx + 1];
+        }
+        __syncthreads();
+    }
+}
+
 // G: the divergence-gauge variant (the penalty variant keeps fewer registers).
 template <bool G>
 __global__ void __launch_bounds__(256, 4) mag3d_apply_kernel(ProbInfo pi, double const* nu, double const* a, double* y)
@@ -2090,8 +2185,13 @@ sil_status sil_mag3d_operator_apply(sil_mag3d_operator op, sil_stream stream, co
 {
     if (op == nullptr || a == nullptr || y == nullptr) return fail(SIL_ERR_INVALID, "sil_mag3d_operator_apply: NULL pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    auto const kern = op->pi.gauge ? mag3d_apply_kernel<true> : mag3d_apply_kernel<false>;
-    kern<<<static_cast<int>((op->pi.nodes + 255) / 256), 256, 0, s>>>(op->pi, op->nu, a, y);
+    if (op->pi.gauge) {
+        mag3d_apply_kernel<true><<<static_cast<int>((op->pi.nodes + 255) / 256), 256, 0, s>>>(op->pi, op->nu, a, y);
+    } else {
+        dim3 const grid(static_cast<unsigned>((op->pi.nx + kZTX - 1) / kZTX), static_cast<unsigned>((op->pi.ny + kZTY - 1) / kZTY),
+                        static_cast<unsigned>((op->pi.nz + kZRun - 1) / kZRun));
+        mag3d_apply_zmarch_kernel<<<grid, kZTX * kZTY, 0, s>>>(op->pi, op->nu, a, y);
+    }
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }

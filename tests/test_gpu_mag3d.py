@@ -47,13 +47,16 @@ def test_apply_matches_oracle(torch, m3, shape, ratio, gamma):
     assert rel_err(ty.cpu().numpy(), ref) <= 1e-12
 
 
+@pytest.mark.parametrize("shape", [(13, 10, 9), (40, 17, 70), (3, 3, 3), (33, 9, 33)])
 @pytest.mark.parametrize("gauge", ["penalty", "divergence"])
-def test_operator_object_matches_the_per_call_apply(torch, m3, gauge):
+def test_operator_object_matches_the_per_call_apply(torch, m3, gauge, shape):
     """The operator object (set-up once, one kernel per apply, replayable from
-    a CUDA graph) gives the per-call apply's result bit for bit, and the
-    oracle's to 1e-12 (penalty gauge)."""
+    a CUDA graph; the penalty gauge by z-marching tiles with the planes in
+    shared memory) gives the per-call apply's result (one thread per node)
+    bit for bit, and the oracle's to 1e-12 (penalty gauge); the shapes
+    cover partial tiles in x and y and several z runs."""
     rng = np.random.default_rng(31)
-    nx, ny, nz = 13, 10, 9
+    nx, ny, nz = shape
     x, y, z, cell_mu = _grid(m3, rng, nx, ny, nz, 1.03)
     mu_h = m3.node_mu(nx, ny, nz, cell_mu)
     mu = torch.from_numpy(mu_h).cuda()
