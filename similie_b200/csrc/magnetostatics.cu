@@ -1935,74 +1935,6 @@ sil_status check_mag3d(sil_mag3d_problem const& q, char const* who, bool need_fi
     return SIL_OK;
 }
 
-// y = K a for the penalty gauge by z-marching tiles: a CTA owns a 32 x 8
-// tile of (x, y) columns over a run of kZRun planes.  The 1-form of the
-// planes k-1, k, k+1 over the tile and a one-node halo sits in shared memory
-// (zero at boundary nodes, which is what the stencil reads there), with the
-// reluctivity of plane k; the reluctivity one plane down is the value a
-// thread read for its own column the step before.  Each node's neighbours
-// come from shared memory, and mag3d_curl_rows forms its rows with the
-// arithmetic of the per-node kernel, so the two agree bit for bit.
-constexpr int kZTX = 32, kZTY = 8, kZRun = 32;
-constexpr int kZPX = kZTX + 2, kZPY = kZTY + 2;
-
-__global__ void __launch_bounds__(kZTX * kZTY) mag3d_apply_zmarch_kernel(ProbInfo pi, double const* nu,
-                                                                       double const* a, double* y)
-{
-    __shared__ double sa[3][kZPY][kZPX][3];
-    __shared__ double snu[kZPY][kZPX];
-    int const nx = static_cast<int>(pi.nx), ny = static_cast<int>(pi.ny), nz = static_cast<int>(pi.nz);
-    int const tx = static_cast<int>(threadIdx.x) % kZTX, ty = static_cast<int>(threadIdx.x) / kZTX;
-    int const i0 = static_cast<int>(blockIdx.x) * kZTX, j0 = static_cast<int>(blockIdx.y) * kZTY;
-    int const k0 = static_cast<int>(blockIdx.z) * kZRun, k1 = min(nz, k0 + kZRun);
-    int const i = i0 + tx, j = j0 + ty;
-    auto interior = [&](int ii, int jj, int kk) {
-        return ii > 0 && jj > 0 && kk > 0 && ii + 1 < nx && jj + 1 < ny && kk + 1 < nz;
-    };
-    auto slot = [](int kk) { return (kk + 3) % 3; };
-    auto load_plane = [&](int kk) {
-        double(*dst)[kZPX][3] = sa[slot(kk)];
-        for (int e = static_cast<int>(threadIdx.x); e < kZPY * kZPX * 3; e += kZTX * kZTY) {
-            int const c = e % 3, q = e / 3, xx = q % kZPX, yy = q / kZPX;
-            int const gi = i0 - 1 + xx, gj = j0 - 1 + yy;
-            dst[yy][xx][c] = interior(gi, gj, kk) ? a[3 * (gi + static_cast<int64_t>(nx) * (gj + static_cast<int64_t>(ny) * kk)) + c]
-                                                   : 0.0;
-        }
-    };
-    bool const mine = i < nx && j < ny;
-    int64_t const plane = static_cast<int64_t>(nx) * ny;
-    double nu_down = (mine && k0 > 0) ? nu[i + static_cast<int64_t>(nx) * j + plane * (k0 - 1)] : 0.0;
-    load_plane(k0 - 1);
-    load_plane(k0);
-    for (int k = k0; k < k1; ++k) {
-        load_plane(k + 1);
-        for (int e = static_cast<int>(threadIdx.x); e < kZPY * kZPX; e += kZTX * kZTY) {
-            int const xx = e % kZPX, yy = e / kZPX;
-            int const gi = i0 - 1 + xx, gj = j0 - 1 + yy;
-            snu[yy][xx] = (gi >= 0 && gj >= 0 && gi < nx && gj < ny) ? nu[gi + static_cast<int64_t>(nx) * gj + plane * k] : 0.0;
-        }
-        __syncthreads();
-        if (mine) {
-            int64_t const node = i + static_cast<int64_t>(nx) * j + plane * k;
-            if (!interior(i, j, k)) {
-                for (int c = 0; c < 3; ++c) y[3 * node + c] = a[3 * node + c];
-            } else {
-                auto A = [&](int di, int dj, int dk, int c) -> double {
-                    return sa[slot(k + dk)][ty + 1 + dj][tx + 1 + di][c];
-                };
-                auto NU = [&](int oi, int oj, int ok) -> double {
-                    return ok == 0 ? snu[ty + 1 + oj][tx + 1 + oi] : nu_down;
-                };
-                double res[3];
-                mag3d_curl_rows<double>(A, NU, pi, i, j, k, res);
-                for (int c = 0; c < 3; ++c) y[3 * node + c] = res[c] + mag3d_penalty<double>(pi, i, j, k, c, A(0, 0, 0, c));
-            }
-            nu_down = snu[ty + 1][tx + 1];
-        }
-        __syncthreads();
-    }
-}
-
 // G: the divergence-gauge variant (the penalty variant keeps fewer registers).
 template <bool G>
 __global__ void __launch_bounds__(256, 4) mag3d_apply_kernel(ProbInfo pi, double const* nu, double const* a, double* y)
@@ -2185,13 +2117,8 @@ sil_status sil_mag3d_operator_apply(sil_mag3d_operator op, sil_stream stream, co
 {
     if (op == nullptr || a == nullptr || y == nullptr) return fail(SIL_ERR_INVALID, "sil_mag3d_operator_apply: NULL pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (op->pi.gauge) {
-        mag3d_apply_kernel<true><<<static_cast<int>((op->pi.nodes + 255) / 256), 256, 0, s>>>(op->pi, op->nu, a, y);
-    } else {
-        dim3 const grid(static_cast<unsigned>((op->pi.nx + kZTX - 1) / kZTX), static_cast<unsigned>((op->pi.ny + kZTY - 1) / kZTY),
-                        static_cast<unsigned>((op->pi.nz + kZRun - 1) / kZRun));
-        mag3d_apply_zmarch_kernel<<<grid, kZTX * kZTY, 0, s>>>(op->pi, op->nu, a, y);
-    }
+    auto const kern = op->pi.gauge ? mag3d_apply_kernel<true> : mag3d_apply_kernel<false>;
+    kern<<<static_cast<int>((op->pi.nodes + 255) / 256), 256, 0, s>>>(op->pi, op->nu, a, y);
     SIL_CUDA_CHECK(cudaGetLastError());
     return SIL_OK;
 }

@@ -51,10 +51,9 @@ def test_apply_matches_oracle(torch, m3, shape, ratio, gamma):
 @pytest.mark.parametrize("gauge", ["penalty", "divergence"])
 def test_operator_object_matches_the_per_call_apply(torch, m3, gauge, shape):
     """The operator object (set-up once, one kernel per apply, replayable from
-    a CUDA graph; the penalty gauge by z-marching tiles with the planes in
-    shared memory) gives the per-call apply's result (one thread per node)
-    bit for bit, and the oracle's to 1e-12 (penalty gauge); the shapes
-    cover partial tiles in x and y and several z runs."""
+    a CUDA graph) gives the per-call apply's result bit for bit, and the
+    oracle's to 1e-12 (penalty gauge), on grids with and without
+    deep-interior nodes."""
     rng = np.random.default_rng(31)
     nx, ny, nz = shape
     x, y, z, cell_mu = _grid(m3, rng, nx, ny, nz, 1.03)
