@@ -1115,21 +1115,27 @@ sil_status launch_lap2d_1form_tma(cudaStream_t stream, Geometry const& geo, sil_
 sil_status autotune_lap2d_1form(cudaStream_t stream, Geometry const& geo, sil_field const& in, sil_field const& out,
                                 int* error_flag, int* best_variant, float* best_ms)
 {
-    // Every shape that fits is timed as a CUDA graph of 10 back-to-back
-    // launches (the way repeated runs reach the GPU, the programmatic launch
-    // overlap included), replayed once in each of three timed rounds that
-    // interleave the shapes, after a warm-up round; a shape's time is its
-    // fastest round.
-    constexpr int kLaunches = 10;
+    // Shapes are timed as CUDA graphs of back-to-back launches (the way
+    // repeated runs reach the GPU, the programmatic launch overlap included).
+    // Screening: every shape that fits, a graph of 10 launches replayed in a
+    // warm-up and two timed rounds that interleave the shapes.  Final: the
+    // two fastest, a graph of 40 launches each, alternated over three timed
+    // rounds after a warm-up; a shape's time is its fastest round.
     int const nv = lap1_variant_count(in.dtype == SIL_F64);
     std::vector<cudaGraphExec_t> exec(nv, nullptr);
     std::vector<float> t(nv, 1e30f);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaStream_t cs = nullptr;
     sil_status st = SIL_OK;
-    auto cleanup = [&]() {
+    auto drop_graphs = [&]() {
         for (cudaGraphExec_t& g : exec)
-            if (g != nullptr) cudaGraphExecDestroy(g);
+            if (g != nullptr) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    };
+    auto cleanup = [&]() {
+        drop_graphs();
         if (e0 != nullptr) cudaEventDestroy(e0);
         if (e1 != nullptr) cudaEventDestroy(e1);
         if (cs != nullptr) cudaStreamDestroy(cs);
@@ -1139,6 +1145,35 @@ sil_status autotune_lap2d_1form(cudaStream_t stream, Geometry const& geo, sil_fi
         cleanup();
         return fail(SIL_ERR_CUDA, "autotune: event or stream creation failed");
     }
+    auto capture = [&](int v, int launches) -> sil_status {
+        cudaGraph_t graph = nullptr;
+        sil_status cst = SIL_OK;
+        cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        for (int i = 0; i < launches && err == cudaSuccess && cst == SIL_OK; ++i)
+            cst = launch_lap2d_1form_tma(cs, geo, in, out, error_flag, v);
+        cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
+        if (err == cudaSuccess) err = err2;
+        if (err == cudaSuccess && cst == SIL_OK) err = cudaGraphInstantiate(&exec[v], graph, 0);
+        if (graph != nullptr) cudaGraphDestroy(graph);
+        if (cst != SIL_OK) return cst;
+        return err == cudaSuccess ? SIL_OK : cuda_fail(err, "autotune graph");
+    };
+    auto rounds = [&](std::vector<int> const& vs, int launches, int timed) -> sil_status {
+        for (int round = 0; round <= timed; ++round) {
+            for (int v : vs) {
+                cudaEventRecord(e0, stream);
+                cudaError_t err = cudaGraphLaunch(exec[v], stream);
+                cudaEventRecord(e1, stream);
+                if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+                if (err != cudaSuccess) return cuda_fail(err, "autotune");
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (round > 0) t[v] = std::min(t[v], ms / launches);  // round 0 warms up
+            }
+        }
+        return SIL_OK;
+    };
+    std::vector<int> fit;
     for (int v = 0; v < nv && st == SIL_OK; ++v) {
         sil_status const probe = launch_lap2d_1form_tma(stream, geo, in, out, error_flag, v);
         if (probe == SIL_ERR_UNSUPPORTED) continue;  // does not fit: skip
@@ -1146,35 +1181,26 @@ sil_status autotune_lap2d_1form(cudaStream_t stream, Geometry const& geo, sil_fi
             st = probe;
             break;
         }
-        cudaGraph_t graph = nullptr;
-        cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-        for (int i = 0; i < kLaunches && err == cudaSuccess && st == SIL_OK; ++i)
-            st = launch_lap2d_1form_tma(cs, geo, in, out, error_flag, v);
-        cudaError_t const err2 = cudaStreamEndCapture(cs, &graph);
-        if (err == cudaSuccess) err = err2;
-        if (err == cudaSuccess && st == SIL_OK) err = cudaGraphInstantiate(&exec[v], graph, 0);
-        if (graph != nullptr) cudaGraphDestroy(graph);
-        if (st == SIL_OK && err != cudaSuccess) st = cuda_fail(err, "autotune graph");
+        st = capture(v, 10);
+        if (st == SIL_OK) fit.push_back(v);
     }
-    for (int round = 0; round < 4 && st == SIL_OK; ++round) {
-        for (int v = 0; v < nv && st == SIL_OK; ++v) {
-            if (exec[v] == nullptr) continue;
-            cudaEventRecord(e0, stream);
-            cudaError_t err = cudaGraphLaunch(exec[v], stream);
-            cudaEventRecord(e1, stream);
-            if (err == cudaSuccess) err = cudaEventSynchronize(e1);
-            if (err != cudaSuccess) {
-                st = cuda_fail(err, "autotune");
-                break;
-            }
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (round > 0) t[v] = std::min(t[v], ms / kLaunches);  // round 0 warms up
+    if (st == SIL_OK) st = rounds(fit, 10, 2);
+    if (st == SIL_OK && fit.size() > 1) {
+        std::vector<int> top = fit;
+        std::sort(top.begin(), top.end(), [&](int a, int b) { return t[a] < t[b]; });
+        top.resize(2);
+        drop_graphs();
+        for (int v : top) {
+            t[v] = 1e30f;
+            if (st == SIL_OK) st = capture(v, 40);
         }
+        for (int v : fit)
+            if (v != top[0] && v != top[1]) t[v] = 1e30f;
+        if (st == SIL_OK) st = rounds(top, 40, 3);
     }
     cleanup();
-    int best_v = 0;
-    for (int v = 1; v < nv; ++v)
+    int best_v = fit.empty() ? 0 : fit[0];
+    for (int v : fit)
         if (t[v] < t[best_v]) best_v = v;
     *best_variant = best_v;
     *best_ms = t[best_v];
