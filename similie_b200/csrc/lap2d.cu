@@ -166,7 +166,9 @@ struct Lap1Params
     int mx, my;                // output extents
     int ox, oy;                // output front relative to the input front
     int strips;                // column strips of width kTJ over the output
-    int64_t work;              // strips * mx (strip-major row items)
+    int band;                  // rows per band
+    int64_t work;              // bands * strips * band row items, band-major: the
+                               // strips of one band of rows are consecutive items
     T const* hx;               // padded spacing arrays [p + 1] (inverse pads are 0)
     T const* ihx;
     T const* hy;
@@ -226,7 +228,10 @@ __device__ __forceinline__ void tma_load_2d(void* dst, CUtensorMap const* map, u
 }
 
 // One strip segment of the persistent work split: strip, output rows
-// [r_begin, r_end) relative to the output front.
+// [r_begin, r_end) relative to the output front (empty for the items of the
+// last band that lie past the output).  The items run band by band, and
+// within a band strip by strip, so the CTAs working at the same time read
+// neighbouring pieces of the same rows.
 struct Segment
 {
     int strip, r_begin, r_end;
@@ -236,10 +241,13 @@ template <class T>
 __device__ __forceinline__ Segment next_segment(Lap1Params<T> const& P, int64_t& item, int64_t end)
 {
     Segment s;
-    s.strip = static_cast<int>(item / P.mx);
-    s.r_begin = static_cast<int>(item % P.mx);
-    int64_t const len = min(end - item, static_cast<int64_t>(P.mx - s.r_begin));
-    s.r_end = s.r_begin + static_cast<int>(len);
+    int64_t const blk = item / P.band;
+    int const r = static_cast<int>(item - blk * P.band);
+    s.strip = static_cast<int>(blk % P.strips);
+    int const b = static_cast<int>(blk / P.strips);
+    int64_t const len = min(end - item, static_cast<int64_t>(P.band - r));
+    s.r_begin = b * P.band + r;
+    s.r_end = min(s.r_begin + static_cast<int>(len), P.mx);
     item += len;
     return s;
 }
@@ -285,6 +293,7 @@ lap2d_1form_tma_kernel(const __grid_constant__ CUtensorMap map_main, const __gri
         int64_t item = begin;
         while (item < end && ok) {
             Segment const sg = next_segment(P, item, end);
+            if (sg.r_end <= sg.r_begin) continue;
             int const col0 = P.oy + sg.strip * kTJ;
             int const load_row0 = P.ox + sg.r_begin - 1;
             int const nload = sg.r_end - sg.r_begin + 2;
@@ -360,6 +369,7 @@ lap2d_1form_tma_kernel(const __grid_constant__ CUtensorMap map_main, const __gri
     int64_t item = begin;
     while (item < end) {
         Segment const sg = next_segment(P, item, end);
+        if (sg.r_end <= sg.r_begin) continue;
         int const col0 = P.oy + sg.strip * kTJ;
         int const j = col0 + tid;
         int const i_first = P.ox + sg.r_begin;
@@ -549,6 +559,7 @@ lap2d_1form_pair_kernel(const __grid_constant__ CUtensorMap map_main, const __gr
         int64_t item = begin;
         while (item < end && ok) {
             Segment const sg = next_segment(P, item, end);
+            if (sg.r_end <= sg.r_begin) continue;
             int const col0 = P.oy + sg.strip * kTJ2;
             int const load_row0 = P.ox + sg.r_begin - 1;
             int const nload = sg.r_end - sg.r_begin + 2;
@@ -621,6 +632,7 @@ lap2d_1form_pair_kernel(const __grid_constant__ CUtensorMap map_main, const __gr
     int64_t item = begin;
     while (item < end) {
         Segment const sg = next_segment(P, item, end);
+        if (sg.r_end <= sg.r_begin) continue;
         int const col0 = P.oy + sg.strip * kTJ2;
         int const jA = col0 + 2 * tid;
         int const i_first = P.ox + sg.r_begin;
@@ -954,17 +966,19 @@ sil_status launch_variant(cudaStream_t stream, Geometry const& geo, sil_field co
     int const occ = lap1_occupancy<T, C>();
     if (occ < 1) return fail(SIL_ERR_UNSUPPORTED, "1-form Laplacian variant does not fit on an SM");
     int const strips = static_cast<int>((my + kTJ - 1) / kTJ);
-    int64_t const work = static_cast<int64_t>(strips) * mx;
     int const per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, occ) : occ;
-    int64_t ctas = std::min<int64_t>(work, static_cast<int64_t>(sm_count()) * per_sm);
+    int64_t ctas = std::min<int64_t>(static_cast<int64_t>(strips) * mx, static_cast<int64_t>(sm_count()) * per_sm);
     if (ctas < 1) ctas = 1;
+    int const bands = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(mx, ctas / strips)));
+    int const band = static_cast<int>((mx + bands - 1) / bands);
+    int64_t const work = static_cast<int64_t>(bands) * strips * band;
     int64_t const gx = in.front[0] - geo.front[0], gy = in.front[1] - geo.front[1];
     T const* const* gh = reinterpret_cast<T const* const*>(f64 ? (void const*)geo.h : (void const*)geo.h32);
     T const* const* gih = reinterpret_cast<T const* const*>(f64 ? (void const*)geo.inv_h : (void const*)geo.inv_h32);
     Lap1Params<T> P {static_cast<T*>(out.data), out.stride[0], static_cast<int>(nx), static_cast<int>(ny),
                      static_cast<int>(mx), static_cast<int>(my), static_cast<int>(out.front[0] - in.front[0]),
-                     static_cast<int>(out.front[1] - in.front[1]), strips, work, gh[0] + gx, gih[0] + gx, gh[1] + gy,
-                     gih[1] + gy, error_flag, wait_tries};
+                     static_cast<int>(out.front[1] - in.front[1]), strips, band, work, gh[0] + gx, gih[0] + gx,
+                     gh[1] + gy, gih[1] + gy, error_flag, wait_tries};
     SIL_CUDA_CHECK(launch_pdl(lap2d_1form_tma_kernel<T, C>, static_cast<unsigned>(ctas), kThreads1, C::kSmemBytes, stream,
                               map_main, map_halo, P));
     return SIL_OK;
@@ -1010,14 +1024,16 @@ sil_status launch_pair_variant(cudaStream_t stream, Geometry const& geo, sil_fie
     int const occ = lap1_pair_occupancy<C>();
     if (occ < 1) return fail(SIL_ERR_UNSUPPORTED, "1-form Laplacian pair variant does not fit on an SM");
     int const strips = static_cast<int>((my + kTJ2 - 1) / kTJ2);
-    int64_t const work = static_cast<int64_t>(strips) * mx;
-    int64_t ctas = std::min<int64_t>(work, static_cast<int64_t>(sm_count()) * occ);
+    int64_t ctas = std::min<int64_t>(static_cast<int64_t>(strips) * mx, static_cast<int64_t>(sm_count()) * occ);
     if (ctas < 1) ctas = 1;
+    int const bands = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(mx, ctas / strips)));
+    int const band = static_cast<int>((mx + bands - 1) / bands);
+    int64_t const work = static_cast<int64_t>(bands) * strips * band;
     int64_t const gx = in.front[0] - geo.front[0], gy = in.front[1] - geo.front[1];
     Lap1Params<double> P {static_cast<double*>(out.data), out.stride[0], static_cast<int>(nx), static_cast<int>(ny),
                           static_cast<int>(mx), static_cast<int>(my), static_cast<int>(out.front[0] - in.front[0]),
-                          static_cast<int>(out.front[1] - in.front[1]), strips, work, geo.h[0] + gx, geo.inv_h[0] + gx,
-                          geo.h[1] + gy, geo.inv_h[1] + gy, error_flag, wait_tries};
+                          static_cast<int>(out.front[1] - in.front[1]), strips, band, work, geo.h[0] + gx,
+                          geo.inv_h[0] + gx, geo.h[1] + gy, geo.inv_h[1] + gy, error_flag, wait_tries};
     SIL_CUDA_CHECK(launch_pdl(lap2d_1form_pair_kernel<C>, static_cast<unsigned>(ctas), kThreads1, C::kSmemBytes, stream,
                               map_main, map_halo, P));
     return SIL_OK;
