@@ -698,6 +698,39 @@ __global__ void __launch_bounds__(kThreads) cg_dir_apply_kernel(Item const* item
     }
 }
 
+// The apply of a batch whose problems are all 3D (the direction formed by
+// cg_direction3_kernel): the 3D rows of cg_dir_apply_kernel in a kernel of
+// their own, so the register budget is the 3D stencil's and three CTAs fit
+// on a multiprocessor (two for the combined kernel).
+template <class T, bool G = false>
+__global__ void __launch_bounds__(kThreads, 3) cg_apply3_kernel(Item const* items, int const* act, ProbInfo const* info,
+                                                                Vecs<T> const* vecs, Scalars* sc, double* part)
+{
+    __shared__ double red[kThreads / 32];
+    Item const it = items[act[blockIdx.x]];
+    Scalars* s = sc + it.prob;
+    if (s->done || s->outer_done) return;
+    ProbInfo const pi = info[it.prob];
+    Vecs<T> const v = vecs[it.prob];
+    T const* pnew = s->pbuf == 0 ? v.p2 : v.p;
+    double pq = 0.0;
+    for (int64_t node = it.begin / 3 + threadIdx.x; node < it.end / 3; node += kThreads) {
+        T q[3];
+        mag3d_apply_node<T, G>(pnew, v.nu, pi, static_cast<int>(node), q);
+        for (int cc = 0; cc < 3; ++cc) {
+            int const row = static_cast<int>(3 * node + cc);
+            v.q[row] = q[cc];
+            pq += static_cast<double>(pnew[row]) * static_cast<double>(q[cc]);
+        }
+    }
+    double const pq_b = block_sum(pq, red);
+    double tot = 0.0;
+    if (finish_reduction(pq_b, part, it.index, pi.first_item, pi.nitems, &s->counter_a, &tot)) {
+        s->alpha = s->rz / tot;
+        if (!isfinite(s->alpha)) s->nonfinite = 1;
+    }
+}
+
 // p = z + beta p_old into the other direction buffer, for the 3D problems of
 // the batch (2D problems form it inside cg_dir_apply_kernel).
 template <class T>
@@ -1445,6 +1478,7 @@ sil_status solve_batch_rows(std::vector<ProblemDesc> const& probs, sil_solve_set
     open_host.reserve(nitems);
     int captured_n = -1;
     bool const any3d = std::any_of(probs.begin(), probs.end(), [](ProblemDesc const& q) { return q.dim == 3; });
+    bool const all3d = std::all_of(probs.begin(), probs.end(), [](ProblemDesc const& q) { return q.dim == 3; });
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     auto build_open = [&]() {
@@ -1464,7 +1498,8 @@ sil_status solve_batch_rows(std::vector<ProblemDesc> const& probs, sil_solve_set
         cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         for (int c = 0; c < chunk && err == cudaSuccess; ++c) {
             if (any3d) cg_direction3_kernel<T><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc);
-            if (any_gauge) cg_dir_apply_kernel<T, true><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_a);
+            if (all3d && !any_gauge) cg_apply3_kernel<T, false><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_a);
+            else if (any_gauge) cg_dir_apply_kernel<T, true><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_a);
             else cg_dir_apply_kernel<T, false><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_a);
             cg_update_kernel<T><<<n, kThreads, 0, cs>>>(d_items, d_act, d_info, d_vecs, d_sc, part_b, part_c);
         }
