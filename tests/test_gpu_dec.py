@@ -443,3 +443,49 @@ def test_vector_laplacian_4096_windows(torch, sil):
         vj1 = (b1 - b0) - (1 if b1 == n else m)
         got = res[a0 + vi0:a0 + vi1, b0 + vj0:b0 + vj1]
         assert rel_err(got, ref[vi0:vi1, vj0:vj1]) <= TOL, (i0, j0)
+
+
+@pytest.mark.parametrize("k,n", [(1, 700), (0, 600)])
+def test_chained_runs_read_the_previous_runs_output(torch, sil, k, n):
+    """Back-to-back runs where each run reads the previous run's output, with
+    no synchronisation between them and again replayed from a CUDA graph: the
+    kernels may start early (programmatic dependent launch) but read their
+    input only once the previous run has finished, so the chain equals the
+    one run step by step with a synchronisation after each, bit for bit."""
+    rng = np.random.default_rng(40 + k)
+    coords = _two_d_case(rng, n, n)
+    geo = _geometry(sil, coords)
+    nc = 2 if k == 1 else 1
+    fields = [dev(torch, rng.standard_normal((n, n, nc)))]
+    for s in range(1, 4):
+        fields.append(torch.full((n - s, n - s, nc), float("nan"), device="cuda", dtype=torch.float64))
+    plans = [sil.make_staged_laplacian(geo, fields[s + 1], fields[s], k) for s in range(3)]
+    for s, p in enumerate(plans):
+        assert p.kernel == (2 if k == 1 else 1)
+        p.run(fields[s + 1], fields[s])
+        torch.cuda.synchronize()
+        p.status()
+    ref = fields[3].clone()
+    for _ in range(3):
+        for f in fields[1:]:
+            f.fill_(float("nan"))
+        for s, p in enumerate(plans):
+            p.run(fields[s + 1], fields[s])
+        torch.cuda.synchronize()
+        assert torch.equal(fields[3], ref)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for s, p in enumerate(plans):
+            p.run(fields[s + 1], fields[s])
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for s, p in enumerate(plans):
+            p.run(fields[s + 1], fields[s])
+    for _ in range(3):
+        for f in fields[1:]:
+            f.fill_(float("nan"))
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(fields[3], ref)
