@@ -18,7 +18,10 @@ last).  With `emulate=True` every value the GPU stores in BF16 (activations,
 pooled inputs, masked gradients fed to the tensor cores, the 32->32 weights)
 is rounded to BF16 here at the same point (the decoder input skip +
 up(coarse) is a sum of two BF16 tensors that the tensor core accumulates in
-FP32, so it is not rounded), so the GPU's results differ only by FP32 summation order; with
+FP32 in the GPU's training pass, so it is not rounded; the GPU's inference
+pass rounds that sum to BF16 once before its decoder convolution, which
+this restatement does not), so the GPU's training-pass results differ only
+by FP32 summation order; with
 `emulate=False` the whole computation is float64, which the finite-difference
 test uses to pin the backward pass.
 """

@@ -1057,6 +1057,23 @@ __global__ void copy_act_kernel(const __grid_constant__ Table t, bf16 const* src
     });
 }
 
+// Decoder input of the inference pass: skip + nearest-upsampled coarse
+// features summed in FP32 and stored in BF16 (zero border), so the decoder
+// convolution reads one operand through the pipelined plain mode.  (The
+// training pass keeps the two operands, which the tensor core sums in FP32,
+// because the weight gradient needs them apart.)
+__global__ void upadd_kernel(const __grid_constant__ Table t, bf16 const* skip, bf16 const* coarse, bf16* out)
+{
+    __shared__ int64_t pre[kMaxImages + 1];
+    walk_active(t, pre, 1, [&](int im, int g) {
+        uint4 v[kChunks];
+        load_pixel(kUpAdd, t, im, g, skip, coarse, nullptr, v);
+        uint4* dst = reinterpret_cast<uint4*>(out) + (t.img[im].offset + g) * kChunks;
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) dst[c] = v[c];
+    });
+}
+
 // ------------------------------------------------------------------ node-level wrapper (FP32)
 
 struct Samples
@@ -1713,8 +1730,8 @@ int g_sms = 0;  // multiprocessor count, read once (outside any stream capture)
 int g_conv_per_sm[5] = {0, 0, 0, 0, 0};  // resident conv CTAs per SM, by input mode
 // Grid-stride kernels of the forward pass and their resident blocks per SM.
 enum WalkKind { kWalkInc = 0, kWalkOut, kWalkGather, kWalkPool, kWalkCopy, kWalkFeat, kWalkPre, kWalkPost, kWalkLogNu,
-                kWalkE2, kWalkKinds };
-int g_walk_per_sm[kWalkKinds] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+                kWalkE2, kWalkUpAdd, kWalkKinds };
+int g_walk_per_sm[kWalkKinds] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
 
 sil_status ensure_attributes()
 {
@@ -1749,7 +1766,8 @@ sil_status ensure_attributes()
         reinterpret_cast<void const*>(out_gather_kernel),  reinterpret_cast<void const*>(pool_kernel),
         reinterpret_cast<void const*>(copy_act_kernel),    reinterpret_cast<void const*>(features_kernel),
         reinterpret_cast<void const*>(wrap_pre_kernel),    reinterpret_cast<void const*>(wrap_post_kernel),
-        reinterpret_cast<void const*>(lognu_feature_kernel), reinterpret_cast<void const*>(wrap_e2_kernel)};
+        reinterpret_cast<void const*>(lognu_feature_kernel), reinterpret_cast<void const*>(wrap_e2_kernel),
+        reinterpret_cast<void const*>(upadd_kernel)};
     for (int k = 0; k < kWalkKinds; ++k) {
         cudaFuncAttributes a {};
         SIL_CUDA_CHECK(cudaFuncGetAttributes(&a, walk_fns[k]));
@@ -1972,10 +1990,21 @@ sil_status net_forward(Net& net, Workspace& w, cudaStream_t st, bool keep)
     for (int l = D - 2; l >= 0; --l) {
         int const wl = weight_level_dec(l);
         Table const tt = dec_table(w, l);
+        if (tt.nimg == 0) continue;
         bool const fold = l == 0 && !keep;
-        sil_status const s = launch_conv(st, tt, kUpAdd, w.h[l].as<bf16>(), w.g[l + 1].as<bf16>(), nullptr,
-                                         big_w(net, kDec, wl), big_b(net, kDec, wl), 1, fold ? nullptr : w.g[l].as<bf16>(),
-                                         nullptr, 0, err, fold ? w.taps.as<float>() : nullptr, net.params + kOffOut, top);
+        sil_status s;
+        if (keep) {
+            s = launch_conv(st, tt, kUpAdd, w.h[l].as<bf16>(), w.g[l + 1].as<bf16>(), nullptr, big_w(net, kDec, wl),
+                            big_b(net, kDec, wl), 1, w.g[l].as<bf16>(), nullptr, 0, err);
+        } else {
+            // the pooled input of this level (pin) has been consumed by the encoder: it holds the sum
+            upadd_kernel<<<walk_grid(tt, 1, kWalkUpAdd), 256, 0, st>>>(tt, w.h[l].as<bf16>(), w.g[l + 1].as<bf16>(),
+                                                                       w.pin[l].as<bf16>());
+            SIL_CUDA_CHECK(cudaGetLastError());
+            s = launch_conv(st, tt, kPlain, w.pin[l].as<bf16>(), nullptr, nullptr, big_w(net, kDec, wl),
+                            big_b(net, kDec, wl), 1, fold ? nullptr : w.g[l].as<bf16>(), nullptr, 0, err,
+                            fold ? w.taps.as<float>() : nullptr, net.params + kOffOut, top);
+        }
         if (s != SIL_OK) return s;
     }
     if (keep) {
