@@ -26,32 +26,6 @@ namespace sil {
 
 namespace {
 
-// Programmatic dependent launch: a kernel launched with the programmatic
-// stream-serialization attribute may start (barrier set-up) while the
-// previous kernel on the stream drains; grid_dependency_wait() returns once
-// that kernel has completed and its writes are visible, so every global
-// access of the kernel comes after it.  Without the attribute both are no-ops.
-__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void grid_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-// Launch with the programmatic stream-serialization attribute, so that
-// back-to-back runs overlap one kernel's drain with the next one's set-up.
-template <class... KArgs, class... Args>
-cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args... args)
-{
-    cudaLaunchConfig_t cfg {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, args...);
-}
-
 // ------------------------------------------------------------------ 0-form
 
 template <class T>
