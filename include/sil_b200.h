@@ -195,10 +195,13 @@ size_t sil_laplacian_plan_scratch_bytes(sil_laplacian_plan plan);
  * 4 fused over stored general-metric Hodge tensors. */
 int sil_laplacian_plan_kernel(sil_laplacian_plan plan);
 /* Launch shape chosen by the autotuner on the plan's first run (-1 before
- * it): kernel 2's pipeline shape (6 candidates), kernel 1's block width (64,
- * 128 or 256 threads: 0, 1, 2).  The first run times each candidate on the
- * caller's fields and synchronises the stream once; SIMILIE_B200_AUTOTUNE=0
- * skips the tuning (kernel 2: shape 0, kernel 1: 256 threads),
+ * it): kernel 2's pipeline shape (9 candidates in FP64: 0-5 one column per
+ * thread, 6-8 column pairs; 6 in FP32), kernel 1's block width (64, 128 or
+ * 256 threads: 0, 1, 2).  The first run times each candidate on the
+ * caller's fields (kernel 2: from CUDA graphs of back-to-back launches) and
+ * synchronises the stream, so it must not be inside a stream capture: run
+ * a plan once before capturing it.  SIMILIE_B200_AUTOTUNE=0 skips the
+ * tuning (kernel 2: shape 0, kernel 1: 256 threads),
  * SIMILIE_B200_LAP1_VARIANT=<digit> forces kernel 2's shape. */
 int sil_laplacian_plan_variant(sil_laplacian_plan plan);
 /* Bound of each pipeline wait of kernel 2, in mbarrier polls (-1: the default,
