@@ -770,47 +770,77 @@ __global__ void __launch_bounds__(256) inc_forward_kernel(const __grid_constant_
         reinterpret_cast<float*>(w4[k])[co] = params[kOffIn + co * kTaps * 2 + k];
     }
     for (int i = threadIdx.x; i < kCh; i += blockDim.x) reinterpret_cast<float*>(b4)[i] = params[kOffIn + kInW + i];
-    walk_active(t, pre, 1, [&](int im, int g) {
+    // Two horizontally adjacent pixels per thread: their 3 x 3 windows share
+    // six of their nine taps, and each weight read from shared memory serves
+    // both; each pixel's sums keep the single-pixel order.
+    scan_active(
+        t.nimg,
+        [&](int k) { return image_active(t, k) ? (t.px_base[k + 1] - t.px_base[k] + 1) / 2 : int64_t(0); }, pre);
+    walk_range(pre, t.nimg, 1, [&](int im, int q) {
         Img const o = t.img[im];
         int const P = o.w + 2;
-        int const y = g / P, x = g - y * P;
-        uint4* dst = reinterpret_cast<uint4*>(out + (o.offset + g) * kCh);
-        if (y == 0 || x == 0 || y > o.h || x > o.w) {
+        int const npx = P * (o.h + 2);
+        int const g0 = 2 * q;
+        bool inside[2];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) dst[q] = make_uint4(0u, 0u, 0u, 0u);
-            return;
+        for (int u = 0; u < 2; ++u) {
+            int const g = g0 + u;
+            int const y = g / P, x = g - y * P;
+            inside[u] = g < npx && !(y == 0 || x == 0 || y > o.h || x > o.w);
         }
-        float in[kTaps * 2];
+        uint4* dst = reinterpret_cast<uint4*>(out + (o.offset + g0) * kCh);
         float2 const* f2 = reinterpret_cast<float2 const*>(feat) + o.offset;
+        // window columns g0-1 .. g0+2 of the rows above, at and below
+        float2 win[3][4];
 #pragma unroll
-        for (int tap = 0; tap < kTaps; ++tap) {
-            float2 const v = f2[g + (tap / 3 - 1) * P + (tap % 3 - 1)];
-            in[2 * tap] = v.x;
-            in[2 * tap + 1] = v.y;
-        }
+        for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                bool const need = (c < 3 && inside[0]) || (c > 0 && inside[1]);
+                win[dy][c] = need ? f2[g0 + (dy - 1) * P + (c - 1)] : make_float2(0.0f, 0.0f);
+            }
+        float in[2][kTaps * 2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int tap = 0; tap < kTaps; ++tap) {
+                float2 const v = win[tap / 3][tap % 3 + u];
+                in[u][2 * tap] = v.x;
+                in[u][2 * tap + 1] = v.y;
+            }
         // eight output channels at a time: bias, then the 18 inputs in order
 #pragma unroll 1
-        for (int q = 0; q < 4; ++q) {
-            float a[8];
-            float4 const b0 = b4[2 * q], b1 = b4[2 * q + 1];
-            a[0] = b0.x; a[1] = b0.y; a[2] = b0.z; a[3] = b0.w;
-            a[4] = b1.x; a[5] = b1.y; a[6] = b1.z; a[7] = b1.w;
+        for (int qq = 0; qq < 4; ++qq) {
+            float a[2][8];
+            float4 const b0 = b4[2 * qq], b1 = b4[2 * qq + 1];
 #pragma unroll
-            for (int k = 0; k < kTaps * 2; ++k) {
-                float const v = in[k];
-                float4 const w0 = w4[k][2 * q], w1 = w4[k][2 * q + 1];
-                a[0] = __fmaf_rn(w0.x, v, a[0]);
-                a[1] = __fmaf_rn(w0.y, v, a[1]);
-                a[2] = __fmaf_rn(w0.z, v, a[2]);
-                a[3] = __fmaf_rn(w0.w, v, a[3]);
-                a[4] = __fmaf_rn(w1.x, v, a[4]);
-                a[5] = __fmaf_rn(w1.y, v, a[5]);
-                a[6] = __fmaf_rn(w1.z, v, a[6]);
-                a[7] = __fmaf_rn(w1.w, v, a[7]);
+            for (int u = 0; u < 2; ++u) {
+                a[u][0] = b0.x; a[u][1] = b0.y; a[u][2] = b0.z; a[u][3] = b0.w;
+                a[u][4] = b1.x; a[u][5] = b1.y; a[u][6] = b1.z; a[u][7] = b1.w;
             }
 #pragma unroll
-            for (int i = 0; i < 8; ++i) a[i] = fmaxf(a[i], 0.0f);
-            dst[q] = pack8(a);
+            for (int k = 0; k < kTaps * 2; ++k) {
+                float4 const w0 = w4[k][2 * qq], w1 = w4[k][2 * qq + 1];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    float const v = in[u][k];
+                    a[u][0] = __fmaf_rn(w0.x, v, a[u][0]);
+                    a[u][1] = __fmaf_rn(w0.y, v, a[u][1]);
+                    a[u][2] = __fmaf_rn(w0.z, v, a[u][2]);
+                    a[u][3] = __fmaf_rn(w0.w, v, a[u][3]);
+                    a[u][4] = __fmaf_rn(w1.x, v, a[u][4]);
+                    a[u][5] = __fmaf_rn(w1.y, v, a[u][5]);
+                    a[u][6] = __fmaf_rn(w1.z, v, a[u][6]);
+                    a[u][7] = __fmaf_rn(w1.w, v, a[u][7]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (g0 + u >= npx) continue;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) a[u][i] = inside[u] ? fmaxf(a[u][i], 0.0f) : 0.0f;
+                dst[u * kChunks + qq] = pack8(a[u]);
+            }
         }
     });
 }
@@ -1963,7 +1993,8 @@ sil_status net_forward(Net& net, Workspace& w, cudaStream_t st, bool keep)
     int* err = net.error_flag;
     {
         Table const t = w.table(0, -1, false);
-        inc_forward_kernel<<<walk_grid(t, 1, kWalkInc), 256, 0, st>>>(t, w.feat.as<float>(), net.params, w.h[0].as<bf16>());
+        inc_forward_kernel<<<(walk_grid(t, 1, kWalkInc) + 1) / 2, 256, 0, st>>>(t, w.feat.as<float>(), net.params,
+                                                                              w.h[0].as<bf16>());
         SIL_CUDA_CHECK(cudaGetLastError());
     }
     for (int l = 1; l < D; ++l) {
